@@ -1,0 +1,167 @@
+"""ctypes access to the CPU oracle libraries (test infrastructure only).
+
+Two libraries share one calling convention:
+  * oracle/liboracle.so      - the C++ restatement in oracle/pt_oracle.cpp (prefix ``orc_``)
+  * oracle/_ref/libptref.so  - the unmodified reference sources + oracle/ref_shim.cpp (prefix ``ref_``)
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import this module, as the checker.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libptref.so")
+COLS = 18
+
+_u16p = ctypes.POINTER(ctypes.c_uint16)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_u64 = ctypes.c_uint64
+_f64 = ctypes.c_double
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t)
+
+
+class CpuLib:
+    """One of the two CPU libraries; ``prefix`` selects the symbol family."""
+
+    def __init__(self, path, prefix):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.path = path
+        self.lib = ctypes.CDLL(path)
+        self.prefix = prefix
+        L = self.lib
+        self._loc = getattr(L, prefix + "Localization")
+        self._loc.restype = _u64
+        self._loc.argtypes = [_u16p, _f64p, _u64, _u64, _u64, _u64, _f64, _f64, _u64, _f64p]
+        self._fit = getattr(L, prefix + "Fitting")
+        self._fit.restype = _u64
+        self._fit.argtypes = [_u16p, _f64p, _u64, _f64p, _u64, _u64, _u64, _u64, _u64, _f64p]
+        self._wav = getattr(L, prefix + "Wavelett")
+        self._wav.restype = None
+        self._wav.argtypes = [_u16p, _f64p, _u64, _u64, _u64, _u64]
+        self._thr = getattr(L, prefix + "AutoThreshold")
+        self._thr.restype = _f64
+        self._thr.argtypes = [_u16p, _u64, _u64, _f64p]
+        self._planes = getattr(L, prefix + "Planes")
+        self._planes.restype = None
+        self._planes.argtypes = [_u16p, _u64, _u64, _f64p]
+        self._cand = getattr(L, prefix + "Candidates")
+        self._cand.restype = _u64
+        self._cand.argtypes = [_u16p, _u64, _u64, _f64, _f64, _f64p, _u64]
+        self._candp = getattr(L, prefix + "CandidatesFromPotential")
+        self._candp.restype = _u64
+        self._candp.argtypes = [_f64p, _u64, _u64, _f64, _f64, _f64p, _u64]
+        self._threads = getattr(L, prefix + "SetThreads")
+        self._threads.restype = None
+        self._threads.argtypes = [ctypes.c_int]
+
+    def set_threads(self, n):
+        self._threads(int(n))
+
+    def localization(self, stack, thr, ratio, fit, params, capacity_doubles=None):
+        stack = np.ascontiguousarray(stack, dtype=np.uint16)
+        if stack.ndim == 2:
+            stack = stack[None]
+        z, h, w = stack.shape
+        if capacity_doubles is None:
+            capacity_doubles = ((h * w) // 5 + 1) * z * COLS
+        out = np.full(max(capacity_doubles, 1), -12345.0)
+        params = np.ascontiguousarray(params, dtype=np.float64)
+        n = self._loc(_ptr(stack, _u16p), _ptr(out, _f64p), capacity_doubles, h, w, z, thr, ratio, fit, _ptr(params, _f64p))
+        return out[:n].reshape(-1, COLS).copy()
+
+    def fitting(self, stack, positions, fit, params):
+        stack = np.ascontiguousarray(stack, dtype=np.uint16)
+        if stack.ndim == 2:
+            stack = stack[None]
+        z, h, w = stack.shape
+        positions = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 6)
+        n = positions.shape[0]
+        out = np.zeros(max(n, 1) * COLS)
+        params = np.ascontiguousarray(params, dtype=np.float64)
+        k = self._fit(_ptr(stack, _u16p), _ptr(positions, _f64p), n, _ptr(out, _f64p), out.size, h, w, z, fit, _ptr(params, _f64p))
+        return out[:k].reshape(-1, COLS).copy()
+
+    def wavelett(self, stack, level):
+        stack = np.ascontiguousarray(stack, dtype=np.uint16)
+        if stack.ndim == 2:
+            stack = stack[None]
+        z, h, w = stack.shape
+        out = np.zeros((z, h, w))
+        self._wav(_ptr(stack, _u16p), _ptr(out, _f64p), h, w, z, level)
+        return out
+
+    def auto_threshold(self, frame, params):
+        frame = np.ascontiguousarray(frame, dtype=np.uint16)
+        h, w = frame.shape[-2:]
+        params = np.ascontiguousarray(params, dtype=np.float64)
+        return self._thr(_ptr(frame, _u16p), h, w, _ptr(params, _f64p))
+
+    def planes(self, frame):
+        frame = np.ascontiguousarray(frame, dtype=np.uint16)
+        h, w = frame.shape
+        out = np.zeros((3, h, w))
+        self._planes(_ptr(frame, _u16p), h, w, _ptr(out, _f64p))
+        return out
+
+    def candidates(self, frame, thr, ratio):
+        frame = np.ascontiguousarray(frame, dtype=np.uint16)
+        h, w = frame.shape
+        cap = h * w // 4 + 16
+        rows = np.zeros((cap, 4))
+        n = self._cand(_ptr(frame, _u16p), h, w, thr, ratio, _ptr(rows, _f64p), cap)
+        return rows[:min(n, cap)].copy()
+
+    def candidates_from_potential(self, potential, thr, ratio):
+        potential = np.ascontiguousarray(potential, dtype=np.float64)
+        h, w = potential.shape
+        cap = h * w // 4 + 16
+        rows = np.zeros((cap, 4))
+        n = self._candp(_ptr(potential, _f64p), h, w, thr, ratio, _ptr(rows, _f64p), cap)
+        return rows[:min(n, cap)].copy()
+
+
+class OracleLib(CpuLib):
+    def __init__(self, path=ORACLE_SO):
+        super().__init__(path, "orc_")
+        self._labels = self.lib.orc_Labels
+        self._labels.restype = _u64
+        self._labels.argtypes = [_u16p, _u64, _u64, _f64, _f64, _u32p]
+
+    def labels(self, frame, thr, ratio):
+        frame = np.ascontiguousarray(frame, dtype=np.uint16)
+        h, w = frame.shape
+        out = np.zeros((h, w), dtype=np.uint32)
+        self._labels(_ptr(frame, _u16p), h, w, thr, ratio, _ptr(out, _u32p))
+        return out
+
+
+class RefLib(CpuLib):
+    def __init__(self, path=REF_SO):
+        super().__init__(path, "ref_")
+        self._astig = self.lib.ref_Astig3DEstimation
+        self._astig.restype = None
+        self._astig.argtypes = [_f64p, _f64p, _u64, _f64, _f64p, _f64]
+
+    def astig_estimation(self, sigmas, pixel_size, model, zmax):
+        sigmas = np.ascontiguousarray(sigmas, dtype=np.float64).reshape(-1, 2)
+        out = np.zeros_like(sigmas)
+        model = np.ascontiguousarray(model, dtype=np.float64)
+        self._astig(_ptr(sigmas, _f64p), _ptr(out, _f64p), sigmas.shape[0], pixel_size, _ptr(model, _f64p), zmax)
+        return out
+
+
+def oracle():
+    return OracleLib()
+
+
+def reference():
+    """The reference built from source, or None when oracle/_ref has not been built."""
+    return RefLib() if os.path.exists(REF_SO) else None

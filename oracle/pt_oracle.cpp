@@ -1,0 +1,1144 @@
+// PALMTracer localization hot path: CPU restatement used as the ORACLE (test infrastructure only).
+//
+// Only tests/, the smoke check and the bench's CPU-baseline leg load this library, and only as the checker.
+// The product (palmtracer-cpp_b200/) neither links nor calls anything here.
+//
+// Every function restates the reference algorithm (tmonseigne/PALMTracer-cpp 1.3.0) in FP64 with the same
+// order of floating-point operations where the result depends on it, so that its outputs can be pinned
+// BIT FOR BIT against the reference built from source (oracle/_ref) and against the reference's own golden
+// CSVs (Tests_CPU/Input/ref/*.csv). Build flags follow the reference's strict mode (-ffp-contract=off).
+//
+// Entry points (extern "C", prefix orc_):
+//   orc_Localization / orc_Fitting / orc_Wavelett / orc_AutoThreshold  - the four C-ABI exports
+//   orc_Planes, orc_Candidates, orc_CandidatesFromPotential, orc_Labels - per-stage products
+#include <omp.h>
+
+#include <algorithm>
+#include <array>
+#include <cfloat>
+#include <cmath>
+#include <compare>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <numbers>
+#include <queue>
+#include <vector>
+
+namespace {
+
+// ---------------------------------------------------------------------------------------------
+// Constants (lib/Constants.hpp:20-24, 53; lib/localization/Segmentation2D.hpp:80; lib/fit/Fitting.hpp:80)
+constexpr int kPlaneId = 1;            // wavelet plane used for detection
+constexpr int kNumPlanes = 3;          // detail planes W0, W1 and the residual V2
+constexpr double kVolumeMin = 4;       // regions need surf > 4
+constexpr int kThresholdIters = 5;     // AutoThreshold iterations
+constexpr double kEps = 1e-7;          // EPSILON: watershed aging step and fill() guards
+constexpr double kSeedFloor = 1e-8;    // Segmentation2D::THRESHOLD
+constexpr int kMaxIter = 75;           // Fitting::N_ITER
+constexpr int kCols = 18;              // localization_columns::Count
+
+enum Col { cId = 0, cPlane, cIndex, cChannel, cX, cY, cZ, cIntensity, cSigmaX, cSigmaY, cTheta,
+           cQualityXY, cQualityZ, cAmplitude, cOffset, cSegIntensity, cSurface, cCircularity };
+
+// Fit modes (lib/fit/Fitting.hpp:22-30)
+enum Mode { kNone = 0, kG2Fixed = 1, kG2Sigma = 2, kG3Fixed = 3, kG3Theta = 4, kSplineEmccd = 5 };
+
+struct Candidate {  // lib/localization/SegmentationInfo.hpp:32-71 (only the fields that leave Segmentation2D)
+	double x = 0, y = 0, z = 0, intensity = 0, surf = 0;
+};
+
+using Row = std::array<double, kCols>;
+
+// ---------------------------------------------------------------------------------------------
+// A trous B3 wavelet (lib/localization/ATrous.cpp:23-38, 49-80).
+// V0 = image; V(k+1) = column pass of (row pass of Vk) with taps 3/8, 1/4, 1/16 at offsets 0, +-2^k, +-2^(k+1),
+// each pass clamping its coordinate into the image; W(k) = Vk - V(k+1); the last plane keeps the residual.
+void Atrous(const uint16_t* img, int H, int W, std::vector<double> planes[kNumPlanes])
+{
+	const size_t n = static_cast<size_t>(H) * W;
+	for (int k = 0; k < kNumPlanes; ++k) { planes[k].assign(n, 0.0); }
+	std::vector<double> tmp(n);
+	for (size_t i = 0; i < n; ++i) { planes[0][i] = static_cast<double>(img[i]); }
+	const double h0 = 3.0 / 8.0, h1 = 1.0 / 4.0, h2 = 1.0 / 16.0;
+	auto cx = [W](int x) { return std::clamp(x, 0, W - 1); };
+	auto cy = [H](int y) { return std::clamp(y, 0, H - 1); };
+	for (int k = 0; k < kNumPlanes - 1; ++k) {
+		const int s = 1 << k, s2 = 2 * s;
+		const std::vector<double>& in = planes[k];
+		std::vector<double>& out = planes[k + 1];
+		for (int y = 0; y < H; ++y) {
+			const double* r = in.data() + static_cast<size_t>(y) * W;
+			for (int x = 0; x < W; ++x) {
+				tmp[static_cast<size_t>(y) * W + x] = (h0 * r[x]) + (h1 * (r[cx(x - s)] + r[cx(x + s)])) + (h2 * (r[cx(x - s2)] + r[cx(x + s2)]));
+			}
+		}
+		for (int y = 0; y < H; ++y) {
+			for (int x = 0; x < W; ++x) {
+				auto at = [&](int yy) { return tmp[static_cast<size_t>(cy(yy)) * W + x]; };
+				out[static_cast<size_t>(y) * W + x] = (h0 * tmp[static_cast<size_t>(y) * W + x]) + (h1 * (at(y - s) + at(y + s))) + (h2 * (at(y - s2) + at(y + s2)));
+			}
+		}
+		std::vector<double>& detail = planes[k];
+		for (size_t i = 0; i < n; ++i) { detail[i] -= out[i]; }
+	}
+}
+
+// ---------------------------------------------------------------------------------------------
+// Segmentation (lib/localization/Segmentation2D.cpp).
+struct Segmenter {
+	int H = 0, W = 0;
+	double ratio = 0;
+	std::vector<double> pot;        // thresholded potential ("output_")
+	std::vector<uint32_t> lab;      // label map ("map_")
+	std::vector<Candidate> cands;   // per label ("infos_")
+
+	size_t at(int y, int x) const { return static_cast<size_t>(y) * W + x; }
+
+	// Strict threshold of plane 1 (Segmentation2D.cpp:50-74, comparison at :62).
+	void Run(const double* plane1, int h, int w, double thr, double r)
+	{
+		H = h; W = w; ratio = r;
+		const size_t n = static_cast<size_t>(H) * W;
+		pot.assign(n, 0.0);
+		lab.assign(n, 0);
+		cands.clear();
+		for (size_t i = 0; i < n; ++i) { pot[i] = plane1[i] > thr ? plane1[i] : 0.0; }
+		Seeds();
+		Flood();
+		if (static_cast<int>(ratio) > 0) {  // WatershedIntelligent, Segmentation2D.cpp:77-85
+			Fuse();
+			Flood();
+		}
+		Statistics();
+		Filter();
+	}
+
+	// Local maxima (Segmentation2D.cpp:294-333): v > 1e-8 and no 8-neighbour strictly greater. A maximum that touches an
+	// already-labelled raster predecessor takes the first such label in 3x3 scan order; otherwise it opens a new label.
+	void Seeds()
+	{
+		std::fill(lab.begin(), lab.end(), 0u);
+		uint32_t next = 1;
+		for (int i = 0; i < H; ++i) {
+			for (int j = 0; j < W; ++j) {
+				const double v = pot[at(i, j)];
+				if (!(v > kSeedFloor)) { continue; }
+				bool dominated = false;
+				for (int ii = std::max(i - 1, 0); ii <= std::min(i + 1, H - 1) && !dominated; ++ii) {
+					for (int jj = std::max(j - 1, 0); jj <= std::min(j + 1, W - 1) && !dominated; ++jj) {
+						if ((ii != i || jj != j) && v < pot[at(ii, jj)]) { dominated = true; }
+					}
+				}
+				if (dominated) { continue; }
+				uint32_t inherit = 0;
+				for (int ii = std::max(i - 1, 0); ii <= std::min(i + 1, H - 1) && inherit == 0; ++ii) {
+					for (int jj = std::max(j - 1, 0); jj <= std::min(j + 1, W - 1) && inherit == 0; ++jj) {
+						if ((ii != i || jj != j) && lab[at(ii, jj)] > 0) { inherit = lab[at(ii, jj)]; }
+					}
+				}
+				lab[at(i, j)] = inherit > 0 ? inherit : next++;
+			}
+		}
+		cands.assign(next - 1, Candidate{});
+	}
+
+	// Priority flood (Segmentation2D.cpp:336-385). Heap order is std::priority_queue with the reference's Pixel
+	// comparison (lib/Structs.hpp:20-27: a < b iff a.v > b.v), so equal keys resolve exactly as in the reference.
+	struct HeapPx {
+		size_t x, y;  // x = row, y = column (reference naming)
+		double v;
+		bool operator<(const HeapPx& o) const { return v > o.v; }
+	};
+
+	void Flood()
+	{
+		std::priority_queue<HeapPx> heap;
+		for (int x = 0; x < H; ++x) {
+			for (int y = 0; y < W; ++y) {
+				if (lab[at(x, y)] == 0) { continue; }
+				bool open = false;
+				for (int dx = -1; dx <= 1 && !open; ++dx) {
+					const int nx = x + dx;
+					if (nx < 0 || nx >= H) { continue; }
+					for (int dy = -1; dy <= 1 && !open; ++dy) {
+						const int ny = y + dy;
+						if ((dx == 0 && dy == 0) || ny < 0 || ny >= W) { continue; }
+						if (lab[at(nx, ny)] == 0) { open = true; }
+					}
+				}
+				if (open) { heap.push(HeapPx{static_cast<size_t>(x), static_cast<size_t>(y), -pot[at(x, y)]}); }
+			}
+		}
+		size_t pops = 0;
+		while (!heap.empty()) {
+			const HeapPx p = heap.top();
+			heap.pop();
+			++pops;
+			for (int dx = -1; dx <= 1; ++dx) {
+				const int nx = static_cast<int>(p.x) + dx;
+				if (nx < 0 || nx >= H) { continue; }
+				for (int dy = -1; dy <= 1; ++dy) {
+					const int ny = static_cast<int>(p.y) + dy;
+					if ((dx == 0 && dy == 0) || ny < 0 || ny >= W) { continue; }
+					const size_t q = at(nx, ny);
+					if (pot[q] > kSeedFloor && lab[q] == 0) {
+						const double key = -pot[q] + (static_cast<double>(pops) * kEps);
+						heap.push(HeapPx{static_cast<size_t>(nx), static_cast<size_t>(ny), key});
+						lab[q] = lab[at(static_cast<int>(p.x), static_cast<int>(p.y))];
+					}
+				}
+			}
+		}
+	}
+
+	// Basin fusion (Segmentation2D.cpp:181-291): repeat until stable; a basin whose relative boundary contrast is below
+	// `ratio` merges into its strongest-boundary neighbour when that neighbour peaks higher; one seed per basin remains.
+	struct Basin {
+		double maxWithNeighbour, minPot, maxPot;
+		uint32_t row, col, neighbour, become, newIndex;
+		bool locked;
+	};
+
+	void Fuse()
+	{
+		std::vector<Basin> b(cands.size());
+		if (b.empty()) { return; }
+		bool change = true;
+		uint32_t count = 0;
+		while (change) {
+			change = false;
+			for (size_t i = 0; i < b.size(); ++i) {
+				b[i].maxWithNeighbour = -1e10;
+				b[i].minPot = +1e10;
+				b[i].maxPot = -1e10;
+				b[i].neighbour = 0;
+				b[i].locked = false;
+				b[i].become = static_cast<uint32_t>(i);
+				b[i].newIndex = 0;
+			}
+			for (int i = 0; i < H; ++i) {
+				for (int j = 0; j < W; ++j) {
+					const uint32_t s = lab[at(i, j)];
+					if (s == 0) { continue; }
+					Basin& r = b[s - 1];
+					const double v = pot[at(i, j)];
+					r.minPot = std::min(r.minPot, v);
+					if (v > r.maxPot) {
+						r.maxPot = v;
+						r.row = static_cast<uint32_t>(i);
+						r.col = static_cast<uint32_t>(j);
+					}
+					for (int ii = std::max(i - 1, 0); ii <= std::min(i + 1, H - 1); ++ii) {
+						for (int jj = std::max(j - 1, 0); jj <= std::min(j + 1, W - 1); ++jj) {
+							if (ii == i && jj == j) { continue; }
+							const uint32_t ns = lab[at(ii, jj)];
+							if (ns != 0 && ns != s && v > r.maxWithNeighbour) {
+								r.maxWithNeighbour = v;
+								r.neighbour = ns;
+							}
+						}
+					}
+				}
+			}
+			for (size_t i = 0; i < b.size(); ++i) {
+				Basin& r = b[i];
+				if (r.neighbour == 0) { continue; }
+				const size_t ni = r.neighbour - 1;
+				if (r.locked || b[ni].locked) { continue; }
+				const double delta = r.maxPot - r.minPot;
+				if (std::abs(delta) <= DBL_EPSILON) { continue; }
+				if ((r.maxPot - r.maxWithNeighbour) / delta < ratio && r.maxPot < b[ni].maxPot) {
+					r.become = static_cast<uint32_t>(ni);
+					b[ni].locked = true;
+					r.locked = true;
+					change = true;
+				}
+			}
+			count = 0;
+			for (size_t i = 0; i < b.size(); ++i) { if (b[i].become == i) { b[i].newIndex = ++count; } }
+			for (uint32_t& s : lab) { if (s != 0) { s = b[b[s - 1].become].newIndex; } }
+			b.resize(count);
+		}
+		cands.assign(count, Candidate{});
+		std::fill(lab.begin(), lab.end(), 0u);
+		for (size_t i = 0; i < b.size(); ++i) {
+			if (b[i].become == i) { lab[at(static_cast<int>(b[i].row), static_cast<int>(b[i].col))] = b[i].newIndex; }
+		}
+	}
+
+	// Region statistics in raster order (Segmentation2D.cpp:144-175); only surf, intensity and the centroid leave.
+	void Statistics()
+	{
+		std::vector<double> sum(cands.size(), 0.0);
+		for (auto& c : cands) { c = Candidate{}; }
+		for (int i = 0; i < H; ++i) {
+			for (int j = 0; j < W; ++j) {
+				const uint32_t s = lab[at(i, j)];
+				if (s == 0) { continue; }
+				Candidate& c = cands[s - 1];
+				const double v = pot[at(i, j)];
+				c.surf += 1;
+				c.x += v * static_cast<double>(j);
+				c.y += v * static_cast<double>(i);
+				sum[s - 1] += v;
+			}
+		}
+		for (size_t k = 0; k < cands.size(); ++k) {
+			Candidate& c = cands[k];
+			if (static_cast<int>(c.surf) == 0) { continue; }
+			c.x /= sum[k];
+			c.y /= sum[k];
+			c.intensity = sum[k];
+		}
+	}
+
+	// Keep regions with surf > VOLUME_MIN, in label order (Segmentation2D.cpp:88-141; filter table :20-39).
+	void Filter()
+	{
+		std::vector<Candidate> kept;
+		kept.reserve(cands.size());
+		for (const auto& c : cands) { if (!(c.surf <= kVolumeMin)) { kept.push_back(c); } }
+		cands.swap(kept);
+	}
+};
+
+// ---------------------------------------------------------------------------------------------
+// Gauss-Jordan inverse with row equilibration and partial pivoting (lib/signal_processing/Matrix.cpp:297-355).
+// Returns false where the reference throws std::domain_error.
+bool InvertGaussJordan(std::vector<double>& a, std::vector<double>& inv, int n)
+{
+	std::fill(inv.begin(), inv.end(), 0.0);
+	for (int i = 0; i < n; ++i) {
+		double scale = 0.0;
+		for (int j = 0; j < n; ++j) {
+			const double v = a[i * n + j];
+			if (!std::isfinite(v)) { return false; }
+			scale = std::max(scale, std::abs(v));
+		}
+		if (scale == 0.0) { return false; }
+		for (int j = 0; j < n; ++j) { a[i * n + j] /= scale; }
+		inv[i * n + i] = 1.0 / scale;
+	}
+	const double tol = std::numeric_limits<double>::epsilon() * static_cast<double>(n);
+	for (int i = 0; i < n; ++i) {
+		int piv = i;
+		for (int j = i + 1; j < n; ++j) { if (std::abs(a[j * n + i]) > std::abs(a[piv * n + i])) { piv = j; } }
+		if (!std::isfinite(a[piv * n + i]) || std::abs(a[piv * n + i]) <= tol) { return false; }
+		if (piv != i) {
+			for (int j = 0; j < n; ++j) {
+				std::swap(a[i * n + j], a[piv * n + j]);
+				std::swap(inv[i * n + j], inv[piv * n + j]);
+			}
+		}
+		const double pinv = 1.0 / a[i * n + i];
+		for (int j = 0; j < n; ++j) {
+			a[i * n + j] *= pinv;
+			inv[i * n + j] *= pinv;
+		}
+		for (int j = 0; j < n; ++j) {
+			if (j == i) { continue; }
+			const double f = a[j * n + i];
+			for (int k = 0; k < n; ++k) {
+				a[j * n + k] -= f * a[i * n + k];
+				inv[j * n + k] -= f * inv[i * n + k];
+			}
+		}
+	}
+	for (double v : a) { if (!std::isfinite(v)) { return false; } }
+	for (double v : inv) { if (!std::isfinite(v)) { return false; } }
+	return true;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Output row fill (lib/fit/Fitting.cpp:61-106).
+void FillRow(int mode, const Candidate& c, Row& r, double x, double y, double z, double offset = -1, double amp = -1,
+             double sx = -1, double sy = -1, double theta = -1, double qxy = -1, double qz = -1)
+{
+	r[cId] = 0; r[cPlane] = 0; r[cIndex] = 0; r[cChannel] = -1;
+	r[cX] = x; r[cY] = y; r[cZ] = z;
+	if (mode == kNone) { r[cIntensity] = c.intensity; }
+	else if (mode == kSplineEmccd) { r[cIntensity] = amp; }
+	else { r[cIntensity] = (amp > kEps && sx > kEps && sy > kEps) ? 2.0 * std::numbers::pi * amp * sx * sy : -1; }
+	r[cSigmaX] = sx; r[cSigmaY] = sy; r[cTheta] = theta;
+	r[cQualityXY] = qxy; r[cQualityZ] = qz;
+	r[cAmplitude] = amp; r[cOffset] = offset;
+	r[cSegIntensity] = c.intensity; r[cSurface] = c.surf;
+	r[cCircularity] = (sx > kEps && sy > kEps) ? std::min(sx, sy) / std::max(sx, sy) : 1;
+}
+
+// Shared per-fit configuration (lib/fit/Fitting.cpp:14-40; GaussianFit.cpp:39-45).
+struct FitConfig {
+	int mode = kNone, nParams = 4, roi = 0, half = 0, n = 0;
+	double sigmaX = 1, sigmaY = 2, theta = 0;
+	int W = 0, H = 0;
+	const uint16_t* img = nullptr;
+
+	void Init(int m, const double* fp, const uint16_t* image, int w, int h)
+	{
+		mode = m; img = image; W = w; H = h;
+		switch (mode) {
+			case kG2Sigma: nParams = 5; break;
+			case kG3Fixed: nParams = 6; break;
+			case kG3Theta: nParams = 7; break;
+			case kSplineEmccd: nParams = 5; break;
+			default: nParams = 4; break;
+		}
+		roi = static_cast<int>(static_cast<size_t>(fp[0]));
+		if (mode >= kG2Fixed && mode <= kG3Theta) { sigmaX = fp[1]; sigmaY = fp[2]; theta = fp[3]; }
+		if (roi % 2 == 0) { roi--; }
+		half = roi / 2;
+		n = roi * roi;
+	}
+
+	// ROI inside the image? (GaussianFit.cpp:51-56; unsigned comparisons as in the reference)
+	bool Inside(size_t ux, size_t uy) const
+	{
+		const size_t h = static_cast<size_t>(half);
+		return !(h > ux || ux >= static_cast<size_t>(W) - h || h > uy || uy >= static_cast<size_t>(H) - h);
+	}
+};
+
+// Gaussian PSF value and gradient at offset (x, y) from the centre (lib/fit/GaussianModel.cpp:19-52).
+struct GaussModel {
+	double off, amp, sx, sy, sx2, sy2, c, s, c2, s2, cs;
+	bool iso, hasSigma, hasTheta;
+
+	static GaussModel Make(int mode, const double* p, double sigma, double theta)
+	{
+		GaussModel m{};
+		m.off = p[0]; m.amp = p[1];
+		if (mode == kG2Fixed || mode == kG2Sigma) {
+			const double sg = mode == kG2Fixed ? sigma : p[4];
+			m.sx = m.sy = sg; m.sx2 = m.sy2 = sg * sg;
+			m.c = 1; m.s = 0; m.c2 = 1; m.s2 = 0; m.cs = 0;
+			m.iso = true; m.hasSigma = mode == kG2Sigma; m.hasTheta = false;
+		}
+		else {
+			const double th = mode == kG3Fixed ? theta : p[6];
+			m.sx = p[4]; m.sy = p[5]; m.sx2 = p[4] * p[4]; m.sy2 = p[5] * p[5];
+			m.c = std::cos(th); m.s = std::sin(th); m.c2 = m.c * m.c; m.s2 = m.s * m.s; m.cs = m.c * m.s;
+			m.iso = false; m.hasSigma = false; m.hasTheta = mode == kG3Theta;
+		}
+		return m;
+	}
+
+	double Eval(double x, double y, double* g) const
+	{
+		const double X2 = x * x, Y2 = y * y;
+		if (iso) {
+			const double e = std::exp(-(X2 + Y2) / (2 * sx2));
+			const double P = amp * e;
+			if (g) {
+				g[0] = 1; g[1] = e; g[2] = P * x / sx2; g[3] = P * y / sx2;
+				if (hasSigma) { g[4] = P / (sx * sx2) * (X2 + Y2); }
+			}
+			return P + off;
+		}
+		const double xc = x * c, xs = x * s, yc = y * c, ys = y * s;
+		const double f1 = (xc - ys) / sx, f2 = (xs + yc) / sy;
+		const double e = std::exp(-((f1 * f1) + (f2 * f2)));
+		const double P = amp * e;
+		if (g) {
+			const double xy = x * y, f3 = 2 * xy * cs, f4 = (2 * xy / sx2) - (2 * xy / sy2);
+			g[0] = 1; g[1] = e;
+			g[2] = P * (-(((-2 * c2 * x) + (2 * y * cs)) / sx2) - (((-2 * s2 * x) - (2 * y * cs)) / sy2));
+			g[3] = P * ((((2 * s2 * y) - (2 * x * cs)) / sx2) - (((-2 * c2 * y) - (2 * x * cs)) / sy2));
+			g[4] = P * (2 * ((xc * xc) - f3 + (ys * ys)) / (sx * sx2));
+			g[5] = P * (2 * ((xs * xs) + f3 + (yc * yc)) / (sy * sy2));
+			if (hasTheta) { g[6] = P * ((2 * cs * (((X2 - Y2) / sx2) + ((Y2 - X2) / sy2))) - (s2 * f4) + (c2 * f4)); }
+		}
+		return P + off;
+	}
+};
+
+// Unweighted least-squares Levenberg-Marquardt (lib/fit/GaussianFit.cpp:48-295).
+void FitGaussian(const FitConfig& cf, const Candidate& c, Row& out)
+{
+	const size_t ux = static_cast<size_t>(c.x), uy = static_cast<size_t>(c.y);
+	if (!cf.Inside(ux, uy)) { FillRow(cf.mode, c, out, c.x, c.y, c.z); return; }
+	const int np = cf.nParams, n = cf.n, h = cf.half;
+	std::vector<double> gx(n), gy(n), gv(n), hat(n);
+	double vmin = std::numeric_limits<double>::max(), vmax = std::numeric_limits<double>::lowest();
+	for (int i = -h; i <= h; ++i) {  // ROI gather, Fitting.cpp:109-123
+		for (int j = -h; j <= h; ++j) {
+			const int k = (i + h) * cf.roi + (j + h);
+			gx[k] = static_cast<double>(ux + j);
+			gy[k] = static_cast<double>(uy + i);
+			gv[k] = static_cast<double>(cf.img[(ux + j) + (uy + i) * static_cast<size_t>(cf.W)]);
+			vmin = std::min(vmin, gv[k]);
+			vmax = std::max(vmax, gv[k]);
+		}
+	}
+	// Initial parameters and bounds (Fitting.cpp:126-175)
+	double lo[7], p[7], hi[7];
+	const double r2 = std::numbers::sqrt2_v<double>;
+	lo[0] = 0; lo[1] = 0; lo[2] = c.x - 1; lo[3] = c.y - 1;
+	p[0] = vmin; p[1] = vmax - vmin; p[2] = c.x; p[3] = c.y;
+	hi[0] = 65535; hi[1] = 65535; hi[2] = c.x + 1; hi[3] = c.y + 1;
+	if (cf.mode == kG2Sigma) { lo[4] = 0.1; p[4] = cf.sigmaX; hi[4] = 20; }
+	if (cf.mode == kG3Fixed || cf.mode == kG3Theta) {
+		lo[4] = lo[5] = 0.1; hi[4] = hi[5] = 20;
+		p[4] = r2 * cf.sigmaX; p[5] = r2 * cf.sigmaY;
+	}
+	if (cf.mode == kG3Theta) { lo[6] = -150; p[6] = cf.theta; hi[6] = 150; }
+
+	std::vector<double> alpha(np * np), alphaR(np * np), alphaRi(np * np);
+	double beta[7], dp[7], pTry[7], grad[7];
+
+	auto evalNormal = [&]() {  // GaussianFit.cpp:219-245
+		std::fill(alpha.begin(), alpha.end(), 0.0);
+		std::fill(beta, beta + np, 0.0);
+		double err = 0.0;
+		const GaussModel m = GaussModel::Make(cf.mode, p, cf.sigmaX, cf.theta);
+		const bool circular = cf.mode == kG3Theta && std::abs(p[4] - p[5]) <= std::numeric_limits<double>::epsilon();
+		for (int i = 0; i < n; ++i) {
+			hat[i] = m.Eval(gx[i] - p[2], gy[i] - p[3], grad);
+			const double d = gv[i] - hat[i];
+			const double dw = 1.0 * d;
+			err += d * dw;
+			if (circular) { grad[6] = 0.0; }
+			for (int a = 0; a < np; ++a) {
+				beta[a] += grad[a] * dw;
+				for (int b = 0; b < np; ++b) { alpha[a * np + b] += 1.0 * grad[a] * grad[b]; }
+			}
+		}
+		return err;
+	};
+	auto trialError = [&]() {  // GaussianFit.cpp:262-271
+		double res = 0.0;
+		const GaussModel m = GaussModel::Make(cf.mode, pTry, cf.sigmaX, cf.theta);
+		for (int i = 0; i < n; ++i) {
+			const double d = gv[i] - m.Eval(gx[i] - pTry[2], gy[i] - pTry[3], nullptr);
+			res += 1.0 * d * d;
+		}
+		return res;
+	};
+	auto maxAbsBeta = [&]() { double m = 0; for (int i = 0; i < np; ++i) { m = std::max(m, std::abs(beta[i])); } return m; };
+	auto relStep = [&]() {
+		double m = 0.0;
+		for (int i = 0; i < np; ++i) { m = std::max(m, std::abs(dp[i]) / std::max(std::abs(p[i]), 1e-12)); }
+		return m;
+	};
+
+	double err = evalNormal();
+	bool finite = std::isfinite(err);
+	for (int i = 0; i < np; ++i) { finite = finite && std::isfinite(beta[i]); }
+	if (!finite) { FillRow(cf.mode, c, out, c.x, c.y, c.z); return; }
+	double lambda = 1e-2;
+	double m = maxAbsBeta();
+	for (int it = (m < 1e-6) ? kMaxIter : 0; it < kMaxIter; ++it) {
+		alphaR = alpha;
+		for (int i = 0; i < np; ++i) {
+			const int d = i * np + i;
+			alphaR[d] = alpha[d] == 0.0 ? 1.0 : (1.0 + lambda) * alpha[d];
+		}
+		if (!InvertGaussJordan(alphaR, alphaRi, np)) {
+			if (lambda < 1e7) { lambda = std::min(lambda * 11, 1e7); continue; }
+			FillRow(cf.mode, c, out, c.x, c.y, c.z);
+			return;
+		}
+		for (int i = 0; i < np; ++i) {
+			dp[i] = 0.0;
+			for (int j = 0; j < np; ++j) { dp[i] += alphaRi[i * np + j] * beta[j]; }
+			if (!std::isfinite(dp[i])) { FillRow(cf.mode, c, out, c.x, c.y, c.z); return; }
+			pTry[i] = std::clamp(p[i] + dp[i], lo[i], hi[i]);
+		}
+		for (int i = 0; i < np; ++i) { dp[i] = pTry[i] - p[i]; }
+		bool tiny = true;
+		for (int i = 0; i < np; ++i) { tiny &= (std::abs(dp[i]) < 1e-15); }
+		if (tiny) {
+			if (lambda >= 1e7) { break; }
+			lambda = std::min(lambda * 11, 1e7);
+			continue;
+		}
+		double quad = 0.0, lin = 0.0;  // predicted gain, GaussianFit.cpp:248-259
+		for (int i = 0; i < np; ++i) {
+			double t = 0.0;
+			for (int j = 0; j < np; ++j) { t += alpha[i * np + j] * dp[j]; }
+			quad += dp[i] * t;
+			lin += dp[i] * beta[i];
+		}
+		const double gain = (2.0 * lin) - quad;
+		if (gain <= 0.0) {
+			if (lambda >= 1e7) { break; }
+			lambda = std::min(lambda * 11, 1e7);
+			if (relStep() < 1e-6 && it >= 2) { break; }
+			continue;
+		}
+		double denom = 0.0;
+		for (int i = 0; i < np; ++i) { denom += dp[i] * ((lambda * dp[i]) + beta[i]); }
+		const double errTry = trialError();
+		const double rho = (err - errTry) / (2.0 * denom);
+		if (rho > 1e-2) {
+			for (int i = 0; i < np; ++i) { p[i] = pTry[i]; }
+			err = evalNormal();
+			lambda = std::max(lambda / 9, 1e-7);
+		}
+		else {
+			if (lambda >= 1e7) { break; }
+			lambda = std::min(lambda * 11, 1e7);
+		}
+		if (it >= 2) {
+			if (relStep() < 1e-6) { break; }
+			if (err / static_cast<double>(n) < 1e-5) { break; }
+			if (maxAbsBeta() < 1e-6) { break; }
+		}
+	}
+	const double offset = p[0], amp = p[1], x = p[2], y = p[3];
+	// Squared correlation of data and model (GaussianFit.cpp:274-295)
+	double muD = 0.0, muM = 0.0;
+	for (int i = 0; i < n; ++i) { muD += gv[i]; }
+	for (int i = 0; i < n; ++i) { muM += hat[i]; }
+	muD /= static_cast<double>(n);
+	muM /= static_cast<double>(n);
+	double t1 = 0.0, t2 = 0.0, t3 = 0.0;
+	for (int i = 0; i < n; ++i) { t1 += (gv[i] - muD) * (hat[i] - muM); }
+	for (int i = 0; i < n; ++i) { t2 += (gv[i] - muD) * (gv[i] - muD); }
+	for (int i = 0; i < n; ++i) { t3 += (hat[i] - muM) * (hat[i] - muM); }
+	const double R = t1 / std::sqrt(t2 * t3);
+	const double r2score = std::isnan(R) ? 0 : R * R;
+	if (r2score < kEps) { FillRow(cf.mode, c, out, x, y, c.z); return; }
+	double sx = cf.sigmaX, sy = cf.sigmaY, th = cf.theta;
+	switch (cf.mode) {
+		case kG2Fixed: sx = sy = cf.sigmaX; th = 0; break;
+		case kG2Sigma: sx = p[4]; sy = sx; th = 0; break;
+		case kG3Fixed: sx = p[4] / r2; sy = p[5] / r2; break;
+		case kG3Theta: sx = p[4] / r2; sy = p[5] / r2; th = p[6]; break;
+		default: break;
+	}
+	FillRow(cf.mode, c, out, x, y, c.z, offset, amp, sx, sy, th, r2score);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Cubic-spline PSF Poisson LM, EMCCD (lib/fit/SplineFit.cpp:36-318).
+struct SplineTable {
+	int roi = 0, half = 0, n = 0, sx = 0, sy = 0, sz = 0;
+	size_t sizeXY = 0, size = 0, offsetXY = 0;
+	double initZ = 0, deltaZ = 0, intensityRatio = 1;
+	const double* coeffs = nullptr;  // SoA [64][sz][sy][sx]
+
+	void Init(const double* fp)
+	{
+		roi = static_cast<int>(static_cast<size_t>(fp[0]));
+		sx = static_cast<int>(static_cast<size_t>(fp[1]));
+		sy = static_cast<int>(static_cast<size_t>(fp[2]));
+		sz = static_cast<int>(static_cast<size_t>(fp[3]));
+		deltaZ = fp[4];
+		coeffs = fp + 5;
+		sizeXY = static_cast<size_t>(sx) * sy;
+		size = sizeXY * sz;
+		initZ = static_cast<double>(sz) / 2.0;
+		const double centre = coeffs[(32 * size) + (sz / 2 * sizeXY) + (sy / 2 * static_cast<size_t>(sx)) + (sx / 2)];
+		intensityRatio = std::abs(centre) < std::numeric_limits<double>::epsilon() ? 1.0 : 4.0 / centre;
+		const int roiParsed = roi;
+		offsetXY = static_cast<size_t>(std::floor((static_cast<double>(sx) + 1.0 - static_cast<double>(roiParsed)) / 2));
+		if (roi % 2 == 0) { roi--; }
+		half = roi / 2;
+		n = roi * roi;
+	}
+};
+
+// Monomial patch weights f = x^k y^j z^i and their derivatives (SplineFit.cpp:296-318).
+void PatchWeights(double x, double y, double z, double f[64], double dfx[64], double dfy[64], double dfz[64])
+{
+	for (int i = 0; i < 64; ++i) { f[i] = dfx[i] = dfy[i] = dfz[i] = 0; }
+	double cz = 1.0;
+	for (int i = 0; i < 4; ++i) {
+		double cy = 1.0;
+		for (int j = 0; j < 4; ++j) {
+			double cx = 1.0;
+			for (int k = 0; k < 4; ++k) {
+				const int id = i * 16 + j * 4 + k;
+				const double w = cz * cy * cx;
+				f[id] = w;
+				if (k + 1 < 4) { dfx[id + 1] = static_cast<double>(k + 1) * w; }
+				if (j + 1 < 4) { dfy[id + 4] = static_cast<double>(j + 1) * w; }
+				if (i + 1 < 4) { dfz[id + 16] = static_cast<double>(i + 1) * w; }
+				cx *= x;
+			}
+			cy *= y;
+		}
+		cz *= z;
+	}
+}
+
+// Model value and derivatives at one spline cell (SplineFit.cpp:219-240); the cell is clamped into the table.
+void SplineEval(const SplineTable& t, long px, long py, long pz, const double f[64], const double dfx[64], const double dfy[64],
+                const double dfz[64], const double* p, double dudt[5], double& model)
+{
+	// Vec3I::Clamp with size_t arithmetic: a negative index wraps to a huge value and clamps to the upper bound.
+	auto clampU = [](long v, int dim) {
+		const size_t u = static_cast<size_t>(v);
+		return std::min<size_t>(u, static_cast<size_t>(dim - 1));
+	};
+	const size_t x = clampU(px, t.sx), y = clampU(py, t.sy), z = clampU(pz, t.sz);
+	const size_t pos = ((z * t.sy) + y) * t.sx + x;
+	for (int i = 0; i < 5; ++i) { dudt[i] = 0.0; }
+	for (int i = 0; i < 64; ++i) {
+		const double cval = t.coeffs[i * t.size + pos];
+		dudt[1] += f[i] * cval;
+		dudt[2] += dfx[i] * cval;
+		dudt[3] += dfy[i] * cval;
+		dudt[4] += dfz[i] * cval;
+	}
+	dudt[0] = 1;
+	dudt[2] *= -1 * p[1];
+	dudt[3] *= -1 * p[1];
+	dudt[4] *= p[1];
+	model = p[0] + (p[1] * dudt[1]);
+}
+
+// Cholesky as in lib/signal_processing/Matrix.cpp:272-294 (l holds the transpose of u).
+bool Cholesky(const double* a, int n, double* l, double* u)
+{
+	for (int i = 0; i < n; ++i) {
+		for (int j = 0; j < i + 1; ++j) {
+			double s = 0;
+			for (int k = 0; k < j; ++k) { s += u[i * n + k] * u[j * n + k]; }
+			if (i == j) {
+				if (a[i * n + i] - s >= 0) {
+					u[i * n + j] = std::sqrt(a[i * n + i] - s);
+					l[j * n + i] = u[i * n + j];
+				}
+				else { return false; }
+			}
+			else {
+				u[i * n + j] = 1.0 / u[j * n + j] * (a[i * n + j] - s);
+				l[j * n + i] = u[i * n + j];
+			}
+		}
+	}
+	return true;
+}
+
+// In-place LU inverse without pivoting (lib/signal_processing/Matrix.cpp:358-410), column-major indexing as there.
+void InverseLU(double* in, double* out, int n)
+{
+	std::vector<double> y(static_cast<size_t>(n) * n);
+	double acc = 0;
+	for (int j = 0; j < n; ++j) {
+		for (int i = 0; i <= j; ++i) {
+			if (i > 0) {
+				for (int k = 0; k <= i - 1; ++k) { acc += in[i + (k * n)] * in[k + (j * n)]; }
+				in[i + (j * n)] -= acc;
+				acc = 0;
+			}
+		}
+		for (int i = j + 1; i < n; ++i) {
+			if (j > 0) {
+				for (int k = 0; k <= j - 1; ++k) { acc += in[i + (k * n)] * in[k + (j * n)]; }
+				in[i + (j * n)] = (1 / in[j + (j * n)]) * (in[i + (j * n)] - acc);
+				acc = 0;
+			}
+			else { in[i + (j * n)] = (1 / in[j + (j * n)]) * in[i + (j * n)]; }
+		}
+	}
+	for (int num = 0; num < n; ++num) {
+		y[0] = num == 0 ? 1 : 0;
+		for (int i = 1; i < n; ++i) {
+			const size_t b = i == num ? 1 : 0;
+			for (int j = 0; j <= i - 1; ++j) { acc += in[i + (j * n)] * y[j]; }
+			y[i] = static_cast<double>(b) - acc;
+			acc = 0;
+		}
+		out[n - 1 + (num * n)] = y[n - 1] / in[(n - 1) + ((n - 1) * n)];
+		for (int i = n - 2; i >= 0; --i) {
+			for (int j = i + 1; j < n; ++j) { acc += in[i + (j * n)] * out[j + (num * n)]; }
+			out[i + (num * n)] = (1 / in[i + (i * n)]) * (y[i] - acc);
+			acc = 0;
+		}
+	}
+}
+
+// Spline fit (SplineFit.cpp:53-216). Its bounds use the raw fitParams[0] (the ROI before it is forced odd).
+void FitSplineFull(const SplineTable& t, double roiParam, const uint16_t* img, int W, int H, const Candidate& c, Row& out)
+{
+	constexpr int np = 5;
+	const size_t ux = static_cast<size_t>(c.x), uy = static_cast<size_t>(c.y);
+	const size_t h = static_cast<size_t>(t.half);
+	if (h > ux || ux >= static_cast<size_t>(W) - h || h > uy || uy >= static_cast<size_t>(H) - h) {
+		FillRow(kSplineEmccd, c, out, c.x, c.y, c.z);
+		return;
+	}
+	const int n = t.n, roi = t.roi, hh = t.half;
+	std::vector<double> gv(n);
+	double vmin = std::numeric_limits<double>::max(), vmax = std::numeric_limits<double>::lowest();
+	for (int i = -hh; i <= hh; ++i) {
+		for (int j = -hh; j <= hh; ++j) {
+			const int k = (i + hh) * roi + (j + hh);
+			gv[k] = static_cast<double>(img[(ux + j) + (uy + i) * static_cast<size_t>(W)]);
+			vmin = std::min(vmin, gv[k]);
+			vmax = std::max(vmax, gv[k]);
+		}
+	}
+	double x = 0, y = 0, sum = 0;
+	for (int i = 0, k = 0; i < roi; ++i) {
+		for (int j = 0; j < roi; ++j, ++k) {
+			y += gv[k] * static_cast<double>(i);
+			x += gv[k] * static_cast<double>(j);
+			sum += gv[k];
+		}
+	}
+	if (sum > 0) { x /= sum; y /= sum; }
+	else { x = static_cast<double>(roi) / 2.0; y = static_cast<double>(roi) / 2.0; }
+	const double roiC = (roiParam - 1) / 2.0, roiD = roiParam / 4.0;
+	const double dmin = roiC - roiD, dmax = roiC + roiD;
+	double lo[np] = {-0.01, -1, dmin, dmin, 0};
+	double p[np] = {vmin, vmax - vmin, x, y, t.initZ};
+	double hi[np] = {0.01, 1, dmax, dmax, 1};
+	p[1] *= t.intensityRatio;
+	hi[4] = static_cast<double>(t.sz);
+	for (int i = 0; i < np; ++i) { p[i] = std::clamp(p[i], lo[i], hi[i]); }
+	double jump[np] = {std::max(20.0, p[1]), std::max(100.0, p[1]), 1.0, 1.0, std::max(static_cast<double>(t.sz) / 3.0, 2.0)};
+
+	double lambda = 0.1, err = std::numeric_limits<double>::max(), mu = 1 + lambda, model = 0;
+	double hess[np * np], l[np * np], u[np * np], jac[np], upd[np] = {0, 0, 0, 0, 0}, dudt[np];
+	double f[64], dfx[64], dfy[64], dfz[64];
+	auto cellOrigin = [&](const double* pp, long& xi, long& yi, long& zi, double& xc, double& yc, double& zc) {
+		const double xr = -1 * (pp[2] - static_cast<double>(hh) + 0.5), yr = -1 * (pp[3] - static_cast<double>(hh) + 0.5);
+		xi = static_cast<int>(std::floor(xr));
+		yi = static_cast<int>(std::floor(yr));
+		zi = static_cast<int>(std::floor(pp[4]));
+		xc = xr - static_cast<double>(xi);
+		yc = yr - static_cast<double>(yi);
+		zc = pp[4] - static_cast<double>(zi);
+	};
+	auto upMu = [&](bool up) {  // SplineFit.cpp:263-273
+		if (up) { mu = std::max((1 + (lambda * 10)) / (1 + lambda), 1.3); lambda = 10 * lambda; }
+		else { lambda = 0.1 * lambda; mu = 1 + lambda; }
+	};
+	bool stop = false;
+	int it = 0;
+	while (!stop) {
+		++it;
+		const double oldErr = err;
+		double oldP[np], oldUpd[np];
+		std::copy(p, p + np, oldP);
+		std::copy(upd, upd + np, oldUpd);
+		const double oldLambda = lambda;
+		std::fill(jac, jac + np, 0.0);
+		std::fill(hess, hess + np * np, 0.0);
+		std::fill(upd, upd + np, 0.0);
+		std::fill(l, l + np * np, 0.0);
+		std::fill(u, u + np * np, 0.0);
+		long xi, yi, zi;
+		double xc, yc, zc;
+		cellOrigin(p, xi, yi, zi, xc, yc, zc);
+		PatchWeights(xc, yc, zc, f, dfx, dfy, dfz);
+		for (int i = 0, k = 0; i < roi; ++i) {
+			const long cx = xi + i + static_cast<long>(t.offsetXY);
+			for (int j = 0; j < roi; ++j, ++k) {
+				const long cy = yi + j + static_cast<long>(t.offsetXY);
+				SplineEval(t, cx, cy, zi, f, dfx, dfy, dfz, p, dudt, model);
+				const double d = gv[k];
+				if (d > 0) { err = err + (2 * (model - d - (d * std::log(model / d)))); }
+				else { err = err + (2 * model); }
+				const double t1 = 1 - (d / model);
+				for (int a = 0; a < np; ++a) { jac[a] += t1 * dudt[a]; }
+				const double t2 = d / (model * model);
+				for (int a = 0; a < np; ++a) {
+					for (int b = a; b < np; ++b) {
+						hess[a * np + b] += t2 * dudt[a] * dudt[b];
+						hess[b * np + a] = hess[a * np + b];
+					}
+				}
+			}
+		}
+		for (int a = 0; a < np; ++a) { hess[a * np + a] = hess[a * np + a] * mu; }
+		if (Cholesky(hess, np, l, u)) {
+			double yv[np];  // forward then backward substitution (SplineFit.cpp:276-294)
+			for (int a = 0; a < np; ++a) {
+				yv[a] = jac[a];
+				for (int b = 0; b < a; ++b) { yv[a] -= l[b * np + a] * yv[b]; }
+				yv[a] /= l[a * np + a];
+			}
+			for (int a = np - 1; a >= 0; --a) {
+				upd[a] = yv[a];
+				for (int b = a + 1; b < np; ++b) { upd[a] -= u[b * np + a] * upd[b]; }
+				upd[a] /= u[a * np + a];
+			}
+			for (int a = 0; a < np; ++a) {
+				if (std::abs(oldUpd[a]) > kEps && upd[a] / oldUpd[a] < -0.5) { jump[a] *= 0.5; }
+				const double scale = upd[a] / (1.0 + (std::abs(upd[a]) / jump[a]));
+				p[a] -= scale;
+				p[a] = std::clamp(p[a], lo[a], hi[a]);
+				upd[a] = scale;
+			}
+			if (err > oldErr) {
+				err = oldErr;
+				std::copy(oldP, oldP + np, p);
+				std::copy(oldUpd, oldUpd + np, upd);
+				lambda = oldLambda;
+				upMu(true);
+			}
+			else { upMu(false); }
+		}
+		else {
+			err = oldErr;
+			std::copy(oldP, oldP + np, p);
+			std::copy(oldUpd, oldUpd + np, upd);
+			lambda = oldLambda;
+			upMu(true);
+		}
+		if (it >= kMaxIter) { stop = true; }
+		if (it > 2 && (err < 1e-6 || std::abs(err - oldErr) / err < 1e-6)) { stop = true; }
+	}
+	// CRLB (SplineFit.cpp:164-205)
+	double fm[np * np] = {}, fmi[np * np] = {}, crlb[np];
+	{
+		long xi, yi, zi;
+		double xc, yc, zc;
+		cellOrigin(p, xi, yi, zi, xc, yc, zc);
+		PatchWeights(xc, yc, zc, f, dfx, dfy, dfz);
+		for (int i = 0; i < roi; ++i) {
+			const long cx = xi + i + static_cast<long>(t.offsetXY);
+			for (int j = 0; j < roi; ++j) {
+				const long cy = yi + j + static_cast<long>(t.offsetXY);
+				SplineEval(t, cx, cy, zi, f, dfx, dfy, dfz, p, dudt, model);
+				for (int a = 0; a < np; ++a) {
+					for (int b = a; b < np; ++b) {
+						fm[a * np + b] += dudt[b] * dudt[a] / model;
+						fm[b * np + a] = fm[a * np + b];
+					}
+				}
+			}
+		}
+	}
+	for (int a = 0; a < np; ++a) {
+		if (std::abs(fm[a * np + a]) < std::numeric_limits<double>::epsilon()) { fm[a * np + a] = 1e-10; }
+	}
+	InverseLU(fm, fmi, np);
+	for (int a = 0; a < np; ++a) { const double v = fmi[a * np + a]; crlb[a] = v >= 0 ? std::sqrt(v) : 0.0; }
+	const double off = crlb[0], amp = crlb[1], qxy = (crlb[2] + crlb[3]) / 2, qz = t.deltaZ * crlb[4];
+	const double xo = p[2] - static_cast<double>(hh) + c.x;
+	const double yo = p[3] - static_cast<double>(hh) + c.y;
+	const double zo = t.deltaZ * (p[4] - t.initZ);
+	FillRow(kSplineEmccd, c, out, xo, yo, zo, off, amp, 0, 0, 0, qxy, qz);
+}
+
+// Strict weak order on (Y, X) with std::weak_order semantics (FrameProcessor.cpp:35-39).
+bool RowLess(const Row& a, const Row& b)
+{
+	if (const auto o = std::weak_order(a[cY], b[cY]); o != 0) { return o < 0; }
+	return std::weak_order(a[cX], b[cX]) < 0;
+}
+
+// One frame: wavelet -> segmentation -> fits of the first maxPoints candidates -> sort (FrameProcessor.cpp:28-82).
+void ProcessFrame(const uint16_t* img, int H, int W, double thr, double ratio, size_t maxPoints, int fit, const double* fp,
+                  std::vector<Row>& rows)
+{
+	std::vector<double> planes[kNumPlanes];
+	Atrous(img, H, W, planes);
+	Segmenter seg;
+	seg.Run(planes[kPlaneId].data(), H, W, thr, ratio);
+	const size_t count = std::min(seg.cands.size(), maxPoints);
+	if (seg.cands.size() > maxPoints) { std::fprintf(stderr, "[WARNING] Density is too high; some points are missed (output capacity exceeded).\n"); }
+	rows.assign(count, Row{});
+	const int mode = (fit >= 1 && fit <= 5) ? fit : kNone;
+	if (mode >= kG2Fixed && mode <= kG3Theta) {
+		FitConfig cf;
+		cf.Init(mode, fp, img, W, H);
+		for (size_t i = 0; i < count; ++i) { FitGaussian(cf, seg.cands[i], rows[i]); }
+	}
+	else if (mode == kSplineEmccd) {
+		SplineTable t;
+		t.Init(fp);
+		for (size_t i = 0; i < count; ++i) { FitSplineFull(t, fp[0], img, W, H, seg.cands[i], rows[i]); }
+	}
+	else {
+		for (size_t i = 0; i < count; ++i) {
+			const Candidate& c = seg.cands[i];
+			FillRow(kNone, c, rows[i], c.x, c.y, c.z, 0, 0);
+		}
+	}
+	std::sort(rows.begin(), rows.end(), RowLess);
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_SetThreads(int n) { if (n > 0) { omp_set_num_threads(n); } }
+
+// Localization (CPU/main.cpp:112-121 -> lib/Palm.cpp:48-70, 24-43).
+uint64_t orc_Localization(const uint16_t* input, double* output, uint64_t outputSize, uint64_t height, uint64_t width,
+                          uint64_t planes, double thr, double ratio, uint64_t fit, const double* fp)
+{
+	const size_t perPlane = planes == 0 ? 0 : (outputSize / kCols) / planes;
+	if (perPlane == 0) { return 0; }
+	const size_t frame = static_cast<size_t>(height) * width;
+	std::vector<std::vector<Row>> all(planes);
+	#pragma omp parallel for schedule(dynamic, 1)
+	for (int64_t z = 0; z < static_cast<int64_t>(planes); ++z) {
+		ProcessFrame(input + z * frame, static_cast<int>(height), static_cast<int>(width), thr, ratio, perPlane,
+		             static_cast<int>(fit), fp, all[z]);
+	}
+	size_t count = 0, id = 1;
+	for (size_t z = 0; z < planes; ++z) {
+		size_t local = 1;
+		for (const Row& r : all[z]) {
+			std::copy(r.begin(), r.end(), output + count);
+			output[count + cId] = static_cast<double>(id++);
+			output[count + cPlane] = static_cast<double>(z + 1);
+			output[count + cIndex] = static_cast<double>(local++);
+			count += kCols;
+		}
+	}
+	return count;
+}
+
+// Fit-only at given positions (CPU/main.cpp:141-148 -> lib/Palm.cpp:73-119). Fit 0 is not supported by the
+// reference here (its GaussianFit throws for the "none" model); this restatement fills no-fit rows for it.
+uint64_t orc_Fitting(const uint16_t* input, const double* positions, uint64_t nPoints, double* output, uint64_t /*outputSize*/,
+                     uint64_t height, uint64_t width, uint64_t planes, uint64_t fit, const double* fp)
+{
+	if (nPoints == 0) { return 0; }
+	std::vector<size_t> localIdx(nPoints), perPlane(planes, 0);
+	for (size_t i = 0; i < nPoints; ++i) { localIdx[i] = ++perPlane[static_cast<size_t>(positions[i * 6 + 1]) - 1]; }
+	const size_t frame = static_cast<size_t>(height) * width;
+	#pragma omp parallel for schedule(static)
+	for (int64_t i = 0; i < static_cast<int64_t>(nPoints); ++i) {
+		const double* pos = positions + i * 6;
+		const size_t plane = static_cast<size_t>(pos[1]) - 1;
+		const uint16_t* img = input + plane * frame;
+		Candidate c;
+		c.x = pos[2]; c.y = pos[3]; c.intensity = pos[4]; c.surf = pos[5];
+		Row r{};
+		if (fit == kSplineEmccd) {
+			SplineTable t;
+			t.Init(fp);
+			FitSplineFull(t, fp[0], img, static_cast<int>(width), static_cast<int>(height), c, r);
+		}
+		else if (fit >= 1 && fit <= 4) {
+			FitConfig cf;
+			cf.Init(static_cast<int>(fit), fp, img, static_cast<int>(width), static_cast<int>(height));
+			FitGaussian(cf, c, r);
+		}
+		else { FillRow(kNone, c, r, c.x, c.y, c.z, 0, 0); }
+		r[cId] = pos[0];
+		r[cPlane] = pos[1];
+		r[cIndex] = static_cast<double>(localIdx[i]);
+		std::copy(r.begin(), r.end(), output + i * kCols);
+	}
+	return nPoints * kCols;
+}
+
+// Wavelett (CPU/main.cpp:257-284).
+void orc_Wavelett(const uint16_t* input, double* output, uint64_t height, uint64_t width, uint64_t planes, uint64_t level)
+{
+	if (planes == 0) { return; }
+	if (level == 0) { level = 1; }
+	const uint64_t lv = std::min<uint64_t>(level - 1, kNumPlanes - 1);
+	const size_t frame = static_cast<size_t>(height) * width;
+	#pragma omp parallel for schedule(static)
+	for (int64_t z = 0; z < static_cast<int64_t>(planes); ++z) {
+		std::vector<double> pl[kNumPlanes];
+		Atrous(input + z * frame, static_cast<int>(height), static_cast<int>(width), pl);
+		std::copy(pl[lv].begin(), pl[lv].end(), output + z * frame);
+	}
+}
+
+// AutoThreshold on frame 0 (CPU/main.cpp:75-85 -> lib/Palm.cpp:122-172).
+double orc_AutoThreshold(const uint16_t* input, uint64_t height, uint64_t width, const double* fp)
+{
+	const size_t size = static_cast<size_t>(height) * width;
+	const auto cap = static_cast<uint64_t>(0.2 * static_cast<double>(height * width) * kCols);
+	const size_t maxPoints = cap / kCols;
+	const double halfRoi = fp[0] / 2;
+	double mu = 0.0;
+	for (size_t i = 0; i < size; ++i) { mu += input[i]; }
+	mu /= static_cast<double>(size);
+	double var = 0.0;
+	for (size_t i = 0; i < size; ++i) { var += (input[i] - mu) * (input[i] - mu); }
+	var /= static_cast<double>(size);
+	double thr = std::sqrt(var);
+	std::vector<char> mask(size);
+	std::vector<Row> pts;
+	const int W = static_cast<int>(width), H = static_cast<int>(height);
+	for (int iter = 0; iter < kThresholdIters; ++iter) {
+		ProcessFrame(input, H, W, thr, 10, maxPoints, 0, fp, pts);
+		std::fill(mask.begin(), mask.end(), 0);
+		for (const Row& p : pts) {
+			const auto x0 = static_cast<size_t>(std::max(0, static_cast<int>(p[cX] - halfRoi)));
+			const auto x1 = std::min(static_cast<size_t>(W), static_cast<size_t>(p[cX] + halfRoi));
+			const auto y0 = static_cast<size_t>(std::max(0, static_cast<int>(p[cY] - halfRoi)));
+			const auto y1 = std::min(static_cast<size_t>(H), static_cast<size_t>(p[cY] + halfRoi));
+			for (size_t yy = y0; yy < y1; ++yy) { for (size_t xx = x0; xx < x1; ++xx) { mask[yy * width + xx] = 1; } }
+		}
+		size_t count = 0;
+		double sum = 0;
+		for (size_t j = 0; j < size; ++j) { if (!mask[j]) { sum += input[j]; ++count; } }
+		if (count == 0) { break; }
+		mu = sum / static_cast<double>(count);
+		var = 0.0;
+		for (size_t j = 0; j < size; ++j) { if (!mask[j]) { var += (input[j] - mu) * (input[j] - mu); } }
+		var /= static_cast<double>(count);
+		var = std::sqrt(var);
+		if (std::abs(thr - var) <= std::numeric_limits<double>::epsilon()) { break; }
+		thr = var;
+	}
+	return thr;
+}
+
+// All wavelet planes of one frame (planes[k*H*W + p]).
+void orc_Planes(const uint16_t* frame, uint64_t height, uint64_t width, double* out)
+{
+	std::vector<double> pl[kNumPlanes];
+	Atrous(frame, static_cast<int>(height), static_cast<int>(width), pl);
+	const size_t n = static_cast<size_t>(height) * width;
+	for (int k = 0; k < kNumPlanes; ++k) { std::copy(pl[k].begin(), pl[k].end(), out + k * n); }
+}
+
+static uint64_t DumpCandidates(const Segmenter& seg, double* rows, uint64_t capacity)
+{
+	for (size_t i = 0; i < seg.cands.size() && i < capacity; ++i) {
+		rows[4 * i + 0] = seg.cands[i].x;
+		rows[4 * i + 1] = seg.cands[i].y;
+		rows[4 * i + 2] = seg.cands[i].intensity;
+		rows[4 * i + 3] = seg.cands[i].surf;
+	}
+	return seg.cands.size();
+}
+
+// Segmentation candidates of one frame in label order: rows (x, y, intensity, surf).
+uint64_t orc_Candidates(const uint16_t* frame, uint64_t height, uint64_t width, double thr, double ratio, double* rows,
+                        uint64_t capacity)
+{
+	std::vector<double> pl[kNumPlanes];
+	Atrous(frame, static_cast<int>(height), static_cast<int>(width), pl);
+	Segmenter seg;
+	seg.Run(pl[kPlaneId].data(), static_cast<int>(height), static_cast<int>(width), thr, ratio);
+	return DumpCandidates(seg, rows, capacity);
+}
+
+uint64_t orc_CandidatesFromPotential(const double* potential, uint64_t height, uint64_t width, double thr, double ratio,
+                                     double* rows, uint64_t capacity)
+{
+	Segmenter seg;
+	seg.Run(potential, static_cast<int>(height), static_cast<int>(width), thr, ratio);
+	return DumpCandidates(seg, rows, capacity);
+}
+
+// Final label map of one frame after the watershed stages, before the surface filter (labels 1..n, 0 = none).
+uint64_t orc_Labels(const uint16_t* frame, uint64_t height, uint64_t width, double thr, double ratio, uint32_t* labels)
+{
+	std::vector<double> pl[kNumPlanes];
+	Atrous(frame, static_cast<int>(height), static_cast<int>(width), pl);
+	Segmenter seg;
+	seg.H = static_cast<int>(height);
+	seg.W = static_cast<int>(width);
+	seg.ratio = ratio;
+	const size_t n = static_cast<size_t>(height) * width;
+	seg.pot.assign(n, 0.0);
+	seg.lab.assign(n, 0);
+	for (size_t i = 0; i < n; ++i) { seg.pot[i] = pl[kPlaneId][i] > thr ? pl[kPlaneId][i] : 0.0; }
+	seg.Seeds();
+	seg.Flood();
+	if (static_cast<int>(ratio) > 0) { seg.Fuse(); seg.Flood(); }
+	std::copy(seg.lab.begin(), seg.lab.end(), labels);
+	return seg.cands.size();
+}
+
+}  // extern "C"
