@@ -1,0 +1,274 @@
+"""Benchmark: localizations/s of the detect + fit hot path on the 2000 x 1024 x 1024 uint16 workload.
+
+One step = one Localization pass (wavelet -> threshold -> watershed -> per-ROI LM fit -> per-plane ordering) over the
+whole synthetic stack. ``value`` is measured on device-resident frames through PTB_LocalizationDevice; ``e2e`` is
+the reference-facing C ABI (Localization) with host buffers, host<->device copies inside the timed region.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--frames Z]
+
+Under torchrun (N > 1) each rank processes its own stack of the same shape (frames shard with no exchange: weak
+scaling); the max over ranks of the device time is reported.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "palmtracer-cpp_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+sys.path.insert(0, ROOT)
+
+METRIC = "localizations/s (detect+MLE fit) at FP64-matched error; p50/p99 stack latency"
+UNIT = "localizations/s"
+WORKLOAD = "c2"
+FIT_MODE = 2
+FIT_PARAMS = np.array([7.0, 1.3, 1.3, 0.0])
+RATIO = 0.0
+PER_PLANE = 8192
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    def __init__(self, index):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.file.read().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.file.name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def mad_threshold_gpu(lib, frame):
+    import synth
+    w1 = lib.wavelett(frame, 2)[0]
+    return synth.mad_threshold(w1)
+
+
+def cpu_reference_rate(frames_host, thr, seconds=10.0, threads=None):
+    """Reference CPU path (oracle/_ref, or the oracle port when the reference build is absent) on a bounded sample."""
+    from oracle.oracle import reference, OracleLib
+    lib = reference()
+    kind = "reference"
+    if lib is None:
+        lib = OracleLib()
+        kind = "port"
+    cores = threads or os.cpu_count()
+    lib.set_threads(cores)
+    z = frames_host.shape[0]
+    n0 = min(z, max(4, cores))
+    t0 = time.perf_counter()
+    rows = lib.localization(frames_host[:n0], thr, RATIO, FIT_MODE, FIT_PARAMS, capacity_doubles=PER_PLANE * n0 * 18)
+    dt0 = time.perf_counter() - t0
+    n1 = int(min(z, max(n0, n0 * seconds / max(dt0, 1e-3))))
+    if n1 > n0:
+        t0 = time.perf_counter()
+        rows = lib.localization(frames_host[:n1], thr, RATIO, FIT_MODE, FIT_PARAMS, capacity_doubles=PER_PLANE * n1 * 18)
+        dt0 = time.perf_counter() - t0
+    else:
+        n1 = n0
+    return rows.shape[0] / dt0, {"kind": kind, "cores": cores, "sample": "%d of the %d frames, fit mode %d" % (n1, z, FIT_MODE),
+                                 "frames": n1, "seconds": dt0, "rows": int(rows.shape[0])}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    import synth
+    import ptb
+
+    frames = args.frames or synth.SHAPES[WORKLOAD][0]
+    h, w = synth.SHAPES[WORKLOAD][1:]
+    config = {"workload": "c2: %d frames of %dx%d uint16, ~2684 emitters/frame, 7x7 ROI, fit mode %d, per-plane capacity %d"
+                          % (frames, h, w, FIT_MODE, PER_PLANE),
+              "frames": frames, "height": h, "width": w, "fit_mode": FIT_MODE, "roi": 7, "watershed_ratio": RATIO,
+              "l2": "inputs (4.2 GB) larger than L2", "parallelism": "frames sharded, no exchange" if world > 1 else "single GPU"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            if world > 1:
+                dist.destroy_process_group()
+            return
+        d, _ = synth.stack_cuda(WORKLOAD, frames=min(frames, 256), seed=1000)
+        host = d.cpu().numpy().view(np.uint16)
+        thr = mad_threshold_gpu(ptb, host[0])
+        del d
+        torch.cuda.empty_cache()
+        rates = []
+        info = None
+        for i in range(args.warmup + args.steps):
+            r, info = cpu_reference_rate(host, thr, seconds=8.0)
+            if i >= args.warmup:
+                rates.append(r)
+        v = float(np.median(rates))
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"], "sample": info["sample"]},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    d_in, em = synth.stack_cuda(WORKLOAD, frames=frames, seed=1000 + rank)
+    torch.cuda.synchronize()
+    thr = mad_threshold_gpu(ptb, d_in[0].cpu().numpy().view(np.uint16))
+    cap = PER_PLANE * frames * 18
+    d_out = torch.empty(cap, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        return ptb.localization_device(d_in.data_ptr(), d_out.data_ptr(), cap, (frames, h, w), thr, RATIO, FIT_MODE, FIT_PARAMS,
+                                       stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        n = step()
+    if n == 0:
+        raise RuntimeError("no localizations: " + ptb.last_error())
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(local)
+    launches0 = ptb.launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    counts = []
+    torch.cuda.synchronize()
+    for e0, e1 in ev:
+        e0.record(stream)
+        counts.append(step())
+        e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = (ptb.launch_count() - launches0) // args.steps
+    step_ms = np.array([a.elapsed_time(b) for a, b in ev])
+    rows = counts[-1] // 18
+    total_ms = float(step_ms.sum())
+    if world > 1:
+        t = torch.tensor([total_ms, float(rows)], device="cuda", dtype=torch.float64)
+        allt = [torch.zeros_like(t) for _ in range(world)]
+        dist.all_gather(allt, t)
+        total_ms = max(float(x[0]) for x in allt)
+        rows_all = sum(float(x[1]) for x in allt)
+    else:
+        rows_all = float(rows)
+    value = rows_all * args.steps / (total_ms / 1000.0)
+
+    # stage breakdown of one more (untimed) pass
+    ptb.set_profiling(1)
+    ptb.stage_times()
+    step()
+    torch.cuda.synchronize()
+    stages = ptb.stage_times()
+    ptb.set_profiling(0)
+    peak, peak_kind = peaks()
+    det_ms, det_l = stages["detect"]
+    det_bytes = 2.0 * h * w * frames
+    achieved = det_bytes / (det_ms / 1000.0) / 1e9 if det_ms > 0 else None
+    roofline = {"kernel": "DetectKernel (wavelet + threshold + seeds)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "algorithmic_bytes_per_launch": det_bytes / max(det_l, 1), "launches": det_l,
+                "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                "stage_ms": {k: round(v[0], 3) for k, v in stages.items()}}
+
+    # end to end through the reference-facing C ABI with host buffers
+    host_in = torch.empty((frames, h, w), dtype=torch.int16, pin_memory=True)
+    host_in.copy_(d_in)
+    host_np = host_in.numpy().view(np.uint16)
+    host_out = torch.empty(cap, dtype=torch.float64, pin_memory=True).numpy()
+    e2e_ms = []
+    for i in range(max(1, args.warmup // 2) + max(2, args.steps // 2)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        n_e2e = ptb.localization_raw(host_np, host_out, thr, RATIO, FIT_MODE, FIT_PARAMS)
+        torch.cuda.synchronize()
+        if i >= max(1, args.warmup // 2):
+            e2e_ms.append((time.perf_counter() - t0) * 1000.0)
+    e2e_value = (n_e2e // 18) * len(e2e_ms) / (sum(e2e_ms) / 1000.0)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sample = host_np[: min(frames, 512)]
+        v, info = cpu_reference_rate(sample, thr, seconds=10.0)
+        cpu = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"], "sample": info["sample"]}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic (seeded, generated on the GPU; no public dataset)", "config": config,
+                "frames_per_s": frames * world * args.steps / (total_ms / 1000.0),
+                "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
+                "localizations_per_step": int(rows_all), "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host_np.nbytes),
+                        "d2h_bytes_per_step": int(n_e2e * 8), "ms_per_step": float(np.mean(e2e_ms))},
+                "gpu_launches": int(launches), "clocks": clk}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

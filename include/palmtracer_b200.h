@@ -1,0 +1,97 @@
+/*
+ * PALMTracer localization hot path on one NVIDIA B200 (sm_100a): public C ABI.
+ *
+ * The first four entry points are drop-in replacements for the exports of the PALMTracer CPU library
+ * (tmonseigne/PALMTracer-cpp 1.3.0, CPU/PALMTracer.def:3-13, declared with PT_API in lib/ExportAPI.hpp:21-30):
+ * same names, argument meaning, buffer layouts, return values and error behaviour (no exception ever crosses the
+ * ABI; bad input yields 0 / no output, failed fits yield the usual -1 sentinel rows). All buffers are caller-owned
+ * HOST memory; the library keeps no pointer after a call returns.
+ *
+ * Layouts (lib/Constants.hpp:31-64):
+ *   input       uint16 [planes][height][width], x fastest
+ *   output      float64 rows of 18 columns: Id, Plane, Index, Channel, X, Y, Z, Integrated intensity, SigmaX, SigmaY,
+ *               Theta, QualityXY, QualityZ, Amplitude, Offset, SegIntensity, Surface, Circularity
+ *   positions   float64 rows of 6 columns: Id, Plane (1-based), X, Y, SegIntensity, Surface
+ *   fit_params  Gaussian modes 1-4: [roi, sigmaX, sigmaY, theta]
+ *               spline mode 5:      [roi, sx, sy, sz, deltaZ, 64*sx*sy*sz coefficients (SoA [64][sz][sy][sx])]
+ *
+ * Fit modes 0-5 keep the reference semantics (0 none, 1 Gaussian fixed sigma, 2 free sigma, 3 sigmaX/sigmaY,
+ * 4 sigmaX/sigmaY/theta, 5 cubic spline EMCCD).
+ */
+#ifndef PALMTRACER_B200_H
+#define PALMTRACER_B200_H
+
+#include <stdint.h>
+
+#if defined(_WIN32)
+#define PTB_API __declspec(dllexport)
+#else
+#define PTB_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Replaces Localization (CPU/main.cpp:112-121): detection (a trous wavelet, threshold, watershed) and per-candidate
+ * fit over a stack. Per-plane capacity is (outputSize / 18) / planes rows (lib/Palm.cpp:51); candidates beyond it
+ * are dropped in label order with one stderr warning. Rows are sorted per plane by (Y, X) and numbered with a
+ * global 1-based Id, the 1-based Plane and the per-plane 1-based Index. Returns the number of doubles written. */
+PTB_API uint64_t Localization(const uint16_t* input, double* output, uint64_t outputSize, uint64_t height,
+                              uint64_t width, uint64_t planes, double thresholdVal, double watershedRatio, uint64_t fit,
+                              const double* fit_params);
+
+/* Replaces Fitting (CPU/main.cpp:141-148 -> lib/Palm.cpp:73-119): fits at caller-given positions, rows in input
+ * order, Id and Plane copied from the input, Index = rank within its plane. Returns nPoints * 18 (0 if empty). */
+PTB_API uint64_t Fitting(const uint16_t* input, const double* positions, uint64_t nPoints, double* output,
+                         uint64_t outputSize, uint64_t height, uint64_t width, uint64_t planes, uint64_t fit,
+                         const double* fit_params);
+
+/* Replaces Wavelett (CPU/main.cpp:257-284): one wavelet plane per frame as float64 [planes][height][width];
+ * levelOutput is 1-based (0 is treated as 1) and clamped to the last plane (the residual). */
+PTB_API void Wavelett(const uint16_t* input, double* output, uint64_t height, uint64_t width, uint64_t planes,
+                      uint64_t levelOutput);
+
+/* Replaces AutoThreshold (CPU/main.cpp:75-85 -> lib/Palm.cpp:122-172): iterative out-of-ROI standard deviation of
+ * the raw pixels of frame 0 (at most 5 rounds of detection with fit 0 and watershed ratio 10). */
+PTB_API double AutoThreshold(const uint16_t* input, uint64_t height, uint64_t width, const double* fit_params);
+
+/* ---- Additions (no counterpart in the reference) ---------------------------------------------------------------- */
+
+/* Same contract as Localization, but d_input and d_output are DEVICE memory of the current CUDA device (fit_params
+ * stays a host array) and the work is ordered after the caller's `stream` (a cudaStream_t; 0 = legacy default
+ * stream), which in turn waits for it. Blocks until the row count is known. Used when frames are already resident
+ * in HBM (the serving and benchmark paths). */
+PTB_API uint64_t PTB_LocalizationDevice(const uint16_t* d_input, double* d_output, uint64_t outputSize,
+                                        uint64_t height, uint64_t width, uint64_t planes, double thresholdVal,
+                                        double watershedRatio, uint64_t fit, const double* fit_params, void* stream);
+
+/* Segmentation mode. 0 (default): each 8-connected component of the thresholded potential is flooded on its own,
+ * in parallel. 1 (strict): each frame is flooded as one unit with a frame-global pop counter, exactly as the
+ * reference's single priority queue does (Segmentation2D.cpp:336-385); slower, exact for any threshold.
+ * Returns the previous mode. */
+PTB_API int PTB_SetSegmentationMode(int mode);
+
+/* Fit arithmetic for the Gaussian least-squares modes 1-4. 0 (default): FP64 iterations (same decisions as the
+ * reference); 1: FP32 iterations with an FP64 re-fit of any ROI whose FP32 run did not converge cleanly.
+ * Returns the previous setting. */
+PTB_API int PTB_SetFitPrecision(int mode);
+
+/* Last error message of the calling thread ("" when none). */
+PTB_API const char* PTB_LastError(void);
+
+/* Number of kernel launches issued by this library in the calling process so far (diagnostics). */
+PTB_API uint64_t PTB_KernelLaunchCount(void);
+
+/* Stage timing (diagnostics). When enabled, every chunk records CUDA events on the library's stream around its
+ * stages and accumulates device milliseconds per stage: [0] detection kernel, [1] segmentation chain, [2] fit
+ * kernels, [3] ordering and numbering, [4] host<->device copies. PTB_StageTimes copies up to n totals into ms and
+ * the matching launch counts into launches (either may be NULL), then resets them. Returns the previous setting. */
+PTB_API int PTB_SetProfiling(int enable);
+PTB_API void PTB_StageTimes(double* ms, uint64_t* launches, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PALMTRACER_B200_H */

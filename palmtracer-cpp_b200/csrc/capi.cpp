@@ -1,0 +1,153 @@
+// C ABI of the B200 localization engine (declared in include/palmtracer_b200.h). No exception crosses it: every
+// entry point catches, records the message for PTB_LastError() and returns the reference's neutral value.
+#include <cuda_runtime.h>
+
+#include <exception>
+#include <iostream>
+#include <mutex>
+
+#include "../../include/palmtracer_b200.h"
+#include "engine.h"
+
+namespace {
+
+void Report(const char* fn)
+{
+	std::cerr << "[PALMTracer-B200] " << fn << " failed: " << ptb::LastError() << "\n";
+}
+
+}  // namespace
+
+extern "C" {
+
+PTB_API uint64_t Localization(const uint16_t* input, double* output, uint64_t outputSize, uint64_t height, uint64_t width,
+                              uint64_t planes, double thresholdVal, double watershedRatio, uint64_t fit, const double* fit_params)
+{
+	ptb::ClearError();
+	try {
+		std::unique_lock<std::mutex> lock;
+		ptb::Engine& e = ptb::EngineFor(lock);
+		const long long n = e.Localize(input, false, output, false, outputSize, height, width, planes, thresholdVal,
+		                               watershedRatio, fit, fit_params);
+		if (n < 0) { Report("Localization"); return 0; }
+		return static_cast<uint64_t>(n);
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("Localization");
+		return 0;
+	}
+}
+
+PTB_API uint64_t Fitting(const uint16_t* input, const double* positions, uint64_t nPoints, double* output, uint64_t /*outputSize*/,
+                         uint64_t height, uint64_t width, uint64_t planes, uint64_t fit, const double* fit_params)
+{
+	ptb::ClearError();
+	try {
+		std::unique_lock<std::mutex> lock;
+		ptb::Engine& e = ptb::EngineFor(lock);
+		const long long n = e.FitPositions(input, positions, nPoints, output, height, width, planes, fit, fit_params);
+		if (n < 0) { Report("Fitting"); return 0; }
+		return static_cast<uint64_t>(n);
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("Fitting");
+		return 0;
+	}
+}
+
+PTB_API void Wavelett(const uint16_t* input, double* output, uint64_t height, uint64_t width, uint64_t planes, uint64_t levelOutput)
+{
+	ptb::ClearError();
+	try {
+		if (planes == 0) { return; }
+		if (levelOutput == 0) { levelOutput = 1; }
+		const int level = static_cast<int>(std::min<uint64_t>(levelOutput - 1, 2));
+		std::unique_lock<std::mutex> lock;
+		ptb::Engine& e = ptb::EngineFor(lock);
+		if (!e.Planes(input, output, height, width, planes, level)) { Report("Wavelett"); }
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("Wavelett");
+	}
+}
+
+PTB_API double AutoThreshold(const uint16_t* input, uint64_t height, uint64_t width, const double* fit_params)
+{
+	ptb::ClearError();
+	try {
+		std::unique_lock<std::mutex> lock;
+		ptb::Engine& e = ptb::EngineFor(lock);
+		const double t = e.AutoThreshold(input, height, width, fit_params);
+		if (!ptb::LastError().empty()) { Report("AutoThreshold"); }
+		return t;
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("AutoThreshold");
+		return 0.0;
+	}
+}
+
+PTB_API uint64_t PTB_LocalizationDevice(const uint16_t* d_input, double* d_output, uint64_t outputSize, uint64_t height,
+                                        uint64_t width, uint64_t planes, double thresholdVal, double watershedRatio, uint64_t fit,
+                                        const double* fit_params, void* stream)
+{
+	ptb::ClearError();
+	try {
+		std::unique_lock<std::mutex> lock;
+		ptb::Engine& e = ptb::EngineFor(lock);
+		if (!e.Init()) { Report("PTB_LocalizationDevice"); return 0; }
+		const cudaStream_t own = e.Stream();
+		cudaStream_t user = static_cast<cudaStream_t>(stream);
+		// order the engine's stream after the caller's work, and the caller's stream after the engine's
+		cudaEvent_t ev;
+		if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) { return 0; }
+		cudaEventRecord(ev, user);
+		cudaStreamWaitEvent(own, ev, 0);
+		const long long n = e.Localize(d_input, true, d_output, true, outputSize, height, width, planes, thresholdVal,
+		                               watershedRatio, fit, fit_params);
+		cudaEventRecord(ev, own);
+		cudaStreamWaitEvent(user, ev, 0);
+		cudaEventDestroy(ev);
+		if (n < 0) { Report("PTB_LocalizationDevice"); return 0; }
+		return static_cast<uint64_t>(n);
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("PTB_LocalizationDevice");
+		return 0;
+	}
+}
+
+PTB_API int PTB_SetSegmentationMode(int mode)
+{
+	std::unique_lock<std::mutex> lock;
+	return ptb::EngineFor(lock).SetStrict(mode ? 1 : 0);
+}
+
+PTB_API int PTB_SetFitPrecision(int mode)
+{
+	std::unique_lock<std::mutex> lock;
+	return ptb::EngineFor(lock).SetPrecision(mode ? 1 : 0);
+}
+
+PTB_API const char* PTB_LastError(void) { return ptb::LastError().c_str(); }
+
+PTB_API uint64_t PTB_KernelLaunchCount(void) { return ptb::LaunchCount(); }
+
+PTB_API int PTB_SetProfiling(int enable)
+{
+	std::unique_lock<std::mutex> lock;
+	return ptb::EngineFor(lock).SetProfiling(enable ? 1 : 0);
+}
+
+PTB_API void PTB_StageTimes(double* ms, uint64_t* launches, int n)
+{
+	std::unique_lock<std::mutex> lock;
+	ptb::EngineFor(lock).StageTimes(ms, launches, n);
+}
+
+}  // extern "C"

@@ -1,0 +1,533 @@
+// Host side of the localization engine: device workspace, the per-chunk kernel chain and the four reference
+// operations (Localization, Fitting, Wavelett, AutoThreshold) over host or device buffers.
+//
+// A call processes its stack in chunks of B frames sized from a device-memory budget. Every list in the workspace
+// is sized for the worst case of its chunk (all pixels in the domain, every other pixel a component), so no
+// capacity can overflow; the budget only bounds B.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <iostream>
+#include <mutex>
+#include <numeric>
+#include <vector>
+
+namespace ptb {
+
+bool LaunchDetect(const Workspace& ws, double thr, cudaStream_t st);
+bool LaunchPlane(const uint16_t* img, double* out, int H, int W, int B, int level, cudaStream_t st);
+bool LaunchSegment(const Workspace& ws, double ratio, int strict, uint32_t maxPoints, cudaStream_t st);
+bool LaunchBuildCandidates(const Workspace& ws, cudaStream_t st);
+bool LaunchSortFrames(const Workspace& ws, double* out, unsigned long long idBase, unsigned long long planeBase, cudaStream_t st);
+bool LaunchFit(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
+               uint32_t cap, const FitParams& fp, double* rows, uint8_t* flags, int precision, cudaStream_t st);
+
+// ---- error plumbing -------------------------------------------------------------------------------------------
+namespace {
+thread_local std::string g_lastError;
+std::atomic<uint64_t> g_launches{0};
+}  // namespace
+
+void SetError(const std::string& msg)
+{
+	if (g_lastError.empty()) { g_lastError = msg; }
+}
+const std::string& LastError() { return g_lastError; }
+void ClearError() { g_lastError.clear(); }
+void CountLaunch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t LaunchCount() { return g_launches.load(std::memory_order_relaxed); }
+
+bool CheckCuda(cudaError_t e, const char* what, const char* file, int line)
+{
+	if (e == cudaSuccess) { return true; }
+	SetError(std::string(what) + ": " + cudaGetErrorString(e) + " (" + file + ":" + std::to_string(line) + ")");
+	return false;
+}
+
+// ---- fit parameters ------------------------------------------------------------------------------------------
+bool ParseFitParams(uint64_t fit, const double* fp, FitParams& out, std::vector<double>& splineHost)
+{
+	out = FitParams{};
+	out.mode = (fit >= 1 && fit <= 5) ? static_cast<int>(fit) : kNone;
+	out.sigmaX = 1.0;
+	out.sigmaY = 2.0;
+	out.theta = 0.0;
+	if (out.mode == kNone) { return true; }
+	if (fp == nullptr) {
+		SetError("fit_params is null");
+		return false;
+	}
+	if (!(fp[0] >= 1.0) || !std::isfinite(fp[0])) {
+		SetError("fit_params[0] (ROI size) must be >= 1");
+		return false;
+	}
+	int roi = static_cast<int>(static_cast<size_t>(fp[0]));
+	out.roiParam = fp[0];
+	if (out.mode == kSplineEmccd) {
+		// [roi, sx, sy, sz, deltaZ, coefficients SoA [64][sz][sy][sx]] (SplineFit.cpp:36-50)
+		out.sx = static_cast<int>(static_cast<size_t>(fp[1]));
+		out.sy = static_cast<int>(static_cast<size_t>(fp[2]));
+		out.sz = static_cast<int>(static_cast<size_t>(fp[3]));
+		out.deltaZ = fp[4];
+		if (out.sx <= 0 || out.sy <= 0 || out.sz <= 0) {
+			SetError("spline dimensions must be positive");
+			return false;
+		}
+		out.splineSize = static_cast<long long>(out.sx) * out.sy * out.sz;
+		const size_t ncoef = static_cast<size_t>(out.splineSize) * 64;
+		splineHost.assign(fp + 5, fp + 5 + ncoef);
+		const double centre = splineHost[(32 * static_cast<size_t>(out.splineSize)) + (out.sz / 2 * static_cast<size_t>(out.sx) * out.sy) +
+		                                 (out.sy / 2 * static_cast<size_t>(out.sx)) + (out.sx / 2)];
+		out.intensityRatio = std::abs(centre) < 2.220446049250313e-16 ? 1.0 : 4.0 / centre;
+		out.offsetXY = static_cast<long long>(std::floor((static_cast<double>(out.sx) + 1.0 - static_cast<double>(roi)) / 2));
+		out.initZ = static_cast<double>(out.sz) / 2.0;
+		out.nParams = 5;
+	}
+	else {
+		out.sigmaX = fp[1];
+		out.sigmaY = fp[2];
+		out.theta = fp[3];
+		out.nParams = out.mode == kG2Fixed ? 4 : out.mode == kG2Sigma ? 5 : out.mode == kG3Fixed ? 6 : 7;
+	}
+	if (roi % 2 == 0) { roi--; }
+	out.roi = roi;
+	out.half = roi / 2;
+	out.n = roi * roi;
+	return true;
+}
+
+// ---- workspace ------------------------------------------------------------------------------------------------
+namespace {
+
+size_t Align(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
+
+uint32_t IndepBound(int H, int W) { return static_cast<uint32_t>(((H + 1) / 2)) * static_cast<uint32_t>(((W + 1) / 2)); }
+
+}  // namespace
+
+// Bytes of workspace for B frames of H x W with `rowsCap` fit rows.
+static size_t PlanWorkspace(Workspace& ws, int H, int W, int B, uint32_t rowsCap, char* base)
+{
+	Geometry g;
+	g.H = H;
+	g.W = W;
+	g.B = B;
+	g.words = (W + 31) / 32;
+	g.N = static_cast<long long>(H) * W;
+	g.P = g.N * B;
+	ws.g = g;
+	const size_t P = static_cast<size_t>(g.P);
+	const uint32_t capComp = IndepBound(H, W) * static_cast<uint32_t>(B) + 1;
+	ws.capDom = static_cast<uint32_t>(P);
+	ws.capSeed = static_cast<uint32_t>(P);
+	ws.capComp = capComp;
+	ws.capRegion = capComp;
+	ws.capRows = std::max<uint32_t>(1, std::min<uint32_t>(rowsCap, capComp));
+	size_t off = 0;
+	auto take = [&](auto*& ptr, size_t count) {
+		using T = std::remove_pointer_t<std::remove_reference_t<decltype(ptr)>>;
+		const size_t bytes = Align(std::max<size_t>(count, 1) * sizeof(T));
+		if (base) { ptr = reinterpret_cast<T*>(base + off); }
+		off += bytes;
+	};
+	const size_t rows = static_cast<size_t>(g.B) * g.H;
+	take(ws.code, P);
+	take(ws.w1, P);
+	take(ws.par, P);
+	take(ws.lab, P);
+	take(ws.rootmask, rows * g.words);
+	take(ws.rowcnt, rows + 1);
+	take(ws.dom, P);
+	take(ws.seeds, P);
+	take(ws.compRoot, capComp);
+	take(ws.compSize, capComp);
+	take(ws.compNRoot, capComp);
+	take(ws.compNSeed, capComp);
+	take(ws.compRegion, capComp);
+	take(ws.multi, capComp);
+	take(ws.gOff, capComp + 1);
+	take(ws.gSeedOff, capComp + 1);
+	take(ws.gRegOff, capComp + 1);
+	take(ws.gCurPix, capComp + 1);
+	take(ws.gCurSeed, capComp + 1);
+	take(ws.gCurReg, capComp + 1);
+	take(ws.gPix, P);
+	take(ws.gSeed, P);
+	take(ws.gReg, capComp);
+	take(ws.heapKey, P);
+	take(ws.heapPix, P);
+	take(ws.regCount, capComp);
+	take(ws.regSumVJ, capComp);
+	take(ws.regSumVI, capComp);
+	take(ws.regSumV, capComp);
+	take(ws.regFrame, capComp);
+	take(ws.regCand, capComp + 1);
+	take(ws.fuMaxWN, capComp);
+	take(ws.fuMinP, capComp);
+	take(ws.fuMaxP, capComp);
+	take(ws.fuMaxPos, capComp);
+	take(ws.fuWNPos, capComp);
+	take(ws.fuNeighbour, capComp);
+	take(ws.fuBecome, capComp);
+	take(ws.fuLocked, capComp);
+	take(ws.frameRegBase, static_cast<size_t>(B) + 1);
+	take(ws.frameCandBase, static_cast<size_t>(B) + 1);
+	take(ws.frameKeep, static_cast<size_t>(B) + 1);
+	take(ws.frameOutBase, static_cast<size_t>(B) + 1);
+	take(ws.candRegion, ws.capRows);
+	take(ws.candFrame, ws.capRows);
+	take(ws.cand, ws.capRows);
+	take(ws.rows, static_cast<size_t>(ws.capRows) * kCols);
+	take(ws.sortedRows, static_cast<size_t>(ws.capRows) * kCols);
+	take(ws.sortIdx, static_cast<size_t>(ws.capRows) * 2);
+	take(ws.sortKey, static_cast<size_t>(ws.capRows) * 4);
+	take(ws.fitFlag, ws.capRows);
+	take(ws.scanBlock, P / 4096 + 64);
+	take(ws.cnt, 1);
+	return off;
+}
+
+Engine::Engine() = default;
+
+Engine::~Engine()
+{
+	if (pool_) { cudaFree(pool_); }
+	if (img_) { cudaFree(img_); }
+	if (spline_) { cudaFree(spline_); }
+	if (hostCnt_) { cudaFreeHost(hostCnt_); }
+	if (stream_) { cudaStreamDestroy(stream_); }
+}
+
+bool Engine::Init()
+{
+	if (stream_) { return true; }
+	if (!PTB_CUDA(cudaGetDevice(&device_))) { return false; }
+	if (!PTB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking))) { return false; }
+	if (!PTB_CUDA(cudaMallocHost(&hostCnt_, sizeof(Counters)))) { return false; }
+	for (auto& e : ev_) {
+		if (!PTB_CUDA(cudaEventCreate(&e))) { return false; }
+	}
+	size_t freeB = 0, totalB = 0;
+	if (!PTB_CUDA(cudaMemGetInfo(&freeB, &totalB))) { return false; }
+	// default budget: a quarter of free memory, at most 24 GiB (leaves room for callers' own buffers)
+	budget_ = std::min<size_t>(freeB / 4, 24ull << 30);
+	if (const char* env = std::getenv("PTB_WORKSPACE_MB")) { budget_ = static_cast<size_t>(std::atoll(env)) << 20; }
+	return true;
+}
+
+bool Engine::Reserve(int H, int W, int B, uint32_t rowsCap)
+{
+	Workspace probe{};
+	const size_t need = PlanWorkspace(probe, H, W, B, rowsCap, nullptr);
+	if (need > poolBytes_) {
+		if (pool_) { cudaFree(pool_); pool_ = nullptr; poolBytes_ = 0; }
+		if (!PTB_CUDA(cudaMalloc(&pool_, need))) { return false; }
+		poolBytes_ = need;
+	}
+	PlanWorkspace(ws_, H, W, B, rowsCap, static_cast<char*>(pool_));
+	return true;
+}
+
+bool Engine::ReserveImage(size_t bytes)
+{
+	if (bytes <= imgBytes_) { return true; }
+	if (img_) { cudaFree(img_); img_ = nullptr; imgBytes_ = 0; }
+	if (!PTB_CUDA(cudaMalloc(&img_, bytes))) { return false; }
+	imgBytes_ = bytes;
+	return true;
+}
+
+int Engine::ChunkFrames(int H, int W, uint64_t planes, uint32_t maxPoints) const
+{
+	const long long N = static_cast<long long>(H) * W;
+	// bytes per frame: ~40 B per pixel of dense lists plus ~100 B per independent-set slot plus fit rows
+	const double perFrame = 48.0 * N + 100.0 * IndepBound(H, W) +
+	                        std::min<double>(maxPoints, IndepBound(H, W)) * 360.0 + 2.0 * N;
+	long long B = static_cast<long long>(static_cast<double>(budget_) / perFrame);
+	B = std::max<long long>(1, std::min<long long>(B, static_cast<long long>(planes)));
+	// global pixel indices of a chunk stay below 2^31 (the top bit tags component ids)
+	B = std::min<long long>(B, std::max<long long>(1, ((1ll << 31) - 1) / std::max<long long>(N, 1)));
+	return static_cast<int>(B);
+}
+
+// Runs detection -> segmentation -> fits -> ordering for B frames whose pixels are at dImg (device). The chunk's
+// rows go to dOut (device) numbered from Id idBase + 1 and Plane planeBase + 1; returns the row count or -1.
+long long Engine::RunChunk(const uint16_t* dImg, int H, int W, int B, double thr, double ratio, uint32_t maxPoints,
+                           const FitParams& fp, double* dOut, unsigned long long idBase, unsigned long long planeBase,
+                           uint32_t* truncatedFrames)
+{
+	ws_.img = dImg;
+	cudaStream_t st = stream_;
+	const bool prof = profiling_ != 0;
+	uint64_t l0 = LaunchCount(), launches[kStages] = {};
+	auto mark = [&](int k) {
+		if (prof) {
+			cudaEventRecord(ev_[k], st);
+			if (k > 0) { launches[k - 1] = LaunchCount() - l0; l0 = LaunchCount(); }
+		}
+	};
+	bool ok = PTB_CUDA(cudaMemsetAsync(ws_.cnt, 0, sizeof(Counters), st));
+	ok = ok && PTB_CUDA(cudaMemsetAsync(ws_.rootmask, 0, sizeof(uint32_t) * static_cast<size_t>(B) * H * ws_.g.words, st));
+	mark(0);
+	ok = ok && LaunchDetect(ws_, thr, st);
+	mark(1);
+	ok = ok && LaunchSegment(ws_, ratio, strict_, maxPoints, st);
+	ok = ok && LaunchBuildCandidates(ws_, st);
+	mark(2);
+	ok = ok && LaunchFit(dImg, H, W, ws_.g.N, ws_.cand, &ws_.cnt->nfit, 0, ws_.capRows, fp, ws_.rows, ws_.fitFlag, precision_, st);
+	mark(3);
+	ok = ok && LaunchSortFrames(ws_, dOut, idBase, planeBase, st);
+	mark(4);
+	ok = ok && PTB_CUDA(cudaMemcpyAsync(hostCnt_, ws_.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+	ok = ok && PTB_CUDA(cudaStreamSynchronize(st));
+	if (!ok) { return -1; }
+	if (prof) {
+		for (int k = 0; k < 4; ++k) {
+			float ms = 0.f;
+			cudaEventElapsedTime(&ms, ev_[k], ev_[k + 1]);
+			stageMs_[k] += ms;
+			stageLaunches_[k] += launches[k];
+		}
+	}
+	if (hostCnt_->overflow) {
+		SetError("internal capacity overflow");
+		return -1;
+	}
+	if (truncatedFrames) { *truncatedFrames += hostCnt_->truncated; }
+	return hostCnt_->nfit;
+}
+
+long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* output, bool outputOnDevice, uint64_t outputSize,
+                           uint64_t height, uint64_t width, uint64_t planes, double thr, double ratio, uint64_t fit,
+                           const double* fitParams)
+{
+	if (planes == 0 || height == 0 || width == 0) { return 0; }
+	const uint64_t perPlane = (outputSize / kCols) / planes;
+	if (perPlane == 0) { return 0; }
+	if (height > (1u << 30) || width > (1u << 30) || height * width > (1ull << 31) - 1) {
+		SetError("frame too large");
+		return -1;
+	}
+	if (!Init()) { return -1; }
+	FitParams fp;
+	std::vector<double> spline;
+	if (!ParseFitParams(fit, fitParams, fp, spline)) { return -1; }
+	if (!UploadSpline(fp, spline)) { return -1; }
+	const int H = static_cast<int>(height), W = static_cast<int>(width);
+	const uint32_t maxPoints = static_cast<uint32_t>(std::min<uint64_t>(perPlane, 0xffffffffu));
+	const int B = ChunkFrames(H, W, planes, maxPoints);
+	const uint32_t rowsCap = static_cast<uint32_t>(std::min<uint64_t>(static_cast<uint64_t>(B) * maxPoints, 0xffffffffu));
+	if (!Reserve(H, W, B, rowsCap)) { return -1; }
+	const size_t N = static_cast<size_t>(H) * W;
+	if (!inputOnDevice && !ReserveImage(N * B * sizeof(uint16_t))) { return -1; }
+	unsigned long long rows = 0;
+	uint32_t truncated = 0;
+	for (uint64_t z0 = 0; z0 < planes; z0 += B) {
+		const int b = static_cast<int>(std::min<uint64_t>(B, planes - z0));
+		PlanWorkspace(ws_, H, W, b, rowsCap, static_cast<char*>(pool_));
+		const uint16_t* dImg = input + z0 * N;
+		if (!inputOnDevice) {
+			if (!PTB_CUDA(cudaMemcpyAsync(img_, input + z0 * N, N * b * sizeof(uint16_t), cudaMemcpyHostToDevice, stream_))) { return -1; }
+			dImg = static_cast<const uint16_t*>(img_);
+		}
+		double* dOut = outputOnDevice ? output + rows * kCols : ws_.sortedRows;
+		const long long n = RunChunk(dImg, H, W, b, thr, ratio, maxPoints, fp, dOut, rows, z0, &truncated);
+		if (n < 0) { return -1; }
+		if (!outputOnDevice && n > 0) {
+			if (!PTB_CUDA(cudaMemcpyAsync(output + rows * kCols, ws_.sortedRows, static_cast<size_t>(n) * kCols * sizeof(double),
+			                              cudaMemcpyDeviceToHost, stream_))) { return -1; }
+			if (!PTB_CUDA(cudaStreamSynchronize(stream_))) { return -1; }
+		}
+		rows += static_cast<unsigned long long>(n);
+	}
+	for (uint32_t i = 0; i < truncated; ++i) {
+		std::cerr << "[WARNING] Density is too high; some points are missed (output capacity exceeded).\n";
+	}
+	return static_cast<long long>(rows * kCols);
+}
+
+void Engine::StageTimes(double* ms, uint64_t* launches, int n)
+{
+	for (int k = 0; k < kStages && k < n; ++k) {
+		if (ms) { ms[k] = stageMs_[k]; }
+		if (launches) { launches[k] = stageLaunches_[k]; }
+		stageMs_[k] = 0;
+		stageLaunches_[k] = 0;
+	}
+}
+
+bool Engine::UploadSpline(FitParams& fp, const std::vector<double>& spline)
+{
+	if (fp.mode != kSplineEmccd) { return true; }
+	const size_t bytes = spline.size() * sizeof(double);
+	if (bytes > splineBytes_) {
+		if (spline_) { cudaFree(spline_); spline_ = nullptr; splineBytes_ = 0; }
+		if (!PTB_CUDA(cudaMalloc(&spline_, bytes))) { return false; }
+		splineBytes_ = bytes;
+	}
+	if (!PTB_CUDA(cudaMemcpyAsync(spline_, spline.data(), bytes, cudaMemcpyHostToDevice, stream_))) { return false; }
+	fp.coeffs = static_cast<const double*>(spline_);
+	return true;
+}
+
+long long Engine::FitPositions(const uint16_t* input, const double* positions, uint64_t nPoints, double* output,
+                               uint64_t height, uint64_t width, uint64_t planes, uint64_t fit, const double* fitParams)
+{
+	if (nPoints == 0) { return 0; }
+	if (!Init()) { return -1; }
+	FitParams fp;
+	std::vector<double> spline;
+	if (!ParseFitParams(fit, fitParams, fp, spline)) { return -1; }
+	if (!UploadSpline(fp, spline)) { return -1; }
+	const size_t N = static_cast<size_t>(height) * width;
+	std::vector<Cand> cands(nPoints);
+	std::vector<double> localIdx(nPoints);
+	std::vector<uint64_t> perPlane(planes, 0);
+	std::vector<uint8_t> invalid(nPoints, 0);
+	for (uint64_t i = 0; i < nPoints; ++i) {
+		const double* pos = positions + i * 6;
+		const double pl = pos[1];
+		Cand c{};
+		c.x = pos[2];
+		c.y = pos[3];
+		c.intensity = pos[4];
+		c.surf = pos[5];
+		if (!(pl >= 1.0) || static_cast<uint64_t>(pl) > planes) {
+			// the reference indexes outside the stack here; this port returns a border-sentinel row instead
+			invalid[i] = 1;
+			c.x = -1.0;
+			c.y = -1.0;
+			c.frame = 0;
+		}
+		else {
+			const uint64_t p = static_cast<uint64_t>(pl) - 1;
+			c.frame = static_cast<int>(p);
+			localIdx[i] = static_cast<double>(++perPlane[p]);
+		}
+		cands[i] = c;
+	}
+	const size_t imgBytes = N * planes * sizeof(uint16_t);
+	if (!ReserveImage(imgBytes)) { return -1; }
+	if (!PTB_CUDA(cudaMemcpyAsync(img_, input, imgBytes, cudaMemcpyHostToDevice, stream_))) { return -1; }
+	Cand* dCand = nullptr;
+	double* dRows = nullptr;
+	uint8_t* dFlag = nullptr;
+	bool ok = PTB_CUDA(cudaMallocAsync(&dCand, sizeof(Cand) * nPoints, stream_));
+	ok = ok && PTB_CUDA(cudaMallocAsync(&dRows, sizeof(double) * kCols * nPoints, stream_));
+	ok = ok && PTB_CUDA(cudaMallocAsync(&dFlag, nPoints, stream_));
+	ok = ok && PTB_CUDA(cudaMemcpyAsync(dCand, cands.data(), sizeof(Cand) * nPoints, cudaMemcpyHostToDevice, stream_));
+	ok = ok && LaunchFit(static_cast<const uint16_t*>(img_), static_cast<int>(height), static_cast<int>(width),
+	                     static_cast<long long>(N), dCand, nullptr, static_cast<uint32_t>(nPoints), static_cast<uint32_t>(nPoints),
+	                     fp, dRows, dFlag, precision_, stream_);
+	ok = ok && PTB_CUDA(cudaMemcpyAsync(output, dRows, sizeof(double) * kCols * nPoints, cudaMemcpyDeviceToHost, stream_));
+	ok = ok && PTB_CUDA(cudaStreamSynchronize(stream_));
+	if (dCand) { cudaFreeAsync(dCand, stream_); }
+	if (dRows) { cudaFreeAsync(dRows, stream_); }
+	if (dFlag) { cudaFreeAsync(dFlag, stream_); }
+	if (!ok) { return -1; }
+	for (uint64_t i = 0; i < nPoints; ++i) {
+		double* r = output + i * kCols;
+		if (invalid[i]) {
+			r[cX] = positions[i * 6 + 2];
+			r[cY] = positions[i * 6 + 3];
+		}
+		r[cId] = positions[i * 6 + 0];
+		r[cPlane] = positions[i * 6 + 1];
+		r[cIndex] = localIdx[i];
+	}
+	return static_cast<long long>(nPoints * kCols);
+}
+
+bool Engine::Planes(const uint16_t* input, double* output, uint64_t height, uint64_t width, uint64_t planes, int level)
+{
+	if (planes == 0 || height == 0 || width == 0) { return true; }
+	if (!Init()) { return false; }
+	const size_t N = static_cast<size_t>(height) * width;
+	// chunk: input + output doubles within the budget
+	const size_t perFrame = N * (sizeof(uint16_t) + sizeof(double));
+	const uint64_t B = std::max<uint64_t>(1, std::min<uint64_t>(planes, budget_ / perFrame));
+	if (!ReserveImage(N * B * sizeof(uint16_t))) { return false; }
+	double* dOut = nullptr;
+	if (!PTB_CUDA(cudaMallocAsync(&dOut, N * B * sizeof(double), stream_))) { return false; }
+	bool ok = true;
+	for (uint64_t z0 = 0; z0 < planes && ok; z0 += B) {
+		const uint64_t b = std::min<uint64_t>(B, planes - z0);
+		ok = ok && PTB_CUDA(cudaMemcpyAsync(img_, input + z0 * N, N * b * sizeof(uint16_t), cudaMemcpyHostToDevice, stream_));
+		ok = ok && LaunchPlane(static_cast<const uint16_t*>(img_), dOut, static_cast<int>(height), static_cast<int>(width),
+		                       static_cast<int>(b), level, stream_);
+		ok = ok && PTB_CUDA(cudaMemcpyAsync(output + z0 * N, dOut, N * b * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+	}
+	ok = ok && PTB_CUDA(cudaStreamSynchronize(stream_));
+	cudaFreeAsync(dOut, stream_);
+	cudaStreamSynchronize(stream_);
+	return ok;
+}
+
+// AutoThreshold (lib/Palm.cpp:122-172): the standard deviations run on the host in the reference's summation order;
+// each round's detection (fit 0, ratio 10) runs on the GPU.
+double Engine::AutoThreshold(const uint16_t* input, uint64_t height, uint64_t width, const double* fitParams)
+{
+	if (!Init()) { return 0.0; }
+	const size_t size = static_cast<size_t>(height) * width;
+	if (size == 0 || fitParams == nullptr) { return 0.0; }
+	const auto cap = static_cast<uint64_t>(0.2 * static_cast<double>(height * width) * kCols);
+	const double halfRoi = fitParams[0] / 2;
+	double mu = 0.0;
+	for (size_t i = 0; i < size; ++i) { mu += input[i]; }
+	mu /= static_cast<double>(size);
+	double var = 0.0;
+	for (size_t i = 0; i < size; ++i) { var += (input[i] - mu) * (input[i] - mu); }
+	var /= static_cast<double>(size);
+	double thr = std::sqrt(var);
+	std::vector<double> rows(std::max<uint64_t>(cap, kCols));
+	std::vector<char> mask(size);
+	const size_t W = width, H = height;
+	for (int iter = 0; iter < kThresholdIters; ++iter) {
+		const long long n = Localize(input, false, rows.data(), false, cap, height, width, 1, thr, 10.0, 0, fitParams);
+		if (n < 0) { return 0.0; }
+		std::fill(mask.begin(), mask.end(), 0);
+		for (long long k = 0; k < n / kCols; ++k) {
+			const double px = rows[k * kCols + cX], py = rows[k * kCols + cY];
+			const auto x0 = static_cast<size_t>(std::max(0, static_cast<int>(px - halfRoi)));
+			const auto x1 = std::min(W, static_cast<size_t>(px + halfRoi));
+			const auto y0 = static_cast<size_t>(std::max(0, static_cast<int>(py - halfRoi)));
+			const auto y1 = std::min(H, static_cast<size_t>(py + halfRoi));
+			for (size_t y = y0; y < y1; ++y) {
+				for (size_t x = x0; x < x1; ++x) { mask[y * W + x] = 1; }
+			}
+		}
+		size_t count = 0;
+		double sum = 0;
+		for (size_t j = 0; j < size; ++j) {
+			if (!mask[j]) { sum += input[j]; ++count; }
+		}
+		if (count == 0) { break; }
+		mu = sum / static_cast<double>(count);
+		var = 0.0;
+		for (size_t j = 0; j < size; ++j) {
+			if (!mask[j]) { var += (input[j] - mu) * (input[j] - mu); }
+		}
+		var /= static_cast<double>(count);
+		var = std::sqrt(var);
+		if (std::abs(thr - var) <= 2.220446049250313e-16) { break; }
+		thr = var;
+	}
+	return thr;
+}
+
+// One engine per device, guarded by a mutex (calls on one device are serialized).
+Engine& EngineFor(std::unique_lock<std::mutex>& lock)
+{
+	static std::mutex mu;
+	static std::vector<std::unique_ptr<Engine>> engines;
+	int dev = 0;
+	cudaGetDevice(&dev);
+	lock = std::unique_lock<std::mutex>(mu);
+	if (static_cast<int>(engines.size()) <= dev) { engines.resize(dev + 1); }
+	if (!engines[dev]) { engines[dev] = std::make_unique<Engine>(); }
+	return *engines[dev];
+}
+
+}  // namespace ptb

@@ -1,0 +1,75 @@
+// Host engine of the B200 localization path (one per device; calls on a device are serialized by a mutex).
+#pragma once
+
+#include <atomic>
+#include <cstdint>
+#include <cstdlib>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "pt_common.cuh"
+
+namespace ptb {
+
+bool ParseFitParams(uint64_t fit, const double* fp, FitParams& out, std::vector<double>& splineHost);
+uint64_t LaunchCount();
+
+class Engine {
+public:
+	Engine();
+	~Engine();
+	Engine(const Engine&) = delete;
+	Engine& operator=(const Engine&) = delete;
+
+	// Localization over host or device buffers; returns doubles written or -1 (error recorded).
+	long long Localize(const uint16_t* input, bool inputOnDevice, double* output, bool outputOnDevice, uint64_t outputSize,
+	                   uint64_t height, uint64_t width, uint64_t planes, double thr, double ratio, uint64_t fit,
+	                   const double* fitParams);
+	long long FitPositions(const uint16_t* input, const double* positions, uint64_t nPoints, double* output, uint64_t height,
+	                       uint64_t width, uint64_t planes, uint64_t fit, const double* fitParams);
+	bool Planes(const uint16_t* input, double* output, uint64_t height, uint64_t width, uint64_t planes, int level);
+	double AutoThreshold(const uint16_t* input, uint64_t height, uint64_t width, const double* fitParams);
+
+	int SetStrict(int s) { const int o = strict_; strict_ = s; return o; }
+	int SetProfiling(int p) { const int o = profiling_; profiling_ = p; return o; }
+	void StageTimes(double* ms, uint64_t* launches, int n);
+	int SetPrecision(int p) { const int o = precision_; precision_ = p; return o; }
+	cudaStream_t Stream() const { return stream_; }
+	void SetStream(cudaStream_t s) { stream_ = s; }
+	bool Init();
+
+private:
+	bool Reserve(int H, int W, int B, uint32_t rowsCap);
+	bool ReserveImage(size_t bytes);
+	bool UploadSpline(FitParams& fp, const std::vector<double>& spline);
+	int ChunkFrames(int H, int W, uint64_t planes, uint32_t maxPoints) const;
+	long long RunChunk(const uint16_t* dImg, int H, int W, int B, double thr, double ratio, uint32_t maxPoints,
+	                   const FitParams& fp, double* dOut, unsigned long long idBase, unsigned long long planeBase,
+	                   uint32_t* truncatedFrames);
+
+	int device_ = 0;
+	cudaStream_t stream_ = nullptr;
+	Counters* hostCnt_ = nullptr;
+	size_t budget_ = 0;
+	void* pool_ = nullptr;
+	size_t poolBytes_ = 0;
+	void* img_ = nullptr;
+	size_t imgBytes_ = 0;
+	void* spline_ = nullptr;
+	size_t splineBytes_ = 0;
+	Workspace ws_{};
+	int strict_ = 0;
+	int precision_ = 0;
+	int profiling_ = 0;
+	static constexpr int kStages = 5;
+	cudaEvent_t ev_[kStages + 1] = {};
+	double stageMs_[kStages] = {};
+	uint64_t stageLaunches_[kStages] = {};
+};
+
+Engine& EngineFor(std::unique_lock<std::mutex>& lock);
+
+}  // namespace ptb

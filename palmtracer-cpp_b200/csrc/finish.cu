@@ -1,0 +1,138 @@
+// Candidate construction from region sums, per-frame (Y, X) ordering of fitted rows and final row numbering.
+//
+// Reference: SegmentationInfo fields from ComputeStatistics (Segmentation2D.cpp:144-175); per-frame sort with
+// std::weak_order on Y then X (FrameProcessor.cpp:35-39); Id / Plane / Index assignment (lib/Palm.cpp:24-43).
+#include "pt_common.cuh"
+
+namespace ptb {
+
+namespace {
+
+// Region sums are exact integers in 2^-16 units, so x = sum(v j) / sum(v) is the reference's FP64 quotient exactly.
+__global__ void BuildCandidates(Workspace ws)
+{
+	const uint32_t n = min(ws.cnt->nfit, ws.capRows);
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		const uint32_t r = ws.candRegion[k];
+		const double sv = static_cast<double>(ws.regSumV[r]);
+		Cand c;
+		c.x = static_cast<double>(ws.regSumVJ[r]) / sv;
+		c.y = static_cast<double>(ws.regSumVI[r]) / sv;
+		c.intensity = sv * kW1Unit;
+		c.surf = static_cast<double>(ws.regCount[r]);
+		c.frame = static_cast<int>(ws.candFrame[k]);
+		c.pad = 0;
+		ws.cand[k] = c;
+	}
+}
+
+// Total order of std::weak_order on doubles: -NaN < -inf < ... < -0 == +0 < ... < +inf < +NaN.
+__device__ __forceinline__ unsigned long long WeakKey(double d)
+{
+	if (d == 0.0) { d = 0.0; }
+	unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(d));
+	if (isnan(d)) { return (b >> 63) ? 0ull : ~0ull; }
+	return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+constexpr int kSortThreads = 512;
+constexpr int kSmemSort = 2048;  // rows sorted in shared memory; larger frames sort in global scratch
+
+__device__ __forceinline__ bool KeyLess(unsigned long long ya, unsigned long long xa, unsigned long long yb, unsigned long long xb)
+{
+	return ya < yb || (ya == yb && xa < xb);
+}
+
+// Bitonic sort of (ky, kx, idx) over a power-of-two length `len`; entries >= n hold +inf keys.
+template <bool SMEM>
+__device__ void Bitonic(unsigned long long* ky, unsigned long long* kx, uint32_t* id, uint32_t len)
+{
+	for (uint32_t size = 2; size <= len; size <<= 1) {
+		for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+			for (uint32_t t = threadIdx.x; t < len / 2; t += blockDim.x) {
+				const uint32_t lo = 2 * t - (t & (stride - 1));
+				const uint32_t hi = lo + stride;
+				const bool up = (lo & size) == 0;
+				const bool swap = up ? KeyLess(ky[hi], kx[hi], ky[lo], kx[lo]) : KeyLess(ky[lo], kx[lo], ky[hi], kx[hi]);
+				if (swap) {
+					const unsigned long long a = ky[lo], b = kx[lo];
+					const uint32_t c = id[lo];
+					ky[lo] = ky[hi]; kx[lo] = kx[hi]; id[lo] = id[hi];
+					ky[hi] = a; kx[hi] = b; id[hi] = c;
+				}
+			}
+			if (SMEM) { __syncthreads(); }
+			else { __syncthreads(); __threadfence_block(); }
+		}
+	}
+}
+
+__device__ void WriteRow(const double* src, double* dst, double id, double plane, double index)
+{
+	for (int c = 0; c < kCols; ++c) { dst[c] = src[c]; }
+	dst[cId] = id;
+	dst[cPlane] = plane;
+	dst[cIndex] = index;
+}
+
+// One CTA per frame: sort that frame's rows by (Y, X) and write them numbered to out (device memory).
+__global__ void __launch_bounds__(kSortThreads) SortFrames(Workspace ws, double* out, unsigned long long idBase,
+                                                            unsigned long long planeBase, uint32_t capScratch)
+{
+	__shared__ unsigned long long sy[kSmemSort];
+	__shared__ unsigned long long sx[kSmemSort];
+	__shared__ uint32_t si[kSmemSort];
+	const int f = blockIdx.x;
+	const uint32_t base = ws.frameOutBase[f];
+	const uint32_t n = ws.frameOutBase[f + 1] - base;
+	if (n == 0) { return; }
+	uint32_t len = 1;
+	while (len < n) { len <<= 1; }
+	const double* rows = ws.rows + static_cast<long long>(base) * kCols;
+	unsigned long long *ky, *kx;
+	uint32_t* id;
+	const bool smem = len <= static_cast<uint32_t>(kSmemSort);
+	if (smem) { ky = sy; kx = sx; id = si; }
+	else {
+		// global scratch of this frame: 2 * len keys from 4 * base and len indices from 2 * base (len < 2 n, so frames
+		// never overlap; the key scratch holds 4 * capRows and the index scratch 2 * capRows entries)
+		if (4ull * base + 2ull * len > 4ull * capScratch) { return; }
+		ky = reinterpret_cast<unsigned long long*>(ws.sortKey) + 4ull * base;
+		kx = ky + len;
+		id = ws.sortIdx + 2ull * base;
+	}
+	for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
+		if (i < n) {
+			ky[i] = WeakKey(rows[static_cast<long long>(i) * kCols + cY]);
+			kx[i] = WeakKey(rows[static_cast<long long>(i) * kCols + cX]);
+		}
+		else { ky[i] = ~0ull; kx[i] = ~0ull; }
+		id[i] = i;
+	}
+	__syncthreads();
+	if (smem) { Bitonic<true>(ky, kx, id, len); }
+	else { Bitonic<false>(ky, kx, id, len); }
+	for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+		WriteRow(rows + static_cast<long long>(id[i]) * kCols, out + (static_cast<long long>(base) + i) * kCols,
+		         static_cast<double>(idBase + base + i + 1), static_cast<double>(planeBase + f + 1), static_cast<double>(i + 1));
+	}
+}
+
+}  // namespace
+
+bool LaunchBuildCandidates(const Workspace& ws, cudaStream_t st)
+{
+	BuildCandidates<<<148 * 4, 256, 0, st>>>(ws);
+	CountLaunch();
+	return PTB_LAUNCHED();
+}
+
+// out: device destination of the chunk's first row (rows already offset by the caller).
+bool LaunchSortFrames(const Workspace& ws, double* out, unsigned long long idBase, unsigned long long planeBase, cudaStream_t st)
+{
+	SortFrames<<<ws.g.B, kSortThreads, 0, st>>>(ws, out, idBase, planeBase, ws.capRows);
+	CountLaunch();
+	return PTB_LAUNCHED();
+}
+
+}  // namespace ptb

@@ -1,0 +1,144 @@
+// Shared definitions of the B200 localization engine: constants of the reference algorithm, error plumbing and
+// the device workspace layout of one chunk of frames.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+namespace ptb {
+
+// ---- Constants of the reference algorithm (lib/Constants.hpp:20-24, 53; Segmentation2D.hpp:80; Fitting.hpp:80)
+constexpr int kCols = 18;            // columns of one localization row
+constexpr double kEps = 1e-7;        // EPSILON: watershed aging step and fill() guards
+constexpr double kSeedFloor = 1e-8;  // potentials above this join the watershed domain
+constexpr double kVolumeMin = 4;     // a region needs surf > 4
+constexpr int kMaxIter = 75;         // LM iteration cap
+constexpr int kThresholdIters = 5;   // AutoThreshold rounds
+
+// Column indices (lib/Constants.hpp:31-51)
+enum Col : int {
+	cId = 0, cPlane, cIndex, cChannel, cX, cY, cZ, cIntensity, cSigmaX, cSigmaY, cTheta,
+	cQualityXY, cQualityZ, cAmplitude, cOffset, cSegIntensity, cSurface, cCircularity
+};
+
+// Fit modes (lib/fit/Fitting.hpp:22-30)
+enum FitMode : int { kNone = 0, kG2Fixed = 1, kG2Sigma = 2, kG3Fixed = 3, kG3Theta = 4, kSplineEmccd = 5 };
+
+// Per-pixel code byte written by the detection kernel.
+constexpr uint8_t kDomain = 1;  // thresholded potential > 1e-8: the watershed floods it
+constexpr uint8_t kSeed = 2;    // local maximum of the thresholded potential
+constexpr int kDirShift = 2;    // bits 2..4: raster-earlier seed neighbour a seed inherits its label from (0 = root)
+
+// W1 values are exact multiples of 2^-16 (B3 taps are dyadic and the input is uint16), kept as int64 "fixed" units.
+constexpr double kW1Unit = 1.0 / 65536.0;
+
+// Component id tag stored in par[root] once components are enumerated.
+constexpr uint32_t kCompTag = 0x80000000u;
+
+// ---- Error plumbing: no exception crosses the C ABI; the first failure of a call is recorded per thread.
+void SetError(const std::string& msg);
+const std::string& LastError();
+void ClearError();
+bool CheckCuda(cudaError_t e, const char* what, const char* file, int line);
+void CountLaunch(uint64_t n = 1);
+
+#define PTB_CUDA(call) ::ptb::CheckCuda((call), #call, __FILE__, __LINE__)
+#define PTB_LAUNCHED() ::ptb::CheckCuda(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+
+// ---- Device counters of one chunk (one struct in device memory, read back once per chunk).
+struct Counters {
+	uint32_t ndom;      // domain pixels appended to dom[]
+	uint32_t nseed;     // seed pixels appended to seeds[]
+	uint32_t ncomp;     // connected components of the domain
+	uint32_t nmulti;    // components holding more than one region
+	uint32_t nregion;   // regions (root seeds)
+	uint32_t ncand;     // regions with surf > 4
+	uint32_t nfit;      // candidates kept under the per-plane capacity
+	uint32_t overflow;  // a list outgrew its capacity (the chunk must be redone with room)
+	uint32_t truncated; // some plane had more candidates than the per-plane capacity
+	uint32_t refit;     // FP32 fits redone in FP64
+	uint32_t pad[6];
+};
+
+// One fit input: a segmentation candidate (x_, y_, intensity_, surf_ of SegmentationInfo) or a caller position.
+struct Cand {
+	double x, y, intensity, surf;
+	int frame;  // plane within the device stack the ROI is read from
+	int pad;
+};
+
+// Fit configuration passed by value to the fit kernels.
+struct FitParams {
+	int mode;        // FitMode
+	int roi;         // forced odd
+	int half;
+	int n;           // roi * roi
+	int nParams;
+	double sigmaX, sigmaY, theta;
+	// spline (mode 5)
+	int sx, sy, sz;
+	long long splineSize;  // sx * sy * sz
+	long long offsetXY;
+	double roiParam, initZ, deltaZ, intensityRatio;
+	const double* coeffs;  // device, SoA [64][sz][sy][sx]
+};
+
+// Geometry of one chunk: B frames of H x W pixels; global pixel index g = f * N + y * W + x (fits in 31 bits).
+struct Geometry {
+	int H, W, B;
+	int words;  // 32-bit words per row of the root bitmask
+	long long N;
+	long long P;  // B * N
+};
+
+// Device workspace of one chunk. Dense arrays have P entries, lists have their stated capacities.
+struct Workspace {
+	Geometry g;
+	// dense
+	const uint16_t* img;  // the chunk's frames (device)
+	uint8_t* code;
+	long long* w1;        // W1 in 2^-16 units, valid on domain pixels only
+	uint32_t* par;        // union-find parent, then component id tag at roots
+	uint32_t* lab;        // region id + 1 on labelled domain pixels
+	uint32_t* rootmask;   // [B][H][words] bit set at root seeds
+	uint32_t* rowcnt;     // [B*H + 1] root seeds per row, scanned in place to row offsets
+	// lists
+	uint32_t* dom;   uint32_t capDom;
+	uint32_t* seeds; uint32_t capSeed;
+	// components
+	uint32_t capComp;
+	uint32_t* compRoot; uint32_t* compSize; uint32_t* compNRoot; uint32_t* compNSeed; uint32_t* compRegion;
+	uint32_t* multi;      // ids of multi-region components (groups)
+	uint32_t* gOff; uint32_t* gSeedOff; uint32_t* gRegOff;  // exclusive scans over groups
+	uint32_t* gCurPix; uint32_t* gCurSeed; uint32_t* gCurReg;
+	uint32_t* gPix;  uint32_t* gSeed; uint32_t* gReg;       // per-group pixel, seed and region lists
+	double* heapKey; uint32_t* heapPix;                     // per-group heaps (capacity = group size)
+	// regions
+	uint32_t capRegion;
+	uint32_t* regCount; unsigned long long* regSumVJ; unsigned long long* regSumVI; unsigned long long* regSumV;
+	uint32_t* regFrame;   // frame (within the chunk) of each region
+	uint32_t* regCand;    // exclusive scan of (surf > 4) over regions
+	// fusion scratch, indexed by region id
+	double* fuMaxWN; double* fuMinP; double* fuMaxP; uint32_t* fuMaxPos; uint32_t* fuWNPos; uint32_t* fuNeighbour;
+	uint32_t* fuBecome; uint8_t* fuLocked;
+	// per frame [B + 1]
+	uint32_t* frameRegBase; uint32_t* frameCandBase; uint32_t* frameKeep; uint32_t* frameOutBase;
+	// candidates / rows
+	uint32_t capRows;
+	uint32_t* candRegion;  // region of each kept candidate, ordered by (frame, label)
+	uint32_t* candFrame;
+	struct Cand* cand;     // fit inputs built from the regions
+	double* rows;          // [capRows][18], unsorted fit results
+	double* sortedRows;    // [capRows][18], per-frame (Y, X) order with Id/Plane/Index
+	uint32_t* sortIdx;     // scratch for the per-frame sort
+	double* sortKey;
+	uint8_t* fitFlag;      // FP32 fits that need an FP64 re-run
+	// scan scratch
+	uint32_t* scanBlock;   // block sums
+	Counters* cnt;
+};
+
+}  // namespace ptb

@@ -1,0 +1,668 @@
+// Segmentation of the thresholded wavelet plane on the GPU: seeds, watershed, basin fusion, region statistics and
+// the ordered candidate list. Reference: lib/localization/Segmentation2D.cpp (whole file) and SegmentationInfo.hpp.
+//
+// Data flow for one chunk of frames (global pixel index g = frame * N + y * W + x):
+//   1. union-find connected components of the domain (8-connectivity) over the sparse domain list;
+//   2. each seed (local maximum) inherits the label of its first raster-earlier seed neighbour, as getLocalMax()
+//      does (Segmentation2D.cpp:309-327); root seeds are numbered in raster order through a per-row bitmask rank;
+//   3. a component with one label is labelled directly; every other component (a "group") is flooded by one thread
+//      with a binary heap whose push/pop steps are those of libstdc++'s std::priority_queue, with the reference key
+//      -v + pops * 1e-7 (Segmentation2D.cpp:336-385) and a pop counter local to the group. In strict mode a group is
+//      a whole frame and the counter is frame-global, which is the reference's process exactly;
+//   4. basin fusion (Segmentation2D.cpp:181-291) per group, then a second flood from one seed per basin;
+//   5. exact integer region sums (W1 is an integer in 2^-16 units) and the surf > 4 filter, in label order.
+#include "pt_common.cuh"
+
+namespace ptb {
+
+bool ExclusiveScan(uint32_t* data, const uint32_t* nptr, uint32_t nconst, uint32_t cap, uint32_t* blockSums,
+                   uint32_t* totalOut, cudaStream_t st);
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kGrid = 148 * 8;  // grid-stride kernels over device-side counts: 8 CTAs per SM
+
+struct Pix {
+	int f, y, x;
+};
+
+__device__ __forceinline__ Pix Decompose(uint32_t g, const Geometry& geo)
+{
+	Pix p;
+	p.f = static_cast<int>(g / static_cast<unsigned long long>(geo.N));
+	const long long r = static_cast<long long>(g) - static_cast<long long>(p.f) * geo.N;
+	p.y = static_cast<int>(r / geo.W);
+	p.x = static_cast<int>(r - static_cast<long long>(p.y) * geo.W);
+	return p;
+}
+
+__device__ __forceinline__ uint32_t Find(const uint32_t* par, uint32_t x)
+{
+	uint32_t p = __ldcg(par + x);
+	while (p != x) {
+		x = p;
+		p = __ldcg(par + x);
+	}
+	return x;
+}
+
+// Union by smaller index; every root ends as the raster-first pixel of its component.
+__device__ void Unite(uint32_t* par, uint32_t a, uint32_t b)
+{
+	for (;;) {
+		a = Find(par, a);
+		b = Find(par, b);
+		if (a == b) { return; }
+		if (a < b) {
+			const uint32_t t = a;
+			a = b;
+			b = t;
+		}
+		const uint32_t old = atomicMin(par + a, b);
+		if (old == a) { return; }
+		a = old;
+	}
+}
+
+__device__ __forceinline__ uint32_t CompOf(const uint32_t* par, uint32_t p)
+{
+	const uint32_t x = __ldcg(par + p);
+	if (x & kCompTag) { return x & ~kCompTag; }
+	return __ldcg(par + x) & ~kCompTag;
+}
+
+__global__ void CclInit(Workspace ws)
+{
+	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		const uint32_t p = ws.dom[k];
+		ws.par[p] = p;
+	}
+}
+
+__global__ void CclUnion(Workspace ws)
+{
+	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
+	const Geometry& geo = ws.g;
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		const uint32_t p = ws.dom[k];
+		const Pix q = Decompose(p, geo);
+		// raster-earlier neighbours: (y-1, x-1), (y-1, x), (y-1, x+1), (y, x-1)
+		if (q.y > 0) {
+			const uint32_t up = p - static_cast<uint32_t>(geo.W);
+			if (q.x > 0 && (ws.code[up - 1] & kDomain)) { Unite(ws.par, p, up - 1); }
+			if (ws.code[up] & kDomain) { Unite(ws.par, p, up); }
+			if (q.x + 1 < geo.W && (ws.code[up + 1] & kDomain)) { Unite(ws.par, p, up + 1); }
+		}
+		if (q.x > 0 && (ws.code[p - 1] & kDomain)) { Unite(ws.par, p, p - 1); }
+	}
+}
+
+__global__ void CclFlatten(Workspace ws)
+{
+	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		const uint32_t p = ws.dom[k];
+		ws.par[p] = Find(ws.par, p);
+	}
+}
+
+// Components: enumerate roots and tag par[root] with the component id.
+__global__ void CompEnumerate(Workspace ws)
+{
+	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		const uint32_t p = ws.dom[k];
+		if (ws.par[p] != p) { continue; }
+		const uint32_t c = atomicAdd(&ws.cnt->ncomp, 1u);
+		if (c >= ws.capComp) { atomicExch(&ws.cnt->overflow, 1u); continue; }
+		ws.compRoot[c] = p;
+		ws.compSize[c] = 0;
+		ws.compNRoot[c] = 0;
+		ws.compNSeed[c] = 0;
+		ws.par[p] = c | kCompTag;
+	}
+}
+
+__global__ void CompCount(Workspace ws)
+{
+	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		const uint32_t p = ws.dom[k];
+		atomicAdd(ws.compSize + CompOf(ws.par, p), 1u);
+	}
+}
+
+// Seed parents (Segmentation2D.cpp:309-327): first seed among (y-1,x-1), (y-1,x), (y-1,x+1), (y,x-1); none = root.
+__global__ void SeedParent(Workspace ws)
+{
+	const uint32_t n = min(ws.cnt->nseed, ws.capSeed);
+	const Geometry& geo = ws.g;
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		const uint32_t s = ws.seeds[k];
+		const Pix q = Decompose(s, geo);
+		int dir = 0;
+		if (q.y > 0) {
+			const uint32_t up = s - static_cast<uint32_t>(geo.W);
+			if (q.x > 0 && (ws.code[up - 1] & kSeed)) { dir = 1; }
+			else if (ws.code[up] & kSeed) { dir = 2; }
+			else if (q.x + 1 < geo.W && (ws.code[up + 1] & kSeed)) { dir = 3; }
+		}
+		if (dir == 0 && q.x > 0 && (ws.code[s - 1] & kSeed)) { dir = 4; }
+		if (dir != 0) { ws.code[s] = static_cast<uint8_t>(ws.code[s] | (dir << kDirShift)); }
+		else {
+			const long long row = static_cast<long long>(q.f) * geo.H + q.y;
+			atomicOr(ws.rootmask + row * geo.words + (q.x >> 5), 1u << (q.x & 31));
+		}
+	}
+}
+
+__global__ void RowCount(Workspace ws)
+{
+	const Geometry& geo = ws.g;
+	const long long rows = static_cast<long long>(geo.B) * geo.H;
+	for (long long r = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; r < rows; r += gridDim.x * static_cast<long long>(blockDim.x)) {
+		uint32_t c = 0;
+		const uint32_t* w = ws.rootmask + r * geo.words;
+		for (int i = 0; i < geo.words; ++i) { c += __popc(w[i]); }
+		ws.rowcnt[r] = c;
+	}
+}
+
+__device__ __forceinline__ uint32_t SeedRoot(const Workspace& ws, uint32_t s)
+{
+	const uint32_t W = static_cast<uint32_t>(ws.g.W);
+	for (;;) {
+		const int dir = (ws.code[s] >> kDirShift) & 7;
+		if (dir == 0) { return s; }
+		s = dir == 1 ? s - W - 1 : dir == 2 ? s - W : dir == 3 ? s - W + 1 : s - 1;
+	}
+}
+
+// Region id of a root seed: raster rank among root seeds of the chunk (frame-major, so labels follow raster order).
+__device__ __forceinline__ uint32_t RegionOfRoot(const Workspace& ws, uint32_t rs)
+{
+	const Pix q = Decompose(rs, ws.g);
+	const long long row = static_cast<long long>(q.f) * ws.g.H + q.y;
+	const uint32_t* w = ws.rootmask + row * ws.g.words;
+	uint32_t rank = ws.rowcnt[row];
+	const int word = q.x >> 5;
+	for (int i = 0; i < word; ++i) { rank += __popc(w[i]); }
+	rank += __popc(w[word] & ((1u << (q.x & 31)) - 1u));
+	return rank;
+}
+
+__global__ void SeedLabel(Workspace ws)
+{
+	const uint32_t n = min(ws.cnt->nseed, ws.capSeed);
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		const uint32_t s = ws.seeds[k];
+		const uint32_t rs = SeedRoot(ws, s);
+		const uint32_t r = RegionOfRoot(ws, rs);
+		if (r >= ws.capRegion) { atomicExch(&ws.cnt->overflow, 1u); continue; }
+		ws.lab[s] = r + 1;
+		const uint32_t c = CompOf(ws.par, s);
+		atomicAdd(ws.compNSeed + c, 1u);
+		if (rs == s) {
+			ws.regCount[r] = 0;
+			ws.regSumV[r] = 0;
+			ws.regSumVJ[r] = 0;
+			ws.regSumVI[r] = 0;
+			ws.regFrame[r] = Decompose(s, ws.g).f;
+			atomicAdd(ws.compNRoot + c, 1u);
+			ws.compRegion[c] = r;
+		}
+	}
+}
+
+// Single-region components are labelled outright; flooded pixels of groups start unlabelled (seeds keep theirs).
+__global__ void LabelDomain(Workspace ws, int strict)
+{
+	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		const uint32_t p = ws.dom[k];
+		if (ws.code[p] & kSeed) { continue; }
+		const uint32_t c = CompOf(ws.par, p);
+		ws.lab[p] = (!strict && ws.compNRoot[c] == 1) ? ws.compRegion[c] + 1 : 0u;
+	}
+}
+
+// Groups (fast mode): components with two or more regions. Sizes go to the offset arrays, scanned next.
+__global__ void GroupEnumerate(Workspace ws)
+{
+	const uint32_t n = min(ws.cnt->ncomp, ws.capComp);
+	for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+		if (ws.compNRoot[c] < 2) { continue; }
+		const uint32_t m = atomicAdd(&ws.cnt->nmulti, 1u);
+		ws.multi[m] = c;
+		ws.compRegion[c] = m;  // from here on: the group index of a multi-region component
+		ws.gOff[m] = ws.compSize[c];
+		ws.gSeedOff[m] = ws.compNSeed[c];
+		ws.gRegOff[m] = ws.compNRoot[c];
+		ws.gCurPix[m] = 0;
+		ws.gCurSeed[m] = 0;
+		ws.gCurReg[m] = 0;
+	}
+}
+
+// Groups (strict mode): one per frame; sizes by atomics.
+__global__ void GroupSizesStrict(Workspace ws)
+{
+	const uint32_t nd = min(ws.cnt->ndom, ws.capDom);
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nd; k += gridDim.x * blockDim.x) {
+		atomicAdd(ws.gOff + Decompose(ws.dom[k], ws.g).f, 1u);
+	}
+	const uint32_t ns = min(ws.cnt->nseed, ws.capSeed);
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ns; k += gridDim.x * blockDim.x) {
+		const uint32_t s = ws.seeds[k];
+		const int f = Decompose(s, ws.g).f;
+		atomicAdd(ws.gSeedOff + f, 1u);
+		if (((ws.code[s] >> kDirShift) & 7) == 0) { atomicAdd(ws.gRegOff + f, 1u); }
+	}
+}
+
+__device__ __forceinline__ int GroupOf(const Workspace& ws, uint32_t p, int strict)
+{
+	if (strict) { return Decompose(p, ws.g).f; }
+	const uint32_t c = CompOf(ws.par, p);
+	return ws.compNRoot[c] >= 2 ? static_cast<int>(ws.compRegion[c]) : -1;
+}
+
+__global__ void GroupScatter(Workspace ws, int strict)
+{
+	const uint32_t nd = min(ws.cnt->ndom, ws.capDom);
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nd; k += gridDim.x * blockDim.x) {
+		const uint32_t p = ws.dom[k];
+		const int m = GroupOf(ws, p, strict);
+		if (m < 0) { continue; }
+		ws.gPix[ws.gOff[m] + atomicAdd(ws.gCurPix + m, 1u)] = p;
+	}
+	const uint32_t ns = min(ws.cnt->nseed, ws.capSeed);
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ns; k += gridDim.x * blockDim.x) {
+		const uint32_t s = ws.seeds[k];
+		const int m = GroupOf(ws, s, strict);
+		if (m < 0) { continue; }
+		ws.gSeed[ws.gSeedOff[m] + atomicAdd(ws.gCurSeed + m, 1u)] = s;
+		if (((ws.code[s] >> kDirShift) & 7) == 0) { ws.gReg[ws.gRegOff[m] + atomicAdd(ws.gCurReg + m, 1u)] = ws.lab[s] - 1; }
+	}
+}
+
+// In-place ascending heapsort of a small uint32 slice (one thread).
+__device__ void SortSlice(uint32_t* a, uint32_t n)
+{
+	if (n < 2) { return; }
+	auto sift = [a](uint32_t i, uint32_t len) {
+		const uint32_t v = a[i];
+		for (;;) {
+			uint32_t c = 2 * i + 1;
+			if (c >= len) { break; }
+			if (c + 1 < len && a[c + 1] > a[c]) { ++c; }
+			if (a[c] <= v) { break; }
+			a[i] = a[c];
+			i = c;
+		}
+		a[i] = v;
+	};
+	for (uint32_t i = n / 2; i-- > 0;) { sift(i, n); }
+	for (uint32_t end = n - 1; end > 0; --end) {
+		const uint32_t t = a[0];
+		a[0] = a[end];
+		a[end] = t;
+		sift(0, end);
+	}
+}
+
+// Binary heap with the steps of libstdc++'s push_heap / pop_heap (bits/stl_heap.h) under the reference comparator
+// (Pixel::operator<, lib/Structs.hpp:20-27): "a before b" iff a.key > b.key, so the top holds the smallest key and
+// equal keys come out in the same order as from the reference's std::priority_queue.
+struct Heap {
+	double* key;
+	uint32_t* pix;
+	uint32_t len;
+
+	__device__ __forceinline__ static bool Less(double a, double b) { return a > b; }
+
+	__device__ void SiftUp(uint32_t hole, uint32_t top, double k, uint32_t v)
+	{
+		uint32_t parent = (hole - 1) / 2;
+		while (hole > top && Less(key[parent], k)) {
+			key[hole] = key[parent];
+			pix[hole] = pix[parent];
+			hole = parent;
+			parent = (hole - 1) / 2;
+		}
+		key[hole] = k;
+		pix[hole] = v;
+	}
+
+	__device__ void Push(double k, uint32_t v)
+	{
+		const uint32_t hole = len++;
+		if (hole == 0) { key[0] = k; pix[0] = v; return; }
+		SiftUp(hole, 0, k, v);
+	}
+
+	// Removes the top; returns its pixel.
+	__device__ uint32_t Pop()
+	{
+		const uint32_t top = pix[0];
+		if (len > 1) {
+			const uint32_t last = len - 1;  // element moved out of the way ("value" in __pop_heap)
+			const double vk = key[last];
+			const uint32_t vp = pix[last];
+			// __adjust_heap(first, 0, len = last, value)
+			const uint32_t n = last;
+			uint32_t hole = 0, child = 0;
+			while (n >= 2 && child < (n - 1) / 2) {
+				child = 2 * (child + 1);
+				if (Less(key[child], key[child - 1])) { --child; }
+				key[hole] = key[child];
+				pix[hole] = pix[child];
+				hole = child;
+			}
+			if ((n & 1) == 0 && child == (n - 2) / 2) {
+				child = 2 * (child + 1);
+				key[hole] = key[child - 1];
+				pix[hole] = pix[child - 1];
+				hole = child - 1;
+			}
+			if (hole == 0) { key[0] = vk; pix[0] = vp; }
+			else { SiftUp(hole, 0, vk, vp); }
+		}
+		--len;
+		return top;
+	}
+};
+
+// Priority flood of one group from its labelled seeds (sorted ascending = raster order), Segmentation2D.cpp:336-385.
+__device__ void FloodGroup(const Workspace& ws, const uint32_t* seedList, uint32_t nSeeds, double* hk, uint32_t* hp)
+{
+	const Geometry& geo = ws.g;
+	Heap heap{hk, hp, 0};
+	for (uint32_t i = 0; i < nSeeds; ++i) {
+		const uint32_t s = seedList[i];
+		const Pix q = Decompose(s, geo);
+		bool open = false;
+		for (int dy = -1; dy <= 1 && !open; ++dy) {
+			const int yy = q.y + dy;
+			if (yy < 0 || yy >= geo.H) { continue; }
+			for (int dx = -1; dx <= 1 && !open; ++dx) {
+				const int xx = q.x + dx;
+				if ((dx == 0 && dy == 0) || xx < 0 || xx >= geo.W) { continue; }
+				const uint32_t nb = s + static_cast<uint32_t>(dy * geo.W + dx);
+				if (!(ws.code[nb] & kDomain) || ws.lab[nb] == 0) { open = true; }
+			}
+		}
+		if (open) { heap.Push(-(static_cast<double>(ws.w1[s]) * kW1Unit), s); }
+	}
+	unsigned long long pops = 0;
+	while (heap.len > 0) {
+		const uint32_t p = heap.Pop();
+		++pops;
+		const Pix q = Decompose(p, geo);
+		const uint32_t L = ws.lab[p];
+		for (int dy = -1; dy <= 1; ++dy) {
+			const int yy = q.y + dy;
+			if (yy < 0 || yy >= geo.H) { continue; }
+			for (int dx = -1; dx <= 1; ++dx) {
+				const int xx = q.x + dx;
+				if ((dx == 0 && dy == 0) || xx < 0 || xx >= geo.W) { continue; }
+				const uint32_t nb = p + static_cast<uint32_t>(dy * geo.W + dx);
+				if ((ws.code[nb] & kDomain) && ws.lab[nb] == 0) {
+					// key = -v + it * EPSILON, both operations rounded separately as in the reference
+					const double k = __dadd_rn(-(static_cast<double>(ws.w1[nb]) * kW1Unit), __dmul_rn(static_cast<double>(pops), kEps));
+					heap.Push(k, nb);
+					ws.lab[nb] = L;
+				}
+			}
+		}
+	}
+}
+
+__global__ void GroupFlood(Workspace ws, uint32_t nGroupsStrict)
+{
+	const uint32_t n = nGroupsStrict ? nGroupsStrict : ws.cnt->nmulti;
+	for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+		const uint32_t nSeeds = ws.gSeedOff[m + 1] - ws.gSeedOff[m];
+		uint32_t* seeds = ws.gSeed + ws.gSeedOff[m];
+		SortSlice(seeds, nSeeds);
+		FloodGroup(ws, seeds, nSeeds, ws.heapKey + ws.gOff[m], ws.heapPix + ws.gOff[m]);
+	}
+}
+
+// Basin fusion of one group (Segmentation2D.cpp:181-291) followed by the reseeded second flood.
+__global__ void GroupFuse(Workspace ws, uint32_t nGroupsStrict, double ratio)
+{
+	const uint32_t n = nGroupsStrict ? nGroupsStrict : ws.cnt->nmulti;
+	const Geometry& geo = ws.g;
+	for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+		uint32_t* regs = ws.gReg + ws.gRegOff[m];
+		uint32_t nReg = ws.gRegOff[m + 1] - ws.gRegOff[m];
+		const uint32_t* pix = ws.gPix + ws.gOff[m];
+		const uint32_t nPix = ws.gOff[m + 1] - ws.gOff[m];
+		if (nReg == 0) { continue; }
+		SortSlice(regs, nReg);  // label order
+		for (uint32_t iter = 0; iter <= nReg; ++iter) {
+			for (uint32_t i = 0; i < nReg; ++i) {
+				const uint32_t r = regs[i];
+				ws.fuMaxWN[r] = -1e10;
+				ws.fuMinP[r] = 1e10;
+				ws.fuMaxP[r] = -1e10;
+				ws.fuMaxPos[r] = 0xffffffffu;
+				ws.fuWNPos[r] = 0xffffffffu;
+				ws.fuNeighbour[r] = 0;
+				ws.fuLocked[r] = 0;
+				ws.fuBecome[r] = r;
+			}
+			for (uint32_t i = 0; i < nPix; ++i) {
+				const uint32_t p = pix[i];
+				const uint32_t L = ws.lab[p];
+				if (L == 0) { continue; }
+				const uint32_t r = L - 1;
+				const double v = static_cast<double>(ws.w1[p]) * kW1Unit;
+				ws.fuMinP[r] = fmin(ws.fuMinP[r], v);
+				// first raster pixel reaching the maximum (strict > in raster order)
+				if (v > ws.fuMaxP[r] || (v == ws.fuMaxP[r] && p < ws.fuMaxPos[r])) {
+					ws.fuMaxP[r] = v;
+					ws.fuMaxPos[r] = p;
+				}
+				// strongest boundary pixel; its first differently-labelled neighbour in 3x3 scan order
+				const Pix q = Decompose(p, geo);
+				uint32_t other = 0;
+				for (int dy = -1; dy <= 1 && other == 0; ++dy) {
+					const int yy = q.y + dy;
+					if (yy < 0 || yy >= geo.H) { continue; }
+					for (int dx = -1; dx <= 1 && other == 0; ++dx) {
+						const int xx = q.x + dx;
+						if ((dx == 0 && dy == 0) || xx < 0 || xx >= geo.W) { continue; }
+						const uint32_t nb = p + static_cast<uint32_t>(dy * geo.W + dx);
+						if (!(ws.code[nb] & kDomain)) { continue; }
+						const uint32_t nl = ws.lab[nb];
+						if (nl != 0 && nl != L) { other = nl; }
+					}
+				}
+				if (other != 0 && (v > ws.fuMaxWN[r] || (v == ws.fuMaxWN[r] && p < ws.fuWNPos[r]))) {
+					ws.fuMaxWN[r] = v;
+					ws.fuWNPos[r] = p;
+					ws.fuNeighbour[r] = other;
+				}
+			}
+			bool change = false;
+			for (uint32_t i = 0; i < nReg; ++i) {
+				const uint32_t r = regs[i];
+				if (ws.fuNeighbour[r] == 0) { continue; }
+				const uint32_t nb = ws.fuNeighbour[r] - 1;
+				if (ws.fuLocked[r] || ws.fuLocked[nb]) { continue; }
+				const double delta = ws.fuMaxP[r] - ws.fuMinP[r];
+				if (fabs(delta) <= 2.220446049250313e-16) { continue; }
+				const double rr = (ws.fuMaxP[r] - ws.fuMaxWN[r]) / delta;
+				if (rr < ratio && ws.fuMaxP[r] < ws.fuMaxP[nb]) {
+					ws.fuBecome[r] = nb;
+					ws.fuLocked[nb] = 1;
+					ws.fuLocked[r] = 1;
+					change = true;
+				}
+			}
+			if (!change) { break; }
+			for (uint32_t i = 0; i < nPix; ++i) {
+				const uint32_t p = pix[i];
+				const uint32_t L = ws.lab[p];
+				if (L != 0) { ws.lab[p] = ws.fuBecome[L - 1] + 1; }
+			}
+			uint32_t kept = 0;
+			for (uint32_t i = 0; i < nReg; ++i) {
+				if (ws.fuBecome[regs[i]] == regs[i]) { regs[kept++] = regs[i]; }
+			}
+			nReg = kept;
+		}
+		// one seed per basin at its first maximum, then flood again
+		for (uint32_t i = 0; i < nPix; ++i) { ws.lab[pix[i]] = 0; }
+		uint32_t* seeds = ws.gSeed + ws.gSeedOff[m];  // reuse the seed slice (nReg <= number of seeds)
+		for (uint32_t i = 0; i < nReg; ++i) {
+			const uint32_t r = regs[i];
+			seeds[i] = ws.fuMaxPos[r];
+			ws.lab[ws.fuMaxPos[r]] = r + 1;
+		}
+		SortSlice(seeds, nReg);
+		FloodGroup(ws, seeds, nReg, ws.heapKey + ws.gOff[m], ws.heapPix + ws.gOff[m]);
+	}
+}
+
+// Exact integer sums per region (ComputeStatistics, Segmentation2D.cpp:144-175).
+__global__ void RegionStats(Workspace ws)
+{
+	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
+	const Geometry& geo = ws.g;
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		const uint32_t p = ws.dom[k];
+		const uint32_t L = ws.lab[p];
+		if (L == 0) { continue; }
+		const uint32_t r = L - 1;
+		const Pix q = Decompose(p, geo);
+		const unsigned long long v = static_cast<unsigned long long>(ws.w1[p]);
+		atomicAdd(ws.regCount + r, 1u);
+		atomicAdd(ws.regSumV + r, v);
+		atomicAdd(ws.regSumVJ + r, v * static_cast<unsigned long long>(q.x));
+		atomicAdd(ws.regSumVI + r, v * static_cast<unsigned long long>(q.y));
+	}
+}
+
+__global__ void CandidateFlags(Workspace ws)
+{
+	const uint32_t n = ws.cnt->nregion;
+	for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+		ws.regCand[r] = static_cast<double>(ws.regCount[r]) > kVolumeMin ? 1u : 0u;  // FilterData, :88-141
+	}
+}
+
+// Per frame: candidate base, kept count (capacity truncation in label order, Fitting.cpp:44-58) and output base.
+__global__ void FrameCandidates(Workspace ws, uint32_t maxPoints)
+{
+	const int B = ws.g.B;
+	for (int f = blockIdx.x * blockDim.x + threadIdx.x; f <= B; f += gridDim.x * blockDim.x) {
+		const uint32_t rb = ws.rowcnt[static_cast<long long>(f) * ws.g.H];
+		ws.frameRegBase[f] = rb;
+		ws.frameCandBase[f] = ws.regCand[rb];
+	}
+}
+
+__global__ void FrameKeep(Workspace ws, uint32_t maxPoints)
+{
+	const int B = ws.g.B;
+	for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < B; f += gridDim.x * blockDim.x) {
+		const uint32_t c = ws.frameCandBase[f + 1] - ws.frameCandBase[f];
+		ws.frameKeep[f] = min(c, maxPoints);
+		if (c > maxPoints) { atomicExch(&ws.cnt->truncated, 1u); }
+	}
+}
+
+__global__ void CandidateEmit(Workspace ws, uint32_t maxPoints)
+{
+	const uint32_t n = ws.cnt->nregion;
+	for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+		if (!(static_cast<double>(ws.regCount[r]) > kVolumeMin)) { continue; }
+		const int f = ws.regFrame[r];
+		const uint32_t k = ws.regCand[r] - ws.frameCandBase[f];
+		if (k >= maxPoints) { continue; }
+		const uint32_t slot = ws.frameOutBase[f] + k;
+		if (slot >= ws.capRows) { atomicExch(&ws.cnt->overflow, 1u); continue; }
+		ws.candRegion[slot] = r;
+		ws.candFrame[slot] = static_cast<uint32_t>(f);
+	}
+}
+
+}  // namespace
+
+// Runs the whole segmentation of a chunk after detection. `strict` selects frame-wide floods.
+bool LaunchSegment(const Workspace& ws, double ratio, int strict, uint32_t maxPoints, cudaStream_t st)
+{
+	const Geometry& g = ws.g;
+	bool ok = true;
+	CclInit<<<kGrid, kThreads, 0, st>>>(ws);
+	CclUnion<<<kGrid, kThreads, 0, st>>>(ws);
+	CclFlatten<<<kGrid, kThreads, 0, st>>>(ws);
+	CompEnumerate<<<kGrid, kThreads, 0, st>>>(ws);
+	CompCount<<<kGrid, kThreads, 0, st>>>(ws);
+	SeedParent<<<kGrid, kThreads, 0, st>>>(ws);
+	RowCount<<<kGrid, kThreads, 0, st>>>(ws);
+	CountLaunch(7);
+	ok = ok && PTB_LAUNCHED();
+	const uint32_t rows = static_cast<uint32_t>(g.B) * static_cast<uint32_t>(g.H);
+	ok = ok && ExclusiveScan(ws.rowcnt, nullptr, rows, rows, ws.scanBlock, &ws.cnt->nregion, st);
+	SeedLabel<<<kGrid, kThreads, 0, st>>>(ws);
+	LabelDomain<<<kGrid, kThreads, 0, st>>>(ws, strict);
+	CountLaunch(2);
+	ok = ok && PTB_LAUNCHED();
+	const uint32_t groupsStrict = strict ? static_cast<uint32_t>(g.B) : 0u;
+	if (strict) {
+		PTB_CUDA(cudaMemsetAsync(ws.gOff, 0, sizeof(uint32_t) * (g.B + 1), st));
+		PTB_CUDA(cudaMemsetAsync(ws.gSeedOff, 0, sizeof(uint32_t) * (g.B + 1), st));
+		PTB_CUDA(cudaMemsetAsync(ws.gRegOff, 0, sizeof(uint32_t) * (g.B + 1), st));
+		PTB_CUDA(cudaMemsetAsync(ws.gCurPix, 0, sizeof(uint32_t) * (g.B + 1), st));
+		PTB_CUDA(cudaMemsetAsync(ws.gCurSeed, 0, sizeof(uint32_t) * (g.B + 1), st));
+		PTB_CUDA(cudaMemsetAsync(ws.gCurReg, 0, sizeof(uint32_t) * (g.B + 1), st));
+		GroupSizesStrict<<<kGrid, kThreads, 0, st>>>(ws);
+		CountLaunch();
+		ok = ok && PTB_LAUNCHED();
+		ok = ok && ExclusiveScan(ws.gOff, nullptr, groupsStrict, groupsStrict, ws.scanBlock, nullptr, st);
+		ok = ok && ExclusiveScan(ws.gSeedOff, nullptr, groupsStrict, groupsStrict, ws.scanBlock, nullptr, st);
+		ok = ok && ExclusiveScan(ws.gRegOff, nullptr, groupsStrict, groupsStrict, ws.scanBlock, nullptr, st);
+	}
+	else {
+		GroupEnumerate<<<kGrid, kThreads, 0, st>>>(ws);
+		CountLaunch();
+		ok = ok && PTB_LAUNCHED();
+		ok = ok && ExclusiveScan(ws.gOff, &ws.cnt->nmulti, 0, ws.capComp, ws.scanBlock, nullptr, st);
+		ok = ok && ExclusiveScan(ws.gSeedOff, &ws.cnt->nmulti, 0, ws.capComp, ws.scanBlock, nullptr, st);
+		ok = ok && ExclusiveScan(ws.gRegOff, &ws.cnt->nmulti, 0, ws.capComp, ws.scanBlock, nullptr, st);
+	}
+	GroupScatter<<<kGrid, kThreads, 0, st>>>(ws, strict);
+	// one thread per group: small CTAs so that many SMs share the (uneven) groups
+	GroupFlood<<<kGrid * 2, 64, 0, st>>>(ws, groupsStrict);
+	CountLaunch(2);
+	ok = ok && PTB_LAUNCHED();
+	if (static_cast<int>(ratio) > 0) {  // WatershedIntelligent, Segmentation2D.cpp:77-85
+		GroupFuse<<<kGrid * 2, 64, 0, st>>>(ws, groupsStrict, ratio);
+		CountLaunch();
+		ok = ok && PTB_LAUNCHED();
+	}
+	RegionStats<<<kGrid, kThreads, 0, st>>>(ws);
+	CandidateFlags<<<kGrid, kThreads, 0, st>>>(ws);
+	CountLaunch(2);
+	ok = ok && PTB_LAUNCHED();
+	ok = ok && ExclusiveScan(ws.regCand, &ws.cnt->nregion, 0, ws.capRegion, ws.scanBlock, &ws.cnt->ncand, st);
+	FrameCandidates<<<(g.B + 256) / 256, 256, 0, st>>>(ws, maxPoints);
+	FrameKeep<<<(g.B + 255) / 256, 256, 0, st>>>(ws, maxPoints);
+	CountLaunch(2);
+	ok = ok && PTB_LAUNCHED();
+	PTB_CUDA(cudaMemcpyAsync(ws.frameOutBase, ws.frameKeep, sizeof(uint32_t) * g.B, cudaMemcpyDeviceToDevice, st));
+	ok = ok && ExclusiveScan(ws.frameOutBase, nullptr, static_cast<uint32_t>(g.B), static_cast<uint32_t>(g.B), ws.scanBlock,
+	                         &ws.cnt->nfit, st);
+	CandidateEmit<<<kGrid, kThreads, 0, st>>>(ws, maxPoints);
+	CountLaunch();
+	ok = ok && PTB_LAUNCHED();
+	return ok;
+}
+
+}  // namespace ptb

@@ -1,0 +1,160 @@
+"""ctypes binding of libpalmtracer_b200.so for Python callers (tests, benchmark, the reference front-end).
+
+The functions mirror the C ABI in include/palmtracer_b200.h one for one; numpy arrays are passed as host buffers.
+Loading fails loudly when the library has not been built: there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpalmtracer_b200.so")
+COLS = 18
+
+# every symbol the public header declares
+EXPORTS = ["Localization", "Fitting", "Wavelett", "AutoThreshold", "PTB_LocalizationDevice",
+           "PTB_SetSegmentationMode", "PTB_SetFitPrecision", "PTB_LastError", "PTB_KernelLaunchCount",
+           "PTB_SetProfiling", "PTB_StageTimes"]
+
+_u16p = ctypes.POINTER(ctypes.c_uint16)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_u64 = ctypes.c_uint64
+_f64 = ctypes.c_double
+
+_lib = None
+
+
+def load(path=LIB_PATH):
+    """Loads the library once (raises OSError when it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError("libpalmtracer_b200.so not built: run python palmtracer-cpp_b200/build.py (%s)" % path)
+    L = ctypes.CDLL(path)
+    L.Localization.restype = _u64
+    L.Localization.argtypes = [_u16p, _f64p, _u64, _u64, _u64, _u64, _f64, _f64, _u64, _f64p]
+    L.Fitting.restype = _u64
+    L.Fitting.argtypes = [_u16p, _f64p, _u64, _f64p, _u64, _u64, _u64, _u64, _u64, _f64p]
+    L.Wavelett.restype = None
+    L.Wavelett.argtypes = [_u16p, _f64p, _u64, _u64, _u64, _u64]
+    L.AutoThreshold.restype = _f64
+    L.AutoThreshold.argtypes = [_u16p, _u64, _u64, _f64p]
+    L.PTB_LocalizationDevice.restype = _u64
+    L.PTB_LocalizationDevice.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _u64, _u64, _u64, _u64, _f64, _f64, _u64, _f64p,
+                                         ctypes.c_void_p]
+    L.PTB_SetSegmentationMode.restype = ctypes.c_int
+    L.PTB_SetSegmentationMode.argtypes = [ctypes.c_int]
+    L.PTB_SetFitPrecision.restype = ctypes.c_int
+    L.PTB_SetFitPrecision.argtypes = [ctypes.c_int]
+    L.PTB_LastError.restype = ctypes.c_char_p
+    L.PTB_LastError.argtypes = []
+    L.PTB_KernelLaunchCount.restype = _u64
+    L.PTB_KernelLaunchCount.argtypes = []
+    L.PTB_SetProfiling.restype = ctypes.c_int
+    L.PTB_SetProfiling.argtypes = [ctypes.c_int]
+    L.PTB_StageTimes.restype = None
+    L.PTB_StageTimes.argtypes = [_f64p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
+    _lib = L
+    return L
+
+
+def _stack(stack):
+    stack = np.ascontiguousarray(stack, dtype=np.uint16)
+    if stack.ndim == 2:
+        stack = stack[None]
+    return stack
+
+
+def last_error():
+    return load().PTB_LastError().decode()
+
+
+def localization(stack, thr, ratio, fit, params, capacity_doubles=None):
+    """Localization over a host stack; returns the [n, 18] float64 rows."""
+    L = load()
+    stack = _stack(stack)
+    z, h, w = stack.shape
+    if capacity_doubles is None:
+        capacity_doubles = ((h * w) // 5 + 1) * z * COLS
+    out = np.full(max(capacity_doubles, 1), -12345.0)
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    n = L.Localization(stack.ctypes.data_as(_u16p), out.ctypes.data_as(_f64p), capacity_doubles, h, w, z, thr, ratio, fit,
+                       params.ctypes.data_as(_f64p))
+    return out[:n].reshape(-1, COLS).copy()
+
+
+def localization_raw(stack, out, thr, ratio, fit, params):
+    """Localization into a caller-given float64 buffer (its size is the capacity); returns doubles written."""
+    L = load()
+    z, h, w = stack.shape
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    return L.Localization(stack.ctypes.data_as(_u16p), out.ctypes.data_as(_f64p), out.size, h, w, z, thr, ratio, fit,
+                          params.ctypes.data_as(_f64p))
+
+
+def fitting(stack, positions, fit, params):
+    L = load()
+    stack = _stack(stack)
+    z, h, w = stack.shape
+    positions = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 6)
+    n = positions.shape[0]
+    out = np.zeros(max(n, 1) * COLS)
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    k = L.Fitting(stack.ctypes.data_as(_u16p), positions.ctypes.data_as(_f64p), n, out.ctypes.data_as(_f64p), out.size, h, w, z,
+                  fit, params.ctypes.data_as(_f64p))
+    return out[:k].reshape(-1, COLS).copy()
+
+
+def wavelett(stack, level):
+    L = load()
+    stack = _stack(stack)
+    z, h, w = stack.shape
+    out = np.zeros((z, h, w))
+    L.Wavelett(stack.ctypes.data_as(_u16p), out.ctypes.data_as(_f64p), h, w, z, level)
+    return out
+
+
+def auto_threshold(frame, params):
+    L = load()
+    frame = np.ascontiguousarray(frame, dtype=np.uint16)
+    h, w = frame.shape[-2:]
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    return L.AutoThreshold(frame.ctypes.data_as(_u16p), h, w, params.ctypes.data_as(_f64p))
+
+
+def localization_device(d_input_ptr, d_output_ptr, capacity_doubles, shape, thr, ratio, fit, params, stream_ptr=0):
+    """Device-buffer variant: pointers are CUDA device addresses (e.g. torch tensor.data_ptr())."""
+    L = load()
+    z, h, w = shape
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    return L.PTB_LocalizationDevice(ctypes.c_void_p(d_input_ptr), ctypes.c_void_p(d_output_ptr), capacity_doubles, h, w, z,
+                                    thr, ratio, fit, params.ctypes.data_as(_f64p), ctypes.c_void_p(stream_ptr))
+
+
+def set_segmentation_mode(mode):
+    return load().PTB_SetSegmentationMode(int(mode))
+
+
+def set_fit_precision(mode):
+    return load().PTB_SetFitPrecision(int(mode))
+
+
+def launch_count():
+    return load().PTB_KernelLaunchCount()
+
+
+STAGES = ["detect", "segment", "fit", "finish", "copies"]
+
+
+def set_profiling(enable):
+    return load().PTB_SetProfiling(int(enable))
+
+
+def stage_times():
+    """{stage: (ms, launches)} accumulated since the last call (profiling must be on)."""
+    ms = np.zeros(5)
+    launches = np.zeros(5, dtype=np.uint64)
+    load().PTB_StageTimes(ms.ctypes.data_as(_f64p), launches.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 5)
+    return {k: (float(ms[i]), int(launches[i])) for i, k in enumerate(STAGES)}

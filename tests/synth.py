@@ -117,3 +117,48 @@ def mad_threshold(w1_plane):
     """Detection threshold k = 3 x 1.4826 x MAD of wavelet plane 1 (the reference's PLANE_ID plane)."""
     med = np.median(w1_plane)
     return float(3.0 * 1.4826 * np.median(np.abs(w1_plane - med)))
+
+
+def stack_cuda(workload, frames=None, seed=1234, size=None, device="cuda", chunk=64):
+    """Same statistics as ``stack`` rendered with torch on the GPU (for the multi-GB benchmark stacks).
+
+    Emitter tables come from the same numpy generator; pixel noise uses torch's CUDA Poisson sampler, so the pixels
+    differ from ``stack`` for the same seed. Returns (int16 tensor [Z, H, W] holding the uint16 bit patterns, emitters).
+    """
+    import torch
+    z, h, w = SHAPES[workload]
+    if frames is not None:
+        z = frames
+    if size is not None:
+        h, w = size
+    em = emitters(workload, z, h, w, seed)
+    bg = torch.as_tensor(background(workload, h, w), dtype=torch.float32, device=device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed + 1)
+    out = torch.empty((z, h, w), dtype=torch.int16, device=device)
+    patch = 8
+    offs = torch.arange(-patch, patch + 1, device=device, dtype=torch.float64)
+    fidx = em[:, 0].astype(np.int64)
+    bounds = np.searchsorted(fidx, np.arange(0, z + chunk, chunk))
+    s2 = math.sqrt(2.0)
+    for c0 in range(0, z, chunk):
+        c1 = min(z, c0 + chunk)
+        e = torch.as_tensor(em[bounds[c0 // chunk]:bounds[c0 // chunk + 1]], device=device)
+        mu = bg.unsqueeze(0).repeat(c1 - c0, 1, 1).reshape(-1)
+        if e.shape[0]:
+            f = e[:, 0].long() - c0
+            x, y, ph, sx, sy = e[:, 1], e[:, 2], e[:, 3], e[:, 4], e[:, 5]
+            xs = x.floor().unsqueeze(1) + offs  # pixel columns
+            ys = y.floor().unsqueeze(1) + offs
+            gx = 0.5 * (torch.erf((xs + 0.5 - x[:, None]) / (s2 * sx[:, None])) - torch.erf((xs - 0.5 - x[:, None]) / (s2 * sx[:, None])))
+            gy = 0.5 * (torch.erf((ys + 0.5 - y[:, None]) / (s2 * sy[:, None])) - torch.erf((ys - 0.5 - y[:, None]) / (s2 * sy[:, None])))
+            val = (ph[:, None, None] * gy[:, :, None] * gx[:, None, :]).float()
+            xi = xs.long()[:, None, :].expand(-1, 2 * patch + 1, -1)
+            yi = ys.long()[:, :, None].expand(-1, -1, 2 * patch + 1)
+            ok = (xi >= 0) & (xi < w) & (yi >= 0) & (yi < h)
+            flat = (f[:, None, None] * (h * w) + yi * w + xi)[ok]
+            mu.index_add_(0, flat, val[ok])
+        counts = torch.poisson(mu.reshape(c1 - c0, h, w), generator=gen)
+        adu = torch.clamp(OFFSET + GAIN * counts, 0, 65535).to(torch.int32)
+        out[c0:c1] = adu.to(torch.int16)
+    return out, em

@@ -1,0 +1,205 @@
+"""GPU path against the oracle and the reference's golden vectors, through the C ABI.
+
+Detection (wavelet planes, candidates: x_, y_, intensity_, surf_) must be bit-exact; fitted values must lie within
+1e-3 px (x, y) and 1e-4 relative (amplitude / photons) of the FP64 oracle; golden CSVs use the reference test's own
+rule (1e-3 absolute + 1e-5 relative, nearest-row matching).
+"""
+import numpy as np
+import pytest
+
+from compare import match_rows, theta_to_degrees, C_X, C_Y, C_AMP, C_OFF, C_SX, C_SY
+from conftest import GAUSS_PARAMS
+
+pytestmark = pytest.mark.gpu
+
+XY_TOL = 1e-3
+REL_TOL = 1e-4
+
+
+def _synth(workload, frames, seed, orc, size=None):
+    import synth
+    s, _ = synth.stack(workload, frames=frames, seed=seed, size=size)
+    thr = synth.mad_threshold(orc.planes(s[0])[1])
+    return s, thr
+
+
+# ---- wavelet ------------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("level", [0, 1, 2, 3, 7])
+def test_wavelett_bitwise(lib, orc, stacks, level):
+    for stack in (stacks["stack"], stacks["stack_quadrant"][:3]):
+        assert np.array_equal(lib.wavelett(stack, level), orc.wavelett(stack, level))
+
+
+@pytest.mark.parametrize("shape", [(1, 1), (1, 9), (9, 1), (7, 13), (3, 200), (130, 67)])
+def test_wavelett_shapes_bitwise(lib, orc, shape):
+    h, w = shape
+    img = ((np.arange(h * w) * 37 + 11) % 4096).astype(np.uint16).reshape(1, h, w)
+    for level in (1, 2, 3):
+        assert np.array_equal(lib.wavelett(img, level), orc.wavelett(img, level))
+
+
+@pytest.mark.parametrize("value", [0, 1, 1024, 65535])
+def test_wavelett_constant(lib, value):
+    img = np.full((2, 7, 11), value, dtype=np.uint16)
+    assert np.all(lib.wavelett(img, 1) == 0) and np.all(lib.wavelett(img, 2) == 0) and np.all(lib.wavelett(img, 3) == value)
+
+
+def test_wavelett_extreme_values(lib, orc):
+    rng = np.random.default_rng(3)
+    img = rng.choice(np.array([0, 65535], dtype=np.uint16), size=(2, 64, 96))
+    for level in (1, 2, 3):
+        assert np.array_equal(lib.wavelett(img, level), orc.wavelett(img, level))
+
+
+# ---- detection (fit 0 rows are pure segmentation output, so they must be identical) -------------------------
+@pytest.mark.parametrize("ratio", [0.0, 10.0, 0.5])
+def test_detection_golden_stack_bitwise(lib, orc, stacks, ratio):
+    for stack in (stacks["stack"], stacks["stack_quadrant"]):
+        a = lib.localization(stack, 103.6, ratio, 0, GAUSS_PARAMS)
+        b = orc.localization(stack, 103.6, ratio, 0, GAUSS_PARAMS)
+        assert a.shape == b.shape and np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("workload,frames,size", [("c1", 12, None), ("c2", 3, None), ("c3", 4, None), ("c4", 4, None),
+                                                  ("c2", 6, (200, 333))])
+@pytest.mark.parametrize("ratio", [0.0, 10.0])
+def test_detection_synthetic_bitwise(lib, orc, workload, frames, size, ratio):
+    s, thr = _synth(workload, frames, 11, orc, size)
+    a = lib.localization(s, thr, ratio, 0, GAUSS_PARAMS)
+    b = orc.localization(s, thr, ratio, 0, GAUSS_PARAMS)
+    assert a.shape == b.shape and np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("scale", [0.3, 0.1, 0.0])
+def test_detection_strict_mode_low_threshold_bitwise(lib, orc, scale):
+    """Giant components: the frame-wide flood (strict mode) reproduces the reference exactly."""
+    s, thr = _synth("c2", 2, 21, orc, (256, 256))
+    prev = lib.set_segmentation_mode(1)
+    try:
+        for ratio in (0.0, 10.0):
+            a = lib.localization(s, thr * scale, ratio, 0, GAUSS_PARAMS)
+            b = orc.localization(s, thr * scale, ratio, 0, GAUSS_PARAMS)
+            assert a.shape == b.shape and np.array_equal(a, b)
+    finally:
+        lib.set_segmentation_mode(prev)
+
+
+def test_detection_edge_cases(lib, orc):
+    # black stack, empty output capacity, single plane, plateaus, tiny frames
+    assert lib.localization(np.zeros((3, 12, 16), np.uint16), 0.0, 0.0, 0, GAUSS_PARAMS).shape[0] == 0
+    s = np.zeros((2, 9, 13), np.uint16)
+    s[:, 3:6, 4:9] = 500
+    for thr in (-1.0, 0.0, 10.0):
+        a = lib.localization(s, thr, 0.0, 0, GAUSS_PARAMS)
+        b = orc.localization(s, thr, 0.0, 0, GAUSS_PARAMS)
+        assert np.array_equal(a, b)
+    for h, w in [(1, 1), (1, 30), (30, 1), (2, 2)]:
+        img = ((np.arange(h * w) * 7919) % 3000 + 100).astype(np.uint16).reshape(1, h, w)
+        assert np.array_equal(lib.localization(img, 1.0, 0.0, 0, GAUSS_PARAMS), orc.localization(img, 1.0, 0.0, 0, GAUSS_PARAMS))
+
+
+def test_bounded_output(lib, stacks):
+    # Tests_CPU/test_Palm.cpp:105-121: capacity of one row per plane
+    st = stacks["stack"]
+    cap = st.shape[0] * 18
+    out = np.full(cap + 2, -12345.0)
+    n = lib.localization_raw(st, out[1:-1], 103.6, 0.0, 0, GAUSS_PARAMS)
+    assert n == cap and out[0] == -12345 and out[-1] == -12345
+    rows = out[1:-1].reshape(-1, 18)
+    assert np.all(rows[:, 0] == np.arange(1, 11)) and np.all(rows[:, 1] == np.arange(1, 11)) and np.all(rows[:, 2] == 1)
+
+
+@pytest.mark.parametrize("leading_empty", [True, False])
+def test_per_plane_capacity(lib, orc, stacks, leading_empty):
+    # Tests_CPU/test_Palm.cpp:124-154
+    st = stacks["stack"]
+    z = 3 if leading_empty else 2
+    first = 1 if leading_empty else 0
+    pix = np.zeros((z,) + st.shape[1:], np.uint16)
+    pix[first:] = st[0]
+    per_plane = 2
+    cap = z * per_plane * 18 + 1
+    out = np.full(cap + 2, -12345.0)
+    n = lib.localization_raw(pix, out[1:-1], 103.6, 0.0, 0, GAUSS_PARAMS)
+    rows_n = (z - first) * per_plane
+    assert n == rows_n * 18
+    assert out[0] == -12345 and out[1 + rows_n * 18] == -12345 and out[-1] == -12345
+    ref_out = np.full(cap, -12345.0)
+    from oracle.oracle import OracleLib  # noqa: F401  (same call on the oracle)
+    m = orc._loc(pix.ctypes.data_as(orc._loc.argtypes[0]), ref_out.ctypes.data_as(orc._loc.argtypes[1]), cap, pix.shape[1],
+                 pix.shape[2], z, 103.6, 0.0, 0, GAUSS_PARAMS.ctypes.data_as(orc._loc.argtypes[9]))
+    assert m == n and np.array_equal(out[1:1 + n], ref_out[:n])
+
+
+# ---- fits ---------------------------------------------------------------------------------------------------
+def _fit_errors(a, b):
+    """Max |dx|, |dy| and max relative error of amplitude / offset between matched rows."""
+    bad, worst, pairs = match_rows(a, b, atol=1e9, rtol=0)
+    assert bad == 0
+    ok = pairs >= 0
+    e = b[pairs[ok]]
+    a = a[ok]
+    fitted = (a[:, C_SX] > 0) & (e[:, C_SX] > 0)
+    dxy = max(np.max(np.abs(a[:, C_X] - e[:, C_X]), initial=0), np.max(np.abs(a[:, C_Y] - e[:, C_Y]), initial=0))
+    rel = np.max(np.abs(a[fitted, C_AMP] - e[fitted, C_AMP]) / np.maximum(np.abs(e[fitted, C_AMP]), 1e-12), initial=0)
+    sentinel_mismatch = int(np.sum((a[:, C_SX] > 0) != (e[:, C_SX] > 0)))
+    return dxy, rel, sentinel_mismatch
+
+
+@pytest.mark.parametrize("watershed", [True, False])
+@pytest.mark.parametrize("fit", [1, 2, 3, 4])
+def test_fit_golden_csv(lib, stacks, goldens, fit, watershed):
+    rows = lib.localization(stacks["stack"], 103.6, 0.0 if watershed else 10.0, fit, GAUSS_PARAMS)
+    key = "stack-localizations-103.6_%s_%d_1.0_0.0_7" % (watershed, fit)
+    bad, worst, _ = match_rows(theta_to_degrees(rows, fit), goldens[key], atol=1e-3, rtol=1e-5)
+    assert bad == 0, (key, worst)
+
+
+def test_fit_golden_quadrants(lib, stacks, goldens):
+    rows = lib.localization(stacks["stack_quadrant"], 103.6, 0.0, 4, GAUSS_PARAMS)
+    bad, worst, _ = match_rows(theta_to_degrees(rows, 4), goldens["stack_quadrant-localizations-103.6_True_4_1.0_0.0_7"])
+    assert bad == 0, worst
+
+
+@pytest.mark.parametrize("fit", [1, 2, 3, 4])
+@pytest.mark.parametrize("workload,frames", [("c1", 10), ("c2", 2), ("c3", 3)])
+def test_fit_synthetic_vs_oracle(lib, orc, fit, workload, frames):
+    s, thr = _synth(workload, frames, 17, orc)
+    a = lib.localization(s, thr, 0.0, fit, GAUSS_PARAMS)
+    b = orc.localization(s, thr, 0.0, fit, GAUSS_PARAMS)
+    assert a.shape == b.shape
+    dxy, rel, sent = _fit_errors(a, b)
+    assert sent == 0 and dxy <= XY_TOL and rel <= REL_TOL, (dxy, rel, sent)
+
+
+def test_fitting_export_matches_localization(lib, orc, stacks):
+    # Tests_CPU/test_Palm.cpp:269-295
+    st = stacks["stack"]
+    det = lib.localization(st, 103.6, 0.0, 0, GAUSS_PARAMS)
+    pos = np.stack([2 * det[:, 0], det[:, 1], det[:, 4], det[:, 5], det[:, 15], det[:, 16]], axis=1)
+    for fit in (1, 2, 3, 4):
+        a = lib.fitting(st, pos, fit, GAUSS_PARAMS)
+        b = orc.fitting(st, pos, fit, GAUSS_PARAMS)
+        assert a.shape == b.shape and np.array_equal(a[:, 0], pos[:, 0]) and np.array_equal(a[:, 2], b[:, 2])
+        dxy, rel, sent = _fit_errors(a, b)
+        assert sent == 0 and dxy <= XY_TOL and rel <= REL_TOL
+
+
+@pytest.mark.parametrize("plane", range(10))
+def test_auto_threshold(lib, stacks, plane):
+    t = lib.auto_threshold(stacks["stack"][plane], np.array([7.0]))
+    assert abs(t - stacks["auto_threshold"][plane]) < 1e-5
+
+
+def test_device_api_matches_host(lib, orc, stacks):
+    import torch
+    st = stacks["stack"]
+    host = lib.localization(st, 103.6, 0.0, 2, GAUSS_PARAMS)
+    d_in = torch.from_numpy(st.astype(np.int16).view(np.int16)).cuda()
+    cap = ((st.shape[1] * st.shape[2]) // 5 + 1) * st.shape[0] * 18
+    d_out = torch.zeros(cap, dtype=torch.float64, device="cuda")
+    n = lib.localization_device(d_in.data_ptr(), d_out.data_ptr(), cap, st.shape, 103.6, 0.0, 2, GAUSS_PARAMS,
+                                torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    dev = d_out[:n].cpu().numpy().reshape(-1, 18)
+    assert np.array_equal(dev, host)

@@ -1,0 +1,117 @@
+"""The oracle pinned against the reference's own golden vectors and, when built, against the reference itself."""
+import numpy as np
+import pytest
+
+from compare import match_rows, theta_to_degrees
+from conftest import GAUSS_PARAMS
+
+
+@pytest.mark.parametrize("watershed", [True, False])
+@pytest.mark.parametrize("fit", [0, 1, 2, 3, 4])
+def test_oracle_matches_golden_csv(orc, stacks, goldens, fit, watershed):
+    # Tests_CPU/test_Palm.cpp:236-249: stack.tif, thr 103.6, roi 7, sigma 1/2, ratio 0 (watershed) or 10
+    rows = orc.localization(stacks["stack"], 103.6, 0.0 if watershed else 10.0, fit, GAUSS_PARAMS)
+    key = "stack-localizations-103.6_%s_%d_1.0_0.0_7" % (watershed, fit)
+    bad, worst, _ = match_rows(theta_to_degrees(rows, fit), goldens[key], atol=1e-3, rtol=1e-5)
+    assert bad == 0, (key, worst)
+
+
+def test_oracle_quadrants(orc, stacks, goldens):
+    # Tests_CPU/test_Palm.cpp:252-264
+    rows = orc.localization(stacks["stack_quadrant"], 103.6, 0.0, 4, GAUSS_PARAMS)
+    bad, worst, _ = match_rows(theta_to_degrees(rows, 4), goldens["stack_quadrant-localizations-103.6_True_4_1.0_0.0_7"])
+    assert bad == 0, worst
+
+
+@pytest.mark.parametrize("fit", [0, 1, 2, 3, 4])
+def test_oracle_first_plane_golden(orc, stacks, goldens, fit):
+    rows = orc.localization(stacks["stack"][:1], 103.6, 0.0, fit, GAUSS_PARAMS)
+    bad, worst, _ = match_rows(theta_to_degrees(rows, fit), goldens["stack-localizations-0_103.6_True_%d_1.0_0.0_7" % fit])
+    assert bad == 0, worst
+
+
+def test_oracle_plane_selection_golden(orc, stacks, goldens):
+    rows = orc.localization(stacks["stack"][2:7], 103.6, 0.0, 4, GAUSS_PARAMS)
+    rows[:, 1] += 2
+    bad, worst, _ = match_rows(theta_to_degrees(rows, 4), goldens["stack-localizations-plane_select-103.6_True_4_1.0_0.0_7"])
+    assert bad == 0, worst
+
+
+@pytest.mark.parametrize("plane", range(10))
+def test_oracle_auto_threshold(orc, stacks, plane):
+    # Tests_CPU/test_Palm.cpp:305-321 (tolerance 1e-5)
+    t = orc.auto_threshold(stacks["stack"][plane], np.array([7.0]))
+    assert abs(t - stacks["auto_threshold"][plane]) < 1e-5
+
+
+def test_oracle_atrous_identities(orc):
+    # Tests_CPU/test_loc_ATrous.cpp: planes sum to the input; constant images have zero details
+    for h, w in [(1, 1), (1, 9), (9, 1), (7, 13)]:
+        img = ((np.arange(h * w) * 37 + 11) % 4096).astype(np.uint16).reshape(h, w)
+        pl = orc.planes(img)
+        assert np.allclose(pl.sum(axis=0), img, atol=1e-10)
+    for v in (0, 1, 1024, 65535):
+        pl = orc.planes(np.full((7, 11), v, dtype=np.uint16))
+        assert np.all(pl[0] == 0) and np.all(pl[1] == 0) and np.all(pl[2] == v)
+
+
+def test_oracle_segmentation_cases(orc):
+    # Tests_CPU/test_loc_Segmentation2D.cpp:173-287 (strict threshold, surface > 4, connected peaks, absorbed peak)
+    pot = np.zeros((5, 7))
+    pot[1:4, 2:5] = 10
+    assert len(orc.candidates_from_potential(pot, 9.0, 0)) == 1
+    assert len(orc.candidates_from_potential(pot, 10.0, 0)) == 0
+    for length, expect in [(3, 0), (4, 0), (5, 1)]:
+        pot = np.zeros((5, 9))
+        pot[2, 1:1 + length] = 10
+        assert len(orc.candidates_from_potential(pot, 0, 0)) == expect
+    for merge in (True, False):
+        for first_higher in (True, False):
+            pot = np.zeros((7, 13))
+            pot[2:5, 2:5] = 100 if first_higher else 60
+            pot[2:5, 8:11] = 60 if first_higher else 100
+            pot[3, 5] = 40 if first_higher else 30
+            pot[3, 6] = 20
+            pot[3, 7] = 30 if first_higher else 40
+            c = orc.candidates_from_potential(pot, 0, 10 if merge else 0)
+            assert len(c) == (1 if merge else 2)
+            assert c[:, 3].sum() == 21 and c[:, 2].sum() == pot.sum()
+    pot = np.zeros((7, 18))
+    pot[2:5, 1:4] = 200
+    pot[2:5, 7:10] = 100
+    pot[2:5, 13:16] = 60
+    pot[3, 10], pot[3, 11], pot[3, 12] = 40, 20, 30
+    c = orc.candidates_from_potential(pot, 0, 10)
+    assert len(c) == 2 and c[0, 3] == 9 and c[0, 2] == 1800 and c[1, 3] == 21 and c[1, 2] == 1530
+
+
+def test_oracle_many_regions(orc):
+    # Tests_CPU/test_loc_Segmentation2D.cpp: labels beyond 16 bits
+    pot = np.zeros((1025, 1025))
+    for y in range(1, 1024, 4):
+        for x in range(1, 1024, 4):
+            pot[y:y + 3, x:x + 3] = 100
+    c = orc.candidates_from_potential(pot, 0, 0)
+    assert len(c) == 65536 and np.all(c[:, 3] == 9) and np.all(c[:, 2] == 900)
+
+
+def test_oracle_equals_reference_build(orc, ref, stacks):
+    """Bit-for-bit against the reference compiled from its own sources (skipped where oracle/_ref is absent)."""
+    if ref is None:
+        pytest.skip("oracle/_ref not built (reference sources absent)")
+    import synth
+    s, _ = synth.stack("c1", frames=6, seed=5)
+    thr = synth.mad_threshold(orc.planes(s[0])[1])
+    for stack, t in ((stacks["stack"], 103.6), (s, thr)):
+        for ratio in (0.0, 10.0):
+            for fit in range(5):
+                a = orc.localization(stack, t, ratio, fit, GAUSS_PARAMS)
+                b = ref.localization(stack, t, ratio, fit, GAUSS_PARAMS)
+                assert a.shape == b.shape and np.array_equal(a, b), (fit, ratio)
+        assert np.array_equal(orc.wavelett(stack, 2), ref.wavelett(stack, 2))
+        for k in range(stack.shape[0]):
+            assert np.array_equal(orc.candidates(stack[k], t, 10.0), ref.candidates(stack[k], t, 10.0))
+    rows = ref.localization(stacks["stack"], 103.6, 0.0, 0, GAUSS_PARAMS)
+    pos = np.stack([rows[:, 0], rows[:, 1], rows[:, 4], rows[:, 5], rows[:, 15], rows[:, 16]], axis=1)
+    for fit in (1, 2, 3, 4):
+        assert np.array_equal(orc.fitting(stacks["stack"], pos, fit, GAUSS_PARAMS), ref.fitting(stacks["stack"], pos, fit, GAUSS_PARAMS))
