@@ -124,6 +124,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", type=int, default=0, help="fit arithmetic (PTB_SetFitPrecision)")
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     import torch
     import torch.distributed as dist
@@ -138,6 +140,7 @@ def main():
     import synth
     import ptb
 
+    ptb.set_fit_precision(args.precision)
     frames = args.frames or synth.SHAPES[WORKLOAD][0]
     h, w = synth.SHAPES[WORKLOAD][1:]
     config = {"workload": "c2: %d frames of %dx%d uint16, ~2684 emitters/frame, 7x7 ROI, fit mode %d, per-plane capacity %d"
@@ -240,14 +243,15 @@ def main():
     host_np = host_in.numpy().view(np.uint16)
     host_out = torch.empty(cap, dtype=torch.float64, pin_memory=True).numpy()
     e2e_ms = []
-    for i in range(max(1, args.warmup // 2) + max(2, args.steps // 2)):
+    n_e2e = 0
+    for i in range(0 if args.no_e2e else max(1, args.warmup // 2) + max(2, args.steps // 2)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         n_e2e = ptb.localization_raw(host_np, host_out, thr, RATIO, FIT_MODE, FIT_PARAMS)
         torch.cuda.synchronize()
         if i >= max(1, args.warmup // 2):
             e2e_ms.append((time.perf_counter() - t0) * 1000.0)
-    e2e_value = (n_e2e // 18) * len(e2e_ms) / (sum(e2e_ms) / 1000.0)
+    e2e_value = (n_e2e // 18) * len(e2e_ms) / (sum(e2e_ms) / 1000.0) if e2e_ms else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -258,12 +262,13 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64", "data": "synthetic (seeded, generated on the GPU; no public dataset)", "config": config,
+                "dtype": "f64" if args.precision != 1 else "f32 (f64 re-fit)", "data": "synthetic (seeded, generated on the GPU; no public dataset)",
+                "config": dict(config, fit_precision=args.precision),
                 "frames_per_s": frames * world * args.steps / (total_ms / 1000.0),
                 "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
                 "localizations_per_step": int(rows_all), "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host_np.nbytes),
-                        "d2h_bytes_per_step": int(n_e2e * 8), "ms_per_step": float(np.mean(e2e_ms))},
+                        "d2h_bytes_per_step": int(n_e2e * 8), "ms_per_step": float(np.mean(e2e_ms)) if e2e_ms else None},
                 "gpu_launches": int(launches), "clocks": clk}
         print(json.dumps(line), flush=True)
     if world > 1:

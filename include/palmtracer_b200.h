@@ -72,8 +72,9 @@ PTB_API uint64_t PTB_LocalizationDevice(const uint16_t* d_input, double* d_outpu
  * Returns the previous mode. */
 PTB_API int PTB_SetSegmentationMode(int mode);
 
-/* Fit arithmetic for the Gaussian least-squares modes 1-4. 0 (default): FP64 iterations (same decisions as the
- * reference); 1: FP32 iterations with an FP64 re-fit of any ROI whose FP32 run did not converge cleanly.
+/* Fit arithmetic for the Gaussian least-squares modes 1-4. 0 (default): FP64, one thread per ROI, in the
+ * reference's exact order of operations (same iteration path as the reference); 1: FP32 iterations, one warp per
+ * ROI, with an FP64 re-fit of every ROI whose FP32 run did not stop cleanly; 2: FP64, one warp per ROI.
  * Returns the previous setting. */
 PTB_API int PTB_SetFitPrecision(int mode);
 

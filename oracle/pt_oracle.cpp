@@ -910,7 +910,7 @@ void FitSplineFull(const SplineTable& t, double roiParam, const uint16_t* img, i
 		if (std::abs(fm[a * np + a]) < std::numeric_limits<double>::epsilon()) { fm[a * np + a] = 1e-10; }
 	}
 	InverseLU(fm, fmi, np);
-	for (int a = 0; a < np; ++a) { const double v = fmi[a * np + a]; crlb[a] = v >= 0 ? std::sqrt(v) : 0.0; }
+	for (int a = 0; a < np; ++a) { const double v = fmi[a * np + a]; crlb[a] = std::isnan(v) ? v : (v >= 0 ? std::sqrt(v) : 0.0); }
 	const double off = crlb[0], amp = crlb[1], qxy = (crlb[2] + crlb[3]) / 2, qz = t.deltaZ * crlb[4];
 	const double xo = p[2] - static_cast<double>(hh) + c.x;
 	const double yo = p[3] - static_cast<double>(hh) + c.y;

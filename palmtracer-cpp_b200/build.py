@@ -28,7 +28,8 @@ def compile_one(src):
     deps.append(os.path.join(HERE, "..", "include", "palmtracer_b200.h"))
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj, ""
-    cmd = [NVCC] + FLAGS + ["-c", src, "-o", obj]
+    extra = ["-fmad=false"] if src.endswith("_exact.cu") else []
+    cmd = [NVCC] + FLAGS + extra + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("nvcc failed on %s:\n%s%s" % (src, r.stdout, r.stderr))

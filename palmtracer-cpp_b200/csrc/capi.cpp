@@ -131,7 +131,7 @@ PTB_API int PTB_SetSegmentationMode(int mode)
 PTB_API int PTB_SetFitPrecision(int mode)
 {
 	std::unique_lock<std::mutex> lock;
-	return ptb::EngineFor(lock).SetPrecision(mode ? 1 : 0);
+	return ptb::EngineFor(lock).SetPrecision(mode < 0 ? 0 : (mode > 2 ? 2 : mode));
 }
 
 PTB_API const char* PTB_LastError(void) { return ptb::LastError().c_str(); }

@@ -361,13 +361,20 @@ void Engine::StageTimes(double* ms, uint64_t* launches, int n)
 bool Engine::UploadSpline(FitParams& fp, const std::vector<double>& spline)
 {
 	if (fp.mode != kSplineEmccd) { return true; }
-	const size_t bytes = spline.size() * sizeof(double);
+	// cell-major copy of the reference's [64][cell] table: one pixel's 64 coefficients become contiguous
+	const size_t cells = static_cast<size_t>(fp.splineSize);
+	std::vector<double> aos(cells * 64);
+	for (size_t i = 0; i < 64; ++i) {
+		for (size_t c = 0; c < cells; ++c) { aos[c * 64 + i] = spline[i * cells + c]; }
+	}
+	const size_t bytes = aos.size() * sizeof(double);
 	if (bytes > splineBytes_) {
 		if (spline_) { cudaFree(spline_); spline_ = nullptr; splineBytes_ = 0; }
 		if (!PTB_CUDA(cudaMalloc(&spline_, bytes))) { return false; }
 		splineBytes_ = bytes;
 	}
-	if (!PTB_CUDA(cudaMemcpyAsync(spline_, spline.data(), bytes, cudaMemcpyHostToDevice, stream_))) { return false; }
+	if (!PTB_CUDA(cudaMemcpyAsync(spline_, aos.data(), bytes, cudaMemcpyHostToDevice, stream_))) { return false; }
+	if (!PTB_CUDA(cudaStreamSynchronize(stream_))) { return false; }
 	fp.coeffs = static_cast<const double*>(spline_);
 	return true;
 }

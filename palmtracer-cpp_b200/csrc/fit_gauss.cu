@@ -550,11 +550,18 @@ bool LaunchGaussT(const uint16_t* img, int H, int W, long long N, const Cand* ca
 
 }  // namespace
 
+bool LaunchSpline(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
+                  uint32_t cap, const FitParams& fp, double* rows, cudaStream_t st);
+bool LaunchExactFit(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
+                    uint32_t cap, const FitParams& fp, double* rows, const uint8_t* only, cudaStream_t st);
+
 // Fits `n` candidates (device count *nptr, or nconst when nptr is null; `cap` bounds it) into rows[k * 18].
-// precision 0: FP64; 1: FP32 first, then FP64 for the candidates the FP32 pass flags.
+// precision 0: FP64 in the reference's order (thread per ROI); 1: FP32 warp-per-ROI first, then the FP64 exact
+// kernel for the candidates the FP32 pass flags; 2: FP64 warp-per-ROI.
 bool LaunchFit(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
                uint32_t cap, const FitParams& fp, double* rows, uint8_t* flags, int precision, cudaStream_t st)
 {
+	if (fp.mode == kSplineEmccd) { return LaunchSpline(img, H, W, N, cands, nptr, nconst, cap, fp, rows, st); }
 	if (fp.mode < kG2Fixed || fp.mode > kG3Theta) {
 		const uint32_t blocks = std::min<uint32_t>((cap + 255) / 256 + 1, 148u * 8u);
 		NoFitKernel<<<blocks, 256, 0, st>>>(cands, nptr, nconst, rows);
@@ -563,9 +570,10 @@ bool LaunchFit(const uint16_t* img, int H, int W, long long N, const Cand* cands
 	}
 	if (precision == 1 && flags) {
 		bool ok = LaunchGaussT<float>(img, H, W, N, cands, nptr, nconst, cap, fp, rows, flags, nullptr, st);
-		return ok && LaunchGaussT<double>(img, H, W, N, cands, nptr, nconst, cap, fp, rows, nullptr, flags, st);
+		return ok && LaunchExactFit(img, H, W, N, cands, nptr, nconst, cap, fp, rows, flags, st);
 	}
-	return LaunchGaussT<double>(img, H, W, N, cands, nptr, nconst, cap, fp, rows, nullptr, nullptr, st);
+	if (precision == 2) { return LaunchGaussT<double>(img, H, W, N, cands, nptr, nconst, cap, fp, rows, nullptr, nullptr, st); }
+	return LaunchExactFit(img, H, W, N, cands, nptr, nconst, cap, fp, rows, nullptr, st);
 }
 
 }  // namespace ptb

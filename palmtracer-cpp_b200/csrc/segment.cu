@@ -443,7 +443,9 @@ __global__ void GroupFuse(Workspace ws, uint32_t nGroupsStrict, double ratio)
 		const uint32_t nPix = ws.gOff[m + 1] - ws.gOff[m];
 		if (nReg == 0) { continue; }
 		SortSlice(regs, nReg);  // label order
-		for (uint32_t iter = 0; iter <= nReg; ++iter) {
+		// every pass that changes something removes at least one basin, so nReg + 1 passes always reach a stable state
+		const uint32_t passes = nReg + 1;
+		for (uint32_t iter = 0; iter < passes; ++iter) {
 			for (uint32_t i = 0; i < nReg; ++i) {
 				const uint32_t r = regs[i];
 				ws.fuMaxWN[r] = -1e10;

@@ -203,3 +203,28 @@ def test_device_api_matches_host(lib, orc, stacks):
     torch.cuda.synchronize()
     dev = d_out[:n].cpu().numpy().reshape(-1, 18)
     assert np.array_equal(dev, host)
+
+
+# ---- cubic spline PSF (mode 5) ------------------------------------------------------------------------------
+@pytest.mark.parametrize("roi", [7, 8, 13])
+def test_spline_mode5_vs_oracle(lib, orc, stacks, roi):
+    import spline_table
+    params = spline_table.fit_params(roi=roi, sx=15, sy=15, sz=31, dz_nm=30.0)
+    st = stacks["stack"][:4]
+    a = lib.localization(st, 103.6, 0.0, 5, params)
+    b = orc.localization(st, 103.6, 0.0, 5, params)
+    assert a.shape == b.shape and a.shape[0] > 0
+    bad, worst, pairs = match_rows(a, b, atol=1e-6, rtol=1e-6)
+    assert bad == 0, worst
+
+
+def test_spline_mode5_fitting_export(lib, orc, stacks):
+    import spline_table
+    params = spline_table.fit_params(roi=7, sx=11, sy=11, sz=21, dz_nm=40.0, distortion=0.3, seed=4)
+    st = stacks["stack"][:3]
+    det = orc.localization(st, 103.6, 10.0, 0, GAUSS_PARAMS)
+    pos = np.stack([det[:, 0], det[:, 1], det[:, 4], det[:, 5], det[:, 15], det[:, 16]], axis=1)
+    a = lib.fitting(st, pos, 5, params)
+    b = orc.fitting(st, pos, 5, params)
+    assert a.shape == b.shape
+    assert np.allclose(a, b, rtol=1e-6, atol=1e-6, equal_nan=True)

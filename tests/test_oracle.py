@@ -115,3 +115,14 @@ def test_oracle_equals_reference_build(orc, ref, stacks):
     pos = np.stack([rows[:, 0], rows[:, 1], rows[:, 4], rows[:, 5], rows[:, 15], rows[:, 16]], axis=1)
     for fit in (1, 2, 3, 4):
         assert np.array_equal(orc.fitting(stacks["stack"], pos, fit, GAUSS_PARAMS), ref.fitting(stacks["stack"], pos, fit, GAUSS_PARAMS))
+
+
+def test_oracle_spline_equals_reference_build(orc, ref, stacks):
+    if ref is None:
+        pytest.skip("oracle/_ref not built (reference sources absent)")
+    import spline_table
+    for roi, dist in ((7, 0.0), (13, 0.3)):
+        params = spline_table.fit_params(roi=roi, sx=15, sy=15, sz=31, dz_nm=30.0, distortion=dist, seed=2)
+        a = orc.localization(stacks["stack"][:4], 103.6, 0.0, 5, params)
+        b = ref.localization(stacks["stack"][:4], 103.6, 0.0, 5, params)
+        assert a.shape == b.shape and np.array_equal(a, b, equal_nan=True)
