@@ -29,6 +29,10 @@ UNIT = "localizations/s"
 WORKLOAD = "c2"
 FIT_MODE = 2
 FIT_PARAMS = np.array([7.0, 1.3, 1.3, 0.0])
+# fit_params per mode for the 7x7 workload: reference Gaussian modes and the Poisson-MLE Gaussian (roi, sigma0,
+# camera offset ADU, gain ADU/photon, max iterations, CRLB filter (0 = off))
+PARAMS_BY_MODE = {1: FIT_PARAMS, 2: FIT_PARAMS, 3: FIT_PARAMS, 4: FIT_PARAMS, 0: FIT_PARAMS,
+                  6: np.array([7.0, 1.3, 100.0, 2.0, 20.0, 0.0])}
 RATIO = 0.0
 PER_PLANE = 8192
 
@@ -126,6 +130,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", type=int, default=0, help="fit arithmetic (PTB_SetFitPrecision)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--fit", type=int, default=None, help="fit mode (default: %d)" % FIT_MODE)
     args = ap.parse_args()
     import torch
     import torch.distributed as dist
@@ -141,6 +146,10 @@ def main():
     import ptb
 
     ptb.set_fit_precision(args.precision)
+    global FIT_MODE, FIT_PARAMS
+    if args.fit is not None:
+        FIT_MODE = args.fit
+        FIT_PARAMS = PARAMS_BY_MODE[FIT_MODE]
     frames = args.frames or synth.SHAPES[WORKLOAD][0]
     h, w = synth.SHAPES[WORKLOAD][1:]
     config = {"workload": "c2: %d frames of %dx%d uint16, ~2684 emitters/frame, 7x7 ROI, fit mode %d, per-plane capacity %d"

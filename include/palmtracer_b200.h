@@ -89,6 +89,10 @@ PTB_API uint64_t PTB_KernelLaunchCount(void);
  * kernels, [3] ordering and numbering, [4] host<->device copies. PTB_StageTimes copies up to n totals into ms and
  * the matching launch counts into launches (either may be NULL), then resets them. Returns the previous setting. */
 PTB_API int PTB_SetProfiling(int enable);
+
+/* FMA throughput probe of the current device (diagnostics): FLOP/s (2 per FMA) of FP64 (fp64 != 0) or FP32
+ * arithmetic, timed with CUDA events over a grid of independent FMA chains; -1 on error. */
+PTB_API double PTB_MeasureFmaPeak(int fp64);
 PTB_API void PTB_StageTimes(double* ms, uint64_t* launches, int n);
 
 #ifdef __cplusplus

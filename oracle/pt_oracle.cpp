@@ -918,6 +918,366 @@ void FitSplineFull(const SplineTable& t, double roiParam, const uint16_t* img, i
 	FillRow(kSplineEmccd, c, out, xo, yo, zo, off, amp, 0, 0, 0, qxy, qz);
 }
 
+}  // namespace
+
+// =============================================================================================================
+// Maximum-likelihood fits (modes 6, 7, 8). These have no counterpart in the reference: they follow the benchmark
+// workloads' definition (Poisson MLE of x, y, I, bg and sigma or z on camera data converted to photons) and are
+// restated here in FP64 from the model maths as the oracle of the GPU modes. Parity for them is pinned by this
+// restatement and by synthetic ground truth, not by the reference.
+//
+// Model: mu_k = bg + I * PSF(pixel k; x, y, s). Mode 6: PSF = Ex(x, sigma) Ey(y, sigma) with Ex the Gaussian
+// integrated over the pixel, Ex = (erf(b) - erf(a)) / 2, a = (c - x - 1/2) / (sqrt2 sigma), b = (c - x + 1/2) /
+// (sqrt2 sigma). Mode 7: sigma_x(z), sigma_y(z) from the astigmatism model of lib/fit/AstigFit.cpp:76-88
+// (sigma_px = A / pixelSize * sqrt(max(0, 1 + U^2 + c3 U^3 + c4 U^4)), U = (z - z0) / w, coefficients per axis in
+// the order [z0, w, c3, c4, A]). Mode 8: PSF = the cubic-spline table of SplineFit (monomial weights per cell), with
+// the PSF centre at table coordinates ((sx - 1) / 2, (sy - 1) / 2) and z_nm = deltaZ * (Z - sz / 2).
+// Objective: Poisson deviance D = 2 sum(mu - d - d ln(mu / d)); damped Fisher scoring (Levenberg-Marquardt with
+// H = 2 sum mu^-1 dmu dmu^T); then up to two undamped Fisher steps in FP64 and the CRLB sqrt(diag(F^-1)).
+namespace {
+
+struct MleCfg {
+	int model = 6, roi = 7, half = 3, n = 49, maxIter = 20;
+	double sigma0 = 1.3, offset = 100, gain = 2, crlbMax = 0;
+	double pixelSize = 160, astig[10] = {}, zMin = -800, zMax = 800;
+	int sx = 0, sy = 0, sz = 0;
+	double dz = 10;
+	const double* coeffs = nullptr;  // SoA [64][sz][sy][sx]
+	size_t cells = 0;
+};
+
+bool ParseMle(int mode, const double* fp, MleCfg& c)
+{
+	c.model = mode;
+	int roi = static_cast<int>(static_cast<size_t>(fp[0]));
+	if (mode == 6) {
+		c.sigma0 = fp[1]; c.offset = fp[2]; c.gain = fp[3]; c.maxIter = static_cast<int>(fp[4]); c.crlbMax = fp[5];
+	}
+	else if (mode == 7) {
+		c.pixelSize = fp[1];
+		for (int i = 0; i < 10; ++i) { c.astig[i] = fp[2 + i]; }
+		c.offset = fp[12]; c.gain = fp[13]; c.maxIter = static_cast<int>(fp[14]); c.zMin = fp[15]; c.zMax = fp[16];
+		c.crlbMax = fp[17];
+	}
+	else {
+		c.sx = static_cast<int>(fp[1]); c.sy = static_cast<int>(fp[2]); c.sz = static_cast<int>(fp[3]); c.dz = fp[4];
+		c.offset = fp[5]; c.gain = fp[6]; c.maxIter = static_cast<int>(fp[7]); c.crlbMax = fp[8];
+		c.coeffs = fp + 9;
+		c.cells = static_cast<size_t>(c.sx) * c.sy * c.sz;
+	}
+	if (roi % 2 == 0) { roi--; }
+	c.roi = roi; c.half = roi / 2; c.n = roi * roi;
+	return roi >= 1 && c.gain > 0;
+}
+
+// Pixel-integrated 1D Gaussian and its derivatives with respect to the emitter position and the width.
+void Erf1D(double c, double x, double s, double& e, double& dx, double& ds)
+{
+	const double k = 1.0 / (1.4142135623730951 * s);
+	const double a = (c - x - 0.5) * k, b = (c - x + 0.5) * k;
+	const double ea = std::exp(-a * a), eb = std::exp(-b * b);
+	e = 0.5 * (std::erf(b) - std::erf(a));
+	dx = (ea - eb) / (2.5066282746310002 * s);
+	ds = (a * ea - b * eb) / (1.7724538509055160 * s);
+}
+
+// Astigmatic width (pixels) and d width / dz for one axis [z0, w, c3, c4, A].
+void AstigSigma(const double* m, double pixelSize, double z, double& s, double& ds)
+{
+	const double u = (z - m[0]) / m[1];
+	const double poly = 1.0 + u * u + m[2] * u * u * u + m[3] * u * u * u * u;
+	const double k = m[4] / pixelSize;
+	if (poly <= 1e-12) { s = k * 1e-6; ds = 0; return; }
+	const double r = std::sqrt(poly);
+	s = k * r;
+	ds = k * (2 * u + 3 * m[2] * u * u + 4 * m[3] * u * u * u) / (2 * r * m[1]);
+}
+
+// Spline PSF value and gradient at table coordinates (X, Y, Z).
+double SplinePsf(const MleCfg& c, double X, double Y, double Z, double& dX, double& dY, double& dZ)
+{
+	auto cell = [](double v, int dim, double& frac) {
+		int i = static_cast<int>(std::floor(v));
+		i = std::min(std::max(i, 0), dim - 1);
+		frac = v - static_cast<double>(i);
+		return i;
+	};
+	double fx, fy, fz;
+	const int ix = cell(X, c.sx, fx), iy = cell(Y, c.sy, fy), iz = cell(Z, c.sz, fz);
+	const size_t pos = (static_cast<size_t>(iz) * c.sy + iy) * c.sx + ix;
+	double px[4] = {1, fx, fx * fx, fx * fx * fx}, py[4] = {1, fy, fy * fy, fy * fy * fy}, pz[4] = {1, fz, fz * fz, fz * fz * fz};
+	double dpx[4] = {0, 1, 2 * fx, 3 * fx * fx}, dpy[4] = {0, 1, 2 * fy, 3 * fy * fy}, dpz[4] = {0, 1, 2 * fz, 3 * fz * fz};
+	double v = 0;
+	dX = dY = dZ = 0;
+	for (int i = 0; i < 4; ++i) {
+		for (int j = 0; j < 4; ++j) {
+			for (int m = 0; m < 4; ++m) {
+				const double co = c.coeffs[static_cast<size_t>(i * 16 + j * 4 + m) * c.cells + pos];
+				v += co * pz[i] * py[j] * px[m];
+				dX += co * pz[i] * py[j] * dpx[m];
+				dY += co * pz[i] * dpy[j] * px[m];
+				dZ += co * dpz[i] * py[j] * px[m];
+			}
+		}
+	}
+	return v;
+}
+
+struct MleRoi {
+	const MleCfg* c;
+	std::vector<double> d;  // photons, row-major
+	double x0, y0;          // local candidate position
+
+	// mu and dmu/dtheta for theta = [bg, I, x, y, s]; returns false for a non-finite model.
+	void Eval(const double* t, std::vector<double>& mu, std::vector<double>& g) const
+	{
+		const MleCfg& C = *c;
+		const int roi = C.roi, h = C.half;
+		mu.assign(C.n, 0);
+		g.assign(static_cast<size_t>(C.n) * 5, 0);
+		if (C.model == 6 || C.model == 7) {
+			double sx = t[4], sy = t[4], dsx = 1, dsy = 1;
+			if (C.model == 7) {
+				AstigSigma(C.astig, C.pixelSize, t[4], sx, dsx);
+				AstigSigma(C.astig + 5, C.pixelSize, t[4], sy, dsy);
+			}
+			std::vector<double> ex(roi), edx(roi), eds(roi), ey(roi), edy(roi), eys(roi);
+			for (int j = 0; j < roi; ++j) { Erf1D(static_cast<double>(j - h), t[2], sx, ex[j], edx[j], eds[j]); }
+			for (int i = 0; i < roi; ++i) { Erf1D(static_cast<double>(i - h), t[3], sy, ey[i], edy[i], eys[i]); }
+			for (int i = 0; i < roi; ++i) {
+				for (int j = 0; j < roi; ++j) {
+					const int k = i * roi + j;
+					const double psf = ex[j] * ey[i];
+					mu[k] = t[0] + t[1] * psf;
+					double* gk = g.data() + static_cast<size_t>(k) * 5;
+					gk[0] = 1;
+					gk[1] = psf;
+					gk[2] = t[1] * edx[j] * ey[i];
+					gk[3] = t[1] * ex[j] * edy[i];
+					gk[4] = t[1] * (eds[j] * dsx * ey[i] + ex[j] * eys[i] * dsy);
+				}
+			}
+			return;
+		}
+		const double X0 = (C.sx - 1) / 2.0, Y0 = (C.sy - 1) / 2.0;
+		for (int i = 0; i < roi; ++i) {
+			for (int j = 0; j < roi; ++j) {
+				const int k = i * roi + j;
+				double dX, dY, dZ;
+				const double psf = SplinePsf(C, X0 + (j - h) - t[2], Y0 + (i - h) - t[3], t[4], dX, dY, dZ);
+				mu[k] = t[0] + t[1] * psf;
+				double* gk = g.data() + static_cast<size_t>(k) * 5;
+				gk[0] = 1;
+				gk[1] = psf;
+				gk[2] = -t[1] * dX;
+				gk[3] = -t[1] * dY;
+				gk[4] = t[1] * dZ;
+			}
+		}
+	}
+
+	// Deviance, gradient and Fisher-scoring matrix (H = 2 sum dmu dmu^T / mu).
+	double Normal(const double* t, double G[5], double Hm[25]) const
+	{
+		std::vector<double> mu, g;
+		Eval(t, mu, g);
+		double D = 0;
+		for (int a = 0; a < 5; ++a) { G[a] = 0; }
+		for (int a = 0; a < 25; ++a) { Hm[a] = 0; }
+		for (int k = 0; k < c->n; ++k) {
+			const double m = std::max(mu[k], 1e-6), dk = d[k];
+			D += dk > 0 ? 2 * (m - dk - dk * std::log(m / dk)) : 2 * m;
+			const double* gk = g.data() + static_cast<size_t>(k) * 5;
+			const double w1 = 2 * (1 - dk / m), w2 = 2 / m;
+			for (int a = 0; a < 5; ++a) {
+				G[a] += w1 * gk[a];
+				for (int b = a; b < 5; ++b) { Hm[a * 5 + b] += w2 * gk[a] * gk[b]; }
+			}
+		}
+		for (int a = 0; a < 5; ++a) {
+			for (int b = 0; b < a; ++b) { Hm[a * 5 + b] = Hm[b * 5 + a]; }
+		}
+		return D;
+	}
+};
+
+// Solves A x = b for a symmetric positive-definite 5x5 A; false if a pivot is not positive.
+bool CholSolve5(const double* A, const double* b, double* x)
+{
+	double L[25] = {};
+	for (int i = 0; i < 5; ++i) {
+		for (int j = 0; j <= i; ++j) {
+			double s = A[i * 5 + j];
+			for (int k = 0; k < j; ++k) { s -= L[i * 5 + k] * L[j * 5 + k]; }
+			if (i == j) {
+				if (!(s > 0)) { return false; }
+				L[i * 5 + i] = std::sqrt(s);
+			}
+			else { L[i * 5 + j] = s / L[j * 5 + j]; }
+		}
+	}
+	double y[5];
+	for (int i = 0; i < 5; ++i) {
+		double s = b[i];
+		for (int k = 0; k < i; ++k) { s -= L[i * 5 + k] * y[k]; }
+		y[i] = s / L[i * 5 + i];
+	}
+	for (int i = 4; i >= 0; --i) {
+		double s = y[i];
+		for (int k = i + 1; k < 5; ++k) { s -= L[k * 5 + i] * x[k]; }
+		x[i] = s / L[i * 5 + i];
+	}
+	return true;
+}
+
+void MleBounds(const MleCfg& c, double x0, double y0, double lo[5], double hi[5])
+{
+	const double h = static_cast<double>(c.half);
+	lo[0] = 1e-3; hi[0] = 1e6;
+	lo[1] = 1.0; hi[1] = 1e9;
+	lo[2] = std::max(x0 - 2.0, -h); hi[2] = std::min(x0 + 2.0, h);
+	lo[3] = std::max(y0 - 2.0, -h); hi[3] = std::min(y0 + 2.0, h);
+	if (c.model == 6) { lo[4] = 0.5; hi[4] = 5.0; }
+	else if (c.model == 7) { lo[4] = c.zMin; hi[4] = c.zMax; }
+	else { lo[4] = 0.0; hi[4] = static_cast<double>(c.sz) - 1e-6; }
+}
+
+// The fit of one candidate (coordinates local to the integer ROI centre); returns false for a failed fit.
+bool MleFit(const MleRoi& R, double t[5], double crlb[5], double& dev)
+{
+	const MleCfg& c = *R.c;
+	double lo[5], hi[5];
+	MleBounds(c, R.x0, R.y0, lo, hi);
+	double dmin = 1e300, sum = 0;
+	for (double v : R.d) { dmin = std::min(dmin, v); sum += v; }
+	t[0] = std::max(dmin, 1e-3);
+	t[1] = std::max(sum - t[0] * c.n, 1.0);
+	t[2] = R.x0;
+	t[3] = R.y0;
+	if (c.model == 6) { t[4] = c.sigma0; }
+	else {
+		// coarse scan of the axial parameter at the initial bg, I, x, y (16 points for mode 7, 8 for mode 8)
+		const int ns = c.model == 7 ? 16 : 8;
+		double best = 1e300, bz = 0.5 * (lo[4] + hi[4]);
+		for (int k = 0; k < ns; ++k) {
+			t[4] = lo[4] + (hi[4] - lo[4]) * (k + 0.5) / ns;
+			double G[5], Hm[25];
+			const double D = R.Normal(t, G, Hm);
+			if (D < best) { best = D; bz = t[4]; }
+		}
+		t[4] = bz;
+	}
+	for (int a = 0; a < 5; ++a) { t[a] = std::min(std::max(t[a], lo[a]), hi[a]); }
+	double G[5], Hm[25];
+	double D = R.Normal(t, G, Hm);
+	if (!std::isfinite(D)) { return false; }
+	double lambda = 1e-3;
+	for (int it = 0; it < c.maxIter; ++it) {
+		double A[25], rhs[5], dt[5];
+		for (int a = 0; a < 25; ++a) { A[a] = Hm[a]; }
+		for (int a = 0; a < 5; ++a) { A[a * 5 + a] *= 1.0 + lambda; rhs[a] = -G[a]; }
+		if (!CholSolve5(A, rhs, dt)) {
+			lambda *= 10;
+			if (lambda > 1e7) { break; }
+			continue;
+		}
+		double tt[5];
+		for (int a = 0; a < 5; ++a) { tt[a] = std::min(std::max(t[a] + dt[a], lo[a]), hi[a]); }
+		double Gt[5], Ht[25];
+		const double Dt = R.Normal(tt, Gt, Ht);
+		if (std::isfinite(Dt) && Dt < D) {
+			const double gainRel = (D - Dt) / (Dt + 1.0);
+			for (int a = 0; a < 5; ++a) { t[a] = tt[a]; G[a] = Gt[a]; }
+			for (int a = 0; a < 25; ++a) { Hm[a] = Ht[a]; }
+			D = Dt;
+			lambda = std::max(lambda * 0.1, 1e-7);
+			if (gainRel < 1e-6) { break; }
+		}
+		else {
+			lambda *= 10;
+			if (lambda > 1e7) { break; }
+		}
+	}
+	// undamped Fisher scoring polish in FP64 (two steps)
+	for (int it = 0; it < 2; ++it) {
+		double rhs[5], dt[5], tt[5];
+		for (int a = 0; a < 5; ++a) { rhs[a] = -G[a]; }
+		if (!CholSolve5(Hm, rhs, dt)) { break; }
+		for (int a = 0; a < 5; ++a) { tt[a] = std::min(std::max(t[a] + dt[a], lo[a]), hi[a]); }
+		double Gt[5], Ht[25];
+		const double Dt = R.Normal(tt, Gt, Ht);
+		if (!(std::isfinite(Dt) && Dt <= D)) { break; }
+		for (int a = 0; a < 5; ++a) { t[a] = tt[a]; G[a] = Gt[a]; }
+		for (int a = 0; a < 25; ++a) { Hm[a] = Ht[a]; }
+		D = Dt;
+	}
+	// CRLB: Fisher information F = H / 2; variances are the diagonal of its inverse
+	for (int a = 0; a < 5; ++a) {
+		double e[5] = {0, 0, 0, 0, 0}, col[5], F[25];
+		for (int q = 0; q < 25; ++q) { F[q] = 0.5 * Hm[q]; }
+		e[a] = 1;
+		if (!CholSolve5(F, e, col)) { return false; }
+		crlb[a] = col[a] > 0 ? std::sqrt(col[a]) : 0.0;
+	}
+	dev = D;
+	for (int a = 0; a < 5; ++a) { if (!std::isfinite(t[a])) { return false; } }
+	return true;
+}
+
+void FitMle(const MleCfg& c, const uint16_t* img, int W, int H, const Candidate& cd, Row& out)
+{
+	const size_t ux = static_cast<size_t>(cd.x), uy = static_cast<size_t>(cd.y);
+	const size_t h = static_cast<size_t>(c.half);
+	const bool nonneg = cd.x >= 0 && cd.y >= 0;
+	if (!nonneg || h > ux || ux >= static_cast<size_t>(W) - h || h > uy || uy >= static_cast<size_t>(H) - h) {
+		FillRow(kG2Sigma, cd, out, cd.x, cd.y, 0);
+		return;
+	}
+	MleRoi R;
+	R.c = &c;
+	R.d.resize(c.n);
+	for (int i = 0; i < c.roi; ++i) {
+		for (int j = 0; j < c.roi; ++j) {
+			const double adu = static_cast<double>(img[(uy - h + i) * static_cast<size_t>(W) + (ux - h + j)]);
+			R.d[i * c.roi + j] = std::max((adu - c.offset) / c.gain, 0.0);
+		}
+	}
+	R.x0 = cd.x - static_cast<double>(ux);
+	R.y0 = cd.y - static_cast<double>(uy);
+	double t[5], crlb[5], dev = 0;
+	const bool ok = MleFit(R, t, crlb, dev);
+	const double qxy = std::sqrt(0.5 * (crlb[2] * crlb[2] + crlb[3] * crlb[3]));
+	if (!ok || (c.crlbMax > 0 && !(qxy <= c.crlbMax))) {
+		FillRow(kG2Sigma, cd, out, cd.x, cd.y, 0);
+		return;
+	}
+	double sx = t[4], sy = t[4], z = 0, qz = -1;
+	if (c.model == 7) {
+		double d1, d2;
+		AstigSigma(c.astig, c.pixelSize, t[4], sx, d1);
+		AstigSigma(c.astig + 5, c.pixelSize, t[4], sy, d2);
+		z = t[4];
+		qz = crlb[4];
+	}
+	if (c.model == 8) { sx = sy = 0; z = c.dz * (t[4] - c.sz / 2.0); qz = c.dz * crlb[4]; }
+	out[cId] = 0; out[cPlane] = 0; out[cIndex] = 0; out[cChannel] = -1;
+	out[cX] = static_cast<double>(ux) + t[2];
+	out[cY] = static_cast<double>(uy) + t[3];
+	out[cZ] = z;
+	out[cIntensity] = t[1];
+	out[cSigmaX] = sx; out[cSigmaY] = sy; out[cTheta] = 0;
+	out[cQualityXY] = qxy; out[cQualityZ] = qz;
+	out[cAmplitude] = (sx > 0 && sy > 0) ? t[1] / (6.283185307179586 * sx * sy) : t[1];
+	out[cOffset] = t[0];
+	out[cSegIntensity] = cd.intensity; out[cSurface] = cd.surf;
+	out[cCircularity] = (sx > kEps && sy > kEps) ? std::min(sx, sy) / std::max(sx, sy) : 1;
+	(void)dev;
+}
+
+}  // namespace
+
+namespace {
+
 // Strict weak order on (Y, X) with std::weak_order semantics (FrameProcessor.cpp:35-39).
 bool RowLess(const Row& a, const Row& b)
 {
@@ -936,8 +1296,13 @@ void ProcessFrame(const uint16_t* img, int H, int W, double thr, double ratio, s
 	const size_t count = std::min(seg.cands.size(), maxPoints);
 	if (seg.cands.size() > maxPoints) { std::fprintf(stderr, "[WARNING] Density is too high; some points are missed (output capacity exceeded).\n"); }
 	rows.assign(count, Row{});
-	const int mode = (fit >= 1 && fit <= 5) ? fit : kNone;
-	if (mode >= kG2Fixed && mode <= kG3Theta) {
+	const int mode = (fit >= 1 && fit <= 8) ? fit : kNone;
+	if (mode >= 6) {
+		MleCfg mc;
+		ParseMle(mode, fp, mc);
+		for (size_t i = 0; i < count; ++i) { FitMle(mc, img, W, H, seg.cands[i], rows[i]); }
+	}
+	else if (mode >= kG2Fixed && mode <= kG3Theta) {
 		FitConfig cf;
 		cf.Init(mode, fp, img, W, H);
 		for (size_t i = 0; i < count; ++i) { FitGaussian(cf, seg.cands[i], rows[i]); }
@@ -1006,7 +1371,12 @@ uint64_t orc_Fitting(const uint16_t* input, const double* positions, uint64_t nP
 		Candidate c;
 		c.x = pos[2]; c.y = pos[3]; c.intensity = pos[4]; c.surf = pos[5];
 		Row r{};
-		if (fit == kSplineEmccd) {
+		if (fit >= 6 && fit <= 8) {
+			MleCfg mc;
+			ParseMle(static_cast<int>(fit), fp, mc);
+			FitMle(mc, img, static_cast<int>(width), static_cast<int>(height), c, r);
+		}
+		else if (fit == kSplineEmccd) {
 			SplineTable t;
 			t.Init(fp);
 			FitSplineFull(t, fp[0], img, static_cast<int>(width), static_cast<int>(height), c, r);

@@ -138,6 +138,12 @@ PTB_API const char* PTB_LastError(void) { return ptb::LastError().c_str(); }
 
 PTB_API uint64_t PTB_KernelLaunchCount(void) { return ptb::LaunchCount(); }
 
+PTB_API double PTB_MeasureFmaPeak(int fp64)
+{
+	ptb::ClearError();
+	return ptb::MeasureFmaPeak(fp64);
+}
+
 PTB_API int PTB_SetProfiling(int enable)
 {
 	std::unique_lock<std::mutex> lock;

@@ -50,7 +50,7 @@ bool CheckCuda(cudaError_t e, const char* what, const char* file, int line)
 bool ParseFitParams(uint64_t fit, const double* fp, FitParams& out, std::vector<double>& splineHost)
 {
 	out = FitParams{};
-	out.mode = (fit >= 1 && fit <= 5) ? static_cast<int>(fit) : kNone;
+	out.mode = (fit >= 1 && fit <= 8) ? static_cast<int>(fit) : kNone;
 	out.sigmaX = 1.0;
 	out.sigmaY = 2.0;
 	out.theta = 0.0;
@@ -65,6 +65,42 @@ bool ParseFitParams(uint64_t fit, const double* fp, FitParams& out, std::vector<
 	}
 	int roi = static_cast<int>(static_cast<size_t>(fp[0]));
 	out.roiParam = fp[0];
+	if (out.mode >= kMleGauss) {
+		MleParams& m = out.mle;
+		m = MleParams{};
+		m.model = out.mode;
+		if (out.mode == kMleGauss) {
+			m.sigma0 = fp[1]; m.offset = fp[2]; m.gain = fp[3]; m.maxIter = static_cast<int>(fp[4]); m.crlbMax = fp[5];
+		}
+		else if (out.mode == kMleAstig) {
+			m.pixelSize = fp[1];
+			for (int i = 0; i < 10; ++i) { m.astig[i] = fp[2 + i]; }
+			m.offset = fp[12]; m.gain = fp[13]; m.maxIter = static_cast<int>(fp[14]); m.zMin = fp[15]; m.zMax = fp[16];
+			m.crlbMax = fp[17];
+		}
+		else {
+			m.sx = static_cast<int>(fp[1]); m.sy = static_cast<int>(fp[2]); m.sz = static_cast<int>(fp[3]); m.dz = fp[4];
+			m.offset = fp[5]; m.gain = fp[6]; m.maxIter = static_cast<int>(fp[7]); m.crlbMax = fp[8];
+			out.sx = m.sx; out.sy = m.sy; out.sz = m.sz;
+			out.splineSize = static_cast<long long>(m.sx) * m.sy * m.sz;
+			if (m.sx <= 0 || m.sy <= 0 || m.sz <= 0) { SetError("spline dimensions must be positive"); return false; }
+			splineHost.assign(fp + 9, fp + 9 + static_cast<size_t>(out.splineSize) * 64);
+		}
+		if (roi % 2 == 0) { roi--; }
+		m.roi = roi;
+		m.half = roi / 2;
+		m.n = roi * roi;
+		if (!(m.gain > 0) || m.maxIter < 0 || roi > 15) {
+			SetError("MLE fit parameters: gain must be > 0, maxIter >= 0 and the ROI at most 15 pixels");
+			return false;
+		}
+		if (out.mode == kMleSpline && (m.sx < roi + 5 || m.sy < roi + 5)) {
+			SetError("spline table must be at least ROI + 5 cells wide in x and y");
+			return false;
+		}
+		out.roi = roi; out.half = roi / 2; out.n = roi * roi; out.nParams = 5;
+		return true;
+	}
 	if (out.mode == kSplineEmccd) {
 		// [roi, sx, sy, sz, deltaZ, coefficients SoA [64][sz][sy][sx]] (SplineFit.cpp:36-50)
 		out.sx = static_cast<int>(static_cast<size_t>(fp[1]));
@@ -196,6 +232,7 @@ Engine::~Engine()
 	if (pool_) { cudaFree(pool_); }
 	if (img_) { cudaFree(img_); }
 	if (spline_) { cudaFree(spline_); }
+	if (fallbacks_) { cudaFree(fallbacks_); }
 	if (hostCnt_) { cudaFreeHost(hostCnt_); }
 	if (stream_) { cudaStreamDestroy(stream_); }
 }
@@ -276,7 +313,9 @@ long long Engine::RunChunk(const uint16_t* dImg, int H, int W, int B, double thr
 	ok = ok && LaunchSegment(ws_, ratio, strict_, maxPoints, st);
 	ok = ok && LaunchBuildCandidates(ws_, st);
 	mark(2);
-	ok = ok && LaunchFit(dImg, H, W, ws_.g.N, ws_.cand, &ws_.cnt->nfit, 0, ws_.capRows, fp, ws_.rows, ws_.fitFlag, precision_, st);
+	FitParams fpr = fp;
+	if (ok && fp.mode >= kMleGauss && fp.lanes == 0) { ok = Autotune(fpr, dImg, H, W); }
+	ok = ok && LaunchFit(dImg, H, W, ws_.g.N, ws_.cand, &ws_.cnt->nfit, 0, ws_.capRows, fpr, ws_.rows, ws_.fitFlag, precision_, st);
 	mark(3);
 	ok = ok && LaunchSortFrames(ws_, dOut, idBase, planeBase, st);
 	mark(4);
@@ -348,6 +387,44 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 	return static_cast<long long>(rows * kCols);
 }
 
+int Engine::TunedLanes(const FitParams& fp) const
+{
+	if (const char* env = std::getenv("PTB_MLE_LANES")) { return std::atoi(env); }
+	const int key = fp.mode * 64 + fp.roi;
+	for (const auto& kv : tuned_) {
+		if (kv.first == key) { return kv.second; }
+	}
+	return 0;  // not tuned yet: the first chunk with candidates tunes it
+}
+
+// Times every lane-group width on this chunk's candidates and keeps the fastest for (mode, ROI).
+bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W)
+{
+	static const int kChoices[] = {1, 8, 16, 32};
+	cudaEvent_t a, b;
+	if (!PTB_CUDA(cudaEventCreate(&a)) || !PTB_CUDA(cudaEventCreate(&b))) { return false; }
+	float best = 1e30f;
+	int bestLanes = 32;
+	for (int lanes : kChoices) {
+		FitParams t = fp;
+		t.lanes = lanes;
+		cudaEventRecord(a, stream_);
+		if (!LaunchFit(dImg, H, W, ws_.g.N, ws_.cand, &ws_.cnt->nfit, 0, ws_.capRows, t, ws_.rows, ws_.fitFlag, precision_, stream_)) {
+			return false;
+		}
+		cudaEventRecord(b, stream_);
+		if (!PTB_CUDA(cudaEventSynchronize(b))) { return false; }
+		float ms = 0;
+		cudaEventElapsedTime(&ms, a, b);
+		if (ms < best) { best = ms; bestLanes = lanes; }
+	}
+	cudaEventDestroy(a);
+	cudaEventDestroy(b);
+	fp.lanes = bestLanes;
+	tuned_.push_back({fp.mode * 64 + fp.roi, bestLanes});
+	return true;
+}
+
 void Engine::StageTimes(double* ms, uint64_t* launches, int n)
 {
 	for (int k = 0; k < kStages && k < n; ++k) {
@@ -360,6 +437,29 @@ void Engine::StageTimes(double* ms, uint64_t* launches, int n)
 
 bool Engine::UploadSpline(FitParams& fp, const std::vector<double>& spline)
 {
+	if (fp.mode >= kMleGauss) {
+		if (!fallbacks_ && !PTB_CUDA(cudaMalloc(&fallbacks_, sizeof(unsigned int)))) { return false; }
+		fp.mle.fallbacks = static_cast<unsigned int*>(fallbacks_);
+		fp.lanes = TunedLanes(fp);
+	}
+	if (fp.mode == kMleSpline) {
+		// FP32 cell-major copy of the [64][cell] table
+		const size_t cells = static_cast<size_t>(fp.splineSize);
+		std::vector<float> aos(cells * 64);
+		for (size_t i = 0; i < 64; ++i) {
+			for (size_t c = 0; c < cells; ++c) { aos[c * 64 + i] = static_cast<float>(spline[i * cells + c]); }
+		}
+		const size_t bytes = aos.size() * sizeof(float);
+		if (bytes > splineBytes_) {
+			if (spline_) { cudaFree(spline_); spline_ = nullptr; splineBytes_ = 0; }
+			if (!PTB_CUDA(cudaMalloc(&spline_, bytes))) { return false; }
+			splineBytes_ = bytes;
+		}
+		if (!PTB_CUDA(cudaMemcpyAsync(spline_, aos.data(), bytes, cudaMemcpyHostToDevice, stream_))) { return false; }
+		if (!PTB_CUDA(cudaStreamSynchronize(stream_))) { return false; }
+		fp.mle.table = static_cast<const float*>(spline_);
+		return true;
+	}
 	if (fp.mode != kSplineEmccd) { return true; }
 	// cell-major copy of the reference's [64][cell] table: one pixel's 64 coefficients become contiguous
 	const size_t cells = static_cast<size_t>(fp.splineSize);

@@ -8,6 +8,7 @@
 #include <mutex>
 #include <string>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "pt_common.cuh"
@@ -16,6 +17,7 @@ namespace ptb {
 
 bool ParseFitParams(uint64_t fit, const double* fp, FitParams& out, std::vector<double>& splineHost);
 uint64_t LaunchCount();
+double MeasureFmaPeak(int fp64);
 
 class Engine {
 public:
@@ -45,6 +47,8 @@ private:
 	bool Reserve(int H, int W, int B, uint32_t rowsCap);
 	bool ReserveImage(size_t bytes);
 	bool UploadSpline(FitParams& fp, const std::vector<double>& spline);
+	int TunedLanes(const FitParams& fp) const;
+	bool Autotune(FitParams& fp, const uint16_t* dImg, int H, int W);
 	int ChunkFrames(int H, int W, uint64_t planes, uint32_t maxPoints) const;
 	long long RunChunk(const uint16_t* dImg, int H, int W, int B, double thr, double ratio, uint32_t maxPoints,
 	                   const FitParams& fp, double* dOut, unsigned long long idBase, unsigned long long planeBase,
@@ -59,6 +63,8 @@ private:
 	void* img_ = nullptr;
 	size_t imgBytes_ = 0;
 	void* spline_ = nullptr;
+	void* fallbacks_ = nullptr;
+	std::vector<std::pair<int, int>> tuned_;  // (mode * 64 + roi) -> lanes per ROI
 	size_t splineBytes_ = 0;
 	Workspace ws_{};
 	int strict_ = 0;

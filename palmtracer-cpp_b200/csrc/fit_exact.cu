@@ -1,15 +1,19 @@
-// Gaussian least-squares LM fits (modes 1-4) in FP64 with the reference's exact order of operations, one thread per
-// ROI. This file is compiled with -fmad=false: every product and sum is rounded on its own, as in the reference
-// built with -ffp-contract=off, so each ROI follows the reference's iteration path decision for decision (sums over
-// pixels are sequential in raster order, the damped matrix is inverted by the same equilibrated Gauss-Jordan and
-// dp = inverse * beta is accumulated in the same order). Results then differ from the reference only where CUDA's
-// exp / sin / cos round differently from the host C library in the last place.
+// Gaussian least-squares LM fits (modes 1-4) in FP64 with the reference's exact order of operations, one warp per
+// ROI. This file is compiled with -fmad=false: every product and sum is rounded on its own, as in the reference built
+// with -ffp-contract=off, so each ROI follows the reference's iteration path decision for decision; results differ
+// from the reference only where CUDA's exp / sin / cos round differently from the host C library in the last place.
 //
 // Reference: lib/fit/GaussianFit.cpp:48-295, lib/fit/GaussianModel.cpp:19-52, lib/fit/Fitting.cpp:61-175,
 // lib/signal_processing/Matrix.cpp:297-355.
 //
-// Mapping: thread per candidate, grid-stride. The per-thread normal matrix, its damped copy and the inverse live in
-// per-thread local memory (L1-resident); the ROI pixels are re-read through the read-only cache each pass.
+// How the order is kept while the warp works in parallel:
+//   * per-pixel terms (model, residual, gradient products) are computed by the lanes, 32 pixels at a time, and staged
+//     in shared memory; each accumulator (err, beta[a], alpha[a][b] for a <= b) is then owned by one lane, which adds
+//     that chunk's terms in pixel order - the reference's sequential sums, term for term;
+//   * the damped matrix is inverted column-parallel: lane c < p owns column c of the matrix, lane p + c column c of
+//     the inverse, and every element goes through exactly the reference's Gauss-Jordan operations (equilibration,
+//     partial pivoting, row normalisation, elimination), whose results do not depend on the order across elements;
+//   * dp = inverse * beta and every other small-vector step run identically on all lanes in the reference's order.
 #include <algorithm>
 
 #include "pt_common.cuh"
@@ -17,6 +21,10 @@
 namespace ptb {
 
 namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWarps = 4;
+constexpr int kMaxTerms = 36;  // 1 + 7 + 28 for mode 4
 
 template <int MODE> struct NpOf;
 template <> struct NpOf<kG2Fixed> { static constexpr int v = 4; };
@@ -86,77 +94,201 @@ struct GModel {
 	}
 };
 
-// Equilibrated Gauss-Jordan inverse with partial pivoting (Matrix.cpp:297-355); false where the reference throws.
-template <int NP>
-__device__ bool InvertGJ(double* a, double* inv)
+struct WarpSmem {
+	double terms[kMaxTerms][33];  // [accumulator][pixel of the chunk], padded
+	double acc[kMaxTerms + 4];    // broadcast of the accumulators
+};
+
+struct Roi {
+	const uint16_t* base;
+	int W, roi, n, half;
+	unsigned long long ux, uy;
+	__device__ __forceinline__ double Pix(int k, double& X, double& Y) const
+	{
+		const int i = k / roi, j = k - i * roi;
+		X = static_cast<double>(ux + j - half);
+		Y = static_cast<double>(uy + i - half);
+		return static_cast<double>(__ldg(base + static_cast<long long>(i) * W + j));
+	}
+};
+
+// err, beta and alpha (upper triangle, row major) at p, summed in pixel order. Every lane returns the same values.
+template <int MODE>
+__device__ double NormalExact(WarpSmem& S, const Roi& R, const GModel<MODE>& m, const double* p, bool circular,
+                              double (&beta)[NpOf<MODE>::v], double (&alphaU)[NpOf<MODE>::v * (NpOf<MODE>::v + 1) / 2])
 {
-	for (int i = 0; i < NP * NP; ++i) { inv[i] = 0.0; }
-	for (int i = 0; i < NP; ++i) {
-		double scale = 0.0;
-		for (int j = 0; j < NP; ++j) {
-			const double v = a[i * NP + j];
-			if (!isfinite(v)) { return false; }
-			scale = fmax(scale, fabs(v));
+	constexpr int NP = NpOf<MODE>::v;
+	constexpr int NT = 1 + NP + NP * (NP + 1) / 2;
+	const int lane = threadIdx.x & 31;
+	double acc0 = 0.0, acc1 = 0.0;  // accumulators lane and lane + 32
+	for (int c0 = 0; c0 < R.n; c0 += 32) {
+		const int k = c0 + lane;
+		if (k < R.n) {
+			double X, Y, g[NP];
+			const double v = R.Pix(k, X, Y);
+			const double hat = m.template Eval<true>(X - p[2], Y - p[3], g);
+			const double d = v - hat;
+			if (circular) { g[NP - 1] = 0.0; }
+			S.terms[0][lane] = d * d;
+			#pragma unroll
+			for (int a = 0; a < NP; ++a) { S.terms[1 + a][lane] = g[a] * d; }
+			int q = 1 + NP;
+			#pragma unroll
+			for (int a = 0; a < NP; ++a) {
+				#pragma unroll
+				for (int b = a; b < NP; ++b) { S.terms[q++][lane] = g[a] * g[b]; }
+			}
 		}
-		if (scale == 0.0) { return false; }
-		for (int j = 0; j < NP; ++j) { a[i * NP + j] /= scale; }
-		inv[i * NP + i] = 1.0 / scale;
+		__syncwarp();
+		const int cnt = min(32, R.n - c0);
+		if (lane < NT) {
+			for (int j = 0; j < cnt; ++j) { acc0 += S.terms[lane][j]; }
+		}
+		if (lane + 32 < NT) {
+			for (int j = 0; j < cnt; ++j) { acc1 += S.terms[lane + 32][j]; }
+		}
+		__syncwarp();
+	}
+	if (lane < NT) { S.acc[lane] = acc0; }
+	if (lane + 32 < NT) { S.acc[lane + 32] = acc1; }
+	__syncwarp();
+	const double err = S.acc[0];
+	#pragma unroll
+	for (int a = 0; a < NP; ++a) { beta[a] = S.acc[1 + a]; }
+	#pragma unroll
+	for (int q = 0; q < NP * (NP + 1) / 2; ++q) { alphaU[q] = S.acc[1 + NP + q]; }
+	__syncwarp();
+	return err;
+}
+
+template <int NP>
+__device__ __forceinline__ int U(int a, int b) { return a <= b ? a * NP - (a * (a - 1)) / 2 + (b - a) : b * NP - (b * (b - 1)) / 2 + (a - b); }
+
+// Column-parallel equilibrated Gauss-Jordan inverse of the damped matrix, then dp = inverse * beta in the reference's
+// order (Matrix.cpp:297-355, GaussianFit.cpp:85-106). Returns false where the reference's inversion throws.
+template <int NP>
+__device__ bool SolveExact(const double (&alphaU)[NP * (NP + 1) / 2], const double (&beta)[NP], double lambda, double (&dp)[NP])
+{
+	const int lane = threadIdx.x & 31;
+	const bool isA = lane < NP, isI = lane >= NP && lane < 2 * NP;
+	const int col = isA ? lane : lane - NP;
+	double cv[NP];
+	bool fin = true;
+	#pragma unroll
+	for (int r = 0; r < NP; ++r) {
+		double v = 0.0;
+		if (isA) {
+			const double a = alphaU[U<NP>(r, col)];
+			v = r == col ? (a == 0.0 ? 1.0 : (1.0 + lambda) * a) : a;
+			fin = fin && isfinite(v);
+		}
+		cv[r] = v;
+	}
+	if (!__all_sync(kFull, fin)) { return false; }
+	// row equilibration: scale_r = max_c |a[r][c]| (order-independent), in /= scale, out[r][r] = 1 / scale
+	#pragma unroll
+	for (int r = 0; r < NP; ++r) {
+		double m = isA ? fabs(cv[r]) : 0.0;
+		#pragma unroll
+		for (int d = 16; d > 0; d >>= 1) { m = fmax(m, __shfl_xor_sync(kFull, m, d)); }
+		if (m == 0.0) { return false; }
+		if (isA) { cv[r] /= m; }
+		if (isI) { cv[r] = r == col ? 1.0 / m : 0.0; }
 	}
 	const double tol = 2.220446049250313e-16 * static_cast<double>(NP);
+	#pragma unroll
 	for (int i = 0; i < NP; ++i) {
 		int piv = i;
+		double best = cv[i];
+		#pragma unroll
 		for (int j = i + 1; j < NP; ++j) {
-			if (fabs(a[j * NP + i]) > fabs(a[piv * NP + i])) { piv = j; }
+			if (fabs(cv[j]) > fabs(best)) { piv = j; best = cv[j]; }
 		}
-		if (!isfinite(a[piv * NP + i]) || fabs(a[piv * NP + i]) <= tol) { return false; }
+		piv = __shfl_sync(kFull, piv, i);
+		best = __shfl_sync(kFull, best, i);
+		if (!isfinite(best) || fabs(best) <= tol) { return false; }
 		if (piv != i) {
-			for (int j = 0; j < NP; ++j) {
-				const double t = a[i * NP + j];
-				a[i * NP + j] = a[piv * NP + j];
-				a[piv * NP + j] = t;
-				const double u = inv[i * NP + j];
-				inv[i * NP + j] = inv[piv * NP + j];
-				inv[piv * NP + j] = u;
+			#pragma unroll
+			for (int j = i + 1; j < NP; ++j) {
+				if (j == piv) {
+					const double t = cv[i];
+					cv[i] = cv[j];
+					cv[j] = t;
+				}
 			}
 		}
-		const double pinv = 1.0 / a[i * NP + i];
-		for (int j = 0; j < NP; ++j) {
-			a[i * NP + j] *= pinv;
-			inv[i * NP + j] *= pinv;
-		}
+		const double pinv = 1.0 / __shfl_sync(kFull, cv[i], i);
+		cv[i] *= pinv;
+		#pragma unroll
 		for (int j = 0; j < NP; ++j) {
 			if (j == i) { continue; }
-			const double f = a[j * NP + i];
-			for (int k = 0; k < NP; ++k) {
-				a[j * NP + k] -= f * a[i * NP + k];
-				inv[j * NP + k] -= f * inv[i * NP + k];
-			}
+			const double f = __shfl_sync(kFull, cv[j], i);
+			cv[j] -= f * cv[i];
 		}
 	}
-	for (int i = 0; i < NP * NP; ++i) {
-		if (!isfinite(a[i]) || !isfinite(inv[i])) { return false; }
+	fin = true;
+	#pragma unroll
+	for (int r = 0; r < NP; ++r) { fin = fin && ((!isA && !isI) || isfinite(cv[r])); }
+	if (!__all_sync(kFull, fin)) { return false; }
+	// dp_i = sum_j inv[i][j] beta_j, j ascending; column j of the inverse is on lane NP + j
+	#pragma unroll
+	for (int i = 0; i < NP; ++i) {
+		double s = 0.0;
+		#pragma unroll
+		for (int j = 0; j < NP; ++j) { s += __shfl_sync(kFull, cv[i], NP + j) * beta[j]; }
+		dp[i] = s;
 	}
 	return true;
 }
 
-__device__ void Store(double* r, int mode, const Cand& c, double x, double y, double off, double amp, double sx, double sy,
-                      double th, double qxy)
+__device__ void StoreRow(double* row, const Cand& c, double x, double y, double off, double amp, double sx, double sy,
+                         double th, double qxy)
 {
-	r[cId] = 0; r[cPlane] = 0; r[cIndex] = 0; r[cChannel] = -1;
-	r[cX] = x; r[cY] = y; r[cZ] = 0;
-	r[cIntensity] = (amp > kEps && sx > kEps && sy > kEps) ? 2.0 * 3.141592653589793 * amp * sx * sy : -1;
-	r[cSigmaX] = sx; r[cSigmaY] = sy; r[cTheta] = th;
-	r[cQualityXY] = qxy; r[cQualityZ] = -1;
-	r[cAmplitude] = amp; r[cOffset] = off;
-	r[cSegIntensity] = c.intensity; r[cSurface] = c.surf;
-	r[cCircularity] = (sx > kEps && sy > kEps) ? fmin(sx, sy) / fmax(sx, sy) : 1;
+	const int lane = threadIdx.x & 31;
+	double v;
+	switch (lane) {
+		case cChannel: v = -1; break;
+		case cX: v = x; break;
+		case cY: v = y; break;
+		case cIntensity: v = (amp > kEps && sx > kEps && sy > kEps) ? 2.0 * 3.141592653589793 * amp * sx * sy : -1; break;
+		case cSigmaX: v = sx; break;
+		case cSigmaY: v = sy; break;
+		case cTheta: v = th; break;
+		case cQualityXY: v = qxy; break;
+		case cQualityZ: v = -1; break;
+		case cAmplitude: v = amp; break;
+		case cOffset: v = off; break;
+		case cSegIntensity: v = c.intensity; break;
+		case cSurface: v = c.surf; break;
+		case cCircularity: v = (sx > kEps && sy > kEps) ? fmin(sx, sy) / fmax(sx, sy) : 1; break;
+		default: v = 0; break;
+	}
+	if (lane < kCols) { row[lane] = v; }
+}
+
+// Sum of the lanes' per-pixel values over the ROI in pixel order (lane 0 of each chunk first).
+__device__ double ChunkedOrderedSum(WarpSmem& S, double mine, int cnt, double total)
+{
+	const int lane = threadIdx.x & 31;
+	S.terms[0][lane] = mine;
+	__syncwarp();
+	if (lane == 0) {
+		for (int j = 0; j < cnt; ++j) { total += S.terms[0][j]; }
+		S.acc[0] = total;
+	}
+	__syncwarp();
+	total = S.acc[0];
+	__syncwarp();
+	return total;
 }
 
 template <int MODE>
-__device__ void FitExact(const uint16_t* frame, int H, int W, const FitParams& fp, const Cand& cd, double* row)
+__device__ void FitWarp(WarpSmem& S, const uint16_t* frame, int H, int W, const FitParams& fp, const Cand& cd, double* row)
 {
 	constexpr int NP = NpOf<MODE>::v;
-	auto sentinel = [&](double x, double y) { Store(row, MODE, cd, x, y, -1, -1, -1, -1, -1, -1); };
+	constexpr int NU = NP * (NP + 1) / 2;
+	const int lane = threadIdx.x & 31;
+	auto sentinel = [&](double x, double y) { StoreRow(row, cd, x, y, -1, -1, -1, -1, -1, -1); };
 	const bool nonneg = cd.x >= 0.0 && cd.y >= 0.0;
 	const unsigned long long ux = nonneg ? static_cast<unsigned long long>(cd.x) : 0ull;
 	const unsigned long long uy = nonneg ? static_cast<unsigned long long>(cd.y) : 0ull;
@@ -165,20 +297,25 @@ __device__ void FitExact(const uint16_t* frame, int H, int W, const FitParams& f
 		sentinel(cd.x, cd.y);
 		return;
 	}
-	const int roi = fp.roi, n = fp.n, hh = fp.half;
-	const uint16_t* base = frame + static_cast<long long>(uy - h) * W + static_cast<long long>(ux - h);
-	auto pix = [&](int k, double& X, double& Y) {
-		const int i = k / roi, j = k - i * roi;
-		X = static_cast<double>(ux + j - hh);
-		Y = static_cast<double>(uy + i - hh);
-		return static_cast<double>(__ldg(base + static_cast<long long>(i) * W + j));
-	};
+	Roi R;
+	R.base = frame + static_cast<long long>(uy - h) * W + static_cast<long long>(ux - h);
+	R.W = W;
+	R.roi = fp.roi;
+	R.n = fp.n;
+	R.half = fp.half;
+	R.ux = ux;
+	R.uy = uy;
 	double vmin = 1.7976931348623157e308, vmax = -1.7976931348623157e308;
-	for (int k = 0; k < n; ++k) {
+	for (int k = lane; k < R.n; k += 32) {
 		double X, Y;
-		const double v = pix(k, X, Y);
+		const double v = R.Pix(k, X, Y);
 		vmin = fmin(vmin, v);
 		vmax = fmax(vmax, v);
+	}
+	#pragma unroll
+	for (int d = 16; d > 0; d >>= 1) {
+		vmin = fmin(vmin, __shfl_xor_sync(kFull, vmin, d));
+		vmax = fmax(vmax, __shfl_xor_sync(kFull, vmax, d));
 	}
 	double lo[NP], p[NP], hi[NP];
 	lo[0] = 0; lo[1] = 0; lo[2] = cd.x - 1; lo[3] = cd.y - 1;
@@ -193,74 +330,64 @@ __device__ void FitExact(const uint16_t* frame, int H, int W, const FitParams& f
 		p[5] = r2 * fp.sigmaY;
 	}
 	if constexpr (MODE == kG3Theta) { lo[6] = -150; p[6] = fp.theta; hi[6] = 150; }
-	double alpha[NP * NP], work[NP * NP], inv[NP * NP], beta[NP], dp[NP], pTry[NP], g[NP];
+	double alphaU[NU], beta[NP], dp[NP], pTry[NP];
 	GModel<MODE> m;
-	auto normal = [&]() {  // GaussianFit.cpp:219-245
-		for (int i = 0; i < NP * NP; ++i) { alpha[i] = 0.0; }
-		for (int i = 0; i < NP; ++i) { beta[i] = 0.0; }
-		double err = 0.0;
+	auto normal = [&]() {
 		m.Make(p, fp.sigmaX, fp.theta);
 		const bool circular = MODE == kG3Theta && fabs(p[4] - p[5]) <= 2.220446049250313e-16;
-		for (int k = 0; k < n; ++k) {
-			double X, Y;
-			const double v = pix(k, X, Y);
-			const double hat = m.template Eval<true>(X - p[2], Y - p[3], g);
-			const double d = v - hat;
-			err += d * d;
-			if (circular) { g[NP - 1] = 0.0; }
-			for (int a = 0; a < NP; ++a) {
-				beta[a] += g[a] * d;
-				for (int b = 0; b < NP; ++b) { alpha[a * NP + b] += g[a] * g[b]; }
-			}
-		}
-		return err;
+		return NormalExact<MODE>(S, R, m, p, circular, beta, alphaU);
 	};
-	auto trial = [&]() {  // GaussianFit.cpp:262-271
+	auto trial = [&]() {
 		GModel<MODE> t;
 		t.Make(pTry, fp.sigmaX, fp.theta);
 		double res = 0.0;
-		for (int k = 0; k < n; ++k) {
-			double X, Y;
-			const double v = pix(k, X, Y);
-			const double d = v - t.template Eval<false>(X - pTry[2], Y - pTry[3], nullptr);
-			res += d * d;
+		for (int c0 = 0; c0 < R.n; c0 += 32) {
+			const int k = c0 + lane;
+			double sq = 0.0;
+			if (k < R.n) {
+				double X, Y;
+				const double v = R.Pix(k, X, Y);
+				const double d = v - t.template Eval<false>(X - pTry[2], Y - pTry[3], nullptr);
+				sq = d * d;
+			}
+			res = ChunkedOrderedSum(S, sq, min(32, R.n - c0), res);
 		}
 		return res;
 	};
 	auto relStep = [&]() {
 		double r = 0.0;
+		#pragma unroll
 		for (int a = 0; a < NP; ++a) { r = fmax(r, fabs(dp[a]) / fmax(fabs(p[a]), 1e-12)); }
 		return r;
 	};
 	auto maxBeta = [&]() {
 		double r = 0.0;
+		#pragma unroll
 		for (int a = 0; a < NP; ++a) { r = fmax(r, fabs(beta[a])); }
 		return r;
 	};
 	double err = normal();
 	bool fin = isfinite(err);
+	#pragma unroll
 	for (int a = 0; a < NP; ++a) { fin = fin && isfinite(beta[a]); }
 	if (!fin) { sentinel(cd.x, cd.y); return; }
 	double lambda = 1e-2;
-	double mm = maxBeta();
+	const double mm = maxBeta();
 	for (int it = (mm < 1e-6) ? kMaxIter : 0; it < kMaxIter; ++it) {
-		for (int i = 0; i < NP * NP; ++i) { work[i] = alpha[i]; }
-		for (int i = 0; i < NP; ++i) {
-			const int d = i * NP + i;
-			work[d] = alpha[d] == 0.0 ? 1.0 : (1.0 + lambda) * alpha[d];
-		}
-		if (!InvertGJ<NP>(work, inv)) {
+		if (!SolveExact<NP>(alphaU, beta, lambda, dp)) {
 			if (lambda < 1e7) { lambda = fmin(lambda * 11, 1e7); continue; }
 			sentinel(cd.x, cd.y);
 			return;
 		}
+		bool dpFin = true;
+		#pragma unroll
 		for (int i = 0; i < NP; ++i) {
-			dp[i] = 0.0;
-			for (int j = 0; j < NP; ++j) { dp[i] += inv[i * NP + j] * beta[j]; }
-			if (!isfinite(dp[i])) { sentinel(cd.x, cd.y); return; }
+			dpFin = dpFin && isfinite(dp[i]);
 			pTry[i] = fmin(fmax(p[i] + dp[i], lo[i]), hi[i]);
 		}
+		if (!dpFin) { sentinel(cd.x, cd.y); return; }
 		bool tiny = true;
+		#pragma unroll
 		for (int i = 0; i < NP; ++i) {
 			dp[i] = pTry[i] - p[i];
 			tiny = tiny && fabs(dp[i]) < 1e-15;
@@ -271,9 +398,11 @@ __device__ void FitExact(const uint16_t* frame, int H, int W, const FitParams& f
 			continue;
 		}
 		double quad = 0.0, lin = 0.0;
+		#pragma unroll
 		for (int i = 0; i < NP; ++i) {
 			double t = 0.0;
-			for (int j = 0; j < NP; ++j) { t += alpha[i * NP + j] * dp[j]; }
+			#pragma unroll
+			for (int j = 0; j < NP; ++j) { t += alphaU[U<NP>(i, j)] * dp[j]; }
 			quad += dp[i] * t;
 			lin += dp[i] * beta[i];
 		}
@@ -285,10 +414,12 @@ __device__ void FitExact(const uint16_t* frame, int H, int W, const FitParams& f
 			continue;
 		}
 		double denom = 0.0;
+		#pragma unroll
 		for (int i = 0; i < NP; ++i) { denom += dp[i] * ((lambda * dp[i]) + beta[i]); }
 		const double errTry = trial();
 		const double rho = (err - errTry) / (2.0 * denom);
 		if (rho > 1e-2) {
+			#pragma unroll
 			for (int i = 0; i < NP; ++i) { p[i] = pTry[i]; }
 			err = normal();
 			lambda = fmax(lambda / 9, 1e-7);
@@ -299,62 +430,87 @@ __device__ void FitExact(const uint16_t* frame, int H, int W, const FitParams& f
 		}
 		if (it >= 2) {
 			if (relStep() < 1e-6) { break; }
-			if (err / static_cast<double>(n) < 1e-5) { break; }
+			if (err / static_cast<double>(R.n) < 1e-5) { break; }
 			if (maxBeta() < 1e-6) { break; }
 		}
 	}
 	// squared correlation on the model of the last accepted parameters (GaussianFit.cpp:274-295)
 	m.Make(p, fp.sigmaX, fp.theta);
 	double muD = 0.0, muM = 0.0;
-	for (int k = 0; k < n; ++k) {
-		double X, Y;
-		muD += pix(k, X, Y);
+	for (int c0 = 0; c0 < R.n; c0 += 32) {
+		const int k = c0 + lane;
+		double v = 0.0;
+		if (k < R.n) {
+			double X, Y;
+			v = R.Pix(k, X, Y);
+		}
+		muD = ChunkedOrderedSum(S, v, min(32, R.n - c0), muD);
 	}
-	for (int k = 0; k < n; ++k) {
-		double X, Y;
-		pix(k, X, Y);
-		muM += m.template Eval<false>(X - p[2], Y - p[3], nullptr);
+	for (int c0 = 0; c0 < R.n; c0 += 32) {
+		const int k = c0 + lane;
+		double hv = 0.0;
+		if (k < R.n) {
+			double X, Y;
+			R.Pix(k, X, Y);
+			hv = m.template Eval<false>(X - p[2], Y - p[3], nullptr);
+		}
+		muM = ChunkedOrderedSum(S, hv, min(32, R.n - c0), muM);
 	}
-	muD /= static_cast<double>(n);
-	muM /= static_cast<double>(n);
+	muD /= static_cast<double>(R.n);
+	muM /= static_cast<double>(R.n);
 	double t1 = 0.0, t2 = 0.0, t3 = 0.0;
-	for (int k = 0; k < n; ++k) {
-		double X, Y;
-		const double d = pix(k, X, Y) - muD;
-		t1 += d * (m.template Eval<false>(X - p[2], Y - p[3], nullptr) - muM);
+	for (int c0 = 0; c0 < R.n; c0 += 32) {
+		const int k = c0 + lane;
+		double a = 0.0, b = 0.0, c = 0.0;
+		if (k < R.n) {
+			double X, Y;
+			const double d = R.Pix(k, X, Y) - muD;
+			const double hm = m.template Eval<false>(X - p[2], Y - p[3], nullptr) - muM;
+			a = d * hm;
+			b = d * d;
+			c = hm * hm;
+		}
+		const int cnt = min(32, R.n - c0);
+		S.terms[0][lane] = a;
+		S.terms[1][lane] = b;
+		S.terms[2][lane] = c;
+		__syncwarp();
+		if (lane < 3) {
+			double acc = lane == 0 ? t1 : lane == 1 ? t2 : t3;
+			for (int j = 0; j < cnt; ++j) { acc += S.terms[lane][j]; }
+			S.acc[lane] = acc;
+		}
+		__syncwarp();
+		t1 = S.acc[0];
+		t2 = S.acc[1];
+		t3 = S.acc[2];
+		__syncwarp();
 	}
-	for (int k = 0; k < n; ++k) {
-		double X, Y;
-		const double d = pix(k, X, Y) - muD;
-		t2 += d * d;
-	}
-	for (int k = 0; k < n; ++k) {
-		double X, Y;
-		pix(k, X, Y);
-		const double hm = m.template Eval<false>(X - p[2], Y - p[3], nullptr) - muM;
-		t3 += hm * hm;
-	}
-	const double R = t1 / sqrt(t2 * t3);
-	const double rr = isnan(R) ? 0 : R * R;
+	const double Rr = t1 / sqrt(t2 * t3);
+	const double rr = isnan(Rr) ? 0 : Rr * Rr;
 	if (rr < kEps) { sentinel(p[2], p[3]); return; }
 	double sx = fp.sigmaX, sy = fp.sigmaY, th = fp.theta;
 	if constexpr (MODE == kG2Fixed) { sx = sy = fp.sigmaX; th = 0; }
 	if constexpr (MODE == kG2Sigma) { sx = p[4]; sy = sx; th = 0; }
 	if constexpr (MODE == kG3Fixed || MODE == kG3Theta) { sx = p[4] / r2; sy = p[5] / r2; }
 	if constexpr (MODE == kG3Theta) { th = p[6]; }
-	Store(row, MODE, cd, p[2], p[3], p[0], p[1], sx, sy, th, rr);
+	StoreRow(row, cd, p[2], p[3], p[0], p[1], sx, sy, th, rr);
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(64) ExactFitKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
-                                                     const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
-                                                     FitParams fp, double* rows, const uint8_t* only)
+__global__ void __launch_bounds__(32 * kWarps) ExactFitKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
+                                                              const Cand* __restrict__ cands, const uint32_t* nptr,
+                                                              uint32_t nconst, FitParams fp, double* rows, const uint8_t* only)
 {
+	__shared__ WarpSmem smem[kWarps];
+	WarpSmem& S = smem[threadIdx.x >> 5];
 	const uint32_t n = nptr ? *nptr : nconst;
-	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+	for (uint32_t k = warp; k < n; k += nw) {
 		if (only && !only[k]) { continue; }
 		const Cand cd = cands[k];
-		FitExact<MODE>(img + static_cast<long long>(cd.frame) * N, H, W, fp, cd, rows + static_cast<long long>(k) * kCols);
+		FitWarp<MODE>(S, img + static_cast<long long>(cd.frame) * N, H, W, fp, cd, rows + static_cast<long long>(k) * kCols);
 	}
 }
 
@@ -363,13 +519,12 @@ __global__ void __launch_bounds__(64) ExactFitKernel(const uint16_t* __restrict_
 bool LaunchExactFit(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
                     uint32_t cap, const FitParams& fp, double* rows, const uint8_t* only, cudaStream_t st)
 {
-	const int threads = 64;
-	const uint32_t blocks = std::min<uint32_t>((std::max<uint32_t>(cap, 1) + threads - 1) / threads, 148u * 32u);
+	const uint32_t blocks = std::min<uint32_t>((std::max<uint32_t>(cap, 1) + kWarps - 1) / kWarps, 148u * 16u);
 	switch (fp.mode) {
-		case kG2Fixed: ExactFitKernel<kG2Fixed><<<blocks, threads, 0, st>>>(img, H, W, N, cands, nptr, nconst, fp, rows, only); break;
-		case kG2Sigma: ExactFitKernel<kG2Sigma><<<blocks, threads, 0, st>>>(img, H, W, N, cands, nptr, nconst, fp, rows, only); break;
-		case kG3Fixed: ExactFitKernel<kG3Fixed><<<blocks, threads, 0, st>>>(img, H, W, N, cands, nptr, nconst, fp, rows, only); break;
-		case kG3Theta: ExactFitKernel<kG3Theta><<<blocks, threads, 0, st>>>(img, H, W, N, cands, nptr, nconst, fp, rows, only); break;
+		case kG2Fixed: ExactFitKernel<kG2Fixed><<<blocks, 32 * kWarps, 0, st>>>(img, H, W, N, cands, nptr, nconst, fp, rows, only); break;
+		case kG2Sigma: ExactFitKernel<kG2Sigma><<<blocks, 32 * kWarps, 0, st>>>(img, H, W, N, cands, nptr, nconst, fp, rows, only); break;
+		case kG3Fixed: ExactFitKernel<kG3Fixed><<<blocks, 32 * kWarps, 0, st>>>(img, H, W, N, cands, nptr, nconst, fp, rows, only); break;
+		case kG3Theta: ExactFitKernel<kG3Theta><<<blocks, 32 * kWarps, 0, st>>>(img, H, W, N, cands, nptr, nconst, fp, rows, only); break;
 		default: return false;
 	}
 	CountLaunch();

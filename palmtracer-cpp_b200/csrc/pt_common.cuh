@@ -25,7 +25,8 @@ enum Col : int {
 };
 
 // Fit modes (lib/fit/Fitting.hpp:22-30)
-enum FitMode : int { kNone = 0, kG2Fixed = 1, kG2Sigma = 2, kG3Fixed = 3, kG3Theta = 4, kSplineEmccd = 5 };
+enum FitMode : int { kNone = 0, kG2Fixed = 1, kG2Sigma = 2, kG3Fixed = 3, kG3Theta = 4, kSplineEmccd = 5,
+                     kMleGauss = 6, kMleAstig = 7, kMleSpline = 8 };
 
 // Per-pixel code byte written by the detection kernel.
 constexpr uint8_t kDomain = 1;  // thresholded potential > 1e-8: the watershed floods it
@@ -70,6 +71,17 @@ struct Cand {
 	int pad;
 };
 
+// Maximum-likelihood modes 6-8 (fit_params layouts in include/palmtracer_b200.h).
+struct MleParams {
+	int model, roi, half, n, maxIter;
+	double sigma0, offset, gain, crlbMax, pixelSize, zMin, zMax;
+	double astig[10];
+	int sx, sy, sz;
+	double dz;
+	const float* table;        // mode 8: cell-major [cell][64], FP32
+	unsigned int* fallbacks;   // FP64 Cholesky re-factorisations (diagnostics)
+};
+
 // Fit configuration passed by value to the fit kernels.
 struct FitParams {
 	int mode;        // FitMode
@@ -83,7 +95,9 @@ struct FitParams {
 	long long splineSize;  // sx * sy * sz
 	long long offsetXY;
 	double roiParam, initZ, deltaZ, intensityRatio;
-	const double* coeffs;  // device, SoA [64][sz][sy][sx]
+	const double* coeffs;  // device, cell-major [cell][64]
+	MleParams mle;         // modes 6-8
+	int lanes;             // ROI lane-group width for modes 6-8 (autotuned)
 };
 
 // Geometry of one chunk: B frames of H x W pixels; global pixel index g = f * N + y * W + x (fits in 31 bits).

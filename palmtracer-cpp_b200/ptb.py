@@ -15,7 +15,7 @@ COLS = 18
 # every symbol the public header declares
 EXPORTS = ["Localization", "Fitting", "Wavelett", "AutoThreshold", "PTB_LocalizationDevice",
            "PTB_SetSegmentationMode", "PTB_SetFitPrecision", "PTB_LastError", "PTB_KernelLaunchCount",
-           "PTB_SetProfiling", "PTB_StageTimes"]
+           "PTB_SetProfiling", "PTB_StageTimes", "PTB_MeasureFmaPeak"]
 
 _u16p = ctypes.POINTER(ctypes.c_uint16)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -56,6 +56,8 @@ def load(path=LIB_PATH):
     L.PTB_SetProfiling.argtypes = [ctypes.c_int]
     L.PTB_StageTimes.restype = None
     L.PTB_StageTimes.argtypes = [_f64p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
+    L.PTB_MeasureFmaPeak.restype = _f64
+    L.PTB_MeasureFmaPeak.argtypes = [ctypes.c_int]
     _lib = L
     return L
 
@@ -158,3 +160,8 @@ def stage_times():
     launches = np.zeros(5, dtype=np.uint64)
     load().PTB_StageTimes(ms.ctypes.data_as(_f64p), launches.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 5)
     return {k: (float(ms[i]), int(launches[i])) for i, k in enumerate(STAGES)}
+
+
+def fma_peak(fp64):
+    """Measured FMA FLOP/s of the current device (FP64 when fp64 is true, else FP32)."""
+    return load().PTB_MeasureFmaPeak(int(bool(fp64)))
