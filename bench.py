@@ -121,6 +121,7 @@ def cpu_reference_rate(frames_host, thr, seconds=10.0, threads=None):
 
 
 def main():
+    global FIT_MODE, FIT_PARAMS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -146,7 +147,6 @@ def main():
     import ptb
 
     ptb.set_fit_precision(args.precision)
-    global FIT_MODE, FIT_PARAMS
     if args.fit is not None:
         FIT_MODE = args.fit
         FIT_PARAMS = PARAMS_BY_MODE[FIT_MODE]

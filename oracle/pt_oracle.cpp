@@ -933,7 +933,7 @@ void FitSplineFull(const SplineTable& t, double roiParam, const uint16_t* img, i
 // the order [z0, w, c3, c4, A]). Mode 8: PSF = the cubic-spline table of SplineFit (monomial weights per cell), with
 // the PSF centre at table coordinates ((sx - 1) / 2, (sy - 1) / 2) and z_nm = deltaZ * (Z - sz / 2).
 // Objective: Poisson deviance D = 2 sum(mu - d - d ln(mu / d)); damped Fisher scoring (Levenberg-Marquardt with
-// H = 2 sum mu^-1 dmu dmu^T); then up to two undamped Fisher steps in FP64 and the CRLB sqrt(diag(F^-1)).
+// H = 2 sum mu^-1 dmu dmu^T); then undamped FP64 Fisher steps to a 1e-10 relative step and the CRLB sqrt(diag(F^-1)).
 namespace {
 
 struct MleCfg {
@@ -1198,18 +1198,27 @@ bool MleFit(const MleRoi& R, double t[5], double crlb[5], double& dev)
 			if (lambda > 1e7) { break; }
 		}
 	}
-	// undamped Fisher scoring polish in FP64 (two steps)
-	for (int it = 0; it < 2; ++it) {
+	// undamped Fisher scoring in FP64 until the step is below 1e-10 (relative, at most 10 steps); a step that does not
+	// lower the deviance is halved up to three times
+	for (int it = 0; it < 10; ++it) {
 		double rhs[5], dt[5], tt[5];
 		for (int a = 0; a < 5; ++a) { rhs[a] = -G[a]; }
 		if (!CholSolve5(Hm, rhs, dt)) { break; }
-		for (int a = 0; a < 5; ++a) { tt[a] = std::min(std::max(t[a] + dt[a], lo[a]), hi[a]); }
-		double Gt[5], Ht[25];
-		const double Dt = R.Normal(tt, Gt, Ht);
-		if (!(std::isfinite(Dt) && Dt <= D)) { break; }
+		bool accepted = false;
+		double Gt[5], Ht[25], Dt = 0;
+		for (int half = 0; half < 4 && !accepted; ++half) {
+			for (int a = 0; a < 5; ++a) { tt[a] = std::min(std::max(t[a] + dt[a], lo[a]), hi[a]); }
+			Dt = R.Normal(tt, Gt, Ht);
+			if (std::isfinite(Dt) && Dt <= D) { accepted = true; }
+			else { for (int a = 0; a < 5; ++a) { dt[a] *= 0.5; } }
+		}
+		if (!accepted) { break; }
+		double step = 0;
+		for (int a = 0; a < 5; ++a) { step = std::max(step, std::abs(tt[a] - t[a]) / std::max(std::abs(t[a]), 1.0)); }
 		for (int a = 0; a < 5; ++a) { t[a] = tt[a]; G[a] = Gt[a]; }
 		for (int a = 0; a < 25; ++a) { Hm[a] = Ht[a]; }
 		D = Dt;
+		if (step < 1e-10) { break; }
 	}
 	// CRLB: Fisher information F = H / 2; variances are the diagonal of its inverse
 	for (int a = 0; a < 5; ++a) {

@@ -1,8 +1,8 @@
 // Poisson maximum-likelihood fits (modes 6 Gaussian, 7 astigmatic 3D, 8 cubic-spline 3D) of (bg, I, x, y, s),
 // s = sigma (mode 6), z in nm (mode 7) or the spline's z coordinate (mode 8). No counterpart in the reference; the
 // model maths, the algorithm and the FP64 oracle are in oracle/pt_oracle.cpp (MleFit), which this file follows step
-// for step: initial values, bounds, axial pre-scan, damped Fisher-scoring LM on the Poisson deviance, two undamped
-// FP64 Fisher steps and the CRLB from the FP64 Fisher information.
+// for step: initial values, bounds, FP64 axial pre-scan, damped Fisher-scoring LM on the Poisson deviance, undamped
+// FP64 Fisher steps to a 1e-10 relative step and the CRLB from the FP64 Fisher information.
 //
 // Precision: the LM iterations run in FP32. The 5x5 damped system is factored by an FP32 Cholesky; when a pivot is not
 // positive or the pivot ratio min(L_ii^2) / max(A_ii) falls below 1e-5 the same system is re-factored in FP64. The
@@ -324,14 +324,16 @@ __global__ void __launch_bounds__(kThreads) MleKernel(const uint16_t* __restrict
 		th[3] = float(y0);
 		if (MODEL == 6) { th[4] = float(mp.sigma0); }
 		else {
+			// axial pre-scan in FP64, as in the oracle, so that both start from the same basin
 			const int ns = MODEL == 7 ? 16 : 8;
-			float best = 3e38f, bz = float(0.5 * (lo[4] + hi[4]));
+			double tsd[5] = {double(th[0]), double(th[1]), double(th[2]), double(th[3]), 0.0};
+			double best = 1e300, bz = 0.5 * (lo[4] + hi[4]);
 			for (int s = 0; s < ns; ++s) {
-				th[4] = float(lo[4] + (hi[4] - lo[4]) * (s + 0.5) / ns);
-				const float D = Normal<float, MODEL, L, false>(mp, base, W, th, nullptr, nullptr, grp);
-				if (D < best) { best = D; bz = th[4]; }
+				tsd[4] = lo[4] + (hi[4] - lo[4]) * (s + 0.5) / ns;
+				const double D = Normal<double, MODEL, L, false>(mp, base, W, tsd, nullptr, nullptr, grp);
+				if (D < best) { best = D; bz = tsd[4]; }
 			}
-			th[4] = bz;
+			th[4] = float(bz);
 		}
 		#pragma unroll
 		for (int a = 0; a < 5; ++a) { th[a] = fminf(fmaxf(th[a], float(lo[a])), float(hi[a])); }
@@ -382,27 +384,40 @@ __global__ void __launch_bounds__(kThreads) MleKernel(const uint16_t* __restrict
 				if (lambda > 1e7f) { break; }
 			}
 		}
-		// FP64: two undamped Fisher steps, then the CRLB
+		// FP64: undamped Fisher steps to a 1e-10 relative step (at most 10, halving a step that does not lower the
+		// deviance up to three times), then the CRLB
 		#pragma unroll
 		for (int a = 0; a < 5; ++a) { t[a] = th[a]; }
 		double Gd[5], Hd[15];
 		double Dd = Normal<double, MODEL, L, true>(mp, base, W, t, Gd, Hd, grp);
 		ok = ok && isfinite(Dd);
-		for (int it = 0; ok && it < 2; ++it) {
+		for (int it = 0; ok && it < 10; ++it) {
 			double rhs[5], dt[5], tt[5];
 			#pragma unroll
 			for (int a = 0; a < 5; ++a) { rhs[a] = -Gd[a]; }
 			if (!Chol5<double>(Hd, 1.0, rhs, dt, nullptr)) { break; }
+			bool accepted = false;
+			double Gt[5], Ht[15], Dt = 0;
+			for (int hv = 0; hv < 4 && !accepted; ++hv) {
+				#pragma unroll
+				for (int a = 0; a < 5; ++a) { tt[a] = fmin(fmax(t[a] + dt[a], lo[a]), hi[a]); }
+				Dt = Normal<double, MODEL, L, true>(mp, base, W, tt, Gt, Ht, grp);
+				if (isfinite(Dt) && Dt <= Dd) { accepted = true; }
+				else {
+					#pragma unroll
+					for (int a = 0; a < 5; ++a) { dt[a] *= 0.5; }
+				}
+			}
+			if (!accepted) { break; }
+			double step = 0;
 			#pragma unroll
-			for (int a = 0; a < 5; ++a) { tt[a] = fmin(fmax(t[a] + dt[a], lo[a]), hi[a]); }
-			double Gt[5], Ht[15];
-			const double Dt = Normal<double, MODEL, L, true>(mp, base, W, tt, Gt, Ht, grp);
-			if (!(isfinite(Dt) && Dt <= Dd)) { break; }
+			for (int a = 0; a < 5; ++a) { step = fmax(step, fabs(tt[a] - t[a]) / fmax(fabs(t[a]), 1.0)); }
 			#pragma unroll
 			for (int a = 0; a < 5; ++a) { t[a] = tt[a]; Gd[a] = Gt[a]; }
 			#pragma unroll
 			for (int a = 0; a < 15; ++a) { Hd[a] = Ht[a]; }
 			Dd = Dt;
+			if (step < 1e-10) { break; }
 		}
 		if (ok) {
 			double F[15];
