@@ -1,8 +1,13 @@
-"""Benchmark: localizations/s of the detect + fit hot path on the 2000 x 1024 x 1024 uint16 workload.
+"""Benchmark: localizations/s of the detect + MLE fit hot path on the 2000 x 1024 x 1024 uint16 workload.
 
-One step = one Localization pass (wavelet -> threshold -> watershed -> per-ROI LM fit -> per-plane ordering) over the
-whole synthetic stack. ``value`` is measured on device-resident frames through PTB_LocalizationDevice; ``e2e`` is
-the reference-facing C ABI (Localization) with host buffers, host<->device copies inside the timed region.
+One step = one Localization pass (wavelet -> threshold -> watershed -> per-ROI Poisson-MLE LM fit (mode 6: x, y,
+sigma, photons, background) -> per-plane ordering) over the whole synthetic stack. ``value`` is measured on
+device-resident frames through PTB_LocalizationDevice; ``e2e`` is the reference-facing C ABI (Localization) with
+host buffers, host<->device copies inside the timed region.
+
+The reference has no maximum-likelihood fit; its CPU arm (``--impl reference`` and ``cpu_baseline``) runs the
+reference's own Localization with its 5-parameter Gaussian least-squares fit (fit mode 2: x, y, sigma, amplitude,
+offset), the closest counterpart of the path, built from its sources (oracle/_ref).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--frames Z]
 
@@ -27,12 +32,19 @@ sys.path.insert(0, ROOT)
 METRIC = "localizations/s (detect+MLE fit) at FP64-matched error; p50/p99 stack latency"
 UNIT = "localizations/s"
 WORKLOAD = "c2"
-FIT_MODE = 2
-FIT_PARAMS = np.array([7.0, 1.3, 1.3, 0.0])
-# fit_params per mode for the 7x7 workload: reference Gaussian modes and the Poisson-MLE Gaussian (roi, sigma0,
-# camera offset ADU, gain ADU/photon, max iterations, CRLB filter (0 = off))
-PARAMS_BY_MODE = {1: FIT_PARAMS, 2: FIT_PARAMS, 3: FIT_PARAMS, 4: FIT_PARAMS, 0: FIT_PARAMS,
+GAUSS_PARAMS = np.array([7.0, 1.3, 1.3, 0.0])
+# fit_params per mode for the 7x7 workload: reference Gaussian least-squares modes (roi, sigma x, sigma y, theta) and
+# the Poisson-MLE Gaussian (roi, sigma0, camera offset ADU, gain ADU/photon, max iterations, CRLB filter (0 = off))
+PARAMS_BY_MODE = {0: GAUSS_PARAMS, 1: GAUSS_PARAMS, 2: GAUSS_PARAMS, 3: GAUSS_PARAMS, 4: GAUSS_PARAMS,
                   6: np.array([7.0, 1.3, 100.0, 2.0, 20.0, 0.0])}
+FIT_MODE = 6
+FIT_PARAMS = PARAMS_BY_MODE[FIT_MODE]
+REF_FIT_MODE = 2  # the reference's own 5-parameter Gaussian fit, for the CPU arm
+# Algorithmic FP32 FLOPs of one pixel of one LM evaluation of the mode-6 model (deviance, gradient, Fisher matrix):
+# separable PSF and its 3 derivatives 8, mu and deviance 10, gradient terms 7, gradient 10, Fisher matrix 35
+# (an FMA counts 2; a division, logarithm or reciprocal 1). Per-evaluation erf tables and the 5x5 solve are not
+# counted.
+FLOP_PER_PIXEL_LM = 71
 RATIO = 0.0
 PER_PLANE = 8192
 
@@ -107,16 +119,18 @@ def cpu_reference_rate(frames_host, thr, seconds=10.0, threads=None):
     z = frames_host.shape[0]
     n0 = min(z, max(4, cores))
     t0 = time.perf_counter()
-    rows = lib.localization(frames_host[:n0], thr, RATIO, FIT_MODE, FIT_PARAMS, capacity_doubles=PER_PLANE * n0 * 18)
+    rows = lib.localization(frames_host[:n0], thr, RATIO, REF_FIT_MODE, GAUSS_PARAMS, capacity_doubles=PER_PLANE * n0 * 18)
     dt0 = time.perf_counter() - t0
     n1 = int(min(z, max(n0, n0 * seconds / max(dt0, 1e-3))))
     if n1 > n0:
         t0 = time.perf_counter()
-        rows = lib.localization(frames_host[:n1], thr, RATIO, FIT_MODE, FIT_PARAMS, capacity_doubles=PER_PLANE * n1 * 18)
+        rows = lib.localization(frames_host[:n1], thr, RATIO, REF_FIT_MODE, GAUSS_PARAMS, capacity_doubles=PER_PLANE * n1 * 18)
         dt0 = time.perf_counter() - t0
     else:
         n1 = n0
-    return rows.shape[0] / dt0, {"kind": kind, "cores": cores, "sample": "%d of the %d frames, fit mode %d" % (n1, z, FIT_MODE),
+    return rows.shape[0] / dt0, {"kind": kind, "cores": cores,
+                                 "sample": "%d of the %d frames, the reference's Localization with its fit mode %d "
+                                           "(Gaussian least squares; the reference has no MLE fit)" % (n1, z, REF_FIT_MODE),
                                  "frames": n1, "seconds": dt0, "rows": int(rows.shape[0])}
 
 
@@ -229,22 +243,36 @@ def main():
         rows_all = float(rows)
     value = rows_all * args.steps / (total_ms / 1000.0)
 
-    # stage breakdown of one more (untimed) pass
+    # stage breakdown of one more (untimed) pass, with the MLE phases timed by CUDA events on the library's stream
     ptb.set_profiling(1)
     ptb.stage_times()
+    ptb.mle_evaluations()
     step()
     torch.cuda.synchronize()
     stages = ptb.stage_times()
+    evals = ptb.mle_evaluations()
     ptb.set_profiling(0)
     peak, peak_kind = peaks()
     det_ms, det_l = stages["detect"]
     det_bytes = 2.0 * h * w * frames
-    achieved = det_bytes / (det_ms / 1000.0) / 1e9 if det_ms > 0 else None
-    roofline = {"kernel": "DetectKernel (wavelet + threshold + seeds)", "bound": "hbm", "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
-                "algorithmic_bytes_per_launch": det_bytes / max(det_l, 1), "launches": det_l,
-                "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                "stage_ms": {k: round(v[0], 3) for k, v in stages.items()}}
+    det_achieved = det_bytes / (det_ms / 1000.0) / 1e9 if det_ms > 0 else None
+    detect_roofline = {"kernel": "DetectKernel (wavelet + threshold + seeds)", "bound": "hbm", "achieved": det_achieved,
+                       "peak": peak, "unit": "GB/s", "frac": (det_achieved / peak) if det_achieved else None,
+                       "algorithmic_bytes_per_launch": det_bytes / max(det_l, 1), "launches": det_l,
+                       "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind}
+    roofline = detect_roofline
+    if FIT_MODE == 6 and stages["fit_lm"][0] > 0:
+        fp32_peak = ptb.fma_peak(False) / 1e12
+        lm_ms = stages["fit_lm"][0]
+        flops = FLOP_PER_PIXEL_LM * 49 * evals["lm"]
+        achieved = flops / (lm_ms / 1000.0) / 1e12
+        roofline = {"kernel": "MleLmKernel<6> (persistent FP32 LM, thread per ROI)", "bound": "fp32", "achieved": achieved,
+                    "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                    "algorithmic_flops_per_launch": flops / max(1, stages["fit_lm"][1]), "launches": stages["fit_lm"][1],
+                    "flop_per_pixel_evaluation": FLOP_PER_PIXEL_LM, "evaluations": evals,
+                    "peak_source": "measured in this run (PTB_MeasureFmaPeak FP32 FMA chains)"}
+    roofline["stage_ms"] = {k: round(v[0], 3) for k, v in stages.items()}
+    roofline["stage_launches"] = {k: v[1] for k, v in stages.items()}
 
     # end to end through the reference-facing C ABI with host buffers
     host_in = torch.empty((frames, h, w), dtype=torch.int16, pin_memory=True)
@@ -271,11 +299,14 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64" if args.precision != 1 else "f32 (f64 re-fit)", "data": "synthetic (seeded, generated on the GPU; no public dataset)",
+                "dtype": ("f32 (LM and Newton polish; f64 Cholesky fallback, axial pre-scan, likelihood, CRLB)" if FIT_MODE >= 6 else
+                          "f64" if args.precision != 1 else "f32 (f64 re-fit)"),
+                "data": "synthetic (seeded, generated on the GPU; no public dataset)",
                 "config": dict(config, fit_precision=args.precision),
                 "frames_per_s": frames * world * args.steps / (total_ms / 1000.0),
                 "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
-                "localizations_per_step": int(rows_all), "roofline": roofline, "cpu_baseline": cpu,
+                "localizations_per_step": int(rows_all), "roofline": roofline, "detect_roofline": detect_roofline,
+                "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host_np.nbytes),
                         "d2h_bytes_per_step": int(n_e2e * 8), "ms_per_step": float(np.mean(e2e_ms)) if e2e_ms else None},
                 "gpu_launches": int(launches), "clocks": clk}

@@ -86,14 +86,22 @@ PTB_API uint64_t PTB_KernelLaunchCount(void);
 
 /* Stage timing (diagnostics). When enabled, every chunk records CUDA events on the library's stream around its
  * stages and accumulates device milliseconds per stage: [0] detection kernel, [1] segmentation chain, [2] fit
- * kernels, [3] ordering and numbering, [4] host<->device copies. PTB_StageTimes copies up to n totals into ms and
- * the matching launch counts into launches (either may be NULL), then resets them. Returns the previous setting. */
+ * kernels, [3] ordering and numbering, [4] host<->device copies, and for fit modes 6-8 the fit's phases: [5]
+ * initial values, [6] Levenberg-Marquardt iterations, [7] Newton polish, FP64 likelihood and CRLB (the warp-per-ROI
+ * mapping runs as one launch, counted in [6]). PTB_StageTimes copies up to n totals into ms and the matching launch
+ * counts into launches (either may be NULL), then resets them. Returns the previous setting. */
 PTB_API int PTB_SetProfiling(int enable);
+PTB_API void PTB_StageTimes(double* ms, uint64_t* launches, int n);
+
+/* Model evaluations of fit modes 6-8 counted while profiling is enabled (diagnostics): [0] FP32 evaluations of the
+ * Levenberg-Marquardt iterations, [1] FP32 evaluations of the Newton polish, [2] FP64 evaluations (axial pre-scan,
+ * final likelihood and Fisher information). One evaluation visits every pixel of one ROI. Copies up to n totals
+ * into counts, then resets them. */
+PTB_API void PTB_MleEvaluations(uint64_t* counts, int n);
 
 /* FMA throughput probe of the current device (diagnostics): FLOP/s (2 per FMA) of FP64 (fp64 != 0) or FP32
  * arithmetic, timed with CUDA events over a grid of independent FMA chains; -1 on error. */
 PTB_API double PTB_MeasureFmaPeak(int fp64);
-PTB_API void PTB_StageTimes(double* ms, uint64_t* launches, int n);
 
 #ifdef __cplusplus
 }

@@ -142,6 +142,33 @@ class OracleLib(CpuLib):
         self._labels(_ptr(frame, _u16p), h, w, thr, ratio, _ptr(out, _u32p))
         return out
 
+    def mle_evaluate(self, frame, cx, cy, fit, params, theta):
+        """FP64 deviance, gradient and exact Hessian of the maximum-likelihood objective at theta (local to the ROI
+        centre floor(cx), floor(cy)); None when the ROI crosses the border."""
+        frame = np.ascontiguousarray(frame, dtype=np.uint16)
+        params = np.ascontiguousarray(params, dtype=np.float64)
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        d, g, h = np.zeros(1), np.zeros(5), np.zeros(25)
+        f = self.lib.orc_MleEvaluate
+        f.restype = ctypes.c_int
+        f.argtypes = [_u16p, _u64, _u64, _f64, _f64, _u64, _f64p, _f64p, _f64p, _f64p, _f64p]
+        if not f(_ptr(frame, _u16p), frame.shape[0], frame.shape[1], cx, cy, fit, _ptr(params, _f64p), _ptr(theta, _f64p),
+                 _ptr(d, _f64p), _ptr(g, _f64p), _ptr(h, _f64p)):
+            return None
+        return float(d[0]), g, h.reshape(5, 5)
+
+    def mle_fit_one(self, frame, cx, cy, fit, params):
+        """(status, theta, crlb, deviance) of one candidate's fit: status 1 success, 2 failed, 0 border."""
+        frame = np.ascontiguousarray(frame, dtype=np.uint16)
+        params = np.ascontiguousarray(params, dtype=np.float64)
+        t, c, d = np.zeros(5), np.zeros(5), np.zeros(1)
+        f = self.lib.orc_MleFitOne
+        f.restype = ctypes.c_int
+        f.argtypes = [_u16p, _u64, _u64, _f64, _f64, _u64, _f64p, _f64p, _f64p, _f64p]
+        st = f(_ptr(frame, _u16p), frame.shape[0], frame.shape[1], cx, cy, fit, _ptr(params, _f64p), _ptr(t, _f64p),
+               _ptr(c, _f64p), _ptr(d, _f64p))
+        return st, t, c, float(d[0])
+
 
 class RefLib(CpuLib):
     def __init__(self, path=REF_SO):

@@ -933,7 +933,8 @@ void FitSplineFull(const SplineTable& t, double roiParam, const uint16_t* img, i
 // the order [z0, w, c3, c4, A]). Mode 8: PSF = the cubic-spline table of SplineFit (monomial weights per cell), with
 // the PSF centre at table coordinates ((sx - 1) / 2, (sy - 1) / 2) and z_nm = deltaZ * (Z - sz / 2).
 // Objective: Poisson deviance D = 2 sum(mu - d - d ln(mu / d)); damped Fisher scoring (Levenberg-Marquardt with
-// H = 2 sum mu^-1 dmu dmu^T); then undamped FP64 Fisher steps to a 1e-10 relative step and the CRLB sqrt(diag(F^-1)).
+// H = 2 sum mu^-1 dmu dmu^T) until the step is small; then FP64 Newton steps on the exact Hessian of the deviance to
+// a 1e-10 relative step, both holding parameters on active bounds (FixActive); the CRLB sqrt(diag(F^-1)) from the FP64 Fisher information F = sum mu^-1 dmu dmu^T.
 namespace {
 
 struct MleCfg {
@@ -970,8 +971,10 @@ bool ParseMle(int mode, const double* fp, MleCfg& c)
 	return roi >= 1 && c.gain > 0;
 }
 
-// Pixel-integrated 1D Gaussian and its derivatives with respect to the emitter position and the width.
-void Erf1D(double c, double x, double s, double& e, double& dx, double& ds)
+// Pixel-integrated 1D Gaussian E(x, s) = (erf(b) - erf(a)) / 2, a = (c - x - 1/2) / (sqrt2 s), b = (c - x + 1/2) /
+// (sqrt2 s), with its first derivatives (position, width) and, when d2 is given, the second derivatives
+// d2 = {E_xx, E_xs, E_ss}.
+void Erf1D(double c, double x, double s, double& e, double& dx, double& ds, double* d2 = nullptr)
 {
 	const double k = 1.0 / (1.4142135623730951 * s);
 	const double a = (c - x - 0.5) * k, b = (c - x + 0.5) * k;
@@ -979,22 +982,31 @@ void Erf1D(double c, double x, double s, double& e, double& dx, double& ds)
 	e = 0.5 * (std::erf(b) - std::erf(a));
 	dx = (ea - eb) / (2.5066282746310002 * s);
 	ds = (a * ea - b * eb) / (1.7724538509055160 * s);
+	if (d2) {
+		d2[0] = (a * ea - b * eb) / (1.7724538509055160 * s * s);
+		d2[1] = (2 * a * a * ea - 2 * b * b * eb - ea + eb) / (2.5066282746310002 * s * s);
+		d2[2] = 2 * (a * (a * a - 1) * ea - b * (b * b - 1) * eb) / (1.7724538509055160 * s * s);
+	}
 }
 
-// Astigmatic width (pixels) and d width / dz for one axis [z0, w, c3, c4, A].
-void AstigSigma(const double* m, double pixelSize, double z, double& s, double& ds)
+// Astigmatic width (pixels), d width / dz and d2 width / dz2 for one axis [z0, w, c3, c4, A].
+void AstigSigma(const double* m, double pixelSize, double z, double& s, double& ds, double* dss = nullptr)
 {
 	const double u = (z - m[0]) / m[1];
 	const double poly = 1.0 + u * u + m[2] * u * u * u + m[3] * u * u * u * u;
 	const double k = m[4] / pixelSize;
-	if (poly <= 1e-12) { s = k * 1e-6; ds = 0; return; }
+	if (poly <= 1e-12) { s = k * 1e-6; ds = 0; if (dss) { *dss = 0; } return; }
 	const double r = std::sqrt(poly);
+	const double p1 = 2 * u + 3 * m[2] * u * u + 4 * m[3] * u * u * u;
+	const double p2 = 2 + 6 * m[2] * u + 12 * m[3] * u * u;
 	s = k * r;
-	ds = k * (2 * u + 3 * m[2] * u * u + 4 * m[3] * u * u * u) / (2 * r * m[1]);
+	ds = k * p1 / (2 * r * m[1]);
+	if (dss) { *dss = k / (m[1] * m[1]) * (p2 / (2 * r) - p1 * p1 / (4 * r * poly)); }
 }
 
-// Spline PSF value and gradient at table coordinates (X, Y, Z).
-double SplinePsf(const MleCfg& c, double X, double Y, double Z, double& dX, double& dY, double& dZ)
+// Spline PSF value and gradient at table coordinates (X, Y, Z); with h2 the second derivatives
+// {S_XX, S_XY, S_XZ, S_YY, S_YZ, S_ZZ}.
+double SplinePsf(const MleCfg& c, double X, double Y, double Z, double& dX, double& dY, double& dZ, double* h2 = nullptr)
 {
 	auto cell = [](double v, int dim, double& frac) {
 		int i = static_cast<int>(std::floor(v));
@@ -1007,8 +1019,10 @@ double SplinePsf(const MleCfg& c, double X, double Y, double Z, double& dX, doub
 	const size_t pos = (static_cast<size_t>(iz) * c.sy + iy) * c.sx + ix;
 	double px[4] = {1, fx, fx * fx, fx * fx * fx}, py[4] = {1, fy, fy * fy, fy * fy * fy}, pz[4] = {1, fz, fz * fz, fz * fz * fz};
 	double dpx[4] = {0, 1, 2 * fx, 3 * fx * fx}, dpy[4] = {0, 1, 2 * fy, 3 * fy * fy}, dpz[4] = {0, 1, 2 * fz, 3 * fz * fz};
+	const double ddpx[4] = {0, 0, 2, 6 * fx}, ddpy[4] = {0, 0, 2, 6 * fy}, ddpz[4] = {0, 0, 2, 6 * fz};
 	double v = 0;
 	dX = dY = dZ = 0;
+	if (h2) { for (int q = 0; q < 6; ++q) { h2[q] = 0; } }
 	for (int i = 0; i < 4; ++i) {
 		for (int j = 0; j < 4; ++j) {
 			for (int m = 0; m < 4; ++m) {
@@ -1017,6 +1031,14 @@ double SplinePsf(const MleCfg& c, double X, double Y, double Z, double& dX, doub
 				dX += co * pz[i] * py[j] * dpx[m];
 				dY += co * pz[i] * dpy[j] * px[m];
 				dZ += co * dpz[i] * py[j] * px[m];
+				if (h2) {
+					h2[0] += co * pz[i] * py[j] * ddpx[m];
+					h2[1] += co * pz[i] * dpy[j] * dpx[m];
+					h2[2] += co * dpz[i] * py[j] * dpx[m];
+					h2[3] += co * pz[i] * ddpy[j] * px[m];
+					h2[4] += co * dpz[i] * dpy[j] * px[m];
+					h2[5] += co * ddpz[i] * py[j] * px[m];
+				}
 			}
 		}
 	}
@@ -1028,33 +1050,59 @@ struct MleRoi {
 	std::vector<double> d;  // photons, row-major
 	double x0, y0;          // local candidate position
 
-	// mu and dmu/dtheta for theta = [bg, I, x, y, s]; returns false for a non-finite model.
-	void Eval(const double* t, std::vector<double>& mu, std::vector<double>& g) const
+	// mu, dmu/dtheta (g, 5 per pixel) and, when h is given, d2mu/dtheta2 (upper triangle, 15 per pixel) for
+	// theta = [bg, I, x, y, s].
+	void Eval(const double* t, std::vector<double>& mu, std::vector<double>& g, std::vector<double>* h = nullptr) const
 	{
 		const MleCfg& C = *c;
-		const int roi = C.roi, h = C.half;
+		const int roi = C.roi, hh = C.half;
 		mu.assign(C.n, 0);
 		g.assign(static_cast<size_t>(C.n) * 5, 0);
+		if (h) { h->assign(static_cast<size_t>(C.n) * 15, 0); }
+		auto put2 = [&](int k, double Pxx, double Pxy, double Pxs, double Pyy, double Pys, double Pss, double Px, double Py, double Ps) {
+			// d2mu: (I,x) = Px, (I,y) = Py, (I,s) = Ps, (x,x) = I Pxx, ... ; bg row and (I,I) are zero
+			double* q = h->data() + static_cast<size_t>(k) * 15;
+			const double I = t[1];
+			// packed order: (0,0..4) (1,1..4) (2,2..4) (3,3..4) (4,4)
+			q[0] = q[1] = q[2] = q[3] = q[4] = 0;
+			q[5] = 0; q[6] = Px; q[7] = Py; q[8] = Ps;
+			q[9] = I * Pxx; q[10] = I * Pxy; q[11] = I * Pxs;
+			q[12] = I * Pyy; q[13] = I * Pys;
+			q[14] = I * Pss;
+		};
 		if (C.model == 6 || C.model == 7) {
-			double sx = t[4], sy = t[4], dsx = 1, dsy = 1;
+			double sx = t[4], sy = t[4], dsx = 1, dsy = 1, ssx = 0, ssy = 0;
 			if (C.model == 7) {
-				AstigSigma(C.astig, C.pixelSize, t[4], sx, dsx);
-				AstigSigma(C.astig + 5, C.pixelSize, t[4], sy, dsy);
+				AstigSigma(C.astig, C.pixelSize, t[4], sx, dsx, &ssx);
+				AstigSigma(C.astig + 5, C.pixelSize, t[4], sy, dsy, &ssy);
 			}
-			std::vector<double> ex(roi), edx(roi), eds(roi), ey(roi), edy(roi), eys(roi);
-			for (int j = 0; j < roi; ++j) { Erf1D(static_cast<double>(j - h), t[2], sx, ex[j], edx[j], eds[j]); }
-			for (int i = 0; i < roi; ++i) { Erf1D(static_cast<double>(i - h), t[3], sy, ey[i], edy[i], eys[i]); }
+			std::vector<double> ex(roi), edx(roi), eds(roi), ey(roi), edy(roi), eys(roi), x2(3 * roi), y2(3 * roi);
+			for (int j = 0; j < roi; ++j) { Erf1D(static_cast<double>(j - hh), t[2], sx, ex[j], edx[j], eds[j], h ? &x2[3 * j] : nullptr); }
+			for (int i = 0; i < roi; ++i) { Erf1D(static_cast<double>(i - hh), t[3], sy, ey[i], edy[i], eys[i], h ? &y2[3 * i] : nullptr); }
 			for (int i = 0; i < roi; ++i) {
 				for (int j = 0; j < roi; ++j) {
 					const int k = i * roi + j;
 					const double psf = ex[j] * ey[i];
 					mu[k] = t[0] + t[1] * psf;
 					double* gk = g.data() + static_cast<size_t>(k) * 5;
+					const double Px = edx[j] * ey[i], Py = ex[j] * edy[i];
+					const double Ps = eds[j] * dsx * ey[i] + ex[j] * eys[i] * dsy;
 					gk[0] = 1;
 					gk[1] = psf;
-					gk[2] = t[1] * edx[j] * ey[i];
-					gk[3] = t[1] * ex[j] * edy[i];
-					gk[4] = t[1] * (eds[j] * dsx * ey[i] + ex[j] * eys[i] * dsy);
+					gk[2] = t[1] * Px;
+					gk[3] = t[1] * Py;
+					gk[4] = t[1] * Ps;
+					if (h) {
+						const double* X2 = &x2[3 * j];
+						const double* Y2 = &y2[3 * i];
+						const double Pxx = X2[0] * ey[i], Pxy = edx[j] * edy[i];
+						const double Pxs = X2[1] * dsx * ey[i] + edx[j] * eys[i] * dsy;
+						const double Pyy = ex[j] * Y2[0];
+						const double Pys = eds[j] * dsx * edy[i] + ex[j] * Y2[1] * dsy;
+						const double Pss = (X2[2] * dsx * dsx + eds[j] * ssx) * ey[i] + 2 * eds[j] * dsx * eys[i] * dsy +
+						                   ex[j] * (Y2[2] * dsy * dsy + eys[i] * ssy);
+						put2(k, Pxx, Pxy, Pxs, Pyy, Pys, Pss, Px, Py, Ps);
+					}
 				}
 			}
 			return;
@@ -1063,8 +1111,8 @@ struct MleRoi {
 		for (int i = 0; i < roi; ++i) {
 			for (int j = 0; j < roi; ++j) {
 				const int k = i * roi + j;
-				double dX, dY, dZ;
-				const double psf = SplinePsf(C, X0 + (j - h) - t[2], Y0 + (i - h) - t[3], t[4], dX, dY, dZ);
+				double dX, dY, dZ, s2[6];
+				const double psf = SplinePsf(C, X0 + (j - hh) - t[2], Y0 + (i - hh) - t[3], t[4], dX, dY, dZ, h ? s2 : nullptr);
 				mu[k] = t[0] + t[1] * psf;
 				double* gk = g.data() + static_cast<size_t>(k) * 5;
 				gk[0] = 1;
@@ -1072,15 +1120,17 @@ struct MleRoi {
 				gk[2] = -t[1] * dX;
 				gk[3] = -t[1] * dY;
 				gk[4] = t[1] * dZ;
+				if (h) { put2(k, s2[0], s2[1], -s2[2], s2[3], -s2[4], s2[5], -dX, -dY, dZ); }
 			}
 		}
 	}
 
-	// Deviance, gradient and Fisher-scoring matrix (H = 2 sum dmu dmu^T / mu).
-	double Normal(const double* t, double G[5], double Hm[25]) const
+	// Deviance D, gradient G and a 5x5 curvature matrix: Fisher scoring H = 2 sum dmu dmu^T / mu, or with `exact`
+	// the Hessian of D, 2 sum [d / mu^2 dmu dmu^T + (1 - d / mu) d2mu].
+	double Normal(const double* t, double G[5], double Hm[25], bool exact = false) const
 	{
-		std::vector<double> mu, g;
-		Eval(t, mu, g);
+		std::vector<double> mu, g, h2;
+		Eval(t, mu, g, exact ? &h2 : nullptr);
 		double D = 0;
 		for (int a = 0; a < 5; ++a) { G[a] = 0; }
 		for (int a = 0; a < 25; ++a) { Hm[a] = 0; }
@@ -1088,10 +1138,14 @@ struct MleRoi {
 			const double m = std::max(mu[k], 1e-6), dk = d[k];
 			D += dk > 0 ? 2 * (m - dk - dk * std::log(m / dk)) : 2 * m;
 			const double* gk = g.data() + static_cast<size_t>(k) * 5;
-			const double w1 = 2 * (1 - dk / m), w2 = 2 / m;
+			const double w1 = 2 * (1 - dk / m), w2 = exact ? 2 * dk / (m * m) : 2 / m;
+			int q = 0;
 			for (int a = 0; a < 5; ++a) {
 				G[a] += w1 * gk[a];
-				for (int b = a; b < 5; ++b) { Hm[a * 5 + b] += w2 * gk[a] * gk[b]; }
+				for (int b = a; b < 5; ++b, ++q) {
+					Hm[a * 5 + b] += w2 * gk[a] * gk[b];
+					if (exact) { Hm[a * 5 + b] += w1 * h2[static_cast<size_t>(k) * 15 + q]; }
+				}
 			}
 		}
 		for (int a = 0; a < 5; ++a) {
@@ -1142,6 +1196,29 @@ void MleBounds(const MleCfg& c, double x0, double y0, double lo[5], double hi[5]
 	else { lo[4] = 0.0; hi[4] = static_cast<double>(c.sz) - 1e-6; }
 }
 
+// Active bounds: a parameter that sits on a bound with the descent direction (-G) pointing outside is held there -
+// its row and column of the system become those of the identity and its right-hand side zero - so that the step of
+// the other parameters is the minimiser of the model restricted to them instead of a clipped full step.
+void FixActive(const double* t, const double* G, const double* lo, const double* hi, double* A, double* rhs)
+{
+	for (int a = 0; a < 5; ++a) {
+		if ((t[a] <= lo[a] && G[a] > 0) || (t[a] >= hi[a] && G[a] < 0)) {
+			for (int b = 0; b < 5; ++b) { A[a * 5 + b] = 0; A[b * 5 + a] = 0; }
+			A[a * 5 + a] = 1;
+			rhs[a] = 0;
+		}
+	}
+}
+
+// LM stop rule: an accepted step below 1e-4 px in x and y, 1e-4 relative in I, bg (floor 1) and the width / z
+// coordinate (1e-4 px for sigma, 1e-2 nm for z in nm, 1e-4 table units for the spline z).
+bool MleStepSmall(const MleCfg& c, const double* a, const double* b)
+{
+	const double sTol = c.model == 7 ? 1e-2 : 1e-4;
+	return std::abs(b[2] - a[2]) < 1e-4 && std::abs(b[3] - a[3]) < 1e-4 && std::abs(b[1] - a[1]) < 1e-4 * std::max(std::abs(a[1]), 1.0) &&
+	       std::abs(b[0] - a[0]) < 1e-4 * std::max(std::abs(a[0]), 1.0) && std::abs(b[4] - a[4]) < sTol;
+}
+
 // The fit of one candidate (coordinates local to the integer ROI centre); returns false for a failed fit.
 bool MleFit(const MleRoi& R, double t[5], double crlb[5], double& dev)
 {
@@ -1176,6 +1253,7 @@ bool MleFit(const MleRoi& R, double t[5], double crlb[5], double& dev)
 		double A[25], rhs[5], dt[5];
 		for (int a = 0; a < 25; ++a) { A[a] = Hm[a]; }
 		for (int a = 0; a < 5; ++a) { A[a * 5 + a] *= 1.0 + lambda; rhs[a] = -G[a]; }
+		FixActive(t, G, lo, hi, A, rhs);
 		if (!CholSolve5(A, rhs, dt)) {
 			lambda *= 10;
 			if (lambda > 1e7) { break; }
@@ -1186,29 +1264,38 @@ bool MleFit(const MleRoi& R, double t[5], double crlb[5], double& dev)
 		double Gt[5], Ht[25];
 		const double Dt = R.Normal(tt, Gt, Ht);
 		if (std::isfinite(Dt) && Dt < D) {
-			const double gainRel = (D - Dt) / (Dt + 1.0);
+			const bool small = MleStepSmall(c, t, tt);
 			for (int a = 0; a < 5; ++a) { t[a] = tt[a]; G[a] = Gt[a]; }
 			for (int a = 0; a < 25; ++a) { Hm[a] = Ht[a]; }
 			D = Dt;
 			lambda = std::max(lambda * 0.1, 1e-7);
-			if (gainRel < 1e-6) { break; }
+			if (small) { break; }
 		}
 		else {
 			lambda *= 10;
 			if (lambda > 1e7) { break; }
 		}
 	}
-	// undamped Fisher scoring in FP64 until the step is below 1e-10 (relative, at most 10 steps); a step that does not
-	// lower the deviance is halved up to three times
-	for (int it = 0; it < 10; ++it) {
-		double rhs[5], dt[5], tt[5];
+	// Newton steps on the exact Hessian of the deviance in FP64 (Fisher scoring where that Hessian is not positive
+	// definite) until the relative step is below 1e-10, at most 6 steps; a step that does not lower the deviance is
+	// halved up to three times
+	D = R.Normal(t, G, Hm, true);
+	for (int it = 0; it < 6; ++it) {
+		double rhs[5], dt[5], tt[5], A[25];
 		for (int a = 0; a < 5; ++a) { rhs[a] = -G[a]; }
-		if (!CholSolve5(Hm, rhs, dt)) { break; }
+		for (int a = 0; a < 25; ++a) { A[a] = Hm[a]; }
+		FixActive(t, G, lo, hi, A, rhs);
+		if (!CholSolve5(A, rhs, dt)) {
+			double Gf[5], Hf[25];
+			R.Normal(t, Gf, Hf, false);
+			FixActive(t, G, lo, hi, Hf, rhs);
+			if (!CholSolve5(Hf, rhs, dt)) { break; }
+		}
 		bool accepted = false;
 		double Gt[5], Ht[25], Dt = 0;
 		for (int half = 0; half < 4 && !accepted; ++half) {
 			for (int a = 0; a < 5; ++a) { tt[a] = std::min(std::max(t[a] + dt[a], lo[a]), hi[a]); }
-			Dt = R.Normal(tt, Gt, Ht);
+			Dt = R.Normal(tt, Gt, Ht, true);
 			if (std::isfinite(Dt) && Dt <= D) { accepted = true; }
 			else { for (int a = 0; a < 5; ++a) { dt[a] *= 0.5; } }
 		}
@@ -1220,6 +1307,7 @@ bool MleFit(const MleRoi& R, double t[5], double crlb[5], double& dev)
 		D = Dt;
 		if (step < 1e-10) { break; }
 	}
+	R.Normal(t, G, Hm, false);  // Fisher information for the CRLB
 	// CRLB: Fisher information F = H / 2; variances are the diagonal of its inverse
 	for (int a = 0; a < 5; ++a) {
 		double e[5] = {0, 0, 0, 0, 0}, col[5], F[25];
@@ -1233,16 +1321,13 @@ bool MleFit(const MleRoi& R, double t[5], double crlb[5], double& dev)
 	return true;
 }
 
-void FitMle(const MleCfg& c, const uint16_t* img, int W, int H, const Candidate& cd, Row& out)
+// ROI photons and local candidate position; false when the ROI crosses the frame border (Fitting.cpp's test).
+bool MleRoiAt(const MleCfg& c, const uint16_t* img, int W, int H, double cx, double cy, MleRoi& R)
 {
-	const size_t ux = static_cast<size_t>(cd.x), uy = static_cast<size_t>(cd.y);
+	const size_t ux = static_cast<size_t>(cx), uy = static_cast<size_t>(cy);
 	const size_t h = static_cast<size_t>(c.half);
-	const bool nonneg = cd.x >= 0 && cd.y >= 0;
-	if (!nonneg || h > ux || ux >= static_cast<size_t>(W) - h || h > uy || uy >= static_cast<size_t>(H) - h) {
-		FillRow(kG2Sigma, cd, out, cd.x, cd.y, 0);
-		return;
-	}
-	MleRoi R;
+	const bool nonneg = cx >= 0 && cy >= 0;
+	if (!nonneg || h > ux || ux >= static_cast<size_t>(W) - h || h > uy || uy >= static_cast<size_t>(H) - h) { return false; }
 	R.c = &c;
 	R.d.resize(c.n);
 	for (int i = 0; i < c.roi; ++i) {
@@ -1251,8 +1336,19 @@ void FitMle(const MleCfg& c, const uint16_t* img, int W, int H, const Candidate&
 			R.d[i * c.roi + j] = std::max((adu - c.offset) / c.gain, 0.0);
 		}
 	}
-	R.x0 = cd.x - static_cast<double>(ux);
-	R.y0 = cd.y - static_cast<double>(uy);
+	R.x0 = cx - static_cast<double>(ux);
+	R.y0 = cy - static_cast<double>(uy);
+	return true;
+}
+
+void FitMle(const MleCfg& c, const uint16_t* img, int W, int H, const Candidate& cd, Row& out)
+{
+	const size_t ux = static_cast<size_t>(cd.x), uy = static_cast<size_t>(cd.y);
+	MleRoi R;
+	if (!MleRoiAt(c, img, W, H, cd.x, cd.y, R)) {
+		FillRow(kG2Sigma, cd, out, cd.x, cd.y, 0);
+		return;
+	}
 	double t[5], crlb[5], dev = 0;
 	const bool ok = MleFit(R, t, crlb, dev);
 	const double qxy = std::sqrt(0.5 * (crlb[2] * crlb[2] + crlb[3] * crlb[3]));
@@ -1518,6 +1614,32 @@ uint64_t orc_Labels(const uint16_t* frame, uint64_t height, uint64_t width, doub
 	if (static_cast<int>(ratio) > 0) { seg.Fuse(); seg.Flood(); }
 	std::copy(seg.lab.begin(), seg.lab.end(), labels);
 	return seg.cands.size();
+}
+
+// Analysis helpers for the maximum-likelihood modes 6-8 (fit_params as for orc_Localization); theta is local to
+// the integer ROI centre floor(cx), floor(cy). Both return 0 when the ROI crosses the frame border.
+// orc_MleEvaluate: FP64 deviance, gradient and exact Hessian (row-major 5x5) at theta.
+int orc_MleEvaluate(const uint16_t* frame, uint64_t height, uint64_t width, double cx, double cy, uint64_t fit, const double* fp,
+                    const double* theta, double* D, double* G, double* Hm)
+{
+	MleCfg c;
+	if (fit < 6 || fit > 8 || !ParseMle(static_cast<int>(fit), fp, c)) { return 0; }
+	MleRoi R;
+	if (!MleRoiAt(c, frame, static_cast<int>(width), static_cast<int>(height), cx, cy, R)) { return 0; }
+	*D = R.Normal(theta, G, Hm, true);
+	return 1;
+}
+
+// orc_MleFitOne: the fit of one candidate (theta, CRLB, final deviance); returns 1 for a successful fit, 2 for a
+// failed one.
+int orc_MleFitOne(const uint16_t* frame, uint64_t height, uint64_t width, double cx, double cy, uint64_t fit, const double* fp,
+                  double* theta, double* crlb, double* dev)
+{
+	MleCfg c;
+	if (fit < 6 || fit > 8 || !ParseMle(static_cast<int>(fit), fp, c)) { return 0; }
+	MleRoi R;
+	if (!MleRoiAt(c, frame, static_cast<int>(width), static_cast<int>(height), cx, cy, R)) { return 0; }
+	return MleFit(R, theta, crlb, *dev) ? 1 : 2;
 }
 
 }  // extern "C"

@@ -156,4 +156,10 @@ PTB_API void PTB_StageTimes(double* ms, uint64_t* launches, int n)
 	ptb::EngineFor(lock).StageTimes(ms, launches, n);
 }
 
+PTB_API void PTB_MleEvaluations(uint64_t* counts, int n)
+{
+	std::unique_lock<std::mutex> lock;
+	ptb::EngineFor(lock).MleEvaluations(counts, n);
+}
+
 }  // extern "C"

@@ -233,6 +233,7 @@ Engine::~Engine()
 	if (img_) { cudaFree(img_); }
 	if (spline_) { cudaFree(spline_); }
 	if (fallbacks_) { cudaFree(fallbacks_); }
+	if (evalDev_) { cudaFree(evalDev_); }
 	if (hostCnt_) { cudaFreeHost(hostCnt_); }
 	if (stream_) { cudaStreamDestroy(stream_); }
 }
@@ -244,6 +245,9 @@ bool Engine::Init()
 	if (!PTB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking))) { return false; }
 	if (!PTB_CUDA(cudaMallocHost(&hostCnt_, sizeof(Counters)))) { return false; }
 	for (auto& e : ev_) {
+		if (!PTB_CUDA(cudaEventCreate(&e))) { return false; }
+	}
+	for (auto& e : mleEv_) {
 		if (!PTB_CUDA(cudaEventCreate(&e))) { return false; }
 	}
 	size_t freeB = 0, totalB = 0;
@@ -315,6 +319,13 @@ long long Engine::RunChunk(const uint16_t* dImg, int H, int W, int B, double thr
 	mark(2);
 	FitParams fpr = fp;
 	if (ok && fp.mode >= kMleGauss && fp.lanes == 0) { ok = Autotune(fpr, dImg, H, W); }
+	const bool mleProf = prof && fp.mode >= kMleGauss;
+	if (mleProf) {
+		if (!evalDev_) { ok = ok && PTB_CUDA(cudaMalloc(&evalDev_, 3 * sizeof(unsigned long long))); }
+		ok = ok && PTB_CUDA(cudaMemsetAsync(evalDev_, 0, 3 * sizeof(unsigned long long), st));
+		fpr.marks = mleEv_;
+		fpr.mle.evals = evalDev_;
+	}
 	ok = ok && LaunchFit(dImg, H, W, ws_.g.N, ws_.cand, &ws_.cnt->nfit, 0, ws_.capRows, fpr, ws_.rows, ws_.fitFlag, precision_, st);
 	mark(3);
 	ok = ok && LaunchSortFrames(ws_, dOut, idBase, planeBase, st);
@@ -329,6 +340,17 @@ long long Engine::RunChunk(const uint16_t* dImg, int H, int W, int B, double thr
 			stageMs_[k] += ms;
 			stageLaunches_[k] += launches[k];
 		}
+	}
+	if (mleProf) {
+		for (int k = 0; k < 3; ++k) {
+			float ms = 0.f;
+			cudaEventElapsedTime(&ms, mleEv_[k], mleEv_[k + 1]);
+			stageMs_[5 + k] += ms;
+			stageLaunches_[5 + k] += (k == 1 || fpr.lanes == 1) ? 1 : 0;
+		}
+		unsigned long long ev[3] = {};
+		if (!PTB_CUDA(cudaMemcpy(ev, evalDev_, sizeof(ev), cudaMemcpyDeviceToHost))) { return -1; }
+		for (int k = 0; k < 3; ++k) { evalTotals_[k] += ev[k]; }
 	}
 	if (hostCnt_->overflow) {
 		SetError("internal capacity overflow");
@@ -387,9 +409,15 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 	return static_cast<long long>(rows * kCols);
 }
 
+int EnvLanes()
+{
+	const char* env = std::getenv("PTB_MLE_LANES");
+	return env ? std::atoi(env) : 0;
+}
+
 int Engine::TunedLanes(const FitParams& fp) const
 {
-	if (const char* env = std::getenv("PTB_MLE_LANES")) { return std::atoi(env); }
+	if (const int env = EnvLanes()) { return env; }
 	const int key = fp.mode * 64 + fp.roi;
 	for (const auto& kv : tuned_) {
 		if (kv.first == key) { return kv.second; }
@@ -397,10 +425,11 @@ int Engine::TunedLanes(const FitParams& fp) const
 	return 0;  // not tuned yet: the first chunk with candidates tunes it
 }
 
-// Times every lane-group width on this chunk's candidates and keeps the fastest for (mode, ROI).
+// Times both ROI mappings (1: thread per ROI, 32: warp per ROI) on this chunk's candidates and keeps the faster for
+// (mode, ROI).
 bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W)
 {
-	static const int kChoices[] = {1, 8, 16, 32};
+	static const int kChoices[] = {1, 32};
 	cudaEvent_t a, b;
 	if (!PTB_CUDA(cudaEventCreate(&a)) || !PTB_CUDA(cudaEventCreate(&b))) { return false; }
 	float best = 1e30f;
@@ -435,6 +464,14 @@ void Engine::StageTimes(double* ms, uint64_t* launches, int n)
 	}
 }
 
+void Engine::MleEvaluations(uint64_t* out, int n)
+{
+	for (int k = 0; k < 3 && k < n; ++k) {
+		if (out) { out[k] = evalTotals_[k]; }
+		evalTotals_[k] = 0;
+	}
+}
+
 bool Engine::UploadSpline(FitParams& fp, const std::vector<double>& spline)
 {
 	if (fp.mode >= kMleGauss) {
@@ -443,21 +480,29 @@ bool Engine::UploadSpline(FitParams& fp, const std::vector<double>& spline)
 		fp.lanes = TunedLanes(fp);
 	}
 	if (fp.mode == kMleSpline) {
-		// FP32 cell-major copy of the [64][cell] table
+		// cell-major copies of the [64][cell] table: FP64 first, then FP32
 		const size_t cells = static_cast<size_t>(fp.splineSize);
-		std::vector<float> aos(cells * 64);
+		std::vector<double> aos64(cells * 64);
+		std::vector<float> aos32(cells * 64);
 		for (size_t i = 0; i < 64; ++i) {
-			for (size_t c = 0; c < cells; ++c) { aos[c * 64 + i] = static_cast<float>(spline[i * cells + c]); }
+			for (size_t c = 0; c < cells; ++c) {
+				aos64[c * 64 + i] = spline[i * cells + c];
+				aos32[c * 64 + i] = static_cast<float>(spline[i * cells + c]);
+			}
 		}
-		const size_t bytes = aos.size() * sizeof(float);
+		const size_t bytes64 = aos64.size() * sizeof(double), bytes32 = aos32.size() * sizeof(float);
+		const size_t bytes = bytes64 + bytes32;
 		if (bytes > splineBytes_) {
 			if (spline_) { cudaFree(spline_); spline_ = nullptr; splineBytes_ = 0; }
 			if (!PTB_CUDA(cudaMalloc(&spline_, bytes))) { return false; }
 			splineBytes_ = bytes;
 		}
-		if (!PTB_CUDA(cudaMemcpyAsync(spline_, aos.data(), bytes, cudaMemcpyHostToDevice, stream_))) { return false; }
+		char* base = static_cast<char*>(spline_);
+		if (!PTB_CUDA(cudaMemcpyAsync(base, aos64.data(), bytes64, cudaMemcpyHostToDevice, stream_))) { return false; }
+		if (!PTB_CUDA(cudaMemcpyAsync(base + bytes64, aos32.data(), bytes32, cudaMemcpyHostToDevice, stream_))) { return false; }
 		if (!PTB_CUDA(cudaStreamSynchronize(stream_))) { return false; }
-		fp.mle.table = static_cast<const float*>(spline_);
+		fp.mle.table64 = reinterpret_cast<const double*>(base);
+		fp.mle.table = reinterpret_cast<const float*>(base + bytes64);
 		return true;
 	}
 	if (fp.mode != kSplineEmccd) { return true; }

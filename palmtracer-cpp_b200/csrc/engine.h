@@ -16,6 +16,7 @@
 namespace ptb {
 
 bool ParseFitParams(uint64_t fit, const double* fp, FitParams& out, std::vector<double>& splineHost);
+int EnvLanes();
 uint64_t LaunchCount();
 double MeasureFmaPeak(int fp64);
 
@@ -38,7 +39,9 @@ public:
 	int SetStrict(int s) { const int o = strict_; strict_ = s; return o; }
 	int SetProfiling(int p) { const int o = profiling_; profiling_ = p; return o; }
 	void StageTimes(double* ms, uint64_t* launches, int n);
+	void MleEvaluations(uint64_t* out, int n);
 	int SetPrecision(int p) { const int o = precision_; precision_ = p; return o; }
+	int Precision() const { return precision_; }
 	cudaStream_t Stream() const { return stream_; }
 	void SetStream(cudaStream_t s) { stream_ = s; }
 	bool Init();
@@ -70,10 +73,14 @@ private:
 	int strict_ = 0;
 	int precision_ = 0;
 	int profiling_ = 0;
-	static constexpr int kStages = 5;
-	cudaEvent_t ev_[kStages + 1] = {};
+	// profiling: detect, segment, fit, finish, copies, then the phases of a modes 6-8 fit (initial values, LM, polish)
+	static constexpr int kStages = 8;
+	cudaEvent_t ev_[6] = {};
+	cudaEvent_t mleEv_[4] = {};
 	double stageMs_[kStages] = {};
 	uint64_t stageLaunches_[kStages] = {};
+	unsigned long long* evalDev_ = nullptr;      // device counters of model evaluations (profiling)
+	unsigned long long evalTotals_[3] = {};      // FP32 LM, FP32 polish, FP64
 };
 
 Engine& EngineFor(std::unique_lock<std::mutex>& lock);

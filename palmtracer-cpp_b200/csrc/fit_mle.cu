@@ -1,19 +1,33 @@
 // Poisson maximum-likelihood fits (modes 6 Gaussian, 7 astigmatic 3D, 8 cubic-spline 3D) of (bg, I, x, y, s),
 // s = sigma (mode 6), z in nm (mode 7) or the spline's z coordinate (mode 8). No counterpart in the reference; the
-// model maths, the algorithm and the FP64 oracle are in oracle/pt_oracle.cpp (MleFit), which this file follows step
-// for step: initial values, bounds, FP64 axial pre-scan, damped Fisher-scoring LM on the Poisson deviance, undamped
-// FP64 Fisher steps to a 1e-10 relative step and the CRLB from the FP64 Fisher information.
+// model maths and the FP64 oracle are in oracle/pt_oracle.cpp (MleFit). This file follows it: the same initial
+// values, bounds and FP64 axial pre-scan, the same damped Fisher-scoring LM on the Poisson deviance with the same
+// step-size stop rule, then Newton steps on the exact Hessian of the deviance, and the CRLB from the Fisher
+// information at the final point.
 //
-// Precision: the LM iterations run in FP32. The 5x5 damped system is factored by an FP32 Cholesky; when a pivot is not
-// positive or the pivot ratio min(L_ii^2) / max(A_ii) falls below 1e-5 the same system is re-factored in FP64. The
-// final polish, the log-likelihood (deviance) and the CRLB are computed in FP64.
+// Precision: the LM iterations and the Newton polish run in FP32. Each 5x5 system is factored by an FP32 Cholesky;
+// when a pivot is not positive or the pivot ratio min(L_ii^2) / max(A_ii) falls below 1e-5 the same system is
+// re-factored in FP64. The initial axial pre-scan (a handful of deviance evaluations that choose the starting basin),
+// the final deviance (log-likelihood) and the Fisher information behind the CRLB are computed in FP64. The oracle
+// polishes in FP64 to a 1e-10 relative step; the FP32 polish stops at a 1e-6 relative step (the FP32 resolution of
+// the deviance), well inside the stated tolerance of 1e-3 px and 1e-4 relative photons.
 //
-// Mapping: L lanes per ROI (L = 1, 8, 16 or 32; 32 / L ROIs per warp), chosen by the autotuner in engine.cu. Sums over
-// pixels are reduced with shuffles masked to the ROI's lane group. For modes 6 and 7 the pixel-integrated Gaussian is
-// separable, so each iteration evaluates the erf terms once per ROI column and row into a per-group shared table.
-// For mode 8 the monomial weights are the same for every pixel of the ROI (pixels differ by whole cells), so each
-// lane forms them once per iteration; the table is FP32, cell-major ([cell][64]).
+// Two mappings, chosen per (mode, ROI) by the autotuner in engine.cu:
+//   * thread per ROI, three launches that hand their state over in the output rows (columns 0-4 theta, column 5 a
+//     status) so that no extra device memory is needed:
+//       MleInitKernel   initial values and FP64 axial pre-scan;
+//       MleLmKernel     persistent FP32 LM: every warp owns a contiguous range of candidates and each lane takes the
+//                       next candidate of the range as soon as its own converges, so a lane never idles while the
+//                       other 31 iterate; ROI photons and the column erf factors are staged per lane in shared memory;
+//       MlePolishKernel FP32 Newton polish, FP64 deviance and Fisher information, CRLB, output row;
+//   * warp per ROI (MleWarpKernel): all four phases in one launch, pixels spread over the lanes, sums reduced with
+//     shuffles; better for large ROIs and for the spline model, whose 64 coefficients per pixel dominate.
+// For modes 6-7 the pixel-integrated Gaussian is separable: the erf factors are formed once per ROI column and row
+// per evaluation. The spline table is cell-major ([cell][64]) in FP32 for the FP32 phases and in FP64 for the FP64
+// ones.
 #include <algorithm>
+#include <mutex>
+#include <type_traits>
 
 #include "pt_common.cuh"
 
@@ -22,7 +36,18 @@ namespace ptb {
 namespace {
 
 constexpr int kMaxRoi = 15;
+constexpr int kMaxPix = kMaxRoi * kMaxRoi;
 constexpr int kThreads = 64;
+
+// State handed between the thread-per-ROI launches in column kStatusCol of the output row.
+constexpr int kStatusCol = 5;
+constexpr double kStOk = 0.0, kStFailed = 1.0, kStBorder = 2.0;
+
+// What one evaluation accumulates: deviance only; deviance, gradient and Fisher-scoring matrix; deviance, gradient,
+// exact Hessian and Fisher information; deviance and Fisher information.
+enum Kind { kDevOnly = 0, kFisher = 1, kExact = 2, kFinal = 3 };
+
+template <int KIND> struct Fields { static constexpr int value = KIND == kDevOnly ? 1 : (KIND == kExact ? 6 : 3); };
 
 template <typename T> __device__ __forceinline__ T Erf(T x);
 template <> __device__ __forceinline__ float Erf<float>(float x) { return erff(x); }
@@ -34,158 +59,322 @@ template <typename T> __device__ __forceinline__ T Ln(T x);
 template <> __device__ __forceinline__ float Ln<float>(float x) { return logf(x); }
 template <> __device__ __forceinline__ double Ln<double>(double x) { return log(x); }
 
-template <int L, typename T>
-__device__ __forceinline__ T GroupSum(T v, unsigned mask)
+template <typename T>
+__device__ __forceinline__ T WarpSum(T v)
 {
 	#pragma unroll
-	for (int d = L / 2; d > 0; d >>= 1) { v += __shfl_xor_sync(mask, v, d); }
+	for (int d = 16; d > 0; d >>= 1) { v += __shfl_xor_sync(0xffffffffu, v, d); }
 	return v;
 }
 
+// Pixel-integrated 1D Gaussian factor E = (erf(b) - erf(a)) / 2 and its derivatives in the position and the width
+// (NF >= 3) and the second derivatives E_xx, E_xs, E_ss (NF == 6).
 template <typename T>
-__device__ __forceinline__ void Erf1D(T c, T x, T s, T& e, T& dx, T& ds)
+struct Fac {
+	T e, dx, ds, xx, xs, ss;
+};
+
+template <typename T, int NF>
+__device__ __forceinline__ Fac<T> Factor(T c, T x, T s)
 {
+	Fac<T> f;
 	const T k = T(1) / (T(1.4142135623730951) * s);
 	const T a = (c - x - T(0.5)) * k, b = (c - x + T(0.5)) * k;
-	const T ea = Ex<T>(-a * a), eb = Ex<T>(-b * b);
-	e = T(0.5) * (Erf<T>(b) - Erf<T>(a));
-	dx = (ea - eb) / (T(2.5066282746310002) * s);
-	ds = (a * ea - b * eb) / (T(1.7724538509055160) * s);
+	f.e = T(0.5) * (Erf<T>(b) - Erf<T>(a));
+	f.dx = f.ds = f.xx = f.xs = f.ss = T(0);
+	if constexpr (NF >= 3) {
+		const T ea = Ex<T>(-a * a), eb = Ex<T>(-b * b);
+		f.dx = (ea - eb) / (T(2.5066282746310002) * s);
+		f.ds = (a * ea - b * eb) / (T(1.7724538509055160) * s);
+		if constexpr (NF == 6) {
+			f.xx = (a * ea - b * eb) / (T(1.7724538509055160) * s * s);
+			f.xs = (T(2) * a * a * ea - T(2) * b * b * eb - ea + eb) / (T(2.5066282746310002) * s * s);
+			f.ss = T(2) * (a * (a * a - T(1)) * ea - b * (b * b - T(1)) * eb) / (T(1.7724538509055160) * s * s);
+		}
+	}
+	return f;
 }
 
+// Factor table in shared memory: field f of entry c at p[(c * NF + f) * s].
 template <typename T>
-__device__ __forceinline__ void AstigSigma(const double* m, double pixelSize, T z, T& s, T& ds)
+struct FacTab {
+	T* p;
+	int s;
+	template <int NF>
+	__device__ __forceinline__ void Put(int c, const Fac<T>& f) const
+	{
+		T* q = p + c * NF * s;
+		q[0] = f.e;
+		if constexpr (NF >= 3) { q[s] = f.dx; q[2 * s] = f.ds; }
+		if constexpr (NF == 6) { q[3 * s] = f.xx; q[4 * s] = f.xs; q[5 * s] = f.ss; }
+	}
+	template <int NF>
+	__device__ __forceinline__ Fac<T> Get(int c) const
+	{
+		const T* q = p + c * NF * s;
+		Fac<T> f;
+		f.e = q[0];
+		f.dx = f.ds = f.xx = f.xs = f.ss = T(0);
+		if constexpr (NF >= 3) { f.dx = q[s]; f.ds = q[2 * s]; }
+		if constexpr (NF == 6) { f.xx = q[3 * s]; f.xs = q[4 * s]; f.ss = q[5 * s]; }
+		return f;
+	}
+};
+
+// Astigmatic width (pixels) and its first and second z derivatives for one axis [z0, w, c3, c4, A].
+template <typename T>
+__device__ __forceinline__ void AstigSigma(const double* m, double pixelSize, T z, T& s, T& ds, T& dss)
 {
 	const T u = (z - T(m[0])) / T(m[1]);
 	const T poly = T(1) + u * u + T(m[2]) * u * u * u + T(m[3]) * u * u * u * u;
 	const T k = T(m[4] / pixelSize);
-	if (poly <= T(1e-12)) { s = k * T(1e-6); ds = T(0); return; }
+	if (poly <= T(1e-12)) { s = k * T(1e-6); ds = T(0); dss = T(0); return; }
 	const T r = sqrt(poly);
+	const T p1 = T(2) * u + T(3 * m[2]) * u * u + T(4 * m[3]) * u * u * u;
+	const T p2 = T(2) + T(6 * m[2]) * u + T(12 * m[3]) * u * u;
 	s = k * r;
-	ds = k * (T(2) * u + T(3 * m[2]) * u * u + T(4 * m[3]) * u * u * u) / (T(2) * r * T(m[1]));
+	ds = k * p1 / (T(2) * r * T(m[1]));
+	dss = k / (T(m[1]) * T(m[1])) * (p2 / (T(2) * r) - p1 * p1 / (T(4) * r * poly));
 }
 
-struct Group {
-	int gl;          // lane within the ROI group
-	unsigned mask;   // lanes of the group
-	void* tab;       // per-group shared scratch (erf tables)
-};
-
-// Deviance D and (when FULL) gradient G and Fisher-scoring matrix H (upper triangle, 15 entries) at theta.
-template <typename T, int MODEL, int L, bool FULL>
-__device__ T Normal(const MleParams& mp, const uint16_t* roiBase, int W, const T th[5], T G[5], T Hm[15], const Group& grp)
+// Separable PSF at one pixel; P1 = d psf / d(x, y, s), P2 = the second derivatives (xx, xy, xs, yy, ys, ss).
+template <typename T, int NF>
+__device__ __forceinline__ T GaussPixel(const Fac<T>& X, const Fac<T>& Y, T dsx, T dsy, T ssx, T ssy, T P1[3], T P2[6])
 {
-	const int roi = mp.roi, h = mp.half, n = mp.n;
-	T* tab = static_cast<T*>(grp.tab);  // [6][kMaxRoi]: ex, edx, eds, ey, edy, eds_y
-	T sx = th[4], sy = th[4], dsx = T(1), dsy = T(1);
-	if constexpr (MODEL == 7) {
-		AstigSigma<T>(mp.astig, mp.pixelSize, th[4], sx, dsx);
-		AstigSigma<T>(mp.astig + 5, mp.pixelSize, th[4], sy, dsy);
+	if constexpr (NF >= 3) {
+		P1[0] = X.dx * Y.e;
+		P1[1] = X.e * Y.dx;
+		P1[2] = X.ds * dsx * Y.e + X.e * Y.ds * dsy;
 	}
-	T px[4], py[4], pz[4], dpx[4], dpy[4], dpz[4];
-	int ix0 = 0, iy0 = 0, iz = 0;
-	if constexpr (MODEL == 6 || MODEL == 7) {
-		for (int k = grp.gl; k < roi; k += L) {
-			T e, dx, ds;
-			Erf1D<T>(T(k - h), th[2], sx, e, dx, ds);
-			tab[0 * kMaxRoi + k] = e;
-			tab[1 * kMaxRoi + k] = dx;
-			tab[2 * kMaxRoi + k] = ds;
-			Erf1D<T>(T(k - h), th[3], sy, e, dx, ds);
-			tab[3 * kMaxRoi + k] = e;
-			tab[4 * kMaxRoi + k] = dx;
-			tab[5 * kMaxRoi + k] = ds;
-		}
-		__syncwarp(grp.mask);
+	if constexpr (NF == 6) {
+		P2[0] = X.xx * Y.e;
+		P2[1] = X.dx * Y.dx;
+		P2[2] = X.xs * dsx * Y.e + X.dx * Y.ds * dsy;
+		P2[3] = X.e * Y.xx;
+		P2[4] = X.ds * dsx * Y.dx + X.e * Y.xs * dsy;
+		P2[5] = (X.ss * dsx * dsx + X.ds * ssx) * Y.e + T(2) * X.ds * dsx * Y.ds * dsy + X.e * (Y.ss * dsy * dsy + Y.ds * ssy);
 	}
-	else {
-		// cell of ROI pixel (0, 0) and the common fractional offsets
-		const T X = T((mp.sx - 1) * 0.5) - T(h) - th[2], Y = T((mp.sy - 1) * 0.5) - T(h) - th[3];
-		const T fxi = floor(X), fyi = floor(Y), fzi = floor(th[4]);
-		ix0 = static_cast<int>(fxi);
-		iy0 = static_cast<int>(fyi);
-		iz = min(max(static_cast<int>(fzi), 0), mp.sz - 1);
-		const T fx = X - fxi, fy = Y - fyi, fz = th[4] - T(iz);
-		px[0] = T(1); px[1] = fx; px[2] = fx * fx; px[3] = fx * fx * fx;
-		py[0] = T(1); py[1] = fy; py[2] = fy * fy; py[3] = fy * fy * fy;
-		pz[0] = T(1); pz[1] = fz; pz[2] = fz * fz; pz[3] = fz * fz * fz;
-		dpx[0] = T(0); dpx[1] = T(1); dpx[2] = T(2) * fx; dpx[3] = T(3) * fx * fx;
-		dpy[0] = T(0); dpy[1] = T(1); dpy[2] = T(2) * fy; dpy[3] = T(3) * fy * fy;
-		dpz[0] = T(0); dpz[1] = T(1); dpz[2] = T(2) * fz; dpz[3] = T(3) * fz * fz;
+	return X.e * Y.e;
+}
+
+__device__ __forceinline__ int SplineCell(double v, int dim) { return min(max(static_cast<int>(floor(v)), 0), dim - 1); }
+__device__ __forceinline__ int SplineCell(float v, int dim) { return min(max(static_cast<int>(floorf(v)), 0), dim - 1); }
+
+// Cubic-spline PSF at table coordinates (X, Y, Z): the cell index is clamped to the table and the fraction taken
+// from the clamped cell, as in the oracle. P1 and P2 are the derivatives in the fit parameters (x, y, s): X and Y
+// decrease as x and y grow, so their odd derivatives change sign.
+template <typename T, int NF>
+__device__ __forceinline__ T SplinePixel(const MleParams& mp, T X, T Y, T Z, T P1[3], T P2[6])
+{
+	const int ix = SplineCell(X, mp.sx), iy = SplineCell(Y, mp.sy), iz = SplineCell(Z, mp.sz);
+	const T f[3] = {X - T(ix), Y - T(iy), Z - T(iz)};
+	T p[3][4], d[3][4], dd[3][4];
+	#pragma unroll
+	for (int a = 0; a < 3; ++a) {
+		p[a][0] = T(1); p[a][1] = f[a]; p[a][2] = f[a] * f[a]; p[a][3] = f[a] * f[a] * f[a];
+		d[a][0] = T(0); d[a][1] = T(1); d[a][2] = T(2) * f[a]; d[a][3] = T(3) * f[a] * f[a];
+		dd[a][0] = T(0); dd[a][1] = T(0); dd[a][2] = T(2); dd[a][3] = T(6) * f[a];
 	}
-	T D = T(0);
-	if constexpr (FULL) {
-		#pragma unroll
-		for (int a = 0; a < 5; ++a) { G[a] = T(0); }
-		#pragma unroll
-		for (int a = 0; a < 15; ++a) { Hm[a] = T(0); }
-	}
-	const T offset = T(mp.offset), invGain = T(1.0 / mp.gain);
-	int i = grp.gl / roi, j = grp.gl - i * roi;
-	for (int idx = grp.gl; idx < n; idx += L) {
-		const T adu = T(__ldg(roiBase + static_cast<long long>(i) * W + j));
-		const T d = max((adu - offset) * invGain, T(0));
-		T psf, g2, g3, g4;
-		if constexpr (MODEL == 6 || MODEL == 7) {
-			const T ex = tab[j], edx = tab[kMaxRoi + j], esx = tab[2 * kMaxRoi + j];
-			const T ey = tab[3 * kMaxRoi + i], edy = tab[4 * kMaxRoi + i], esy = tab[5 * kMaxRoi + i];
-			psf = ex * ey;
-			g2 = th[1] * edx * ey;
-			g3 = th[1] * ex * edy;
-			g4 = th[1] * (esx * dsx * ey + ex * esy * dsy);
+	const long long cell = (static_cast<long long>(iz) * mp.sy + iy) * mp.sx + ix;
+	T v = T(0), sX = T(0), sY = T(0), sZ = T(0), sXX = T(0), sXY = T(0), sXZ = T(0), sYY = T(0), sYZ = T(0), sZZ = T(0);
+	#pragma unroll
+	for (int q = 0; q < 16; ++q) {  // q = zi * 4 + yj: the four x-monomials of one (z, y) pair
+		T c0, c1, c2, c3;
+		if constexpr (std::is_same<T, float>::value) {
+			const float4 c = __ldg(reinterpret_cast<const float4*>(mp.table + cell * 64) + q);
+			c0 = c.x; c1 = c.y; c2 = c.z; c3 = c.w;
 		}
 		else {
-			const int cx = min(max(ix0 + j, 0), mp.sx - 1), cy = min(max(iy0 + i, 0), mp.sy - 1);
-			const float4* c4 = reinterpret_cast<const float4*>(mp.table + ((static_cast<long long>(iz) * mp.sy + cy) * mp.sx + cx) * 64);
-			T v = T(0), vx = T(0), vy = T(0), vz = T(0);
-			#pragma unroll
-			for (int q = 0; q < 16; ++q) {  // q = zi * 4 + yj: the four x-monomials of one (z, y) pair
-				const float4 c = __ldg(c4 + q);
-				const int zi = q >> 2, yj = q & 3;
-				const T w = pz[zi] * py[yj];
-				const T sxv = T(c.x) * px[0] + T(c.y) * px[1] + T(c.z) * px[2] + T(c.w) * px[3];
-				const T sdx = T(c.y) * dpx[1] + T(c.z) * dpx[2] + T(c.w) * dpx[3];
-				v += w * sxv;
-				vx += w * sdx;
-				vy += pz[zi] * dpy[yj] * sxv;
-				vz += dpz[zi] * py[yj] * sxv;
-			}
-			psf = v;
-			g2 = -th[1] * vx;
-			g3 = -th[1] * vy;
-			g4 = th[1] * vz;
+			const double2 a = __ldg(reinterpret_cast<const double2*>(mp.table64 + cell * 64) + 2 * q);
+			const double2 b = __ldg(reinterpret_cast<const double2*>(mp.table64 + cell * 64) + 2 * q + 1);
+			c0 = a.x; c1 = a.y; c2 = b.x; c3 = b.y;
 		}
-		const T mu = max(th[0] + th[1] * psf, T(1e-6));
-		D += d > T(0) ? T(2) * (mu - d - d * Ln<T>(mu / d)) : T(2) * mu;
-		if constexpr (FULL) {
-			const T gk[5] = {T(1), psf, g2, g3, g4};
-			const T w1 = T(2) * (T(1) - d / mu), w2 = T(2) / mu;
+		const int zi = q >> 2, yj = q & 3;
+		const T sx = c0 * p[0][0] + c1 * p[0][1] + c2 * p[0][2] + c3 * p[0][3];
+		const T zy = p[2][zi] * p[1][yj];
+		v += zy * sx;
+		if constexpr (NF >= 3) {
+			const T dx = c1 * d[0][1] + c2 * d[0][2] + c3 * d[0][3];
+			sX += zy * dx;
+			sY += p[2][zi] * d[1][yj] * sx;
+			sZ += d[2][zi] * p[1][yj] * sx;
+			if constexpr (NF == 6) {
+				const T ddx = c2 * dd[0][2] + c3 * dd[0][3];
+				sXX += zy * ddx;
+				sXY += p[2][zi] * d[1][yj] * dx;
+				sXZ += d[2][zi] * p[1][yj] * dx;
+				sYY += p[2][zi] * dd[1][yj] * sx;
+				sYZ += d[2][zi] * d[1][yj] * sx;
+				sZZ += dd[2][zi] * p[1][yj] * sx;
+			}
+		}
+	}
+	if constexpr (NF >= 3) { P1[0] = -sX; P1[1] = -sY; P1[2] = sZ; }
+	if constexpr (NF == 6) { P2[0] = sXX; P2[1] = sXY; P2[2] = -sXZ; P2[3] = sYY; P2[4] = -sYZ; P2[5] = sZZ; }
+	return v;
+}
+
+// One pixel's share of the sums. Fisher scoring: Hm = 2 sum dmu dmu^T / mu. Exact: Hm = the Hessian of the deviance,
+// 2 sum [d / mu^2 dmu dmu^T + (1 - d / mu) d2mu], and Fm = sum dmu dmu^T / mu (Fisher information). Final: Fm only.
+template <typename T, int KIND>
+__device__ __forceinline__ void Accumulate(T d, T bg, T I, T psf, const T P1[3], const T P2[6], T& D, T G[5], T Hm[15], T Fm[15])
+{
+	const T mu = max(bg + I * psf, T(1e-6));
+	D += d > T(0) ? T(2) * (mu - d - d * Ln<T>(mu / d)) : T(2) * mu;
+	if constexpr (KIND != kDevOnly) {
+		const T gk[5] = {T(1), psf, I * P1[0], I * P1[1], I * P1[2]};
+		const T rmu = T(1) / mu;
+		if constexpr (KIND == kFinal) {
+			int q = 0;
+			#pragma unroll
+			for (int a = 0; a < 5; ++a) {
+				const T wa = rmu * gk[a];
+				#pragma unroll
+				for (int b = a; b < 5; ++b) { Fm[q++] += wa * gk[b]; }
+			}
+		}
+		else {
+			const T w1 = T(2) * (T(1) - d * rmu);
+			const T w2 = KIND == kExact ? T(2) * d * rmu * rmu : T(2) * rmu;
 			int q = 0;
 			#pragma unroll
 			for (int a = 0; a < 5; ++a) {
 				G[a] += w1 * gk[a];
 				const T wa = w2 * gk[a];
+				const T fa = rmu * gk[a];
 				#pragma unroll
-				for (int b = a; b < 5; ++b) { Hm[q++] += wa * gk[b]; }
+				for (int b = a; b < 5; ++b) {
+					Hm[q] += wa * gk[b];
+					if constexpr (KIND == kExact) { Fm[q] += fa * gk[b]; }
+					++q;
+				}
+			}
+			if constexpr (KIND == kExact) {
+				// d2mu in the packed upper triangle: (I, x) = Px, (I, y) = Py, (I, s) = Ps, (x, x) = I Pxx, ...
+				Hm[6] += w1 * P1[0];
+				Hm[7] += w1 * P1[1];
+				Hm[8] += w1 * P1[2];
+				Hm[9] += w1 * I * P2[0];
+				Hm[10] += w1 * I * P2[1];
+				Hm[11] += w1 * I * P2[2];
+				Hm[12] += w1 * I * P2[3];
+				Hm[13] += w1 * I * P2[4];
+				Hm[14] += w1 * I * P2[5];
 			}
 		}
-		j += L;
-		while (j >= roi) { j -= roi; ++i; }
 	}
-	if constexpr (MODEL == 6 || MODEL == 7) { __syncwarp(grp.mask); }  // tables are rewritten by the next call
-	D = GroupSum<L>(D, grp.mask);
-	if constexpr (FULL) {
+}
+
+// Where an evaluation reads the ROI's photons: FP32 photons staged in shared memory (pixel k at sm[k * ss]), or the
+// frame (FP64 evaluations, and FP32 ones without staging).
+struct Pix {
+	const float* sm;
+	int ss;
+	const uint16_t* g;  // ROI origin in the frame
+	int W;
+	float off32, inv32;
+	double off64, inv64;
+};
+
+template <typename T>
+__device__ __forceinline__ T Photons(const Pix& px, int i, int j, int k)
+{
+	if constexpr (std::is_same<T, float>::value) {
+		if (px.sm) { return px.sm[k * px.ss]; }
+		return fmaxf((float(__ldg(px.g + i * px.W + j)) - px.off32) * px.inv32, 0.f);
+	}
+	else { return fmax((double(__ldg(px.g + i * px.W + j)) - px.off64) * px.inv64, 0.0); }
+}
+
+// Deviance D at theta and, by KIND, the gradient G, the curvature Hm and the Fisher information Fm (upper
+// triangles, 15 entries). L = 1: the calling thread sums the whole ROI, the column factors go to its table xt. L = 32:
+// the warp shares the pixels, the column and row factors go to the warp's tables xt and yt, the sums are reduced
+// over the warp and every lane returns them.
+template <typename T, int MODEL, int L, int KIND>
+__device__ T Normal(const MleParams& mp, const Pix& px, const T th[5], T G[5], T Hm[15], T Fm[15], FacTab<T> xt, FacTab<T> yt)
+{
+	constexpr int NF = Fields<KIND>::value;
+	const int roi = mp.roi, h = mp.half, n = mp.n;
+	const int gl = L == 1 ? 0 : (threadIdx.x & 31);
+	T sx = th[4], sy = th[4], dsx = T(1), dsy = T(1), ssx = T(0), ssy = T(0);
+	if constexpr (MODEL == 7) {
+		AstigSigma<T>(mp.astig, mp.pixelSize, th[4], sx, dsx, ssx);
+		AstigSigma<T>(mp.astig + 5, mp.pixelSize, th[4], sy, dsy, ssy);
+	}
+	T D = T(0);
+	if constexpr (KIND == kFisher || KIND == kExact) {
 		#pragma unroll
-		for (int a = 0; a < 5; ++a) { G[a] = GroupSum<L>(G[a], grp.mask); }
+		for (int a = 0; a < 5; ++a) { G[a] = T(0); }
 		#pragma unroll
-		for (int a = 0; a < 15; ++a) { Hm[a] = GroupSum<L>(Hm[a], grp.mask); }
+		for (int a = 0; a < 15; ++a) { Hm[a] = T(0); }
+	}
+	if constexpr (KIND == kExact || KIND == kFinal) {
+		#pragma unroll
+		for (int a = 0; a < 15; ++a) { Fm[a] = T(0); }
+	}
+	T P1[3] = {T(0), T(0), T(0)}, P2[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+	if constexpr (MODEL == 8) {
+		const T X0 = T((mp.sx - 1) * 0.5), Y0 = T((mp.sy - 1) * 0.5);
+		int i = gl / roi, j = gl - i * roi;
+		const int di = L / roi, dj = L - di * roi;
+		for (int k = gl; k < n; k += L) {
+			const T d = Photons<T>(px, i, j, k);
+			const T psf = SplinePixel<T, NF>(mp, X0 + T(j - h) - th[2], Y0 + T(i - h) - th[3], th[4], P1, P2);
+			Accumulate<T, KIND>(d, th[0], th[1], psf, P1, P2, D, G, Hm, Fm);
+			i += di;
+			j += dj;
+			if (j >= roi) { j -= roi; ++i; }
+		}
+	}
+	else if constexpr (L == 1) {
+		for (int c = 0; c < roi; ++c) { xt.template Put<NF>(c, Factor<T, NF>(T(c - h), th[2], sx)); }
+		int k = 0;
+		for (int i = 0; i < roi; ++i) {
+			const Fac<T> yf = Factor<T, NF>(T(i - h), th[3], sy);
+			for (int j = 0; j < roi; ++j, ++k) {
+				const T d = Photons<T>(px, i, j, k);
+				const T psf = GaussPixel<T, NF>(xt.template Get<NF>(j), yf, dsx, dsy, ssx, ssy, P1, P2);
+				Accumulate<T, KIND>(d, th[0], th[1], psf, P1, P2, D, G, Hm, Fm);
+			}
+		}
+	}
+	else {
+		for (int c = gl; c < roi; c += L) {
+			xt.template Put<NF>(c, Factor<T, NF>(T(c - h), th[2], sx));
+			yt.template Put<NF>(c, Factor<T, NF>(T(c - h), th[3], sy));
+		}
+		__syncwarp();
+		int i = gl / roi, j = gl - i * roi;
+		const int di = L / roi, dj = L - di * roi;
+		for (int k = gl; k < n; k += L) {
+			const T d = Photons<T>(px, i, j, k);
+			const T psf = GaussPixel<T, NF>(xt.template Get<NF>(j), yt.template Get<NF>(i), dsx, dsy, ssx, ssy, P1, P2);
+			Accumulate<T, KIND>(d, th[0], th[1], psf, P1, P2, D, G, Hm, Fm);
+			i += di;
+			j += dj;
+			if (j >= roi) { j -= roi; ++i; }
+		}
+		__syncwarp();  // the tables are rewritten by the next evaluation
+	}
+	if constexpr (L > 1) {
+		D = WarpSum(D);
+		if constexpr (KIND == kFisher || KIND == kExact) {
+			#pragma unroll
+			for (int a = 0; a < 5; ++a) { G[a] = WarpSum(G[a]); }
+			#pragma unroll
+			for (int a = 0; a < 15; ++a) { Hm[a] = WarpSum(Hm[a]); }
+		}
+		if constexpr (KIND == kExact || KIND == kFinal) {
+			#pragma unroll
+			for (int a = 0; a < 15; ++a) { Fm[a] = WarpSum(Fm[a]); }
+		}
 	}
 	return D;
 }
 
 __device__ __forceinline__ int Ut(int a, int b) { return a <= b ? a * 5 - (a * (a - 1)) / 2 + (b - a) : b * 5 - (b * (b - 1)) / 2 + (a - b); }
 
-// Cholesky solve of the packed symmetric system (upper triangle) with the given diagonal scaling.
+// Cholesky solve of the packed symmetric system (upper triangle) with the diagonal multiplied by diagScale.
 template <typename T>
 __device__ bool Chol5(const T Hm[15], T diagScale, const T rhs[5], T x[5], T* pivotRatio)
 {
@@ -226,7 +415,242 @@ __device__ bool Chol5(const T Hm[15], T diagScale, const T rhs[5], T x[5], T* pi
 	return true;
 }
 
-__device__ void StoreMleRow(double* row, int lane, const MleParams& mp, const Cand& cd, const double t[5], const double crlb[5],
+// FP32 solve of (Hm with its diagonal scaled) dt = rhs; re-factored in FP64 when the FP32 factorisation fails or its
+// pivot ratio is below 1e-5 (counted in *fallbacks when count is set).
+__device__ bool Solve32(const float Hm[15], float scale, const float rhs[5], float dt[5], unsigned* fallbacks, bool count)
+{
+	float ratio = 0.f;
+	if (Chol5<float>(Hm, scale, rhs, dt, &ratio) && ratio >= 1e-5f) { return true; }
+	double Hd[15], rd[5], xd[5];
+	#pragma unroll
+	for (int a = 0; a < 15; ++a) { Hd[a] = Hm[a]; }
+	#pragma unroll
+	for (int a = 0; a < 5; ++a) { rd[a] = rhs[a]; }
+	const bool ok = Chol5<double>(Hd, static_cast<double>(scale), rd, xd, nullptr);
+	if (count && fallbacks) { atomicAdd(fallbacks, 1u); }
+	#pragma unroll
+	for (int a = 0; a < 5; ++a) { dt[a] = static_cast<float>(xd[a]); }
+	return ok;
+}
+
+// Bounds of theta (MleBounds in the oracle); x0, y0 = candidate position relative to the ROI centre.
+template <int MODEL>
+__device__ __forceinline__ void Bounds(const MleParams& mp, double x0, double y0, double lo[5], double hi[5])
+{
+	const double hf = static_cast<double>(mp.half);
+	lo[0] = 1e-3; hi[0] = 1e6;
+	lo[1] = 1.0; hi[1] = 1e9;
+	lo[2] = fmax(x0 - 2.0, -hf); hi[2] = fmin(x0 + 2.0, hf);
+	lo[3] = fmax(y0 - 2.0, -hf); hi[3] = fmin(y0 + 2.0, hf);
+	if (MODEL == 6) { lo[4] = 0.5; hi[4] = 5.0; }
+	else if (MODEL == 7) { lo[4] = mp.zMin; hi[4] = mp.zMax; }
+	else { lo[4] = 0.0; hi[4] = static_cast<double>(mp.sz) - 1e-6; }
+}
+
+// The same bounds in FP32 (the spline's upper z bound is the largest float below sz).
+template <int MODEL>
+__device__ __forceinline__ void Bounds32(const MleParams& mp, float x0, float y0, float lo[5], float hi[5])
+{
+	const float hf = static_cast<float>(mp.half);
+	lo[0] = 1e-3f; hi[0] = 1e6f;
+	lo[1] = 1.f; hi[1] = 1e9f;
+	lo[2] = fmaxf(x0 - 2.f, -hf); hi[2] = fminf(x0 + 2.f, hf);
+	lo[3] = fmaxf(y0 - 2.f, -hf); hi[3] = fminf(y0 + 2.f, hf);
+	if (MODEL == 6) { lo[4] = 0.5f; hi[4] = 5.f; }
+	else if (MODEL == 7) { lo[4] = static_cast<float>(mp.zMin); hi[4] = static_cast<float>(mp.zMax); }
+	else { lo[4] = 0.f; hi[4] = nextafterf(static_cast<float>(mp.sz), 0.f); }
+}
+
+template <int MODEL>
+__device__ __forceinline__ void Clamp32(const MleParams& mp, float x0, float y0, float t[5])
+{
+	float lo[5], hi[5];
+	Bounds32<MODEL>(mp, x0, y0, lo, hi);
+	#pragma unroll
+	for (int a = 0; a < 5; ++a) { t[a] = fminf(fmaxf(t[a], lo[a]), hi[a]); }
+}
+
+// Active bounds (FixActive in the oracle): a parameter on a bound whose descent direction -G points outside is held
+// there - its row and column of the packed system become those of the identity, its right-hand side zero.
+template <int MODEL>
+__device__ __forceinline__ void FixActive32(const MleParams& mp, float x0, float y0, const float t[5], const float G[5], float A[15],
+                                            float rhs[5])
+{
+	float lo[5], hi[5];
+	Bounds32<MODEL>(mp, x0, y0, lo, hi);
+	#pragma unroll
+	for (int a = 0; a < 5; ++a) {
+		if ((t[a] <= lo[a] && G[a] > 0.f) || (t[a] >= hi[a] && G[a] < 0.f)) {
+			#pragma unroll
+			for (int b = 0; b < 5; ++b) { A[Ut(a, b)] = 0.f; }
+			A[Ut(a, a)] = 1.f;
+			rhs[a] = 0.f;
+		}
+	}
+}
+
+// LM stop rule of the oracle (MleStepSmall).
+__device__ __forceinline__ bool StepSmall(int model, const float a[5], const float b[5])
+{
+	const float sTol = model == 7 ? 1e-2f : 1e-4f;
+	return fabsf(b[2] - a[2]) < 1e-4f && fabsf(b[3] - a[3]) < 1e-4f && fabsf(b[1] - a[1]) < 1e-4f * fmaxf(fabsf(a[1]), 1.f) &&
+	       fabsf(b[0] - a[0]) < 1e-4f * fmaxf(fabsf(a[0]), 1.f) && fabsf(b[4] - a[4]) < sTol;
+}
+
+// ROI geometry of a candidate; false when the ROI crosses the frame border (the reference's test, Fitting.cpp).
+struct RoiAt {
+	unsigned long long ux, uy;
+	double x0, y0;
+	const uint16_t* base;
+};
+
+__device__ __forceinline__ bool Locate(const uint16_t* img, int H, int W, long long N, const MleParams& mp, const Cand& cd, RoiAt& r)
+{
+	const bool nonneg = cd.x >= 0.0 && cd.y >= 0.0;
+	r.ux = nonneg ? static_cast<unsigned long long>(cd.x) : 0ull;
+	r.uy = nonneg ? static_cast<unsigned long long>(cd.y) : 0ull;
+	const unsigned long long hh = static_cast<unsigned long long>(mp.half);
+	if (!nonneg || hh > r.ux || r.ux >= static_cast<unsigned long long>(W) - hh || hh > r.uy || r.uy >= static_cast<unsigned long long>(H) - hh) {
+		return false;
+	}
+	r.x0 = cd.x - static_cast<double>(r.ux);
+	r.y0 = cd.y - static_cast<double>(r.uy);
+	r.base = img + static_cast<long long>(cd.frame) * N + static_cast<long long>(r.uy - hh) * W + static_cast<long long>(r.ux - hh);
+	return true;
+}
+
+__device__ __forceinline__ Pix MakePix(const MleParams& mp, const uint16_t* base, int W, const float* sm, int ss)
+{
+	Pix p;
+	p.sm = sm;
+	p.ss = ss;
+	p.g = base;
+	p.W = W;
+	p.off32 = static_cast<float>(mp.offset);
+	p.inv32 = static_cast<float>(1.0 / mp.gain);
+	p.off64 = mp.offset;
+	p.inv64 = 1.0 / mp.gain;
+	return p;
+}
+
+// Initial values (oracle MleFit): bg = min photons (>= 1e-3), I = photons above bg (>= 1), x, y = candidate, s =
+// sigma0 (mode 6) or the best of an FP64 deviance scan of the axial range (16 points for mode 7, 8 for mode 8).
+template <int MODEL, int L>
+__device__ int InitTheta(const MleParams& mp, const Pix& px, const RoiAt& r, double t[5], FacTab<double> xt, FacTab<double> yt)
+{
+	int evals = 0;
+	const int gl = L == 1 ? 0 : (threadIdx.x & 31);
+	double dmin = 1e300, sum = 0;
+	for (int k = gl; k < mp.n; k += L) {
+		const int i = k / mp.roi, j = k - i * mp.roi;
+		const double d = Photons<double>(px, i, j, k);
+		dmin = fmin(dmin, d);
+		sum += d;
+	}
+	if constexpr (L > 1) {
+		#pragma unroll
+		for (int d = 16; d > 0; d >>= 1) {
+			dmin = fmin(dmin, __shfl_xor_sync(0xffffffffu, dmin, d));
+			sum += __shfl_xor_sync(0xffffffffu, sum, d);
+		}
+	}
+	double lo[5], hi[5];
+	Bounds<MODEL>(mp, r.x0, r.y0, lo, hi);
+	t[0] = fmax(dmin, 1e-3);
+	t[1] = fmax(sum - t[0] * mp.n, 1.0);
+	t[2] = r.x0;
+	t[3] = r.y0;
+	if (MODEL == 6) { t[4] = mp.sigma0; }
+	else {
+		const int ns = MODEL == 7 ? 16 : 8;
+		double best = 1e300, bz = 0.5 * (lo[4] + hi[4]);
+		for (int s = 0; s < ns; ++s) {
+			t[4] = lo[4] + (hi[4] - lo[4]) * (s + 0.5) / ns;
+			const double D = Normal<double, MODEL, L, kDevOnly>(mp, px, t, nullptr, nullptr, nullptr, xt, yt);
+			++evals;
+			if (D < best) { best = D; bz = t[4]; }
+		}
+		t[4] = bz;
+	}
+	#pragma unroll
+	for (int a = 0; a < 5; ++a) { t[a] = fmin(fmax(t[a], lo[a]), hi[a]); }
+	return evals;
+}
+
+// FP32 Newton steps on the exact Hessian of the deviance (Fisher scoring where that Hessian is not positive
+// definite), parameters on active bounds held, at most 6, a step that raises the deviance beyond its FP32 rounding halved up to three times; stops at
+// a 1e-6 relative step.
+template <int MODEL, int L>
+__device__ int Polish(const MleParams& mp, const Pix& px, float x0, float y0, float th[5], FacTab<float> xt, FacTab<float> yt)
+{
+	float G[5], Hm[15], Fm[15];
+	float D = Normal<float, MODEL, L, kExact>(mp, px, th, G, Hm, Fm, xt, yt);
+	int evals = 1;
+	if (!isfinite(D)) { return evals; }
+	for (int it = 0; it < 6; ++it) {
+		float rhs[5], dt[5], tt[5];
+		#pragma unroll
+		for (int a = 0; a < 5; ++a) { rhs[a] = -G[a]; }
+		FixActive32<MODEL>(mp, x0, y0, th, G, Hm, rhs);
+		if (!Solve32(Hm, 1.f, rhs, dt, nullptr, false)) {
+			float Hf[15];
+			#pragma unroll
+			for (int a = 0; a < 15; ++a) { Hf[a] = 2.f * Fm[a]; }
+			FixActive32<MODEL>(mp, x0, y0, th, G, Hf, rhs);
+			if (!Solve32(Hf, 1.f, rhs, dt, nullptr, false)) { break; }
+		}
+		bool accepted = false;
+		float Gt[5], Ht[15], Ft[15], Dt = 0.f;
+		const float slack = 1e-5f * (fabsf(D) + 1.f);
+		for (int hv = 0; hv < 4 && !accepted; ++hv) {
+			#pragma unroll
+			for (int a = 0; a < 5; ++a) { tt[a] = th[a] + dt[a]; }
+			Clamp32<MODEL>(mp, x0, y0, tt);
+			Dt = Normal<float, MODEL, L, kExact>(mp, px, tt, Gt, Ht, Ft, xt, yt);
+			++evals;
+			if (isfinite(Dt) && Dt <= D + slack) { accepted = true; }
+			else {
+				#pragma unroll
+				for (int a = 0; a < 5; ++a) { dt[a] *= 0.5f; }
+			}
+		}
+		if (!accepted) { break; }
+		float step = 0.f;
+		#pragma unroll
+		for (int a = 0; a < 5; ++a) { step = fmaxf(step, fabsf(tt[a] - th[a]) / fmaxf(fabsf(th[a]), 1.f)); }
+		#pragma unroll
+		for (int a = 0; a < 5; ++a) { th[a] = tt[a]; G[a] = Gt[a]; }
+		#pragma unroll
+		for (int a = 0; a < 15; ++a) { Hm[a] = Ht[a]; Fm[a] = Ft[a]; }
+		D = Dt;
+		if (step < 1e-6f) { break; }
+	}
+	return evals;
+}
+
+// FP64 deviance and Fisher information at t; CRLB = sqrt(diag(F^-1)). False when either is unusable.
+template <int MODEL, int L>
+__device__ bool Final(const MleParams& mp, const Pix& px, const double t[5], double crlb[5], FacTab<double> xt, FacTab<double> yt)
+{
+	double Fm[15];
+	const double D = Normal<double, MODEL, L, kFinal>(mp, px, t, nullptr, nullptr, Fm, xt, yt);
+	if (!isfinite(D)) { return false; }
+	#pragma unroll
+	for (int a = 0; a < 5; ++a) {
+		double e[5] = {0, 0, 0, 0, 0}, cv[5];
+		e[a] = 1.0;
+		if (!Chol5<double>(Fm, 1.0, e, cv, nullptr)) { return false; }
+		crlb[a] = cv[a] > 0 ? sqrt(cv[a]) : 0.0;
+	}
+	#pragma unroll
+	for (int a = 0; a < 5; ++a) {
+		if (!isfinite(t[a])) { return false; }
+	}
+	return true;
+}
+
+// Output row; col < 0: the calling thread writes all 18 columns, else only column col.
+__device__ void StoreMleRow(double* row, int col, const MleParams& mp, const Cand& cd, const double t[5], const double crlb[5],
                             unsigned long long ux, unsigned long long uy, bool ok)
 {
 	double v[kCols];
@@ -241,8 +665,8 @@ __device__ void StoreMleRow(double* row, int lane, const MleParams& mp, const Ca
 		double sx = t[4], sy = t[4], z = 0, qz = -1;
 		if (mp.model == 7) {
 			double d1, d2;
-			AstigSigma<double>(mp.astig, mp.pixelSize, t[4], sx, d1);
-			AstigSigma<double>(mp.astig + 5, mp.pixelSize, t[4], sy, d2);
+			AstigSigma<double>(mp.astig, mp.pixelSize, t[4], sx, d1, d2);
+			AstigSigma<double>(mp.astig + 5, mp.pixelSize, t[4], sy, d1, d2);
 			z = t[4];
 			qz = crlb[4];
 		}
@@ -258,213 +682,410 @@ __device__ void StoreMleRow(double* row, int lane, const MleParams& mp, const Ca
 		v[cCircularity] = (sx > kEps && sy > kEps) ? fmin(sx, sy) / fmax(sx, sy) : 1;
 	}
 	v[cSegIntensity] = cd.intensity; v[cSurface] = cd.surf;
-	#pragma unroll
-	for (int c = 0; c < kCols; ++c) {
-		if (lane == c) { row[c] = v[c]; }
+	if (col < 0) {
+		#pragma unroll
+		for (int c = 0; c < kCols; ++c) { row[c] = v[c]; }
+	}
+	else {
+		#pragma unroll
+		for (int c = 0; c < kCols; ++c) {
+			if (col == c) { row[c] = v[c]; }
+		}
 	}
 }
 
-template <int MODEL, int L>
-__global__ void __launch_bounds__(kThreads) MleKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
-                                                      const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
-                                                      MleParams mp, double* rows)
+__device__ __forceinline__ uint32_t CandCount(const uint32_t* nptr, uint32_t nconst) { return nptr ? *nptr : nconst; }
+
+// ---------------------------------------------------------------------------------------------------------------
+// Thread per ROI.
+
+// Initial values; shared memory: per thread the FP64 column values of the axial pre-scan (roi doubles).
+template <int MODEL>
+__global__ void __launch_bounds__(kThreads) MleInitKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
+                                                          const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
+                                                          MleParams mp, double* rows)
 {
-	constexpr int kGroups = kThreads / L;
-	__shared__ double scratch[kGroups][6 * kMaxRoi];
-	const int lane = threadIdx.x & 31;
-	const int gIdx = threadIdx.x / L;
-	Group grp;
-	grp.gl = threadIdx.x % L;
-	grp.mask = L == 32 ? 0xffffffffu : (((1u << L) - 1u) << ((lane / L) * L));
-	grp.tab = scratch[gIdx];
-	const uint32_t n = nptr ? *nptr : nconst;
-	const uint32_t first = (blockIdx.x * blockDim.x + threadIdx.x) / L;
-	const uint32_t stride = (gridDim.x * blockDim.x) / L;
-	for (uint32_t k = first; k < n; k += stride) {
-		const Cand cd = cands[k];
+	extern __shared__ __align__(16) unsigned char smem[];
+	const FacTab<double> xt{reinterpret_cast<double*>(smem) + threadIdx.x, static_cast<int>(blockDim.x)};
+	const uint32_t n = CandCount(nptr, nconst);
+	unsigned long long evals = 0;
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
 		double* row = rows + static_cast<long long>(k) * kCols;
-		const bool nonneg = cd.x >= 0.0 && cd.y >= 0.0;
-		const unsigned long long ux = nonneg ? static_cast<unsigned long long>(cd.x) : 0ull;
-		const unsigned long long uy = nonneg ? static_cast<unsigned long long>(cd.y) : 0ull;
-		const unsigned long long hh = static_cast<unsigned long long>(mp.half);
-		double t[5] = {0, 0, 0, 0, 0}, crlb[5] = {0, 0, 0, 0, 0};
-		const int rowLane = L == 32 ? lane : grp.gl;  // lanes of the group write the row columns
-		if (!nonneg || hh > ux || ux >= static_cast<unsigned long long>(W) - hh || hh > uy || uy >= static_cast<unsigned long long>(H) - hh) {
-			if (L >= kCols) { StoreMleRow(row, rowLane, mp, cd, t, crlb, ux, uy, false); }
-			else if (grp.gl == 0) { for (int c = 0; c < kCols; ++c) { StoreMleRow(row, c, mp, cd, t, crlb, ux, uy, false); } }
+		RoiAt r;
+		if (!Locate(img, H, W, N, mp, cands[k], r)) {
+			row[kStatusCol] = kStBorder;
 			continue;
 		}
-		const uint16_t* base = img + static_cast<long long>(cd.frame) * N + static_cast<long long>(uy - hh) * W + static_cast<long long>(ux - hh);
-		// initial values (MleFit in the oracle): bg = min photons, I = photons above it, x, y = centroid
-		float dmin = 3e38f, dsum = 0.f;
-		for (int idx = grp.gl; idx < mp.n; idx += L) {
-			const int i = idx / mp.roi, j = idx - i * mp.roi;
-			const float d = fmaxf((float(__ldg(base + static_cast<long long>(i) * W + j)) - float(mp.offset)) * float(1.0 / mp.gain), 0.f);
-			dmin = fminf(dmin, d);
-			dsum += d;
-		}
+		const Pix px = MakePix(mp, r.base, W, nullptr, 0);
+		double t[5];
+		evals += InitTheta<MODEL, 1>(mp, px, r, t, xt, xt);
 		#pragma unroll
-		for (int d = L / 2; d > 0; d >>= 1) {
-			dmin = fminf(dmin, __shfl_xor_sync(grp.mask, dmin, d));
-			dsum += __shfl_xor_sync(grp.mask, dsum, d);
-		}
-		const double x0 = cd.x - static_cast<double>(ux), y0 = cd.y - static_cast<double>(uy);
-		double lo[5], hi[5];
-		const double hf = static_cast<double>(mp.half);
-		lo[0] = 1e-3; hi[0] = 1e6; lo[1] = 1.0; hi[1] = 1e9;
-		lo[2] = fmax(x0 - 2.0, -hf); hi[2] = fmin(x0 + 2.0, hf);
-		lo[3] = fmax(y0 - 2.0, -hf); hi[3] = fmin(y0 + 2.0, hf);
-		if (MODEL == 6) { lo[4] = 0.5; hi[4] = 5.0; }
-		else if (MODEL == 7) { lo[4] = mp.zMin; hi[4] = mp.zMax; }
-		else { lo[4] = 0.0; hi[4] = static_cast<double>(mp.sz) - 1e-6; }
-		float th[5];
-		th[0] = fmaxf(dmin, 1e-3f);
-		th[1] = fmaxf(dsum - th[0] * float(mp.n), 1.f);
-		th[2] = float(x0);
-		th[3] = float(y0);
-		if (MODEL == 6) { th[4] = float(mp.sigma0); }
-		else {
-			// axial pre-scan in FP64, as in the oracle, so that both start from the same basin
-			const int ns = MODEL == 7 ? 16 : 8;
-			double tsd[5] = {double(th[0]), double(th[1]), double(th[2]), double(th[3]), 0.0};
-			double best = 1e300, bz = 0.5 * (lo[4] + hi[4]);
-			for (int s = 0; s < ns; ++s) {
-				tsd[4] = lo[4] + (hi[4] - lo[4]) * (s + 0.5) / ns;
-				const double D = Normal<double, MODEL, L, false>(mp, base, W, tsd, nullptr, nullptr, grp);
-				if (D < best) { best = D; bz = tsd[4]; }
+		for (int a = 0; a < 5; ++a) { row[a] = t[a]; }
+		row[kStatusCol] = kStOk;
+	}
+	if (mp.evals && evals) { atomicAdd(mp.evals + 2, evals); }
+}
+
+// Persistent FP32 LM. Warp w owns candidates [w * chunk, (w + 1) * chunk); a lane whose fit ends takes the next one of
+// the range. Every pass of the loop makes each busy lane evaluate the deviance, gradient and Fisher matrix once: at
+// the start point of a new candidate, or at the trial point of an LM step. Shared memory per lane: the ROI photons
+// (n floats) and the column factors (3 roi floats), lane-interleaved.
+template <int MODEL>
+__global__ void __launch_bounds__(kThreads) MleLmKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
+                                                        const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
+                                                        MleParams mp, double* rows)
+{
+	extern __shared__ __align__(16) unsigned char smem[];
+	const int T = blockDim.x;
+	float* ph = reinterpret_cast<float*>(smem) + threadIdx.x;
+	const FacTab<float> xt{reinterpret_cast<float*>(smem) + mp.n * T + threadIdx.x, T};
+	const uint32_t n = CandCount(nptr, nconst);
+	const int lane = threadIdx.x & 31;
+	const uint32_t warps = gridDim.x * (blockDim.x / 32);
+	const uint32_t gw = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+	const uint32_t chunk = std::max<uint32_t>(32u, (n + warps - 1) / warps);
+	const unsigned long long beginL = static_cast<unsigned long long>(gw) * chunk;
+	if (beginL >= n) { return; }
+	uint32_t cursor = static_cast<uint32_t>(beginL);
+	const uint32_t end = static_cast<uint32_t>(std::min<unsigned long long>(n, beginL + chunk));
+	constexpr uint32_t kNone = 0xffffffffu;
+	uint32_t k = kNone;
+	bool fresh = false;
+	float th[5] = {0, 0, 0, 0, 0}, G[5], Hm[15], D = 0.f, lambda = 1e-3f, x0 = 0.f, y0 = 0.f;
+	int it = 0;
+	unsigned long long evals = 0;
+	Pix px = MakePix(mp, img, W, ph, T);
+	while (true) {
+		// refill idle lanes from the warp's range, in lane order
+		const bool need = k == kNone;
+		const unsigned needMask = __ballot_sync(0xffffffffu, need);
+		if (need) {
+			const uint32_t kk = cursor + __popc(needMask & ((1u << lane) - 1u));
+			if (kk < end && rows[static_cast<long long>(kk) * kCols + kStatusCol] == kStOk) {
+				RoiAt r;
+				Locate(img, H, W, N, mp, cands[kk], r);
+				px.g = r.base;
+				for (int i = 0, q = 0; i < mp.roi; ++i) {
+					for (int j = 0; j < mp.roi; ++j, ++q) {
+						ph[q * T] = fmaxf((float(__ldg(r.base + i * W + j)) - px.off32) * px.inv32, 0.f);
+					}
+				}
+				const double* row = rows + static_cast<long long>(kk) * kCols;
+				#pragma unroll
+				for (int a = 0; a < 5; ++a) { th[a] = static_cast<float>(row[a]); }
+				x0 = static_cast<float>(r.x0);
+				y0 = static_cast<float>(r.y0);
+				k = kk;
+				fresh = true;
 			}
-			th[4] = float(bz);
 		}
+		cursor = std::min<uint32_t>(end, cursor + __popc(needMask));
+		const bool busy = k != kNone;
+		if (__ballot_sync(0xffffffffu, busy) == 0) {
+			if (cursor >= end) { break; }
+			continue;
+		}
+		
+		float tt[5];
+		bool eval = false, finish = false, failed = false;
+		if (busy) {
+			if (fresh) {
+				#pragma unroll
+				for (int a = 0; a < 5; ++a) { tt[a] = th[a]; }
+				eval = true;
+			}
+			else {
+				float rhs[5], dt[5];
+				#pragma unroll
+				for (int a = 0; a < 5; ++a) { rhs[a] = -G[a]; }
+				FixActive32<MODEL>(mp, x0, y0, th, G, Hm, rhs);  // in place: Hm is replaced when a step is accepted
+				if (Solve32(Hm, 1.f + lambda, rhs, dt, mp.fallbacks, true)) {
+					#pragma unroll
+					for (int a = 0; a < 5; ++a) { tt[a] = th[a] + dt[a]; }
+					Clamp32<MODEL>(mp, x0, y0, tt);
+					eval = true;
+				}
+				else {
+					++it;
+					lambda *= 10.f;
+					finish = lambda > 1e7f || it >= mp.maxIter;
+				}
+			}
+		}
+		float Gt[5], Ht[15], Dt = 0.f;
+		if (eval) {
+			Dt = Normal<float, MODEL, 1, kFisher>(mp, px, tt, Gt, Ht, nullptr, xt, xt);
+			++evals;
+		}
+		if (eval) {
+			if (fresh) {
+				fresh = false;
+				D = Dt;
+				#pragma unroll
+				for (int a = 0; a < 5; ++a) { G[a] = Gt[a]; }
+				#pragma unroll
+				for (int a = 0; a < 15; ++a) { Hm[a] = Ht[a]; }
+				lambda = 1e-3f;
+				it = 0;
+				failed = !isfinite(D);
+				finish = failed || mp.maxIter <= 0;
+			}
+			else {
+				++it;
+				if (isfinite(Dt) && Dt < D) {
+					const bool small = StepSmall(MODEL, th, tt);
+					#pragma unroll
+					for (int a = 0; a < 5; ++a) { th[a] = tt[a]; G[a] = Gt[a]; }
+					#pragma unroll
+					for (int a = 0; a < 15; ++a) { Hm[a] = Ht[a]; }
+					D = Dt;
+					lambda = fmaxf(lambda * 0.1f, 1e-7f);
+					finish = small;
+				}
+				else {
+					lambda *= 10.f;
+					finish = lambda > 1e7f;
+				}
+				finish = finish || it >= mp.maxIter;
+			}
+		}
+		if (finish) {
+			double* row = rows + static_cast<long long>(k) * kCols;
+			#pragma unroll
+			for (int a = 0; a < 5; ++a) { row[a] = th[a]; }
+			row[kStatusCol] = failed ? kStFailed : kStOk;
+			k = kNone;
+		}
+	}
+	if (mp.evals && evals) { atomicAdd(mp.evals, evals); }
+}
+
+// FP32 Newton polish, FP64 deviance, Fisher information and CRLB, output row. Shared memory: the column factors, in
+// two separate lane-interleaved regions - 6 roi floats per thread for the polish, then 3 roi doubles per thread for
+// the FP64 pass. (One region for both would not do: with 4- and 8-byte entries interleaved over the threads, a
+// thread that reaches the FP64 pass early would overwrite the FP32 entries of threads still polishing.)
+template <int MODEL>
+__global__ void __launch_bounds__(kThreads) MlePolishKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
+                                                            const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
+                                                            MleParams mp, double* rows)
+{
+	extern __shared__ __align__(16) unsigned char smem[];
+	const int T = blockDim.x;
+	double* region64 = reinterpret_cast<double*>(smem);
+	float* region32 = reinterpret_cast<float*>(region64 + 3 * mp.roi * T);
+	const FacTab<float> xt32{region32 + threadIdx.x, T};
+	const FacTab<double> xt64{region64 + threadIdx.x, T};
+	const uint32_t n = CandCount(nptr, nconst);
+	unsigned long long evals32 = 0, evals64 = 0;
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		double* row = rows + static_cast<long long>(k) * kCols;
+		const Cand cd = cands[k];
+		const double status = row[kStatusCol];
+		RoiAt r;
+		double t[5] = {0, 0, 0, 0, 0}, crlb[5] = {0, 0, 0, 0, 0};
+		const bool inside = Locate(img, H, W, N, mp, cd, r);
+		bool ok = inside && status == kStOk;
+		if (ok) {
+			const Pix px = MakePix(mp, r.base, W, nullptr, 0);
+			float th[5];
+			#pragma unroll
+			for (int a = 0; a < 5; ++a) { th[a] = static_cast<float>(row[a]); }
+			evals32 += Polish<MODEL, 1>(mp, px, static_cast<float>(r.x0), static_cast<float>(r.y0), th, xt32, xt32);
+			#pragma unroll
+			for (int a = 0; a < 5; ++a) { t[a] = th[a]; }
+			ok = Final<MODEL, 1>(mp, px, t, crlb, xt64, xt64);
+			++evals64;
+		}
+		StoreMleRow(row, -1, mp, cd, t, crlb, r.ux, r.uy, ok);
+	}
+	if (mp.evals && evals32) { atomicAdd(mp.evals + 1, evals32); }
+	if (mp.evals && evals64) { atomicAdd(mp.evals + 2, evals64); }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Warp per ROI: all phases in one launch.
+
+struct WarpSmem {
+	float photons[kMaxPix];
+	double xt[6 * kMaxRoi];
+	double yt[6 * kMaxRoi];
+};
+
+template <int MODEL>
+__global__ void __launch_bounds__(kThreads) MleWarpKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
+                                                          const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
+                                                          MleParams mp, double* rows)
+{
+	__shared__ WarpSmem sm[kThreads / 32];
+	WarpSmem& ws = sm[threadIdx.x / 32];
+	const FacTab<float> xt32{reinterpret_cast<float*>(ws.xt), 1}, yt32{reinterpret_cast<float*>(ws.yt), 1};
+	const FacTab<double> xt64{ws.xt, 1}, yt64{ws.yt, 1};
+	const int lane = threadIdx.x & 31;
+	const uint32_t n = CandCount(nptr, nconst);
+	const uint32_t warps = gridDim.x * (blockDim.x / 32);
+	unsigned long long ev[3] = {0, 0, 0};
+	for (uint32_t k = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; k < n; k += warps) {
+		const Cand cd = cands[k];
+		double* row = rows + static_cast<long long>(k) * kCols;
+		double t[5] = {0, 0, 0, 0, 0}, crlb[5] = {0, 0, 0, 0, 0};
+		RoiAt r;
+		if (!Locate(img, H, W, N, mp, cd, r)) {
+			StoreMleRow(row, lane, mp, cd, t, crlb, r.ux, r.uy, false);
+			continue;
+		}
+		Pix px = MakePix(mp, r.base, W, nullptr, 0);
+		ev[2] += InitTheta<MODEL, 32>(mp, px, r, t, xt64, yt64);
+		for (int q = lane; q < mp.n; q += 32) {
+			const int i = q / mp.roi, j = q - i * mp.roi;
+			ws.photons[q] = fmaxf((float(__ldg(r.base + i * W + j)) - px.off32) * px.inv32, 0.f);
+		}
+		__syncwarp();
+		Pix ps = px;
+		ps.sm = ws.photons;
+		ps.ss = 1;
+		const float x0 = static_cast<float>(r.x0), y0 = static_cast<float>(r.y0);
+		float th[5];
 		#pragma unroll
-		for (int a = 0; a < 5; ++a) { th[a] = fminf(fmaxf(th[a], float(lo[a])), float(hi[a])); }
+		for (int a = 0; a < 5; ++a) { th[a] = static_cast<float>(t[a]); }
 		float G[5], Hm[15];
-		float D = Normal<float, MODEL, L, true>(mp, base, W, th, G, Hm, grp);
+		float D = Normal<float, MODEL, 32, kFisher>(mp, ps, th, G, Hm, nullptr, xt32, yt32);
+		++ev[0];
 		bool ok = isfinite(D);
 		float lambda = 1e-3f;
 		for (int it = 0; ok && it < mp.maxIter; ++it) {
 			float rhs[5], dt[5];
 			#pragma unroll
 			for (int a = 0; a < 5; ++a) { rhs[a] = -G[a]; }
-			float ratio = 0.f;
-			bool solved = Chol5<float>(Hm, 1.f + lambda, rhs, dt, &ratio);
-			if (!solved || ratio < 1e-5f) {
-				// FP64 re-factorisation of the same damped system
-				double Hd[15], rd[5], xd[5];
-				#pragma unroll
-				for (int a = 0; a < 15; ++a) { Hd[a] = Hm[a]; }
-				#pragma unroll
-				for (int a = 0; a < 5; ++a) { rd[a] = rhs[a]; }
-				solved = Chol5<double>(Hd, 1.0 + lambda, rd, xd, nullptr);
-				if (grp.gl == 0 && mp.fallbacks) { atomicAdd(mp.fallbacks, 1u); }
-				#pragma unroll
-				for (int a = 0; a < 5; ++a) { dt[a] = float(xd[a]); }
-			}
-			if (!solved) {
+			FixActive32<MODEL>(mp, x0, y0, th, G, Hm, rhs);
+			if (!Solve32(Hm, 1.f + lambda, rhs, dt, mp.fallbacks, lane == 0)) {
 				lambda *= 10.f;
 				if (lambda > 1e7f) { break; }
 				continue;
 			}
 			float tt[5];
 			#pragma unroll
-			for (int a = 0; a < 5; ++a) { tt[a] = fminf(fmaxf(th[a] + dt[a], float(lo[a])), float(hi[a])); }
+			for (int a = 0; a < 5; ++a) { tt[a] = th[a] + dt[a]; }
+			Clamp32<MODEL>(mp, x0, y0, tt);
 			float Gt[5], Ht[15];
-			const float Dt = Normal<float, MODEL, L, true>(mp, base, W, tt, Gt, Ht, grp);
+			const float Dt = Normal<float, MODEL, 32, kFisher>(mp, ps, tt, Gt, Ht, nullptr, xt32, yt32);
+			++ev[0];
 			if (isfinite(Dt) && Dt < D) {
-				const float gainRel = (D - Dt) / (Dt + 1.f);
+				const bool small = StepSmall(MODEL, th, tt);
 				#pragma unroll
 				for (int a = 0; a < 5; ++a) { th[a] = tt[a]; G[a] = Gt[a]; }
 				#pragma unroll
 				for (int a = 0; a < 15; ++a) { Hm[a] = Ht[a]; }
 				D = Dt;
 				lambda = fmaxf(lambda * 0.1f, 1e-7f);
-				if (gainRel < 1e-6f) { break; }
+				if (small) { break; }
 			}
 			else {
 				lambda *= 10.f;
 				if (lambda > 1e7f) { break; }
 			}
 		}
-		// FP64: undamped Fisher steps to a 1e-10 relative step (at most 10, halving a step that does not lower the
-		// deviance up to three times), then the CRLB
-		#pragma unroll
-		for (int a = 0; a < 5; ++a) { t[a] = th[a]; }
-		double Gd[5], Hd[15];
-		double Dd = Normal<double, MODEL, L, true>(mp, base, W, t, Gd, Hd, grp);
-		ok = ok && isfinite(Dd);
-		for (int it = 0; ok && it < 10; ++it) {
-			double rhs[5], dt[5], tt[5];
-			#pragma unroll
-			for (int a = 0; a < 5; ++a) { rhs[a] = -Gd[a]; }
-			if (!Chol5<double>(Hd, 1.0, rhs, dt, nullptr)) { break; }
-			bool accepted = false;
-			double Gt[5], Ht[15], Dt = 0;
-			for (int hv = 0; hv < 4 && !accepted; ++hv) {
-				#pragma unroll
-				for (int a = 0; a < 5; ++a) { tt[a] = fmin(fmax(t[a] + dt[a], lo[a]), hi[a]); }
-				Dt = Normal<double, MODEL, L, true>(mp, base, W, tt, Gt, Ht, grp);
-				if (isfinite(Dt) && Dt <= Dd) { accepted = true; }
-				else {
-					#pragma unroll
-					for (int a = 0; a < 5; ++a) { dt[a] *= 0.5; }
-				}
-			}
-			if (!accepted) { break; }
-			double step = 0;
-			#pragma unroll
-			for (int a = 0; a < 5; ++a) { step = fmax(step, fabs(tt[a] - t[a]) / fmax(fabs(t[a]), 1.0)); }
-			#pragma unroll
-			for (int a = 0; a < 5; ++a) { t[a] = tt[a]; Gd[a] = Gt[a]; }
-			#pragma unroll
-			for (int a = 0; a < 15; ++a) { Hd[a] = Ht[a]; }
-			Dd = Dt;
-			if (step < 1e-10) { break; }
-		}
 		if (ok) {
-			double F[15];
+			ev[1] += Polish<MODEL, 32>(mp, ps, x0, y0, th, xt32, yt32);
 			#pragma unroll
-			for (int a = 0; a < 15; ++a) { F[a] = 0.5 * Hd[a]; }
-			#pragma unroll
-			for (int a = 0; a < 5; ++a) {
-				double e[5] = {0, 0, 0, 0, 0}, col[5];
-				e[a] = 1.0;
-				if (!Chol5<double>(F, 1.0, e, col, nullptr)) { ok = false; break; }
-				crlb[a] = col[a] > 0 ? sqrt(col[a]) : 0.0;
-			}
+			for (int a = 0; a < 5; ++a) { t[a] = th[a]; }
+			ok = Final<MODEL, 32>(mp, px, t, crlb, xt64, yt64);
+			++ev[2];
 		}
+		__syncwarp();  // photons are rewritten for the next candidate
+		StoreMleRow(row, lane, mp, cd, t, crlb, r.ux, r.uy, ok);
+	}
+	if (mp.evals && lane == 0) {
 		#pragma unroll
-		for (int a = 0; a < 5; ++a) { ok = ok && isfinite(t[a]); }
-		if (L >= kCols) { StoreMleRow(row, rowLane, mp, cd, t, crlb, ux, uy, ok); }
-		else if (grp.gl == 0) {
-			for (int c = 0; c < kCols; ++c) { StoreMleRow(row, c, mp, cd, t, crlb, ux, uy, ok); }
+		for (int a = 0; a < 3; ++a) {
+			if (ev[a]) { atomicAdd(mp.evals + a, ev[a]); }
 		}
 	}
 }
 
-template <int MODEL>
-bool LaunchModel(int lanes, const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr,
-                 uint32_t nconst, uint32_t cap, const MleParams& mp, double* rows, cudaStream_t st)
+// ---------------------------------------------------------------------------------------------------------------
+
+int SmCount()
 {
-	const uint32_t perBlock = kThreads / lanes;
-	const uint32_t blocks = std::min<uint32_t>((std::max<uint32_t>(cap, 1) + perBlock - 1) / perBlock, 148u * 32u);
-	switch (lanes) {
-		case 1: MleKernel<MODEL, 1><<<blocks, kThreads, 0, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows); break;
-		case 8: MleKernel<MODEL, 8><<<blocks, kThreads, 0, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows); break;
-		case 16: MleKernel<MODEL, 16><<<blocks, kThreads, 0, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows); break;
-		default: MleKernel<MODEL, 32><<<blocks, kThreads, 0, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows); break;
+	int dev = 0, sms = 148;
+	if (cudaGetDevice(&dev) == cudaSuccess) { cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev); }
+	return sms;
+}
+
+template <typename K>
+void AllowSmem(K kernel, size_t bytes)
+{
+	if (bytes > 48 * 1024) { cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)); }
+}
+
+// marks (profiling, or null): 4 events recorded before the initial values, the LM, the polish and after it.
+template <int MODEL>
+bool LaunchThreadPerRoi(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
+                        uint32_t cap, const MleParams& mp, double* rows, cudaEvent_t* marks, cudaStream_t st)
+{
+	const int sms = SmCount();
+	const uint32_t blocks = std::min<uint32_t>((std::max<uint32_t>(cap, 1) + kThreads - 1) / kThreads, static_cast<uint32_t>(sms) * 32u);
+	const size_t initBytes = static_cast<size_t>(mp.roi) * sizeof(double) * kThreads;
+	const size_t lmBytes = static_cast<size_t>(mp.n + 3 * mp.roi) * sizeof(float) * kThreads;
+	const size_t polishBytes = static_cast<size_t>(3 * mp.roi) * (sizeof(double) + 2 * sizeof(float)) * kThreads;
+	AllowSmem(MleLmKernel<MODEL>, lmBytes);
+	int perSm = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, MleLmKernel<MODEL>, kThreads, lmBytes) != cudaSuccess || perSm < 1) {
+		perSm = 1;
+	}
+	const uint32_t lmBlocks = std::min<uint32_t>(blocks, static_cast<uint32_t>(sms * perSm));
+	if (marks) { cudaEventRecord(marks[0], st); }
+	MleInitKernel<MODEL><<<blocks, kThreads, initBytes, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows);
+	if (marks) { cudaEventRecord(marks[1], st); }
+	MleLmKernel<MODEL><<<lmBlocks, kThreads, lmBytes, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows);
+	if (marks) { cudaEventRecord(marks[2], st); }
+	MlePolishKernel<MODEL><<<blocks, kThreads, polishBytes, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows);
+	if (marks) { cudaEventRecord(marks[3], st); }
+	CountLaunch(3);
+	return PTB_LAUNCHED();
+}
+
+// marks: the single launch is timed as the LM phase (marks 0-2 before it, mark 3 after it).
+template <int MODEL>
+bool LaunchWarpPerRoi(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
+                      uint32_t cap, const MleParams& mp, double* rows, cudaEvent_t* marks, cudaStream_t st)
+{
+	const uint32_t perBlock = kThreads / 32;
+	const uint32_t blocks = std::min<uint32_t>((std::max<uint32_t>(cap, 1) + perBlock - 1) / perBlock, static_cast<uint32_t>(SmCount()) * 32u);
+	if (marks) {
+		cudaEventRecord(marks[0], st);
+		cudaEventRecord(marks[1], st);
+	}
+	MleWarpKernel<MODEL><<<blocks, kThreads, 0, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows);
+	if (marks) {
+		cudaEventRecord(marks[2], st);
+		cudaEventRecord(marks[3], st);
 	}
 	CountLaunch();
 	return PTB_LAUNCHED();
 }
 
+template <int MODEL>
+bool LaunchModel(int lanes, const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr,
+                 uint32_t nconst, uint32_t cap, const MleParams& mp, double* rows, cudaEvent_t* marks, cudaStream_t st)
+{
+	if (lanes == 1) { return LaunchThreadPerRoi<MODEL>(img, H, W, N, cands, nptr, nconst, cap, mp, rows, marks, st); }
+	return LaunchWarpPerRoi<MODEL>(img, H, W, N, cands, nptr, nconst, cap, mp, rows, marks, st);
+}
+
 }  // namespace
 
+// lanes: 1 = thread per ROI, anything else = warp per ROI. marks: profiling events (4) or null.
 bool LaunchMle(int lanes, const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
-               uint32_t cap, const MleParams& mp, double* rows, cudaStream_t st)
+               uint32_t cap, const MleParams& mp, double* rows, cudaEvent_t* marks, cudaStream_t st)
 {
+	if (mp.roi < 1 || mp.roi > kMaxRoi) {
+		SetError("MLE fit: ROI size must be 1-15");
+		return false;
+	}
 	switch (mp.model) {
-		case 6: return LaunchModel<6>(lanes, img, H, W, N, cands, nptr, nconst, cap, mp, rows, st);
-		case 7: return LaunchModel<7>(lanes, img, H, W, N, cands, nptr, nconst, cap, mp, rows, st);
-		case 8: return LaunchModel<8>(lanes, img, H, W, N, cands, nptr, nconst, cap, mp, rows, st);
+		case 6: return LaunchModel<6>(lanes, img, H, W, N, cands, nptr, nconst, cap, mp, rows, marks, st);
+		case 7: return LaunchModel<7>(lanes, img, H, W, N, cands, nptr, nconst, cap, mp, rows, marks, st);
+		case 8: return LaunchModel<8>(lanes, img, H, W, N, cands, nptr, nconst, cap, mp, rows, marks, st);
 		default: return false;
 	}
 }

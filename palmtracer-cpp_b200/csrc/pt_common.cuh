@@ -78,8 +78,10 @@ struct MleParams {
 	double astig[10];
 	int sx, sy, sz;
 	double dz;
-	const float* table;        // mode 8: cell-major [cell][64], FP32
+	const float* table;        // mode 8: cell-major [cell][64], FP32 (FP32 phases)
+	const double* table64;     // mode 8: the same in FP64 (FP64 phases)
 	unsigned int* fallbacks;   // FP64 Cholesky re-factorisations (diagnostics)
+	unsigned long long* evals; // profiling, or null: model evaluations [FP32 LM, FP32 polish, FP64 pre-scan + final]
 };
 
 // Fit configuration passed by value to the fit kernels.
@@ -97,7 +99,8 @@ struct FitParams {
 	double roiParam, initZ, deltaZ, intensityRatio;
 	const double* coeffs;  // device, cell-major [cell][64]
 	MleParams mle;         // modes 6-8
-	int lanes;             // ROI lane-group width for modes 6-8 (autotuned)
+	int lanes;             // ROI mapping for modes 6-8: 1 thread per ROI, else warp per ROI (autotuned)
+	cudaEvent_t* marks;    // profiling, or null: 4 events recorded around the phases of the modes 6-8 fit
 };
 
 // Geometry of one chunk: B frames of H x W pixels; global pixel index g = f * N + y * W + x (fits in 31 bits).

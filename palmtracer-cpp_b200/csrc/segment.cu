@@ -72,30 +72,49 @@ __device__ __forceinline__ uint32_t CompOf(const uint32_t* par, uint32_t p)
 	return __ldcg(par + x) & ~kCompTag;
 }
 
+// 8-connectivity decision tree over the raster-earlier neighbours a = (y-1, x-1), b = (y-1, x), c = (y-1, x+1),
+// d = (y, x-1): a pixel links to one of them at initialisation; only c together with a or d (b absent) joins two
+// trees that are not yet known to touch, which is the single union left for CclUnion.
+__device__ __forceinline__ void EarlierNeighbours(const Workspace& ws, uint32_t p, uint32_t& link, uint32_t& extra)
+{
+	const Pix q = Decompose(p, ws.g);
+	const uint32_t W = static_cast<uint32_t>(ws.g.W);
+	const bool up = q.y > 0, left = q.x > 0, right = q.x + 1 < ws.g.W;
+	const bool a = up && left && (ws.code[p - W - 1] & kDomain);
+	const bool b = up && (ws.code[p - W] & kDomain);
+	const bool c = up && right && (ws.code[p - W + 1] & kDomain);
+	const bool d = left && (ws.code[p - 1] & kDomain);
+	link = p;
+	extra = p;
+	if (b) { link = p - W; }
+	else if (c) {
+		link = p - W + 1;
+		if (a) { extra = p - W - 1; }
+		else if (d) { extra = p - 1; }
+	}
+	else if (a) { link = p - W - 1; }
+	else if (d) { link = p - 1; }
+}
+
 __global__ void CclInit(Workspace ws)
 {
 	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
 	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
 		const uint32_t p = ws.dom[k];
-		ws.par[p] = p;
+		uint32_t link, extra;
+		EarlierNeighbours(ws, p, link, extra);
+		ws.par[p] = link;
 	}
 }
 
 __global__ void CclUnion(Workspace ws)
 {
 	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
-	const Geometry& geo = ws.g;
 	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
 		const uint32_t p = ws.dom[k];
-		const Pix q = Decompose(p, geo);
-		// raster-earlier neighbours: (y-1, x-1), (y-1, x), (y-1, x+1), (y, x-1)
-		if (q.y > 0) {
-			const uint32_t up = p - static_cast<uint32_t>(geo.W);
-			if (q.x > 0 && (ws.code[up - 1] & kDomain)) { Unite(ws.par, p, up - 1); }
-			if (ws.code[up] & kDomain) { Unite(ws.par, p, up); }
-			if (q.x + 1 < geo.W && (ws.code[up + 1] & kDomain)) { Unite(ws.par, p, up + 1); }
-		}
-		if (q.x > 0 && (ws.code[p - 1] & kDomain)) { Unite(ws.par, p, p - 1); }
+		uint32_t link, extra;
+		EarlierNeighbours(ws, p, link, extra);
+		if (extra != p) { Unite(ws.par, p, extra); }
 	}
 }
 

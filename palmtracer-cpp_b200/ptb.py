@@ -15,7 +15,7 @@ COLS = 18
 # every symbol the public header declares
 EXPORTS = ["Localization", "Fitting", "Wavelett", "AutoThreshold", "PTB_LocalizationDevice",
            "PTB_SetSegmentationMode", "PTB_SetFitPrecision", "PTB_LastError", "PTB_KernelLaunchCount",
-           "PTB_SetProfiling", "PTB_StageTimes", "PTB_MeasureFmaPeak"]
+           "PTB_SetProfiling", "PTB_StageTimes", "PTB_MleEvaluations", "PTB_MeasureFmaPeak"]
 
 _u16p = ctypes.POINTER(ctypes.c_uint16)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -56,6 +56,8 @@ def load(path=LIB_PATH):
     L.PTB_SetProfiling.argtypes = [ctypes.c_int]
     L.PTB_StageTimes.restype = None
     L.PTB_StageTimes.argtypes = [_f64p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
+    L.PTB_MleEvaluations.restype = None
+    L.PTB_MleEvaluations.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
     L.PTB_MeasureFmaPeak.restype = _f64
     L.PTB_MeasureFmaPeak.argtypes = [ctypes.c_int]
     _lib = L
@@ -147,7 +149,7 @@ def launch_count():
     return load().PTB_KernelLaunchCount()
 
 
-STAGES = ["detect", "segment", "fit", "finish", "copies"]
+STAGES = ["detect", "segment", "fit", "finish", "copies", "fit_init", "fit_lm", "fit_polish"]
 
 
 def set_profiling(enable):
@@ -156,12 +158,22 @@ def set_profiling(enable):
 
 def stage_times():
     """{stage: (ms, launches)} accumulated since the last call (profiling must be on)."""
-    ms = np.zeros(5)
-    launches = np.zeros(5, dtype=np.uint64)
-    load().PTB_StageTimes(ms.ctypes.data_as(_f64p), launches.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 5)
+    n = len(STAGES)
+    ms = np.zeros(n)
+    launches = np.zeros(n, dtype=np.uint64)
+    load().PTB_StageTimes(ms.ctypes.data_as(_f64p), launches.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), n)
     return {k: (float(ms[i]), int(launches[i])) for i, k in enumerate(STAGES)}
+
+
+def mle_evaluations():
+    """{"lm": FP32 LM evaluations, "polish": FP32 polish evaluations, "fp64": FP64 evaluations} counted while
+    profiling was on (modes 6-8), since the last call."""
+    out = np.zeros(3, dtype=np.uint64)
+    load().PTB_MleEvaluations(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 3)
+    return {"lm": int(out[0]), "polish": int(out[1]), "fp64": int(out[2])}
 
 
 def fma_peak(fp64):
     """Measured FMA FLOP/s of the current device (FP64 when fp64 is true, else FP32)."""
     return load().PTB_MeasureFmaPeak(int(bool(fp64)))
+

@@ -22,8 +22,9 @@ def theta_to_degrees(rows, fit):
     return rows
 
 
-def match_rows(actual, expected, atol=1e-3, rtol=1e-5, columns=None):
-    """Returns (n_bad_rows, worst_excess, pairs). ``pairs`` maps each actual row to its matched expected row."""
+def match_rows(actual, expected, atol=1e-3, rtol=1e-5, columns=None, keys=(C_X, C_Y, C_Z)):
+    """Returns (n_bad_rows, worst_excess, pairs). ``pairs`` maps each actual row to its matched expected row;
+    ``keys`` are the columns of the nearest-row distance (X, Y, Z as in the reference test; X, Y where Z is in nm)."""
     actual = np.asarray(actual, dtype=np.float64).reshape(-1, COLS)
     expected = np.asarray(expected, dtype=np.float64).reshape(-1, COLS)
     if actual.shape[0] != expected.shape[0]:
@@ -43,7 +44,9 @@ def match_rows(actual, expected, atol=1e-3, rtol=1e-5, columns=None):
             worst = np.inf
             continue
         e = expected[cand]
-        d = ((e[:, C_X] - row[C_X]) ** 2 + (e[:, C_Y] - row[C_Y]) ** 2 + (e[:, C_Z] - row[C_Z]) ** 2)
+        d = np.zeros(len(cand))
+        for k in keys:
+            d += (e[:, k] - row[k]) ** 2
         j = cand[int(np.argmin(d))]
         used[j] = True
         pairs[i] = j
