@@ -66,6 +66,20 @@ PTB_API uint64_t PTB_LocalizationDevice(const uint16_t* d_input, double* d_outpu
                                         uint64_t height, uint64_t width, uint64_t planes, double thresholdVal,
                                         double watershedRatio, uint64_t fit, const double* fit_params, void* stream);
 
+/* Fit-only at caller-given positions with no device memory allocation: for callers that cannot call cudaMalloc
+ * (code running inside another runtime's stream callbacks or under a fixed pre-sized memory pool) but can pass device
+ * buffers. No counterpart in the reference; same result as Fitting for the same inputs. d_input is the device stack
+ * uint16 [planes][height][width], d_positions the device rows [nPoints][6] (Id, Plane, X, Y, SegIntensity, Surface),
+ * d_output the device rows [nPoints][18]; fit_params stays a host array. Work is enqueued on `stream` (cudaStream_t,
+ * 0 = legacy default) and the call returns without waiting for it. Limits: at most 65536 points and 65536 planes,
+ * fit modes 0-4, 6 and 7 (the spline modes need a device coefficient table); larger calls return 0 with an error.
+ * Scratch lives in one static device array of about 3 MB that every GPU loading the library keeps until exit; it is
+ * shared by all calls, so calls that overlap on the GPU race. The first call on a device looks up the array's device
+ * address; make that first call before any stream capture. Returns nPoints * 18, or 0 (error or empty input). */
+PTB_API uint64_t PTB_FittingDeviceNoAlloc(const uint16_t* d_input, const double* d_positions, uint64_t nPoints,
+                                          double* d_output, uint64_t height, uint64_t width, uint64_t planes, uint64_t fit,
+                                          const double* fit_params, void* stream);
+
 /* Segmentation mode. 0 (default): each 8-connected component of the thresholded potential is flooded on its own,
  * in parallel. 1 (strict): each frame is flooded as one unit with a frame-global pop counter, exactly as the
  * reference's single priority queue does (Segmentation2D.cpp:336-385); slower, exact for any threshold.

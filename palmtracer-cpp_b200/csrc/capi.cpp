@@ -122,6 +122,29 @@ PTB_API uint64_t PTB_LocalizationDevice(const uint16_t* d_input, double* d_outpu
 	}
 }
 
+PTB_API uint64_t PTB_FittingDeviceNoAlloc(const uint16_t* d_input, const double* d_positions, uint64_t nPoints,
+                                          double* d_output, uint64_t height, uint64_t width, uint64_t planes, uint64_t fit,
+                                          const double* fit_params, void* stream)
+{
+	ptb::ClearError();
+	try {
+		int precision = 0;
+		{
+			std::unique_lock<std::mutex> lock;
+			precision = ptb::EngineFor(lock).Precision();  // reads a setting; initialises no device state
+		}
+		const long long n = ptb::FittingDeviceNoAlloc(d_input, d_positions, nPoints, d_output, height, width, planes, fit,
+		                                              fit_params, precision, ptb::EnvLanes(), static_cast<cudaStream_t>(stream));
+		if (n < 0) { Report("PTB_FittingDeviceNoAlloc"); return 0; }
+		return static_cast<uint64_t>(n);
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("PTB_FittingDeviceNoAlloc");
+		return 0;
+	}
+}
+
 PTB_API int PTB_SetSegmentationMode(int mode)
 {
 	std::unique_lock<std::mutex> lock;

@@ -16,6 +16,9 @@
 namespace ptb {
 
 bool ParseFitParams(uint64_t fit, const double* fp, FitParams& out, std::vector<double>& splineHost);
+long long FittingDeviceNoAlloc(const uint16_t* dStack, const double* dPositions, uint64_t nPoints, double* dOutput,
+                               uint64_t height, uint64_t width, uint64_t planes, uint64_t fit, const double* fitParams,
+                               int precision, int lanes, cudaStream_t st);
 int EnvLanes();
 uint64_t LaunchCount();
 double MeasureFmaPeak(int fp64);

@@ -15,7 +15,7 @@ COLS = 18
 # every symbol the public header declares
 EXPORTS = ["Localization", "Fitting", "Wavelett", "AutoThreshold", "PTB_LocalizationDevice",
            "PTB_SetSegmentationMode", "PTB_SetFitPrecision", "PTB_LastError", "PTB_KernelLaunchCount",
-           "PTB_SetProfiling", "PTB_StageTimes", "PTB_MleEvaluations", "PTB_MeasureFmaPeak"]
+           "PTB_SetProfiling", "PTB_StageTimes", "PTB_MleEvaluations", "PTB_MeasureFmaPeak", "PTB_FittingDeviceNoAlloc"]
 
 _u16p = ctypes.POINTER(ctypes.c_uint16)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -58,6 +58,9 @@ def load(path=LIB_PATH):
     L.PTB_StageTimes.argtypes = [_f64p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
     L.PTB_MleEvaluations.restype = None
     L.PTB_MleEvaluations.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
+    L.PTB_FittingDeviceNoAlloc.restype = _u64
+    L.PTB_FittingDeviceNoAlloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _u64, ctypes.c_void_p, _u64, _u64, _u64, _u64,
+                                           _f64p, ctypes.c_void_p]
     L.PTB_MeasureFmaPeak.restype = _f64
     L.PTB_MeasureFmaPeak.argtypes = [ctypes.c_int]
     _lib = L
@@ -177,3 +180,11 @@ def fma_peak(fp64):
     """Measured FMA FLOP/s of the current device (FP64 when fp64 is true, else FP32)."""
     return load().PTB_MeasureFmaPeak(int(bool(fp64)))
 
+
+def fitting_device_noalloc(d_stack_ptr, d_positions_ptr, n_points, d_output_ptr, shape, fit, params, stream_ptr=0):
+    """Fit-only on device buffers without any device allocation (PTB_FittingDeviceNoAlloc); returns doubles written."""
+    z, h, w = shape
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    return load().PTB_FittingDeviceNoAlloc(ctypes.c_void_p(d_stack_ptr), ctypes.c_void_p(d_positions_ptr), n_points,
+                                           ctypes.c_void_p(d_output_ptr), h, w, z, fit, params.ctypes.data_as(_f64p),
+                                           ctypes.c_void_p(stream_ptr))
