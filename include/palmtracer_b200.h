@@ -101,8 +101,8 @@ PTB_API uint64_t PTB_KernelLaunchCount(void);
 /* Stage timing (diagnostics). When enabled, every chunk records CUDA events on the library's stream around its
  * stages and accumulates device milliseconds per stage: [0] detection kernel, [1] segmentation chain, [2] fit
  * kernels, [3] ordering and numbering, [4] host<->device copies, and for fit modes 6-8 the fit's phases: [5]
- * initial values, [6] Levenberg-Marquardt iterations, [7] Newton polish, FP64 likelihood and CRLB (the warp-per-ROI
- * mapping runs as one launch, counted in [6]). PTB_StageTimes copies up to n totals into ms and the matching launch
+ * initial values, [6] Levenberg-Marquardt iterations, [7] Newton polish, [8] FP64 likelihood and CRLB (the
+ * warp-per-ROI mapping runs as one launch, counted in [6]). PTB_StageTimes copies up to n totals into ms and the matching launch
  * counts into launches (either may be NULL), then resets them. Returns the previous setting. */
 PTB_API int PTB_SetProfiling(int enable);
 PTB_API void PTB_StageTimes(double* ms, uint64_t* launches, int n);

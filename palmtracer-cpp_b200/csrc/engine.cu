@@ -342,7 +342,7 @@ long long Engine::RunChunk(const uint16_t* dImg, int H, int W, int B, double thr
 		}
 	}
 	if (mleProf) {
-		for (int k = 0; k < 3; ++k) {
+		for (int k = 0; k < 4; ++k) {
 			float ms = 0.f;
 			cudaEventElapsedTime(&ms, mleEv_[k], mleEv_[k + 1]);
 			stageMs_[5 + k] += ms;

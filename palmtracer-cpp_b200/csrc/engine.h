@@ -76,10 +76,11 @@ private:
 	int strict_ = 0;
 	int precision_ = 0;
 	int profiling_ = 0;
-	// profiling: detect, segment, fit, finish, copies, then the phases of a modes 6-8 fit (initial values, LM, polish)
-	static constexpr int kStages = 8;
+	// profiling: detect, segment, fit, finish, copies, then the phases of a modes 6-8 fit (initial values, LM, polish,
+	// FP64 likelihood and CRLB)
+	static constexpr int kStages = 9;
 	cudaEvent_t ev_[6] = {};
-	cudaEvent_t mleEv_[4] = {};
+	cudaEvent_t mleEv_[5] = {};
 	double stageMs_[kStages] = {};
 	uint64_t stageLaunches_[kStages] = {};
 	unsigned long long* evalDev_ = nullptr;      // device counters of model evaluations (profiling)

@@ -1,9 +1,9 @@
 // Poisson maximum-likelihood fits (modes 6 Gaussian, 7 astigmatic 3D, 8 cubic-spline 3D) of (bg, I, x, y, s),
 // s = sigma (mode 6), z in nm (mode 7) or the spline's z coordinate (mode 8). No counterpart in the reference; the
 // model maths and the FP64 oracle are in oracle/pt_oracle.cpp (MleFit). This file follows it: the same initial
-// values, bounds and FP64 axial pre-scan, the same damped Fisher-scoring LM on the Poisson deviance with the same
-// step-size stop rule, then Newton steps on the exact Hessian of the deviance, and the CRLB from the Fisher
-// information at the final point.
+// values, bounds and FP64 axial pre-scan, the same damped Fisher-scoring LM on the Poisson deviance (its step-size
+// stop rule one decade looser, see StepSmall), then Newton steps on the exact Hessian of the deviance, parameters on
+// active bounds held throughout, and the CRLB from the Fisher information at the final point.
 //
 // Precision: the LM iterations and the Newton polish run in FP32. Each 5x5 system is factored by an FP32 Cholesky;
 // when a pivot is not positive or the pivot ratio min(L_ii^2) / max(A_ii) falls below 1e-5 the same system is
@@ -13,13 +13,14 @@
 // the deviance), well inside the stated tolerance of 1e-3 px and 1e-4 relative photons.
 //
 // Two mappings, chosen per (mode, ROI) by the autotuner in engine.cu:
-//   * thread per ROI, three launches that hand their state over in the output rows (columns 0-4 theta, column 5 a
+//   * thread per ROI, four launches that hand their state over in the output rows (columns 0-4 theta, column 5 a
 //     status) so that no extra device memory is needed:
 //       MleInitKernel   initial values and FP64 axial pre-scan;
 //       MleLmKernel     persistent FP32 LM: every warp owns a contiguous range of candidates and each lane takes the
 //                       next candidate of the range as soon as its own converges, so a lane never idles while the
 //                       other 31 iterate; ROI photons and the column erf factors are staged per lane in shared memory;
-//       MlePolishKernel FP32 Newton polish, FP64 deviance and Fisher information, CRLB, output row;
+//       MlePolishKernel persistent FP32 Newton polish, organised the same way;
+//       MleFinalKernel  FP64 deviance and Fisher information, CRLB, output row;
 //   * warp per ROI (MleWarpKernel): all four phases in one launch, pixels spread over the lanes, sums reduced with
 //     shuffles; better for large ROIs and for the spline model, whose 64 coefficients per pixel dominate.
 // For modes 6-7 the pixel-integrated Gaussian is separable: the erf factors are formed once per ROI column and row
@@ -489,13 +490,40 @@ __device__ __forceinline__ void FixActive32(const MleParams& mp, float x0, float
 	}
 }
 
-// LM stop rule of the oracle (MleStepSmall).
+// LM stop rule: the oracle's (MleStepSmall: 1e-4 px in x and y, 1e-4 relative in I and bg with floor 1, 1e-4 for
+// sigma and the spline z, 1e-2 nm for z) with every threshold multiplied by kLmStepScale. The FP32 deviance cannot
+// resolve the last LM steps of the oracle (a 1e-4 px step changes the deviance by about 1e-5, the size of its FP32
+// rounding), so the FP32 LM hands over to the Newton polish one decade earlier; the polish converges quadratically
+// from there, to the same optimum.
+constexpr float kLmStepScale = 10.f;
 __device__ __forceinline__ bool StepSmall(int model, const float a[5], const float b[5])
 {
-	const float sTol = model == 7 ? 1e-2f : 1e-4f;
-	return fabsf(b[2] - a[2]) < 1e-4f && fabsf(b[3] - a[3]) < 1e-4f && fabsf(b[1] - a[1]) < 1e-4f * fmaxf(fabsf(a[1]), 1.f) &&
-	       fabsf(b[0] - a[0]) < 1e-4f * fmaxf(fabsf(a[0]), 1.f) && fabsf(b[4] - a[4]) < sTol;
+	const float t = 1e-4f * kLmStepScale, sTol = (model == 7 ? 1e-2f : 1e-4f) * kLmStepScale;
+	return fabsf(b[2] - a[2]) < t && fabsf(b[3] - a[3]) < t && fabsf(b[1] - a[1]) < t * fmaxf(fabsf(a[1]), 1.f) &&
+	       fabsf(b[0] - a[0]) < t * fmaxf(fabsf(a[0]), 1.f) && fabsf(b[4] - a[4]) < sTol;
 }
+
+// Newton direction at th: the exact Hessian with active bounds held, Fisher scoring where that Hessian is not
+// positive definite. Hm is modified in place.
+template <int MODEL>
+__device__ __forceinline__ bool NewtonDirection(const MleParams& mp, float x0, float y0, const float th[5], const float G[5], float Hm[15],
+                                                const float Fm[15], float dt[5])
+{
+	float rhs[5];
+	#pragma unroll
+	for (int a = 0; a < 5; ++a) { rhs[a] = -G[a]; }
+	FixActive32<MODEL>(mp, x0, y0, th, G, Hm, rhs);
+	if (Solve32(Hm, 1.f, rhs, dt, nullptr, false)) { return true; }
+	float Hf[15];
+	#pragma unroll
+	for (int a = 0; a < 15; ++a) { Hf[a] = 2.f * Fm[a]; }
+	FixActive32<MODEL>(mp, x0, y0, th, G, Hf, rhs);
+	return Solve32(Hf, 1.f, rhs, dt, nullptr, false);
+}
+
+// Newton polish acceptance: the trial deviance may exceed the current one by its FP32 rounding (steps near the
+// optimum change the deviance by less than that).
+__device__ __forceinline__ bool PolishAccept(float Dt, float D) { return isfinite(Dt) && Dt <= D + 1e-5f * (fabsf(D) + 1.f); }
 
 // ROI geometry of a candidate; false when the ROI crosses the frame border (the reference's test, Fitting.cpp).
 struct RoiAt {
@@ -577,9 +605,8 @@ __device__ int InitTheta(const MleParams& mp, const Pix& px, const RoiAt& r, dou
 	return evals;
 }
 
-// FP32 Newton steps on the exact Hessian of the deviance (Fisher scoring where that Hessian is not positive
-// definite), parameters on active bounds held, at most 6, a step that raises the deviance beyond its FP32 rounding halved up to three times; stops at
-// a 1e-6 relative step.
+// FP32 Newton steps on the exact Hessian of the deviance (NewtonDirection), at most 6; a step that the deviance does
+// not accept (PolishAccept) is halved up to three times; stops at a 1e-6 relative step (the oracle: FP64, 1e-10).
 template <int MODEL, int L>
 __device__ int Polish(const MleParams& mp, const Pix& px, float x0, float y0, float th[5], FacTab<float> xt, FacTab<float> yt)
 {
@@ -588,27 +615,17 @@ __device__ int Polish(const MleParams& mp, const Pix& px, float x0, float y0, fl
 	int evals = 1;
 	if (!isfinite(D)) { return evals; }
 	for (int it = 0; it < 6; ++it) {
-		float rhs[5], dt[5], tt[5];
-		#pragma unroll
-		for (int a = 0; a < 5; ++a) { rhs[a] = -G[a]; }
-		FixActive32<MODEL>(mp, x0, y0, th, G, Hm, rhs);
-		if (!Solve32(Hm, 1.f, rhs, dt, nullptr, false)) {
-			float Hf[15];
-			#pragma unroll
-			for (int a = 0; a < 15; ++a) { Hf[a] = 2.f * Fm[a]; }
-			FixActive32<MODEL>(mp, x0, y0, th, G, Hf, rhs);
-			if (!Solve32(Hf, 1.f, rhs, dt, nullptr, false)) { break; }
-		}
+		float dt[5], tt[5];
+		if (!NewtonDirection<MODEL>(mp, x0, y0, th, G, Hm, Fm, dt)) { break; }
 		bool accepted = false;
 		float Gt[5], Ht[15], Ft[15], Dt = 0.f;
-		const float slack = 1e-5f * (fabsf(D) + 1.f);
 		for (int hv = 0; hv < 4 && !accepted; ++hv) {
 			#pragma unroll
 			for (int a = 0; a < 5; ++a) { tt[a] = th[a] + dt[a]; }
 			Clamp32<MODEL>(mp, x0, y0, tt);
 			Dt = Normal<float, MODEL, L, kExact>(mp, px, tt, Gt, Ht, Ft, xt, yt);
 			++evals;
-			if (isfinite(Dt) && Dt <= D + slack) { accepted = true; }
+			if (PolishAccept(Dt, D)) { accepted = true; }
 			else {
 				#pragma unroll
 				for (int a = 0; a < 5; ++a) { dt[a] *= 0.5f; }
@@ -726,10 +743,53 @@ __global__ void __launch_bounds__(kThreads) MleInitKernel(const uint16_t* __rest
 	if (mp.evals && evals) { atomicAdd(mp.evals + 2, evals); }
 }
 
-// Persistent FP32 LM. Warp w owns candidates [w * chunk, (w + 1) * chunk); a lane whose fit ends takes the next one of
-// the range. Every pass of the loop makes each busy lane evaluate the deviance, gradient and Fisher matrix once: at
-// the start point of a new candidate, or at the trial point of an LM step. Shared memory per lane: the ROI photons
-// (n floats) and the column factors (3 roi floats), lane-interleaved.
+constexpr uint32_t kNone = 0xffffffffu;
+
+// Work queue of the persistent kernels: warp w owns candidates [w * chunk, (w + 1) * chunk), chunk >= 32; lanes that
+// need work take the next candidates of the range in lane order.
+struct WarpQueue {
+	uint32_t cursor, end;
+	__device__ __forceinline__ bool Init(uint32_t n)
+	{
+		const uint32_t warps = gridDim.x * (blockDim.x / 32);
+		const uint32_t gw = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+		const uint32_t chunk = max(32u, (n + warps - 1) / warps);
+		const unsigned long long begin = static_cast<unsigned long long>(gw) * chunk;
+		cursor = static_cast<uint32_t>(min(begin, static_cast<unsigned long long>(n)));
+		end = static_cast<uint32_t>(min(begin + chunk, static_cast<unsigned long long>(n)));
+		return cursor < end;
+	}
+	// Called by all 32 lanes; returns the candidate taken by a lane with `need` set (kNone when the range is done).
+	__device__ __forceinline__ uint32_t Take(bool need)
+	{
+		const unsigned mask = __ballot_sync(0xffffffffu, need);
+		const uint32_t k = cursor + __popc(mask & ((1u << (threadIdx.x & 31)) - 1u));
+		cursor = min(end, cursor + static_cast<uint32_t>(__popc(mask)));
+		return need && k < end ? k : kNone;
+	}
+	__device__ __forceinline__ bool Done() const { return cursor >= end; }
+};
+
+// Stages the ROI of candidate k for the calling lane: FP32 photons at ph[q * T], theta from the row, position.
+__device__ __forceinline__ void LoadRoi(const uint16_t* img, int H, int W, long long N, const MleParams& mp, const Cand* cands,
+                                        const double* rows, uint32_t k, float* ph, int T, Pix& px, float th[5], float& x0, float& y0)
+{
+	RoiAt r;
+	Locate(img, H, W, N, mp, cands[k], r);
+	px.g = r.base;
+	for (int i = 0, q = 0; i < mp.roi; ++i) {
+		for (int j = 0; j < mp.roi; ++j, ++q) { ph[q * T] = fmaxf((float(__ldg(r.base + i * W + j)) - px.off32) * px.inv32, 0.f); }
+	}
+	const double* row = rows + static_cast<long long>(k) * kCols;
+	#pragma unroll
+	for (int a = 0; a < 5; ++a) { th[a] = static_cast<float>(row[a]); }
+	x0 = static_cast<float>(r.x0);
+	y0 = static_cast<float>(r.y0);
+}
+
+// Persistent FP32 LM (WarpQueue). Every pass of the loop makes each busy lane evaluate the deviance, gradient and
+// Fisher matrix once: at the start point of a new candidate, or at the trial point of an LM step. Shared memory per
+// lane, lane-interleaved: the ROI photons (n floats) and the column factors (3 roi floats).
 template <int MODEL>
 __global__ void __launch_bounds__(kThreads) MleLmKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
                                                         const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
@@ -739,16 +799,8 @@ __global__ void __launch_bounds__(kThreads) MleLmKernel(const uint16_t* __restri
 	const int T = blockDim.x;
 	float* ph = reinterpret_cast<float*>(smem) + threadIdx.x;
 	const FacTab<float> xt{reinterpret_cast<float*>(smem) + mp.n * T + threadIdx.x, T};
-	const uint32_t n = CandCount(nptr, nconst);
-	const int lane = threadIdx.x & 31;
-	const uint32_t warps = gridDim.x * (blockDim.x / 32);
-	const uint32_t gw = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-	const uint32_t chunk = std::max<uint32_t>(32u, (n + warps - 1) / warps);
-	const unsigned long long beginL = static_cast<unsigned long long>(gw) * chunk;
-	if (beginL >= n) { return; }
-	uint32_t cursor = static_cast<uint32_t>(beginL);
-	const uint32_t end = static_cast<uint32_t>(std::min<unsigned long long>(n, beginL + chunk));
-	constexpr uint32_t kNone = 0xffffffffu;
+	WarpQueue q;
+	if (!q.Init(CandCount(nptr, nconst))) { return; }
 	uint32_t k = kNone;
 	bool fresh = false;
 	float th[5] = {0, 0, 0, 0, 0}, G[5], Hm[15], D = 0.f, lambda = 1e-3f, x0 = 0.f, y0 = 0.f;
@@ -756,36 +808,17 @@ __global__ void __launch_bounds__(kThreads) MleLmKernel(const uint16_t* __restri
 	unsigned long long evals = 0;
 	Pix px = MakePix(mp, img, W, ph, T);
 	while (true) {
-		// refill idle lanes from the warp's range, in lane order
-		const bool need = k == kNone;
-		const unsigned needMask = __ballot_sync(0xffffffffu, need);
-		if (need) {
-			const uint32_t kk = cursor + __popc(needMask & ((1u << lane) - 1u));
-			if (kk < end && rows[static_cast<long long>(kk) * kCols + kStatusCol] == kStOk) {
-				RoiAt r;
-				Locate(img, H, W, N, mp, cands[kk], r);
-				px.g = r.base;
-				for (int i = 0, q = 0; i < mp.roi; ++i) {
-					for (int j = 0; j < mp.roi; ++j, ++q) {
-						ph[q * T] = fmaxf((float(__ldg(r.base + i * W + j)) - px.off32) * px.inv32, 0.f);
-					}
-				}
-				const double* row = rows + static_cast<long long>(kk) * kCols;
-				#pragma unroll
-				for (int a = 0; a < 5; ++a) { th[a] = static_cast<float>(row[a]); }
-				x0 = static_cast<float>(r.x0);
-				y0 = static_cast<float>(r.y0);
-				k = kk;
-				fresh = true;
-			}
+		const uint32_t kk = q.Take(k == kNone);
+		if (kk != kNone && rows[static_cast<long long>(kk) * kCols + kStatusCol] == kStOk) {
+			LoadRoi(img, H, W, N, mp, cands, rows, kk, ph, T, px, th, x0, y0);
+			k = kk;
+			fresh = true;
 		}
-		cursor = std::min<uint32_t>(end, cursor + __popc(needMask));
 		const bool busy = k != kNone;
 		if (__ballot_sync(0xffffffffu, busy) == 0) {
-			if (cursor >= end) { break; }
+			if (q.Done()) { break; }
 			continue;
 		}
-		
 		float tt[5];
 		bool eval = false, finish = false, failed = false;
 		if (busy) {
@@ -816,8 +849,6 @@ __global__ void __launch_bounds__(kThreads) MleLmKernel(const uint16_t* __restri
 		if (eval) {
 			Dt = Normal<float, MODEL, 1, kFisher>(mp, px, tt, Gt, Ht, nullptr, xt, xt);
 			++evals;
-		}
-		if (eval) {
 			if (fresh) {
 				fresh = false;
 				D = Dt;
@@ -860,10 +891,10 @@ __global__ void __launch_bounds__(kThreads) MleLmKernel(const uint16_t* __restri
 	if (mp.evals && evals) { atomicAdd(mp.evals, evals); }
 }
 
-// FP32 Newton polish, FP64 deviance, Fisher information and CRLB, output row. Shared memory: the column factors, in
-// two separate lane-interleaved regions - 6 roi floats per thread for the polish, then 3 roi doubles per thread for
-// the FP64 pass. (One region for both would not do: with 4- and 8-byte entries interleaved over the threads, a
-// thread that reaches the FP64 pass early would overwrite the FP32 entries of threads still polishing.)
+// Persistent FP32 Newton polish (WarpQueue), the steps of Polish() as a per-lane state machine: each pass evaluates
+// the deviance, gradient, exact Hessian and Fisher information once per busy lane - at the LM result of a new
+// candidate or at a trial point - and then accepts, halves or ends. Shared memory per lane: the ROI photons (n
+// floats) and the column factors with second derivatives (6 roi floats).
 template <int MODEL>
 __global__ void __launch_bounds__(kThreads) MlePolishKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
                                                             const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
@@ -871,35 +902,102 @@ __global__ void __launch_bounds__(kThreads) MlePolishKernel(const uint16_t* __re
 {
 	extern __shared__ __align__(16) unsigned char smem[];
 	const int T = blockDim.x;
-	double* region64 = reinterpret_cast<double*>(smem);
-	float* region32 = reinterpret_cast<float*>(region64 + 3 * mp.roi * T);
-	const FacTab<float> xt32{region32 + threadIdx.x, T};
-	const FacTab<double> xt64{region64 + threadIdx.x, T};
+	float* ph = reinterpret_cast<float*>(smem) + threadIdx.x;
+	const FacTab<float> xt{reinterpret_cast<float*>(smem) + mp.n * T + threadIdx.x, T};
+	WarpQueue q;
+	if (!q.Init(CandCount(nptr, nconst))) { return; }
+	uint32_t k = kNone;
+	bool fresh = false;
+	float th[5] = {0, 0, 0, 0, 0}, dt[5] = {0, 0, 0, 0, 0}, G[5], Hm[15], Fm[15], D = 0.f, x0 = 0.f, y0 = 0.f;
+	int it = 0, hv = 0;
+	unsigned long long evals = 0;
+	Pix px = MakePix(mp, img, W, ph, T);
+	while (true) {
+		const uint32_t kk = q.Take(k == kNone);
+		if (kk != kNone && rows[static_cast<long long>(kk) * kCols + kStatusCol] == kStOk) {
+			LoadRoi(img, H, W, N, mp, cands, rows, kk, ph, T, px, th, x0, y0);
+			k = kk;
+			fresh = true;
+		}
+		const bool busy = k != kNone;
+		if (__ballot_sync(0xffffffffu, busy) == 0) {
+			if (q.Done()) { break; }
+			continue;
+		}
+		float tt[5], Gt[5], Ht[15], Ft[15], Dt = 0.f;
+		bool finish = false;
+		if (busy) {
+			#pragma unroll
+			for (int a = 0; a < 5; ++a) { tt[a] = fresh ? th[a] : th[a] + dt[a]; }
+			if (!fresh) { Clamp32<MODEL>(mp, x0, y0, tt); }
+			Dt = Normal<float, MODEL, 1, kExact>(mp, px, tt, Gt, Ht, Ft, xt, xt);
+			++evals;
+			bool moved = false;
+			if (fresh) {
+				fresh = false;
+				it = 0;
+				moved = isfinite(Dt);
+				finish = !moved;
+			}
+			else if (PolishAccept(Dt, D)) {
+				float step = 0.f;
+				#pragma unroll
+				for (int a = 0; a < 5; ++a) { step = fmaxf(step, fabsf(tt[a] - th[a]) / fmaxf(fabsf(th[a]), 1.f)); }
+				++it;
+				finish = step < 1e-6f || it >= 6;
+				moved = true;
+			}
+			else if (++hv >= 4) { finish = true; }
+			else {
+				#pragma unroll
+				for (int a = 0; a < 5; ++a) { dt[a] *= 0.5f; }
+			}
+			if (moved) {
+				#pragma unroll
+				for (int a = 0; a < 5; ++a) { th[a] = tt[a]; G[a] = Gt[a]; }
+				#pragma unroll
+				for (int a = 0; a < 15; ++a) { Hm[a] = Ht[a]; Fm[a] = Ft[a]; }
+				D = Dt;
+				hv = 0;
+				if (!finish) { finish = !NewtonDirection<MODEL>(mp, x0, y0, th, G, Hm, Fm, dt); }
+			}
+		}
+		if (finish) {
+			double* row = rows + static_cast<long long>(k) * kCols;
+			#pragma unroll
+			for (int a = 0; a < 5; ++a) { row[a] = th[a]; }
+			k = kNone;
+		}
+	}
+	if (mp.evals && evals) { atomicAdd(mp.evals + 1, evals); }
+}
+
+// FP64 deviance, Fisher information and CRLB at the polished theta; writes the output row. Shared memory per thread:
+// the FP64 column factors (3 roi doubles).
+template <int MODEL>
+__global__ void __launch_bounds__(kThreads) MleFinalKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
+                                                           const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
+                                                           MleParams mp, double* rows)
+{
+	extern __shared__ __align__(16) unsigned char smem[];
+	const FacTab<double> xt{reinterpret_cast<double*>(smem) + threadIdx.x, static_cast<int>(blockDim.x)};
 	const uint32_t n = CandCount(nptr, nconst);
-	unsigned long long evals32 = 0, evals64 = 0;
+	unsigned long long evals = 0;
 	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
 		double* row = rows + static_cast<long long>(k) * kCols;
 		const Cand cd = cands[k];
-		const double status = row[kStatusCol];
 		RoiAt r;
 		double t[5] = {0, 0, 0, 0, 0}, crlb[5] = {0, 0, 0, 0, 0};
-		const bool inside = Locate(img, H, W, N, mp, cd, r);
-		bool ok = inside && status == kStOk;
+		bool ok = Locate(img, H, W, N, mp, cd, r) && row[kStatusCol] == kStOk;
 		if (ok) {
-			const Pix px = MakePix(mp, r.base, W, nullptr, 0);
-			float th[5];
 			#pragma unroll
-			for (int a = 0; a < 5; ++a) { th[a] = static_cast<float>(row[a]); }
-			evals32 += Polish<MODEL, 1>(mp, px, static_cast<float>(r.x0), static_cast<float>(r.y0), th, xt32, xt32);
-			#pragma unroll
-			for (int a = 0; a < 5; ++a) { t[a] = th[a]; }
-			ok = Final<MODEL, 1>(mp, px, t, crlb, xt64, xt64);
-			++evals64;
+			for (int a = 0; a < 5; ++a) { t[a] = row[a]; }
+			ok = Final<MODEL, 1>(mp, MakePix(mp, r.base, W, nullptr, 0), t, crlb, xt, xt);
+			++evals;
 		}
 		StoreMleRow(row, -1, mp, cd, t, crlb, r.ux, r.uy, ok);
 	}
-	if (mp.evals && evals32) { atomicAdd(mp.evals + 1, evals32); }
-	if (mp.evals && evals64) { atomicAdd(mp.evals + 2, evals64); }
+	if (mp.evals && evals) { atomicAdd(mp.evals + 2, evals); }
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -1017,7 +1115,17 @@ void AllowSmem(K kernel, size_t bytes)
 	if (bytes > 48 * 1024) { cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)); }
 }
 
-// marks (profiling, or null): 4 events recorded before the initial values, the LM, the polish and after it.
+// marks (profiling, or null): 5 events, recorded before the initial values, the LM, the polish, the FP64 pass and
+// after it.
+template <typename K>
+int PersistentBlocks(K kernel, size_t smemBytes, int sms, uint32_t cap)
+{
+	AllowSmem(kernel, smemBytes);
+	int perSm = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kThreads, smemBytes) != cudaSuccess || perSm < 1) { perSm = 1; }
+	return static_cast<int>(std::min<uint32_t>((std::max<uint32_t>(cap, 1) + kThreads - 1) / kThreads, static_cast<uint32_t>(sms * perSm)));
+}
+
 template <int MODEL>
 bool LaunchThreadPerRoi(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
                         uint32_t cap, const MleParams& mp, double* rows, cudaEvent_t* marks, cudaStream_t st)
@@ -1026,25 +1134,24 @@ bool LaunchThreadPerRoi(const uint16_t* img, int H, int W, long long N, const Ca
 	const uint32_t blocks = std::min<uint32_t>((std::max<uint32_t>(cap, 1) + kThreads - 1) / kThreads, static_cast<uint32_t>(sms) * 32u);
 	const size_t initBytes = static_cast<size_t>(mp.roi) * sizeof(double) * kThreads;
 	const size_t lmBytes = static_cast<size_t>(mp.n + 3 * mp.roi) * sizeof(float) * kThreads;
-	const size_t polishBytes = static_cast<size_t>(3 * mp.roi) * (sizeof(double) + 2 * sizeof(float)) * kThreads;
-	AllowSmem(MleLmKernel<MODEL>, lmBytes);
-	int perSm = 0;
-	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, MleLmKernel<MODEL>, kThreads, lmBytes) != cudaSuccess || perSm < 1) {
-		perSm = 1;
-	}
-	const uint32_t lmBlocks = std::min<uint32_t>(blocks, static_cast<uint32_t>(sms * perSm));
+	const size_t polishBytes = static_cast<size_t>(mp.n + 6 * mp.roi) * sizeof(float) * kThreads;
+	const size_t finalBytes = static_cast<size_t>(3 * mp.roi) * sizeof(double) * kThreads;
+	const int lmBlocks = PersistentBlocks(MleLmKernel<MODEL>, lmBytes, sms, cap);
+	const int polishBlocks = PersistentBlocks(MlePolishKernel<MODEL>, polishBytes, sms, cap);
 	if (marks) { cudaEventRecord(marks[0], st); }
 	MleInitKernel<MODEL><<<blocks, kThreads, initBytes, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows);
 	if (marks) { cudaEventRecord(marks[1], st); }
 	MleLmKernel<MODEL><<<lmBlocks, kThreads, lmBytes, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows);
 	if (marks) { cudaEventRecord(marks[2], st); }
-	MlePolishKernel<MODEL><<<blocks, kThreads, polishBytes, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows);
+	MlePolishKernel<MODEL><<<polishBlocks, kThreads, polishBytes, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows);
 	if (marks) { cudaEventRecord(marks[3], st); }
-	CountLaunch(3);
+	MleFinalKernel<MODEL><<<blocks, kThreads, finalBytes, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows);
+	if (marks) { cudaEventRecord(marks[4], st); }
+	CountLaunch(4);
 	return PTB_LAUNCHED();
 }
 
-// marks: the single launch is timed as the LM phase (marks 0-2 before it, mark 3 after it).
+// marks: the single launch is timed as the LM phase (marks 0-1 before it, marks 2-4 after it).
 template <int MODEL>
 bool LaunchWarpPerRoi(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
                       uint32_t cap, const MleParams& mp, double* rows, cudaEvent_t* marks, cudaStream_t st)
@@ -1059,6 +1166,7 @@ bool LaunchWarpPerRoi(const uint16_t* img, int H, int W, long long N, const Cand
 	if (marks) {
 		cudaEventRecord(marks[2], st);
 		cudaEventRecord(marks[3], st);
+		cudaEventRecord(marks[4], st);
 	}
 	CountLaunch();
 	return PTB_LAUNCHED();
@@ -1074,7 +1182,7 @@ bool LaunchModel(int lanes, const uint16_t* img, int H, int W, long long N, cons
 
 }  // namespace
 
-// lanes: 1 = thread per ROI, anything else = warp per ROI. marks: profiling events (4) or null.
+// lanes: 1 = thread per ROI, anything else = warp per ROI. marks: profiling events (5) or null.
 bool LaunchMle(int lanes, const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
                uint32_t cap, const MleParams& mp, double* rows, cudaEvent_t* marks, cudaStream_t st)
 {

@@ -100,7 +100,7 @@ struct FitParams {
 	const double* coeffs;  // device, cell-major [cell][64]
 	MleParams mle;         // modes 6-8
 	int lanes;             // ROI mapping for modes 6-8: 1 thread per ROI, else warp per ROI (autotuned)
-	cudaEvent_t* marks;    // profiling, or null: 4 events recorded around the phases of the modes 6-8 fit
+	cudaEvent_t* marks;    // profiling, or null: 5 events recorded around the phases of the modes 6-8 fit
 };
 
 // Geometry of one chunk: B frames of H x W pixels; global pixel index g = f * N + y * W + x (fits in 31 bits).

@@ -152,7 +152,7 @@ def launch_count():
     return load().PTB_KernelLaunchCount()
 
 
-STAGES = ["detect", "segment", "fit", "finish", "copies", "fit_init", "fit_lm", "fit_polish"]
+STAGES = ["detect", "segment", "fit", "finish", "copies", "fit_init", "fit_lm", "fit_polish", "fit_final"]
 
 
 def set_profiling(enable):
