@@ -100,68 +100,208 @@ __device__ __forceinline__ long long W1At(const TileSmem& s, int r, int c)
 	return static_cast<long long>(s.a.v1[r + 4][c + 4]) * 256 - static_cast<long long>(s.v2[r][c]);
 }
 
-// Appends `g` to list[] for every lane with pred set: one atomic per warp. Entries beyond cap raise *overflow.
-__device__ __forceinline__ void WarpAppend(bool pred, uint32_t g, uint32_t* list, uint32_t* counter, uint32_t cap,
-                                           uint32_t* overflow)
+// ---- Detection kernel ------------------------------------------------------------------------------------------
+// Five register-blocked passes over one 128 x 32 tile. Borders: every intermediate array is kept edge-replicated
+// (an entry whose coordinate lies outside the frame holds the value of the nearest in-frame entry), which is what
+// the reference's clamping of every neighbour access amounts to, so no pass clamps an index:
+//   A  C1 = vertical level-1 taps of the input, one lane per column sliding down 46 clamped input rows (rows outside
+//      the frame are then replicated);   tile rows [-5, 37), cols [-7, 145)
+//   B  V1 = horizontal level-1 taps of C1, 8 columns per task from 3 vector loads (columns outside the frame are
+//      then replicated);                 tile rows [-5, 37), cols [-5, 139)
+//   C  C2 = vertical level-2 taps (rows +-2, +-4) of V1, one lane per column and 12-row run;   rows [-1, 33)
+//   D  W1 = V1 * 256 - V2 on the ring (tile +-1), V2 = horizontal level-2 taps of C2, 8 columns per task, stored
+//      in place of V1 as max(W1, 0) (W1 < 2^32; a non-positive W1 can neither be in the domain nor dominate a
+//      domain pixel) and 0 outside the frame (the reference skips neighbours outside the frame);
+//   E  threshold and 3 x 3 maximum for 8 pixels per task; code bytes, W1 of domain pixels, and the domain and seed
+//      lists with one atomic per block and list.
+constexpr int kP1 = 152;  // C1 pitch (tile col = index - 7); C2 (pitch kPV, tile col = index - 5) reuses its space
+constexpr int kPV = 144;  // V1 pitch (tile col = index - 5, tile row = index - 5); W1 ring in place
+constexpr int kRows1 = TY + 10;  // C1 and V1 rows
+constexpr int kRows2 = TY + 2;   // C2 rows and ring rows (tile row = index - 1)
+constexpr int kDetectWords = kRows1 * kP1 + kRows1 * kPV;
+static_assert(kRows2 * kPV <= kRows1 * kP1, "C2 must fit in the C1 space");
+
+__device__ __forceinline__ uint32_t Tap(uint32_t m2, uint32_t m1, uint32_t c, uint32_t p1, uint32_t p2)
 {
-	const unsigned mask = __ballot_sync(0xffffffffu, pred);
-	if (mask == 0) { return; }
-	const int lane = threadIdx.x & 31;
-	const int leader = __ffs(mask) - 1;
-	uint32_t base = 0;
-	if (lane == leader) { base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask))); }
-	base = __shfl_sync(0xffffffffu, base, leader);
-	if (pred) {
-		const uint32_t pos = base + __popc(mask & ((1u << lane) - 1u));
-		if (pos < cap) { list[pos] = g; }
-		else { atomicExch(overflow, 1u); }
-	}
+	return 6u * c + 4u * (m1 + p1) + (m2 + p2);
 }
 
-// One CTA per (tile, frame): W1, domain and seed flags for the tile; W1 stored on domain pixels only.
 __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restrict__ img, Workspace ws, long long thrFixed)
 {
 	extern __shared__ __align__(16) unsigned char smemRaw[];
-	TileSmem& s = *reinterpret_cast<TileSmem*>(smemRaw);
+	uint32_t* c1 = reinterpret_cast<uint32_t*>(smemRaw);
+	uint32_t* c2 = c1;
+	uint32_t* v1 = c1 + kRows1 * kP1;
+	__shared__ uint32_t scanSm[2 * kWarps + 2];
 	const int H = ws.g.H, W = ws.g.W;
 	const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, f = blockIdx.z;
 	const uint16_t* frame = img + static_cast<long long>(f) * ws.g.N;
-	WaveletTile(s, frame, H, W, x0, y0);
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	const long long thr = thrFixed > 0 ? thrFixed : 0;  // domain: W1 > thr and W1 > 1e-8, i.e. W1_fixed >= 1
-	// every thread visits the same number of pixels (uniform for the warp-wide appends)
-	for (int ty = warp; ty < TY; ty += kWarps) {
+	const int tid = threadIdx.x;
+
+	// A: C1, one lane per column
+	for (int i = tid; i < kP1; i += kThreads) {
+		const uint16_t* col = frame + clampi(x0 - 7 + i, 0, W - 1);
+		uint32_t w0 = __ldg(col + static_cast<long long>(clampi(y0 - 7, 0, H - 1)) * W);
+		uint32_t w1 = __ldg(col + static_cast<long long>(clampi(y0 - 6, 0, H - 1)) * W);
+		uint32_t w2 = __ldg(col + static_cast<long long>(clampi(y0 - 5, 0, H - 1)) * W);
+		uint32_t w3 = __ldg(col + static_cast<long long>(clampi(y0 - 4, 0, H - 1)) * W);
+		#pragma unroll 6
+		for (int r = 0; r < kRows1; ++r) {
+			const uint32_t w4 = __ldg(col + static_cast<long long>(clampi(y0 - 3 + r, 0, H - 1)) * W);
+			c1[r * kP1 + i] = Tap(w0, w1, w2, w3, w4);
+			w0 = w1; w1 = w2; w2 = w3; w3 = w4;
+		}
+		const int rlo = max(0, 5 - y0), rhi = min(kRows1 - 1, H - 1 - y0 + 5);
+		for (int r = 0; r < rlo; ++r) { c1[r * kP1 + i] = c1[rlo * kP1 + i]; }
+		for (int r = rhi + 1; r < kRows1; ++r) { c1[r * kP1 + i] = c1[rhi * kP1 + i]; }
+	}
+	__syncthreads();
+	// B: V1, 8 columns per task
+	for (int task = tid; task < kRows1 * 18; task += kThreads) {
+		const int r = task / 18, m = task - r * 18;
+		const uint4* src = reinterpret_cast<const uint4*>(c1 + r * kP1 + 8 * m);
+		const uint4 a = src[0], b = src[1], c = src[2];
+		const uint32_t v[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+		uint32_t o[8];
+		#pragma unroll
+		for (int k = 0; k < 8; ++k) { o[k] = Tap(v[k], v[k + 1], v[k + 2], v[k + 3], v[k + 4]); }
+		uint4* dst = reinterpret_cast<uint4*>(v1 + r * kPV + 8 * m);
+		dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+		dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+	}
+	__syncthreads();
+	{
+		const int clo = max(0, 5 - x0), chi = min(kPV - 1, W - 1 - x0 + 5);
+		if (clo > 0 || chi < kPV - 1) {
+			for (int idx = tid; idx < kRows1 * kPV; idx += kThreads) {
+				const int r = idx / kPV, i = idx - r * kPV;
+				if (i < clo) { v1[r * kPV + i] = v1[r * kPV + clo]; }
+				else if (i > chi) { v1[r * kPV + i] = v1[r * kPV + chi]; }
+			}
+			__syncthreads();
+		}
+	}
+	// C: C2, one lane per column and run of up to 12 rows (C1 is dead: C2 takes its space)
+	for (int task = tid; task < kPV * 3; task += kThreads) {
+		const int q = task / kPV, i = task - q * kPV;
+		const int r0 = 12 * q, nr = min(12, kRows2 - r0);
+		uint32_t v[20];
+		#pragma unroll
+		for (int t = 0; t < 20; ++t) { v[t] = t < nr + 8 ? v1[(r0 + t) * kPV + i] : 0u; }
+		#pragma unroll
+		for (int t = 0; t < 12; ++t) {
+			if (t < nr) { c2[(r0 + t) * kPV + i] = Tap(v[t], v[t + 2], v[t + 4], v[t + 6], v[t + 8]); }
+		}
+	}
+	__syncthreads();
+	// D: W1 on the ring, in place of V1
+	for (int task = tid; task < kRows2 * 17; task += kThreads) {
+		const int q = task / 17, m = task - q * 17;
+		const uint4* src = reinterpret_cast<const uint4*>(c2 + q * kPV + 8 * m);
+		const uint4 a = src[0], b = src[1], c = src[2], d = src[3];
+		const uint32_t u[16] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w};
+		uint4* vp = reinterpret_cast<uint4*>(v1 + (q + 4) * kPV + 8 * m + 4);
+		const uint4 e = vp[0], g = vp[1];
+		const uint32_t v[8] = {e.x, e.y, e.z, e.w, g.x, g.y, g.z, g.w};
+		const int y = y0 + q - 1;
+		const bool rowIn = y >= 0 && y < H;
+		uint32_t o[8];
+		#pragma unroll
+		for (int k = 0; k < 8; ++k) {
+			const uint32_t v2 = Tap(u[k], u[k + 2], u[k + 4], u[k + 6], u[k + 8]);
+			const uint32_t v1s = v[k] << 8;
+			const int x = x0 + 8 * m - 1 + k;
+			o[k] = (rowIn && x >= 0 && x < W && v1s > v2) ? v1s - v2 : 0u;
+		}
+		vp[0] = make_uint4(o[0], o[1], o[2], o[3]);
+		vp[1] = make_uint4(o[4], o[5], o[6], o[7]);
+	}
+	__syncthreads();
+	// E: domain and seeds, 8 pixels per task, two tasks per thread
+	const uint32_t thr = thrFixed <= 0 ? 0u : (thrFixed >= 0xffffffffll ? 0xffffffffu : static_cast<uint32_t>(thrFixed));
+	uint32_t dmask[2] = {0, 0}, smask[2] = {0, 0};
+	uint32_t val[2][8];
+	#pragma unroll
+	for (int h = 0; h < 2; ++h) {
+		const int task = tid + h * kThreads;
+		const int ty = task >> 4, m = task & 15;
+		uint32_t a[3][12];
+		#pragma unroll
+		for (int rr = 0; rr < 3; ++rr) {
+			const uint4* src = reinterpret_cast<const uint4*>(v1 + (ty + 4 + rr) * kPV + 8 * m + 4);
+			const uint4 p = src[0], q = src[1], r = src[2];
+			a[rr][0] = p.x; a[rr][1] = p.y; a[rr][2] = p.z; a[rr][3] = p.w;
+			a[rr][4] = q.x; a[rr][5] = q.y; a[rr][6] = q.z; a[rr][7] = q.w;
+			a[rr][8] = r.x; a[rr][9] = r.y; a[rr][10] = r.z; a[rr][11] = r.w;
+		}
 		const int y = y0 + ty;
-		for (int tx = lane; tx < TX; tx += 32) {
-			const int x = x0 + tx;
-			const bool inside = y < H && x < W;
-			bool domain = false, seed = false;
-			long long v = 0;
-			if (inside) {
-				v = W1At(s, ty + 1, tx + 1);
-				domain = v > thr;
-				if (domain) {
-					seed = true;
-					// a neighbour dominates only if its thresholded value is strictly larger; since v > thr, that is
-					// exactly W1(neighbour) > W1(pixel)
-					for (int dy = -1; dy <= 1; ++dy) {
-						const int yy = y + dy;
-						if (yy < 0 || yy >= H) { continue; }
-						for (int dx = -1; dx <= 1; ++dx) {
-							const int xx = x + dx;
-							if ((dx == 0 && dy == 0) || xx < 0 || xx >= W) { continue; }
-							if (W1At(s, ty + 1 + dy, tx + 1 + dx) > v) { seed = false; }
-						}
-					}
-				}
+		#pragma unroll
+		for (int k = 0; k < 8; ++k) {
+			const uint32_t mx = max(max(max(a[0][k], a[0][k + 1]), max(a[0][k + 2], a[1][k])),
+			                        max(max(a[1][k + 2], a[2][k]), max(a[2][k + 1], a[2][k + 2])));
+			const uint32_t v = a[1][k + 1];
+			val[h][k] = v;
+			const bool dom = y < H && x0 + 8 * m + k < W && v > thr;
+			if (dom) {
+				dmask[h] |= 1u << k;
+				if (v >= mx) { smask[h] |= 1u << k; }
 			}
-			const long long gl = static_cast<long long>(f) * ws.g.N + static_cast<long long>(y) * W + x;
-			if (inside) {
-				ws.code[gl] = static_cast<uint8_t>((domain ? kDomain : 0) | (seed ? kSeed : 0));
-				if (domain) { ws.w1[gl] = v; }
+		}
+	}
+	// block-wide positions in the domain and seed lists: one atomic per list
+	const int lane = tid & 31, warp = tid >> 5;
+	const uint32_t nd = __popc(dmask[0]) + __popc(dmask[1]), ns = __popc(smask[0]) + __popc(smask[1]);
+	uint32_t id = nd, is = ns;
+	#pragma unroll
+	for (int d = 1; d < 32; d <<= 1) {
+		const uint32_t td = __shfl_up_sync(0xffffffffu, id, d), ts = __shfl_up_sync(0xffffffffu, is, d);
+		if (lane >= d) { id += td; is += ts; }
+	}
+	if (lane == 31) { scanSm[warp] = id; scanSm[kWarps + warp] = is; }
+	__syncthreads();
+	if (tid == 0) {
+		uint32_t sd = 0, ss = 0;
+		for (int w = 0; w < kWarps; ++w) {
+			const uint32_t a = scanSm[w], b = scanSm[kWarps + w];
+			scanSm[w] = sd; scanSm[kWarps + w] = ss;
+			sd += a; ss += b;
+		}
+		scanSm[2 * kWarps] = sd ? atomicAdd(&ws.cnt->ndom, sd) : 0u;
+		scanSm[2 * kWarps + 1] = ss ? atomicAdd(&ws.cnt->nseed, ss) : 0u;
+	}
+	__syncthreads();
+	uint32_t pd = scanSm[2 * kWarps] + scanSm[warp] + id - nd;
+	uint32_t ps = scanSm[2 * kWarps + 1] + scanSm[kWarps + warp] + is - ns;
+	#pragma unroll
+	for (int h = 0; h < 2; ++h) {
+		const int task = tid + h * kThreads;
+		const int ty = task >> 4, m = task & 15;
+		const int y = y0 + ty, xb = x0 + 8 * m;
+		if (y >= H || xb >= W) { continue; }
+		const long long g = static_cast<long long>(f) * ws.g.N + static_cast<long long>(y) * W + xb;
+		unsigned long long packed = 0;
+		#pragma unroll
+		for (int k = 0; k < 8; ++k) {
+			const unsigned long long byte = ((dmask[h] >> k) & 1u ? kDomain : 0u) | ((smask[h] >> k) & 1u ? kSeed : 0u);
+			packed |= byte << (8 * k);
+		}
+		if (xb + 8 <= W && (g & 7) == 0) { *reinterpret_cast<unsigned long long*>(ws.code + g) = packed; }
+		else {
+			for (int k = 0; k < 8 && xb + k < W; ++k) { ws.code[g + k] = static_cast<uint8_t>(packed >> (8 * k)); }
+		}
+		#pragma unroll
+		for (int k = 0; k < 8; ++k) {
+			if ((dmask[h] >> k) & 1u) {
+				ws.w1[g + k] = static_cast<long long>(val[h][k]);
+				if (pd < ws.capDom) { ws.dom[pd] = static_cast<uint32_t>(g + k); }
+				else { atomicExch(&ws.cnt->overflow, 1u); }
+				++pd;
 			}
-			WarpAppend(domain, static_cast<uint32_t>(gl), ws.dom, &ws.cnt->ndom, ws.capDom, &ws.cnt->overflow);
-			WarpAppend(seed, static_cast<uint32_t>(gl), ws.seeds, &ws.cnt->nseed, ws.capSeed, &ws.cnt->overflow);
+			if ((smask[h] >> k) & 1u) {
+				if (ps < ws.capSeed) { ws.seeds[ps] = static_cast<uint32_t>(g + k); }
+				else { atomicExch(&ws.cnt->overflow, 1u); }
+				++ps;
+			}
 		}
 	}
 }
@@ -200,7 +340,8 @@ bool ConfigureSmem()
 	static bool done = false;
 	if (done) { return true; }
 	const int bytes = static_cast<int>(sizeof(TileSmem));
-	bool ok = PTB_CUDA(cudaFuncSetAttribute(DetectKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+	bool ok = PTB_CUDA(cudaFuncSetAttribute(DetectKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                        static_cast<int>(kDetectWords * sizeof(uint32_t))));
 	ok = ok && PTB_CUDA(cudaFuncSetAttribute(PlaneKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
 	done = ok;
 	return ok;
@@ -221,7 +362,7 @@ bool LaunchDetect(const Workspace& ws, double thr, cudaStream_t st)
 {
 	if (!ConfigureSmem()) { return false; }
 	const dim3 grid((ws.g.W + TX - 1) / TX, (ws.g.H + TY - 1) / TY, ws.g.B);
-	DetectKernel<<<grid, kThreads, sizeof(TileSmem), st>>>(ws.img, ws, ThresholdFixed(thr));
+	DetectKernel<<<grid, kThreads, kDetectWords * sizeof(uint32_t), st>>>(ws.img, ws, ThresholdFixed(thr));
 	CountLaunch();
 	return PTB_LAUNCHED();
 }
