@@ -29,6 +29,9 @@ def compile_one(src):
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj, ""
     extra = ["-fmad=false"] if src.endswith("_exact.cu") else []
+    if src.endswith("fit_mle.cu"):
+        # FP32 LM and polish: approximate FP32 division and square root, denormals flushed (FP64 is unaffected)
+        extra = ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
     cmd = [NVCC] + FLAGS + extra + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

@@ -153,6 +153,8 @@ static size_t PlanWorkspace(Workspace& ws, int H, int W, int B, uint32_t rowsCap
 	g.words = (W + 31) / 32;
 	g.N = static_cast<long long>(H) * W;
 	g.P = g.N * B;
+	g.divN = MakeFastDiv(static_cast<uint32_t>(g.N));
+	g.divW = MakeFastDiv(static_cast<uint32_t>(W));
 	ws.g = g;
 	const size_t P = static_cast<size_t>(g.P);
 	const uint32_t capComp = IndepBound(H, W) * static_cast<uint32_t>(B) + 1;
@@ -470,13 +472,24 @@ void Engine::MleEvaluations(uint64_t* out, int n)
 		if (out) { out[k] = evalTotals_[k]; }
 		evalTotals_[k] = 0;
 	}
+	if (n > 3) {
+		// [3]: FP64 re-factorisations since the last call
+		unsigned int fb = 0;
+		if (fallbacks_ && Init() && PTB_CUDA(cudaStreamSynchronize(stream_)) &&
+		    PTB_CUDA(cudaMemcpy(&fb, fallbacks_, sizeof(fb), cudaMemcpyDeviceToHost))) {
+			cudaMemset(fallbacks_, 0, sizeof(unsigned int));
+		}
+		if (out) { out[3] = fb; }
+	}
 }
 
 bool Engine::UploadSpline(FitParams& fp, const std::vector<double>& spline)
 {
 	if (fp.mode >= kMleGauss) {
-		if (!fallbacks_ && !PTB_CUDA(cudaMalloc(&fallbacks_, sizeof(unsigned int)))) { return false; }
+		// [0] FP64 re-factorisation count, [1..2] work-queue counters of the persistent fit kernels
+		if (!fallbacks_ && !PTB_CUDA(cudaMalloc(&fallbacks_, 4 * sizeof(unsigned int)))) { return false; }
 		fp.mle.fallbacks = static_cast<unsigned int*>(fallbacks_);
+		fp.mle.queue = static_cast<unsigned int*>(fallbacks_) + 1;
 		fp.lanes = TunedLanes(fp);
 	}
 	if (fp.mode == kMleSpline) {

@@ -6,7 +6,7 @@
 // active bounds held throughout, and the CRLB from the Fisher information at the final point.
 //
 // Precision: the LM iterations and the Newton polish run in FP32. Each 5x5 system is factored by an FP32 Cholesky;
-// when a pivot is not positive or the pivot ratio min(L_ii^2) / max(A_ii) falls below 1e-5 the same system is
+// when a pivot is not positive or the pivot ratio min(L_ii^2 / A_ii) falls below 1e-5 the same system is
 // re-factored in FP64. The initial axial pre-scan (a handful of deviance evaluations that choose the starting basin),
 // the final deviance (log-likelihood) and the Fisher information behind the CRLB are computed in FP64. The oracle
 // polishes in FP64 to a 1e-10 relative step; the FP32 polish stops at a 1e-6 relative step (the FP32 resolution of
@@ -68,29 +68,67 @@ __device__ __forceinline__ T WarpSum(T v)
 	return v;
 }
 
-// Pixel-integrated 1D Gaussian factor E = (erf(b) - erf(a)) / 2 and its derivatives in the position and the width
-// (NF >= 3) and the second derivatives E_xx, E_xs, E_ss (NF == 6).
+// Pixel-integrated 1D Gaussian factor E = (erf(b) - erf(a)) / 2, a = (c - x - 1/2) k, b = (c - x + 1/2) k,
+// k = 1 / (sqrt2 s), and its derivatives in the position and the width (NF >= 3) and the second derivatives E_xx,
+// E_xs, E_ss (NF == 6).
 template <typename T>
 struct Fac {
 	T e, dx, ds, xx, xs, ss;
 };
 
+// The factors are formed from values at the pixel boundaries: pixel j spans boundaries j and j + 1, so a row of roi pixels
+// needs roi + 1 erf and exp evaluations instead of 2 roi. Boundary u at z = ((u - h) - x - 1/2) k, k = 1 / (sqrt2 s):
+// E = erf(z), Q0 = exp(-z^2), Q1 = z Q0, Q2 = z Q1, Q3 = z Q2; with r1 = 1 / (sqrt(2 pi) s), r2 = 1 / (sqrt(pi) s)
+// the factor of pixel [a, b] is e = (E_b - E_a) / 2, dx = (Q0_a - Q0_b) r1, ds = (Q1_a - Q1_b) r2 and
+// xx = ds / s, xs = (2 (Q2_a - Q2_b) - Q0_a + Q0_b) r1 / s, ss = 2 (Q3_a - Q1_a - Q3_b + Q1_b) r2 / s.
+template <typename T>
+struct Bound {
+	T E, Q0, Q1, Q2, Q3;
+};
+
+template <typename T>
+struct AxisConst {
+	T k, r1, r2, inv;
+	__device__ __forceinline__ explicit AxisConst(T s)
+	{
+		k = T(1) / (T(1.4142135623730951) * s);
+		r1 = T(1) / (T(2.5066282746310002) * s);
+		r2 = T(1) / (T(1.7724538509055160) * s);
+		inv = T(1) / s;
+	}
+};
+
 template <typename T, int NF>
-__device__ __forceinline__ Fac<T> Factor(T c, T x, T s)
+__device__ __forceinline__ Bound<T> MakeBound(int u, int h, T x, T k)
+{
+	Bound<T> b;
+	const T z = (T(u - h) - x - T(0.5)) * k;
+	b.E = Erf<T>(z);
+	b.Q0 = b.Q1 = b.Q2 = b.Q3 = T(0);
+	if constexpr (NF >= 3) {
+		b.Q0 = Ex<T>(-z * z);
+		b.Q1 = z * b.Q0;
+		if constexpr (NF == 6) {
+			b.Q2 = z * b.Q1;
+			b.Q3 = z * b.Q2;
+		}
+	}
+	return b;
+}
+
+template <typename T, int NF>
+__device__ __forceinline__ Fac<T> FacOf(const Bound<T>& a, const Bound<T>& b, const AxisConst<T>& ac)
 {
 	Fac<T> f;
-	const T k = T(1) / (T(1.4142135623730951) * s);
-	const T a = (c - x - T(0.5)) * k, b = (c - x + T(0.5)) * k;
-	f.e = T(0.5) * (Erf<T>(b) - Erf<T>(a));
+	f.e = T(0.5) * (b.E - a.E);
 	f.dx = f.ds = f.xx = f.xs = f.ss = T(0);
 	if constexpr (NF >= 3) {
-		const T ea = Ex<T>(-a * a), eb = Ex<T>(-b * b);
-		f.dx = (ea - eb) / (T(2.5066282746310002) * s);
-		f.ds = (a * ea - b * eb) / (T(1.7724538509055160) * s);
+		f.dx = (a.Q0 - b.Q0) * ac.r1;
+		f.ds = (a.Q1 - b.Q1) * ac.r2;
 		if constexpr (NF == 6) {
-			f.xx = (a * ea - b * eb) / (T(1.7724538509055160) * s * s);
-			f.xs = (T(2) * a * a * ea - T(2) * b * b * eb - ea + eb) / (T(2.5066282746310002) * s * s);
-			f.ss = T(2) * (a * (a * a - T(1)) * ea - b * (b * b - T(1)) * eb) / (T(1.7724538509055160) * s * s);
+			f.xx = f.ds * ac.inv;
+			f.xs = (T(2) * (a.Q2 - b.Q2) - a.Q0 + b.Q0) * ac.r1 * ac.inv;
+			f.ss = T(2) * (a.Q3 - a.Q1 - b.Q3 + b.Q1) * ac.r2 * ac.inv;
 		}
 	}
 	return f;
@@ -328,10 +366,19 @@ __device__ T Normal(const MleParams& mp, const Pix& px, const T th[5], T G[5], T
 		}
 	}
 	else if constexpr (L == 1) {
-		for (int c = 0; c < roi; ++c) { xt.template Put<NF>(c, Factor<T, NF>(T(c - h), th[2], sx)); }
+		const AxisConst<T> cx(sx), cy(sy);
+		Bound<T> bp = MakeBound<T, NF>(0, h, th[2], cx.k);
+		for (int c = 0; c < roi; ++c) {
+			const Bound<T> bn = MakeBound<T, NF>(c + 1, h, th[2], cx.k);
+			xt.template Put<NF>(c, FacOf<T, NF>(bp, bn, cx));
+			bp = bn;
+		}
+		bp = MakeBound<T, NF>(0, h, th[3], cy.k);
 		int k = 0;
 		for (int i = 0; i < roi; ++i) {
-			const Fac<T> yf = Factor<T, NF>(T(i - h), th[3], sy);
+			const Bound<T> bn = MakeBound<T, NF>(i + 1, h, th[3], cy.k);
+			const Fac<T> yf = FacOf<T, NF>(bp, bn, cy);
+			bp = bn;
 			for (int j = 0; j < roi; ++j, ++k) {
 				const T d = Photons<T>(px, i, j, k);
 				const T psf = GaussPixel<T, NF>(xt.template Get<NF>(j), yf, dsx, dsy, ssx, ssy, P1, P2);
@@ -340,9 +387,21 @@ __device__ T Normal(const MleParams& mp, const Pix& px, const T th[5], T G[5], T
 		}
 	}
 	else {
-		for (int c = gl; c < roi; c += L) {
-			xt.template Put<NF>(c, Factor<T, NF>(T(c - h), th[2], sx));
-			yt.template Put<NF>(c, Factor<T, NF>(T(c - h), th[3], sy));
+		// lanes 0..roi hold the x boundaries, lanes 16..16+roi the y boundaries; pixel factors from lane pairs
+		const AxisConst<T> cx(sx), cy(sy);
+		const bool isY = gl >= 16;
+		const int u = isY ? gl - 16 : gl;
+		Bound<T> b{T(0), T(0), T(0), T(0), T(0)};
+		if (u <= roi) { b = isY ? MakeBound<T, NF>(u, h, th[3], cy.k) : MakeBound<T, NF>(u, h, th[2], cx.k); }
+		Bound<T> bn;
+		bn.E = __shfl_down_sync(0xffffffffu, b.E, 1);
+		bn.Q0 = __shfl_down_sync(0xffffffffu, b.Q0, 1);
+		bn.Q1 = __shfl_down_sync(0xffffffffu, b.Q1, 1);
+		bn.Q2 = __shfl_down_sync(0xffffffffu, b.Q2, 1);
+		bn.Q3 = __shfl_down_sync(0xffffffffu, b.Q3, 1);
+		if (u < roi) {
+			if (isY) { yt.template Put<NF>(u, FacOf<T, NF>(b, bn, cy)); }
+			else { xt.template Put<NF>(u, FacOf<T, NF>(b, bn, cx)); }
 		}
 		__syncwarp();
 		int i = gl / roi, j = gl - i * roi;
@@ -375,23 +434,26 @@ __device__ T Normal(const MleParams& mp, const Pix& px, const T th[5], T G[5], T
 
 __device__ __forceinline__ int Ut(int a, int b) { return a <= b ? a * 5 - (a * (a - 1)) / 2 + (b - a) : b * 5 - (b * (b - 1)) / 2 + (a - b); }
 
-// Cholesky solve of the packed symmetric system (upper triangle) with the diagonal multiplied by diagScale.
+// Cholesky solve of the packed symmetric system (upper triangle) with the diagonal multiplied by diagScale. The pivot
+// ratio is min_i L_ii^2 / A_ii: the pivots of the Jacobi-equilibrated system (unit diagonal), so it measures the
+// conditioning independently of the parameters' units (photons, pixels, nm); 1 for a diagonal system.
 template <typename T>
 __device__ bool Chol5(const T Hm[15], T diagScale, const T rhs[5], T x[5], T* pivotRatio)
 {
 	T Lm[5][5];
-	T maxDiag = T(0), minPiv = T(3e38);
+	T minRatio = T(1);
 	#pragma unroll
 	for (int i = 0; i < 5; ++i) {
 		#pragma unroll
 		for (int j = 0; j <= i; ++j) {
 			T s = Hm[Ut(i, j)];
-			if (i == j) { s *= diagScale; maxDiag = max(maxDiag, s); }
+			const T diag = s * diagScale;
+			if (i == j) { s = diag; }
 			#pragma unroll
 			for (int k = 0; k < j; ++k) { s -= Lm[i][k] * Lm[j][k]; }
 			if (i == j) {
 				if (!(s > T(0))) { return false; }
-				minPiv = min(minPiv, s);
+				minRatio = min(minRatio, s / diag);
 				Lm[i][i] = sqrt(s);
 			}
 			else { Lm[i][j] = s / Lm[j][j]; }
@@ -412,12 +474,13 @@ __device__ bool Chol5(const T Hm[15], T diagScale, const T rhs[5], T x[5], T* pi
 		for (int k = i + 1; k < 5; ++k) { s -= Lm[k][i] * x[k]; }
 		x[i] = s / Lm[i][i];
 	}
-	if (pivotRatio) { *pivotRatio = maxDiag > T(0) ? minPiv / maxDiag : T(0); }
+	if (pivotRatio) { *pivotRatio = minRatio; }
 	return true;
 }
 
 // FP32 solve of (Hm with its diagonal scaled) dt = rhs; re-factored in FP64 when the FP32 factorisation fails or its
-// pivot ratio is below 1e-5 (counted in *fallbacks when count is set).
+// pivot ratio is below 1e-5, i.e. when elimination cancelled more than 5 of the 7 significant digits of FP32 in some
+// pivot (counted in *fallbacks when count is set).
 __device__ bool Solve32(const float Hm[15], float scale, const float rhs[5], float dt[5], unsigned* fallbacks, bool count)
 {
 	float ratio = 0.f;
@@ -745,12 +808,20 @@ __global__ void __launch_bounds__(kThreads) MleInitKernel(const uint16_t* __rest
 
 constexpr uint32_t kNone = 0xffffffffu;
 
-// Work queue of the persistent kernels: warp w owns candidates [w * chunk, (w + 1) * chunk), chunk >= 32; lanes that
-// need work take the next candidates of the range in lane order.
+// Work queue of the persistent kernels. With a counter (zeroed before the launch) it is global: lanes that need work
+// take the next candidates with one atomic per warp, so warps that finish early keep taking work until all
+// candidates are out. Without one, warp w owns the static range [w * chunk, (w + 1) * chunk), chunk >= 32.
 struct WarpQueue {
 	uint32_t cursor, end;
-	__device__ __forceinline__ bool Init(uint32_t n)
+	unsigned int* counter;
+	__device__ __forceinline__ bool Init(uint32_t n, unsigned int* ctr)
 	{
+		counter = ctr;
+		if (counter) {
+			cursor = 0;
+			end = n;
+			return n > 0;
+		}
 		const uint32_t warps = gridDim.x * (blockDim.x / 32);
 		const uint32_t gw = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
 		const uint32_t chunk = max(32u, (n + warps - 1) / warps);
@@ -759,11 +830,22 @@ struct WarpQueue {
 		end = static_cast<uint32_t>(min(begin + chunk, static_cast<unsigned long long>(n)));
 		return cursor < end;
 	}
-	// Called by all 32 lanes; returns the candidate taken by a lane with `need` set (kNone when the range is done).
+	// Called by all 32 lanes; returns the candidate taken by a lane with `need` set (kNone when the queue is done).
 	__device__ __forceinline__ uint32_t Take(bool need)
 	{
 		const unsigned mask = __ballot_sync(0xffffffffu, need);
-		const uint32_t k = cursor + __popc(mask & ((1u << (threadIdx.x & 31)) - 1u));
+		const int lane = threadIdx.x & 31;
+		if (counter) {
+			if (mask == 0 || cursor >= end) { return kNone; }
+			const int leader = __ffs(mask) - 1;
+			uint32_t base = 0;
+			if (lane == leader) { base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask))); }
+			base = __shfl_sync(0xffffffffu, base, leader);
+			if (base + static_cast<uint32_t>(__popc(mask)) >= end) { cursor = end; }  // the queue ran out: stop taking
+			const uint32_t k = base + __popc(mask & ((1u << lane) - 1u));
+			return need && k < end ? k : kNone;
+		}
+		const uint32_t k = cursor + __popc(mask & ((1u << lane) - 1u));
 		cursor = min(end, cursor + static_cast<uint32_t>(__popc(mask)));
 		return need && k < end ? k : kNone;
 	}
@@ -800,7 +882,7 @@ __global__ void __launch_bounds__(kThreads) MleLmKernel(const uint16_t* __restri
 	float* ph = reinterpret_cast<float*>(smem) + threadIdx.x;
 	const FacTab<float> xt{reinterpret_cast<float*>(smem) + mp.n * T + threadIdx.x, T};
 	WarpQueue q;
-	if (!q.Init(CandCount(nptr, nconst))) { return; }
+	if (!q.Init(CandCount(nptr, nconst), mp.queue)) { return; }
 	uint32_t k = kNone;
 	bool fresh = false;
 	float th[5] = {0, 0, 0, 0, 0}, G[5], Hm[15], D = 0.f, lambda = 1e-3f, x0 = 0.f, y0 = 0.f;
@@ -905,7 +987,7 @@ __global__ void __launch_bounds__(kThreads) MlePolishKernel(const uint16_t* __re
 	float* ph = reinterpret_cast<float*>(smem) + threadIdx.x;
 	const FacTab<float> xt{reinterpret_cast<float*>(smem) + mp.n * T + threadIdx.x, T};
 	WarpQueue q;
-	if (!q.Init(CandCount(nptr, nconst))) { return; }
+	if (!q.Init(CandCount(nptr, nconst), mp.queue ? mp.queue + 1 : nullptr)) { return; }
 	uint32_t k = kNone;
 	bool fresh = false;
 	float th[5] = {0, 0, 0, 0, 0}, dt[5] = {0, 0, 0, 0, 0}, G[5], Hm[15], Fm[15], D = 0.f, x0 = 0.f, y0 = 0.f;
@@ -1138,6 +1220,7 @@ bool LaunchThreadPerRoi(const uint16_t* img, int H, int W, long long N, const Ca
 	const size_t finalBytes = static_cast<size_t>(3 * mp.roi) * sizeof(double) * kThreads;
 	const int lmBlocks = PersistentBlocks(MleLmKernel<MODEL>, lmBytes, sms, cap);
 	const int polishBlocks = PersistentBlocks(MlePolishKernel<MODEL>, polishBytes, sms, cap);
+	if (mp.queue && !PTB_CUDA(cudaMemsetAsync(mp.queue, 0, 2 * sizeof(unsigned int), st))) { return false; }
 	if (marks) { cudaEventRecord(marks[0], st); }
 	MleInitKernel<MODEL><<<blocks, kThreads, initBytes, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows);
 	if (marks) { cudaEventRecord(marks[1], st); }

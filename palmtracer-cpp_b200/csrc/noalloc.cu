@@ -33,6 +33,7 @@ struct NoAllocScratch {
 	uint32_t planeCount[kNoAllocMaxPlanes];
 	uint8_t flags[kNoAllocMaxPoints];
 	unsigned int fallbacks;
+	unsigned int mleQueue[2];  // work-queue counters of the persistent fit kernels (zeroed by the fit launch)
 };
 
 // The scratch. In host code this name is only a stand-in for the symbol, never a device address: kernels receive
@@ -151,6 +152,7 @@ long long FittingDeviceNoAlloc(const uint16_t* dStack, const double* dPositions,
 	NoAllocScratch* s = ScratchForCurrentDevice();
 	if (s == nullptr) { return -1; }
 	fp.mle.fallbacks = &s->fallbacks;
+	fp.mle.queue = s->mleQueue;
 	fp.lanes = lanes;
 	const uint32_t n = static_cast<uint32_t>(nPoints);
 	const uint32_t blocks = std::min<uint32_t>((n + 255) / 256, 148u * 4u);

@@ -81,6 +81,7 @@ struct MleParams {
 	const float* table;        // mode 8: cell-major [cell][64], FP32 (FP32 phases)
 	const double* table64;     // mode 8: the same in FP64 (FP64 phases)
 	unsigned int* fallbacks;   // FP64 Cholesky re-factorisations (diagnostics)
+	unsigned int* queue;       // 2 work-queue counters of the persistent fit kernels (zeroed by the launch), or null
 	unsigned long long* evals; // profiling, or null: model evaluations [FP32 LM, FP32 polish, FP64 pre-scan + final]
 };
 
@@ -103,12 +104,35 @@ struct FitParams {
 	cudaEvent_t* marks;    // profiling, or null: 5 events recorded around the phases of the modes 6-8 fit
 };
 
+// Division of a 31-bit unsigned value by a fixed divisor d >= 1 as one multiply and a shift (division by invariant
+// integers, Granlund and Montgomery 1994): with s = ceil(log2 d) and m = ceil(2^(31+s) / d) (m < 2^32),
+// (n * m) >> (31 + s) equals floor(n / d) for every n < 2^31, because m * d - 2^(31+s) < d <= 2^s.
+struct FastDiv {
+	uint32_t d, m, s;
+};
+
+inline FastDiv MakeFastDiv(uint32_t d)
+{
+	FastDiv f;
+	f.d = d;
+	f.s = 0;
+	while ((1ull << f.s) < d) { ++f.s; }
+	f.m = static_cast<uint32_t>(((1ull << (31 + f.s)) + d - 1) / d);
+	return f;
+}
+
+__host__ __device__ __forceinline__ uint32_t FastDivide(uint32_t n, const FastDiv& f)
+{
+	return static_cast<uint32_t>((static_cast<unsigned long long>(n) * f.m) >> (31 + f.s));
+}
+
 // Geometry of one chunk: B frames of H x W pixels; global pixel index g = f * N + y * W + x (fits in 31 bits).
 struct Geometry {
 	int H, W, B;
 	int words;  // 32-bit words per row of the root bitmask
 	long long N;
 	long long P;  // B * N
+	FastDiv divN, divW;
 };
 
 // Device workspace of one chunk. Dense arrays have P entries, lists have their stated capacities.

@@ -30,11 +30,44 @@ struct Pix {
 __device__ __forceinline__ Pix Decompose(uint32_t g, const Geometry& geo)
 {
 	Pix p;
-	p.f = static_cast<int>(g / static_cast<unsigned long long>(geo.N));
-	const long long r = static_cast<long long>(g) - static_cast<long long>(p.f) * geo.N;
-	p.y = static_cast<int>(r / geo.W);
-	p.x = static_cast<int>(r - static_cast<long long>(p.y) * geo.W);
+	const uint32_t f = FastDivide(g, geo.divN);
+	const uint32_t r = g - f * geo.divN.d;
+	const uint32_t y = FastDivide(r, geo.divW);
+	p.f = static_cast<int>(f);
+	p.y = static_cast<int>(y);
+	p.x = static_cast<int>(r - y * geo.divW.d);
 	return p;
+}
+
+// Position of each predicated lane in a list grown by `counter`: one atomic per warp. Called by all 32 lanes.
+__device__ __forceinline__ uint32_t WarpAppendIndex(bool pred, uint32_t* counter)
+{
+	const unsigned mask = __ballot_sync(0xffffffffu, pred);
+	if (mask == 0) { return 0; }
+	const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+	uint32_t base = 0;
+	if (lane == leader) { base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask))); }
+	base = __shfl_sync(0xffffffffu, base, leader);
+	return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+// Sum of v over the run of consecutive lanes holding the same key as this lane, valid in the run's first lane
+// (returned head = true); runs are maximal stretches of equal keys. Called by all 32 lanes.
+template <typename T>
+__device__ __forceinline__ T RunSum(uint32_t key, T v, bool& head)
+{
+	const int lane = threadIdx.x & 31;
+	const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+	head = lane == 0 || prev != key;
+	const unsigned heads = __ballot_sync(0xffffffffu, head);
+	const unsigned after = lane == 31 ? 0u : (heads & (0xffffffffu << (lane + 1)));
+	const int runEnd = after ? __ffs(after) - 2 : 31;
+	#pragma unroll
+	for (int d = 1; d < 32; d <<= 1) {
+		const T t = __shfl_down_sync(0xffffffffu, v, d);
+		if (lane + d <= runEnd) { v += t; }
+	}
+	return v;
 }
 
 __device__ __forceinline__ uint32_t Find(const uint32_t* par, uint32_t x)
@@ -128,13 +161,25 @@ __global__ void CclFlatten(Workspace ws)
 }
 
 // Components: enumerate roots and tag par[root] with the component id.
+// Grid-stride loop in whole warps: every lane of a warp runs the same iterations (k may be >= n on the last one), so
+// warp-wide collectives are safe inside.
+#define PTB_WARP_LOOP(k, n)                                                                                        \
+	for (uint32_t k##Base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u, k = k##Base + (threadIdx.x & 31u); \
+	     k##Base < (n); k##Base += gridDim.x * blockDim.x, k = k##Base + (threadIdx.x & 31u))
+
 __global__ void CompEnumerate(Workspace ws)
 {
 	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
-	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-		const uint32_t p = ws.dom[k];
-		if (ws.par[p] != p) { continue; }
-		const uint32_t c = atomicAdd(&ws.cnt->ncomp, 1u);
+	PTB_WARP_LOOP(k, n)
+	{
+		uint32_t p = 0;
+		bool root = false;
+		if (k < n) {
+			p = ws.dom[k];
+			root = ws.par[p] == p;
+		}
+		const uint32_t c = WarpAppendIndex(root, &ws.cnt->ncomp);
+		if (!root) { continue; }
 		if (c >= ws.capComp) { atomicExch(&ws.cnt->overflow, 1u); continue; }
 		ws.compRoot[c] = p;
 		ws.compSize[c] = 0;
@@ -147,9 +192,12 @@ __global__ void CompEnumerate(Workspace ws)
 __global__ void CompCount(Workspace ws)
 {
 	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
-	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-		const uint32_t p = ws.dom[k];
-		atomicAdd(ws.compSize + CompOf(ws.par, p), 1u);
+	PTB_WARP_LOOP(k, n)
+	{
+		const uint32_t c = k < n ? CompOf(ws.par, ws.dom[k]) : 0xffffffffu;
+		bool head;
+		const uint32_t count = RunSum<uint32_t>(c, 1u, head);
+		if (head && c != 0xffffffffu) { atomicAdd(ws.compSize + c, count); }
 	}
 }
 
@@ -251,9 +299,11 @@ __global__ void LabelDomain(Workspace ws, int strict)
 __global__ void GroupEnumerate(Workspace ws)
 {
 	const uint32_t n = min(ws.cnt->ncomp, ws.capComp);
-	for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-		if (ws.compNRoot[c] < 2) { continue; }
-		const uint32_t m = atomicAdd(&ws.cnt->nmulti, 1u);
+	PTB_WARP_LOOP(c, n)
+	{
+		const bool multi = c < n && ws.compNRoot[c] >= 2;
+		const uint32_t m = WarpAppendIndex(multi, &ws.cnt->nmulti);
+		if (!multi) { continue; }
 		ws.multi[m] = c;
 		ws.compRegion[c] = m;  // from here on: the group index of a multi-region component
 		ws.gOff[m] = ws.compSize[c];
@@ -335,58 +385,79 @@ __device__ void SortSlice(uint32_t* a, uint32_t n)
 // Binary heap with the steps of libstdc++'s push_heap / pop_heap (bits/stl_heap.h) under the reference comparator
 // (Pixel::operator<, lib/Structs.hpp:20-27): "a before b" iff a.key > b.key, so the top holds the smallest key and
 // equal keys come out in the same order as from the reference's std::priority_queue.
+// Entry i lives at key[i * stride], pix[i * stride]: a lane-interleaved slice of shared memory while the heap holds at
+// most `cap` entries, then (Spill) the group's own slice of global memory, sized for the whole group.
 struct Heap {
 	double* key;
 	uint32_t* pix;
 	uint32_t len;
+	uint32_t stride;
+	uint32_t cap;
+	double* gkey;
+	uint32_t* gpix;
 
 	__device__ __forceinline__ static bool Less(double a, double b) { return a > b; }
+	__device__ __forceinline__ double& K(uint32_t i) { return key[i * stride]; }
+	__device__ __forceinline__ uint32_t& P(uint32_t i) { return pix[i * stride]; }
+
+	__device__ void Spill()
+	{
+		for (uint32_t i = 0; i < len; ++i) {
+			gkey[i] = K(i);
+			gpix[i] = P(i);
+		}
+		key = gkey;
+		pix = gpix;
+		stride = 1;
+		cap = 0xffffffffu;
+	}
 
 	__device__ void SiftUp(uint32_t hole, uint32_t top, double k, uint32_t v)
 	{
 		uint32_t parent = (hole - 1) / 2;
-		while (hole > top && Less(key[parent], k)) {
-			key[hole] = key[parent];
-			pix[hole] = pix[parent];
+		while (hole > top && Less(K(parent), k)) {
+			K(hole) = K(parent);
+			P(hole) = P(parent);
 			hole = parent;
 			parent = (hole - 1) / 2;
 		}
-		key[hole] = k;
-		pix[hole] = v;
+		K(hole) = k;
+		P(hole) = v;
 	}
 
 	__device__ void Push(double k, uint32_t v)
 	{
+		if (len == cap) { Spill(); }
 		const uint32_t hole = len++;
-		if (hole == 0) { key[0] = k; pix[0] = v; return; }
+		if (hole == 0) { K(0) = k; P(0) = v; return; }
 		SiftUp(hole, 0, k, v);
 	}
 
 	// Removes the top; returns its pixel.
 	__device__ uint32_t Pop()
 	{
-		const uint32_t top = pix[0];
+		const uint32_t top = P(0);
 		if (len > 1) {
 			const uint32_t last = len - 1;  // element moved out of the way ("value" in __pop_heap)
-			const double vk = key[last];
-			const uint32_t vp = pix[last];
+			const double vk = K(last);
+			const uint32_t vp = P(last);
 			// __adjust_heap(first, 0, len = last, value)
 			const uint32_t n = last;
 			uint32_t hole = 0, child = 0;
 			while (n >= 2 && child < (n - 1) / 2) {
 				child = 2 * (child + 1);
-				if (Less(key[child], key[child - 1])) { --child; }
-				key[hole] = key[child];
-				pix[hole] = pix[child];
+				if (Less(K(child), K(child - 1))) { --child; }
+				K(hole) = K(child);
+				P(hole) = P(child);
 				hole = child;
 			}
 			if ((n & 1) == 0 && child == (n - 2) / 2) {
 				child = 2 * (child + 1);
-				key[hole] = key[child - 1];
-				pix[hole] = pix[child - 1];
+				K(hole) = K(child - 1);
+				P(hole) = P(child - 1);
 				hole = child - 1;
 			}
-			if (hole == 0) { key[0] = vk; pix[0] = vp; }
+			if (hole == 0) { K(0) = vk; P(0) = vp; }
 			else { SiftUp(hole, 0, vk, vp); }
 		}
 		--len;
@@ -394,11 +465,20 @@ struct Heap {
 	}
 };
 
+constexpr int kFloodThreads = 64;
+constexpr uint32_t kSmemHeap = 48;  // shared-memory heap entries per thread (12 bytes each)
+
+struct FloodSmem {
+	double key[kSmemHeap * kFloodThreads];
+	uint32_t pix[kSmemHeap * kFloodThreads];
+};
+
 // Priority flood of one group from its labelled seeds (sorted ascending = raster order), Segmentation2D.cpp:336-385.
-__device__ void FloodGroup(const Workspace& ws, const uint32_t* seedList, uint32_t nSeeds, double* hk, uint32_t* hp)
+// The heap starts in the thread's shared-memory slice and moves to the group's global slice (hk, hp) if it outgrows it.
+__device__ void FloodGroup(const Workspace& ws, const uint32_t* seedList, uint32_t nSeeds, double* hk, uint32_t* hp, FloodSmem& sm)
 {
 	const Geometry& geo = ws.g;
-	Heap heap{hk, hp, 0};
+	Heap heap{sm.key + threadIdx.x, sm.pix + threadIdx.x, 0, kFloodThreads, kSmemHeap, hk, hp};
 	for (uint32_t i = 0; i < nSeeds; ++i) {
 		const uint32_t s = seedList[i];
 		const Pix q = Decompose(s, geo);
@@ -421,38 +501,56 @@ __device__ void FloodGroup(const Workspace& ws, const uint32_t* seedList, uint32
 		++pops;
 		const Pix q = Decompose(p, geo);
 		const uint32_t L = ws.lab[p];
-		for (int dy = -1; dy <= 1; ++dy) {
-			const int yy = q.y + dy;
-			if (yy < 0 || yy >= geo.H) { continue; }
-			for (int dx = -1; dx <= 1; ++dx) {
-				const int xx = q.x + dx;
-				if ((dx == 0 && dy == 0) || xx < 0 || xx >= geo.W) { continue; }
-				const uint32_t nb = p + static_cast<uint32_t>(dy * geo.W + dx);
-				if ((ws.code[nb] & kDomain) && ws.lab[nb] == 0) {
-					// key = -v + it * EPSILON, both operations rounded separately as in the reference
-					const double k = __dadd_rn(-(static_cast<double>(ws.w1[nb]) * kW1Unit), __dmul_rn(static_cast<double>(pops), kEps));
-					heap.Push(k, nb);
-					ws.lab[nb] = L;
-				}
+		// the 8 neighbours in the reference's scan order; their code, label and W1 are loaded together (each
+		// neighbour's label is written at most once below, after its own test)
+		uint32_t nb[8];
+		bool in[8];
+		uint8_t cd[8];
+		uint32_t lb[8];
+		long long wv[8];
+		#pragma unroll
+		for (int t = 0; t < 8; ++t) {
+			const int dy = t < 3 ? -1 : (t < 5 ? 0 : 1);
+			const int dx = t < 3 ? t - 1 : (t < 5 ? (t == 3 ? -1 : 1) : t - 6);
+			const int yy = q.y + dy, xx = q.x + dx;
+			in[t] = yy >= 0 && yy < geo.H && xx >= 0 && xx < geo.W;
+			nb[t] = p + static_cast<uint32_t>(dy * geo.W + dx);
+		}
+		#pragma unroll
+		for (int t = 0; t < 8; ++t) {
+			cd[t] = in[t] ? __ldg(ws.code + nb[t]) : static_cast<uint8_t>(0);
+			lb[t] = in[t] ? ws.lab[nb[t]] : 1u;
+			wv[t] = in[t] ? __ldg(ws.w1 + nb[t]) : 0ll;
+		}
+		const double age = __dmul_rn(static_cast<double>(pops), kEps);
+		#pragma unroll
+		for (int t = 0; t < 8; ++t) {
+			if ((cd[t] & kDomain) && lb[t] == 0) {
+				// key = -v + it * EPSILON, both operations rounded separately as in the reference
+				const double k = __dadd_rn(-(static_cast<double>(wv[t]) * kW1Unit), age);
+				heap.Push(k, nb[t]);
+				ws.lab[nb[t]] = L;
 			}
 		}
 	}
 }
 
-__global__ void GroupFlood(Workspace ws, uint32_t nGroupsStrict)
+__global__ void __launch_bounds__(kFloodThreads) GroupFlood(Workspace ws, uint32_t nGroupsStrict)
 {
+	__shared__ FloodSmem sm;
 	const uint32_t n = nGroupsStrict ? nGroupsStrict : ws.cnt->nmulti;
 	for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
 		const uint32_t nSeeds = ws.gSeedOff[m + 1] - ws.gSeedOff[m];
 		uint32_t* seeds = ws.gSeed + ws.gSeedOff[m];
 		SortSlice(seeds, nSeeds);
-		FloodGroup(ws, seeds, nSeeds, ws.heapKey + ws.gOff[m], ws.heapPix + ws.gOff[m]);
+		FloodGroup(ws, seeds, nSeeds, ws.heapKey + ws.gOff[m], ws.heapPix + ws.gOff[m], sm);
 	}
 }
 
 // Basin fusion of one group (Segmentation2D.cpp:181-291) followed by the reseeded second flood.
-__global__ void GroupFuse(Workspace ws, uint32_t nGroupsStrict, double ratio)
+__global__ void __launch_bounds__(kFloodThreads) GroupFuse(Workspace ws, uint32_t nGroupsStrict, double ratio)
 {
+	__shared__ FloodSmem sm;
 	const uint32_t n = nGroupsStrict ? nGroupsStrict : ws.cnt->nmulti;
 	const Geometry& geo = ws.g;
 	for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
@@ -546,26 +644,43 @@ __global__ void GroupFuse(Workspace ws, uint32_t nGroupsStrict, double ratio)
 			ws.lab[ws.fuMaxPos[r]] = r + 1;
 		}
 		SortSlice(seeds, nReg);
-		FloodGroup(ws, seeds, nReg, ws.heapKey + ws.gOff[m], ws.heapPix + ws.gOff[m]);
+		FloodGroup(ws, seeds, nReg, ws.heapKey + ws.gOff[m], ws.heapPix + ws.gOff[m], sm);
 	}
 }
 
 // Exact integer sums per region (ComputeStatistics, Segmentation2D.cpp:144-175).
+// Consecutive domain-list entries of one warp that belong to the same region are summed with shuffles first, so
+// there is one set of atomics per run instead of per pixel (integer sums: the order does not matter).
 __global__ void RegionStats(Workspace ws)
 {
 	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
 	const Geometry& geo = ws.g;
-	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-		const uint32_t p = ws.dom[k];
-		const uint32_t L = ws.lab[p];
-		if (L == 0) { continue; }
-		const uint32_t r = L - 1;
-		const Pix q = Decompose(p, geo);
-		const unsigned long long v = static_cast<unsigned long long>(ws.w1[p]);
-		atomicAdd(ws.regCount + r, 1u);
-		atomicAdd(ws.regSumV + r, v);
-		atomicAdd(ws.regSumVJ + r, v * static_cast<unsigned long long>(q.x));
-		atomicAdd(ws.regSumVI + r, v * static_cast<unsigned long long>(q.y));
+	PTB_WARP_LOOP(k, n)
+	{
+		uint32_t r = 0xffffffffu;
+		unsigned long long v = 0, vx = 0, vy = 0;
+		if (k < n) {
+			const uint32_t p = ws.dom[k];
+			const uint32_t L = ws.lab[p];
+			if (L != 0) {
+				r = L - 1;
+				const Pix q = Decompose(p, geo);
+				v = static_cast<unsigned long long>(ws.w1[p]);
+				vx = v * static_cast<unsigned long long>(q.x);
+				vy = v * static_cast<unsigned long long>(q.y);
+			}
+		}
+		bool head;
+		const uint32_t cnt = RunSum<uint32_t>(r, r != 0xffffffffu ? 1u : 0u, head);
+		v = RunSum<unsigned long long>(r, v, head);
+		vx = RunSum<unsigned long long>(r, vx, head);
+		vy = RunSum<unsigned long long>(r, vy, head);
+		if (head && r != 0xffffffffu) {
+			atomicAdd(ws.regCount + r, cnt);
+			atomicAdd(ws.regSumV + r, v);
+			atomicAdd(ws.regSumVJ + r, vx);
+			atomicAdd(ws.regSumVI + r, vy);
+		}
 	}
 }
 
@@ -660,11 +775,11 @@ bool LaunchSegment(const Workspace& ws, double ratio, int strict, uint32_t maxPo
 	}
 	GroupScatter<<<kGrid, kThreads, 0, st>>>(ws, strict);
 	// one thread per group: small CTAs so that many SMs share the (uneven) groups
-	GroupFlood<<<kGrid * 2, 64, 0, st>>>(ws, groupsStrict);
+	GroupFlood<<<kGrid * 2, kFloodThreads, 0, st>>>(ws, groupsStrict);
 	CountLaunch(2);
 	ok = ok && PTB_LAUNCHED();
 	if (static_cast<int>(ratio) > 0) {  // WatershedIntelligent, Segmentation2D.cpp:77-85
-		GroupFuse<<<kGrid * 2, 64, 0, st>>>(ws, groupsStrict, ratio);
+		GroupFuse<<<kGrid * 2, kFloodThreads, 0, st>>>(ws, groupsStrict, ratio);
 		CountLaunch();
 		ok = ok && PTB_LAUNCHED();
 	}
