@@ -20,7 +20,8 @@ bool LaunchDetect(const Workspace& ws, double thr, cudaStream_t st);
 bool LaunchPlane(const uint16_t* img, double* out, int H, int W, int B, int level, cudaStream_t st);
 bool LaunchSegment(const Workspace& ws, double ratio, int strict, uint32_t maxPoints, cudaStream_t st);
 bool LaunchBuildCandidates(const Workspace& ws, cudaStream_t st);
-bool LaunchSortFrames(const Workspace& ws, double* out, unsigned long long idBase, unsigned long long planeBase, cudaStream_t st);
+bool LaunchSortFrames(const Workspace& ws, double* out, unsigned long long* rowBase, bool offsetOut, unsigned long long planeBase,
+                      cudaStream_t st);
 bool LaunchFit(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
                uint32_t cap, const FitParams& fp, double* rows, uint8_t* flags, int precision, cudaStream_t st);
 
@@ -236,7 +237,10 @@ Engine::~Engine()
 	if (spline_) { cudaFree(spline_); }
 	if (fallbacks_) { cudaFree(fallbacks_); }
 	if (evalDev_) { cudaFree(evalDev_); }
+	if (rowBase_) { cudaFree(rowBase_); }
+	if (rows2_) { cudaFree(rows2_); }
 	if (hostCnt_) { cudaFreeHost(hostCnt_); }
+	if (copy_) { cudaStreamDestroy(copy_); }
 	if (stream_) { cudaStreamDestroy(stream_); }
 }
 
@@ -245,7 +249,16 @@ bool Engine::Init()
 	if (stream_) { return true; }
 	if (!PTB_CUDA(cudaGetDevice(&device_))) { return false; }
 	if (!PTB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking))) { return false; }
-	if (!PTB_CUDA(cudaMallocHost(&hostCnt_, sizeof(Counters)))) { return false; }
+	if (!PTB_CUDA(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking))) { return false; }
+	if (!PTB_CUDA(cudaMallocHost(&hostCnt_, 2 * sizeof(Counters)))) { return false; }
+	if (!PTB_CUDA(cudaMalloc(&rowBase_, sizeof(unsigned long long)))) { return false; }
+	for (int k = 0; k < 2; ++k) {
+		if (!PTB_CUDA(cudaEventCreateWithFlags(&h2d_[k], cudaEventDisableTiming)) ||
+		    !PTB_CUDA(cudaEventCreateWithFlags(&done_[k], cudaEventDisableTiming)) ||
+		    !PTB_CUDA(cudaEventCreateWithFlags(&d2h_[k], cudaEventDisableTiming))) {
+			return false;
+		}
+	}
 	for (auto& e : ev_) {
 		if (!PTB_CUDA(cudaEventCreate(&e))) { return false; }
 	}
@@ -297,18 +310,26 @@ int Engine::ChunkFrames(int H, int W, uint64_t planes, uint32_t maxPoints) const
 
 // Runs detection -> segmentation -> fits -> ordering for B frames whose pixels are at dImg (device). The chunk's
 // rows go to dOut (device) numbered from Id idBase + 1 and Plane planeBase + 1; returns the row count or -1.
-long long Engine::RunChunk(const uint16_t* dImg, int H, int W, int B, double thr, double ratio, uint32_t maxPoints,
-                           const FitParams& fp, double* dOut, unsigned long long idBase, unsigned long long planeBase,
-                           uint32_t* truncatedFrames)
+bool Engine::ReserveRows2(size_t bytes)
+{
+	if (bytes <= rows2Bytes_) { return true; }
+	if (rows2_) { cudaFree(rows2_); rows2_ = nullptr; rows2Bytes_ = 0; }
+	if (!PTB_CUDA(cudaMalloc(&rows2_, bytes))) { return false; }
+	rows2Bytes_ = bytes;
+	return true;
+}
+
+bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, double thr, double ratio, uint32_t maxPoints,
+                          const FitParams& fp, double* dOut, bool offsetOut, unsigned long long planeBase)
 {
 	ws_.img = dImg;
 	cudaStream_t st = stream_;
 	const bool prof = profiling_ != 0;
-	uint64_t l0 = LaunchCount(), launches[kStages] = {};
+	uint64_t l0 = LaunchCount();
 	auto mark = [&](int k) {
 		if (prof) {
 			cudaEventRecord(ev_[k], st);
-			if (k > 0) { launches[k - 1] = LaunchCount() - l0; l0 = LaunchCount(); }
+			if (k > 0) { pendLaunches_[k - 1] = LaunchCount() - l0; l0 = LaunchCount(); }
 		}
 	};
 	bool ok = PTB_CUDA(cudaMemsetAsync(ws_.cnt, 0, sizeof(Counters), st));
@@ -321,8 +342,9 @@ long long Engine::RunChunk(const uint16_t* dImg, int H, int W, int B, double thr
 	mark(2);
 	FitParams fpr = fp;
 	if (ok && fp.mode >= kMleGauss && fp.lanes == 0) { ok = Autotune(fpr, dImg, H, W); }
-	const bool mleProf = prof && fp.mode >= kMleGauss;
-	if (mleProf) {
+	pendMleProf_ = prof && fp.mode >= kMleGauss;
+	pendLanes_ = fpr.lanes;
+	if (pendMleProf_) {
 		if (!evalDev_) { ok = ok && PTB_CUDA(cudaMalloc(&evalDev_, 3 * sizeof(unsigned long long))); }
 		ok = ok && PTB_CUDA(cudaMemsetAsync(evalDev_, 0, 3 * sizeof(unsigned long long), st));
 		fpr.marks = mleEv_;
@@ -330,38 +352,49 @@ long long Engine::RunChunk(const uint16_t* dImg, int H, int W, int B, double thr
 	}
 	ok = ok && LaunchFit(dImg, H, W, ws_.g.N, ws_.cand, &ws_.cnt->nfit, 0, ws_.capRows, fpr, ws_.rows, ws_.fitFlag, precision_, st);
 	mark(3);
-	ok = ok && LaunchSortFrames(ws_, dOut, idBase, planeBase, st);
+	ok = ok && LaunchSortFrames(ws_, dOut, rowBase_, offsetOut, planeBase, st);
 	mark(4);
-	ok = ok && PTB_CUDA(cudaMemcpyAsync(hostCnt_, ws_.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
-	ok = ok && PTB_CUDA(cudaStreamSynchronize(st));
-	if (!ok) { return -1; }
-	if (prof) {
+	ok = ok && PTB_CUDA(cudaMemcpyAsync(hostCnt_ + slot, ws_.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+	ok = ok && PTB_CUDA(cudaEventRecord(done_[slot], st));
+	return ok;
+}
+
+long long Engine::CompleteChunk(int slot, uint32_t* truncatedFrames)
+{
+	if (!PTB_CUDA(cudaEventSynchronize(done_[slot]))) { return -1; }
+	if (profiling_) {
 		for (int k = 0; k < 4; ++k) {
 			float ms = 0.f;
 			cudaEventElapsedTime(&ms, ev_[k], ev_[k + 1]);
 			stageMs_[k] += ms;
-			stageLaunches_[k] += launches[k];
+			stageLaunches_[k] += pendLaunches_[k];
 		}
 	}
-	if (mleProf) {
+	if (pendMleProf_) {
 		for (int k = 0; k < 4; ++k) {
 			float ms = 0.f;
 			cudaEventElapsedTime(&ms, mleEv_[k], mleEv_[k + 1]);
 			stageMs_[5 + k] += ms;
-			stageLaunches_[5 + k] += (k == 1 || fpr.lanes == 1) ? 1 : 0;
+			stageLaunches_[5 + k] += (k == 1 || pendLanes_ == 1) ? 1 : 0;
 		}
 		unsigned long long ev[3] = {};
 		if (!PTB_CUDA(cudaMemcpy(ev, evalDev_, sizeof(ev), cudaMemcpyDeviceToHost))) { return -1; }
 		for (int k = 0; k < 3; ++k) { evalTotals_[k] += ev[k]; }
+		pendMleProf_ = false;
 	}
-	if (hostCnt_->overflow) {
+	const Counters& c = hostCnt_[slot];
+	if (c.overflow) {
 		SetError("internal capacity overflow");
 		return -1;
 	}
-	if (truncatedFrames) { *truncatedFrames += hostCnt_->truncated; }
-	return hostCnt_->nfit;
+	if (truncatedFrames) { *truncatedFrames += c.truncated; }
+	return c.nfit;
 }
 
+// Chunks run back to back on the compute stream; with host buffers, the input of chunk k + 1 is copied in and the rows
+// of chunk k - 1 are copied out on the copy stream while chunk k computes (two staging slots for the frames and, for
+// host output, for the ordered rows). Row numbering continues across chunks through a device-side row count, so the
+// host waits for a chunk only to learn how many rows it copies out.
 long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* output, bool outputOnDevice, uint64_t outputSize,
                            uint64_t height, uint64_t width, uint64_t planes, double thr, double ratio, uint64_t fit,
                            const double* fitParams)
@@ -384,26 +417,61 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 	const uint32_t rowsCap = static_cast<uint32_t>(std::min<uint64_t>(static_cast<uint64_t>(B) * maxPoints, 0xffffffffu));
 	if (!Reserve(H, W, B, rowsCap)) { return -1; }
 	const size_t N = static_cast<size_t>(H) * W;
-	if (!inputOnDevice && !ReserveImage(N * B * sizeof(uint16_t))) { return -1; }
+	const uint64_t chunks = (planes + B - 1) / B;
+	const size_t slotBytes = N * B * sizeof(uint16_t);
+	if (!inputOnDevice && !ReserveImage((chunks > 1 ? 2 : 1) * slotBytes)) { return -1; }
+	if (!outputOnDevice && chunks > 1 && !ReserveRows2(static_cast<size_t>(ws_.capRows) * kCols * sizeof(double))) { return -1; }
+	double* outSlot[2] = {ws_.sortedRows, static_cast<double*>(rows2_)};
+	auto imgSlot = [&](int slot) { return static_cast<uint16_t*>(img_) + (slot ? N * B : 0); };
+	auto framesOf = [&](uint64_t k) { return static_cast<int>(std::min<uint64_t>(B, planes - k * B)); };
+	if (!PTB_CUDA(cudaMemsetAsync(rowBase_, 0, sizeof(unsigned long long), stream_))) { return -1; }
+	// input of chunk k into its slot; the slot's previous chunk (k - 2) must have finished reading it
+	auto copyIn = [&](uint64_t k) {
+		const int slot = static_cast<int>(k & 1);
+		if (k >= 2 && !PTB_CUDA(cudaStreamWaitEvent(copy_, done_[slot], 0))) { return false; }
+		if (!PTB_CUDA(cudaMemcpyAsync(imgSlot(slot), input + k * B * N, N * framesOf(k) * sizeof(uint16_t), cudaMemcpyHostToDevice, copy_))) {
+			return false;
+		}
+		return PTB_CUDA(cudaEventRecord(h2d_[slot], copy_));
+	};
 	unsigned long long rows = 0;
 	uint32_t truncated = 0;
-	for (uint64_t z0 = 0; z0 < planes; z0 += B) {
-		const int b = static_cast<int>(std::min<uint64_t>(B, planes - z0));
-		PlanWorkspace(ws_, H, W, b, rowsCap, static_cast<char*>(pool_));
-		const uint16_t* dImg = input + z0 * N;
-		if (!inputOnDevice) {
-			if (!PTB_CUDA(cudaMemcpyAsync(img_, input + z0 * N, N * b * sizeof(uint16_t), cudaMemcpyHostToDevice, stream_))) { return -1; }
-			dImg = static_cast<const uint16_t*>(img_);
-		}
-		double* dOut = outputOnDevice ? output + rows * kCols : ws_.sortedRows;
-		const long long n = RunChunk(dImg, H, W, b, thr, ratio, maxPoints, fp, dOut, rows, z0, &truncated);
-		if (n < 0) { return -1; }
+	// waits for chunk k and, for host output, copies its rows out
+	auto complete = [&](uint64_t k) {
+		const int slot = static_cast<int>(k & 1);
+		const long long n = CompleteChunk(slot, &truncated);
+		if (n < 0) { return false; }
 		if (!outputOnDevice && n > 0) {
-			if (!PTB_CUDA(cudaMemcpyAsync(output + rows * kCols, ws_.sortedRows, static_cast<size_t>(n) * kCols * sizeof(double),
-			                              cudaMemcpyDeviceToHost, stream_))) { return -1; }
-			if (!PTB_CUDA(cudaStreamSynchronize(stream_))) { return -1; }
+			if (!PTB_CUDA(cudaMemcpyAsync(output + rows * kCols, outSlot[slot], static_cast<size_t>(n) * kCols * sizeof(double),
+			                              cudaMemcpyDeviceToHost, copy_))) {
+				return false;
+			}
 		}
+		if (!PTB_CUDA(cudaEventRecord(d2h_[slot], copy_))) { return false; }
 		rows += static_cast<unsigned long long>(n);
+		return true;
+	};
+	bool ok = inputOnDevice || copyIn(0);
+	for (uint64_t k = 0; ok && k < chunks; ++k) {
+		const int slot = static_cast<int>(k & 1);
+		const int b = framesOf(k);
+		PlanWorkspace(ws_, H, W, b, rowsCap, static_cast<char*>(pool_));
+		const uint16_t* dImg = inputOnDevice ? input + k * B * N : imgSlot(slot);
+		if (!inputOnDevice) { ok = PTB_CUDA(cudaStreamWaitEvent(stream_, h2d_[slot], 0)); }
+		// the output slot of chunk k - 2 must be copied out before this chunk orders its rows into it
+		if (ok && !outputOnDevice && k >= 2) { ok = PTB_CUDA(cudaStreamWaitEvent(stream_, d2h_[slot], 0)); }
+		double* dOut = outputOnDevice ? output : outSlot[slot];
+		ok = ok && EnqueueChunk(slot, dImg, H, W, b, thr, ratio, maxPoints, fp, dOut, outputOnDevice, k * B);
+		if (ok && !inputOnDevice && k + 1 < chunks) { ok = copyIn(k + 1); }
+		if (ok && profiling_) { ok = complete(k); }  // stage timing needs each chunk finished before the next starts
+		else if (ok && k >= 1) { ok = complete(k - 1); }
+	}
+	if (ok && !profiling_ && chunks > 0) { ok = complete(chunks - 1); }
+	ok = ok && PTB_CUDA(cudaStreamSynchronize(copy_));
+	if (!ok) {
+		cudaStreamSynchronize(stream_);
+		cudaStreamSynchronize(copy_);
+		return -1;
 	}
 	for (uint32_t i = 0; i < truncated; ++i) {
 		std::cerr << "[WARNING] Density is too high; some points are missed (output capacity exceeded).\n";

@@ -56,13 +56,22 @@ private:
 	int TunedLanes(const FitParams& fp) const;
 	bool Autotune(FitParams& fp, const uint16_t* dImg, int H, int W);
 	int ChunkFrames(int H, int W, uint64_t planes, uint32_t maxPoints) const;
-	long long RunChunk(const uint16_t* dImg, int H, int W, int B, double thr, double ratio, uint32_t maxPoints,
-	                   const FitParams& fp, double* dOut, unsigned long long idBase, unsigned long long planeBase,
-	                   uint32_t* truncatedFrames);
+	// One chunk of B frames on the compute stream: detection, segmentation, fits, ordering into dOut (at dOut +
+	// rows so far when offsetOut), counters copied to the slot's pinned buffer, completion event recorded.
+	bool EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, double thr, double ratio, uint32_t maxPoints,
+	                  const FitParams& fp, double* dOut, bool offsetOut, unsigned long long planeBase);
+	// Waits for the slot's chunk; returns its row count or -1 (error recorded).
+	long long CompleteChunk(int slot, uint32_t* truncatedFrames);
+	bool ReserveRows2(size_t bytes);
 
 	int device_ = 0;
 	cudaStream_t stream_ = nullptr;
-	Counters* hostCnt_ = nullptr;
+	cudaStream_t copy_ = nullptr;            // host<->device copies that overlap the compute stream
+	cudaEvent_t h2d_[2] = {}, done_[2] = {}, d2h_[2] = {};  // per staging slot
+	Counters* hostCnt_ = nullptr;             // pinned, one per staging slot
+	unsigned long long* rowBase_ = nullptr;   // device: rows written by the earlier chunks of the current call
+	void* rows2_ = nullptr;                   // second output staging buffer (host output)
+	size_t rows2Bytes_ = 0;
 	size_t budget_ = 0;
 	void* pool_ = nullptr;
 	size_t poolBytes_ = 0;
@@ -85,6 +94,10 @@ private:
 	uint64_t stageLaunches_[kStages] = {};
 	unsigned long long* evalDev_ = nullptr;      // device counters of model evaluations (profiling)
 	unsigned long long evalTotals_[3] = {};      // FP32 LM, FP32 polish, FP64
+	// profiling bookkeeping of the chunk in flight
+	uint64_t pendLaunches_[kStages] = {};
+	bool pendMleProf_ = false;
+	int pendLanes_ = 0;
 };
 
 Engine& EngineFor(std::unique_lock<std::mutex>& lock);

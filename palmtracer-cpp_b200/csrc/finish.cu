@@ -75,9 +75,10 @@ __device__ void WriteRow(const double* src, double* dst, double id, double plane
 	dst[cIndex] = index;
 }
 
-// One CTA per frame: sort that frame's rows by (Y, X) and write them numbered to out (device memory).
-__global__ void __launch_bounds__(kSortThreads) SortFrames(Workspace ws, double* out, unsigned long long idBase,
-                                                            unsigned long long planeBase, uint32_t capScratch)
+// One CTA per frame: sort that frame's rows by (Y, X) and write them numbered to out (device memory). Ids continue
+// from *rowBase (rows written by earlier chunks); with offsetOut the rows also land at out + *rowBase rows.
+__global__ void __launch_bounds__(kSortThreads) SortFrames(Workspace ws, double* out, const unsigned long long* rowBase,
+                                                            int offsetOut, unsigned long long planeBase, uint32_t capScratch)
 {
 	__shared__ unsigned long long sy[kSmemSort];
 	__shared__ unsigned long long sx[kSmemSort];
@@ -112,10 +113,18 @@ __global__ void __launch_bounds__(kSortThreads) SortFrames(Workspace ws, double*
 	__syncthreads();
 	if (smem) { Bitonic<true>(ky, kx, id, len); }
 	else { Bitonic<false>(ky, kx, id, len); }
+	const unsigned long long idBase = *rowBase;
+	double* dst = out + (offsetOut ? static_cast<long long>(idBase) * kCols : 0ll);
 	for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-		WriteRow(rows + static_cast<long long>(id[i]) * kCols, out + (static_cast<long long>(base) + i) * kCols,
+		WriteRow(rows + static_cast<long long>(id[i]) * kCols, dst + (static_cast<long long>(base) + i) * kCols,
 		         static_cast<double>(idBase + base + i + 1), static_cast<double>(planeBase + f + 1), static_cast<double>(i + 1));
 	}
+}
+
+// After SortFrames: the chunk's rows join the running count.
+__global__ void AdvanceRowBase(Workspace ws, unsigned long long* rowBase)
+{
+	*rowBase += ws.frameOutBase[ws.g.B];
 }
 
 }  // namespace
@@ -127,11 +136,14 @@ bool LaunchBuildCandidates(const Workspace& ws, cudaStream_t st)
 	return PTB_LAUNCHED();
 }
 
-// out: device destination of the chunk's first row (rows already offset by the caller).
-bool LaunchSortFrames(const Workspace& ws, double* out, unsigned long long idBase, unsigned long long planeBase, cudaStream_t st)
+// out: device destination of the rows. rowBase: device count of the rows written by earlier chunks (Ids continue from it; it is advanced by this chunk's
+// rows); offsetOut: write at out + rowBase rows instead of out.
+bool LaunchSortFrames(const Workspace& ws, double* out, unsigned long long* rowBase, bool offsetOut, unsigned long long planeBase,
+                      cudaStream_t st)
 {
-	SortFrames<<<ws.g.B, kSortThreads, 0, st>>>(ws, out, idBase, planeBase, ws.capRows);
-	CountLaunch();
+	SortFrames<<<ws.g.B, kSortThreads, 0, st>>>(ws, out, rowBase, offsetOut ? 1 : 0, planeBase, ws.capRows);
+	AdvanceRowBase<<<1, 1, 0, st>>>(ws, rowBase);
+	CountLaunch(2);
 	return PTB_LAUNCHED();
 }
 
