@@ -45,6 +45,11 @@ REF_FIT_MODE = 2  # the reference's own 5-parameter Gaussian fit, for the CPU ar
 # (an FMA counts 2; a division, logarithm or reciprocal 1). Per-evaluation erf tables and the 5x5 solve are not
 # counted.
 FLOP_PER_PIXEL_LM = 71
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per frame of one launch, from ncu captures of smaller
+# chunks of the same workload, scaled by the frames a benchmark launch processes (traffic grows with the frames):
+# MleLmKernel<6> 104.1 MB over a 50-frame chunk, DetectKernel 90.6 MB over a 22-frame chunk.
+LM_DRAM_BYTES_PER_FRAME = 104.13e6 / 50
+DETECT_DRAM_BYTES_PER_FRAME = 90.60e6 / 22
 RATIO = 0.0
 PER_PLANE = 8192
 
@@ -256,8 +261,10 @@ def main():
     det_ms, det_l = stages["detect"]
     det_bytes = 2.0 * h * w * frames
     det_achieved = det_bytes / (det_ms / 1000.0) / 1e9 if det_ms > 0 else None
+    frames_per_launch = frames / max(det_l, 1)
     detect_roofline = {"kernel": "DetectKernel (wavelet + threshold + seeds)", "bound": "hbm", "achieved": det_achieved,
                        "peak": peak, "unit": "GB/s", "frac": (det_achieved / peak) if det_achieved else None,
+                       "traffic": DETECT_DRAM_BYTES_PER_FRAME * frames_per_launch, "traffic_unit": "bytes per launch (ncu, scaled)",
                        "algorithmic_bytes_per_launch": det_bytes / max(det_l, 1), "launches": det_l,
                        "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind}
     roofline = detect_roofline
@@ -267,7 +274,9 @@ def main():
         flops = FLOP_PER_PIXEL_LM * 49 * evals["lm"]
         achieved = flops / (lm_ms / 1000.0) / 1e12
         roofline = {"kernel": "MleLmKernel<6> (persistent FP32 LM, thread per ROI)", "bound": "fp32", "achieved": achieved,
-                    "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                    "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                    "traffic": LM_DRAM_BYTES_PER_FRAME * frames / max(1, stages["fit_lm"][1]),
+                    "traffic_unit": "bytes per launch (ncu, scaled)",
                     "algorithmic_flops_per_launch": flops / max(1, stages["fit_lm"][1]), "launches": stages["fit_lm"][1],
                     "flop_per_pixel_evaluation": FLOP_PER_PIXEL_LM, "evaluations": evals,
                     "peak_source": "measured in this run (PTB_MeasureFmaPeak FP32 FMA chains)"}
