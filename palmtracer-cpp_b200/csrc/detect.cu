@@ -140,14 +140,15 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 
 	// A: C1, one lane per column
 	for (int i = tid; i < kP1; i += kThreads) {
+		// frame offsets fit in 32 bits (H * W < 2^31)
 		const uint16_t* col = frame + clampi(x0 - 7 + i, 0, W - 1);
-		uint32_t w0 = __ldg(col + static_cast<long long>(clampi(y0 - 7, 0, H - 1)) * W);
-		uint32_t w1 = __ldg(col + static_cast<long long>(clampi(y0 - 6, 0, H - 1)) * W);
-		uint32_t w2 = __ldg(col + static_cast<long long>(clampi(y0 - 5, 0, H - 1)) * W);
-		uint32_t w3 = __ldg(col + static_cast<long long>(clampi(y0 - 4, 0, H - 1)) * W);
+		uint32_t w0 = __ldg(col + clampi(y0 - 7, 0, H - 1) * W);
+		uint32_t w1 = __ldg(col + clampi(y0 - 6, 0, H - 1) * W);
+		uint32_t w2 = __ldg(col + clampi(y0 - 5, 0, H - 1) * W);
+		uint32_t w3 = __ldg(col + clampi(y0 - 4, 0, H - 1) * W);
 		#pragma unroll 6
 		for (int r = 0; r < kRows1; ++r) {
-			const uint32_t w4 = __ldg(col + static_cast<long long>(clampi(y0 - 3 + r, 0, H - 1)) * W);
+			const uint32_t w4 = __ldg(col + clampi(y0 - 3 + r, 0, H - 1) * W);
 			c1[r * kP1 + i] = Tap(w0, w1, w2, w3, w4);
 			w0 = w1; w1 = w2; w2 = w3; w3 = w4;
 		}

@@ -36,7 +36,8 @@ __device__ __forceinline__ unsigned long long WeakKey(double d)
 }
 
 constexpr int kSortThreads = 512;
-constexpr int kSmemSort = 2048;  // rows sorted in shared memory; larger frames sort in global scratch
+constexpr int kSmemSort = 4096;  // rows sorted in shared memory (80 KB); larger frames sort in global scratch
+constexpr size_t kSortSmemBytes = kSmemSort * (2 * sizeof(unsigned long long) + sizeof(uint32_t));
 
 __device__ __forceinline__ bool KeyLess(unsigned long long ya, unsigned long long xa, unsigned long long yb, unsigned long long xb)
 {
@@ -80,9 +81,10 @@ __device__ void WriteRow(const double* src, double* dst, double id, double plane
 __global__ void __launch_bounds__(kSortThreads) SortFrames(Workspace ws, double* out, const unsigned long long* rowBase,
                                                             int offsetOut, unsigned long long planeBase, uint32_t capScratch)
 {
-	__shared__ unsigned long long sy[kSmemSort];
-	__shared__ unsigned long long sx[kSmemSort];
-	__shared__ uint32_t si[kSmemSort];
+	extern __shared__ __align__(16) unsigned long long sortSmem[];
+	unsigned long long* sy = sortSmem;
+	unsigned long long* sx = sy + kSmemSort;
+	uint32_t* si = reinterpret_cast<uint32_t*>(sx + kSmemSort);
 	const int f = blockIdx.x;
 	const uint32_t base = ws.frameOutBase[f];
 	const uint32_t n = ws.frameOutBase[f + 1] - base;
@@ -136,12 +138,15 @@ bool LaunchBuildCandidates(const Workspace& ws, cudaStream_t st)
 	return PTB_LAUNCHED();
 }
 
-// out: device destination of the rows. rowBase: device count of the rows written by earlier chunks (Ids continue from it; it is advanced by this chunk's
-// rows); offsetOut: write at out + rowBase rows instead of out.
+// out: device destination of the rows. rowBase: device count of the rows written by earlier chunks (Ids continue
+// from it; it is advanced by this chunk's rows); offsetOut: write at out + rowBase rows instead of out.
 bool LaunchSortFrames(const Workspace& ws, double* out, unsigned long long* rowBase, bool offsetOut, unsigned long long planeBase,
                       cudaStream_t st)
 {
-	SortFrames<<<ws.g.B, kSortThreads, 0, st>>>(ws, out, rowBase, offsetOut ? 1 : 0, planeBase, ws.capRows);
+	static const bool configured = PTB_CUDA(cudaFuncSetAttribute(SortFrames, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                                             static_cast<int>(kSortSmemBytes)));
+	if (!configured) { return false; }
+	SortFrames<<<ws.g.B, kSortThreads, kSortSmemBytes, st>>>(ws, out, rowBase, offsetOut ? 1 : 0, planeBase, ws.capRows);
 	AdvanceRowBase<<<1, 1, 0, st>>>(ws, rowBase);
 	CountLaunch(2);
 	return PTB_LAUNCHED();

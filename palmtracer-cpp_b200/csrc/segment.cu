@@ -167,18 +167,36 @@ __global__ void CclFlatten(Workspace ws)
 	for (uint32_t k##Base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u, k = k##Base + (threadIdx.x & 31u); \
 	     k##Base < (n); k##Base += gridDim.x * blockDim.x, k = k##Base + (threadIdx.x & 31u))
 
-__global__ void CompEnumerate(Workspace ws)
+// Component ids: one atomic per block and grid-stride step (roots are few, but a single counter hit by every warp
+// serialises at the L2).
+__global__ void __launch_bounds__(kThreads) CompEnumerate(Workspace ws)
 {
+	__shared__ uint32_t warpBase[kThreads / 32 + 1];
 	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
-	PTB_WARP_LOOP(k, n)
-	{
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+		const uint32_t k = base + threadIdx.x;
 		uint32_t p = 0;
 		bool root = false;
 		if (k < n) {
 			p = ws.dom[k];
 			root = ws.par[p] == p;
 		}
-		const uint32_t c = WarpAppendIndex(root, &ws.cnt->ncomp);
+		const unsigned mask = __ballot_sync(0xffffffffu, root);
+		if (lane == 0) { warpBase[warp] = __popc(mask); }
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			uint32_t total = 0;
+			for (int w = 0; w < kThreads / 32; ++w) {
+				const uint32_t c = warpBase[w];
+				warpBase[w] = total;
+				total += c;
+			}
+			warpBase[kThreads / 32] = total ? atomicAdd(&ws.cnt->ncomp, total) : 0u;
+		}
+		__syncthreads();
+		const uint32_t c = warpBase[kThreads / 32] + warpBase[warp] + __popc(mask & ((1u << lane) - 1u));
+		__syncthreads();  // warpBase is rewritten by the next step
 		if (!root) { continue; }
 		if (c >= ws.capComp) { atomicExch(&ws.cnt->overflow, 1u); continue; }
 		ws.compRoot[c] = p;
