@@ -52,6 +52,14 @@ LM_DRAM_BYTES_PER_FRAME = 104.13e6 / 50
 DETECT_DRAM_BYTES_PER_FRAME = 90.60e6 / 22
 RATIO = 0.0
 PER_PLANE = 8192
+# Serving mix (C5): Poisson arrivals at 20 stacks/s of square frames from {128, 256, 512, 1024, 2048}, lengths 1-500,
+# half 2D Gaussian (C1 statistics, MLE mode 6, 7x7) and half astigmatic 3D (C3 statistics, MLE mode 7, 11x11).
+SERVE_SIZES = [128, 256, 512, 1024, 2048]
+SERVE_RATE = 20.0
+SERVE_SLOTS = 4
+SERVE_PER_PLANE = 2048
+ASTIG = [150.0, 400.0, 0.05, 0.0, 1.3 * 160, -150.0, 400.0, -0.05, 0.0, 1.3 * 160]
+MLE7_PARAMS = np.array([11.0, 160.0] + ASTIG + [100.0, 2.0, 20.0, -600.0, 600.0, 0.0])
 
 
 def peaks():
@@ -139,6 +147,90 @@ def cpu_reference_rate(frames_host, thr, seconds=10.0, threads=None):
                                  "frames": n1, "seconds": dt0, "rows": int(rows.shape[0])}
 
 
+def serving_run(ptb, torch, n_req, seed=2026):
+    """C5 serving mix through PTB_ServerStart / PTB_SubmitStack / PTB_StackResult: a Poisson-arrival run at
+    SERVE_RATE, a saturated run (every request submitted at once) and the plain one-call-per-frame form on a
+    bounded sample of the same frames. Latencies are measured by the library from submission to completion."""
+    import synth
+    rng = np.random.default_rng(seed)
+    sizes = rng.choice(SERVE_SIZES, n_req)
+    kinds = rng.integers(0, 2, n_req)
+    lengths = rng.integers(1, 501, n_req)
+    arrivals = np.cumsum(rng.exponential(1.0 / SERVE_RATE, n_req))
+    base = {}
+    for size, kind in sorted(set(zip(sizes.tolist(), kinds.tolist()))):
+        frames = int(lengths[(sizes == size) & (kinds == kind)].max())
+        d, _ = synth.stack_cuda("c1" if kind == 0 else "c3", frames=frames, seed=seed + 7 * size + kind, size=(size, size))
+        host = torch.empty(d.shape, dtype=torch.int16, pin_memory=True)
+        host.copy_(d)
+        del d
+        arr = host.numpy().view(np.uint16)
+        base[(size, kind)] = (host, arr, mad_threshold_gpu(ptb, arr[0]))
+    torch.cuda.empty_cache()
+    fit_of = {0: (6, PARAMS_BY_MODE[6]), 1: (7, MLE7_PARAMS)}
+    server = ptb.Server(slots=SERVE_SLOTS)
+
+    def submit(i):
+        _, arr, thr = base[(int(sizes[i]), int(kinds[i]))]
+        fit, params = fit_of[int(kinds[i])]
+        return server.submit(arr[:int(lengths[i])], thr, RATIO, fit, params, capacity_doubles=SERVE_PER_PLANE * int(lengths[i]) * 18)
+
+    def collect(tickets):
+        rows, lat = 0, []
+        for t in tickets:
+            r, _, latency = server.result(t)
+            rows += r.shape[0]
+            lat.append(latency * 1000.0)
+        return rows, np.array(lat)
+
+    try:
+        for kind in (0, 1):  # warm-up: one small stack per model
+            i = int(np.argmin(np.where(kinds == kind, sizes * lengths, 1 << 40)))
+            collect([submit(i)])
+        t0 = time.perf_counter()
+        tickets = []
+        for i in range(n_req):
+            wait = t0 + arrivals[i] - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            tickets.append(submit(i))
+        rows, lat = collect(tickets)
+        poisson_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        rows_sat, lat_sat = collect([submit(i) for i in range(n_req)])
+        sat_s = time.perf_counter() - t0
+    finally:
+        server.stop()
+    # plain form: one Localization call per frame, on the first frames of the same requests (bounded sample)
+    plain_rows, plain_frames, plain_lat, t_start = 0, 0, [], time.perf_counter()
+    for i in range(n_req):
+        _, arr, thr = base[(int(sizes[i]), int(kinds[i]))]
+        fit, params = fit_of[int(kinds[i])]
+        for z in range(min(int(lengths[i]), 8)):
+            t1 = time.perf_counter()
+            r = ptb.localization(arr[z:z + 1], thr, RATIO, fit, params, capacity_doubles=SERVE_PER_PLANE * 18)
+            plain_lat.append((time.perf_counter() - t1) * 1000.0)
+            plain_rows += r.shape[0]
+            plain_frames += 1
+        if time.perf_counter() - t_start > 8.0:
+            break
+    plain_s = time.perf_counter() - t_start
+    frames_total = int(lengths.sum())
+    return {
+        "workload": "C5: %d stacks, Poisson arrivals at %.0f stacks/s, square frames of %s px, 1-500 frames (%d in all), "
+                    "half 2D Gaussian (MLE mode 6, 7x7), half astigmatic 3D (MLE mode 7, 11x11); %d server slots"
+                    % (n_req, SERVE_RATE, "/".join(str(s) for s in SERVE_SIZES), frames_total, SERVE_SLOTS),
+        "poisson": {"localizations_per_s": rows / poisson_s, "frames_per_s": frames_total / poisson_s, "seconds": poisson_s,
+                    "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))}},
+        "saturated": {"localizations_per_s": rows_sat / sat_s, "frames_per_s": frames_total / sat_s, "seconds": sat_s,
+                      "latency_ms": {"p50": float(np.percentile(lat_sat, 50)), "p99": float(np.percentile(lat_sat, 99))}},
+        "plain_per_frame": {"localizations_per_s": plain_rows / plain_s, "frames_per_s": plain_frames / plain_s,
+                            "sample_frames": plain_frames,
+                            "call_latency_ms": {"p50": float(np.percentile(plain_lat, 50)), "p99": float(np.percentile(plain_lat, 99))}},
+        "localizations": int(rows),
+    }
+
+
 def main():
     global FIT_MODE, FIT_PARAMS
     ap = argparse.ArgumentParser()
@@ -151,6 +243,8 @@ def main():
     ap.add_argument("--precision", type=int, default=0, help="fit arithmetic (PTB_SetFitPrecision)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--fit", type=int, default=None, help="fit mode (default: %d)" % FIT_MODE)
+    ap.add_argument("--no-serving", action="store_true", help="skip the C5 serving mix")
+    ap.add_argument("--serve-requests", type=int, default=40)
     args = ap.parse_args()
     import torch
     import torch.distributed as dist
@@ -287,6 +381,7 @@ def main():
     host_in = torch.empty((frames, h, w), dtype=torch.int16, pin_memory=True)
     host_in.copy_(d_in)
     host_np = host_in.numpy().view(np.uint16)
+    h2d_bytes = int(host_np.nbytes)
     host_out = torch.empty(cap, dtype=torch.float64, pin_memory=True).numpy()
     e2e_ms = []
     n_e2e = 0
@@ -299,11 +394,18 @@ def main():
             e2e_ms.append((time.perf_counter() - t0) * 1000.0)
     e2e_value = (n_e2e // 18) * len(e2e_ms) / (sum(e2e_ms) / 1000.0) if e2e_ms else None
 
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        del host_in, host_np, host_out
+        serving = serving_run(ptb, torch, args.serve_requests)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sample = host_np[: min(frames, 512)]
+        sample = d_in[: min(frames, 512)].cpu().numpy().view(np.uint16)
         v, info = cpu_reference_rate(sample, thr, seconds=10.0)
-        cpu = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"], "sample": info["sample"]}
+        v1, info1 = cpu_reference_rate(sample, thr, seconds=5.0, threads=1)
+        cpu = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"], "sample": info["sample"],
+               "single_thread": {"value": v1, "cores": 1, "sample": info1["sample"]}}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -316,9 +418,9 @@ def main():
                 "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
                 "localizations_per_step": int(rows_all), "roofline": roofline, "detect_roofline": detect_roofline,
                 "cpu_baseline": cpu,
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(host_np.nbytes),
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_bytes,
                         "d2h_bytes_per_step": int(n_e2e * 8), "ms_per_step": float(np.mean(e2e_ms)) if e2e_ms else None},
-                "gpu_launches": int(launches), "clocks": clk}
+                "gpu_launches": int(launches), "clocks": clk, "serving": serving}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

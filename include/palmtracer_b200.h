@@ -66,6 +66,24 @@ PTB_API uint64_t PTB_LocalizationDevice(const uint16_t* d_input, double* d_outpu
                                         uint64_t height, uint64_t width, uint64_t planes, double thresholdVal,
                                         double watershedRatio, uint64_t fit, const double* fit_params, void* stream);
 
+/* Serving (additive surface; no counterpart in the reference). PTB_ServerStart starts `slots` worker slots on the
+ * current device, each with its own CUDA stream and chunk workspace and an equal share of `budgetBytes` of device
+ * memory (0 = half of the free memory); returns 1, or 0 on error. PTB_SubmitStack queues one Localization (same
+ * arguments and output layout) and returns a ticket (0 on error); the input and output buffers stay owned by the
+ * caller and must stay valid until the request completes (fit_params is copied). A queued stack starts when a slot is
+ * free and its estimated device memory fits in what the running stacks leave of the budget (first fit in submission
+ * order); stacks on different slots run concurrently on the device. Each result equals what Localization returns for
+ * the same stack. PTB_PollStack: 0 queued or running, 1 done, -1 failed or unknown ticket. PTB_StackResult waits for
+ * the request, releases the ticket and returns the doubles written (-1 on failure, message in PTB_LastError);
+ * `times` (NULL or 2 doubles) receives the queueing delay and the latency from submission to completion in seconds.
+ * PTB_ServerStop finishes the running stacks and fails the queued ones; call it with no other server call in flight. */
+PTB_API int PTB_ServerStart(int slots, uint64_t budgetBytes);
+PTB_API uint64_t PTB_SubmitStack(const uint16_t* input, double* output, uint64_t outputSize, uint64_t height, uint64_t width,
+                                 uint64_t planes, double thresholdVal, double watershedRatio, uint64_t fit, const double* fit_params);
+PTB_API int PTB_PollStack(uint64_t ticket);
+PTB_API int64_t PTB_StackResult(uint64_t ticket, double* times);
+PTB_API void PTB_ServerStop(void);
+
 /* Fit-only at caller-given positions with no device memory allocation: for callers that cannot call cudaMalloc
  * (code running inside another runtime's stream callbacks or under a fixed pre-sized memory pool) but can pass device
  * buffers. No counterpart in the reference; same result as Fitting for the same inputs. d_input is the device stack

@@ -179,6 +179,72 @@ PTB_API void PTB_StageTimes(double* ms, uint64_t* launches, int n)
 	ptb::EngineFor(lock).StageTimes(ms, launches, n);
 }
 
+PTB_API int PTB_ServerStart(int slots, uint64_t budgetBytes)
+{
+	ptb::ClearError();
+	try {
+		if (ptb::ServerStart(slots, budgetBytes)) { return 1; }
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+	}
+	Report("PTB_ServerStart");
+	return 0;
+}
+
+PTB_API void PTB_ServerStop(void)
+{
+	try {
+		ptb::ServerStop();
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("PTB_ServerStop");
+	}
+}
+
+PTB_API uint64_t PTB_SubmitStack(const uint16_t* input, double* output, uint64_t outputSize, uint64_t height, uint64_t width,
+                                 uint64_t planes, double thresholdVal, double watershedRatio, uint64_t fit, const double* fit_params)
+{
+	ptb::ClearError();
+	try {
+		const uint64_t id = ptb::SubmitStack(input, output, outputSize, height, width, planes, thresholdVal, watershedRatio, fit,
+		                                     fit_params, ptb::FitParamCount(fit, fit_params));
+		if (id == 0) { Report("PTB_SubmitStack"); }
+		return id;
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("PTB_SubmitStack");
+		return 0;
+	}
+}
+
+PTB_API int PTB_PollStack(uint64_t ticket)
+{
+	try {
+		return ptb::PollStack(ticket);
+	}
+	catch (const std::exception&) {
+		return -1;
+	}
+}
+
+PTB_API int64_t PTB_StackResult(uint64_t ticket, double* times)
+{
+	ptb::ClearError();
+	try {
+		const long long n = ptb::StackResult(ticket, times);
+		if (n < 0) { Report("PTB_StackResult"); }
+		return n;
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("PTB_StackResult");
+		return -1;
+	}
+}
+
 PTB_API void PTB_MleEvaluations(uint64_t* counts, int n)
 {
 	std::unique_lock<std::mutex> lock;

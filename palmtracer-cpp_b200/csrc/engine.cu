@@ -135,6 +135,22 @@ bool ParseFitParams(uint64_t fit, const double* fp, FitParams& out, std::vector<
 	return true;
 }
 
+size_t FitParamCount(uint64_t fit, const double* fp)
+{
+	if (fp == nullptr) { return 0; }
+	auto cells = [](double a, double b, double c) {
+		return static_cast<size_t>(std::max(0.0, a)) * static_cast<size_t>(std::max(0.0, b)) * static_cast<size_t>(std::max(0.0, c));
+	};
+	switch (fit) {
+		case kG2Fixed: case kG2Sigma: case kG3Fixed: case kG3Theta: return 4;
+		case kSplineEmccd: return 5 + 64 * cells(fp[1], fp[2], fp[3]);
+		case kMleGauss: return 6;
+		case kMleAstig: return 18;
+		case kMleSpline: return 9 + 64 * cells(fp[1], fp[2], fp[3]);
+		default: return 0;
+	}
+}
+
 // ---- workspace ------------------------------------------------------------------------------------------------
 namespace {
 
@@ -270,6 +286,7 @@ bool Engine::Init()
 	// default budget: a quarter of free memory, at most 24 GiB (leaves room for callers' own buffers)
 	budget_ = std::min<size_t>(freeB / 4, 24ull << 30);
 	if (const char* env = std::getenv("PTB_WORKSPACE_MB")) { budget_ = static_cast<size_t>(std::atoll(env)) << 20; }
+	if (fixedBudget_) { budget_ = fixedBudget_; }
 	return true;
 }
 
@@ -293,6 +310,20 @@ bool Engine::ReserveImage(size_t bytes)
 	if (!PTB_CUDA(cudaMalloc(&img_, bytes))) { return false; }
 	imgBytes_ = bytes;
 	return true;
+}
+
+size_t Engine::EstimateBytes(uint64_t height, uint64_t width, uint64_t planes, uint64_t outputSize) const
+{
+	if (planes == 0 || height == 0 || width == 0) { return 0; }
+	const int H = static_cast<int>(height), W = static_cast<int>(width);
+	const uint32_t maxPoints = static_cast<uint32_t>(std::min<uint64_t>((outputSize / kCols) / planes, 0xffffffffu));
+	const int B = ChunkFrames(H, W, planes, maxPoints);
+	const uint32_t rowsCap = static_cast<uint32_t>(std::min<uint64_t>(static_cast<uint64_t>(B) * maxPoints, 0xffffffffu));
+	Workspace probe{};
+	const size_t ws = PlanWorkspace(probe, H, W, B, rowsCap, nullptr);
+	const size_t img = 2ull * static_cast<size_t>(H) * W * B * sizeof(uint16_t);
+	const size_t rows2 = static_cast<size_t>(probe.capRows) * kCols * sizeof(double);
+	return ws + img + rows2;
 }
 
 int Engine::ChunkFrames(int H, int W, uint64_t planes, uint32_t maxPoints) const

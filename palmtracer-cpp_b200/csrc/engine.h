@@ -20,6 +20,15 @@ long long FittingDeviceNoAlloc(const uint16_t* dStack, const double* dPositions,
                                uint64_t height, uint64_t width, uint64_t planes, uint64_t fit, const double* fitParams,
                                int precision, int lanes, cudaStream_t st);
 int EnvLanes();
+// Serving (server.cpp)
+bool ServerStart(int slots, uint64_t budgetBytes);
+void ServerStop();
+uint64_t SubmitStack(const uint16_t* input, double* output, uint64_t outputSize, uint64_t height, uint64_t width, uint64_t planes,
+                     double thr, double ratio, uint64_t fit, const double* fitParams, size_t nParams);
+int PollStack(uint64_t id);
+long long StackResult(uint64_t id, double* times);
+// Number of fit_params entries the given fit mode reads (0 for mode 0 or an unknown mode).
+size_t FitParamCount(uint64_t fit, const double* fp);
 uint64_t LaunchCount();
 double MeasureFmaPeak(int fp64);
 
@@ -46,6 +55,12 @@ public:
 	int SetPrecision(int p) { const int o = precision_; precision_ = p; return o; }
 	int Precision() const { return precision_; }
 	cudaStream_t Stream() const { return stream_; }
+	// Device-memory budget of the chunk workspace (bytes); 0 = a quarter of free memory at first use, at most 24 GiB
+	// (or PTB_WORKSPACE_MB). Takes effect at the engine's first call.
+	void SetBudget(size_t bytes) { fixedBudget_ = bytes; }
+	size_t Budget() const { return budget_; }
+	// Device bytes a Localize call of this shape would hold (chunk workspace and staging), for admission control.
+	size_t EstimateBytes(uint64_t height, uint64_t width, uint64_t planes, uint64_t outputSize) const;
 	void SetStream(cudaStream_t s) { stream_ = s; }
 	bool Init();
 
@@ -73,6 +88,7 @@ private:
 	void* rows2_ = nullptr;                   // second output staging buffer (host output)
 	size_t rows2Bytes_ = 0;
 	size_t budget_ = 0;
+	size_t fixedBudget_ = 0;
 	void* pool_ = nullptr;
 	size_t poolBytes_ = 0;
 	void* img_ = nullptr;

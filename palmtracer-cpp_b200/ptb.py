@@ -15,7 +15,8 @@ COLS = 18
 # every symbol the public header declares
 EXPORTS = ["Localization", "Fitting", "Wavelett", "AutoThreshold", "PTB_LocalizationDevice",
            "PTB_SetSegmentationMode", "PTB_SetFitPrecision", "PTB_LastError", "PTB_KernelLaunchCount",
-           "PTB_SetProfiling", "PTB_StageTimes", "PTB_MleEvaluations", "PTB_MeasureFmaPeak", "PTB_FittingDeviceNoAlloc"]
+           "PTB_SetProfiling", "PTB_StageTimes", "PTB_MleEvaluations", "PTB_MeasureFmaPeak", "PTB_FittingDeviceNoAlloc",
+           "PTB_ServerStart", "PTB_SubmitStack", "PTB_PollStack", "PTB_StackResult", "PTB_ServerStop"]
 
 _u16p = ctypes.POINTER(ctypes.c_uint16)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -61,6 +62,16 @@ def load(path=LIB_PATH):
     L.PTB_FittingDeviceNoAlloc.restype = _u64
     L.PTB_FittingDeviceNoAlloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _u64, ctypes.c_void_p, _u64, _u64, _u64, _u64,
                                            _f64p, ctypes.c_void_p]
+    L.PTB_ServerStart.restype = ctypes.c_int
+    L.PTB_ServerStart.argtypes = [ctypes.c_int, _u64]
+    L.PTB_SubmitStack.restype = _u64
+    L.PTB_SubmitStack.argtypes = [_u16p, _f64p, _u64, _u64, _u64, _u64, _f64, _f64, _u64, _f64p]
+    L.PTB_PollStack.restype = ctypes.c_int
+    L.PTB_PollStack.argtypes = [_u64]
+    L.PTB_StackResult.restype = ctypes.c_int64
+    L.PTB_StackResult.argtypes = [_u64, _f64p]
+    L.PTB_ServerStop.restype = None
+    L.PTB_ServerStop.argtypes = []
     L.PTB_MeasureFmaPeak.restype = _f64
     L.PTB_MeasureFmaPeak.argtypes = [ctypes.c_int]
     _lib = L
@@ -188,3 +199,43 @@ def fitting_device_noalloc(d_stack_ptr, d_positions_ptr, n_points, d_output_ptr,
     return load().PTB_FittingDeviceNoAlloc(ctypes.c_void_p(d_stack_ptr), ctypes.c_void_p(d_positions_ptr), n_points,
                                            ctypes.c_void_p(d_output_ptr), h, w, z, fit, params.ctypes.data_as(_f64p),
                                            ctypes.c_void_p(stream_ptr))
+
+
+class Server:
+    """Serving front end (PTB_ServerStart / PTB_SubmitStack / PTB_StackResult). submit() keeps references to the
+    stack and the output buffer until result() returns, because the library reads and writes them asynchronously."""
+
+    def __init__(self, slots=4, budget_bytes=0):
+        if not load().PTB_ServerStart(int(slots), int(budget_bytes)):
+            raise RuntimeError("PTB_ServerStart failed: " + last_error())
+        self._live = {}
+
+    def submit(self, stack, thr, ratio, fit, params, capacity_doubles=None):
+        stack = _stack(stack)
+        z, h, w = stack.shape
+        if capacity_doubles is None:
+            capacity_doubles = ((h * w) // 5 + 1) * z * COLS
+        out = np.empty(max(capacity_doubles, 1))
+        params = np.ascontiguousarray(params, dtype=np.float64)
+        t = load().PTB_SubmitStack(stack.ctypes.data_as(_u16p), out.ctypes.data_as(_f64p), capacity_doubles, h, w, z, thr, ratio,
+                                   fit, params.ctypes.data_as(_f64p))
+        if t == 0:
+            raise RuntimeError("PTB_SubmitStack failed: " + last_error())
+        self._live[t] = (stack, out)
+        return t
+
+    def poll(self, ticket):
+        return load().PTB_PollStack(ticket)
+
+    def result(self, ticket):
+        """(rows [n, 18], queueing delay s, latency s)."""
+        times = np.zeros(2)
+        n = load().PTB_StackResult(ticket, times.ctypes.data_as(_f64p))
+        held = self._live.pop(ticket, None)
+        if n < 0 or held is None:
+            raise RuntimeError("PTB_StackResult failed: " + last_error())
+        out = held[1]
+        return out[:n].reshape(-1, COLS).copy(), float(times[0]), float(times[1])
+
+    def stop(self):
+        load().PTB_ServerStop()
