@@ -56,6 +56,13 @@ PTB_API void Wavelett(const uint16_t* input, double* output, uint64_t height, ui
  * the raw pixels of frame 0 (at most 5 rounds of detection with fit 0 and watershed ratio 10). */
 PTB_API double AutoThreshold(const uint16_t* input, uint64_t height, uint64_t width, const double* fit_params);
 
+/* Replaces Astigmatism3DEstimation (CPU/main.cpp:324-353 -> lib/fit/AstigFit.cpp:36-72, 342-447): z of each point
+ * from its fitted widths. input [size][2] = (sigma_x, sigma_y) in pixels, output [size][2] = (z in nm, compatibility
+ * score in (0, 1]), model = [z0, w, c3, c4, A] of the x axis then of the y axis (nm), z searched in [-zMax, zMax]
+ * (201-point grid, then Brent). Equals the reference bit for bit. */
+PTB_API void Astigmatism3DEstimation(const double* input, double* output, uint64_t size, double pixelSize, const double* model,
+                                     double zMax);
+
 /* ---- Additions (no counterpart in the reference) ---------------------------------------------------------------- */
 
 /* Same contract as Localization, but d_input and d_output are DEVICE memory of the current CUDA device (fit_params

@@ -62,6 +62,17 @@ class CpuLib:
         self._threads.restype = None
         self._threads.argtypes = [ctypes.c_int]
 
+    def astig_estimation(self, sigmas, pixel_size, model, zmax):
+        """Astigmatism3DEstimation: [n, 2] (sigma_x, sigma_y) px -> [n, 2] (z nm, score)."""
+        f = getattr(self.lib, self.prefix + "Astig3DEstimation")
+        f.restype = None
+        f.argtypes = [_f64p, _f64p, _u64, _f64, _f64p, _f64]
+        sigmas = np.ascontiguousarray(sigmas, dtype=np.float64).reshape(-1, 2)
+        out = np.zeros_like(sigmas)
+        model = np.ascontiguousarray(model, dtype=np.float64)
+        f(_ptr(sigmas, _f64p), _ptr(out, _f64p), sigmas.shape[0], pixel_size, _ptr(model, _f64p), zmax)
+        return out
+
     def set_threads(self, n):
         self._threads(int(n))
 
@@ -173,16 +184,6 @@ class OracleLib(CpuLib):
 class RefLib(CpuLib):
     def __init__(self, path=REF_SO):
         super().__init__(path, "ref_")
-        self._astig = self.lib.ref_Astig3DEstimation
-        self._astig.restype = None
-        self._astig.argtypes = [_f64p, _f64p, _u64, _f64, _f64p, _f64]
-
-    def astig_estimation(self, sigmas, pixel_size, model, zmax):
-        sigmas = np.ascontiguousarray(sigmas, dtype=np.float64).reshape(-1, 2)
-        out = np.zeros_like(sigmas)
-        model = np.ascontiguousarray(model, dtype=np.float64)
-        self._astig(_ptr(sigmas, _f64p), _ptr(out, _f64p), sigmas.shape[0], pixel_size, _ptr(model, _f64p), zmax)
-        return out
 
 
 def oracle():

@@ -11,6 +11,7 @@
 // Entry points (extern "C", prefix orc_):
 //   orc_Localization / orc_Fitting / orc_Wavelett / orc_AutoThreshold  - the four C-ABI exports
 //   orc_Planes, orc_Candidates, orc_CandidatesFromPotential, orc_Labels - per-stage products
+//   orc_Astig3DEstimation - z from (sigma_x, sigma_y) with the astigmatism model (the reference's export of that name)
 #include <omp.h>
 
 #include <algorithm>
@@ -1614,6 +1615,101 @@ uint64_t orc_Labels(const uint16_t* frame, uint64_t height, uint64_t width, doub
 	if (static_cast<int>(ratio) > 0) { seg.Fuse(); seg.Flood(); }
 	std::copy(seg.lab.begin(), seg.lab.end(), labels);
 	return seg.cands.size();
+}
+
+// z from the fitted widths (AstigFit::Estimate, lib/fit/AstigFit.cpp:36-59, exported as Astigmatism3DEstimation,
+// CPU/main.cpp:324-353). Per point: the squared width error over a 201-point grid of [-zMax, zMax], Brent's
+// minimisation (golden section with parabolic steps, Brent 1973) on the best grid point +-2 grid steps (:342-447,
+// constants AstigFit.hpp:110-114), the grid point kept when Brent does not improve on it, and the compatibility
+// score 1 / (1 + (Rx^2 + Ry^2) / 2), R = relative width error / 0.2 (:99-109). Widths from the model
+// sigma_px = A / pixelSize * sqrt(max(0, 1 + U^2 + c3 U^3 + c4 U^4)), U = (z - z0) / w (:76-88).
+// input [size][2] = (sigma_x, sigma_y) px, output [size][2] = (z nm, score), model [z0, w, c3, c4, A] x then y.
+void orc_Astig3DEstimation(const double* input, double* output, uint64_t size, double pixelSize, const double* model, double zMax)
+{
+	struct Axis { double z0, w, c3, c4, a; };
+	const Axis ax[2] = {{model[0], model[1], model[2], model[3], model[4]}, {model[5], model[6], model[7], model[8], model[9]}};
+	const double scale = 1.0 / pixelSize;  // sampling (1) over the pixel size, then times the width in nm
+	auto width = [&](const Axis& m, double z) {
+		const double u = (z - m.z0) / m.w;
+		const double u2 = u * u, u3 = u2 * u, u4 = u3 * u;
+		const double poly = 1.0 + u2 + (m.c3 * u3) + (m.c4 * u4);
+		return scale * (m.a * std::sqrt(std::max(0.0, poly)));
+	};
+	auto err = [&](double z, double sx, double sy) {
+		const double dx = width(ax[0], z) - sx, dy = width(ax[1], z) - sy;
+		return (dx * dx) + (dy * dy);
+	};
+	constexpr int kGrid = 201, kIter = 80;
+	constexpr double kTol = 1e-3, kZTol = 1e-9, kQ = 0.2;
+	const double lo = -zMax, hi = zMax, span = hi - lo;
+	#pragma omp parallel for
+	for (long long i = 0; i < static_cast<long long>(size); ++i) {
+		const double sx = input[2 * i], sy = input[2 * i + 1];
+		double bestZ = lo, bestE = std::numeric_limits<double>::infinity();
+		for (int g = 0; g < kGrid; ++g) {
+			const double z = lo + ((static_cast<double>(g) / static_cast<double>(kGrid - 1)) * span);
+			const double e = err(z, sx, sy);
+			if (e < bestE) { bestE = e; bestZ = z; }
+		}
+		const double step = span / static_cast<double>(kGrid - 1);
+		double a = std::max(lo, std::min(bestZ - (2.0 * step), hi));
+		double b = std::max(lo, std::min(bestZ + (2.0 * step), hi));
+		if (b < a) { std::swap(a, b); }
+		// Brent: x best point so far, w second best, v the previous w; d the last step, e the one before
+		constexpr double kGold = 1.0 - 0.6180339887498948482;
+		double x = a + (kGold * (b - a)), w = x, v = x;
+		double fx = err(x, sx, sy), fw = fx, fv = fx, d = 0.0, e = 0.0;
+		double rz = x, rf = fx;
+		bool stopped = false;
+		for (int it = 0; it < kIter && !stopped; ++it) {
+			const double mid = 0.5 * (a + b);
+			const double tol1 = (kTol * std::abs(x)) + 1e-12, tol2 = 2.0 * tol1;
+			if (std::abs(x - mid) <= tol2 - (0.5 * (b - a))) { stopped = true; break; }
+			bool para = false;
+			if (std::abs(e) > tol1) {
+				const double r = (x - w) * (fx - fv);
+				double q = (x - v) * (fx - fw);
+				double p = ((x - v) * q) - ((x - w) * r);
+				q = 2.0 * (q - r);
+				if (q > 0.0) { p = -p; }
+				q = std::abs(q);
+				const double eOld = e;
+				e = d;
+				if (std::abs(p) < std::abs(0.5 * q * eOld) && p > q * (a - x) && p < q * (b - x)) {
+					para = true;
+					d = p / q;
+					const double u = x + d;
+					if (u - a < tol2 || b - u < tol2) { d = x < mid ? tol1 : -tol1; }
+				}
+			}
+			if (!para) {
+				e = x < mid ? b - x : a - x;
+				d = kGold * e;
+			}
+			const double u = x + (std::abs(d) >= tol1 ? d : (d > 0.0 ? tol1 : -tol1));
+			const double fu = err(u, sx, sy);
+			if (fu <= fx) {
+				if (u < x) { b = x; } else { a = x; }
+				v = w; fv = fw; w = x; fw = fx; x = u; fx = fu;
+			}
+			else {
+				if (u < x) { a = u; } else { b = u; }
+				if (fu <= fw || std::abs(x - w) <= kZTol) { v = w; fv = fw; w = u; fw = fu; }
+				else if (fu <= fv || std::abs(v - x) <= kZTol || std::abs(v - w) <= kZTol) { v = u; fv = fu; }
+			}
+		}
+		rz = x;
+		rf = fx;
+		const double z = rf < bestE ? rz : bestZ;
+		const double px = width(ax[0], z), py = width(ax[1], z);
+		double score = 0.0;
+		if (std::isfinite(px) && std::isfinite(py) && px > 0 && py > 0 && std::isfinite(sx) && std::isfinite(sy) && sx > 0 && sy > 0) {
+			const double rx = (sx - px) / px / kQ, ry = (sy - py) / py / kQ;
+			score = 1.0 / (1.0 + (0.5 * ((rx * rx) + (ry * ry))));
+		}
+		output[2 * i] = z;
+		output[2 * i + 1] = score;
+	}
 }
 
 // Analysis helpers for the maximum-likelihood modes 6-8 (fit_params as for orc_Localization); theta is local to

@@ -91,6 +91,21 @@ PTB_API double AutoThreshold(const uint16_t* input, uint64_t height, uint64_t wi
 	}
 }
 
+PTB_API void Astigmatism3DEstimation(const double* input, double* output, uint64_t size, double pixelSize, const double* model,
+                                     double zMax)
+{
+	ptb::ClearError();
+	try {
+		if (size == 0) { return; }
+		std::unique_lock<std::mutex> lock;
+		if (!ptb::EngineFor(lock).AstigEstimate(input, output, size, pixelSize, model, zMax)) { Report("Astigmatism3DEstimation"); }
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("Astigmatism3DEstimation");
+	}
+}
+
 PTB_API uint64_t PTB_LocalizationDevice(const uint16_t* d_input, double* d_output, uint64_t outputSize, uint64_t height,
                                         uint64_t width, uint64_t planes, double thresholdVal, double watershedRatio, uint64_t fit,
                                         const double* fit_params, void* stream)

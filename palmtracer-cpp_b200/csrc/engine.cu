@@ -24,6 +24,7 @@ bool LaunchSortFrames(const Workspace& ws, double* out, unsigned long long* rowB
                       cudaStream_t st);
 bool LaunchFit(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
                uint32_t cap, const FitParams& fp, double* rows, uint8_t* flags, int precision, cudaStream_t st);
+bool LaunchAstigEstimate(const double* dIn, double* dOut, uint64_t n, double pixelSize, const double* model, double zMax, cudaStream_t st);
 
 // ---- error plumbing -------------------------------------------------------------------------------------------
 namespace {
@@ -782,6 +783,23 @@ double Engine::AutoThreshold(const uint16_t* input, uint64_t height, uint64_t wi
 }
 
 // One engine per device, guarded by a mutex (calls on one device are serialized).
+bool Engine::AstigEstimate(const double* input, double* output, uint64_t n, double pixelSize, const double* model, double zMax)
+{
+	if (n == 0) { return true; }
+	if (!Init()) { return false; }
+	const size_t bytes = static_cast<size_t>(n) * 2 * sizeof(double);
+	double* dIn = nullptr;
+	double* dOut = nullptr;
+	bool ok = PTB_CUDA(cudaMallocAsync(&dIn, bytes, stream_));
+	ok = ok && PTB_CUDA(cudaMallocAsync(&dOut, bytes, stream_));
+	ok = ok && PTB_CUDA(cudaMemcpyAsync(dIn, input, bytes, cudaMemcpyHostToDevice, stream_));
+	ok = ok && LaunchAstigEstimate(dIn, dOut, n, pixelSize, model, zMax, stream_);
+	ok = ok && PTB_CUDA(cudaMemcpyAsync(output, dOut, bytes, cudaMemcpyDeviceToHost, stream_));
+	if (dIn) { cudaFreeAsync(dIn, stream_); }
+	if (dOut) { cudaFreeAsync(dOut, stream_); }
+	return PTB_CUDA(cudaStreamSynchronize(stream_)) && ok;
+}
+
 Engine& EngineFor(std::unique_lock<std::mutex>& lock)
 {
 	static std::mutex mu;

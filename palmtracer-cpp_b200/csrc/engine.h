@@ -47,6 +47,8 @@ public:
 	                       uint64_t width, uint64_t planes, uint64_t fit, const double* fitParams);
 	bool Planes(const uint16_t* input, double* output, uint64_t height, uint64_t width, uint64_t planes, int level);
 	double AutoThreshold(const uint16_t* input, uint64_t height, uint64_t width, const double* fitParams);
+	// Astigmatism3DEstimation over host buffers: [n][2] widths (px) -> [n][2] (z nm, score).
+	bool AstigEstimate(const double* input, double* output, uint64_t n, double pixelSize, const double* model, double zMax);
 
 	int SetStrict(int s) { const int o = strict_; strict_ = s; return o; }
 	int SetProfiling(int p) { const int o = profiling_; profiling_ = p; return o; }

@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libpalmtracer_b200.so")
 COLS = 18
 
 # every symbol the public header declares
-EXPORTS = ["Localization", "Fitting", "Wavelett", "AutoThreshold", "PTB_LocalizationDevice",
+EXPORTS = ["Localization", "Fitting", "Wavelett", "AutoThreshold", "Astigmatism3DEstimation", "PTB_LocalizationDevice",
            "PTB_SetSegmentationMode", "PTB_SetFitPrecision", "PTB_LastError", "PTB_KernelLaunchCount",
            "PTB_SetProfiling", "PTB_StageTimes", "PTB_MleEvaluations", "PTB_MeasureFmaPeak", "PTB_FittingDeviceNoAlloc",
            "PTB_ServerStart", "PTB_SubmitStack", "PTB_PollStack", "PTB_StackResult", "PTB_ServerStop"]
@@ -42,6 +42,8 @@ def load(path=LIB_PATH):
     L.Wavelett.argtypes = [_u16p, _f64p, _u64, _u64, _u64, _u64]
     L.AutoThreshold.restype = _f64
     L.AutoThreshold.argtypes = [_u16p, _u64, _u64, _f64p]
+    L.Astigmatism3DEstimation.restype = None
+    L.Astigmatism3DEstimation.argtypes = [_f64p, _f64p, _u64, _f64, _f64p, _f64]
     L.PTB_LocalizationDevice.restype = _u64
     L.PTB_LocalizationDevice.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _u64, _u64, _u64, _u64, _f64, _f64, _u64, _f64p,
                                          ctypes.c_void_p]
@@ -140,6 +142,16 @@ def auto_threshold(frame, params):
     h, w = frame.shape[-2:]
     params = np.ascontiguousarray(params, dtype=np.float64)
     return L.AutoThreshold(frame.ctypes.data_as(_u16p), h, w, params.ctypes.data_as(_f64p))
+
+
+def astig_estimation(sigmas, pixel_size, model, zmax):
+    """Astigmatism3DEstimation: [n, 2] (sigma_x, sigma_y) px -> [n, 2] (z nm, score)."""
+    sigmas = np.ascontiguousarray(sigmas, dtype=np.float64).reshape(-1, 2)
+    out = np.zeros_like(sigmas)
+    model = np.ascontiguousarray(model, dtype=np.float64)
+    load().Astigmatism3DEstimation(sigmas.ctypes.data_as(_f64p), out.ctypes.data_as(_f64p), sigmas.shape[0], pixel_size,
+                                   model.ctypes.data_as(_f64p), zmax)
+    return out
 
 
 def localization_device(d_input_ptr, d_output_ptr, capacity_doubles, shape, thr, ratio, fit, params, stream_ptr=0):

@@ -16,7 +16,7 @@ def declared():
 
 def test_header_declares_reference_exports():
     names = declared()
-    for n in ("Localization", "Fitting", "Wavelett", "AutoThreshold"):
+    for n in ("Localization", "Fitting", "Wavelett", "AutoThreshold", "Astigmatism3DEstimation"):
         assert n in names
 
 

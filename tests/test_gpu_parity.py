@@ -383,3 +383,17 @@ def test_mle_autotuned_matches_fixed(lib, orc):
     a = lib.localization(s, thr, 0.0, 6, MLE6)
     b = orc.localization(s, thr, 0.0, 6, MLE6)
     _mle_check(a, b, "mode6 gauss c1 autotuned", 6, 1 / 500, orc, s, thr, MLE6)
+
+
+# ---- Astigmatism3DEstimation: bit-exact against the oracle (itself pinned to the reference build) ---------------
+def test_astig_estimation_bitwise(lib, orc):
+    from test_oracle import BENCH_ASTIG, ESTIMATE_MODEL, _astig_widths
+    rng = np.random.default_rng(5)
+    for model, zmax in ((BENCH_ASTIG, 600.0), (ESTIMATE_MODEL, 500.0)):
+        z = rng.uniform(-1.2 * zmax, 1.2 * zmax, 20000)
+        s = _astig_widths(model, z) * rng.normal(1.0, 0.05, (z.size, 2))
+        s[:5] = [[0.0, 1.0], [-1.0, 2.0], [np.nan, 1.0], [1.0, np.inf], [1e-9, 1e-9]]
+        a = lib.astig_estimation(s, 160.0, model, zmax)
+        b = orc.astig_estimation(s, 160.0, model, zmax)
+        assert np.array_equal(a, b, equal_nan=True), float(np.nanmax(np.abs(a - b)))
+    assert lib.astig_estimation(np.zeros((0, 2)), 160.0, BENCH_ASTIG, 600.0).shape == (0, 2)

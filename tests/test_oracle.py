@@ -126,3 +126,54 @@ def test_oracle_spline_equals_reference_build(orc, ref, stacks):
         a = orc.localization(stacks["stack"][:4], 103.6, 0.0, 5, params)
         b = ref.localization(stacks["stack"][:4], 103.6, 0.0, 5, params)
         assert a.shape == b.shape and np.array_equal(a, b, equal_nan=True)
+
+
+# ---- Astigmatism3DEstimation (AstigFit::Estimate) -----------------------------------------------------------------
+ESTIMATE_MODEL = [-1000.0, 1000.0, 0.0, 0.0, 160.0, 1000.0, 1000.0, 0.0, 0.0, 160.0]
+BENCH_ASTIG = [150.0, 400.0, 0.05, 0.0, 1.3 * 160, -150.0, 400.0, -0.05, 0.0, 1.3 * 160]
+
+
+def _astig_widths(model, z, pixel_size=160.0):
+    out = []
+    for k in (0, 5):
+        z0, w, c3, c4, a = model[k:k + 5]
+        u = (z - z0) / w
+        out.append(a / pixel_size * np.sqrt(np.maximum(0.0, 1 + u * u + c3 * u ** 3 + c4 * u ** 4)))
+    return np.stack(out, axis=1)
+
+
+def test_astig_estimation_matches_reference_bitwise(orc, ref):
+    """The restated z estimate equals the reference build bit for bit (grid, Brent steps, score)."""
+    rng = np.random.default_rng(11)
+    for model, zmax in ((BENCH_ASTIG, 600.0), (ESTIMATE_MODEL, 500.0), ([-60.0, 300.0, 0.06, 0.02, 140.0, 60.0, 300.0, -0.06, 0.02, 140.0], 600.0)):
+        z = rng.uniform(-1.2 * zmax, 1.2 * zmax, 3000)
+        s = _astig_widths(model, z) * rng.normal(1.0, 0.05, (z.size, 2))
+        s[:5] = [[0.0, 1.0], [-1.0, 2.0], [np.nan, 1.0], [1.0, np.inf], [1e-9, 1e-9]]  # degenerate widths
+        a = orc.astig_estimation(s, 160.0, model, zmax)
+        b = ref.astig_estimation(s, 160.0, model, zmax)
+        assert np.array_equal(a, b, equal_nan=True)
+
+
+@pytest.mark.parametrize("observed, expected", [(-600.0, -500.0), (-500.0, -500.0), (-499.0, -499.0), (-123.4, -123.4),
+                                                (0.0, 0.0), (123.4, 123.4), (499.0, 499.0), (500.0, 500.0), (600.0, 500.0)])
+def test_astig_estimation_reference_cases(orc, observed, expected):
+    """The reference test's estimate cases (Tests_CPU/test_fit_AstigFit.cpp:37-50, 241-256): exact at the bounds,
+    within 1 nm inside."""
+    s = _astig_widths(ESTIMATE_MODEL, np.array([observed]))
+    z, score = orc.astig_estimation(s, 160.0, ESTIMATE_MODEL, 500.0)[0]
+    if abs(expected) == 500.0:
+        assert z == expected
+    else:
+        assert abs(z - expected) <= 1.0 and -500.0 < z < 500.0
+        assert score > 0.999
+
+
+def test_astig_estimation_recovers_noisy_z(orc):
+    """Reference test Estimate (test_fit_AstigFit.cpp:223-238): 0.02 px noise, z in [-200, 200], within 40 nm, score
+    > 0.95."""
+    model = [-60.0, 300.0, 0.06, 0.02, 140.0, 60.0, 300.0, -0.06, 0.02, 140.0]
+    rng = np.random.default_rng(42)
+    z = rng.uniform(-200.0, 200.0, 10)
+    s = _astig_widths(model, z) + rng.normal(0.0, 0.02, (10, 2))
+    r = orc.astig_estimation(s, 160.0, model, 800.0)
+    assert np.all(np.abs(r[:, 0] - z) <= 40.0) and np.all(r[:, 1] > 0.95) and np.all(r[:, 1] <= 1.0)
