@@ -449,19 +449,33 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 	const uint32_t rowsCap = static_cast<uint32_t>(std::min<uint64_t>(static_cast<uint64_t>(B) * maxPoints, 0xffffffffu));
 	if (!Reserve(H, W, B, rowsCap)) { return -1; }
 	const size_t N = static_cast<size_t>(H) * W;
-	const uint64_t chunks = (planes + B - 1) / B;
+	// chunk schedule: B frames each; with host input the last chunk is split so that at most about B / 8 frames
+	// remain to compute after the final copy-in (the copy-in, not the compute, is then the critical path)
+	std::vector<uint64_t> first, count;
+	for (uint64_t z0 = 0; z0 < planes; z0 += B) {
+		first.push_back(z0);
+		count.push_back(std::min<uint64_t>(B, planes - z0));
+	}
+	const uint64_t tail = std::max<uint64_t>(1, static_cast<uint64_t>(B) / 8);
+	if (!inputOnDevice && first.size() > 1 && count.back() > tail) {
+		const uint64_t last = count.back();
+		count.back() = last - tail;
+		first.push_back(first.back() + last - tail);
+		count.push_back(tail);
+	}
+	const uint64_t chunks = first.size();
 	const size_t slotBytes = N * B * sizeof(uint16_t);
 	if (!inputOnDevice && !ReserveImage((chunks > 1 ? 2 : 1) * slotBytes)) { return -1; }
 	if (!outputOnDevice && chunks > 1 && !ReserveRows2(static_cast<size_t>(ws_.capRows) * kCols * sizeof(double))) { return -1; }
 	double* outSlot[2] = {ws_.sortedRows, static_cast<double*>(rows2_)};
 	auto imgSlot = [&](int slot) { return static_cast<uint16_t*>(img_) + (slot ? N * B : 0); };
-	auto framesOf = [&](uint64_t k) { return static_cast<int>(std::min<uint64_t>(B, planes - k * B)); };
+	auto framesOf = [&](uint64_t k) { return static_cast<int>(count[k]); };
 	if (!PTB_CUDA(cudaMemsetAsync(rowBase_, 0, sizeof(unsigned long long), stream_))) { return -1; }
 	// input of chunk k into its slot; the slot's previous chunk (k - 2) must have finished reading it
 	auto copyIn = [&](uint64_t k) {
 		const int slot = static_cast<int>(k & 1);
 		if (k >= 2 && !PTB_CUDA(cudaStreamWaitEvent(copy_, done_[slot], 0))) { return false; }
-		if (!PTB_CUDA(cudaMemcpyAsync(imgSlot(slot), input + k * B * N, N * framesOf(k) * sizeof(uint16_t), cudaMemcpyHostToDevice, copy_))) {
+		if (!PTB_CUDA(cudaMemcpyAsync(imgSlot(slot), input + first[k] * N, N * framesOf(k) * sizeof(uint16_t), cudaMemcpyHostToDevice, copy_))) {
 			return false;
 		}
 		return PTB_CUDA(cudaEventRecord(h2d_[slot], copy_));
@@ -488,12 +502,12 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 		const int slot = static_cast<int>(k & 1);
 		const int b = framesOf(k);
 		PlanWorkspace(ws_, H, W, b, rowsCap, static_cast<char*>(pool_));
-		const uint16_t* dImg = inputOnDevice ? input + k * B * N : imgSlot(slot);
+		const uint16_t* dImg = inputOnDevice ? input + first[k] * N : imgSlot(slot);
 		if (!inputOnDevice) { ok = PTB_CUDA(cudaStreamWaitEvent(stream_, h2d_[slot], 0)); }
 		// the output slot of chunk k - 2 must be copied out before this chunk orders its rows into it
 		if (ok && !outputOnDevice && k >= 2) { ok = PTB_CUDA(cudaStreamWaitEvent(stream_, d2h_[slot], 0)); }
 		double* dOut = outputOnDevice ? output : outSlot[slot];
-		ok = ok && EnqueueChunk(slot, dImg, H, W, b, thr, ratio, maxPoints, fp, dOut, outputOnDevice, k * B);
+		ok = ok && EnqueueChunk(slot, dImg, H, W, b, thr, ratio, maxPoints, fp, dOut, outputOnDevice, first[k]);
 		if (ok && !inputOnDevice && k + 1 < chunks) { ok = copyIn(k + 1); }
 		if (ok && profiling_) { ok = complete(k); }  // stage timing needs each chunk finished before the next starts
 		else if (ok && k >= 1) { ok = complete(k - 1); }

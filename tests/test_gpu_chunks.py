@@ -45,7 +45,8 @@ def _one_chunk(lib, s, thr, fit, params):
     return lib.localization(s, thr, 0.0, fit, params)
 
 
-def test_many_chunks_match_one_chunk(lib, orc, tmp_path, monkeypatch):
+@pytest.mark.parametrize("budget_mb", ["8", "30"])  # 1 frame per chunk; 3 per chunk with the last chunk split (3, 3, 2, 1)
+def test_many_chunks_match_one_chunk(lib, orc, tmp_path, monkeypatch, budget_mb):
     import synth
     monkeypatch.setenv("PTB_MLE_LANES", "1")
     s, _ = synth.stack("c1", frames=9, seed=77)
@@ -56,7 +57,7 @@ def test_many_chunks_match_one_chunk(lib, orc, tmp_path, monkeypatch):
     inp = tmp_path / "in.npz"
     outp = tmp_path / "out.npz"
     np.savez(inp, stack=s, thr=thr, fit_g=2, params_g=GAUSS_PARAMS, fit_m=6, params_m=MLE6)
-    env = dict(os.environ, PTB_WORKSPACE_MB="8", PTB_MLE_LANES="1")
+    env = dict(os.environ, PTB_WORKSPACE_MB=budget_mb, PTB_MLE_LANES="1")
     r = subprocess.run([sys.executable, "-c", CHILD, ROOT, str(inp), str(outp)], env=env, capture_output=True, text=True,
                        timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
