@@ -1,5 +1,7 @@
 // Exclusive prefix sum of uint32 in place, with the element count either known on the host or read from device
 // memory (so a chain of kernels needs no host round trip). data[n] receives the total; `total`, when given, too.
+#include <algorithm>
+
 #include "pt_common.cuh"
 
 namespace ptb {
@@ -40,14 +42,10 @@ __device__ uint32_t BlockExclusive(uint32_t v, uint32_t* warpSums, uint32_t* tot
 	return warpBase + x - v;
 }
 
-// Phase 1: local exclusive scan of each tile in place; tile sums to blockSums.
-__global__ void __launch_bounds__(kScanThreads) ScanTiles(uint32_t* data, const uint32_t* nptr, uint32_t nconst,
-                                                          uint32_t* blockSums)
+// One tile of kScanTile entries: exclusive scan in place, the tile's sum to blockSums[tile].
+__device__ void ScanTile(uint32_t* data, uint32_t n, long long tile, uint32_t* warpSums, uint32_t* blockSums)
 {
-	__shared__ uint32_t warpSums[32];
-	const uint32_t n = CountOf(nptr, nconst);
-	const long long base = static_cast<long long>(blockIdx.x) * kScanTile;
-	if (base >= n) { return; }
+	const long long base = tile * kScanTile;
 	uint32_t v[kScanItems];
 	uint32_t sum = 0;
 	#pragma unroll
@@ -64,8 +62,21 @@ __global__ void __launch_bounds__(kScanThreads) ScanTiles(uint32_t* data, const 
 		if (i < n) { data[i] = off; }
 		off += v[k];
 	}
-	if (threadIdx.x == 0) { blockSums[blockIdx.x] = total; }
+	if (threadIdx.x == 0) { blockSums[tile] = total; }
 }
+
+// Phase 1: local exclusive scan of each tile in place; tile sums to blockSums. Tiles are visited grid-stride, so the
+// grid stays small when the device-side count is far below the capacity.
+__global__ void __launch_bounds__(kScanThreads) ScanTiles(uint32_t* data, const uint32_t* nptr, uint32_t nconst,
+                                                          uint32_t* blockSums)
+{
+	__shared__ uint32_t warpSums[32];
+	const uint32_t n = CountOf(nptr, nconst);
+	for (long long tile = blockIdx.x; tile * kScanTile < n; tile += gridDim.x) {
+		ScanTile(data, n, tile, warpSums, blockSums);
+	}
+}
+
 
 // Phase 2: one CTA scans the tile sums (exclusive) and stores the grand total.
 __global__ void __launch_bounds__(kScanThreads) ScanSums(uint32_t* blockSums, const uint32_t* nptr, uint32_t nconst,
@@ -94,13 +105,15 @@ __global__ void __launch_bounds__(kScanThreads) ScanAdd(uint32_t* data, const ui
                                                         const uint32_t* blockSums)
 {
 	const uint32_t n = CountOf(nptr, nconst);
-	const long long base = static_cast<long long>(blockIdx.x) * kScanTile;
-	if (base >= n || blockIdx.x == 0) { return; }
-	const uint32_t add = blockSums[blockIdx.x];
-	#pragma unroll
-	for (int k = 0; k < kScanItems; ++k) {
-		const long long i = base + static_cast<long long>(k) * kScanThreads + threadIdx.x;
-		if (i < n) { data[i] += add; }
+	for (long long tile = blockIdx.x; tile * kScanTile < n; tile += gridDim.x) {
+		if (tile == 0) { continue; }
+		const long long base = tile * kScanTile;
+		const uint32_t add = blockSums[tile];
+		#pragma unroll
+		for (int k = 0; k < kScanItems; ++k) {
+			const long long i = base + static_cast<long long>(k) * kScanThreads + threadIdx.x;
+			if (i < n) { data[i] += add; }
+		}
 	}
 }
 
@@ -111,7 +124,7 @@ bool ExclusiveScan(uint32_t* data, const uint32_t* nptr, uint32_t nconst, uint32
                    uint32_t* totalOut, cudaStream_t st)
 {
 	const uint32_t tiles = static_cast<uint32_t>((static_cast<unsigned long long>(cap) + kScanTile - 1) / kScanTile);
-	const uint32_t grid = tiles > 0 ? tiles : 1;
+	const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(tiles, 2 * 148));
 	ScanTiles<<<grid, kScanThreads, 0, st>>>(data, nptr, nconst, blockSums);
 	ScanSums<<<1, kScanThreads, 0, st>>>(blockSums, nptr, nconst, data, totalOut);
 	ScanAdd<<<grid, kScanThreads, 0, st>>>(data, nptr, nconst, blockSums);
