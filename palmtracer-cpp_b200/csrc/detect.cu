@@ -101,7 +101,8 @@ __device__ __forceinline__ long long W1At(const TileSmem& s, int r, int c)
 }
 
 // ---- Detection kernel ------------------------------------------------------------------------------------------
-// Five register-blocked passes over one 128 x 32 tile. Borders: every intermediate array is kept edge-replicated
+// The input tile is first staged in shared memory with 16-byte loads; then five register-blocked passes over one
+// 128 x 32 tile. Borders: every intermediate array is kept edge-replicated
 // (an entry whose coordinate lies outside the frame holds the value of the nearest in-frame entry), which is what
 // the reference's clamping of every neighbour access amounts to, so no pass clamps an index:
 //   A  C1 = vertical level-1 taps of the input, one lane per column sliding down 46 clamped input rows (rows outside
@@ -119,7 +120,10 @@ constexpr int kPV = 144;  // V1 pitch (tile col = index - 5, tile row = index - 
 constexpr int kRows1 = TY + 10;  // C1 and V1 rows
 constexpr int kRows2 = TY + 2;   // C2 rows and ring rows (tile row = index - 1)
 constexpr int kDetectWords = kRows1 * kP1 + kRows1 * kPV;
+constexpr int kInRows = TY + 14, kInW = 160;  // staged input tile (uint16): rows y0-7.., columns x0-8..
 static_assert(kRows2 * kPV <= kRows1 * kP1, "C2 must fit in the C1 space");
+static_assert(kInRows * kInW * 2 <= kRows1 * kPV * 4, "the staged input must fit in the V1 space");
+static_assert(kP1 + 1 <= kInW, "C1 columns read staged columns 1 .. kP1");
 
 __device__ __forceinline__ uint32_t Tap(uint32_t m2, uint32_t m1, uint32_t c, uint32_t p1, uint32_t p2)
 {
@@ -138,17 +142,35 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 	const uint16_t* frame = img + static_cast<long long>(f) * ws.g.N;
 	const int tid = threadIdx.x;
 
-	// A: C1, one lane per column
+	// stage the input tile (rows y0-7 .. y0+38, columns x0-8 .. x0+151, clamped into the frame) in the V1 space,
+	// which pass B fills only after pass A: every thread issues independent 16-byte loads when the tile's columns lie
+	// inside the frame and rows are 16-byte aligned, clamped 2-byte loads otherwise (frame offsets fit in 32 bits)
+	uint16_t* in = reinterpret_cast<uint16_t*>(v1);
+	{
+		const bool vec = x0 - 8 >= 0 && x0 - 8 + kInW <= W && (W & 7) == 0 &&
+		                 (reinterpret_cast<uintptr_t>(frame) & 15) == 0;
+		if (vec) {
+			for (int q = tid; q < kInRows * (kInW / 8); q += kThreads) {
+				const int r = q / (kInW / 8), v = q - r * (kInW / 8);
+				const uint4* src = reinterpret_cast<const uint4*>(frame + clampi(y0 - 7 + r, 0, H - 1) * W + x0 - 8) + v;
+				reinterpret_cast<uint4*>(in + r * kInW)[v] = __ldg(src);
+			}
+		}
+		else {
+			for (int q = tid; q < kInRows * kInW; q += kThreads) {
+				const int r = q / kInW, c = q - r * kInW;
+				in[q] = __ldg(frame + clampi(y0 - 7 + r, 0, H - 1) * W + clampi(x0 - 8 + c, 0, W - 1));
+			}
+		}
+	}
+	__syncthreads();
+	// A: C1, one lane per column (C1 column i = staged column i + 1)
 	for (int i = tid; i < kP1; i += kThreads) {
-		// frame offsets fit in 32 bits (H * W < 2^31)
-		const uint16_t* col = frame + clampi(x0 - 7 + i, 0, W - 1);
-		uint32_t w0 = __ldg(col + clampi(y0 - 7, 0, H - 1) * W);
-		uint32_t w1 = __ldg(col + clampi(y0 - 6, 0, H - 1) * W);
-		uint32_t w2 = __ldg(col + clampi(y0 - 5, 0, H - 1) * W);
-		uint32_t w3 = __ldg(col + clampi(y0 - 4, 0, H - 1) * W);
+		const uint16_t* col = in + i + 1;
+		uint32_t w0 = col[0], w1 = col[kInW], w2 = col[2 * kInW], w3 = col[3 * kInW];
 		#pragma unroll 6
 		for (int r = 0; r < kRows1; ++r) {
-			const uint32_t w4 = __ldg(col + clampi(y0 - 3 + r, 0, H - 1) * W);
+			const uint32_t w4 = col[(r + 4) * kInW];
 			c1[r * kP1 + i] = Tap(w0, w1, w2, w3, w4);
 			w0 = w1; w1 = w2; w2 = w3; w3 = w4;
 		}
