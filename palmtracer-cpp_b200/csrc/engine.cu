@@ -255,9 +255,11 @@ Engine::~Engine()
 	if (fallbacks_) { cudaFree(fallbacks_); }
 	if (evalDev_) { cudaFree(evalDev_); }
 	if (rowBase_) { cudaFree(rowBase_); }
-	if (rows2_) { cudaFree(rows2_); }
 	if (hostCnt_) { cudaFreeHost(hostCnt_); }
 	if (copy_) { cudaStreamDestroy(copy_); }
+	if (copyOut_) { cudaStreamDestroy(copyOut_); }
+	if (pool1_) { cudaFree(pool1_); }
+	if (stream1_) { cudaStreamDestroy(stream1_); }
 	if (stream_) { cudaStreamDestroy(stream_); }
 }
 
@@ -267,6 +269,12 @@ bool Engine::Init()
 	if (!PTB_CUDA(cudaGetDevice(&device_))) { return false; }
 	if (!PTB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking))) { return false; }
 	if (!PTB_CUDA(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking))) { return false; }
+	if (!PTB_CUDA(cudaStreamCreateWithFlags(&copyOut_, cudaStreamNonBlocking))) { return false; }
+	if (!PTB_CUDA(cudaStreamCreateWithFlags(&stream1_, cudaStreamNonBlocking))) { return false; }
+	for (auto& e : sortDone_) {
+		if (!PTB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming))) { return false; }
+	}
+	if (!PTB_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming))) { return false; }
 	if (!PTB_CUDA(cudaMallocHost(&hostCnt_, 2 * sizeof(Counters)))) { return false; }
 	if (!PTB_CUDA(cudaMalloc(&rowBase_, sizeof(unsigned long long)))) { return false; }
 	for (int k = 0; k < 2; ++k) {
@@ -291,7 +299,7 @@ bool Engine::Init()
 	return true;
 }
 
-bool Engine::Reserve(int H, int W, int B, uint32_t rowsCap)
+bool Engine::Reserve(int H, int W, int B, uint32_t rowsCap, int slots)
 {
 	Workspace probe{};
 	const size_t need = PlanWorkspace(probe, H, W, B, rowsCap, nullptr);
@@ -301,6 +309,14 @@ bool Engine::Reserve(int H, int W, int B, uint32_t rowsCap)
 		poolBytes_ = need;
 	}
 	PlanWorkspace(ws_, H, W, B, rowsCap, static_cast<char*>(pool_));
+	if (slots > 1) {
+		if (need > pool1Bytes_) {
+			if (pool1_) { cudaFree(pool1_); pool1_ = nullptr; pool1Bytes_ = 0; }
+			if (!PTB_CUDA(cudaMalloc(&pool1_, need))) { return false; }
+			pool1Bytes_ = need;
+		}
+		PlanWorkspace(ws1_, H, W, B, rowsCap, static_cast<char*>(pool1_));
+	}
 	return true;
 }
 
@@ -318,44 +334,48 @@ size_t Engine::EstimateBytes(uint64_t height, uint64_t width, uint64_t planes, u
 	if (planes == 0 || height == 0 || width == 0) { return 0; }
 	const int H = static_cast<int>(height), W = static_cast<int>(width);
 	const uint32_t maxPoints = static_cast<uint32_t>(std::min<uint64_t>((outputSize / kCols) / planes, 0xffffffffu));
-	const int B = ChunkFrames(H, W, planes, maxPoints);
+	int B = 1, slots = 1;
+	ChunkPlan(H, W, planes, maxPoints, B, slots);
 	const uint32_t rowsCap = static_cast<uint32_t>(std::min<uint64_t>(static_cast<uint64_t>(B) * maxPoints, 0xffffffffu));
 	Workspace probe{};
 	const size_t ws = PlanWorkspace(probe, H, W, B, rowsCap, nullptr);
 	const size_t img = 2ull * static_cast<size_t>(H) * W * B * sizeof(uint16_t);
-	const size_t rows2 = static_cast<size_t>(probe.capRows) * kCols * sizeof(double);
-	return ws + img + rows2;
+	return slots * ws + img;
 }
 
-int Engine::ChunkFrames(int H, int W, uint64_t planes, uint32_t maxPoints) const
+int Engine::ChunkFrames(int H, int W, uint64_t planes, uint32_t maxPoints, size_t budget) const
 {
 	const long long N = static_cast<long long>(H) * W;
 	// bytes per frame: ~40 B per pixel of dense lists plus ~100 B per independent-set slot plus fit rows
 	const double perFrame = 48.0 * N + 100.0 * IndepBound(H, W) +
 	                        std::min<double>(maxPoints, IndepBound(H, W)) * 360.0 + 2.0 * N;
-	long long B = static_cast<long long>(static_cast<double>(budget_) / perFrame);
+	long long B = static_cast<long long>(static_cast<double>(budget) / perFrame);
 	B = std::max<long long>(1, std::min<long long>(B, static_cast<long long>(planes)));
 	// global pixel indices of a chunk stay below 2^31 (the top bit tags component ids)
 	B = std::min<long long>(B, std::max<long long>(1, ((1ll << 31) - 1) / std::max<long long>(N, 1)));
 	return static_cast<int>(B);
 }
 
-// Runs detection -> segmentation -> fits -> ordering for B frames whose pixels are at dImg (device). The chunk's
-// rows go to dOut (device) numbered from Id idBase + 1 and Plane planeBase + 1; returns the row count or -1.
-bool Engine::ReserveRows2(size_t bytes)
+// One chunk when the whole stack fits the budget; otherwise two chunk slots with half the budget each, so that two
+// chunks are in flight on two compute streams.
+void Engine::ChunkPlan(int H, int W, uint64_t planes, uint32_t maxPoints, int& B, int& slots) const
 {
-	if (bytes <= rows2Bytes_) { return true; }
-	if (rows2_) { cudaFree(rows2_); rows2_ = nullptr; rows2Bytes_ = 0; }
-	if (!PTB_CUDA(cudaMalloc(&rows2_, bytes))) { return false; }
-	rows2Bytes_ = bytes;
-	return true;
+	B = ChunkFrames(H, W, planes, maxPoints, budget_);
+	slots = 1;
+	if (static_cast<uint64_t>(B) < planes) {
+		B = ChunkFrames(H, W, planes, maxPoints, budget_ / 2);
+		slots = 2;
+	}
 }
 
+// Runs detection -> segmentation -> fits -> ordering for B frames whose pixels are at dImg (device). The chunk's
+// rows go to dOut (device) numbered from Id idBase + 1 and Plane planeBase + 1; returns the row count or -1.
 bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, double thr, double ratio, uint32_t maxPoints,
-                          const FitParams& fp, double* dOut, bool offsetOut, unsigned long long planeBase)
+                          const FitParams& fp, double* dOut, bool offsetOut, unsigned long long planeBase, bool afterOther)
 {
-	ws_.img = dImg;
-	cudaStream_t st = stream_;
+	Workspace& ws = Ws(slot);
+	ws.img = dImg;
+	cudaStream_t st = St(slot);
 	const bool prof = profiling_ != 0;
 	uint64_t l0 = LaunchCount();
 	auto mark = [&](int k) {
@@ -364,16 +384,17 @@ bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, d
 			if (k > 0) { pendLaunches_[k - 1] = LaunchCount() - l0; l0 = LaunchCount(); }
 		}
 	};
-	bool ok = PTB_CUDA(cudaMemsetAsync(ws_.cnt, 0, sizeof(Counters), st));
-	ok = ok && PTB_CUDA(cudaMemsetAsync(ws_.rootmask, 0, sizeof(uint32_t) * static_cast<size_t>(B) * H * ws_.g.words, st));
+	bool ok = PTB_CUDA(cudaMemsetAsync(ws.cnt, 0, sizeof(Counters), st));
+	ok = ok && PTB_CUDA(cudaMemsetAsync(ws.rootmask, 0, sizeof(uint32_t) * static_cast<size_t>(B) * H * ws.g.words, st));
 	mark(0);
-	ok = ok && LaunchDetect(ws_, thr, st);
+	ok = ok && LaunchDetect(ws, thr, st);
 	mark(1);
-	ok = ok && LaunchSegment(ws_, ratio, strict_, maxPoints, st);
-	ok = ok && LaunchBuildCandidates(ws_, st);
+	ok = ok && LaunchSegment(ws, ratio, strict_, maxPoints, st);
+	ok = ok && LaunchBuildCandidates(ws, st);
 	mark(2);
 	FitParams fpr = fp;
-	if (ok && fp.mode >= kMleGauss && fp.lanes == 0) { ok = Autotune(fpr, dImg, H, W); }
+	if (ok && fp.mode >= kMleGauss && fp.lanes == 0) { ok = Autotune(fpr, dImg, H, W, slot); }
+	if (fp.mode >= kMleGauss) { fpr.mle.queue = ws.cnt->pad; }  // this slot's work-queue counters
 	pendMleProf_ = prof && fp.mode >= kMleGauss;
 	pendLanes_ = fpr.lanes;
 	if (pendMleProf_) {
@@ -382,11 +403,13 @@ bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, d
 		fpr.marks = mleEv_;
 		fpr.mle.evals = evalDev_;
 	}
-	ok = ok && LaunchFit(dImg, H, W, ws_.g.N, ws_.cand, &ws_.cnt->nfit, 0, ws_.capRows, fpr, ws_.rows, ws_.fitFlag, precision_, st);
+	ok = ok && LaunchFit(dImg, H, W, ws.g.N, ws.cand, &ws.cnt->nfit, 0, ws.capRows, fpr, ws.rows, ws.fitFlag, precision_, st);
 	mark(3);
-	ok = ok && LaunchSortFrames(ws_, dOut, rowBase_, offsetOut, planeBase, st);
+	if (afterOther) { ok = ok && PTB_CUDA(cudaStreamWaitEvent(st, sortDone_[1 - slot], 0)); }
+	ok = ok && LaunchSortFrames(ws, dOut, rowBase_, offsetOut, planeBase, st);
+	ok = ok && PTB_CUDA(cudaEventRecord(sortDone_[slot], st));
 	mark(4);
-	ok = ok && PTB_CUDA(cudaMemcpyAsync(hostCnt_ + slot, ws_.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+	ok = ok && PTB_CUDA(cudaMemcpyAsync(hostCnt_ + slot, ws.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
 	ok = ok && PTB_CUDA(cudaEventRecord(done_[slot], st));
 	return ok;
 }
@@ -423,10 +446,12 @@ long long Engine::CompleteChunk(int slot, uint32_t* truncatedFrames)
 	return c.nfit;
 }
 
-// Chunks run back to back on the compute stream; with host buffers, the input of chunk k + 1 is copied in and the rows
-// of chunk k - 1 are copied out on the copy stream while chunk k computes (two staging slots for the frames and, for
-// host output, for the ordered rows). Row numbering continues across chunks through a device-side row count, so the
-// host waits for a chunk only to learn how many rows it copies out.
+// A stack that fits the budget runs as one chunk. A longer one runs as chunks of half the budget on two chunk slots,
+// each with its own compute stream and workspace, so that one chunk's serial tail (the last fits, the ordering)
+// overlaps the next chunk's detection. With host buffers, the input of chunk k + 1 is copied in on one copy stream and
+// the rows of chunk k - 1 are copied out on another while chunk k computes (two staging slots for the frames). Row
+// numbering continues across chunks through a device-side row count that each chunk's ordering step advances after
+// the previous chunk's, so the host waits for a chunk only to learn how many rows it copies out.
 long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* output, bool outputOnDevice, uint64_t outputSize,
                            uint64_t height, uint64_t width, uint64_t planes, double thr, double ratio, uint64_t fit,
                            const double* fitParams)
@@ -445,9 +470,11 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 	if (!UploadSpline(fp, spline)) { return -1; }
 	const int H = static_cast<int>(height), W = static_cast<int>(width);
 	const uint32_t maxPoints = static_cast<uint32_t>(std::min<uint64_t>(perPlane, 0xffffffffu));
-	const int B = ChunkFrames(H, W, planes, maxPoints);
+	int B = 1, slots = 1;
+	ChunkPlan(H, W, planes, maxPoints, B, slots);
 	const uint32_t rowsCap = static_cast<uint32_t>(std::min<uint64_t>(static_cast<uint64_t>(B) * maxPoints, 0xffffffffu));
-	if (!Reserve(H, W, B, rowsCap)) { return -1; }
+	if (!Reserve(H, W, B, rowsCap, slots)) { return -1; }
+	char* poolOf[2] = {static_cast<char*>(pool_), static_cast<char*>(pool1_)};
 	const size_t N = static_cast<size_t>(H) * W;
 	// chunk schedule: B frames each; with host input the last chunk is split so that at most about B / 8 frames
 	// remain to compute after the final copy-in (the copy-in, not the compute, is then the critical path)
@@ -466,11 +493,16 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 	const uint64_t chunks = first.size();
 	const size_t slotBytes = N * B * sizeof(uint16_t);
 	if (!inputOnDevice && !ReserveImage((chunks > 1 ? 2 : 1) * slotBytes)) { return -1; }
-	if (!outputOnDevice && chunks > 1 && !ReserveRows2(static_cast<size_t>(ws_.capRows) * kCols * sizeof(double))) { return -1; }
-	double* outSlot[2] = {ws_.sortedRows, static_cast<double*>(rows2_)};
+	// with two chunk slots, chunk k runs on slot k % 2 (its own stream and workspace); with host output its ordered
+	// rows stay in that workspace (where the chunk's own plan puts them) until copied out
+	double* outSlot[2] = {nullptr, nullptr};
 	auto imgSlot = [&](int slot) { return static_cast<uint16_t*>(img_) + (slot ? N * B : 0); };
 	auto framesOf = [&](uint64_t k) { return static_cast<int>(count[k]); };
 	if (!PTB_CUDA(cudaMemsetAsync(rowBase_, 0, sizeof(unsigned long long), stream_))) { return -1; }
+	// the second compute stream starts after everything ordered before this call on the first (the caller's input)
+	if (slots > 1 && (!PTB_CUDA(cudaEventRecord(fork_, stream_)) || !PTB_CUDA(cudaStreamWaitEvent(stream1_, fork_, 0)))) {
+		return -1;
+	}
 	// input of chunk k into its slot; the slot's previous chunk (k - 2) must have finished reading it
 	auto copyIn = [&](uint64_t k) {
 		const int slot = static_cast<int>(k & 1);
@@ -489,34 +521,40 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 		if (n < 0) { return false; }
 		if (!outputOnDevice && n > 0) {
 			if (!PTB_CUDA(cudaMemcpyAsync(output + rows * kCols, outSlot[slot], static_cast<size_t>(n) * kCols * sizeof(double),
-			                              cudaMemcpyDeviceToHost, copy_))) {
+			                              cudaMemcpyDeviceToHost, copyOut_))) {
 				return false;
 			}
 		}
-		if (!PTB_CUDA(cudaEventRecord(d2h_[slot], copy_))) { return false; }
+		if (!PTB_CUDA(cudaEventRecord(d2h_[slot], copyOut_))) { return false; }
 		rows += static_cast<unsigned long long>(n);
 		return true;
 	};
 	bool ok = inputOnDevice || copyIn(0);
 	for (uint64_t k = 0; ok && k < chunks; ++k) {
 		const int slot = static_cast<int>(k & 1);
+		const int ws = slots > 1 ? slot : 0;  // workspace and compute stream of this chunk
 		const int b = framesOf(k);
-		PlanWorkspace(ws_, H, W, b, rowsCap, static_cast<char*>(pool_));
+		PlanWorkspace(Ws(ws), H, W, b, rowsCap, poolOf[ws]);
 		const uint16_t* dImg = inputOnDevice ? input + first[k] * N : imgSlot(slot);
-		if (!inputOnDevice) { ok = PTB_CUDA(cudaStreamWaitEvent(stream_, h2d_[slot], 0)); }
+		if (!inputOnDevice) { ok = PTB_CUDA(cudaStreamWaitEvent(St(ws), h2d_[slot], 0)); }
 		// the output slot of chunk k - 2 must be copied out before this chunk orders its rows into it
-		if (ok && !outputOnDevice && k >= 2) { ok = PTB_CUDA(cudaStreamWaitEvent(stream_, d2h_[slot], 0)); }
+		if (ok && !outputOnDevice && k >= 2) { ok = PTB_CUDA(cudaStreamWaitEvent(St(ws), d2h_[slot], 0)); }
+		outSlot[slot] = Ws(ws).sortedRows;
 		double* dOut = outputOnDevice ? output : outSlot[slot];
-		ok = ok && EnqueueChunk(slot, dImg, H, W, b, thr, ratio, maxPoints, fp, dOut, outputOnDevice, first[k]);
+		ok = ok && EnqueueChunk(ws, dImg, H, W, b, thr, ratio, maxPoints, fp, dOut, outputOnDevice, first[k], slots > 1 && k > 0);
 		if (ok && !inputOnDevice && k + 1 < chunks) { ok = copyIn(k + 1); }
 		if (ok && profiling_) { ok = complete(k); }  // stage timing needs each chunk finished before the next starts
 		else if (ok && k >= 1) { ok = complete(k - 1); }
 	}
 	if (ok && !profiling_ && chunks > 0) { ok = complete(chunks - 1); }
-	ok = ok && PTB_CUDA(cudaStreamSynchronize(copy_));
+	// work ordered after this call on the first compute stream also follows the second's
+	if (ok && slots > 1) { ok = PTB_CUDA(cudaStreamWaitEvent(stream_, done_[1], 0)); }
+	ok = ok && PTB_CUDA(cudaStreamSynchronize(copy_)) && PTB_CUDA(cudaStreamSynchronize(copyOut_));
 	if (!ok) {
 		cudaStreamSynchronize(stream_);
+		cudaStreamSynchronize(stream1_);
 		cudaStreamSynchronize(copy_);
+		cudaStreamSynchronize(copyOut_);
 		return -1;
 	}
 	for (uint32_t i = 0; i < truncated; ++i) {
@@ -543,8 +581,10 @@ int Engine::TunedLanes(const FitParams& fp) const
 
 // Times both ROI mappings (1: thread per ROI, 32: warp per ROI) on this chunk's candidates and keeps the faster for
 // (mode, ROI).
-bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W)
+bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slot)
 {
+	Workspace& ws = Ws(slot);
+	cudaStream_t st = St(slot);
 	static const int kChoices[] = {1, 32};
 	cudaEvent_t a, b;
 	if (!PTB_CUDA(cudaEventCreate(&a)) || !PTB_CUDA(cudaEventCreate(&b))) { return false; }
@@ -553,11 +593,12 @@ bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W)
 	for (int lanes : kChoices) {
 		FitParams t = fp;
 		t.lanes = lanes;
-		cudaEventRecord(a, stream_);
-		if (!LaunchFit(dImg, H, W, ws_.g.N, ws_.cand, &ws_.cnt->nfit, 0, ws_.capRows, t, ws_.rows, ws_.fitFlag, precision_, stream_)) {
+		t.mle.queue = ws.cnt->pad;
+		cudaEventRecord(a, st);
+		if (!LaunchFit(dImg, H, W, ws.g.N, ws.cand, &ws.cnt->nfit, 0, ws.capRows, t, ws.rows, ws.fitFlag, precision_, st)) {
 			return false;
 		}
-		cudaEventRecord(b, stream_);
+		cudaEventRecord(b, st);
 		if (!PTB_CUDA(cudaEventSynchronize(b))) { return false; }
 		float ms = 0;
 		cudaEventElapsedTime(&ms, a, b);

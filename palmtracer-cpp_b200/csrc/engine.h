@@ -67,28 +67,37 @@ public:
 	bool Init();
 
 private:
-	bool Reserve(int H, int W, int B, uint32_t rowsCap);
+	bool Reserve(int H, int W, int B, uint32_t rowsCap, int slots);
 	bool ReserveImage(size_t bytes);
 	bool UploadSpline(FitParams& fp, const std::vector<double>& spline);
 	int TunedLanes(const FitParams& fp) const;
-	bool Autotune(FitParams& fp, const uint16_t* dImg, int H, int W);
-	int ChunkFrames(int H, int W, uint64_t planes, uint32_t maxPoints) const;
+	bool Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slot);
+	int ChunkFrames(int H, int W, uint64_t planes, uint32_t maxPoints, size_t budget) const;
+	// Chunk size and number of concurrent chunk slots (2 when the stack needs more than one chunk).
+	void ChunkPlan(int H, int W, uint64_t planes, uint32_t maxPoints, int& B, int& slots) const;
+	Workspace& Ws(int slot) { return slot ? ws1_ : ws_; }
+	cudaStream_t St(int slot) const { return slot ? stream1_ : stream_; }
 	// One chunk of B frames on the compute stream: detection, segmentation, fits, ordering into dOut (at dOut +
 	// rows so far when offsetOut), counters copied to the slot's pinned buffer, completion event recorded.
+	// afterOther: the chunk orders its rows after the chunk in flight on the other slot (its Ids continue from it).
 	bool EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, double thr, double ratio, uint32_t maxPoints,
-	                  const FitParams& fp, double* dOut, bool offsetOut, unsigned long long planeBase);
+	                  const FitParams& fp, double* dOut, bool offsetOut, unsigned long long planeBase, bool afterOther);
 	// Waits for the slot's chunk; returns its row count or -1 (error recorded).
 	long long CompleteChunk(int slot, uint32_t* truncatedFrames);
-	bool ReserveRows2(size_t bytes);
 
 	int device_ = 0;
 	cudaStream_t stream_ = nullptr;
-	cudaStream_t copy_ = nullptr;            // host<->device copies that overlap the compute stream
+	cudaStream_t copy_ = nullptr;            // host-to-device copies that overlap the compute streams
+	cudaStream_t copyOut_ = nullptr;         // device-to-host copies (the other direction of the link, concurrently)
+	cudaStream_t stream1_ = nullptr;         // second compute stream (second chunk slot)
+	cudaEvent_t sortDone_[2] = {};           // per chunk slot: its rows are ordered (Ids of the next chunk follow)
+	cudaEvent_t fork_ = nullptr;              // start of a two-slot call on the first compute stream
+	Workspace ws1_{};                        // second chunk slot's workspace and pool
+	void* pool1_ = nullptr;
+	size_t pool1Bytes_ = 0;
 	cudaEvent_t h2d_[2] = {}, done_[2] = {}, d2h_[2] = {};  // per staging slot
 	Counters* hostCnt_ = nullptr;             // pinned, one per staging slot
 	unsigned long long* rowBase_ = nullptr;   // device: rows written by the earlier chunks of the current call
-	void* rows2_ = nullptr;                   // second output staging buffer (host output)
-	size_t rows2Bytes_ = 0;
 	size_t budget_ = 0;
 	size_t fixedBudget_ = 0;
 	void* pool_ = nullptr;
