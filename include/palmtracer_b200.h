@@ -139,6 +139,12 @@ PTB_API void PTB_StageTimes(double* ms, uint64_t* launches, int n);
  * then resets them. */
 PTB_API void PTB_MleEvaluations(uint64_t* counts, int n);
 
+/* Launch-chain graphs of the current device's engine (diagnostics). A chunk's compute chain (counter reset,
+ * detection, segmentation, candidates, fits) is launched directly the first time its launch arguments occur, captured
+ * into a CUDA graph the second time and replayed from the graph after that (PTB_GRAPHS=0 turns graphs off).
+ * counts: [chunks captured, chunks replayed, chunks launched directly] since the last call (up to n entries). */
+PTB_API void PTB_GraphStats(uint64_t* counts, int n);
+
 /* FMA throughput probe of the current device (diagnostics): FLOP/s (2 per FMA) of FP64 (fp64 != 0) or FP32
  * arithmetic, timed with CUDA events over a grid of independent FMA chains; -1 on error. */
 PTB_API double PTB_MeasureFmaPeak(int fp64);

@@ -266,4 +266,10 @@ PTB_API void PTB_MleEvaluations(uint64_t* counts, int n)
 	ptb::EngineFor(lock).MleEvaluations(counts, n);
 }
 
+PTB_API void PTB_GraphStats(uint64_t* counts, int n)
+{
+	std::unique_lock<std::mutex> lock;
+	ptb::EngineFor(lock).GraphStats(counts, n);
+}
+
 }  // extern "C"

@@ -249,6 +249,9 @@ Engine::Engine() = default;
 
 Engine::~Engine()
 {
+	for (auto& list : graphs_) {
+		for (auto& g : list) { cudaGraphExecDestroy(g.exec); }
+	}
 	if (pool_) { cudaFree(pool_); }
 	if (img_) { cudaFree(img_); }
 	if (spline_) { cudaFree(spline_); }
@@ -267,6 +270,7 @@ bool Engine::Init()
 {
 	if (stream_) { return true; }
 	if (!PTB_CUDA(cudaGetDevice(&device_))) { return false; }
+	if (const char* env = std::getenv("PTB_GRAPHS")) { useGraphs_ = std::atoi(env) != 0; }
 	if (!PTB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking))) { return false; }
 	if (!PTB_CUDA(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking))) { return false; }
 	if (!PTB_CUDA(cudaStreamCreateWithFlags(&copyOut_, cudaStreamNonBlocking))) { return false; }
@@ -368,8 +372,89 @@ void Engine::ChunkPlan(int H, int W, uint64_t planes, uint32_t maxPoints, int& B
 	}
 }
 
+// Key of a chunk's launch chain: every value that the captured launches take by value (workspace plan, image
+// pointer, threshold, segmentation settings, fit configuration). Two chunks with equal keys launch identical kernels
+// with identical arguments, so a graph captured for one replays the other.
+static std::vector<uint64_t> ChainKey(int slot, const Workspace& ws, const uint16_t* dImg, double thr, double ratio,
+                                      int strict, uint32_t maxPoints, uint32_t rowsCap, int precision, const FitParams& f)
+{
+	std::vector<uint64_t> k;
+	k.reserve(64);
+	auto u = [&](uint64_t v) { k.push_back(v); };
+	auto d = [&](double v) { uint64_t b; std::memcpy(&b, &v, sizeof b); k.push_back(b); };
+	auto p = [&](const void* v) { k.push_back(reinterpret_cast<uintptr_t>(v)); };
+	u(static_cast<uint64_t>(slot)); p(ws.code); p(dImg);
+	u(static_cast<uint64_t>(ws.g.H)); u(static_cast<uint64_t>(ws.g.W)); u(static_cast<uint64_t>(ws.g.B)); u(rowsCap);
+	d(thr); d(ratio); u(static_cast<uint64_t>(strict)); u(maxPoints); u(static_cast<uint64_t>(precision));
+	u(static_cast<uint64_t>(f.mode)); u(static_cast<uint64_t>(f.roi)); u(static_cast<uint64_t>(f.half));
+	u(static_cast<uint64_t>(f.n)); u(static_cast<uint64_t>(f.nParams)); d(f.sigmaX); d(f.sigmaY); d(f.theta);
+	u(static_cast<uint64_t>(f.sx)); u(static_cast<uint64_t>(f.sy)); u(static_cast<uint64_t>(f.sz));
+	u(static_cast<uint64_t>(f.splineSize)); u(static_cast<uint64_t>(f.offsetXY)); d(f.roiParam); d(f.initZ); d(f.deltaZ);
+	d(f.intensityRatio); p(f.coeffs); u(static_cast<uint64_t>(f.lanes)); p(f.marks);
+	const MleParams& m = f.mle;
+	u(static_cast<uint64_t>(m.model)); u(static_cast<uint64_t>(m.roi)); u(static_cast<uint64_t>(m.half));
+	u(static_cast<uint64_t>(m.n)); u(static_cast<uint64_t>(m.maxIter)); d(m.sigma0); d(m.offset); d(m.gain); d(m.crlbMax);
+	d(m.pixelSize); d(m.zMin); d(m.zMax);
+	for (double a : m.astig) { d(a); }
+	u(static_cast<uint64_t>(m.sx)); u(static_cast<uint64_t>(m.sy)); u(static_cast<uint64_t>(m.sz)); d(m.dz);
+	p(m.table); p(m.table64); p(m.fallbacks); p(m.queue); p(m.evals);
+	return k;
+}
+
+Engine::GraphEntry* Engine::FindGraph(int slot, const std::vector<uint64_t>& key)
+{
+	for (auto& e : graphs_[slot]) {
+		if (e.key == key) {
+			e.lastUse = ++graphClock_;
+			return &e;
+		}
+	}
+	return nullptr;
+}
+
+// Captures the compute part of a chunk (launch) on the slot's stream into a graph and keeps its executable (evicting
+// the least recently used of kGraphsPerSlot). Returns false, with no error recorded, when the capture or the
+// instantiation fails; the caller then launches directly.
+Engine::GraphEntry* Engine::CaptureGraph(int slot, std::vector<uint64_t> key, const std::function<bool()>& launch)
+{
+	cudaStream_t st = St(slot);
+	const std::string before = LastError();
+	cudaGraph_t graph = nullptr;
+	cudaGraphExec_t exec = nullptr;
+	const uint64_t l0 = LaunchCount();
+	bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+	if (ok) {
+		const bool launched = launch();
+		ok = cudaStreamEndCapture(st, &graph) == cudaSuccess && launched;
+	}
+	const uint64_t launches = LaunchCount() - l0;
+	ok = ok && cudaGraphInstantiateWithFlags(&exec, graph, 0) == cudaSuccess;
+	if (graph) { cudaGraphDestroy(graph); }
+	if (!ok) {
+		// leave no trace of the failed capture: the chunk is launched directly instead
+		if (exec) { cudaGraphExecDestroy(exec); }
+		cudaGetLastError();
+		ClearError();
+		if (!before.empty()) { SetError(before); }
+		graphsOff_ = true;
+		return nullptr;
+	}
+	auto& list = graphs_[slot];
+	if (list.size() >= kGraphsPerSlot) {
+		auto lru = std::min_element(list.begin(), list.end(), [](const GraphEntry& a, const GraphEntry& b) { return a.lastUse < b.lastUse; });
+		cudaGraphExecDestroy(lru->exec);
+		list.erase(lru);
+	}
+	// the captured launches were counted while recording; the first replay is therefore not counted again
+	list.push_back(GraphEntry{std::move(key), exec, launches, ++graphClock_, true});
+	return &list.back();
+}
+
 // Runs detection -> segmentation -> fits -> ordering for B frames whose pixels are at dImg (device). The chunk's
 // rows go to dOut (device) numbered from Id idBase + 1 and Plane planeBase + 1; returns the row count or -1.
+// The compute part (counters reset through the fits) is replayed from a CUDA graph when an earlier chunk had the same
+// launch chain (the second occurrence of a chain captures it); the ordering step, which follows the other slot's
+// ordering, is launched directly.
 bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, double thr, double ratio, uint32_t maxPoints,
                           const FitParams& fp, double* dOut, bool offsetOut, unsigned long long planeBase, bool afterOther)
 {
@@ -384,26 +469,65 @@ bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, d
 			if (k > 0) { pendLaunches_[k - 1] = LaunchCount() - l0; l0 = LaunchCount(); }
 		}
 	};
-	bool ok = PTB_CUDA(cudaMemsetAsync(ws.cnt, 0, sizeof(Counters), st));
-	ok = ok && PTB_CUDA(cudaMemsetAsync(ws.rootmask, 0, sizeof(uint32_t) * static_cast<size_t>(B) * H * ws.g.words, st));
-	mark(0);
-	ok = ok && LaunchDetect(ws, thr, st);
-	mark(1);
-	ok = ok && LaunchSegment(ws, ratio, strict_, maxPoints, st);
-	ok = ok && LaunchBuildCandidates(ws, st);
-	mark(2);
 	FitParams fpr = fp;
-	if (ok && fp.mode >= kMleGauss && fp.lanes == 0) { ok = Autotune(fpr, dImg, H, W, slot); }
-	if (fp.mode >= kMleGauss) { fpr.mle.queue = ws.cnt->pad; }  // this slot's work-queue counters
-	pendMleProf_ = prof && fp.mode >= kMleGauss;
-	pendLanes_ = fpr.lanes;
+	if (fpr.mode >= kMleGauss) {
+		if (fpr.lanes == 0) { fpr.lanes = TunedLanes(fpr); }
+		fpr.mle.queue = ws.cnt->pad;  // this slot's work-queue counters
+	}
+	const bool tune = fpr.mode >= kMleGauss && fpr.lanes == 0;  // first chunk of this (mode, ROI): time both mappings
+	pendMleProf_ = prof && fpr.mode >= kMleGauss;
+	bool ok = true;
 	if (pendMleProf_) {
 		if (!evalDev_) { ok = ok && PTB_CUDA(cudaMalloc(&evalDev_, 3 * sizeof(unsigned long long))); }
 		ok = ok && PTB_CUDA(cudaMemsetAsync(evalDev_, 0, 3 * sizeof(unsigned long long), st));
 		fpr.marks = mleEv_;
 		fpr.mle.evals = evalDev_;
 	}
-	ok = ok && LaunchFit(dImg, H, W, ws.g.N, ws.cand, &ws.cnt->nfit, 0, ws.capRows, fpr, ws.rows, ws.fitFlag, precision_, st);
+	const uint32_t rowsCap = ws.capRows;
+	auto segmentAndDetect = [&]() {
+		bool k = PTB_CUDA(cudaMemsetAsync(ws.cnt, 0, sizeof(Counters), st));
+		k = k && PTB_CUDA(cudaMemsetAsync(ws.rootmask, 0, sizeof(uint32_t) * static_cast<size_t>(B) * H * ws.g.words, st));
+		mark(0);
+		k = k && LaunchDetect(ws, thr, st);
+		mark(1);
+		k = k && LaunchSegment(ws, ratio, strict_, maxPoints, st);
+		k = k && LaunchBuildCandidates(ws, st);
+		mark(2);
+		return k;
+	};
+	auto fit = [&]() {
+		return LaunchFit(dImg, H, W, ws.g.N, ws.cand, &ws.cnt->nfit, 0, ws.capRows, fpr, ws.rows, ws.fitFlag, precision_, st);
+	};
+	bool direct = true;
+	if (ok && !prof && !tune && !graphsOff_ && useGraphs_) {
+		std::vector<uint64_t> key = ChainKey(slot, ws, dImg, thr, ratio, strict_, maxPoints, rowsCap, precision_, fpr);
+		GraphEntry* g = FindGraph(slot, key);
+		if (!g) {
+			auto seen = std::find(seen_[slot].begin(), seen_[slot].end(), key);
+			if (seen != seen_[slot].end()) {
+				seen_[slot].erase(seen);
+				g = CaptureGraph(slot, std::move(key), [&]() { return segmentAndDetect() && fit(); });
+			}
+			else {
+				if (seen_[slot].size() >= kGraphsPerSlot) { seen_[slot].erase(seen_[slot].begin()); }
+				seen_[slot].push_back(std::move(key));
+			}
+		}
+		if (g) {
+			ok = PTB_CUDA(cudaGraphLaunch(g->exec, st));
+			if (!g->fresh) { CountLaunch(g->launches); }
+			++graphCounts_[g->fresh ? 0 : 1];
+			g->fresh = false;
+			direct = false;
+		}
+	}
+	if (direct) {
+		++graphCounts_[2];
+		ok = ok && segmentAndDetect();
+		if (ok && tune) { ok = Autotune(fpr, dImg, H, W, slot); }
+		ok = ok && fit();
+	}
+	pendLanes_ = fpr.lanes;
 	mark(3);
 	if (afterOther) { ok = ok && PTB_CUDA(cudaStreamWaitEvent(st, sortDone_[1 - slot], 0)); }
 	ok = ok && LaunchSortFrames(ws, dOut, rowBase_, offsetOut, planeBase, st);
@@ -609,6 +733,14 @@ bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slo
 	fp.lanes = bestLanes;
 	tuned_.push_back({fp.mode * 64 + fp.roi, bestLanes});
 	return true;
+}
+
+void Engine::GraphStats(uint64_t* out, int n)
+{
+	for (int k = 0; k < 3 && k < n; ++k) {
+		if (out) { out[k] = graphCounts_[k]; }
+		graphCounts_[k] = 0;
+	}
 }
 
 void Engine::StageTimes(double* ms, uint64_t* launches, int n)

@@ -4,6 +4,7 @@
 #include <atomic>
 #include <cstdint>
 #include <cstdlib>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -54,6 +55,8 @@ public:
 	int SetProfiling(int p) { const int o = profiling_; profiling_ = p; return o; }
 	void StageTimes(double* ms, uint64_t* launches, int n);
 	void MleEvaluations(uint64_t* out, int n);
+	// [chunks captured into graphs, chunks replayed from graphs, chunks launched directly] since the last call.
+	void GraphStats(uint64_t* out, int n);
 	int SetPrecision(int p) { const int o = precision_; precision_ = p; return o; }
 	int Precision() const { return precision_; }
 	cudaStream_t Stream() const { return stream_; }
@@ -82,6 +85,17 @@ private:
 	// afterOther: the chunk orders its rows after the chunk in flight on the other slot (its Ids continue from it).
 	bool EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, double thr, double ratio, uint32_t maxPoints,
 	                  const FitParams& fp, double* dOut, bool offsetOut, unsigned long long planeBase, bool afterOther);
+	// Executable graphs of chunk launch chains, per chunk slot, keyed by every argument the chain's launches take.
+	struct GraphEntry {
+		std::vector<uint64_t> key;
+		cudaGraphExec_t exec;
+		uint64_t launches;  // kernels in the graph
+		uint64_t lastUse;
+		bool fresh;         // captured, not replayed yet (its launches were counted while recording)
+	};
+	static constexpr size_t kGraphsPerSlot = 32;
+	GraphEntry* FindGraph(int slot, const std::vector<uint64_t>& key);
+	GraphEntry* CaptureGraph(int slot, std::vector<uint64_t> key, const std::function<bool()>& launch);
 	// Waits for the slot's chunk; returns its row count or -1 (error recorded).
 	long long CompleteChunk(int slot, uint32_t* truncatedFrames);
 
@@ -92,6 +106,12 @@ private:
 	cudaStream_t stream1_ = nullptr;         // second compute stream (second chunk slot)
 	cudaEvent_t sortDone_[2] = {};           // per chunk slot: its rows are ordered (Ids of the next chunk follow)
 	cudaEvent_t fork_ = nullptr;              // start of a two-slot call on the first compute stream
+	std::vector<GraphEntry> graphs_[2];
+	std::vector<std::vector<uint64_t>> seen_[2];  // chains launched once directly (the next occurrence is captured)
+	uint64_t graphClock_ = 0;
+	uint64_t graphCounts_[3] = {};            // captured, replayed, direct
+	bool useGraphs_ = true;                   // PTB_GRAPHS=0 launches every chunk directly
+	bool graphsOff_ = false;                  // a capture failed: direct launches from then on
 	Workspace ws1_{};                        // second chunk slot's workspace and pool
 	void* pool1_ = nullptr;
 	size_t pool1Bytes_ = 0;

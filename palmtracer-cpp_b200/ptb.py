@@ -15,7 +15,7 @@ COLS = 18
 # every symbol the public header declares
 EXPORTS = ["Localization", "Fitting", "Wavelett", "AutoThreshold", "Astigmatism3DEstimation", "PTB_LocalizationDevice",
            "PTB_SetSegmentationMode", "PTB_SetFitPrecision", "PTB_LastError", "PTB_KernelLaunchCount",
-           "PTB_SetProfiling", "PTB_StageTimes", "PTB_MleEvaluations", "PTB_MeasureFmaPeak", "PTB_FittingDeviceNoAlloc",
+           "PTB_SetProfiling", "PTB_StageTimes", "PTB_MleEvaluations", "PTB_GraphStats", "PTB_MeasureFmaPeak", "PTB_FittingDeviceNoAlloc",
            "PTB_ServerStart", "PTB_SubmitStack", "PTB_PollStack", "PTB_StackResult", "PTB_ServerStop"]
 
 _u16p = ctypes.POINTER(ctypes.c_uint16)
@@ -61,6 +61,8 @@ def load(path=LIB_PATH):
     L.PTB_StageTimes.argtypes = [_f64p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
     L.PTB_MleEvaluations.restype = None
     L.PTB_MleEvaluations.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
+    L.PTB_GraphStats.restype = None
+    L.PTB_GraphStats.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
     L.PTB_FittingDeviceNoAlloc.restype = _u64
     L.PTB_FittingDeviceNoAlloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _u64, ctypes.c_void_p, _u64, _u64, _u64, _u64,
                                            _f64p, ctypes.c_void_p]
@@ -197,6 +199,14 @@ def mle_evaluations():
     out = np.zeros(4, dtype=np.uint64)
     load().PTB_MleEvaluations(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 4)
     return {"lm": int(out[0]), "polish": int(out[1]), "fp64": int(out[2]), "fp64_cholesky": int(out[3])}
+
+
+def graph_stats():
+    """{"captured", "replayed", "direct"}: chunks of this device's engine captured into launch-chain graphs, replayed
+    from them and launched directly, since the last call."""
+    out = np.zeros(3, dtype=np.uint64)
+    load().PTB_GraphStats(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 3)
+    return {"captured": int(out[0]), "replayed": int(out[1]), "direct": int(out[2])}
 
 
 def fma_peak(fp64):
