@@ -216,13 +216,17 @@ def serving_run(ptb, torch, n_req, seed=2026):
             break
     plain_s = time.perf_counter() - t_start
     frames_total = int(lengths.sum())
+    # pixels copied host -> device for the whole mix: with the GPU faster than the link, this is what bounds it
+    in_bytes = int((lengths.astype(np.int64) * sizes.astype(np.int64) ** 2 * 2).sum())
     return {
         "workload": "C5: %d stacks, Poisson arrivals at %.0f stacks/s, square frames of %s px, 1-500 frames (%d in all), "
                     "half 2D Gaussian (MLE mode 6, 7x7), half astigmatic 3D (MLE mode 7, 11x11); %d server slots"
                     % (n_req, SERVE_RATE, "/".join(str(s) for s in SERVE_SIZES), frames_total, SERVE_SLOTS),
+        "input_bytes": in_bytes,
         "poisson": {"localizations_per_s": rows / poisson_s, "frames_per_s": frames_total / poisson_s, "seconds": poisson_s,
                     "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))}},
         "saturated": {"localizations_per_s": rows_sat / sat_s, "frames_per_s": frames_total / sat_s, "seconds": sat_s,
+                      "h2d_gbs": in_bytes / sat_s / 1e9,
                       "latency_ms": {"p50": float(np.percentile(lat_sat, 50)), "p99": float(np.percentile(lat_sat, 99))}},
         "plain_per_frame": {"localizations_per_s": plain_rows / plain_s, "frames_per_s": plain_frames / plain_s,
                             "sample_frames": plain_frames,
@@ -393,6 +397,22 @@ def main():
         if i >= max(1, args.warmup // 2):
             e2e_ms.append((time.perf_counter() - t0) * 1000.0)
     e2e_value = (n_e2e // 18) * len(e2e_ms) / (sum(e2e_ms) / 1000.0) if e2e_ms else None
+    # the link's own host -> device rate from pinned memory (one 1 GiB copy of the same buffer, best of 3): the
+    # roofline of the e2e number
+    link_gbs = None
+    if e2e_ms:
+        part = host_in.view(-1)[: min(host_in.numel(), 1 << 29)]
+        dev = torch.empty_like(part, device="cuda")
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = 1e30
+        for _ in range(3):
+            ev0.record()
+            dev.copy_(part, non_blocking=True)
+            ev1.record()
+            ev1.synchronize()
+            best = min(best, ev0.elapsed_time(ev1))
+        link_gbs = part.numel() * 2 / (best / 1000.0) / 1e9
+        del dev
 
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
@@ -419,7 +439,10 @@ def main():
                 "localizations_per_step": int(rows_all), "roofline": roofline, "detect_roofline": detect_roofline,
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_bytes,
-                        "d2h_bytes_per_step": int(n_e2e * 8), "ms_per_step": float(np.mean(e2e_ms)) if e2e_ms else None},
+                        "d2h_bytes_per_step": int(n_e2e * 8), "ms_per_step": float(np.mean(e2e_ms)) if e2e_ms else None,
+                        # host -> device rate over the call (the frames cross PCIe once; the link is the e2e bound)
+                        "h2d_gbs": h2d_bytes / (float(np.mean(e2e_ms)) / 1000.0) / 1e9 if e2e_ms else None,
+                        "h2d_link_gbs": link_gbs},
                 "gpu_launches": int(launches), "clocks": clk, "serving": serving}
         print(json.dumps(line), flush=True)
     if world > 1:

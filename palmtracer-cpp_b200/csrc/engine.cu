@@ -372,6 +372,19 @@ void Engine::ChunkPlan(int H, int W, uint64_t planes, uint32_t maxPoints, int& B
 	}
 }
 
+// Size class of a chunk for the fit autotuner: the bit length of its pixel count. Which ROI mapping is faster depends
+// on how many ROIs one launch fits (a warp per ROI finishes a small batch sooner; a thread per ROI has the higher
+// throughput once the batch fills the GPU many times over), and the candidate count grows with the pixel count.
+static int SizeClass(int B, int H, int W)
+{
+	uint64_t p = static_cast<uint64_t>(B) * static_cast<uint64_t>(H) * static_cast<uint64_t>(W);
+	int c = 0;
+	while (p) { ++c; p >>= 1; }
+	return c;
+}
+
+static int TuneKey(const FitParams& fp, int sizeClass) { return (fp.mode * 64 + fp.roi) * 64 + sizeClass; }
+
 // Key of a chunk's launch chain: every value that the captured launches take by value (workspace plan, image
 // pointer, threshold, segmentation settings, fit configuration). Two chunks with equal keys launch identical kernels
 // with identical arguments, so a graph captured for one replays the other.
@@ -471,7 +484,7 @@ bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, d
 	};
 	FitParams fpr = fp;
 	if (fpr.mode >= kMleGauss) {
-		if (fpr.lanes == 0) { fpr.lanes = TunedLanes(fpr); }
+		if (fpr.lanes == 0) { fpr.lanes = TunedLanes(fpr, SizeClass(B, H, W)); }
 		fpr.mle.queue = ws.cnt->pad;  // this slot's work-queue counters
 	}
 	const bool tune = fpr.mode >= kMleGauss && fpr.lanes == 0;  // first chunk of this (mode, ROI): time both mappings
@@ -524,7 +537,7 @@ bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, d
 	if (direct) {
 		++graphCounts_[2];
 		ok = ok && segmentAndDetect();
-		if (ok && tune) { ok = Autotune(fpr, dImg, H, W, slot); }
+		if (ok && tune) { ok = Autotune(fpr, dImg, H, W, slot, SizeClass(B, H, W)); }
 		ok = ok && fit();
 	}
 	pendLanes_ = fpr.lanes;
@@ -693,19 +706,19 @@ int EnvLanes()
 	return env ? std::atoi(env) : 0;
 }
 
-int Engine::TunedLanes(const FitParams& fp) const
+int Engine::TunedLanes(const FitParams& fp, int sizeClass) const
 {
 	if (const int env = EnvLanes()) { return env; }
-	const int key = fp.mode * 64 + fp.roi;
+	const int key = TuneKey(fp, sizeClass);
 	for (const auto& kv : tuned_) {
 		if (kv.first == key) { return kv.second; }
 	}
-	return 0;  // not tuned yet: the first chunk with candidates tunes it
+	return 0;  // not tuned yet: the first chunk of this class with candidates tunes it
 }
 
 // Times both ROI mappings (1: thread per ROI, 32: warp per ROI) on this chunk's candidates and keeps the faster for
-// (mode, ROI).
-bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slot)
+// (mode, ROI, chunk size class).
+bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slot, int sizeClass)
 {
 	Workspace& ws = Ws(slot);
 	cudaStream_t st = St(slot);
@@ -731,7 +744,7 @@ bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slo
 	cudaEventDestroy(a);
 	cudaEventDestroy(b);
 	fp.lanes = bestLanes;
-	tuned_.push_back({fp.mode * 64 + fp.roi, bestLanes});
+	tuned_.push_back({TuneKey(fp, sizeClass), bestLanes});
 	return true;
 }
 
@@ -777,7 +790,7 @@ bool Engine::UploadSpline(FitParams& fp, const std::vector<double>& spline)
 		if (!fallbacks_ && !PTB_CUDA(cudaMalloc(&fallbacks_, 4 * sizeof(unsigned int)))) { return false; }
 		fp.mle.fallbacks = static_cast<unsigned int*>(fallbacks_);
 		fp.mle.queue = static_cast<unsigned int*>(fallbacks_) + 1;
-		fp.lanes = TunedLanes(fp);
+		fp.lanes = EnvLanes();  // 0: chosen per chunk by the autotuner
 	}
 	if (fp.mode == kMleSpline) {
 		// cell-major copies of the [64][cell] table: FP64 first, then FP32
@@ -870,6 +883,8 @@ long long Engine::FitPositions(const uint16_t* input, const double* positions, u
 	ok = ok && PTB_CUDA(cudaMallocAsync(&dRows, sizeof(double) * kCols * nPoints, stream_));
 	ok = ok && PTB_CUDA(cudaMallocAsync(&dFlag, nPoints, stream_));
 	ok = ok && PTB_CUDA(cudaMemcpyAsync(dCand, cands.data(), sizeof(Cand) * nPoints, cudaMemcpyHostToDevice, stream_));
+	// modes 6-8: a warp per ROI while the points fill the GPU a few times at most (shortest call), else a thread per ROI
+	if (fp.mode >= kMleGauss && fp.lanes == 0) { fp.lanes = nPoints <= 148ull * 64 ? 32 : 1; }
 	ok = ok && LaunchFit(static_cast<const uint16_t*>(img_), static_cast<int>(height), static_cast<int>(width),
 	                     static_cast<long long>(N), dCand, nullptr, static_cast<uint32_t>(nPoints), static_cast<uint32_t>(nPoints),
 	                     fp, dRows, dFlag, precision_, stream_);

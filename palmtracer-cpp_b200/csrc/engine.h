@@ -73,8 +73,8 @@ private:
 	bool Reserve(int H, int W, int B, uint32_t rowsCap, int slots);
 	bool ReserveImage(size_t bytes);
 	bool UploadSpline(FitParams& fp, const std::vector<double>& spline);
-	int TunedLanes(const FitParams& fp) const;
-	bool Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slot);
+	int TunedLanes(const FitParams& fp, int sizeClass) const;
+	bool Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slot, int sizeClass);
 	int ChunkFrames(int H, int W, uint64_t planes, uint32_t maxPoints, size_t budget) const;
 	// Chunk size and number of concurrent chunk slots (2 when the stack needs more than one chunk).
 	void ChunkPlan(int H, int W, uint64_t planes, uint32_t maxPoints, int& B, int& slots) const;
@@ -126,7 +126,7 @@ private:
 	size_t imgBytes_ = 0;
 	void* spline_ = nullptr;
 	void* fallbacks_ = nullptr;
-	std::vector<std::pair<int, int>> tuned_;  // (mode * 64 + roi) -> lanes per ROI
+	std::vector<std::pair<int, int>> tuned_;  // ((mode * 64 + roi) * 64 + chunk size class) -> lanes per ROI
 	size_t splineBytes_ = 0;
 	Workspace ws_{};
 	int strict_ = 0;
