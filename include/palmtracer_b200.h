@@ -65,6 +65,20 @@ PTB_API void Astigmatism3DEstimation(const double* input, double* output, uint64
 
 /* ---- Additions (no counterpart in the reference) ---------------------------------------------------------------- */
 
+/* TIFF stacks (the reference's test-harness loader, Tests_CPU/TiffManagement.hpp:8-55, reads them with libtiff).
+ * Multi-page, 16 bits and one sample per pixel, uncompressed strips, classic TIFF or BigTIFF in either byte order;
+ * every page must have the first page's size (the reference's two checks). Host-only: no CUDA call.
+ * PTB_TiffInfo: 1 and the stack's width, height and page count, or 0 (error in PTB_LastError()).
+ * PTB_TiffRead: pages [first, first + count) into output ([count][height][width], host byte order); returns count,
+ * or 0 on error. */
+PTB_API int PTB_TiffInfo(const char* path, uint64_t* width, uint64_t* height, uint64_t* planes);
+PTB_API uint64_t PTB_TiffRead(const char* path, uint16_t* output, uint64_t first, uint64_t count);
+
+/* Localization of a TIFF stack on disk: same output, return value and parameters as Localization over the file's
+ * pages. Chunk k + 1 is read from the file into pinned staging while chunk k computes on the GPU. */
+PTB_API uint64_t PTB_LocalizationTiff(const char* path, double* output, uint64_t outputSize, double thresholdVal,
+                                      double watershedRatio, uint64_t fit, const double* fit_params);
+
 /* Same contract as Localization, but d_input and d_output are DEVICE memory of the current CUDA device (fit_params
  * stays a host array) and the work is ordered after the caller's `stream` (a cudaStream_t; 0 = legacy default
  * stream), which in turn waits for it. Blocks until the row count is known. Used when frames are already resident

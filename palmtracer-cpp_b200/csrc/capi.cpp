@@ -8,6 +8,7 @@
 
 #include "../../include/palmtracer_b200.h"
 #include "engine.h"
+#include "tiff.h"
 
 namespace {
 
@@ -103,6 +104,61 @@ PTB_API void Astigmatism3DEstimation(const double* input, double* output, uint64
 	catch (const std::exception& ex) {
 		ptb::SetError(ex.what());
 		Report("Astigmatism3DEstimation");
+	}
+}
+
+PTB_API int PTB_TiffInfo(const char* path, uint64_t* width, uint64_t* height, uint64_t* planes)
+{
+	ptb::ClearError();
+	try {
+		ptb::TiffStack t;
+		if (!t.Open(path)) { Report("PTB_TiffInfo"); return 0; }
+		if (width) { *width = t.Width(); }
+		if (height) { *height = t.Height(); }
+		if (planes) { *planes = t.Planes(); }
+		return 1;
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("PTB_TiffInfo");
+		return 0;
+	}
+}
+
+PTB_API uint64_t PTB_TiffRead(const char* path, uint16_t* output, uint64_t first, uint64_t count)
+{
+	ptb::ClearError();
+	try {
+		ptb::TiffStack t;
+		if (!t.Open(path) || !t.Read(first, count, output)) { Report("PTB_TiffRead"); return 0; }
+		return count;
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("PTB_TiffRead");
+		return 0;
+	}
+}
+
+PTB_API uint64_t PTB_LocalizationTiff(const char* path, double* output, uint64_t outputSize, double thresholdVal,
+                                      double watershedRatio, uint64_t fit, const double* fit_params)
+{
+	ptb::ClearError();
+	try {
+		ptb::TiffStack t;
+		if (!t.Open(path)) { Report("PTB_LocalizationTiff"); return 0; }
+		const ptb::Engine::PageSource source = [&t](uint64_t first, uint64_t count, uint16_t* dst) { return t.Read(first, count, dst); };
+		std::unique_lock<std::mutex> lock;
+		ptb::Engine& e = ptb::EngineFor(lock);
+		const long long n = e.Localize(nullptr, false, output, false, outputSize, t.Height(), t.Width(), t.Planes(), thresholdVal,
+		                               watershedRatio, fit, fit_params, &source);
+		if (n < 0) { Report("PTB_LocalizationTiff"); return 0; }
+		return static_cast<uint64_t>(n);
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("PTB_LocalizationTiff");
+		return 0;
 	}
 }
 

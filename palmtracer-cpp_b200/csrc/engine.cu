@@ -254,6 +254,7 @@ Engine::~Engine()
 	}
 	if (pool_) { cudaFree(pool_); }
 	if (img_) { cudaFree(img_); }
+	if (hostStage_) { cudaFreeHost(hostStage_); }
 	if (spline_) { cudaFree(spline_); }
 	if (fallbacks_) { cudaFree(fallbacks_); }
 	if (evalDev_) { cudaFree(evalDev_); }
@@ -591,8 +592,12 @@ long long Engine::CompleteChunk(int slot, uint32_t* truncatedFrames)
 // the previous chunk's, so the host waits for a chunk only to learn how many rows it copies out.
 long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* output, bool outputOnDevice, uint64_t outputSize,
                            uint64_t height, uint64_t width, uint64_t planes, double thr, double ratio, uint64_t fit,
-                           const double* fitParams)
+                           const double* fitParams, const PageSource* source)
 {
+	if (source && (inputOnDevice || outputOnDevice)) {
+		SetError("a page source takes host output");
+		return -1;
+	}
 	if (planes == 0 || height == 0 || width == 0) { return 0; }
 	const uint64_t perPlane = (outputSize / kCols) / planes;
 	if (perPlane == 0) { return 0; }
@@ -630,6 +635,11 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 	const uint64_t chunks = first.size();
 	const size_t slotBytes = N * B * sizeof(uint16_t);
 	if (!inputOnDevice && !ReserveImage((chunks > 1 ? 2 : 1) * slotBytes)) { return -1; }
+	if (source && hostStageBytes_ < (chunks > 1 ? 2 : 1) * slotBytes) {
+		if (hostStage_) { cudaFreeHost(hostStage_); hostStage_ = nullptr; hostStageBytes_ = 0; }
+		if (!PTB_CUDA(cudaMallocHost(&hostStage_, (chunks > 1 ? 2 : 1) * slotBytes))) { return -1; }
+		hostStageBytes_ = (chunks > 1 ? 2 : 1) * slotBytes;
+	}
 	// with two chunk slots, chunk k runs on slot k % 2 (its own stream and workspace); with host output its ordered
 	// rows stay in that workspace (where the chunk's own plan puts them) until copied out
 	double* outSlot[2] = {nullptr, nullptr};
@@ -643,8 +653,19 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 	// input of chunk k into its slot; the slot's previous chunk (k - 2) must have finished reading it
 	auto copyIn = [&](uint64_t k) {
 		const int slot = static_cast<int>(k & 1);
+		const uint16_t* src = source ? nullptr : input + first[k] * N;
+		if (source) {
+			// the pinned slot's previous frames (chunk k - 2) must have reached the device before it is refilled
+			uint16_t* stage = static_cast<uint16_t*>(hostStage_) + (slot ? N * B : 0);
+			if (k >= 2 && !PTB_CUDA(cudaEventSynchronize(h2d_[slot]))) { return false; }
+			if (!(*source)(first[k], count[k], stage)) {
+				SetError("page source failed");
+				return false;
+			}
+			src = stage;
+		}
 		if (k >= 2 && !PTB_CUDA(cudaStreamWaitEvent(copy_, done_[slot], 0))) { return false; }
-		if (!PTB_CUDA(cudaMemcpyAsync(imgSlot(slot), input + first[k] * N, N * framesOf(k) * sizeof(uint16_t), cudaMemcpyHostToDevice, copy_))) {
+		if (!PTB_CUDA(cudaMemcpyAsync(imgSlot(slot), src, N * framesOf(k) * sizeof(uint16_t), cudaMemcpyHostToDevice, copy_))) {
 			return false;
 		}
 		return PTB_CUDA(cudaEventRecord(h2d_[slot], copy_));

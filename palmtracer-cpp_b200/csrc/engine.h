@@ -40,10 +40,14 @@ public:
 	Engine(const Engine&) = delete;
 	Engine& operator=(const Engine&) = delete;
 
-	// Localization over host or device buffers; returns doubles written or -1 (error recorded).
+	// Fills frames [first, first + count) of the stack into a host buffer ([count][height][width]); false on error.
+	using PageSource = std::function<bool(uint64_t first, uint64_t count, uint16_t* dst)>;
+	// Localization over host or device buffers; returns doubles written or -1 (error recorded). With a page source
+	// (input null, host output), each chunk's frames are produced into pinned staging on the host while the previous
+	// chunk computes.
 	long long Localize(const uint16_t* input, bool inputOnDevice, double* output, bool outputOnDevice, uint64_t outputSize,
 	                   uint64_t height, uint64_t width, uint64_t planes, double thr, double ratio, uint64_t fit,
-	                   const double* fitParams);
+	                   const double* fitParams, const PageSource* source = nullptr);
 	long long FitPositions(const uint16_t* input, const double* positions, uint64_t nPoints, double* output, uint64_t height,
 	                       uint64_t width, uint64_t planes, uint64_t fit, const double* fitParams);
 	bool Planes(const uint16_t* input, double* output, uint64_t height, uint64_t width, uint64_t planes, int level);
@@ -124,6 +128,8 @@ private:
 	size_t poolBytes_ = 0;
 	void* img_ = nullptr;
 	size_t imgBytes_ = 0;
+	void* hostStage_ = nullptr;               // pinned frame staging of page sources (two slots)
+	size_t hostStageBytes_ = 0;
 	void* spline_ = nullptr;
 	void* fallbacks_ = nullptr;
 	std::vector<std::pair<int, int>> tuned_;  // ((mode * 64 + roi) * 64 + chunk size class) -> lanes per ROI

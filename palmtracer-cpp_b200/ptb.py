@@ -16,7 +16,8 @@ COLS = 18
 EXPORTS = ["Localization", "Fitting", "Wavelett", "AutoThreshold", "Astigmatism3DEstimation", "PTB_LocalizationDevice",
            "PTB_SetSegmentationMode", "PTB_SetFitPrecision", "PTB_LastError", "PTB_KernelLaunchCount",
            "PTB_SetProfiling", "PTB_StageTimes", "PTB_MleEvaluations", "PTB_GraphStats", "PTB_MeasureFmaPeak", "PTB_FittingDeviceNoAlloc",
-           "PTB_ServerStart", "PTB_SubmitStack", "PTB_PollStack", "PTB_StackResult", "PTB_ServerStop"]
+           "PTB_ServerStart", "PTB_SubmitStack", "PTB_PollStack", "PTB_StackResult", "PTB_ServerStop",
+           "PTB_TiffInfo", "PTB_TiffRead", "PTB_LocalizationTiff"]
 
 _u16p = ctypes.POINTER(ctypes.c_uint16)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -61,6 +62,12 @@ def load(path=LIB_PATH):
     L.PTB_StageTimes.argtypes = [_f64p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
     L.PTB_MleEvaluations.restype = None
     L.PTB_MleEvaluations.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
+    L.PTB_TiffInfo.restype = ctypes.c_int
+    L.PTB_TiffInfo.argtypes = [ctypes.c_char_p, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u64)]
+    L.PTB_TiffRead.restype = _u64
+    L.PTB_TiffRead.argtypes = [ctypes.c_char_p, _u16p, _u64, _u64]
+    L.PTB_LocalizationTiff.restype = _u64
+    L.PTB_LocalizationTiff.argtypes = [ctypes.c_char_p, _f64p, _u64, _f64, _f64, _u64, _f64p]
     L.PTB_GraphStats.restype = None
     L.PTB_GraphStats.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
     L.PTB_FittingDeviceNoAlloc.restype = _u64
@@ -199,6 +206,43 @@ def mle_evaluations():
     out = np.zeros(4, dtype=np.uint64)
     load().PTB_MleEvaluations(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 4)
     return {"lm": int(out[0]), "polish": int(out[1]), "fp64": int(out[2]), "fp64_cholesky": int(out[3])}
+
+
+def tiff_info(path):
+    """(width, height, planes) of a 16-bit TIFF stack; RuntimeError on an unreadable or unsupported file."""
+    w, h, z = _u64(), _u64(), _u64()
+    if not load().PTB_TiffInfo(os.fsencode(path), ctypes.byref(w), ctypes.byref(h), ctypes.byref(z)):
+        raise RuntimeError("PTB_TiffInfo failed: " + last_error())
+    return w.value, h.value, z.value
+
+
+def tiff_read(path, first=0, count=None):
+    """Pages [first, first + count) of a TIFF stack as a uint16 [count, height, width] array."""
+    w, h, z = tiff_info(path)
+    if count is None:
+        count = z - first
+    out = np.empty((count, h, w), dtype=np.uint16)
+    if count and load().PTB_TiffRead(os.fsencode(path), out.ctypes.data_as(_u16p), first, count) != count:
+        raise RuntimeError("PTB_TiffRead failed: " + last_error())
+    return out
+
+
+def localization_tiff(path, thr, ratio, fit, params, capacity_doubles=None, out=None):
+    """Localization of a TIFF stack on disk; returns the [n, 18] float64 rows (a view of ``out`` when given: a
+    caller-owned float64 buffer, ideally pinned, whose size is the capacity)."""
+    if out is not None:
+        capacity_doubles = out.size
+    else:
+        w, h, z = tiff_info(path)
+        if capacity_doubles is None:
+            capacity_doubles = ((h * w) // 5 + 1) * z * COLS
+        out = np.full(max(capacity_doubles, 1), -12345.0)
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    n = load().PTB_LocalizationTiff(os.fsencode(path), out.ctypes.data_as(_f64p), capacity_doubles, thr, ratio, fit,
+                                    params.ctypes.data_as(_f64p))
+    if n == 0 and last_error():
+        raise RuntimeError("PTB_LocalizationTiff failed: " + last_error())
+    return out[:n].reshape(-1, COLS)
 
 
 def graph_stats():
