@@ -63,7 +63,18 @@ PTB_API double AutoThreshold(const uint16_t* input, uint64_t height, uint64_t wi
 PTB_API void Astigmatism3DEstimation(const double* input, double* output, uint64_t size, double pixelSize, const double* model,
                                      double zMax);
 
+/* Replaces Tracking (CPU/main.cpp:159-164 -> lib/tracking/Tracks.cpp:69-212): links localizations of consecutive
+ * planes greedily by increasing squared distance (pairs with dx^2 + dy^2 <= maxDistance^2, ties by source then target
+ * in point order), then numbers the tracks 1, 2, ... from their first point. input [nPoints][4] = (Id, Plane, X, Y),
+ * any order; output [nPoints][2] = (Id, Track) in (Plane, Id) order. Same results as the reference for distinct
+ * (Plane, Id) pairs (equal pairs keep their input order). Writes nothing for nPoints = 0. */
+PTB_API void Tracking(const double* input, uint64_t* output, uint64_t nPoints, double maxDistance);
+
 /* ---- Additions (no counterpart in the reference) ---------------------------------------------------------------- */
+
+/* Tracking on DEVICE buffers of the current CUDA device, ordered on `stream` (a cudaStream_t; the call synchronizes
+ * it, since the plane range and the pair count size its scratch). Returns 2 * nPoints, or 0 on error. */
+PTB_API uint64_t PTB_TrackingDevice(const double* d_input, uint64_t* d_output, uint64_t nPoints, double maxDistance, void* stream);
 
 /* TIFF stacks (the reference's test-harness loader, Tests_CPU/TiffManagement.hpp:8-55, reads them with libtiff).
  * Multi-page, 16 bits and one sample per pixel, uncompressed strips, classic TIFF or BigTIFF in either byte order;

@@ -25,10 +25,11 @@ SRCS=(
 	"$REF/lib/fit/SplineFit.cpp"
 	"$REF/lib/fit/AstigFit.cpp"
 	"$REF/lib/signal_processing/Matrix.cpp"
+	"$REF/lib/tracking/Tracks.cpp"
 	"$HERE/ref_shim.cpp"
 )
 g++ -std=c++20 -O2 -fopenmp -ffp-contract=off -fPIC -shared \
-	-I"$REF/lib" -I"$REF/lib/localization" -I"$REF/lib/fit" -I"$REF/lib/signal_processing" \
+	-I"$REF/lib" -I"$REF/lib/localization" -I"$REF/lib/fit" -I"$REF/lib/signal_processing" -I"$REF/lib/tracking" \
 	"${SRCS[@]}" -o "$OUT/libptref.so.tmp"
 mv "$OUT/libptref.so.tmp" "$OUT/libptref.so"
 echo "built $OUT/libptref.so"

@@ -73,6 +73,17 @@ class CpuLib:
         f(_ptr(sigmas, _f64p), _ptr(out, _f64p), sigmas.shape[0], pixel_size, _ptr(model, _f64p), zmax)
         return out
 
+    def tracking(self, points, max_distance):
+        """Tracking: points [n, 4] (Id, Plane, X, Y) -> [n, 2] uint64 (Id, Track) in (Plane, Id) order."""
+        f = getattr(self.lib, self.prefix + "Tracking")
+        f.restype = _u64
+        f.argtypes = [_f64p, ctypes.POINTER(ctypes.c_uint64), _u64, _f64]
+        points = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 4)
+        out = np.zeros((points.shape[0], 2), dtype=np.uint64)
+        if points.shape[0]:
+            f(_ptr(points, _f64p), out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), points.shape[0], max_distance)
+        return out
+
     def set_threads(self, n):
         self._threads(int(n))
 

@@ -12,6 +12,7 @@
 //   orc_Localization / orc_Fitting / orc_Wavelett / orc_AutoThreshold  - the four C-ABI exports
 //   orc_Planes, orc_Candidates, orc_CandidatesFromPotential, orc_Labels - per-stage products
 //   orc_Astig3DEstimation - z from (sigma_x, sigma_y) with the astigmatism model (the reference's export of that name)
+//   orc_Tracking          - frame-to-frame linking (the reference's export of that name)
 #include <omp.h>
 
 #include <algorithm>
@@ -1736,6 +1737,79 @@ int orc_MleFitOne(const uint16_t* frame, uint64_t height, uint64_t width, double
 	MleRoi R;
 	if (!MleRoiAt(c, frame, static_cast<int>(width), static_cast<int>(height), cx, cy, R)) { return 0; }
 	return MleFit(R, theta, crlb, *dev) ? 1 : 2;
+}
+
+// Frame-to-frame linking (Tracks::Tracking, lib/tracking/Tracks.cpp:69-212, exported as Tracking, CPU/main.cpp:159-164).
+// Points (Id, Plane, X, Y) ordered by (Plane, Id) (:80-98; equal pairs by input position here, unspecified there);
+// for every two consecutive planes that both hold points, the pairs with (xa - xb)^2 + (ya - yb)^2 <= maxDistance^2
+// (:131-145) in increasing (d2, source, target) order link when the source has no successor and the target no
+// predecessor yet (:148-186); track numbers 1, 2, ... go to the chain heads in point order and along their chains
+// (:188-199). output [n][2] = (Id, Track) in point order; returns 2 n.
+uint64_t orc_Tracking(const double* input, uint64_t* output, uint64_t nPoints, double maxDistance)
+{
+	if (nPoints == 0) { return 0; }
+	struct Pt {
+		size_t plane, id, src;
+		double x, y;
+	};
+	std::vector<Pt> pts(nPoints);
+	for (size_t i = 0; i < nPoints; ++i) {
+		const double* r = input + 4 * i;
+		pts[i] = {static_cast<size_t>(r[1]), static_cast<size_t>(r[0]), i, r[2], r[3]};
+	}
+	std::sort(pts.begin(), pts.end(), [](const Pt& a, const Pt& b) {
+		if (a.plane != b.plane) { return a.plane < b.plane; }
+		if (a.id != b.id) { return a.id < b.id; }
+		return a.src < b.src;
+	});
+	constexpr size_t kNone = std::numeric_limits<size_t>::max();
+	std::vector<size_t> succ(nPoints, kNone), pred(nPoints, kNone), track(nPoints, 0);
+	const double r2 = maxDistance * maxDistance;
+	struct Link {
+		double d2;
+		size_t from, to;
+	};
+	std::vector<Link> links;
+	// runs of equal planes: [a, b) is plane q, [b, c) the next run
+	for (size_t a = 0; a < nPoints;) {
+		size_t b = a;
+		while (b < nPoints && pts[b].plane == pts[a].plane) { ++b; }
+		size_t c = b;
+		while (c < nPoints && pts[c].plane == pts[b < nPoints ? b : a].plane) { ++c; }
+		if (b < nPoints && pts[b].plane == pts[a].plane + 1) {
+			links.clear();
+			for (size_t i = a; i < b; ++i) {
+				for (size_t j = b; j < c; ++j) {
+					const double dx = pts[i].x - pts[j].x, dy = pts[i].y - pts[j].y;
+					const double d2 = (dx * dx) + (dy * dy);
+					if (d2 <= r2) { links.push_back({d2, i, j}); }
+				}
+			}
+			std::sort(links.begin(), links.end(), [](const Link& u, const Link& v) {
+				if (u.d2 != v.d2) { return u.d2 < v.d2; }
+				if (u.from != v.from) { return u.from < v.from; }
+				return u.to < v.to;
+			});
+			for (const Link& l : links) {
+				if (succ[l.from] == kNone && pred[l.to] == kNone) {
+					succ[l.from] = l.to;
+					pred[l.to] = l.from;
+				}
+			}
+		}
+		a = b;
+	}
+	size_t next = 1;
+	for (size_t k = 0; k < nPoints; ++k) {
+		if (pred[k] != kNone) { continue; }
+		for (size_t m = k; m != kNone; m = succ[m]) { track[m] = next; }
+		++next;
+	}
+	for (size_t k = 0; k < nPoints; ++k) {
+		output[2 * k] = pts[k].id;
+		output[2 * k + 1] = track[k];
+	}
+	return 2 * nPoints;
 }
 
 }  // extern "C"

@@ -9,7 +9,7 @@
 //   ref_Fitting       -> CPU/main.cpp:141-148 (Fitting)
 //   ref_Wavelett      -> CPU/main.cpp:257-284 (Wavelett)
 //   ref_AutoThreshold -> CPU/main.cpp:75-85   (AutoThreshold)
-// ref_Astig3DEstimation mirrors CPU/main.cpp:324-353. The remaining entry points expose intermediate
+// ref_Astig3DEstimation mirrors CPU/main.cpp:324-353, ref_Tracking CPU/main.cpp:159-164 (Tracking). The remaining entry points expose intermediate
 // products (wavelet planes, segmentation candidates, label map) for bitwise checks of each stage.
 #include <omp.h>
 
@@ -23,6 +23,7 @@
 #include "fit/AstigFit.hpp"
 #include "localization/ATrous.hpp"
 #include "localization/Segmentation2D.hpp"
+#include "tracking/Tracks.hpp"
 
 namespace pt = palm_tracer;
 
@@ -134,5 +135,10 @@ void ref_Astig3DEstimation(const double* input, double* output, uint64_t size, d
 		output[2 * i]     = res[i].x;
 		output[2 * i + 1] = res[i].y;
 	}
+}
+
+uint64_t ref_Tracking(const double* input, uint64_t* output, uint64_t nPoints, double maxDistance)
+{
+	return pt::tracking::Tracks::Tracking(input, output, nPoints, maxDistance);
 }
 }

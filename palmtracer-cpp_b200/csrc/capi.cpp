@@ -107,6 +107,39 @@ PTB_API void Astigmatism3DEstimation(const double* input, double* output, uint64
 	}
 }
 
+PTB_API void Tracking(const double* input, uint64_t* output, uint64_t nPoints, double maxDistance)
+{
+	ptb::ClearError();
+	try {
+		std::unique_lock<std::mutex> lock;
+		if (!ptb::EngineFor(lock).Track(input, output, nPoints, maxDistance)) { Report("Tracking"); }
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("Tracking");
+	}
+}
+
+PTB_API uint64_t PTB_TrackingDevice(const double* d_input, uint64_t* d_output, uint64_t nPoints, double maxDistance, void* stream)
+{
+	ptb::ClearError();
+	try {
+		std::unique_lock<std::mutex> lock;
+		ptb::Engine& e = ptb::EngineFor(lock);
+		if (!e.Init()) { Report("PTB_TrackingDevice"); return 0; }
+		if (!ptb::TrackDevice(d_input, d_output, nPoints, maxDistance, static_cast<cudaStream_t>(stream))) {
+			Report("PTB_TrackingDevice");
+			return 0;
+		}
+		return 2 * nPoints;
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("PTB_TrackingDevice");
+		return 0;
+	}
+}
+
 PTB_API int PTB_TiffInfo(const char* path, uint64_t* width, uint64_t* height, uint64_t* planes)
 {
 	ptb::ClearError();

@@ -25,6 +25,7 @@ bool LaunchSortFrames(const Workspace& ws, double* out, unsigned long long* rowB
 bool LaunchFit(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
                uint32_t cap, const FitParams& fp, double* rows, uint8_t* flags, int precision, cudaStream_t st);
 bool LaunchAstigEstimate(const double* dIn, double* dOut, uint64_t n, double pixelSize, const double* model, double zMax, cudaStream_t st);
+bool TrackDevice(const double* dIn, uint64_t* dOut, uint64_t nPoints, double maxDistance, cudaStream_t st);
 
 // ---- error plumbing -------------------------------------------------------------------------------------------
 namespace {
@@ -1006,6 +1007,23 @@ double Engine::AutoThreshold(const uint16_t* input, uint64_t height, uint64_t wi
 }
 
 // One engine per device, guarded by a mutex (calls on one device are serialized).
+// Tracking over host buffers: [n][4] (Id, Plane, X, Y) -> [n][2] (Id, Track) in (Plane, Id) order.
+bool Engine::Track(const double* input, uint64_t* output, uint64_t n, double maxDistance)
+{
+	if (n == 0) { return true; }
+	if (!Init()) { return false; }
+	double* dIn = nullptr;
+	uint64_t* dOut = nullptr;
+	bool ok = PTB_CUDA(cudaMallocAsync(&dIn, n * 4 * sizeof(double), stream_));
+	ok = ok && PTB_CUDA(cudaMallocAsync(&dOut, n * 2 * sizeof(uint64_t), stream_));
+	ok = ok && PTB_CUDA(cudaMemcpyAsync(dIn, input, n * 4 * sizeof(double), cudaMemcpyHostToDevice, stream_));
+	ok = ok && TrackDevice(dIn, dOut, n, maxDistance, stream_);
+	ok = ok && PTB_CUDA(cudaMemcpyAsync(output, dOut, n * 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream_));
+	if (dIn) { cudaFreeAsync(dIn, stream_); }
+	if (dOut) { cudaFreeAsync(dOut, stream_); }
+	return PTB_CUDA(cudaStreamSynchronize(stream_)) && ok;
+}
+
 bool Engine::AstigEstimate(const double* input, double* output, uint64_t n, double pixelSize, const double* model, double zMax)
 {
 	if (n == 0) { return true; }

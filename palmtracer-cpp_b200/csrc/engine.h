@@ -31,6 +31,7 @@ long long StackResult(uint64_t id, double* times);
 // Number of fit_params entries the given fit mode reads (0 for mode 0 or an unknown mode).
 size_t FitParamCount(uint64_t fit, const double* fp);
 uint64_t LaunchCount();
+bool TrackDevice(const double* dIn, uint64_t* dOut, uint64_t nPoints, double maxDistance, cudaStream_t st);
 double MeasureFmaPeak(int fp64);
 
 class Engine {
@@ -54,6 +55,8 @@ public:
 	double AutoThreshold(const uint16_t* input, uint64_t height, uint64_t width, const double* fitParams);
 	// Astigmatism3DEstimation over host buffers: [n][2] widths (px) -> [n][2] (z nm, score).
 	bool AstigEstimate(const double* input, double* output, uint64_t n, double pixelSize, const double* model, double zMax);
+	// Tracking over host buffers: [n][4] (Id, Plane, X, Y) -> [n][2] (Id, Track) in (Plane, Id) order.
+	bool Track(const double* input, uint64_t* output, uint64_t n, double maxDistance);
 
 	int SetStrict(int s) { const int o = strict_; strict_ = s; return o; }
 	int SetProfiling(int p) { const int o = profiling_; profiling_ = p; return o; }

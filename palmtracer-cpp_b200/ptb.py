@@ -17,7 +17,7 @@ EXPORTS = ["Localization", "Fitting", "Wavelett", "AutoThreshold", "Astigmatism3
            "PTB_SetSegmentationMode", "PTB_SetFitPrecision", "PTB_LastError", "PTB_KernelLaunchCount",
            "PTB_SetProfiling", "PTB_StageTimes", "PTB_MleEvaluations", "PTB_GraphStats", "PTB_MeasureFmaPeak", "PTB_FittingDeviceNoAlloc",
            "PTB_ServerStart", "PTB_SubmitStack", "PTB_PollStack", "PTB_StackResult", "PTB_ServerStop",
-           "PTB_TiffInfo", "PTB_TiffRead", "PTB_LocalizationTiff"]
+           "PTB_TiffInfo", "PTB_TiffRead", "PTB_LocalizationTiff", "Tracking", "PTB_TrackingDevice"]
 
 _u16p = ctypes.POINTER(ctypes.c_uint16)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -62,6 +62,10 @@ def load(path=LIB_PATH):
     L.PTB_StageTimes.argtypes = [_f64p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
     L.PTB_MleEvaluations.restype = None
     L.PTB_MleEvaluations.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
+    L.Tracking.restype = None
+    L.Tracking.argtypes = [_f64p, ctypes.POINTER(_u64), _u64, _f64]
+    L.PTB_TrackingDevice.restype = _u64
+    L.PTB_TrackingDevice.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _u64, _f64, ctypes.c_void_p]
     L.PTB_TiffInfo.restype = ctypes.c_int
     L.PTB_TiffInfo.argtypes = [ctypes.c_char_p, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u64)]
     L.PTB_TiffRead.restype = _u64
@@ -206,6 +210,17 @@ def mle_evaluations():
     out = np.zeros(4, dtype=np.uint64)
     load().PTB_MleEvaluations(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 4)
     return {"lm": int(out[0]), "polish": int(out[1]), "fp64": int(out[2]), "fp64_cholesky": int(out[3])}
+
+
+def tracking(points, max_distance):
+    """Tracking: points [n, 4] (Id, Plane, X, Y) -> [n, 2] uint64 (Id, Track) in (Plane, Id) order."""
+    points = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 4)
+    out = np.zeros((points.shape[0], 2), dtype=np.uint64)
+    if points.shape[0]:
+        load().Tracking(points.ctypes.data_as(_f64p), out.ctypes.data_as(ctypes.POINTER(_u64)), points.shape[0], max_distance)
+        if last_error():
+            raise RuntimeError("Tracking failed: " + last_error())
+    return out
 
 
 def tiff_info(path):

@@ -4,6 +4,7 @@ Reads (text and TIFF only, nothing executed) from the reference tree:
   Tests_CPU/Input/stack.tif, Tests_CPU/Input/stack_quadrant.tif           -> stacks.npz
   Tests_CPU/Input/ref/stack-localizations-*.csv,
   Tests_CPU/Input/ref/stack_quadrant-localizations-*.csv                  -> localizations.npz
+  Tests_CPU/Input/ref/stack-tracking-*-5.csv                              -> tracking.npz
 The AutoThreshold known answers come from Tests_CPU/test_Palm.cpp:307-310 and are stored beside them.
 
 Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
@@ -54,6 +55,13 @@ def main(ref_root):
         locs[key] = data
     locs["__header__"] = np.array(header)
     np.savez_compressed(os.path.join(HERE, "localizations.npz"), **locs)
+    # Tracking known answers (Tests_CPU/test_tr_Tracks.cpp:250-268): Track, Plane, Id, ... of the localizations with
+    # positive integrated intensity, linked with maxDistance 5
+    tracks = {}
+    for path in sorted(glob.glob(os.path.join(inp, "ref", "stack-tracking-*.csv"))):
+        _, data = load_csv(path)
+        tracks[os.path.basename(path)[:-4]] = data
+    np.savez_compressed(os.path.join(HERE, "tracking.npz"), **tracks)
     print({k: v.shape for k, v in stacks.items()}, len(locs) - 1, "csv tables")
 
 
