@@ -147,6 +147,62 @@ def cpu_reference_rate(frames_host, thr, seconds=10.0, threads=None):
                                  "frames": n1, "seconds": dt0, "rows": int(rows.shape[0])}
 
 
+TRACK_DISTANCE = 5.0  # maxDistance of the reference's tracking tests (Tests_CPU/test_tr_Tracks.cpp:262)
+
+
+def tracking_run(ptb, torch, d_rows, n_rows, sample_planes=200):
+    """Tracking (the reference's Tracking export) of the benchmark's own localization table: device-resident through
+    PTB_TrackingDevice (CUDA events around the call, which synchronizes once to size its scratch), end to end through
+    the host Tracking export, and the reference CPU build on the table's first `sample_planes` planes with all host
+    threads; the GPU result on that sample is compared bit for bit with the reference's."""
+    from oracle.oracle import reference, OracleLib
+    rows = d_rows[: n_rows * 18].view(n_rows, 18)
+    pts = rows[:, [0, 1, 4, 5]].contiguous()
+    n = pts.shape[0]
+    out = torch.empty((n, 2), dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream()
+    L = ptb.load()
+    dev_ms = []
+    for i in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if L.PTB_TrackingDevice(pts.data_ptr(), out.data_ptr(), n, TRACK_DISTANCE, stream.cuda_stream) != 2 * n:
+            raise RuntimeError("PTB_TrackingDevice failed: " + ptb.last_error())
+        e1.record(stream)
+        e1.synchronize()
+        if i:
+            dev_ms.append(e0.elapsed_time(e1))
+    host_pts = pts.cpu().numpy()
+    e2e_s = []
+    for i in range(3):
+        t0 = time.perf_counter()
+        got = ptb.tracking(host_pts, TRACK_DISTANCE)
+        if i:
+            e2e_s.append(time.perf_counter() - t0)
+    tracks = int(got[:, 1].max()) if n else 0
+    cpu = reference()
+    kind = "reference"
+    if cpu is None:
+        cpu, kind = OracleLib(), "port"
+    cores = os.cpu_count()
+    cpu.set_threads(cores)
+    sample = host_pts[host_pts[:, 1] <= sample_planes]
+    t0 = time.perf_counter()
+    want = cpu.tracking(sample, TRACK_DISTANCE)
+    cpu_s = time.perf_counter() - t0
+    same = bool(np.array_equal(ptb.tracking(sample, TRACK_DISTANCE), want))
+    dev = float(np.median(dev_ms)) / 1000.0
+    return {"workload": "the benchmark's %d localizations over %d planes, maxDistance %.1f px (%d tracks)"
+                        % (n, int(host_pts[:, 1].max()), TRACK_DISTANCE, tracks),
+            "unit": "points/s", "device": {"value": n / dev, "ms": dev * 1000.0},
+            "e2e": {"value": n / float(np.median(e2e_s)), "ms": float(np.median(e2e_s)) * 1000.0,
+                    "h2d_bytes": int(n * 32), "d2h_bytes": int(n * 16)},
+            "cpu_baseline": {"value": sample.shape[0] / cpu_s, "kind": kind, "cores": cores,
+                             "sample": "the first %d planes (%d points)" % (sample_planes, sample.shape[0]),
+                             "seconds": cpu_s},
+            "parity_on_sample": same}
+
+
 def serving_run(ptb, torch, n_req, seed=2026):
     """C5 serving mix through PTB_ServerStart / PTB_SubmitStack / PTB_StackResult: a Poisson-arrival run at
     SERVE_RATE, a saturated run (every request submitted at once) and the plain one-call-per-frame form on a
@@ -248,6 +304,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--fit", type=int, default=None, help="fit mode (default: %d)" % FIT_MODE)
     ap.add_argument("--no-serving", action="store_true", help="skip the C5 serving mix")
+    ap.add_argument("--no-tracking", action="store_true", help="skip tracking the benchmark's localizations")
     ap.add_argument("--serve-requests", type=int, default=40)
     args = ap.parse_args()
     import torch
@@ -414,6 +471,10 @@ def main():
         link_gbs = part.numel() * 2 / (best / 1000.0) / 1e9
         del dev
 
+    tracking = None
+    if rank == 0 and world == 1 and not args.no_tracking:
+        tracking = tracking_run(ptb, torch, d_out, int(rows))
+
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
         del host_in, host_np, host_out
@@ -443,7 +504,7 @@ def main():
                         # host -> device rate over the call (the frames cross PCIe once; the link is the e2e bound)
                         "h2d_gbs": h2d_bytes / (float(np.mean(e2e_ms)) / 1000.0) / 1e9 if e2e_ms else None,
                         "h2d_link_gbs": link_gbs},
-                "gpu_launches": int(launches), "clocks": clk, "serving": serving}
+                "gpu_launches": int(launches), "clocks": clk, "serving": serving, "tracking": tracking}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

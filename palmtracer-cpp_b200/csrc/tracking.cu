@@ -8,14 +8,18 @@
 //   3. in that order a pair links when its source has no successor and its target no predecessor yet
 //   4. track numbers 1, 2, ... given to the chain heads in point order, then along each chain (:188-199)
 //   5. output (Id, Track) per point in point order                                          (:203-212)
-// On the GPU: the (Plane, Id) order is a counting sort by plane followed by a per-plane sort of (Id, input index);
-// step 2 runs one CTA per source plane with the next plane staged in shared memory, in two passes (count, emit);
-// step 3 sorts each transition's pairs in one CTA and links them in order with one thread per transition
+// On the GPU: the (Plane, Id) order is a counting sort by plane followed by a per-plane sort of (Id, input index).
+// Step 2 does not test every pair: each plane is also sorted by X, and every point scans only the window of the next
+// plane whose X lies within w of its own (binary search, then a forward scan), w slightly above maxDistance. A pair
+// outside the window has fl(dx * dx) > maxDistance^2, so fl(fl(dx^2) + fl(dy^2)) > maxDistance^2 too (rounding is
+// monotone) and the reference rejects it; inside, the reference's own test decides. Two passes, count then emit.
+// Step 3 sorts each transition's pairs in one CTA and links them in order with one thread per transition
 // (transitions touch disjoint successor and predecessor entries); step 4 is a scan over chain heads and pointer
 // jumping along predecessor links. d2 is formed with explicitly rounded FP64 operations (no contraction), so the
 // admitted pairs and their order are the reference's; ties in (Plane, Id), which the reference's unstable sort
 // leaves unspecified, are ordered by input index.
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "pt_common.cuh"
@@ -29,8 +33,8 @@ namespace {
 
 constexpr uint32_t kNoLink = 0xffffffffu;
 constexpr int kTrackThreads = 256;
-constexpr int kSegSmem = 2048;  // pairs sorted in shared memory (32 KB); longer segments sort in global scratch
-constexpr int kNextTile = 1024; // next-plane points staged per pass (16 KB)
+constexpr int kSegSmem = 4096;  // pairs sorted in shared memory (64 KB); longer segments sort in global scratch
+constexpr int kSortThreads = 512;
 
 // static_cast<size_t>(double) of the reference for the values a localization table holds (non-negative integers)
 __device__ __forceinline__ uint64_t ToIndex(double v) { return __double2ull_rz(v); }
@@ -104,10 +108,12 @@ __device__ void BitonicPairs(unsigned long long* k1, unsigned long long* k2, uin
 
 // One CTA per segment [off[s], off[s + 1]): sorts its (k1, k2) pairs ascending. Segments longer than kSegSmem sort
 // in global scratch at [2 off[s], 2 off[s] + 2 len) (a power of two below 2 len, so segments never overlap).
-__global__ void __launch_bounds__(kTrackThreads) SegmentSort(unsigned long long* k1, unsigned long long* k2, const uint32_t* __restrict__ off,
-                                                             uint32_t nseg, unsigned long long* s1, unsigned long long* s2)
+__global__ void __launch_bounds__(kSortThreads) SegmentSort(unsigned long long* k1, unsigned long long* k2, const uint32_t* __restrict__ off,
+                                                            uint32_t nseg, unsigned long long* s1, unsigned long long* s2)
 {
-	__shared__ unsigned long long a1[kSegSmem], a2[kSegSmem];
+	extern __shared__ unsigned long long segSmem[];
+	unsigned long long* a1 = segSmem;
+	unsigned long long* a2 = segSmem + kSegSmem;
 	for (uint32_t s = blockIdx.x; s < nseg; s += gridDim.x) {
 		const uint32_t b = off[s], len = off[s + 1] - b;
 		if (len <= 1) { continue; }
@@ -131,12 +137,27 @@ __global__ void __launch_bounds__(kTrackThreads) SegmentSort(unsigned long long*
 	}
 }
 
-// Point order established: coordinates of each ordered point.
-__global__ void TrackGather(const double* __restrict__ in, const unsigned long long* __restrict__ src, uint32_t n, double2* xy)
+// Order-preserving map of a double to unsigned 64 bits (NaN, either sign, after +inf).
+__device__ __forceinline__ unsigned long long XKey(double d)
+{
+	if (isnan(d)) { return ~0ull; }
+	if (d == 0.0) { d = 0.0; }
+	const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(d));
+	return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+// Point order established: coordinates and plane of each ordered point, and the (X, point) pairs that the per-plane
+// X sort orders.
+__global__ void TrackGather(const double* __restrict__ in, const unsigned long long* __restrict__ src, const uint64_t* __restrict__ plane,
+                            uint32_t n, uint64_t minPlane, double2* xy, uint32_t* rel, unsigned long long* xk1, unsigned long long* xk2)
 {
 	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
 		const uint32_t i = static_cast<uint32_t>(src[k]);
-		xy[k] = make_double2(in[4ull * i + 2], in[4ull * i + 3]);
+		const double x = in[4ull * i + 2];
+		xy[k] = make_double2(x, in[4ull * i + 3]);
+		rel[k] = static_cast<uint32_t>(plane[i] - minPlane);
+		xk1[k] = XKey(x);
+		xk2[k] = k;
 	}
 }
 
@@ -146,51 +167,58 @@ __device__ __forceinline__ double SqDistance(double2 a, double2 b)
 	return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
 }
 
-// One CTA per source plane p: every point of p against every point of p + 1, the next plane staged in shared
-// memory. EMIT = false counts the admitted pairs of each source point (count[k], and their total); EMIT = true writes
-// them at their offsets as (d2 bits, source << 32 | target) — d2 >= 0, so its bits order like its value.
+// One thread per point k: the points of the next plane inside its X window (all of them when the window is
+// unbounded), tested with the reference's rule d2 <= r2. xs1/xs2: per plane, X keys ascending and their points.
+// EMIT = false counts the admitted pairs of each point (count[k], and their total); EMIT = true writes them at their
+// offsets as (d2 bits, source << 32 | target) — d2 >= 0, so its bits order like its value.
 template <bool EMIT>
-__global__ void __launch_bounds__(kTrackThreads) TrackPairs(const double2* __restrict__ xy, const uint32_t* __restrict__ begin, uint32_t P,
-                                                            double r2, uint32_t* count, unsigned long long* total,
+__global__ void __launch_bounds__(kTrackThreads) TrackPairs(const double2* __restrict__ xy, const uint32_t* __restrict__ rel,
+                                                            const uint32_t* __restrict__ begin, const unsigned long long* __restrict__ xs1,
+                                                            const unsigned long long* __restrict__ xs2, uint32_t n, uint32_t P, double r2,
+                                                            double w, uint32_t* count, unsigned long long* total,
                                                             unsigned long long* k1, unsigned long long* k2)
 {
-	__shared__ double2 tile[kNextTile];
-	for (uint32_t p = blockIdx.x; p + 1 < P; p += gridDim.x) {
-		const uint32_t a = begin[p], b = begin[p + 1], c = begin[p + 2];
-		if (a == b || b == c) { continue; }
-		unsigned long long mine = 0;
-		for (uint32_t k0 = a; k0 < b; k0 += blockDim.x) {
-			const uint32_t k = k0 + threadIdx.x;
-			const bool active = k < b;
-			const double2 me = active ? xy[k] : make_double2(0.0, 0.0);
-			uint32_t found = 0;
-			uint32_t at = EMIT && active ? count[k] : 0u;
-			for (uint32_t j0 = b; j0 < c; j0 += kNextTile) {
-				const uint32_t m = min(static_cast<uint32_t>(kNextTile), c - j0);
-				__syncthreads();
-				for (uint32_t t = threadIdx.x; t < m; t += blockDim.x) { tile[t] = xy[j0 + t]; }
-				__syncthreads();
-				if (active) {
-					for (uint32_t t = 0; t < m; ++t) {
-						const double d2 = SqDistance(me, tile[t]);
-						if (d2 <= r2) {
-							if (EMIT) {
-								k1[at] = static_cast<unsigned long long>(__double_as_longlong(d2));
-								k2[at] = (static_cast<unsigned long long>(k) << 32) | (j0 + t);
-								++at;
-							}
-							++found;
-						}
-					}
-				}
+	unsigned long long mine = 0;
+	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		const uint32_t p = rel[k];
+		if (p + 1 >= P) { continue; }
+		uint32_t pos = begin[p + 1];
+		const uint32_t c = begin[p + 2];
+		const double2 me = xy[k];
+		if (pos == c || isnan(me.x)) { continue; }  // a NaN coordinate admits no pair under any radius
+		unsigned long long hiKey = ~0ull;
+		if (w < __longlong_as_double(0x7ff0000000000000ll)) {
+			// first X >= me.x - w, then forward while X <= me.x + w
+			const unsigned long long loKey = XKey(me.x - w);
+			hiKey = XKey(me.x + w);
+			uint32_t lo = pos, hi = c;
+			while (lo < hi) {
+				const uint32_t mid = lo + ((hi - lo) >> 1);
+				if (xs1[mid] < loKey) { lo = mid + 1; }
+				else { hi = mid; }
 			}
-			if (!EMIT && active) { count[k] = found; }
-			mine += found;
+			pos = lo;
 		}
-		if (!EMIT) {
-			for (int d = 16; d > 0; d >>= 1) { mine += __shfl_xor_sync(0xffffffffu, mine, d); }
-			if ((threadIdx.x & 31) == 0 && mine) { atomicAdd(total, mine); }
+		uint32_t found = 0;
+		uint32_t at = EMIT ? count[k] : 0u;
+		for (; pos < c && xs1[pos] <= hiKey; ++pos) {
+			const uint32_t j = static_cast<uint32_t>(xs2[pos]);
+			const double d2 = SqDistance(me, xy[j]);
+			if (d2 <= r2) {
+				if (EMIT) {
+					k1[at] = static_cast<unsigned long long>(__double_as_longlong(d2));
+					k2[at] = (static_cast<unsigned long long>(k) << 32) | j;
+					++at;
+				}
+				++found;
+			}
 		}
+		if (!EMIT) { count[k] = found; }
+		mine += found;
+	}
+	if (!EMIT) {
+		for (int d = 16; d > 0; d >>= 1) { mine += __shfl_xor_sync(0xffffffffu, mine, d); }
+		if ((threadIdx.x & 31) == 0 && mine) { atomicAdd(total, mine); }
 	}
 }
 
@@ -237,6 +265,19 @@ __global__ void TrackOutput(const unsigned long long* __restrict__ id, const uin
 		out[2ull * k] = id[k];
 		out[2ull * k + 1] = static_cast<uint64_t>(headRank[root[k]]) + 1;
 	}
+}
+
+constexpr size_t kSegSmemBytes = 2 * kSegSmem * sizeof(unsigned long long);
+
+bool LaunchSegmentSort(unsigned long long* k1, unsigned long long* k2, const uint32_t* off, uint32_t nseg, unsigned long long* s1,
+                       unsigned long long* s2, cudaStream_t st)
+{
+	static const bool configured = PTB_CUDA(cudaFuncSetAttribute(SegmentSort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                                             static_cast<int>(kSegSmemBytes)));
+	if (!configured) { return false; }
+	SegmentSort<<<std::max<uint32_t>(1, std::min<uint32_t>(nseg, 148u * 32)), kSortThreads, kSegSmemBytes, st>>>(k1, k2, off, nseg, s1, s2);
+	CountLaunch();
+	return PTB_LAUNCHED();
 }
 
 uint32_t Grid(uint64_t n, int threads) { return static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>((n + threads - 1) / threads, 148ull * 16))); }
@@ -291,9 +332,11 @@ bool TrackDevice(const double* dIn, uint64_t* dOut, uint64_t nPoints, double max
 	uint32_t *begin = nullptr, *cursor = nullptr, *scanScratch = nullptr;
 	unsigned long long *pk1 = nullptr, *pk2 = nullptr, *s1 = nullptr, *s2 = nullptr;
 	double2* xy = nullptr;
+	uint32_t* rel = nullptr;
+	unsigned long long *xk1 = nullptr, *xk2 = nullptr;
 	const uint32_t scanCap = std::max(n, P) + 2;
 	ok = alloc(begin, P + 2) && alloc(cursor, P) && alloc(scanScratch, scanCap / 4096 + 2) && alloc(pk1, n) && alloc(pk2, n) &&
-	     alloc(s1, 2ull * n) && alloc(s2, 2ull * n) && alloc(xy, n);
+	     alloc(s1, 2ull * n) && alloc(s2, 2ull * n) && alloc(xy, n) && alloc(rel, n) && alloc(xk1, n) && alloc(xk2, n);
 	ok = ok && PTB_CUDA(cudaMemsetAsync(begin, 0, sizeof(uint32_t) * (P + 2), st)) &&
 	     PTB_CUDA(cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * P, st));
 	if (ok) {
@@ -304,10 +347,14 @@ bool TrackDevice(const double* dIn, uint64_t* dOut, uint64_t nPoints, double max
 	}
 	if (ok) {
 		PlaneScatter<<<G, kTrackThreads, 0, st>>>(plane, id, n, minPlane, begin, cursor, pk1, pk2);
-		SegmentSort<<<std::min<uint32_t>(P, 148u * 64), kTrackThreads, 0, st>>>(pk1, pk2, begin, P, s1, s2);
-		TrackGather<<<G, kTrackThreads, 0, st>>>(dIn, pk2, n, xy);
-		CountLaunch(3);
-		ok = PTB_LAUNCHED();
+		CountLaunch();
+		ok = PTB_LAUNCHED() && LaunchSegmentSort(pk1, pk2, begin, P, s1, s2, st);
+	}
+	if (ok) {
+		// coordinates in point order, then each plane's points by X for the window search
+		TrackGather<<<G, kTrackThreads, 0, st>>>(dIn, pk2, plane, n, minPlane, xy, rel, xk1, xk2);
+		CountLaunch();
+		ok = PTB_LAUNCHED() && LaunchSegmentSort(xk1, xk2, begin, P, s1, s2, st);
 	}
 	// admitted pairs: count, offsets, emit
 	uint32_t* pairBegin = nullptr;
@@ -315,9 +362,11 @@ bool TrackDevice(const double* dIn, uint64_t* dOut, uint64_t nPoints, double max
 	ok = ok && alloc(pairBegin, n + 2) && alloc(total, 1) && PTB_CUDA(cudaMemsetAsync(total, 0, sizeof(unsigned long long), st)) &&
 	     PTB_CUDA(cudaMemsetAsync(pairBegin, 0, sizeof(uint32_t) * (n + 2), st));
 	const double r2 = maxDistance * maxDistance;
-	const uint32_t planeGrid = std::max<uint32_t>(1, std::min<uint32_t>(P, 148u * 64));
+	// X half-width of the search window: above sqrt(r2) by more than the rounding of dx, dx^2 and the bounds (and
+	// above the largest |dx| whose square underflows to 0); unbounded when r2 is infinite or NaN
+	const double w = std::isfinite(r2) ? std::max(std::sqrt(r2) * (1.0 + std::ldexp(1.0, -30)), 1e-150) : HUGE_VAL;
 	if (ok) {
-		TrackPairs<false><<<planeGrid, kTrackThreads, 0, st>>>(xy, begin, P, r2, pairBegin, total, nullptr, nullptr);
+		TrackPairs<false><<<G, kTrackThreads, 0, st>>>(xy, rel, begin, xk1, xk2, n, P, r2, w, pairBegin, total, nullptr, nullptr);
 		CountLaunch();
 		ok = PTB_LAUNCHED();
 	}
@@ -333,16 +382,19 @@ bool TrackDevice(const double* dIn, uint64_t* dOut, uint64_t nPoints, double max
 	ok = ok && alloc(ck1, pairs) && alloc(ck2, pairs) && alloc(c1, 2 * pairs) && alloc(c2, 2 * pairs) && alloc(off, P + 1) &&
 	     alloc(next, n) && alloc(prev, n) && alloc(head, n + 2) && alloc(root, n);
 	if (ok && pairs > 0) {
-		TrackPairs<true><<<planeGrid, kTrackThreads, 0, st>>>(xy, begin, P, r2, pairBegin, nullptr, ck1, ck2);
+		TrackPairs<true><<<G, kTrackThreads, 0, st>>>(xy, rel, begin, xk1, xk2, n, P, r2, w, pairBegin, nullptr, ck1, ck2);
 		CountLaunch();
 		ok = PTB_LAUNCHED();
 	}
 	ok = ok && PTB_CUDA(cudaMemsetAsync(next, 0xff, sizeof(uint32_t) * n, st)) && PTB_CUDA(cudaMemsetAsync(prev, 0xff, sizeof(uint32_t) * n, st));
 	if (ok && pairs > 0) {
 		TransitionOffsets<<<Grid(P + 1, kTrackThreads), kTrackThreads, 0, st>>>(begin, pairBegin, P, off);
-		SegmentSort<<<std::min<uint32_t>(P, 148u * 64), kTrackThreads, 0, st>>>(ck1, ck2, off, P, c1, c2);
+		CountLaunch();
+		ok = PTB_LAUNCHED() && LaunchSegmentSort(ck1, ck2, off, P, c1, c2, st);
+	}
+	if (ok && pairs > 0) {
 		TrackLink<<<Grid(P, 128), 128, 0, st>>>(ck2, off, P, next, prev);
-		CountLaunch(3);
+		CountLaunch();
 		ok = PTB_LAUNCHED();
 	}
 	if (ok) {

@@ -42,6 +42,30 @@ def test_tracking_edge_cases(lib, orc):
     assert np.array_equal(lib.tracking(sparse, 2.0), orc.tracking(sparse, 2.0))
 
 
+def _boundary_points(x0, y0, r, seed):
+    """A source point and targets on and just around the circle of radius r (the window search's edge cases)."""
+    rng = np.random.default_rng(seed)
+    rows = [[1, 1, x0, y0]]
+    targets = [(x0 + r, y0), (x0 - r, y0), (np.nextafter(x0 + r, np.inf), y0), (np.nextafter(x0 - r, -np.inf), y0),
+               (x0, y0 + r), (x0, np.nextafter(y0 - r, -np.inf))]
+    for t in rng.uniform(0, 2 * np.pi, 40):
+        targets.append((x0 + r * np.cos(t), y0 + r * np.sin(t)))
+    for k, (x, y) in enumerate(targets):
+        rows.append([k + 2, 2, x, y])
+    # more sources in plane 1 on the same circle, so that many pairs sit at distance ~r
+    for k, t in enumerate(rng.uniform(0, 2 * np.pi, 20)):
+        rows.append([100 + k, 1, x0 + r * np.cos(t), y0 + r * np.sin(t)])
+    return np.array(rows, dtype=np.float64)
+
+
+@pytest.mark.parametrize("r", [2.0, 0.1, 5.0, 1e-140, 1e140, 3.0e-5])
+@pytest.mark.parametrize("x0", [0.0, 1000.3, 1.0e6 + 0.123])
+def test_tracking_window_boundary(lib, orc, r, x0):
+    pts = _boundary_points(x0, 17.25, r, seed=int(x0) % 97 + 3)
+    for radius in (r, np.nextafter(r, 0.0), np.nextafter(r, np.inf)):
+        assert np.array_equal(lib.tracking(pts, radius), orc.tracking(pts, radius)), radius
+
+
 def test_tracking_large(lib, orc):
     pts = tc.synthetic(33, planes=400, per_plane=1500, size=2048.0, step=1.0, blink=0.2, gap_every=37)
     assert pts.shape[0] > 400000
