@@ -47,9 +47,9 @@ REF_FIT_MODE = 2  # the reference's own 5-parameter Gaussian fit, for the CPU ar
 FLOP_PER_PIXEL_LM = 71
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per frame of one launch, from ncu captures of smaller
 # chunks of the same workload, scaled by the frames a benchmark launch processes (traffic grows with the frames):
-# MleLmKernel<6> 104.1 MB over a 50-frame chunk, DetectKernel 90.6 MB over a 22-frame chunk.
-LM_DRAM_BYTES_PER_FRAME = 104.13e6 / 50
-DETECT_DRAM_BYTES_PER_FRAME = 90.60e6 / 22
+# MleLmKernel<6> 127.27 MB and DetectKernel 262.41 MB over one 64-frame chunk (profiles/*_c2_64frames.md).
+LM_DRAM_BYTES_PER_FRAME = 127.27e6 / 64
+DETECT_DRAM_BYTES_PER_FRAME = 262.41e6 / 64
 RATIO = 0.0
 PER_PLANE = 8192
 # Serving mix (C5): Poisson arrivals at 20 stacks/s of square frames from {128, 256, 512, 1024, 2048}, lengths 1-500,
