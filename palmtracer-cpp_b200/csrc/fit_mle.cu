@@ -5,7 +5,9 @@
 // stop rule one decade looser, see StepSmall), then Newton steps on the exact Hessian of the deviance, parameters on
 // active bounds held throughout, and the CRLB from the Fisher information at the final point.
 //
-// Precision: the LM iterations and the Newton polish run in FP32. Each 5x5 system is factored by an FP32 Cholesky;
+// Precision: the LM iterations and the Newton polish run in FP32, with the hardware approximations of exp and log
+// (__expf: a few ulp; __logf: absolute error about 2^-21 near 1) and erff; the per-pixel logarithm of the deviance
+// had been a fifth of the LM's time. Each 5x5 system is factored by an FP32 Cholesky;
 // when a pivot is not positive or the pivot ratio min(L_ii^2 / A_ii) falls below 1e-5 the same system is
 // re-factored in FP64. The initial axial pre-scan (a handful of deviance evaluations that choose the starting basin),
 // the final deviance (log-likelihood) and the Fisher information behind the CRLB are computed in FP64. The oracle
@@ -54,11 +56,16 @@ template <typename T> __device__ __forceinline__ T Erf(T x);
 template <> __device__ __forceinline__ float Erf<float>(float x) { return erff(x); }
 template <> __device__ __forceinline__ double Erf<double>(double x) { return erf(x); }
 template <typename T> __device__ __forceinline__ T Ex(T x);
-template <> __device__ __forceinline__ float Ex<float>(float x) { return expf(x); }
+template <> __device__ __forceinline__ float Ex<float>(float x) { return __expf(x); }  // hardware ex2 based
 template <> __device__ __forceinline__ double Ex<double>(double x) { return exp(x); }
 template <typename T> __device__ __forceinline__ T Ln(T x);
-template <> __device__ __forceinline__ float Ln<float>(float x) { return logf(x); }
+template <> __device__ __forceinline__ float Ln<float>(float x) { return __logf(x); }  // hardware lg2 based
 template <> __device__ __forceinline__ double Ln<double>(double x) { return log(x); }
+
+// Division in the per-pixel sums: FP32 with the hardware approximation (divisors here are photon counts and model
+// values, far inside its range), FP64 exact.
+template <typename T> __device__ __forceinline__ T Div(T a, T b) { return a / b; }
+template <> __device__ __forceinline__ float Div<float>(float a, float b) { return __fdividef(a, b); }
 
 template <typename T>
 __device__ __forceinline__ T WarpSum(T v)
@@ -259,10 +266,10 @@ template <typename T, int KIND>
 __device__ __forceinline__ void Accumulate(T d, T bg, T I, T psf, const T P1[3], const T P2[6], T& D, T G[5], T Hm[15], T Fm[15])
 {
 	const T mu = max(bg + I * psf, T(1e-6));
-	D += d > T(0) ? T(2) * (mu - d - d * Ln<T>(mu / d)) : T(2) * mu;
+	D += d > T(0) ? T(2) * (mu - d - d * Ln<T>(Div<T>(mu, d))) : T(2) * mu;
 	if constexpr (KIND != kDevOnly) {
 		const T gk[5] = {T(1), psf, I * P1[0], I * P1[1], I * P1[2]};
-		const T rmu = T(1) / mu;
+		const T rmu = Div<T>(T(1), mu);
 		if constexpr (KIND == kFinal) {
 			int q = 0;
 			#pragma unroll
