@@ -9,8 +9,9 @@
 // (__expf: a few ulp; __logf: absolute error about 2^-21 near 1) and erff; the per-pixel logarithm of the deviance
 // had been a fifth of the LM's time. Each 5x5 system is factored by an FP32 Cholesky;
 // when a pivot is not positive or the pivot ratio min(L_ii^2 / A_ii) falls below 1e-5 the same system is
-// re-factored in FP64. The initial axial pre-scan (a handful of deviance evaluations that choose the starting basin),
-// the final deviance (log-likelihood) and the Fisher information behind the CRLB are computed in FP64. The oracle
+// re-factored in FP64. The initial axial pre-scan (a handful of deviance evaluations that choose the starting basin)
+// and the Fisher information behind the CRLB are computed in FP64 (the final point's deviance is not part of the
+// output, so the final pass does not form it). The oracle
 // polishes in FP64 to a 1e-10 relative step; the FP32 polish stops at a 1e-6 relative step (the FP32 resolution of
 // the deviance), well inside the stated tolerance of 1e-3 px and 1e-4 relative photons.
 //
@@ -22,7 +23,7 @@
 //                       next candidate of the range as soon as its own converges, so a lane never idles while the
 //                       other 31 iterate; ROI photons and the column erf factors are staged per lane in shared memory;
 //       MlePolishKernel persistent FP32 Newton polish, organised the same way;
-//       MleFinalKernel  FP64 deviance and Fisher information, CRLB, output row;
+//       MleFinalKernel  FP64 Fisher information, CRLB, output row;
 //   * warp per ROI (MleWarpKernel): all four phases in one launch, pixels spread over the lanes, sums reduced with
 //     shuffles; better for large ROIs and for the spline model, whose 64 coefficients per pixel dominate.
 // For modes 6-7 the pixel-integrated Gaussian is separable: the erf factors are formed once per ROI column and row
@@ -266,7 +267,8 @@ template <typename T, int KIND>
 __device__ __forceinline__ void Accumulate(T d, T bg, T I, T psf, const T P1[3], const T P2[6], T& D, T G[5], T Hm[15], T Fm[15])
 {
 	const T mu = max(bg + I * psf, T(1e-6));
-	D += d > T(0) ? T(2) * (mu - d - d * Ln<T>(Div<T>(mu, d))) : T(2) * mu;
+	// the final pass needs only the Fisher information (the CRLB); its deviance would be discarded
+	if constexpr (KIND != kFinal) { D += d > T(0) ? T(2) * (mu - d - d * Ln<T>(Div<T>(mu, d))) : T(2) * mu; }
 	if constexpr (KIND != kDevOnly) {
 		const T gk[5] = {T(1), psf, I * P1[0], I * P1[1], I * P1[2]};
 		const T rmu = Div<T>(T(1), mu);
@@ -715,13 +717,13 @@ __device__ int Polish(const MleParams& mp, const Pix& px, float x0, float y0, fl
 	return evals;
 }
 
-// FP64 deviance and Fisher information at t; CRLB = sqrt(diag(F^-1)). False when either is unusable.
+// FP64 Fisher information at t; CRLB = sqrt(diag(F^-1)). False when it cannot be inverted or t is not finite (the
+// oracle's final step, which computes no deviance either).
 template <int MODEL, int L>
 __device__ bool Final(const MleParams& mp, const Pix& px, const double t[5], double crlb[5], FacTab<double> xt, FacTab<double> yt)
 {
 	double Fm[15];
-	const double D = Normal<double, MODEL, L, kFinal>(mp, px, t, nullptr, nullptr, Fm, xt, yt);
-	if (!isfinite(D)) { return false; }
+	Normal<double, MODEL, L, kFinal>(mp, px, t, nullptr, nullptr, Fm, xt, yt);  // a non-finite entry fails the Cholesky
 	#pragma unroll
 	for (int a = 0; a < 5; ++a) {
 		double e[5] = {0, 0, 0, 0, 0}, cv[5];
