@@ -289,13 +289,8 @@ __device__ __forceinline__ void Accumulate(T d, T bg, T I, T psf, const T P1[3],
 			for (int a = 0; a < 5; ++a) {
 				G[a] += w1 * gk[a];
 				const T wa = w2 * gk[a];
-				const T fa = rmu * gk[a];
 				#pragma unroll
-				for (int b = a; b < 5; ++b) {
-					Hm[q] += wa * gk[b];
-					if constexpr (KIND == kExact) { Fm[q] += fa * gk[b]; }
-					++q;
-				}
+				for (int b = a; b < 5; ++b) { Hm[q++] += wa * gk[b]; }
 			}
 			if constexpr (KIND == kExact) {
 				// d2mu in the packed upper triangle: (I, x) = Px, (I, y) = Py, (I, s) = Ps, (x, x) = I Pxx, ...
@@ -356,7 +351,7 @@ __device__ T Normal(const MleParams& mp, const Pix& px, const T th[5], T G[5], T
 		#pragma unroll
 		for (int a = 0; a < 15; ++a) { Hm[a] = T(0); }
 	}
-	if constexpr (KIND == kExact || KIND == kFinal) {
+	if constexpr (KIND == kFinal) {
 		#pragma unroll
 		for (int a = 0; a < 15; ++a) { Fm[a] = T(0); }
 	}
@@ -433,7 +428,7 @@ __device__ T Normal(const MleParams& mp, const Pix& px, const T th[5], T G[5], T
 			#pragma unroll
 			for (int a = 0; a < 15; ++a) { Hm[a] = WarpSum(Hm[a]); }
 		}
-		if constexpr (KIND == kExact || KIND == kFinal) {
+		if constexpr (KIND == kFinal) {
 			#pragma unroll
 			for (int a = 0; a < 15; ++a) { Fm[a] = WarpSum(Fm[a]); }
 		}
@@ -576,10 +571,11 @@ __device__ __forceinline__ bool StepSmall(int model, const float a[5], const flo
 }
 
 // Newton direction at th: the exact Hessian with active bounds held, Fisher scoring where that Hessian is not
-// positive definite. Hm is modified in place.
-template <int MODEL>
+// positive definite. Hm is modified in place. fisher(Hf) fills Hf with the Fisher-scoring matrix 2 F at th (an extra
+// evaluation, made only in that case).
+template <int MODEL, typename FisherFn>
 __device__ __forceinline__ bool NewtonDirection(const MleParams& mp, float x0, float y0, const float th[5], const float G[5], float Hm[15],
-                                                const float Fm[15], float dt[5])
+                                                float dt[5], FisherFn fisher)
 {
 	float rhs[5];
 	#pragma unroll
@@ -587,8 +583,7 @@ __device__ __forceinline__ bool NewtonDirection(const MleParams& mp, float x0, f
 	FixActive32<MODEL>(mp, x0, y0, th, G, Hm, rhs);
 	if (Solve32(Hm, 1.f, rhs, dt, nullptr, false)) { return true; }
 	float Hf[15];
-	#pragma unroll
-	for (int a = 0; a < 15; ++a) { Hf[a] = 2.f * Fm[a]; }
+	fisher(Hf);
 	FixActive32<MODEL>(mp, x0, y0, th, G, Hf, rhs);
 	return Solve32(Hf, 1.f, rhs, dt, nullptr, false);
 }
@@ -682,20 +677,25 @@ __device__ int InitTheta(const MleParams& mp, const Pix& px, const RoiAt& r, dou
 template <int MODEL, int L>
 __device__ int Polish(const MleParams& mp, const Pix& px, float x0, float y0, float th[5], FacTab<float> xt, FacTab<float> yt)
 {
-	float G[5], Hm[15], Fm[15];
-	float D = Normal<float, MODEL, L, kExact>(mp, px, th, G, Hm, Fm, xt, yt);
+	float G[5], Hm[15];
+	float D = Normal<float, MODEL, L, kExact>(mp, px, th, G, Hm, nullptr, xt, yt);
 	int evals = 1;
 	if (!isfinite(D)) { return evals; }
 	for (int it = 0; it < 6; ++it) {
 		float dt[5], tt[5];
-		if (!NewtonDirection<MODEL>(mp, x0, y0, th, G, Hm, Fm, dt)) { break; }
+		auto fisher = [&](float Hf[15]) {
+			float Gf[5];
+			Normal<float, MODEL, L, kFisher>(mp, px, th, Gf, Hf, nullptr, xt, yt);
+			++evals;
+		};
+		if (!NewtonDirection<MODEL>(mp, x0, y0, th, G, Hm, dt, fisher)) { break; }
 		bool accepted = false;
-		float Gt[5], Ht[15], Ft[15], Dt = 0.f;
+		float Gt[5], Ht[15], Dt = 0.f;
 		for (int hv = 0; hv < 4 && !accepted; ++hv) {
 			#pragma unroll
 			for (int a = 0; a < 5; ++a) { tt[a] = th[a] + dt[a]; }
 			Clamp32<MODEL>(mp, x0, y0, tt);
-			Dt = Normal<float, MODEL, L, kExact>(mp, px, tt, Gt, Ht, Ft, xt, yt);
+			Dt = Normal<float, MODEL, L, kExact>(mp, px, tt, Gt, Ht, nullptr, xt, yt);
 			++evals;
 			if (PolishAccept(Dt, D)) { accepted = true; }
 			else {
@@ -710,7 +710,7 @@ __device__ int Polish(const MleParams& mp, const Pix& px, float x0, float y0, fl
 		#pragma unroll
 		for (int a = 0; a < 5; ++a) { th[a] = tt[a]; G[a] = Gt[a]; }
 		#pragma unroll
-		for (int a = 0; a < 15; ++a) { Hm[a] = Ht[a]; Fm[a] = Ft[a]; }
+		for (int a = 0; a < 15; ++a) { Hm[a] = Ht[a]; }
 		D = Dt;
 		if (step < 1e-6f) { break; }
 	}
@@ -983,7 +983,7 @@ __global__ void __launch_bounds__(kThreads) MleLmKernel(const uint16_t* __restri
 }
 
 // Persistent FP32 Newton polish (WarpQueue), the steps of Polish() as a per-lane state machine: each pass evaluates
-// the deviance, gradient, exact Hessian and Fisher information once per busy lane - at the LM result of a new
+// the deviance, gradient and exact Hessian once per busy lane - at the LM result of a new
 // candidate or at a trial point - and then accepts, halves or ends. Shared memory per lane: the ROI photons (n
 // floats) and the column factors with second derivatives (6 roi floats).
 template <int MODEL>
@@ -999,7 +999,7 @@ __global__ void __launch_bounds__(kThreads) MlePolishKernel(const uint16_t* __re
 	if (!q.Init(CandCount(nptr, nconst), mp.queue ? mp.queue + 1 : nullptr)) { return; }
 	uint32_t k = kNone;
 	bool fresh = false;
-	float th[5] = {0, 0, 0, 0, 0}, dt[5] = {0, 0, 0, 0, 0}, G[5], Hm[15], Fm[15], D = 0.f, x0 = 0.f, y0 = 0.f;
+	float th[5] = {0, 0, 0, 0, 0}, dt[5] = {0, 0, 0, 0, 0}, G[5], Hm[15], D = 0.f, x0 = 0.f, y0 = 0.f;
 	int it = 0, hv = 0;
 	unsigned long long evals = 0;
 	Pix px = MakePix(mp, img, W, ph, T);
@@ -1015,13 +1015,13 @@ __global__ void __launch_bounds__(kThreads) MlePolishKernel(const uint16_t* __re
 			if (q.Done()) { break; }
 			continue;
 		}
-		float tt[5], Gt[5], Ht[15], Ft[15], Dt = 0.f;
+		float tt[5], Gt[5], Ht[15], Dt = 0.f;
 		bool finish = false;
 		if (busy) {
 			#pragma unroll
 			for (int a = 0; a < 5; ++a) { tt[a] = fresh ? th[a] : th[a] + dt[a]; }
 			if (!fresh) { Clamp32<MODEL>(mp, x0, y0, tt); }
-			Dt = Normal<float, MODEL, 1, kExact>(mp, px, tt, Gt, Ht, Ft, xt, xt);
+			Dt = Normal<float, MODEL, 1, kExact>(mp, px, tt, Gt, Ht, nullptr, xt, xt);
 			++evals;
 			bool moved = false;
 			if (fresh) {
@@ -1047,10 +1047,17 @@ __global__ void __launch_bounds__(kThreads) MlePolishKernel(const uint16_t* __re
 				#pragma unroll
 				for (int a = 0; a < 5; ++a) { th[a] = tt[a]; G[a] = Gt[a]; }
 				#pragma unroll
-				for (int a = 0; a < 15; ++a) { Hm[a] = Ht[a]; Fm[a] = Ft[a]; }
+				for (int a = 0; a < 15; ++a) { Hm[a] = Ht[a]; }
 				D = Dt;
 				hv = 0;
-				if (!finish) { finish = !NewtonDirection<MODEL>(mp, x0, y0, th, G, Hm, Fm, dt); }
+				if (!finish) {
+					auto fisher = [&](float Hf[15]) {
+						float Gf[5];
+						Normal<float, MODEL, 1, kFisher>(mp, px, th, Gf, Hf, nullptr, xt, xt);
+						++evals;
+					};
+					finish = !NewtonDirection<MODEL>(mp, x0, y0, th, G, Hm, dt, fisher);
+				}
 			}
 		}
 		if (finish) {
