@@ -147,6 +147,45 @@ def cpu_reference_rate(frames_host, thr, seconds=10.0, threads=None):
                                  "frames": n1, "seconds": dt0, "rows": int(rows.shape[0])}
 
 
+def workload_runs(ptb, torch, steps=3, warmup=3):
+    """The other named workloads, device-resident through PTB_LocalizationDevice, each timed with CUDA events over
+    `steps` steps after `warmup`: C1 200 x 256^2 (MLE mode 6, 7x7), C3 1000 x 512^2 astigmatic (mode 7, 11x11), C4
+    1500 x 512^2 with 0-1500 emitters per frame and a 25 x 25 x 121 cubic-spline PSF table (mode 8, 13x13)."""
+    import spline_table
+    import synth
+    p8 = spline_table.fit_params(roi=13, sx=25, sy=25, sz=121, dz_nm=10.0, distortion=0.2, seed=9)
+    mle8 = np.concatenate([p8[:5], [100.0, 2.0, 20.0, 0.0], p8[5:]])
+    out = {}
+    for name, fit, params, roi in (("c1", 6, PARAMS_BY_MODE[6], 7), ("c3", 7, MLE7_PARAMS, 11), ("c4", 8, mle8, 13)):
+        d_in, _ = synth.stack_cuda(name, seed=4242)
+        z, h, w = d_in.shape
+        thr = mad_threshold_gpu(ptb, d_in[0].cpu().numpy().view(np.uint16))
+        cap = PER_PLANE * z * 18
+        d_out = torch.empty(cap, dtype=torch.float64, device="cuda")
+        stream = torch.cuda.current_stream()
+
+        def step():
+            return ptb.localization_device(d_in.data_ptr(), d_out.data_ptr(), cap, (z, h, w), thr, RATIO, fit, params,
+                                           stream.cuda_stream)
+
+        for _ in range(warmup):
+            n = step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            n = step()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        rows = n // 18
+        out[name] = {"frames": z, "height": h, "width": w, "fit_mode": fit, "roi": roi, "localizations_per_step": int(rows),
+                     "ms_per_step": ms, "localizations_per_s": rows / (ms / 1000.0), "frames_per_s": z / (ms / 1000.0)}
+        del d_in, d_out
+        torch.cuda.empty_cache()
+    return out
+
+
 TRACK_DISTANCE = 5.0  # maxDistance of the reference's tracking tests (Tests_CPU/test_tr_Tracks.cpp:262)
 
 
@@ -305,6 +344,7 @@ def main():
     ap.add_argument("--fit", type=int, default=None, help="fit mode (default: %d)" % FIT_MODE)
     ap.add_argument("--no-serving", action="store_true", help="skip the C5 serving mix")
     ap.add_argument("--no-tracking", action="store_true", help="skip tracking the benchmark's localizations")
+    ap.add_argument("--no-workloads", action="store_true", help="skip the C1, C3 and C4 workloads")
     ap.add_argument("--serve-requests", type=int, default=40)
     args = ap.parse_args()
     import torch
@@ -474,6 +514,9 @@ def main():
     tracking = None
     if rank == 0 and world == 1 and not args.no_tracking:
         tracking = tracking_run(ptb, torch, d_out, int(rows))
+    workloads = None
+    if rank == 0 and world == 1 and not args.no_workloads:
+        workloads = workload_runs(ptb, torch)
 
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
@@ -504,7 +547,8 @@ def main():
                         # host -> device rate over the call (the frames cross PCIe once; the link is the e2e bound)
                         "h2d_gbs": h2d_bytes / (float(np.mean(e2e_ms)) / 1000.0) / 1e9 if e2e_ms else None,
                         "h2d_link_gbs": link_gbs},
-                "gpu_launches": int(launches), "clocks": clk, "serving": serving, "tracking": tracking}
+                "gpu_launches": int(launches), "clocks": clk, "serving": serving, "tracking": tracking,
+                "workloads": workloads}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
