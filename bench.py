@@ -534,7 +534,7 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": ("f32 (LM and Newton polish; f64 Cholesky fallback, axial pre-scan, likelihood, CRLB)" if FIT_MODE >= 6 else
+                "dtype": ("f32 (axial pre-scan, LM and Newton polish; f64 Cholesky fallback, Fisher information, CRLB)" if FIT_MODE >= 6 else
                           "f64" if args.precision != 1 else "f32 (f64 re-fit)"),
                 "data": "synthetic (seeded, generated on the GPU; no public dataset)",
                 "config": dict(config, fit_precision=args.precision),

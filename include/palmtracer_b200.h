@@ -158,8 +158,9 @@ PTB_API int PTB_SetProfiling(int enable);
 PTB_API void PTB_StageTimes(double* ms, uint64_t* launches, int n);
 
 /* Model evaluations of fit modes 6-8 counted while profiling is enabled (diagnostics): [0] FP32 evaluations of the
- * Levenberg-Marquardt iterations, [1] FP32 evaluations of the Newton polish, [2] FP64 evaluations (axial pre-scan,
- * final likelihood and Fisher information); one evaluation visits every pixel of one ROI. [3] FP32 Cholesky
+ * Levenberg-Marquardt iterations, [1] FP32 evaluations of the Newton polish (with the rare Fisher-scoring fallbacks),
+ * [2] evaluations of the initial axial pre-scan (FP32) and of the final Fisher information (FP64); one evaluation
+ * visits every pixel of one ROI. [3] FP32 Cholesky
  * factorisations redone in FP64 (ill-conditioned or failed), counted always. Copies up to n totals into counts,
  * then resets them. */
 PTB_API void PTB_MleEvaluations(uint64_t* counts, int n);

@@ -1,24 +1,24 @@
 // Poisson maximum-likelihood fits (modes 6 Gaussian, 7 astigmatic 3D, 8 cubic-spline 3D) of (bg, I, x, y, s),
 // s = sigma (mode 6), z in nm (mode 7) or the spline's z coordinate (mode 8). No counterpart in the reference; the
 // model maths and the FP64 oracle are in oracle/pt_oracle.cpp (MleFit). This file follows it: the same initial
-// values, bounds and FP64 axial pre-scan, the same damped Fisher-scoring LM on the Poisson deviance (its step-size
-// stop rule one decade looser, see StepSmall), then Newton steps on the exact Hessian of the deviance, parameters on
-// active bounds held throughout, and the CRLB from the Fisher information at the final point.
+// values, bounds and axial pre-scan (here in FP32), the same damped Fisher-scoring LM on the Poisson deviance (its
+// step-size stop rule one decade looser, see StepSmall), then Newton steps on the exact Hessian of the deviance,
+// parameters on active bounds held throughout, and the CRLB from the Fisher information at the final point.
 //
 // Precision: the LM iterations and the Newton polish run in FP32, with the hardware approximations of exp and log
 // (__expf: a few ulp; __logf: absolute error about 2^-21 near 1) and erff; the per-pixel logarithm of the deviance
 // had been a fifth of the LM's time. Each 5x5 system is factored by an FP32 Cholesky;
 // when a pivot is not positive or the pivot ratio min(L_ii^2 / A_ii) falls below 1e-5 the same system is
-// re-factored in FP64. The initial axial pre-scan (a handful of deviance evaluations that choose the starting basin)
-// and the Fisher information behind the CRLB are computed in FP64 (the final point's deviance is not part of the
-// output, so the final pass does not form it). The oracle
+// re-factored in FP64. The Fisher information behind the CRLB is computed in FP64 (the final point's deviance is not
+// part of the output, so the final pass does not form it); the initial axial pre-scan, a handful of deviance
+// evaluations that choose the starting basin, runs in FP32 like the LM. The oracle
 // polishes in FP64 to a 1e-10 relative step; the FP32 polish stops at a 1e-6 relative step (the FP32 resolution of
 // the deviance), well inside the stated tolerance of 1e-3 px and 1e-4 relative photons.
 //
 // Two mappings, chosen per (mode, ROI) by the autotuner in engine.cu:
 //   * thread per ROI, four launches that hand their state over in the output rows (columns 0-4 theta, column 5 a
 //     status) so that no extra device memory is needed:
-//       MleInitKernel   initial values and FP64 axial pre-scan;
+//       MleInitKernel   initial values and axial pre-scan;
 //       MleLmKernel     persistent FP32 LM: every warp owns a contiguous range of candidates and each lane takes the
 //                       next candidate of the range as soon as its own converges, so a lane never idles while the
 //                       other 31 iterate; ROI photons and the column erf factors are staged per lane in shared memory;
@@ -61,7 +61,6 @@ template <> __device__ __forceinline__ float Ex<float>(float x) { return __expf(
 template <> __device__ __forceinline__ double Ex<double>(double x) { return exp(x); }
 template <typename T> __device__ __forceinline__ T Ln(T x);
 template <> __device__ __forceinline__ float Ln<float>(float x) { return __logf(x); }  // hardware lg2 based
-template <> __device__ __forceinline__ double Ln<double>(double x) { return log(x); }
 
 // Division in the per-pixel sums: FP32 with the hardware approximation (divisors here are photon counts and model
 // values, far inside its range), FP64 exact.
@@ -629,9 +628,11 @@ __device__ __forceinline__ Pix MakePix(const MleParams& mp, const uint16_t* base
 }
 
 // Initial values (oracle MleFit): bg = min photons (>= 1e-3), I = photons above bg (>= 1), x, y = candidate, s =
-// sigma0 (mode 6) or the best of an FP64 deviance scan of the axial range (16 points for mode 7, 8 for mode 8).
+// sigma0 (mode 6) or the best of a deviance scan of the axial range (16 points for mode 7, 8 for mode 8). The oracle
+// scans in FP64; here the scan runs in FP32 like the LM it starts (its choice differs only where two grid points'
+// deviances agree to FP32 rounding, and the LM then descends into the same basin). xt, yt: FP32 factor tables.
 template <int MODEL, int L>
-__device__ int InitTheta(const MleParams& mp, const Pix& px, const RoiAt& r, double t[5], FacTab<double> xt, FacTab<double> yt)
+__device__ int InitTheta(const MleParams& mp, const Pix& px, const RoiAt& r, double t[5], FacTab<float> xt, FacTab<float> yt)
 {
 	int evals = 0;
 	const int gl = L == 1 ? 0 : (threadIdx.x & 31);
@@ -658,12 +659,14 @@ __device__ int InitTheta(const MleParams& mp, const Pix& px, const RoiAt& r, dou
 	if (MODEL == 6) { t[4] = mp.sigma0; }
 	else {
 		const int ns = MODEL == 7 ? 16 : 8;
-		double best = 1e300, bz = 0.5 * (lo[4] + hi[4]);
+		float best = __int_as_float(0x7f800000), tf[5] = {float(t[0]), float(t[1]), float(t[2]), float(t[3]), 0.f};
+		double bz = 0.5 * (lo[4] + hi[4]);
 		for (int s = 0; s < ns; ++s) {
-			t[4] = lo[4] + (hi[4] - lo[4]) * (s + 0.5) / ns;
-			const double D = Normal<double, MODEL, L, kDevOnly>(mp, px, t, nullptr, nullptr, nullptr, xt, yt);
+			const double z = lo[4] + (hi[4] - lo[4]) * (s + 0.5) / ns;
+			tf[4] = float(z);
+			const float D = Normal<float, MODEL, L, kDevOnly>(mp, px, tf, nullptr, nullptr, nullptr, xt, yt);
 			++evals;
-			if (D < best) { best = D; bz = t[4]; }
+			if (D < best) { best = D; bz = z; }
 		}
 		t[4] = bz;
 	}
@@ -788,14 +791,14 @@ __device__ __forceinline__ uint32_t CandCount(const uint32_t* nptr, uint32_t nco
 // ---------------------------------------------------------------------------------------------------------------
 // Thread per ROI.
 
-// Initial values; shared memory: per thread the FP64 column values of the axial pre-scan (roi doubles).
+// Initial values; shared memory: per thread the FP32 column factors of the axial pre-scan (roi floats).
 template <int MODEL>
 __global__ void __launch_bounds__(kThreads) MleInitKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
                                                           const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
                                                           MleParams mp, double* rows)
 {
 	extern __shared__ __align__(16) unsigned char smem[];
-	const FacTab<double> xt{reinterpret_cast<double*>(smem) + threadIdx.x, static_cast<int>(blockDim.x)};
+	const FacTab<float> xt{reinterpret_cast<float*>(smem) + threadIdx.x, static_cast<int>(blockDim.x)};
 	const uint32_t n = CandCount(nptr, nconst);
 	unsigned long long evals = 0;
 	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -1130,7 +1133,7 @@ __global__ void __launch_bounds__(kThreads) MleWarpKernel(const uint16_t* __rest
 			continue;
 		}
 		Pix px = MakePix(mp, r.base, W, nullptr, 0);
-		ev[2] += InitTheta<MODEL, 32>(mp, px, r, t, xt64, yt64);
+		ev[2] += InitTheta<MODEL, 32>(mp, px, r, t, xt32, yt32);
 		for (int q = lane; q < mp.n; q += 32) {
 			const int i = q / mp.roi, j = q - i * mp.roi;
 			ws.photons[q] = fmaxf((float(__ldg(r.base + i * W + j)) - px.off32) * px.inv32, 0.f);
@@ -1230,7 +1233,7 @@ bool LaunchThreadPerRoi(const uint16_t* img, int H, int W, long long N, const Ca
 {
 	const int sms = SmCount();
 	const uint32_t blocks = std::min<uint32_t>((std::max<uint32_t>(cap, 1) + kThreads - 1) / kThreads, static_cast<uint32_t>(sms) * 32u);
-	const size_t initBytes = static_cast<size_t>(mp.roi) * sizeof(double) * kThreads;
+	const size_t initBytes = static_cast<size_t>(mp.roi) * sizeof(float) * kThreads;
 	const size_t lmBytes = static_cast<size_t>(mp.n + 3 * mp.roi) * sizeof(float) * kThreads;
 	const size_t polishBytes = static_cast<size_t>(mp.n + 6 * mp.roi) * sizeof(float) * kThreads;
 	const size_t finalBytes = static_cast<size_t>(3 * mp.roi) * sizeof(double) * kThreads;

@@ -205,11 +205,12 @@ def stage_times():
 
 
 def mle_evaluations():
-    """{"lm": FP32 LM evaluations, "polish": FP32 polish evaluations, "fp64": FP64 evaluations} counted while
-    profiling was on (modes 6-8), and "fp64_cholesky": FP32 Cholesky solves redone in FP64, since the last call."""
+    """{"lm": FP32 LM evaluations, "polish": FP32 polish evaluations, "init_final": axial pre-scan (FP32) and final
+    Fisher (FP64) evaluations} counted while profiling was on (modes 6-8), and "fp64_cholesky": FP32 Cholesky solves
+    redone in FP64, since the last call."""
     out = np.zeros(4, dtype=np.uint64)
     load().PTB_MleEvaluations(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 4)
-    return {"lm": int(out[0]), "polish": int(out[1]), "fp64": int(out[2]), "fp64_cholesky": int(out[3])}
+    return {"lm": int(out[0]), "polish": int(out[1]), "init_final": int(out[2]), "fp64_cholesky": int(out[3])}
 
 
 def tracking(points, max_distance):
