@@ -619,8 +619,9 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 	if (!Reserve(H, W, B, rowsCap, slots)) { return -1; }
 	char* poolOf[2] = {static_cast<char*>(pool_), static_cast<char*>(pool1_)};
 	const size_t N = static_cast<size_t>(H) * W;
-	// chunk schedule: B frames each; with host input the last chunk is split so that at most about B / 8 frames
-	// remain to compute after the final copy-in (the copy-in, not the compute, is then the critical path)
+	// chunk schedule: B frames each; with host input the first and the last chunks are split so that compute starts
+	// after a copy-in of about B / 8 frames and at most about B / 8 frames remain to compute after the final one
+	// (the copy-in, not the compute, is then the critical path at both ends)
 	std::vector<uint64_t> first, count;
 	for (uint64_t z0 = 0; z0 < planes; z0 += B) {
 		first.push_back(z0);
@@ -632,6 +633,11 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 		count.back() = last - tail;
 		first.push_back(first.back() + last - tail);
 		count.push_back(tail);
+	}
+	if (!inputOnDevice && first.size() > 2 && count.front() > tail) {
+		count.insert(count.begin() + 1, count.front() - tail);
+		first.insert(first.begin() + 1, tail);
+		count.front() = tail;
 	}
 	const uint64_t chunks = first.size();
 	const size_t slotBytes = N * B * sizeof(uint16_t);

@@ -45,7 +45,7 @@ def _one_chunk(lib, s, thr, fit, params):
     return lib.localization(s, thr, 0.0, fit, params)
 
 
-@pytest.mark.parametrize("budget_mb", ["8", "30"])  # 1 frame per chunk; 3 per chunk with the last chunk split (3, 3, 2, 1)
+@pytest.mark.parametrize("budget_mb", ["8", "30"])  # 1 frame per chunk; 3 per chunk, first and last split (1, 2, 3, 2, 1)
 def test_many_chunks_match_one_chunk(lib, orc, tmp_path, monkeypatch, budget_mb):
     import synth
     monkeypatch.setenv("PTB_MLE_LANES", "1")
