@@ -113,6 +113,15 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def over_ranks(dist, torch, total_ms, rows, device):
+    """Whole-job figures of a multi-rank run (one process per GPU, each on its own stack): the slowest rank's timed
+    milliseconds and the rows of all ranks. Every rank takes this one collective at the same point."""
+    t = torch.tensor([float(total_ms), float(rows)], device=device, dtype=torch.float64)
+    allt = [torch.zeros_like(t) for _ in range(dist.get_world_size())]
+    dist.all_gather(allt, t)
+    return max(float(x[0]) for x in allt), sum(float(x[1]) for x in allt)
+
+
 def mad_threshold_gpu(lib, frame):
     import synth
     w1 = lib.wavelett(frame, 2)[0]
@@ -355,7 +364,7 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=180))
     torch.cuda.set_device(local)
     import synth
     import ptb
@@ -434,11 +443,7 @@ def main():
     rows = counts[-1] // 18
     total_ms = float(step_ms.sum())
     if world > 1:
-        t = torch.tensor([total_ms, float(rows)], device="cuda", dtype=torch.float64)
-        allt = [torch.zeros_like(t) for _ in range(world)]
-        dist.all_gather(allt, t)
-        total_ms = max(float(x[0]) for x in allt)
-        rows_all = sum(float(x[1]) for x in allt)
+        total_ms, rows_all = over_ranks(dist, torch, total_ms, rows, "cuda")
     else:
         rows_all = float(rows)
     value = rows_all * args.steps / (total_ms / 1000.0)
