@@ -368,7 +368,8 @@ void Engine::ChunkPlan(int H, int W, uint64_t planes, uint32_t maxPoints, int& B
 {
 	B = ChunkFrames(H, W, planes, maxPoints, budget_);
 	slots = 1;
-	if (static_cast<uint64_t>(B) < planes) {
+	static const int maxSlots = [] { const char* e = std::getenv("PTB_CHUNK_SLOTS"); return e ? std::atoi(e) : 2; }();
+	if (static_cast<uint64_t>(B) < planes && maxSlots >= 2) {
 		B = ChunkFrames(H, W, planes, maxPoints, budget_ / 2);
 		slots = 2;
 	}
