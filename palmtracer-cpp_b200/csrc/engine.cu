@@ -609,7 +609,7 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 	}
 	if (!Init()) { return -1; }
 	FitParams fp;
-	std::vector<double> spline;
+	std::vector<double>& spline = splineIn_;
 	if (!ParseFitParams(fit, fitParams, fp, spline)) { return -1; }
 	if (!UploadSpline(fp, spline)) { return -1; }
 	const int H = static_cast<int>(height), W = static_cast<int>(width);
@@ -821,9 +821,19 @@ bool Engine::UploadSpline(FitParams& fp, const std::vector<double>& spline)
 		fp.mle.queue = static_cast<unsigned int*>(fallbacks_) + 1;
 		fp.lanes = EnvLanes();  // 0: chosen per chunk by the autotuner
 	}
+	if (fp.mode != kMleSpline && fp.mode != kSplineEmccd) { return true; }
+	// the same table as the last upload (a stack fitted chunk by chunk, or call after call): reuse the device copy
+	const bool same = spline_ && splineCacheMode_ == fp.mode && splineCache_.size() == spline.size() &&
+	                  std::memcmp(splineCache_.data(), spline.data(), spline.size() * sizeof(double)) == 0;
+	if (!same) { splineCacheMode_ = -1; }  // the device copy is about to change: no longer the cached table
 	if (fp.mode == kMleSpline) {
 		// cell-major copies of the [64][cell] table: FP64 first, then FP32
 		const size_t cells = static_cast<size_t>(fp.splineSize);
+		if (same) {
+			fp.mle.table64 = static_cast<const double*>(spline_);
+			fp.mle.table = reinterpret_cast<const float*>(static_cast<const char*>(spline_) + cells * 64 * sizeof(double));
+			return true;
+		}
 		std::vector<double> aos64(cells * 64);
 		std::vector<float> aos32(cells * 64);
 		for (size_t i = 0; i < 64; ++i) {
@@ -845,11 +855,16 @@ bool Engine::UploadSpline(FitParams& fp, const std::vector<double>& spline)
 		if (!PTB_CUDA(cudaStreamSynchronize(stream_))) { return false; }
 		fp.mle.table64 = reinterpret_cast<const double*>(base);
 		fp.mle.table = reinterpret_cast<const float*>(base + bytes64);
+		splineCache_ = spline;
+		splineCacheMode_ = fp.mode;
 		return true;
 	}
-	if (fp.mode != kSplineEmccd) { return true; }
 	// cell-major copy of the reference's [64][cell] table: one pixel's 64 coefficients become contiguous
 	const size_t cells = static_cast<size_t>(fp.splineSize);
+	if (same) {
+		fp.coeffs = static_cast<const double*>(spline_);
+		return true;
+	}
 	std::vector<double> aos(cells * 64);
 	for (size_t i = 0; i < 64; ++i) {
 		for (size_t c = 0; c < cells; ++c) { aos[c * 64 + i] = spline[i * cells + c]; }
@@ -863,6 +878,8 @@ bool Engine::UploadSpline(FitParams& fp, const std::vector<double>& spline)
 	if (!PTB_CUDA(cudaMemcpyAsync(spline_, aos.data(), bytes, cudaMemcpyHostToDevice, stream_))) { return false; }
 	if (!PTB_CUDA(cudaStreamSynchronize(stream_))) { return false; }
 	fp.coeffs = static_cast<const double*>(spline_);
+	splineCache_ = spline;
+	splineCacheMode_ = fp.mode;
 	return true;
 }
 
@@ -872,7 +889,7 @@ long long Engine::FitPositions(const uint16_t* input, const double* positions, u
 	if (nPoints == 0) { return 0; }
 	if (!Init()) { return -1; }
 	FitParams fp;
-	std::vector<double> spline;
+	std::vector<double>& spline = splineIn_;
 	if (!ParseFitParams(fit, fitParams, fp, spline)) { return -1; }
 	if (!UploadSpline(fp, spline)) { return -1; }
 	const size_t N = static_cast<size_t>(height) * width;

@@ -134,6 +134,9 @@ private:
 	void* hostStage_ = nullptr;               // pinned frame staging of page sources (two slots)
 	size_t hostStageBytes_ = 0;
 	void* spline_ = nullptr;
+	std::vector<double> splineIn_;            // the call's spline table as given (reused between calls)
+	std::vector<double> splineCache_;         // the table behind spline_ (its upload is skipped when unchanged)
+	int splineCacheMode_ = -1;
 	void* fallbacks_ = nullptr;
 	std::vector<std::pair<int, int>> tuned_;  // ((mode * 64 + roi) * 64 + chunk size class) -> lanes per ROI
 	size_t splineBytes_ = 0;

@@ -249,6 +249,29 @@ def test_spline_mode5_fitting_export(lib, orc, stacks):
     assert np.allclose(a, b, rtol=1e-6, atol=1e-6, equal_nan=True)
 
 
+def test_spline_table_reuse_follows_changes(lib, orc, stacks):
+    """The device copy of the spline table is reused while the caller's table is unchanged: a changed table, a
+    changed mode and a return to the first table must each give the oracle's rows."""
+    import spline_table
+    t1 = spline_table.fit_params(roi=7, sx=11, sy=11, sz=21, dz_nm=40.0, distortion=0.3, seed=4)
+    t2 = t1.copy()
+    t2[5:] *= 1.25  # same shape, other coefficients
+    st = stacks["stack"][:2]
+    first = None
+    for params in (t1, t1, t2, t1):
+        a = lib.localization(st, 103.6, 0.0, 5, params)
+        b = orc.localization(st, 103.6, 0.0, 5, params)
+        assert a.shape == b.shape and a.shape[0] > 0
+        assert match_rows(a, b, atol=1e-6, rtol=1e-6)[0] == 0
+        if first is None:
+            first = a
+    assert np.array_equal(first, a)
+    p8 = _mle8_params(roi=13)
+    lib.localization(st, 103.6, 0.0, 8, p8)  # the other spline mode in between
+    a = lib.localization(st, 103.6, 0.0, 5, t1)
+    assert np.array_equal(first, a)
+
+
 # ---- maximum-likelihood modes 6-8 (no reference counterpart: FP64 oracle from the model maths) -------------------
 MLE6 = np.array([7.0, 1.3, 100.0, 2.0, 20, 0.0])
 ASTIG = [150.0, 400.0, 0.05, 0.0, 1.3 * 160, -150.0, 400.0, -0.05, 0.0, 1.3 * 160]
