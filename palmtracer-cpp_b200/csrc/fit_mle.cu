@@ -677,6 +677,21 @@ __device__ int InitTheta(const MleParams& mp, const Pix& px, const RoiAt& r, dou
 	return evals;
 }
 
+// A Newton step below the polish's 1e-6 relative stop is applied without evaluating the deviance there: the
+// evaluation could only confirm a change below the FP32 resolution of the parameters.
+template <int MODEL>
+__device__ __forceinline__ bool ApplyIfTiny(const MleParams& mp, float x0, float y0, float th[5], const float dt[5])
+{
+	float step = 0.f;
+	#pragma unroll
+	for (int a = 0; a < 5; ++a) { step = fmaxf(step, fabsf(dt[a]) / fmaxf(fabsf(th[a]), 1.f)); }
+	if (!(step < 1e-6f)) { return false; }
+	#pragma unroll
+	for (int a = 0; a < 5; ++a) { th[a] += dt[a]; }
+	Clamp32<MODEL>(mp, x0, y0, th);
+	return true;
+}
+
 // FP32 Newton steps on the exact Hessian of the deviance (NewtonDirection), at most 6; a step that the deviance does
 // not accept (PolishAccept) is halved up to three times; stops at a 1e-6 relative step (the oracle: FP64, 1e-10).
 template <int MODEL, int L>
@@ -694,6 +709,7 @@ __device__ int Polish(const MleParams& mp, const Pix& px, float x0, float y0, fl
 			++evals;
 		};
 		if (!NewtonDirection<MODEL>(mp, x0, y0, th, G, Hm, dt, fisher)) { break; }
+		if (ApplyIfTiny<MODEL>(mp, x0, y0, th, dt)) { break; }
 		bool accepted = false;
 		float Gt[5], Ht[15], Dt = 0.f;
 		for (int hv = 0; hv < 4 && !accepted; ++hv) {
@@ -1061,7 +1077,7 @@ __global__ void __launch_bounds__(kThreads) MlePolishKernel(const uint16_t* __re
 						Normal<float, MODEL, 1, kFisher>(mp, px, th, Gf, Hf, nullptr, xt, xt);
 						++evals;
 					};
-					finish = !NewtonDirection<MODEL>(mp, x0, y0, th, G, Hm, dt, fisher);
+					finish = !NewtonDirection<MODEL>(mp, x0, y0, th, G, Hm, dt, fisher) || ApplyIfTiny<MODEL>(mp, x0, y0, th, dt);
 				}
 			}
 		}
