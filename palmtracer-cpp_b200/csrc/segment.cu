@@ -301,18 +301,6 @@ __global__ void SeedLabel(Workspace ws)
 	}
 }
 
-// Single-region components are labelled outright; flooded pixels of groups start unlabelled (seeds keep theirs).
-__global__ void LabelDomain(Workspace ws, int strict)
-{
-	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
-	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-		const uint32_t p = ws.dom[k];
-		if (ws.code[p] & kSeed) { continue; }
-		const uint32_t c = CompOf(ws.par, p);
-		ws.lab[p] = (!strict && ws.compNRoot[c] == 1) ? ws.compRegion[c] + 1 : 0u;
-	}
-}
-
 // Groups (fast mode): components with two or more regions. Sizes go to the offset arrays, scanned next.
 __global__ void GroupEnumerate(Workspace ws)
 {
@@ -356,12 +344,26 @@ __device__ __forceinline__ int GroupOf(const Workspace& ws, uint32_t p, int stri
 	return ws.compNRoot[c] >= 2 ? static_cast<int>(ws.compRegion[c]) : -1;
 }
 
+// Domain pixels: labels of the non-seed pixels (single-region components take their region outright; flooded
+// pixels of groups start unlabelled, seeds keep theirs) and the pixel lists of the groups. compRegion holds the
+// region of a single-region component and the group index of a multi-region one.
 __global__ void GroupScatter(Workspace ws, int strict)
 {
 	const uint32_t nd = min(ws.cnt->ndom, ws.capDom);
 	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nd; k += gridDim.x * blockDim.x) {
 		const uint32_t p = ws.dom[k];
-		const int m = GroupOf(ws, p, strict);
+		const bool seed = (ws.code[p] & kSeed) != 0;
+		int m;
+		if (strict) {
+			if (!seed) { ws.lab[p] = 0u; }
+			m = Decompose(p, ws.g).f;
+		}
+		else {
+			const uint32_t c = CompOf(ws.par, p);
+			const uint32_t nroot = ws.compNRoot[c], r = ws.compRegion[c];
+			if (!seed) { ws.lab[p] = nroot == 1 ? r + 1 : 0u; }
+			m = nroot >= 2 ? static_cast<int>(r) : -1;
+		}
 		if (m < 0) { continue; }
 		ws.gPix[ws.gOff[m] + atomicAdd(ws.gCurPix + m, 1u)] = p;
 	}
@@ -765,8 +767,7 @@ bool LaunchSegment(const Workspace& ws, double ratio, int strict, uint32_t maxPo
 	const uint32_t rows = static_cast<uint32_t>(g.B) * static_cast<uint32_t>(g.H);
 	ok = ok && ExclusiveScan(ws.rowcnt, nullptr, rows, rows, ws.scanBlock, &ws.cnt->nregion, st);
 	SeedLabel<<<kGrid, kThreads, 0, st>>>(ws);
-	LabelDomain<<<kGrid, kThreads, 0, st>>>(ws, strict);
-	CountLaunch(2);
+	CountLaunch();
 	ok = ok && PTB_LAUNCHED();
 	const uint32_t groupsStrict = strict ? static_cast<uint32_t>(g.B) : 0u;
 	if (strict) {
