@@ -283,12 +283,8 @@ bool Engine::Init()
 	if (!PTB_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming))) { return false; }
 	if (!PTB_CUDA(cudaMallocHost(&hostCnt_, 2 * sizeof(Counters)))) { return false; }
 	if (!PTB_CUDA(cudaMalloc(&rowBase_, sizeof(unsigned long long)))) { return false; }
-	for (int k = 0; k < 2; ++k) {
-		if (!PTB_CUDA(cudaEventCreateWithFlags(&h2d_[k], cudaEventDisableTiming)) ||
-		    !PTB_CUDA(cudaEventCreateWithFlags(&done_[k], cudaEventDisableTiming)) ||
-		    !PTB_CUDA(cudaEventCreateWithFlags(&d2h_[k], cudaEventDisableTiming))) {
-			return false;
-		}
+	for (cudaEvent_t* e : {&h2d_[0], &h2d_[1], &h2d_[2], &imgFree_[0], &imgFree_[1], &imgFree_[2], &done_[0], &done_[1], &d2h_[0], &d2h_[1]}) {
+		if (!PTB_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming))) { return false; }
 	}
 	for (auto& e : ev_) {
 		if (!PTB_CUDA(cudaEventCreate(&e))) { return false; }
@@ -586,6 +582,36 @@ long long Engine::CompleteChunk(int slot, uint32_t* truncatedFrames)
 	return c.nfit;
 }
 
+// Frame counts of the chunks of a stack of `planes` frames, at most B each. Device input: B frames each, the last one
+// shorter. Host input, where the copy-in is the critical path: the stack's end is cut into chunks that shrink by a
+// factor of about 0.7 down to about B / 16 frames, so that each chunk computes while the next, smaller one is copied
+// in and little compute is left after the final copy-in; the rest is cut into equal chunks of at most B, of which
+// the first is split so that compute starts after a copy-in of about B / 8 frames.
+static void ChunkSchedule(uint64_t planes, uint64_t B, bool hostInput, std::vector<uint64_t>& count)
+{
+	count.clear();
+	if (!hostInput || planes <= B) {
+		for (uint64_t z0 = 0; z0 < planes; z0 += B) { count.push_back(std::min<uint64_t>(B, planes - z0)); }
+		return;
+	}
+	std::vector<uint64_t> back;  // the end, last chunk first
+	uint64_t left = planes;
+	for (uint64_t t = std::max<uint64_t>(1, B / 16); left > 0 && t < B; t = std::max(t + 1, t * 10 / 7)) {
+		back.push_back(std::min(t, left));
+		left -= back.back();
+	}
+	if (left > 0) {
+		const uint64_t n = (left + B - 1) / B;
+		for (uint64_t k = 0; k < n; ++k) { count.push_back(left / n + (k < left % n ? 1 : 0)); }
+		const uint64_t head = std::max<uint64_t>(1, B / 8);
+		if (count.front() > head) {
+			count.insert(count.begin() + 1, count.front() - head);
+			count.front() = head;
+		}
+	}
+	count.insert(count.end(), back.rbegin(), back.rend());
+}
+
 // A stack that fits the budget runs as one chunk. A longer one runs as chunks of half the budget on two chunk slots,
 // each with its own compute stream and workspace, so that one chunk's serial tail (the last fits, the ordering)
 // overlaps the next chunk's detection. With host buffers, the input of chunk k + 1 is copied in on one copy stream and
@@ -620,59 +646,48 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 	if (!Reserve(H, W, B, rowsCap, slots)) { return -1; }
 	char* poolOf[2] = {static_cast<char*>(pool_), static_cast<char*>(pool1_)};
 	const size_t N = static_cast<size_t>(H) * W;
-	// chunk schedule: B frames each; with host input the first and the last chunks are split so that compute starts
-	// after a copy-in of about B / 8 frames and at most about B / 8 frames remain to compute after the final one
-	// (the copy-in, not the compute, is then the critical path at both ends)
 	std::vector<uint64_t> first, count;
-	for (uint64_t z0 = 0; z0 < planes; z0 += B) {
-		first.push_back(z0);
-		count.push_back(std::min<uint64_t>(B, planes - z0));
-	}
-	const uint64_t tail = std::max<uint64_t>(1, static_cast<uint64_t>(B) / 8);
-	if (!inputOnDevice && first.size() > 1 && count.back() > tail) {
-		const uint64_t last = count.back();
-		count.back() = last - tail;
-		first.push_back(first.back() + last - tail);
-		count.push_back(tail);
-	}
-	if (!inputOnDevice && first.size() > 2 && count.front() > tail) {
-		count.insert(count.begin() + 1, count.front() - tail);
-		first.insert(first.begin() + 1, tail);
-		count.front() = tail;
-	}
+	ChunkSchedule(planes, static_cast<uint64_t>(B), !inputOnDevice, count);
+	for (uint64_t k = 0, z0 = 0; k < count.size(); z0 += count[k], ++k) { first.push_back(z0); }
 	const uint64_t chunks = first.size();
 	const size_t slotBytes = N * B * sizeof(uint16_t);
-	if (!inputOnDevice && !ReserveImage((chunks > 1 ? 2 : 1) * slotBytes)) { return -1; }
+	// host input: frames go through up to three device staging slots (chunk k in slot k % 3), so that a copy-in waits
+	// for the chunk three back, not for the one still computing beside the current one
+	const uint64_t imgSlots = std::min<uint64_t>(chunks, 3);
+	if (!inputOnDevice && !ReserveImage(imgSlots * slotBytes)) { return -1; }
 	if (source && hostStageBytes_ < (chunks > 1 ? 2 : 1) * slotBytes) {
 		if (hostStage_) { cudaFreeHost(hostStage_); hostStage_ = nullptr; hostStageBytes_ = 0; }
 		if (!PTB_CUDA(cudaMallocHost(&hostStage_, (chunks > 1 ? 2 : 1) * slotBytes))) { return -1; }
 		hostStageBytes_ = (chunks > 1 ? 2 : 1) * slotBytes;
 	}
-	// with two chunk slots, chunk k runs on slot k % 2 (its own stream and workspace); with host output its ordered
-	// rows stay in that workspace (where the chunk's own plan puts them) until copied out
+	// with two chunk slots, chunk k runs on chunk slot k % 2 (its own stream, workspace, counters and events), with one
+	// on slot 0; with host output its ordered rows stay in that workspace (where the chunk's own plan puts them) until
+	// copied out
 	double* outSlot[2] = {nullptr, nullptr};
-	auto imgSlot = [&](int slot) { return static_cast<uint16_t*>(img_) + (slot ? N * B : 0); };
+	auto chunkSlot = [&](uint64_t k) { return slots > 1 ? static_cast<int>(k & 1) : 0; };
+	auto imgSlotOf = [&](uint64_t k) { return static_cast<int>(k % imgSlots); };
+	auto imgSlot = [&](int slot) { return static_cast<uint16_t*>(img_) + N * B * slot; };
 	auto framesOf = [&](uint64_t k) { return static_cast<int>(count[k]); };
 	if (!PTB_CUDA(cudaMemsetAsync(rowBase_, 0, sizeof(unsigned long long), stream_))) { return -1; }
 	// the second compute stream starts after everything ordered before this call on the first (the caller's input)
 	if (slots > 1 && (!PTB_CUDA(cudaEventRecord(fork_, stream_)) || !PTB_CUDA(cudaStreamWaitEvent(stream1_, fork_, 0)))) {
 		return -1;
 	}
-	// input of chunk k into its slot; the slot's previous chunk (k - 2) must have finished reading it
+	// input of chunk k into its staging slot; the slot's previous chunk (k - imgSlots) must have finished reading it
 	auto copyIn = [&](uint64_t k) {
-		const int slot = static_cast<int>(k & 1);
+		const int slot = imgSlotOf(k);
 		const uint16_t* src = source ? nullptr : input + first[k] * N;
 		if (source) {
-			// the pinned slot's previous frames (chunk k - 2) must have reached the device before it is refilled
-			uint16_t* stage = static_cast<uint16_t*>(hostStage_) + (slot ? N * B : 0);
-			if (k >= 2 && !PTB_CUDA(cudaEventSynchronize(h2d_[slot]))) { return false; }
+			// the pinned host slot's previous frames (chunk k - 2) must have reached the device before it is refilled
+			uint16_t* stage = static_cast<uint16_t*>(hostStage_) + ((k & 1) ? N * B : 0);
+			if (k >= 2 && !PTB_CUDA(cudaEventSynchronize(h2d_[imgSlotOf(k - 2)]))) { return false; }
 			if (!(*source)(first[k], count[k], stage)) {
 				SetError("page source failed");
 				return false;
 			}
 			src = stage;
 		}
-		if (k >= 2 && !PTB_CUDA(cudaStreamWaitEvent(copy_, done_[slot], 0))) { return false; }
+		if (k >= imgSlots && !PTB_CUDA(cudaStreamWaitEvent(copy_, imgFree_[slot], 0))) { return false; }
 		if (!PTB_CUDA(cudaMemcpyAsync(imgSlot(slot), src, N * framesOf(k) * sizeof(uint16_t), cudaMemcpyHostToDevice, copy_))) {
 			return false;
 		}
@@ -682,7 +697,7 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 	uint32_t truncated = 0;
 	// waits for chunk k and, for host output, copies its rows out
 	auto complete = [&](uint64_t k) {
-		const int slot = static_cast<int>(k & 1);
+		const int slot = chunkSlot(k);
 		const long long n = CompleteChunk(slot, &truncated);
 		if (n < 0) { return false; }
 		if (!outputOnDevice && n > 0) {
@@ -695,24 +710,27 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 		rows += static_cast<unsigned long long>(n);
 		return true;
 	};
+	// one chunk slot: the previous chunk is completed (and its rows copied out of the shared workspace) before the
+	// next is enqueued; two: chunk k - 1 is completed after chunk k is enqueued
+	const bool serial = profiling_ || slots == 1;  // stage timing needs each chunk finished before the next starts
 	bool ok = inputOnDevice || copyIn(0);
 	for (uint64_t k = 0; ok && k < chunks; ++k) {
-		const int slot = static_cast<int>(k & 1);
-		const int ws = slots > 1 ? slot : 0;  // workspace and compute stream of this chunk
+		const int ws = chunkSlot(k);  // workspace, compute stream, counters and events of this chunk
 		const int b = framesOf(k);
 		PlanWorkspace(Ws(ws), H, W, b, rowsCap, poolOf[ws]);
-		const uint16_t* dImg = inputOnDevice ? input + first[k] * N : imgSlot(slot);
-		if (!inputOnDevice) { ok = PTB_CUDA(cudaStreamWaitEvent(St(ws), h2d_[slot], 0)); }
-		// the output slot of chunk k - 2 must be copied out before this chunk orders its rows into it
-		if (ok && !outputOnDevice && k >= 2) { ok = PTB_CUDA(cudaStreamWaitEvent(St(ws), d2h_[slot], 0)); }
-		outSlot[slot] = Ws(ws).sortedRows;
-		double* dOut = outputOnDevice ? output : outSlot[slot];
+		const uint16_t* dImg = inputOnDevice ? input + first[k] * N : imgSlot(imgSlotOf(k));
+		if (!inputOnDevice) { ok = PTB_CUDA(cudaStreamWaitEvent(St(ws), h2d_[imgSlotOf(k)], 0)); }
+		// the rows of the chunk slot's previous chunk must be copied out before this chunk orders its rows there
+		if (ok && !outputOnDevice && k >= static_cast<uint64_t>(slots)) { ok = PTB_CUDA(cudaStreamWaitEvent(St(ws), d2h_[ws], 0)); }
+		outSlot[ws] = Ws(ws).sortedRows;
+		double* dOut = outputOnDevice ? output : outSlot[ws];
 		ok = ok && EnqueueChunk(ws, dImg, H, W, b, thr, ratio, maxPoints, fp, dOut, outputOnDevice, first[k], slots > 1 && k > 0);
+		ok = ok && (inputOnDevice || PTB_CUDA(cudaEventRecord(imgFree_[imgSlotOf(k)], St(ws))));
 		if (ok && !inputOnDevice && k + 1 < chunks) { ok = copyIn(k + 1); }
-		if (ok && profiling_) { ok = complete(k); }  // stage timing needs each chunk finished before the next starts
+		if (ok && serial) { ok = complete(k); }
 		else if (ok && k >= 1) { ok = complete(k - 1); }
 	}
-	if (ok && !profiling_ && chunks > 0) { ok = complete(chunks - 1); }
+	if (ok && !serial && chunks > 0) { ok = complete(chunks - 1); }
 	// work ordered after this call on the first compute stream also follows the second's
 	if (ok && slots > 1) { ok = PTB_CUDA(cudaStreamWaitEvent(stream_, done_[1], 0)); }
 	ok = ok && PTB_CUDA(cudaStreamSynchronize(copy_)) && PTB_CUDA(cudaStreamSynchronize(copyOut_));

@@ -122,8 +122,9 @@ private:
 	Workspace ws1_{};                        // second chunk slot's workspace and pool
 	void* pool1_ = nullptr;
 	size_t pool1Bytes_ = 0;
-	cudaEvent_t h2d_[2] = {}, done_[2] = {}, d2h_[2] = {};  // per staging slot
-	Counters* hostCnt_ = nullptr;             // pinned, one per staging slot
+	cudaEvent_t h2d_[3] = {}, imgFree_[3] = {};  // per frame staging slot on the device: copied in, read by its chunk
+	cudaEvent_t done_[2] = {}, d2h_[2] = {};     // per chunk slot: chunk finished, its rows copied out
+	Counters* hostCnt_ = nullptr;             // pinned, one per chunk slot
 	unsigned long long* rowBase_ = nullptr;   // device: rows written by the earlier chunks of the current call
 	size_t budget_ = 0;
 	size_t fixedBudget_ = 0;

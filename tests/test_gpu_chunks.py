@@ -1,9 +1,11 @@
 """Chunked processing: a stack split into many chunks (small device-memory budget) gives the same rows as one chunk.
 
-With host buffers the library copies chunk k + 1 in and the rows of chunk k - 1 out while chunk k computes, using two
-staging slots, and numbers rows across chunks with a device-side count. A budget of a few MB forces about two frames
-per chunk, so every slot is reused several times; the rows (Id numbering included) must be bit-identical to a run
-that holds the whole stack in one chunk, through both the host-buffer and the device-buffer entry points.
+With host buffers the library copies chunk k + 1 in and the rows of chunk k - 1 out while chunk k computes, using three
+device staging slots for the frames and two chunk slots (stream, workspace) for the compute, and numbers rows across
+chunks with a device-side count. A budget of a few MB forces one to three frames per chunk, so every slot is reused
+several times; the rows (Id numbering included) must be bit-identical to a run that holds the whole stack in one
+chunk, through both the host-buffer and the device-buffer entry points. PTB_CHUNK_SLOTS=1 runs the chunks on one
+chunk slot, one after the other.
 """
 import os
 import subprocess
@@ -45,8 +47,9 @@ def _one_chunk(lib, s, thr, fit, params):
     return lib.localization(s, thr, 0.0, fit, params)
 
 
-@pytest.mark.parametrize("budget_mb", ["8", "30"])  # 1 frame per chunk; 3 per chunk, first and last split (1, 2, 3, 2, 1)
-def test_many_chunks_match_one_chunk(lib, orc, tmp_path, monkeypatch, budget_mb):
+# 8 MB: 1 frame per chunk; 30 MB: 3 per chunk, the first split and the end shrinking (1, 2, 3, 2, 1)
+@pytest.mark.parametrize("budget_mb,slots", [("8", "2"), ("30", "2"), ("8", "1"), ("30", "1")])
+def test_many_chunks_match_one_chunk(lib, orc, tmp_path, monkeypatch, budget_mb, slots):
     import synth
     monkeypatch.setenv("PTB_MLE_LANES", "1")
     s, _ = synth.stack("c1", frames=9, seed=77)
@@ -57,7 +60,7 @@ def test_many_chunks_match_one_chunk(lib, orc, tmp_path, monkeypatch, budget_mb)
     inp = tmp_path / "in.npz"
     outp = tmp_path / "out.npz"
     np.savez(inp, stack=s, thr=thr, fit_g=2, params_g=GAUSS_PARAMS, fit_m=6, params_m=MLE6)
-    env = dict(os.environ, PTB_WORKSPACE_MB=budget_mb, PTB_MLE_LANES="1")
+    env = dict(os.environ, PTB_WORKSPACE_MB=budget_mb, PTB_MLE_LANES="1", PTB_CHUNK_SLOTS=slots)
     r = subprocess.run([sys.executable, "-c", CHILD, ROOT, str(inp), str(outp)], env=env, capture_output=True, text=True,
                        timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
