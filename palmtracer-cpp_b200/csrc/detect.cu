@@ -130,6 +130,9 @@ __device__ __forceinline__ uint32_t Tap(uint32_t m2, uint32_t m1, uint32_t c, ui
 	return 6u * c + 4u * (m1 + p1) + (m2 + p2);
 }
 
+// Bits 0-3 of m to the low bits of bytes 0-3 (the shifted copies 0, 7, 14, 21 do not overlap, so nothing carries).
+__device__ __forceinline__ uint32_t Spread4(uint32_t m) { return (m * 0x00204081u) & 0x01010101u; }
+
 __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restrict__ img, Workspace ws, long long thrFixed)
 {
 	extern __shared__ __align__(16) unsigned char smemRaw[];
@@ -226,15 +229,25 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 		uint4* vp = reinterpret_cast<uint4*>(v1 + (q + 4) * kPV + 8 * m + 4);
 		const uint4 e = vp[0], g = vp[1];
 		const uint32_t v[8] = {e.x, e.y, e.z, e.w, g.x, g.y, g.z, g.w};
-		const int y = y0 + q - 1;
+		const int y = y0 + q - 1, xs = x0 + 8 * m - 1;
 		const bool rowIn = y >= 0 && y < H;
 		uint32_t o[8];
-		#pragma unroll
-		for (int k = 0; k < 8; ++k) {
-			const uint32_t v2 = Tap(u[k], u[k + 2], u[k + 4], u[k + 6], u[k + 8]);
-			const uint32_t v1s = v[k] << 8;
-			const int x = x0 + 8 * m - 1 + k;
-			o[k] = (rowIn && x >= 0 && x < W && v1s > v2) ? v1s - v2 : 0u;
+		if (rowIn && xs >= 0 && xs + 8 <= W) {
+			// all eight inside the frame: max(W1, 0) = max(V1 * 256, V2) - V2
+			#pragma unroll
+			for (int k = 0; k < 8; ++k) {
+				const uint32_t v2 = Tap(u[k], u[k + 2], u[k + 4], u[k + 6], u[k + 8]);
+				o[k] = max(v[k] << 8, v2) - v2;
+			}
+		}
+		else {
+			#pragma unroll
+			for (int k = 0; k < 8; ++k) {
+				const uint32_t v2 = Tap(u[k], u[k + 2], u[k + 4], u[k + 6], u[k + 8]);
+				const uint32_t v1s = v[k] << 8;
+				const int x = xs + k;
+				o[k] = (rowIn && x >= 0 && x < W && v1s > v2) ? v1s - v2 : 0u;
+			}
 		}
 		vp[0] = make_uint4(o[0], o[1], o[2], o[3]);
 		vp[1] = make_uint4(o[4], o[5], o[6], o[7]);
@@ -243,7 +256,6 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 	// E: domain and seeds, 8 pixels per task, two tasks per thread
 	const uint32_t thr = thrFixed <= 0 ? 0u : (thrFixed >= 0xffffffffll ? 0xffffffffu : static_cast<uint32_t>(thrFixed));
 	uint32_t dmask[2] = {0, 0}, smask[2] = {0, 0};
-	uint32_t val[2][8];
 	#pragma unroll
 	for (int h = 0; h < 2; ++h) {
 		const int task = tid + h * kThreads;
@@ -257,18 +269,18 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 			a[rr][4] = q.x; a[rr][5] = q.y; a[rr][6] = q.z; a[rr][7] = q.w;
 			a[rr][8] = r.x; a[rr][9] = r.y; a[rr][10] = r.z; a[rr][11] = r.w;
 		}
-		const int y = y0 + ty;
+		// 3 x 3 maximum as column maxima, then the maximum of three of them; a seed is not below the maximum of its
+		// window, which holds the pixel itself, so this equals "no neighbour strictly greater"
+		uint32_t cm[10];
+		#pragma unroll
+		for (int j = 0; j < 10; ++j) { cm[j] = __vimax3_u32(a[0][j], a[1][j], a[2][j]); }
+		const int inFrame = y0 + ty < H ? W - (x0 + 8 * m) : 0;  // pixels k < inFrame lie inside the frame
 		#pragma unroll
 		for (int k = 0; k < 8; ++k) {
-			const uint32_t mx = max(max(max(a[0][k], a[0][k + 1]), max(a[0][k + 2], a[1][k])),
-			                        max(max(a[1][k + 2], a[2][k]), max(a[2][k + 1], a[2][k + 2])));
 			const uint32_t v = a[1][k + 1];
-			val[h][k] = v;
-			const bool dom = y < H && x0 + 8 * m + k < W && v > thr;
-			if (dom) {
-				dmask[h] |= 1u << k;
-				if (v >= mx) { smask[h] |= 1u << k; }
-			}
+			const bool dom = k < inFrame && v > thr;
+			dmask[h] |= static_cast<uint32_t>(dom) << k;
+			smask[h] |= static_cast<uint32_t>(dom && v >= __vimax3_u32(cm[k], cm[k + 1], cm[k + 2])) << k;
 		}
 	}
 	// block-wide positions in the domain and seed lists: one atomic per list
@@ -302,29 +314,28 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 		const int y = y0 + ty, xb = x0 + 8 * m;
 		if (y >= H || xb >= W) { continue; }
 		const long long g = static_cast<long long>(f) * ws.g.N + static_cast<long long>(y) * W + xb;
-		unsigned long long packed = 0;
-		#pragma unroll
-		for (int k = 0; k < 8; ++k) {
-			const unsigned long long byte = ((dmask[h] >> k) & 1u ? kDomain : 0u) | ((smask[h] >> k) & 1u ? kSeed : 0u);
-			packed |= byte << (8 * k);
-		}
-		if (xb + 8 <= W && (g & 7) == 0) { *reinterpret_cast<unsigned long long*>(ws.code + g) = packed; }
+		// code bytes of the eight pixels: each mask bit spread to the low bit of its byte, times the flag
+		const uint32_t dm = dmask[h], sm = smask[h];
+		const uint32_t lo = Spread4(dm & 15u) * kDomain | Spread4(sm & 15u) * kSeed;
+		const uint32_t hi = Spread4(dm >> 4) * kDomain | Spread4(sm >> 4) * kSeed;
+		if (xb + 8 <= W && (g & 7) == 0) { *reinterpret_cast<uint2*>(ws.code + g) = make_uint2(lo, hi); }
 		else {
-			for (int k = 0; k < 8 && xb + k < W; ++k) { ws.code[g + k] = static_cast<uint8_t>(packed >> (8 * k)); }
+			for (int k = 0; k < 8 && xb + k < W; ++k) { ws.code[g + k] = static_cast<uint8_t>((k < 4 ? lo >> (8 * k) : hi >> (8 * k - 32))); }
 		}
-		#pragma unroll
-		for (int k = 0; k < 8; ++k) {
-			if ((dmask[h] >> k) & 1u) {
-				ws.w1[g + k] = static_cast<long long>(val[h][k]);
-				if (pd < ws.capDom) { ws.dom[pd] = static_cast<uint32_t>(g + k); }
-				else { atomicExch(&ws.cnt->overflow, 1u); }
-				++pd;
-			}
-			if ((smask[h] >> k) & 1u) {
-				if (ps < ws.capSeed) { ws.seeds[ps] = static_cast<uint32_t>(g + k); }
-				else { atomicExch(&ws.cnt->overflow, 1u); }
-				++ps;
-			}
+		// domain pixels (their W1 is still in shared memory) and seeds, lowest pixel first
+		const uint32_t* w1row = v1 + (ty + 5) * kPV + 8 * m + 5;
+		for (uint32_t b = dm; b; b &= b - 1u) {
+			const int k = __ffs(b) - 1;
+			ws.w1[g + k] = static_cast<long long>(w1row[k]);
+			if (pd < ws.capDom) { ws.dom[pd] = static_cast<uint32_t>(g + k); }
+			else { atomicExch(&ws.cnt->overflow, 1u); }
+			++pd;
+		}
+		for (uint32_t b = sm; b; b &= b - 1u) {
+			const int k = __ffs(b) - 1;
+			if (ps < ws.capSeed) { ws.seeds[ps] = static_cast<uint32_t>(g + k); }
+			else { atomicExch(&ws.cnt->overflow, 1u); }
+			++ps;
 		}
 	}
 }
