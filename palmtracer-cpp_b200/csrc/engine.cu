@@ -355,6 +355,8 @@ int Engine::ChunkFrames(int H, int W, uint64_t planes, uint32_t maxPoints, size_
 	B = std::max<long long>(1, std::min<long long>(B, static_cast<long long>(planes)));
 	// global pixel indices of a chunk stay below 2^31 (the top bit tags component ids)
 	B = std::min<long long>(B, std::max<long long>(1, ((1ll << 31) - 1) / std::max<long long>(N, 1)));
+	// the per-frame kernels (detection, wavelet planes, tile components) take the frame from grid.z
+	B = std::min<long long>(B, 65535);
 	return static_cast<int>(B);
 }
 

@@ -481,6 +481,50 @@ __device__ bool Chol5(const T Hm[15], T diagScale, const T rhs[5], T x[5], T* pi
 	return true;
 }
 
+// Diagonal of the inverse of the packed symmetric matrix F (upper triangle): one Cholesky factorisation F = L L^T,
+// M = L^-1 by forward substitution with the reciprocal pivots, and (F^-1)_aa = sum_i M_ia^2. False when a pivot is not
+// positive (the failure rule of Chol5).
+template <typename T>
+__device__ bool InverseDiag5(const T Fm[15], T out[5])
+{
+	T L[5][5], d[5];
+	#pragma unroll
+	for (int i = 0; i < 5; ++i) {
+		#pragma unroll
+		for (int j = 0; j <= i; ++j) {
+			T s = Fm[Ut(i, j)];
+			#pragma unroll
+			for (int k = 0; k < j; ++k) { s -= L[i][k] * L[j][k]; }
+			if (i == j) {
+				if (!(s > T(0))) { return false; }
+				L[i][i] = sqrt(s);
+				d[i] = T(1) / L[i][i];
+			}
+			else { L[i][j] = s * d[j]; }
+		}
+	}
+	T M[5][5];
+	#pragma unroll
+	for (int j = 0; j < 5; ++j) {
+		M[j][j] = d[j];
+		#pragma unroll
+		for (int i = j + 1; i < 5; ++i) {
+			T s = T(0);
+			#pragma unroll
+			for (int k = j; k < i; ++k) { s += L[i][k] * M[k][j]; }
+			M[i][j] = -s * d[i];
+		}
+	}
+	#pragma unroll
+	for (int a = 0; a < 5; ++a) {
+		T v = T(0);
+		#pragma unroll
+		for (int i = a; i < 5; ++i) { v += M[i][a] * M[i][a]; }
+		out[a] = v;
+	}
+	return true;
+}
+
 // FP32 solve of (Hm with its diagonal scaled) dt = rhs; re-factored in FP64 when the FP32 factorisation fails or its
 // pivot ratio is below 1e-5, i.e. when elimination cancelled more than 5 of the 7 significant digits of FP32 in some
 // pivot (counted in *fallbacks when count is set).
@@ -743,15 +787,11 @@ __device__ int Polish(const MleParams& mp, const Pix& px, float x0, float y0, fl
 template <int MODEL, int L>
 __device__ bool Final(const MleParams& mp, const Pix& px, const double t[5], double crlb[5], FacTab<double> xt, FacTab<double> yt)
 {
-	double Fm[15];
+	double Fm[15], cv[5];
 	Normal<double, MODEL, L, kFinal>(mp, px, t, nullptr, nullptr, Fm, xt, yt);  // a non-finite entry fails the Cholesky
+	if (!InverseDiag5<double>(Fm, cv)) { return false; }
 	#pragma unroll
-	for (int a = 0; a < 5; ++a) {
-		double e[5] = {0, 0, 0, 0, 0}, cv[5];
-		e[a] = 1.0;
-		if (!Chol5<double>(Fm, 1.0, e, cv, nullptr)) { return false; }
-		crlb[a] = cv[a] > 0 ? sqrt(cv[a]) : 0.0;
-	}
+	for (int a = 0; a < 5; ++a) { crlb[a] = cv[a] > 0 ? sqrt(cv[a]) : 0.0; }
 	#pragma unroll
 	for (int a = 0; a < 5; ++a) {
 		if (!isfinite(t[a])) { return false; }

@@ -101,6 +101,22 @@ def test_detection_edge_cases(lib, orc):
         assert np.array_equal(lib.localization(img, 1.0, 0.0, 0, GAUSS_PARAMS), orc.localization(img, 1.0, 0.0, 0, GAUSS_PARAMS))
 
 
+def test_more_frames_than_one_grid_holds(lib, orc):
+    # 70 000 frames of 6 x 10: more frames than one launch grid's z extent (65 535), so the stack is cut into chunks
+    rng = np.random.default_rng(8)
+    s = (100 + rng.poisson(20.0, (70000, 6, 10))).astype(np.uint16)
+    s[::7, 2:4, 3:6] += 400
+    for fit in (0, 2):
+        a = lib.localization(s, 30.0, 0.0, fit, GAUSS_PARAMS)
+        b = orc.localization(s, 30.0, 0.0, fit, GAUSS_PARAMS)
+        assert a.shape[0] >= 10000 and a.shape == b.shape
+        if fit == 0:
+            assert np.array_equal(a, b)
+        else:
+            dxy, rel, sent = _fit_errors(a, b)
+            assert sent == 0 and dxy <= XY_TOL and rel <= REL_TOL, (dxy, rel, sent)
+
+
 def test_bounded_output(lib, stacks):
     # Tests_CPU/test_Palm.cpp:105-121: capacity of one row per plane
     st = stacks["stack"]
