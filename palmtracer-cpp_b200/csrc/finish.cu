@@ -68,14 +68,6 @@ __device__ void Bitonic(unsigned long long* ky, unsigned long long* kx, uint32_t
 	}
 }
 
-__device__ void WriteRow(const double* src, double* dst, double id, double plane, double index)
-{
-	for (int c = 0; c < kCols; ++c) { dst[c] = src[c]; }
-	dst[cId] = id;
-	dst[cPlane] = plane;
-	dst[cIndex] = index;
-}
-
 // One CTA per frame: sort that frame's rows by (Y, X) and write them numbered to out (device memory). Ids continue
 // from *rowBase (rows written by earlier chunks); with offsetOut the rows also land at out + *rowBase rows.
 __global__ void __launch_bounds__(kSortThreads) SortFrames(Workspace ws, double* out, const unsigned long long* rowBase,
@@ -91,7 +83,7 @@ __global__ void __launch_bounds__(kSortThreads) SortFrames(Workspace ws, double*
 	if (n == 0) { return; }
 	uint32_t len = 1;
 	while (len < n) { len <<= 1; }
-	const double* rows = ws.rows + static_cast<long long>(base) * kCols;
+	const double* __restrict__ rows = ws.rows + static_cast<long long>(base) * kCols;
 	unsigned long long *ky, *kx;
 	uint32_t* id;
 	const bool smem = len <= static_cast<uint32_t>(kSmemSort);
@@ -104,22 +96,56 @@ __global__ void __launch_bounds__(kSortThreads) SortFrames(Workspace ws, double*
 		kx = ky + len;
 		id = ws.sortIdx + 2ull * base;
 	}
-	for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
-		if (i < n) {
-			ky[i] = WeakKey(rows[static_cast<long long>(i) * kCols + cY]);
-			kx[i] = WeakKey(rows[static_cast<long long>(i) * kCols + cX]);
+	// keys: four rows per thread and pass, their loads issued before any key is stored
+	for (uint32_t i0 = threadIdx.x; i0 < len; i0 += 4 * blockDim.x) {
+		double y[4], x[4];
+		#pragma unroll
+		for (int u = 0; u < 4; ++u) {
+			const uint32_t i = i0 + u * blockDim.x;
+			y[u] = x[u] = 0.0;
+			if (i < n) {
+				y[u] = __ldg(rows + static_cast<long long>(i) * kCols + cY);
+				x[u] = __ldg(rows + static_cast<long long>(i) * kCols + cX);
+			}
 		}
-		else { ky[i] = ~0ull; kx[i] = ~0ull; }
-		id[i] = i;
+		#pragma unroll
+		for (int u = 0; u < 4; ++u) {
+			const uint32_t i = i0 + u * blockDim.x;
+			if (i < len) {
+				ky[i] = i < n ? WeakKey(y[u]) : ~0ull;
+				kx[i] = i < n ? WeakKey(x[u]) : ~0ull;
+				id[i] = i;
+			}
+		}
 	}
 	__syncthreads();
 	if (smem) { Bitonic<true>(ky, kx, id, len); }
 	else { Bitonic<false>(ky, kx, id, len); }
 	const unsigned long long idBase = *rowBase;
-	double* dst = out + (offsetOut ? static_cast<long long>(idBase) * kCols : 0ll);
-	for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-		WriteRow(rows + static_cast<long long>(id[i]) * kCols, dst + (static_cast<long long>(base) + i) * kCols,
-		         static_cast<double>(idBase + base + i + 1), static_cast<double>(planeBase + f + 1), static_cast<double>(i + 1));
+	double* __restrict__ dst = out + (offsetOut ? static_cast<long long>(idBase) * kCols : 0ll) + static_cast<long long>(base) * kCols;
+	// numbered rows in sorted order, element by element (consecutive threads: consecutive columns of a row, then the
+	// next row), four elements per thread and pass with their loads issued first
+	const double plane = static_cast<double>(planeBase + f + 1);
+	const uint32_t total = n * static_cast<uint32_t>(kCols);
+	for (uint32_t e0 = threadIdx.x; e0 < total; e0 += 4 * blockDim.x) {
+		double v[4];
+		#pragma unroll
+		for (int u = 0; u < 4; ++u) {
+			const uint32_t e = e0 + u * blockDim.x;
+			v[u] = 0.0;
+			if (e < total) {
+				const uint32_t i = e / kCols, c = e - i * kCols;
+				v[u] = __ldg(rows + static_cast<long long>(id[i]) * kCols + c);
+			}
+		}
+		#pragma unroll
+		for (int u = 0; u < 4; ++u) {
+			const uint32_t e = e0 + u * blockDim.x;
+			if (e < total) {
+				const uint32_t i = e / kCols, c = e - i * kCols;
+				dst[e] = c == cId ? static_cast<double>(idBase + base + i + 1) : c == cPlane ? plane : c == cIndex ? static_cast<double>(i + 1) : v[u];
+			}
+		}
 	}
 }
 
