@@ -493,12 +493,43 @@ struct FloodSmem {
 	uint32_t pix[kSmemHeap * kFloodThreads];
 };
 
+// The pixel data a flood reads and the labels it writes, in global memory (any group) ...
+struct GlobalView {
+	const Workspace& ws;
+	__device__ __forceinline__ bool Dom(uint32_t p, int, int) const { return (__ldg(ws.code + p) & kDomain) != 0; }
+	__device__ __forceinline__ uint32_t Lab(uint32_t p, int, int) const { return ws.lab[p]; }
+	__device__ __forceinline__ void SetLab(uint32_t p, int, int, uint32_t v) const { ws.lab[p] = v; }
+	__device__ __forceinline__ double W1(uint32_t p, int, int) const { return static_cast<double>(__ldg(ws.w1 + p)); }
+};
+
+// ... or staged in shared memory: the group's bounding box with a one-pixel ring, row-major from (bx0, by0). Every
+// pixel a flood of the group touches lies in it (a domain neighbour of a group pixel belongs to the group).
+constexpr int kBoxCap = 320;          // staged pixels per group
+constexpr uint32_t kBoxHeap = 64;     // shared-memory heap entries per group (12 bytes each)
+constexpr int kBoxWarps = 8;          // groups (warps) per CTA
+
+struct BoxSmem {
+	double key[kBoxHeap];
+	uint32_t pix[kBoxHeap];
+	uint32_t w1[kBoxCap];   // W1 in 2^-16 units (0 < W1 < 2^32 on the domain)
+	uint32_t lab[kBoxCap];
+	uint8_t flag[kBoxCap];  // bit 0: domain; bit 1: unlabelled when staged (the flood's labels are written back)
+};
+
+struct BoxView {
+	BoxSmem& sm;
+	int bx0, by0, bw;
+	__device__ __forceinline__ int At(int y, int x) const { return (y - by0) * bw + (x - bx0); }
+	__device__ __forceinline__ bool Dom(uint32_t, int y, int x) const { return (sm.flag[At(y, x)] & 1u) != 0; }
+	__device__ __forceinline__ uint32_t Lab(uint32_t, int y, int x) const { return sm.lab[At(y, x)]; }
+	__device__ __forceinline__ void SetLab(uint32_t, int y, int x, uint32_t v) const { sm.lab[At(y, x)] = v; }
+	__device__ __forceinline__ double W1(uint32_t, int y, int x) const { return static_cast<double>(sm.w1[At(y, x)]); }
+};
+
 // Priority flood of one group from its labelled seeds (sorted ascending = raster order), Segmentation2D.cpp:336-385.
-// The heap starts in the thread's shared-memory slice and moves to the group's global slice (hk, hp) if it outgrows it.
-__device__ void FloodGroup(const Workspace& ws, const uint32_t* seedList, uint32_t nSeeds, double* hk, uint32_t* hp, FloodSmem& sm)
+template <class View>
+__device__ void FloodGroup(const Geometry& geo, const View& v, const uint32_t* seedList, uint32_t nSeeds, Heap& heap)
 {
-	const Geometry& geo = ws.g;
-	Heap heap{sm.key + threadIdx.x, sm.pix + threadIdx.x, 0, kFloodThreads, kSmemHeap, hk, hp};
 	for (uint32_t i = 0; i < nSeeds; ++i) {
 		const uint32_t s = seedList[i];
 		const Pix q = Decompose(s, geo);
@@ -510,49 +541,58 @@ __device__ void FloodGroup(const Workspace& ws, const uint32_t* seedList, uint32
 				const int xx = q.x + dx;
 				if ((dx == 0 && dy == 0) || xx < 0 || xx >= geo.W) { continue; }
 				const uint32_t nb = s + static_cast<uint32_t>(dy * geo.W + dx);
-				if (!(ws.code[nb] & kDomain) || ws.lab[nb] == 0) { open = true; }
+				if (!v.Dom(nb, yy, xx) || v.Lab(nb, yy, xx) == 0) { open = true; }
 			}
 		}
-		if (open) { heap.Push(-(static_cast<double>(ws.w1[s]) * kW1Unit), s); }
+		if (open) { heap.Push(-(v.W1(s, q.y, q.x) * kW1Unit), s); }
 	}
 	unsigned long long pops = 0;
 	while (heap.len > 0) {
 		const uint32_t p = heap.Pop();
 		++pops;
 		const Pix q = Decompose(p, geo);
-		const uint32_t L = ws.lab[p];
-		// the 8 neighbours in the reference's scan order; their code, label and W1 are loaded together (each
+		const uint32_t L = v.Lab(p, q.y, q.x);
+		// the 8 neighbours in the reference's scan order; their domain flag, label and W1 are loaded together (each
 		// neighbour's label is written at most once below, after its own test)
 		uint32_t nb[8];
-		bool in[8];
-		uint8_t cd[8];
+		int ny[8], nx[8];
+		bool in[8], dm[8];
 		uint32_t lb[8];
-		long long wv[8];
+		double wv[8];
 		#pragma unroll
 		for (int t = 0; t < 8; ++t) {
 			const int dy = t < 3 ? -1 : (t < 5 ? 0 : 1);
 			const int dx = t < 3 ? t - 1 : (t < 5 ? (t == 3 ? -1 : 1) : t - 6);
-			const int yy = q.y + dy, xx = q.x + dx;
-			in[t] = yy >= 0 && yy < geo.H && xx >= 0 && xx < geo.W;
+			ny[t] = q.y + dy;
+			nx[t] = q.x + dx;
+			in[t] = ny[t] >= 0 && ny[t] < geo.H && nx[t] >= 0 && nx[t] < geo.W;
 			nb[t] = p + static_cast<uint32_t>(dy * geo.W + dx);
 		}
 		#pragma unroll
 		for (int t = 0; t < 8; ++t) {
-			cd[t] = in[t] ? __ldg(ws.code + nb[t]) : static_cast<uint8_t>(0);
-			lb[t] = in[t] ? ws.lab[nb[t]] : 1u;
-			wv[t] = in[t] ? __ldg(ws.w1 + nb[t]) : 0ll;
+			dm[t] = in[t] && v.Dom(nb[t], ny[t], nx[t]);
+			lb[t] = dm[t] ? v.Lab(nb[t], ny[t], nx[t]) : 1u;
+			wv[t] = dm[t] ? v.W1(nb[t], ny[t], nx[t]) : 0.0;
 		}
 		const double age = __dmul_rn(static_cast<double>(pops), kEps);
 		#pragma unroll
 		for (int t = 0; t < 8; ++t) {
-			if ((cd[t] & kDomain) && lb[t] == 0) {
+			if (dm[t] && lb[t] == 0) {
 				// key = -v + it * EPSILON, both operations rounded separately as in the reference
-				const double k = __dadd_rn(-(static_cast<double>(wv[t]) * kW1Unit), age);
+				const double k = __dadd_rn(-(wv[t] * kW1Unit), age);
 				heap.Push(k, nb[t]);
-				ws.lab[nb[t]] = L;
+				v.SetLab(nb[t], ny[t], nx[t], L);
 			}
 		}
 	}
+}
+
+// Flood with the heap in this thread's shared-memory slice, moving to the group's global slice (hk, hp) if it outgrows it.
+__device__ void FloodGroupGlobal(const Workspace& ws, const uint32_t* seedList, uint32_t nSeeds, double* hk, uint32_t* hp,
+                                 FloodSmem& sm)
+{
+	Heap heap{sm.key + threadIdx.x, sm.pix + threadIdx.x, 0, kFloodThreads, kSmemHeap, hk, hp};
+	FloodGroup(ws.g, GlobalView{ws}, seedList, nSeeds, heap);
 }
 
 __global__ void __launch_bounds__(kFloodThreads) GroupFlood(Workspace ws, uint32_t nGroupsStrict)
@@ -563,7 +603,76 @@ __global__ void __launch_bounds__(kFloodThreads) GroupFlood(Workspace ws, uint32
 		const uint32_t nSeeds = ws.gSeedOff[m + 1] - ws.gSeedOff[m];
 		uint32_t* seeds = ws.gSeed + ws.gSeedOff[m];
 		SortSlice(seeds, nSeeds);
-		FloodGroup(ws, seeds, nSeeds, ws.heapKey + ws.gOff[m], ws.heapPix + ws.gOff[m], sm);
+		FloodGroupGlobal(ws, seeds, nSeeds, ws.heapKey + ws.gOff[m], ws.heapPix + ws.gOff[m], sm);
+	}
+}
+
+// One warp per group (groups are components, never whole frames): the lanes stage the group's bounding box with a
+// one-pixel ring in shared memory, lane 0 floods it there (the flood is one serial chain of heap operations; with
+// the box in shared memory each of its steps waits on shared memory instead of on L2 or DRAM), and the lanes write
+// back the labels the flood set. A group whose box exceeds kBoxCap pixels is flooded in global memory by lane 0.
+__global__ void __launch_bounds__(kBoxWarps * 32) GroupFloodBox(Workspace ws)
+{
+	__shared__ BoxSmem boxes[kBoxWarps];
+	BoxSmem& sm = boxes[threadIdx.x / 32];
+	const int lane = threadIdx.x & 31;
+	const Geometry& geo = ws.g;
+	const uint32_t n = ws.cnt->nmulti;
+	for (uint32_t m = blockIdx.x * kBoxWarps + threadIdx.x / 32; m < n; m += gridDim.x * kBoxWarps) {
+		const uint32_t off = ws.gOff[m], nPix = ws.gOff[m + 1] - off;
+		const uint32_t nSeeds = ws.gSeedOff[m + 1] - ws.gSeedOff[m];
+		uint32_t* seeds = ws.gSeed + ws.gSeedOff[m];
+		int x0 = geo.W, y0 = geo.H, x1 = -1, y1 = -1, f = 0;
+		for (uint32_t i = lane; i < nPix; i += 32) {
+			const Pix q = Decompose(ws.gPix[off + i], geo);
+			x0 = min(x0, q.x); x1 = max(x1, q.x); y0 = min(y0, q.y); y1 = max(y1, q.y);
+			f = q.f;
+		}
+		#pragma unroll
+		for (int d = 16; d > 0; d >>= 1) {
+			x0 = min(x0, __shfl_xor_sync(0xffffffffu, x0, d));
+			y0 = min(y0, __shfl_xor_sync(0xffffffffu, y0, d));
+			x1 = max(x1, __shfl_xor_sync(0xffffffffu, x1, d));
+			y1 = max(y1, __shfl_xor_sync(0xffffffffu, y1, d));
+		}
+		f = __shfl_sync(0xffffffffu, f, 0);  // lane 0 holds the group's first pixel (a group has at least two)
+		const int bx0 = max(x0 - 1, 0), by0 = max(y0 - 1, 0);
+		const int bw = min(x1 + 1, geo.W - 1) - bx0 + 1, bh = min(y1 + 1, geo.H - 1) - by0 + 1;
+		double* hk = ws.heapKey + off;
+		uint32_t* hp = ws.heapPix + off;
+		if (nPix == 0 || bw * bh > kBoxCap) {
+			if (lane == 0 && nPix > 0) {
+				SortSlice(seeds, nSeeds);
+				Heap heap{sm.key, sm.pix, 0, 1, kBoxHeap, hk, hp};
+				FloodGroup(geo, GlobalView{ws}, seeds, nSeeds, heap);
+			}
+			__syncwarp();
+			continue;
+		}
+		const uint32_t base = static_cast<uint32_t>(f) * static_cast<uint32_t>(geo.N) + static_cast<uint32_t>(by0 * geo.W + bx0);
+		for (int i = lane; i < bw * bh; i += 32) {
+			const int r = i / bw, c = i - r * bw;
+			const uint32_t p = base + static_cast<uint32_t>(r * geo.W + c);
+			const bool dom = (__ldg(ws.code + p) & kDomain) != 0;
+			const uint32_t lb = dom ? ws.lab[p] : 0u;
+			sm.w1[i] = dom ? static_cast<uint32_t>(__ldg(ws.w1 + p)) : 0u;
+			sm.lab[i] = lb;
+			sm.flag[i] = static_cast<uint8_t>((dom ? 1u : 0u) | (dom && lb == 0 ? 2u : 0u));
+		}
+		__syncwarp();
+		if (lane == 0) {
+			SortSlice(seeds, nSeeds);
+			Heap heap{sm.key, sm.pix, 0, 1, kBoxHeap, hk, hp};
+			FloodGroup(geo, BoxView{sm, bx0, by0, bw}, seeds, nSeeds, heap);
+		}
+		__syncwarp();
+		for (int i = lane; i < bw * bh; i += 32) {
+			if ((sm.flag[i] & 2u) && sm.lab[i] != 0) {
+				const int r = i / bw, c = i - r * bw;
+				ws.lab[base + static_cast<uint32_t>(r * geo.W + c)] = sm.lab[i];
+			}
+		}
+		__syncwarp();
 	}
 }
 
@@ -664,7 +773,7 @@ __global__ void __launch_bounds__(kFloodThreads) GroupFuse(Workspace ws, uint32_
 			ws.lab[ws.fuMaxPos[r]] = r + 1;
 		}
 		SortSlice(seeds, nReg);
-		FloodGroup(ws, seeds, nReg, ws.heapKey + ws.gOff[m], ws.heapPix + ws.gOff[m], sm);
+		FloodGroupGlobal(ws, seeds, nReg, ws.heapKey + ws.gOff[m], ws.heapPix + ws.gOff[m], sm);
 	}
 }
 
@@ -793,8 +902,12 @@ bool LaunchSegment(const Workspace& ws, double ratio, int strict, uint32_t maxPo
 		ok = ok && ExclusiveScan(ws.gRegOff, &ws.cnt->nmulti, 0, ws.capComp, ws.scanBlock, nullptr, st);
 	}
 	GroupScatter<<<kGrid, kThreads, 0, st>>>(ws, strict);
-	// one thread per group: small CTAs so that many SMs share the (uneven) groups
-	GroupFlood<<<kGrid * 2, kFloodThreads, 0, st>>>(ws, groupsStrict);
+	if (strict) {  // frame-wide groups: one thread per group, small CTAs so that many SMs share the frames
+		GroupFlood<<<kGrid * 2, kFloodThreads, 0, st>>>(ws, groupsStrict);
+	}
+	else {  // one warp per group, staged in shared memory
+		GroupFloodBox<<<kGrid, kBoxWarps * 32, 0, st>>>(ws);
+	}
 	CountLaunch(2);
 	ok = ok && PTB_LAUNCHED();
 	if (static_cast<int>(ratio) > 0) {  // WatershedIntelligent, Segmentation2D.cpp:77-85
