@@ -294,8 +294,9 @@ bool Engine::Init()
 	}
 	size_t freeB = 0, totalB = 0;
 	if (!PTB_CUDA(cudaMemGetInfo(&freeB, &totalB))) { return false; }
-	// default budget: a quarter of free memory, at most 24 GiB (leaves room for callers' own buffers)
-	budget_ = std::min<size_t>(freeB / 4, 24ull << 30);
+	// default budget: a quarter of free memory, at most 48 GiB (leaves room for callers' own buffers); on a B200 about
+	// 280 frames of 1024 x 1024 per chunk slot, which halves the chunks (and their serial tails) of 24 GiB
+	budget_ = std::min<size_t>(freeB / 4, 48ull << 30);
 	if (const char* env = std::getenv("PTB_WORKSPACE_MB")) { budget_ = static_cast<size_t>(std::atoll(env)) << 20; }
 	if (fixedBudget_) { budget_ = fixedBudget_; }
 	return true;

@@ -67,7 +67,7 @@ public:
 	int SetPrecision(int p) { const int o = precision_; precision_ = p; return o; }
 	int Precision() const { return precision_; }
 	cudaStream_t Stream() const { return stream_; }
-	// Device-memory budget of the chunk workspace (bytes); 0 = a quarter of free memory at first use, at most 24 GiB
+	// Device-memory budget of the chunk workspace (bytes); 0 = a quarter of free memory at first use, at most 48 GiB
 	// (or PTB_WORKSPACE_MB). Takes effect at the engine's first call.
 	void SetBudget(size_t bytes) { fixedBudget_ = bytes; }
 	size_t Budget() const { return budget_; }
