@@ -603,11 +603,11 @@ __device__ __forceinline__ void FixActive32(const MleParams& mp, float x0, float
 // LM stop rule: the oracle's (MleStepSmall: 1e-4 px in x and y, 1e-4 relative in I and bg with floor 1, 1e-4 for
 // sigma and the spline z, 1e-2 nm for z) with every threshold multiplied by kLmStepScale. The FP32 deviance cannot
 // resolve the last LM steps of the oracle (a 1e-4 px step changes the deviance by about 1e-5, the size of its FP32
-// rounding), so the FP32 LM hands over to the Newton polish two decades earlier (a 1e-2 px step): the polish
-// converges quadratically from there to the same optimum. Measured on the 2000-frame benchmark against handing over
-// at 10x: LM evaluations 36.9 M -> 24.2 M, polish evaluations 15.1 M -> 16.4 M, fit 23.2 -> 21.3 ms, and the same
-// error table.
-constexpr float kLmStepScale = 100.f;
+// rounding), so the FP32 LM hands over to the Newton polish earlier (a 3e-2 px step): the polish converges
+// quadratically from there to the same optimum. Measured on the 2000-frame benchmark (LM / polish evaluations, fit
+// stage, step): 10x 36.9 M / 15.1 M; 100x 24.2 M / 11.6 M, 16.9 ms, 41.9 ms; 300x 21.2 M / 12.5 M, 16.6 ms,
+// 41.5 ms; 1000x 17.9 M / 14.2 M, 16.5 ms, 41.5 ms; the same error table throughout.
+constexpr float kLmStepScale = 300.f;
 __device__ __forceinline__ bool StepSmall(int model, const float a[5], const float b[5])
 {
 	const float t = 1e-4f * kLmStepScale, sTol = (model == 7 ? 1e-2f : 1e-4f) * kLmStepScale;
