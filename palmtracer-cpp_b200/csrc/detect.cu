@@ -15,8 +15,8 @@
 // offsetTest() clamping of every neighbour access, so border tiles need no special case. The strict threshold
 // W1 > thr is evaluated as W1_fixed > floor(thr * 2^16), which is the same test for an integer W1_fixed.
 //
-// Layout: a 128 x 32 output tile per CTA of 8 warps; every stage loops rows over warps and columns over lanes (no
-// index division); shared buffers are reused across stages (input -> V1, T1 -> T2), 66 KB in all.
+// Layout: a 128 x 28 output tile per CTA of 8 warps (the Wavelett planes: every stage loops rows over warps and
+// columns over lanes; shared buffers are reused across stages, input -> V1, T1 -> T2).
 #include <algorithm>
 #include <cmath>
 
@@ -26,7 +26,7 @@ namespace ptb {
 
 namespace {
 
-constexpr int TX = 128, TY = 32;          // output tile
+constexpr int TX = 128, TY = 28;          // output tile (28 rows: 44 KB of shared memory, 5 CTAs per SM)
 constexpr int HIN = 7;                    // input halo: W1 on the tile +-1 ring needs V2 +-1, V1 +-5, input +-7
 constexpr int IW = TX + 2 * HIN, IH = TY + 2 * HIN;
 constexpr int V1W = TX + 10, V1H = TY + 10;
@@ -102,14 +102,15 @@ __device__ __forceinline__ long long W1At(const TileSmem& s, int r, int c)
 
 // ---- Detection kernel ------------------------------------------------------------------------------------------
 // The input tile is first staged in shared memory with 16-byte loads; then five register-blocked passes over one
-// 128 x 32 tile. Borders: every intermediate array is kept edge-replicated
+// 128 x 28 tile (44 KB of shared memory, so 5 CTAs per SM; 128 x 32 took 49.7 KB, 4 CTAs per SM, and measured 2 %
+// slower for 2 % less halo work). Borders: every intermediate array is kept edge-replicated
 // (an entry whose coordinate lies outside the frame holds the value of the nearest in-frame entry), which is what
 // the reference's clamping of every neighbour access amounts to, so no pass clamps an index:
-//   A  C1 = vertical level-1 taps of the input, one lane per column sliding down 46 clamped input rows (rows outside
-//      the frame are then replicated);   tile rows [-5, 37), cols [-7, 145)
+//   A  C1 = vertical level-1 taps of the input, one lane per column sliding down 42 clamped input rows (rows outside
+//      the frame are then replicated);   tile rows [-5, 33), cols [-7, 145)
 //   B  V1 = horizontal level-1 taps of C1, 8 columns per task from 3 vector loads (columns outside the frame are
-//      then replicated);                 tile rows [-5, 37), cols [-5, 139)
-//   C  C2 = vertical level-2 taps (rows +-2, +-4) of V1, one lane per column and 12-row run;   rows [-1, 33)
+//      then replicated);                 tile rows [-5, 33), cols [-5, 139)
+//   C  C2 = vertical level-2 taps (rows +-2, +-4) of V1, one lane per column and 12-row run;   rows [-1, 29)
 //   D  W1 = V1 * 256 - V2 on the ring (tile +-1), V2 = horizontal level-2 taps of C2, 8 columns per task, stored
 //      in place of V1 as max(W1, 0) (W1 < 2^32; a non-positive W1 can neither be in the domain nor dominate a
 //      domain pixel) and 0 outside the frame (the reference skips neighbours outside the frame);
@@ -124,6 +125,8 @@ constexpr int kInRows = TY + 14, kInW = 160;  // staged input tile (uint16): row
 static_assert(kRows2 * kPV <= kRows1 * kP1, "C2 must fit in the C1 space");
 static_assert(kInRows * kInW * 2 <= kRows1 * kPV * 4, "the staged input must fit in the V1 space");
 static_assert(kP1 + 1 <= kInW, "C1 columns read staged columns 1 .. kP1");
+static_assert(kRows2 <= 36, "pass C covers C2 rows in three runs of 12");
+static_assert(TY * 16 <= 2 * kThreads, "pass E: two tasks of 8 pixels per thread");
 
 __device__ __forceinline__ uint32_t Tap(uint32_t m2, uint32_t m1, uint32_t c, uint32_t p1, uint32_t p2)
 {
@@ -260,6 +263,7 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 	for (int h = 0; h < 2; ++h) {
 		const int task = tid + h * kThreads;
 		const int ty = task >> 4, m = task & 15;
+		if (ty >= TY) { continue; }  // 16 tasks per tile row; the last thread slots have none
 		uint32_t a[3][12];
 		#pragma unroll
 		for (int rr = 0; rr < 3; ++rr) {
@@ -312,7 +316,7 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 		const int task = tid + h * kThreads;
 		const int ty = task >> 4, m = task & 15;
 		const int y = y0 + ty, xb = x0 + 8 * m;
-		if (y >= H || xb >= W) { continue; }
+		if (ty >= TY || y >= H || xb >= W) { continue; }
 		const long long g = static_cast<long long>(f) * ws.g.N + static_cast<long long>(y) * W + xb;
 		// code bytes of the eight pixels: each mask bit spread to the low bit of its byte, times the flag
 		const uint32_t dm = dmask[h], sm = smask[h];
