@@ -32,6 +32,7 @@ enum FitMode : int { kNone = 0, kG2Fixed = 1, kG2Sigma = 2, kG3Fixed = 3, kG3The
 constexpr uint8_t kDomain = 1;  // thresholded potential > 1e-8: the watershed floods it
 constexpr uint8_t kSeed = 2;    // local maximum of the thresholded potential
 constexpr int kDirShift = 2;    // bits 2..4: raster-earlier seed neighbour a seed inherits its label from (0 = root)
+constexpr uint8_t kUnion = 32;  // bit 5: the pixel joins two union-find trees (set by CclInit for CclUnion)
 
 // W1 values are exact multiples of 2^-16 (B3 taps are dyadic and the input is uint16), kept as int64 "fixed" units.
 constexpr double kW1Unit = 1.0 / 65536.0;

@@ -137,6 +137,7 @@ __global__ void CclInit(Workspace ws)
 		uint32_t link, extra;
 		EarlierNeighbours(ws, p, link, extra);
 		ws.par[p] = link;
+		if (extra != p) { ws.code[p] = static_cast<uint8_t>(ws.code[p] | kUnion); }  // only this thread writes p's byte
 	}
 }
 
@@ -145,9 +146,10 @@ __global__ void CclUnion(Workspace ws)
 	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
 	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
 		const uint32_t p = ws.dom[k];
+		if (!(ws.code[p] & kUnion)) { continue; }  // most pixels have one raster-earlier link at most
 		uint32_t link, extra;
 		EarlierNeighbours(ws, p, link, extra);
-		if (extra != p) { Unite(ws.par, p, extra); }
+		Unite(ws.par, p, extra);
 	}
 }
 
