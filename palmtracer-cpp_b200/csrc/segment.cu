@@ -6,6 +6,7 @@
 //   2. each seed (local maximum) inherits the label of its first raster-earlier seed neighbour, as getLocalMax()
 //      does (Segmentation2D.cpp:309-327); root seeds are numbered in raster order through a per-row bitmask rank;
 //   3. a component with one label is labelled directly; every other component (a "group") is flooded by one thread
+//      (lane 0 of a warp that stages the group's box in shared memory; in strict mode a thread on global memory)
 //      with a binary heap whose push/pop steps are those of libstdc++'s std::priority_queue, with the reference key
 //      -v + pops * 1e-7 (Segmentation2D.cpp:336-385) and a pop counter local to the group. In strict mode a group is
 //      a whole frame and the counter is frame-global, which is the reference's process exactly;
