@@ -466,20 +466,24 @@ def main():
                        "peak": peak, "unit": "GB/s", "frac": (det_achieved / peak) if det_achieved else None,
                        "traffic": DETECT_DRAM_BYTES_PER_FRAME * frames_per_launch, "traffic_unit": "bytes per launch (ncu, scaled)",
                        "algorithmic_bytes_per_launch": det_bytes / max(det_l, 1), "launches": det_l,
-                       "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind}
-    roofline = detect_roofline
+                       "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                       "why_this_kernel": "largest share of device time in the launch list "
+                                          "(profiles/launch_list_mle6_c2_2000x1024.md)"}
+    # the FP32 roofline of the fit's largest kernel, the second largest share
+    fit_roofline = None
     if FIT_MODE == 6 and stages["fit_lm"][0] > 0:
         fp32_peak = ptb.fma_peak(False) / 1e12
         lm_ms = stages["fit_lm"][0]
         flops = FLOP_PER_PIXEL_LM * 49 * evals["lm"]
         achieved = flops / (lm_ms / 1000.0) / 1e12
-        roofline = {"kernel": "MleLmKernel<6> (persistent FP32 LM, thread per ROI)", "bound": "fp32", "achieved": achieved,
+        fit_roofline = {"kernel": "MleLmKernel<6> (persistent FP32 LM, thread per ROI)", "bound": "fp32", "achieved": achieved,
                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                     "traffic": LM_DRAM_BYTES_PER_FRAME * frames / max(1, stages["fit_lm"][1]),
                     "traffic_unit": "bytes per launch (ncu, scaled)",
                     "algorithmic_flops_per_launch": flops / max(1, stages["fit_lm"][1]), "launches": stages["fit_lm"][1],
                     "flop_per_pixel_evaluation": FLOP_PER_PIXEL_LM, "evaluations": evals,
                     "peak_source": "measured in this run (PTB_MeasureFmaPeak FP32 FMA chains)"}
+    roofline = detect_roofline
     roofline["stage_ms"] = {k: round(v[0], 3) for k, v in stages.items()}
     roofline["stage_launches"] = {k: v[1] for k, v in stages.items()}
 
@@ -549,7 +553,7 @@ def main():
                 "config": dict(config, fit_precision=args.precision),
                 "frames_per_s": frames * world * args.steps / (total_ms / 1000.0),
                 "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
-                "localizations_per_step": int(rows_all), "roofline": roofline, "detect_roofline": detect_roofline,
+                "localizations_per_step": int(rows_all), "roofline": roofline, "fit_roofline": fit_roofline,
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_bytes,
                         "d2h_bytes_per_step": int(n_e2e * 8), "ms_per_step": float(np.median(e2e_ms)) if e2e_ms else None,
