@@ -128,6 +128,15 @@ def mad_threshold_gpu(lib, frame):
     return synth.mad_threshold(w1)
 
 
+def reference_threshold(frame):
+    """The MAD threshold of a frame's W1 plane computed by the reference build's own Wavelett (the oracle port when
+    the build is absent), for the reference arm: the same value as the GPU arm's, since the planes are bit-exact."""
+    import synth
+    from oracle.oracle import reference, OracleLib
+    lib = reference() or OracleLib()
+    return synth.mad_threshold(lib.wavelett(frame, 2)[0])
+
+
 def cpu_reference_rate(frames_host, thr, seconds=10.0, threads=None):
     """Reference CPU path (oracle/_ref, or the oracle port when the reference build is absent) on a bounded sample."""
     from oracle.oracle import reference, OracleLib
@@ -367,9 +376,7 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=180))
     torch.cuda.set_device(local)
     import synth
-    import ptb
 
-    ptb.set_fit_precision(args.precision)
     if args.fit is not None:
         FIT_MODE = args.fit
         FIT_PARAMS = PARAMS_BY_MODE[FIT_MODE]
@@ -385,9 +392,10 @@ def main():
             if world > 1:
                 dist.destroy_process_group()
             return
+        # the frames come from the same seeded GPU generator as the other arm's; nothing of this library runs here
         d, _ = synth.stack_cuda(WORKLOAD, frames=min(frames, 256), seed=1000)
         host = d.cpu().numpy().view(np.uint16)
-        thr = mad_threshold_gpu(ptb, host[0])
+        thr = reference_threshold(host[0])
         del d
         torch.cuda.empty_cache()
         rates = []
@@ -407,6 +415,8 @@ def main():
             dist.destroy_process_group()
         return
 
+    import ptb
+    ptb.set_fit_precision(args.precision)
     d_in, em = synth.stack_cuda(WORKLOAD, frames=frames, seed=1000 + rank)
     torch.cuda.synchronize()
     thr = mad_threshold_gpu(ptb, d_in[0].cpu().numpy().view(np.uint16))
