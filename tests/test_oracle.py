@@ -177,3 +177,17 @@ def test_astig_estimation_recovers_noisy_z(orc):
     s = _astig_widths(model, z) + rng.normal(0.0, 0.02, (10, 2))
     r = orc.astig_estimation(s, 160.0, model, 800.0)
     assert np.all(np.abs(r[:, 0] - z) <= 40.0) and np.all(r[:, 1] > 0.95) and np.all(r[:, 1] <= 1.0)
+
+
+def test_bench_reference_arm_threshold(orc):
+    # bench.py's reference arm takes the threshold from the reference build's own Wavelett (the oracle port without
+    # it): it must be the MAD threshold of the frame's W1 plane, the value the GPU arm computes from its bit-exact plane
+    import os
+    import sys
+    import synth
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if root not in sys.path:
+        sys.path.insert(0, root)
+    import bench
+    s, _ = synth.stack("c2", frames=1, seed=3, size=(256, 256))
+    assert bench.reference_threshold(s[0]) == synth.mad_threshold(orc.planes(s[0])[1])
