@@ -4,10 +4,11 @@
 # Compiles the reference sources where they lie (nothing is copied into this repository) with the
 # reference's strict floating-point setting (-ffp-contract=off, CMakeLists.txt:7-12), plus oracle/ref_shim.cpp.
 # Output goes only to oracle/_ref/ (git-ignored; it still travels with the working tree to a GPU host).
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default: $PTB_REFERENCE_ROOT, else /root/reference)
+# The root it built from is recorded in oracle/_ref/reference_root.txt for the tests that read reference fixtures.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${PTB_REFERENCE_ROOT:-/root/reference}}"
 OUT="$HERE/_ref"
 if [ ! -d "$REF/lib" ]; then
 	echo "reference tree not found at $REF; keeping any prebuilt $OUT/libptref.so" >&2
@@ -32,4 +33,5 @@ g++ -std=c++20 -O2 -fopenmp -ffp-contract=off -fPIC -shared \
 	-I"$REF/lib" -I"$REF/lib/localization" -I"$REF/lib/fit" -I"$REF/lib/signal_processing" -I"$REF/lib/tracking" \
 	"${SRCS[@]}" -o "$OUT/libptref.so.tmp"
 mv "$OUT/libptref.so.tmp" "$OUT/libptref.so"
+(cd "$REF" && pwd) > "$OUT/reference_root.txt"
 echo "built $OUT/libptref.so"

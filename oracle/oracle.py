@@ -204,3 +204,15 @@ def oracle():
 def reference():
     """The reference built from source, or None when oracle/_ref has not been built."""
     return RefLib() if os.path.exists(REF_SO) else None
+
+
+def reference_root():
+    """The reference source tree (for tests that read its fixtures): $PTB_REFERENCE_ROOT, else the tree oracle/_ref was
+    built from; None when neither exists on this machine."""
+    root = os.environ.get("PTB_REFERENCE_ROOT")
+    if not root:
+        rec = os.path.join(HERE, "_ref", "reference_root.txt")
+        if os.path.exists(rec):
+            with open(rec) as f:
+                root = f.read().strip()
+    return root if root and os.path.isdir(root) else None

@@ -7,7 +7,7 @@ Reads (text and TIFF only, nothing executed) from the reference tree:
   Tests_CPU/Input/ref/stack-tracking-*-5.csv                              -> tracking.npz
 The AutoThreshold known answers come from Tests_CPU/test_Palm.cpp:307-310 and are stored beside them.
 
-Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage: python tests/golden/make_golden.py REFERENCE_ROOT   (or set PTB_REFERENCE_ROOT)
 """
 import glob
 import os
@@ -66,4 +66,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PTB_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT (or set PTB_REFERENCE_ROOT)")
+    main(root)

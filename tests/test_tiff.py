@@ -14,7 +14,13 @@ import pytest
 
 import tiffgen
 
-REF_INPUT = os.environ.get("PTB_REFERENCE_INPUT", "/root/reference/Tests_CPU/Input")
+def _reference_input():
+    from oracle.oracle import reference_root
+    root = reference_root()
+    return os.path.join(root, "Tests_CPU", "Input") if root else None
+
+
+REF_INPUT = _reference_input()
 
 
 @pytest.fixture(scope="module")
@@ -30,9 +36,9 @@ def _frames(seed, n=4, h=37, w=53):
 
 @pytest.mark.parametrize("name", ["stack", "stack_quadrant"])
 def test_reference_stacks_decode_to_golden(ptbmod, name):
+    if REF_INPUT is None or not os.path.exists(os.path.join(REF_INPUT, name + ".tif")):
+        pytest.skip("reference test inputs not present (set PTB_REFERENCE_ROOT)")
     path = os.path.join(REF_INPUT, name + ".tif")
-    if not os.path.exists(path):
-        pytest.skip("reference test inputs not present")
     golden = np.load(os.path.join(os.path.dirname(__file__), "golden", "stacks.npz"))[name]
     assert ptbmod.tiff_info(path) == (golden.shape[2], golden.shape[1], golden.shape[0])
     assert np.array_equal(ptbmod.tiff_read(path), golden)
