@@ -47,7 +47,7 @@ REF_FIT_MODE = 2  # the reference's own 5-parameter Gaussian fit, for the CPU ar
 FLOP_PER_PIXEL_LM = 71
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per frame of one launch, from ncu captures of smaller
 # chunks of the same workload, scaled by the frames a benchmark launch processes (traffic grows with the frames):
-# MleLmKernel<6> 126.65 MB and DetectKernel 262.59 MB over one 64-frame chunk (profiles/*_c2_64frames.md).
+# MleLmKernel<6> 126.65 MB and DetectKernel 262.59 MB over one 64-frame chunk.
 LM_DRAM_BYTES_PER_FRAME = 126.77e6 / 64
 DETECT_DRAM_BYTES_PER_FRAME = 262.52e6 / 64
 RATIO = 0.0
@@ -348,6 +348,130 @@ def serving_run(ptb, torch, n_req, seed=2026):
     }
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def parity_run(ptb, d_in, thr, n_cand=16, n_mle=4):
+    """Parity of the benchmark's own frames, outside the timed region: the candidate rows (fit 0: Id, Plane, Index,
+    X, Y, SegIntensity, Surface of every candidate) of the first `n_cand` frames against the reference build, bit
+    for bit, and the error table of the benchmark fit (mode 6) on the first `n_mle` frames against the FP64 oracle
+    (median / p99 / max of |GPU - oracle| per quantity; x, y, sigma in px, photons and background relative)."""
+    from compare import match_rows, C_X, C_Y, C_SX, C_OFF
+    from oracle.oracle import reference, OracleLib
+    host = d_in[:n_cand].cpu().numpy().view(np.uint16)
+    cap = PER_PLANE * n_cand * 18
+    ref = reference()
+    kind = "reference build" if ref is not None else "oracle port"
+    ref = ref or OracleLib()
+    ref.set_threads(os.cpu_count())
+    a = ptb.localization(host, thr, RATIO, 0, GAUSS_PARAMS, capacity_doubles=cap)
+    b = ref.localization(host, thr, RATIO, 0, GAUSS_PARAMS, capacity_doubles=cap)
+    same = bool(a.shape == b.shape and np.array_equal(a, b))
+    orc = OracleLib()
+    orc.set_threads(os.cpu_count())
+    m = host[:n_mle]
+    ga = ptb.localization(m, thr, RATIO, FIT_MODE, FIT_PARAMS, capacity_doubles=PER_PLANE * n_mle * 18)
+    gb = orc.localization(m, thr, RATIO, FIT_MODE, FIT_PARAMS, capacity_doubles=PER_PLANE * n_mle * 18)
+    out = {"candidates_equal": same, "candidate_frames": n_cand, "candidates": int(a.shape[0]), "candidates_against": kind,
+           "mle_frames": n_mle, "mle_fits": int(ga.shape[0]), "mle_against": "FP64 oracle (oracle/pt_oracle.cpp)"}
+    bad, _, pairs = match_rows(ga, gb, atol=1e9, rtol=0, keys=(C_X, C_Y))
+    if pairs is None or bad:
+        out["mle_errors"] = None
+        out["mle_unmatched_rows"] = int(bad)
+        return out
+    e = gb[pairs]
+    both = (ga[:, C_SX] >= 0) & (e[:, C_SX] >= 0)
+    tol = {"x": ("abs", C_X, 1e-3), "y": ("abs", C_Y, 1e-3), "photons": ("rel", 7, 1e-4), "background": ("rel", C_OFF, 1e-4),
+           "sigma": ("abs", C_SX, 1e-4)}
+    beyond = np.zeros(len(ga), dtype=bool)
+    errs = {}
+    for key, (kind_, c, t) in tol.items():
+        d = np.abs(ga[:, c] - e[:, c])
+        if kind_ == "rel":
+            d = d / np.abs(e[:, c])
+        d = d[both]
+        beyond[both] |= d > t
+        errs[key] = {"kind": kind_, "tol": t, "median": float(np.median(d)), "p99": float(np.percentile(d, 99)),
+                     "max": float(np.max(d))}
+    out["mle_errors"] = errs
+    out["mle_fits_compared"] = int(both.sum())
+    out["mle_beyond_tolerance"] = int(beyond.sum())
+    out["mle_status_flips"] = int(np.sum((ga[:, C_SX] >= 0) != (e[:, C_SX] >= 0)))
+    return out
+
+
+def same_work_run(ptb, torch, d_in, thr, frames, h, w, steps=3):
+    """The reference arm's own fit (mode 2: Gaussian least squares, FP64, the reference's operation order) on the
+    benchmark stack: device-resident and end to end through Localization with pinned host buffers. Beside the
+    reference arm's number this is a same-work ratio."""
+    cap = PER_PLANE * frames * 18
+    d_out = torch.empty(cap, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        return ptb.localization_device(d_in.data_ptr(), d_out.data_ptr(), cap, (frames, h, w), thr, RATIO, REF_FIT_MODE,
+                                       GAUSS_PARAMS, stream.cuda_stream)
+
+    n = step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        n = step()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    rows = n // 18
+    del d_out
+    host_in = torch.empty((frames, h, w), dtype=torch.int16, pin_memory=True)
+    host_in.copy_(d_in)
+    host_np = host_in.numpy().view(np.uint16)
+    host_out = torch.empty(cap, dtype=torch.float64, pin_memory=True).numpy()
+    e2e = []
+    for i in range(steps + 1):
+        t0 = time.perf_counter()
+        k = ptb.localization_raw(host_np, host_out, thr, RATIO, REF_FIT_MODE, GAUSS_PARAMS)
+        if i:
+            e2e.append(time.perf_counter() - t0)
+    del host_in, host_out
+    e2e_s = float(np.median(e2e))
+    return {"fit_mode": REF_FIT_MODE, "fit": "Gaussian least squares (x, y, sigma, amplitude, offset), FP64, in the "
+                                             "reference's order of operations", "localizations_per_step": int(rows),
+            "device": {"ms_per_step": ms, "localizations_per_s": rows / (ms / 1000.0)},
+            "e2e": {"ms_per_step": e2e_s * 1000.0, "localizations_per_s": (k // 18) / e2e_s}}
+
+
+def plain_per_frame_run(ptb, host_frames, thr, seconds=6.0):
+    """The plain drop-in form on the benchmark's own frames: one Localization call per 1024 x 1024 frame with
+    pageable host buffers, as a front end that hands over frame after frame would call it; call latency p50 / p99 and
+    the throughput of the calls (a bounded sample)."""
+    lat, rows, t_start = [], [], time.perf_counter()
+    for z in range(host_frames.shape[0]):
+        frame = np.ascontiguousarray(host_frames[z:z + 1])
+        t1 = time.perf_counter()
+        r = ptb.localization(frame, thr, RATIO, FIT_MODE, FIT_PARAMS, capacity_doubles=PER_PLANE * 18)
+        lat.append(time.perf_counter() - t1)
+        rows.append(r.shape[0])
+        if time.perf_counter() - t_start > seconds and z >= 20:
+            break
+    lat = np.array(lat[2:])  # the first two calls launch the chain directly, then capture its graph
+    total = float(lat.sum())
+    per_frame = float(np.mean(rows[2:]))
+    p99 = float(np.percentile(lat, 99))
+    return {"frames": int(len(lat)), "localizations_per_s": per_frame * len(lat) / total,
+            "call_latency_ms": {"p50": float(np.percentile(lat, 50)) * 1000.0, "p99": p99 * 1000.0},
+            # throughput of a front end that budgets every call at the p99 latency
+            "p99_bounded_localizations_per_s": per_frame / p99}
+
+
 def main():
     global FIT_MODE, FIT_PARAMS
     ap = argparse.ArgumentParser()
@@ -364,6 +488,8 @@ def main():
     ap.add_argument("--no-tracking", action="store_true", help="skip tracking the benchmark's localizations")
     ap.add_argument("--no-workloads", action="store_true", help="skip the C1, C3 and C4 workloads")
     ap.add_argument("--serve-requests", type=int, default=40)
+    ap.add_argument("--no-parity", action="store_true", help="skip the parity check of the benchmark's own frames")
+    ap.add_argument("--no-pageable", action="store_true", help="skip the end-to-end run from pageable host memory")
     args = ap.parse_args()
     import torch
     import torch.distributed as dist
@@ -382,9 +508,11 @@ def main():
         FIT_PARAMS = PARAMS_BY_MODE[FIT_MODE]
     frames = args.frames or synth.SHAPES[WORKLOAD][0]
     h, w = synth.SHAPES[WORKLOAD][1:]
-    config = {"workload": "c2: %d frames of %dx%d uint16, ~2684 emitters/frame, 7x7 ROI, fit mode %d, per-plane capacity %d"
-                          % (frames, h, w, FIT_MODE, PER_PLANE),
-              "frames": frames, "height": h, "width": w, "fit_mode": FIT_MODE, "roi": 7, "watershed_ratio": RATIO,
+    # one config for both arms (the reference has no MLE fit: its arm runs its own least-squares mode 2)
+    config = {"workload": "c2: %d frames of %dx%d uint16, ~2684 emitters/frame, 7x7 ROI, per-plane capacity %d"
+                          % (frames, h, w, PER_PLANE),
+              "frames": frames, "height": h, "width": w, "roi": 7, "watershed_ratio": RATIO,
+              "fit_modes": {"this_library": FIT_MODE, "reference_arm": REF_FIT_MODE},
               "l2": "inputs (4.2 GB) larger than L2", "parallelism": "frames sharded, no exchange" if world > 1 else "single GPU"}
 
     if args.impl == "reference":
@@ -408,7 +536,8 @@ def main():
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
                 "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "config": config,
-                "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"], "sample": info["sample"]},
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"], "sample": info["sample"],
+                                 "cpu_model": cpu_model()},
                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         if world > 1:
@@ -436,6 +565,7 @@ def main():
     if world > 1:
         dist.barrier()
     clocks = Clocks(local)
+    ptb.segmentation_stats()
     launches0 = ptb.launch_count()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     counts = []
@@ -449,6 +579,7 @@ def main():
         dist.barrier()
     clk = clocks.stop()
     launches = (ptb.launch_count() - launches0) // args.steps
+    seg = ptb.segmentation_stats()
     step_ms = np.array([a.elapsed_time(b) for a, b in ev])
     rows = counts[-1] // 18
     total_ms = float(step_ms.sum())
@@ -477,8 +608,7 @@ def main():
                        "traffic": DETECT_DRAM_BYTES_PER_FRAME * frames_per_launch, "traffic_unit": "bytes per launch (ncu, scaled)",
                        "algorithmic_bytes_per_launch": det_bytes / max(det_l, 1), "launches": det_l,
                        "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                       "why_this_kernel": "largest share of device time in the launch list "
-                                          "(profiles/launch_list_mle6_c2_2000x1024.md)"}
+                       "why_this_kernel": "largest share of device time in the ncu launch list of this command"}
     # the FP32 roofline of the fit's largest kernel, the second largest share
     fit_roofline = None
     if FIT_MODE == 6 and stages["fit_lm"][0] > 0:
@@ -496,6 +626,11 @@ def main():
     roofline = detect_roofline
     roofline["stage_ms"] = {k: round(v[0], 3) for k, v in stages.items()}
     roofline["stage_launches"] = {k: v[1] for k, v in stages.items()}
+
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = parity_run(ptb, d_in, thr)
+        parity["frames_flooded_again_frame_wide"] = {"timed_steps": seg["routed"], "frames_segmented": seg["frames"]}
 
     # end to end through the reference-facing C ABI with host buffers
     host_in = torch.empty((frames, h, w), dtype=torch.int16, pin_memory=True)
@@ -534,6 +669,32 @@ def main():
         link_gbs = part.numel() * 2 / (best / 1000.0) / 1e9
         del dev
 
+    # the same call with a pageable numpy copy of the input and pageable output, as most front ends pass them
+    e2e_pageable = None
+    if e2e_ms and rank == 0 and not args.no_pageable:
+        page_in = np.array(host_np, copy=True)
+        page_out = np.empty(cap, dtype=np.float64)
+        pg = []
+        for i in range(1 + max(3, min(args.steps, 5))):
+            t0 = time.perf_counter()
+            n_pg = ptb.localization_raw(page_in, page_out, thr, RATIO, FIT_MODE, FIT_PARAMS)
+            if i:
+                pg.append((time.perf_counter() - t0) * 1000.0)
+        e2e_pageable = {"value": (n_pg // 18) / (float(np.median(pg)) / 1000.0), "unit": UNIT,
+                        "ms_per_step": float(np.median(pg)), "ms_each": [round(t, 3) for t in pg],
+                        "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": int(n_pg * 8)}
+        del page_in, page_out
+
+    same_work = None
+    plain_c2 = None
+    if rank == 0 and world == 1 and not args.no_workloads:
+        same_work = same_work_run(ptb, torch, d_in, thr, frames, h, w)
+        plain_c2 = plain_per_frame_run(ptb, host_np[:400], thr)
+        plain_c2["batched_e2e_over_plain"] = e2e_value / plain_c2["localizations_per_s"] if e2e_value else None
+        plain_c2["batched_device_over_plain"] = value / plain_c2["localizations_per_s"]
+        plain_c2["batched_e2e_over_plain_p99_bounded"] = (e2e_value / plain_c2["p99_bounded_localizations_per_s"]
+                                                         if e2e_value else None)
+
     tracking = None
     if rank == 0 and world == 1 and not args.no_tracking:
         tracking = tracking_run(ptb, torch, d_out, int(rows))
@@ -552,7 +713,7 @@ def main():
         v, info = cpu_reference_rate(sample, thr, seconds=10.0)
         v1, info1 = cpu_reference_rate(sample, thr, seconds=5.0, threads=1)
         cpu = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"], "sample": info["sample"],
-               "single_thread": {"value": v1, "cores": 1, "sample": info1["sample"]}}
+               "cpu_model": cpu_model(), "single_thread": {"value": v1, "cores": 1, "sample": info1["sample"]}}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -560,7 +721,7 @@ def main():
                 "dtype": ("f32 (axial pre-scan, LM and Newton polish; f64 Cholesky fallback, Fisher information, CRLB)" if FIT_MODE >= 6 else
                           "f64" if args.precision != 1 else "f32 (f64 re-fit)"),
                 "data": "synthetic (seeded, generated on the GPU; no public dataset)",
-                "config": dict(config, fit_precision=args.precision),
+                "config": config, "fit_precision": args.precision,
                 "frames_per_s": frames * world * args.steps / (total_ms / 1000.0),
                 "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
                 "localizations_per_step": int(rows_all), "roofline": roofline, "fit_roofline": fit_roofline,
@@ -571,8 +732,9 @@ def main():
                         # host -> device rate over the median call (the frames cross PCIe once; the link is the e2e bound)
                         "h2d_gbs": h2d_bytes / (float(np.median(e2e_ms)) / 1000.0) / 1e9 if e2e_ms else None,
                         "h2d_link_gbs": link_gbs},
+                "e2e_pageable": e2e_pageable, "parity": parity,
                 "gpu_launches": int(launches), "clocks": clk, "serving": serving, "tracking": tracking,
-                "workloads": workloads}
+                "workloads": dict(workloads or {}, c2_mode2=same_work, plain_per_frame_c2=plain_c2)}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
