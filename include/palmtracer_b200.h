@@ -17,6 +17,26 @@
  *
  * Fit modes 0-5 keep the reference semantics (0 none, 1 Gaussian fixed sigma, 2 free sigma, 3 sigmaX/sigmaY,
  * 4 sigmaX/sigmaY/theta, 5 cubic spline EMCCD).
+ *
+ * Fit modes 6-8 are additions (the reference's fitRegions has no branch for them): Poisson maximum-likelihood fits of
+ * (background, photons, x, y, s) on photon counts (ADU - offset) / gain, FP32 iterations, FP64 final pass.
+ *   6 pixel-integrated Gaussian, s = sigma (px):  [roi, sigma0, offset, gain, maxIter, crlbMax]
+ *   7 astigmatic Gaussian, s = z (nm):            [roi, pixelSize (nm), z0x, wx, c3x, c4x, Ax, z0y, wy, c3y, c4y, Ay,
+ *                                                  offset, gain, maxIter, zMin, zMax, crlbMax]
+ *     sigma_axis(z) = (A / pixelSize) sqrt(1 + u^2 + c3 u^3 + c4 u^4), u = (z - z0) / w (the AstigFit model)
+ *   8 cubic spline, s = z (table cells):          [roi, sx, sy, sz, deltaZ, offset, gain, maxIter, crlbMax,
+ *                                                  64*sx*sy*sz coefficients (SoA [64][sz][sy][sx])]
+ * Their rows: X, Y, Z (nm; 0 for mode 6), Integrated intensity = photons, SigmaX/SigmaY (px; 0 for mode 8),
+ * Theta = the FP64 Poisson deviance of the fit (-2 log of its likelihood ratio to the saturated model; a goodness of
+ * fit), QualityXY = sqrt((CRLB_x^2 + CRLB_y^2) / 2) (px), QualityZ = CRLB_z (nm; -1 for mode 6), Amplitude, Offset =
+ * background photons per pixel. A fit whose QualityXY exceeds crlbMax (when > 0) or that fails is a sentinel row
+ * (-1 entries).
+ *
+ * Threading: every entry point may be called from several host threads at once (the reference is reentrant,
+ * CPU/main.cpp:18-26). Each call leases an engine of the current device's pool - its own CUDA streams, device
+ * workspace and launch-chain graphs - so concurrent calls run side by side on the GPU; a pool grows on demand up to
+ * PTB_MAX_ENGINES engines per device (default 8), after which callers wait for a free engine. Results do not depend
+ * on which engine ran a call.
  */
 #ifndef PALMTRACER_B200_H
 #define PALMTRACER_B200_H
@@ -70,6 +90,15 @@ PTB_API void Astigmatism3DEstimation(const double* input, double* output, uint64
  * (Plane, Id) pairs (equal pairs keep their input order). Writes nothing for nPoints = 0. */
 PTB_API void Tracking(const double* input, uint64_t* output, uint64_t nPoints, double maxDistance);
 
+/* Replaces the coefficient step of the spline calibration (lib/signal_processing/BSpline3D.cpp:17-164, run by
+ * Spline::Calibrate at lib/signal_processing/Spline.cpp:52 on the averaged bead PSF with lambda = {0, 0, 100 / dz}):
+ * the cubic smoothing-spline coefficient table of a PSF volume psf [nz][ny][nx] (x fastest; every dimension >= 2),
+ * with regularisation lambda[3] per axis x, y, z (NULL: none, an interpolating spline). coeffs receives
+ * 64 * (nx - 1) * (ny - 1) * (nz - 1) doubles in the layout the spline fits read, SoA [64][nz - 1][ny - 1][nx - 1]
+ * (the reference emits [cell][64]): the table of fit_params for modes 5 and 8 with sx = nx - 1, sy = ny - 1,
+ * sz = nz - 1. Returns the doubles written, 0 on error. */
+PTB_API uint64_t PTB_SplineCoefficients(const double* psf, uint64_t nx, uint64_t ny, uint64_t nz, const double* lambda, double* coeffs);
+
 /* ---- Additions (no counterpart in the reference) ---------------------------------------------------------------- */
 
 /* Tracking on DEVICE buffers of the current CUDA device, ordered on `stream` (a cudaStream_t; the call synchronizes
@@ -108,13 +137,19 @@ PTB_API uint64_t PTB_LocalizationDevice(const uint16_t* d_input, double* d_outpu
  * the same stack. PTB_PollStack: 0 queued or running, 1 done, -1 failed or unknown ticket. PTB_StackResult waits for
  * the request, releases the ticket and returns the doubles written (-1 on failure, message in PTB_LastError);
  * `times` (NULL or 2 doubles) receives the queueing delay and the latency from submission to completion in seconds.
- * PTB_ServerStop finishes the running stacks and fails the queued ones; call it with no other server call in flight. */
+ * PTB_ServerStop finishes the running stacks and fails the queued ones; call it with no other server call in flight.
+ * Fit modes 6-8 are fused across requests: the slots hand each chunk's candidates to one fit stage, which waits a
+ * short window (PTB_FUSE_WINDOW_US, default 300 us) for the chunks of the other busy slots and fits all chunks with
+ * the same fit settings in ONE persistent launch over a shared device work queue, then scatters the rows back per
+ * request (PTB_FUSE_FITS=0: each slot fits its own chunks). PTB_ServerFuseStats: counts[0] fused launches, counts[1]
+ * chunks fitted by them, since the server started. */
 PTB_API int PTB_ServerStart(int slots, uint64_t budgetBytes);
 PTB_API uint64_t PTB_SubmitStack(const uint16_t* input, double* output, uint64_t outputSize, uint64_t height, uint64_t width,
                                  uint64_t planes, double thresholdVal, double watershedRatio, uint64_t fit, const double* fit_params);
 PTB_API int PTB_PollStack(uint64_t ticket);
 PTB_API int64_t PTB_StackResult(uint64_t ticket, double* times);
 PTB_API void PTB_ServerStop(void);
+PTB_API void PTB_ServerFuseStats(uint64_t* counts, int n);
 
 /* Fit-only at caller-given positions with no device memory allocation: for callers that cannot call cudaMalloc
  * (code running inside another runtime's stream callbacks or under a fixed pre-sized memory pool) but can pass device
@@ -130,11 +165,22 @@ PTB_API uint64_t PTB_FittingDeviceNoAlloc(const uint16_t* d_input, const double*
                                           double* d_output, uint64_t height, uint64_t width, uint64_t planes, uint64_t fit,
                                           const double* fit_params, void* stream);
 
-/* Segmentation mode. 0 (default): each 8-connected component of the thresholded potential is flooded on its own,
- * in parallel. 1 (strict): each frame is flooded as one unit with a frame-global pop counter, exactly as the
- * reference's single priority queue does (Segmentation2D.cpp:336-385); slower, exact for any threshold.
+/* Segmentation mode. Both modes give the reference's labels (Segmentation2D.cpp:336-385) for any threshold.
+ * 0 (default): each 8-connected component of the thresholded potential is flooded on its own, in parallel, and then
+ * tested: the flood of a component equals the reference's frame-wide flood when, at every basin boundary, the lowest
+ * W1 along the winning parent chain exceeds the competing neighbour's W1 by more than the largest aging term the
+ * frame-wide flood can add (the frame's domain pixel count x 1e-7). A frame failing the test anywhere is flooded
+ * again as one unit with the frame-global pop counter. 1 (strict): every frame is flooded as one unit.
  * Returns the previous mode. */
 PTB_API int PTB_SetSegmentationMode(int mode);
+
+/* Segmentation diagnostics of the current device's engines since the last call: counts[0] frames segmented,
+ * counts[1] frames flooded again frame-wide in mode 0 (up to n entries). */
+PTB_API void PTB_SegmentationStats(uint64_t* counts, int n);
+
+/* Engine pool of the current device (diagnostics): counts[0] engines created, counts[1] the most engines leased at
+ * the same time (up to n entries). */
+PTB_API void PTB_EnginePoolStats(uint64_t* counts, int n);
 
 /* Fit arithmetic for the Gaussian least-squares modes 1-4. 0 (default): FP64, one thread per ROI, in the
  * reference's exact order of operations (same iteration path as the reference); 1: FP32 iterations, one warp per
@@ -165,7 +211,7 @@ PTB_API void PTB_StageTimes(double* ms, uint64_t* launches, int n);
  * then resets them. */
 PTB_API void PTB_MleEvaluations(uint64_t* counts, int n);
 
-/* Launch-chain graphs of the current device's engine (diagnostics). A chunk's compute chain (counter reset,
+/* Launch-chain graphs of the current device's engines (diagnostics). A chunk's compute chain (counter reset,
  * detection, segmentation, candidates, fits) is launched directly the first time its launch arguments occur, captured
  * into a CUDA graph the second time and replayed from the graph after that (PTB_GRAPHS=0 turns graphs off).
  * counts: [chunks captured, chunks replayed, chunks launched directly] since the last call (up to n entries). */

@@ -179,6 +179,25 @@ class OracleLib(CpuLib):
             return None
         return float(d[0]), g, h.reshape(5, 5)
 
+    def spline_coefficients(self, volume, lam=None, with_centres=False):
+        """The spline calibration's coefficient table of a PSF volume [nz, ny, nx]: [cells, 64] in the reference's
+        layout (cells z, y, x); with_centres also returns the spline's values at the voxel centres."""
+        volume = np.ascontiguousarray(volume, dtype=np.float64)
+        nz, ny, nx = volume.shape
+        out = np.zeros(((nz - 1) * (ny - 1) * (nx - 1), 64))
+        hdr = np.zeros_like(volume)
+        f = self.lib.orc_SplineCoefficients
+        f.restype = _u64
+        f.argtypes = [_f64p, _u64, _u64, _u64, _f64p, _f64p, _f64p]
+        lam_p = None
+        if lam is not None:
+            lam = np.ascontiguousarray(lam, dtype=np.float64)
+            lam_p = _ptr(lam, _f64p)
+        n = f(_ptr(volume, _f64p), nx, ny, nz, lam_p, _ptr(out, _f64p), _ptr(hdr, _f64p))
+        if n == 0 or n != out.size:
+            raise RuntimeError("orc_SplineCoefficients failed")
+        return (out, hdr) if with_centres else out
+
     def mle_fit_one(self, frame, cx, cy, fit, params):
         """(status, theta, crlb, deviance) of one candidate's fit: status 1 success, 2 failed, 0 border."""
         frame = np.ascontiguousarray(frame, dtype=np.uint16)

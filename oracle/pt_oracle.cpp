@@ -13,6 +13,7 @@
 //   orc_Planes, orc_Candidates, orc_CandidatesFromPotential, orc_Labels - per-stage products
 //   orc_Astig3DEstimation - z from (sigma_x, sigma_y) with the astigmatism model (the reference's export of that name)
 //   orc_Tracking          - frame-to-frame linking (the reference's export of that name)
+//   orc_SplineCoefficients - cubic-spline coefficient table of a PSF volume (spline calibration's BSpline3D step)
 #include <omp.h>
 
 #include <algorithm>
@@ -20,6 +21,7 @@
 #include <cfloat>
 #include <cmath>
 #include <compare>
+#include <complex>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -1372,13 +1374,13 @@ void FitMle(const MleCfg& c, const uint16_t* img, int W, int H, const Candidate&
 	out[cY] = static_cast<double>(uy) + t[3];
 	out[cZ] = z;
 	out[cIntensity] = t[1];
-	out[cSigmaX] = sx; out[cSigmaY] = sy; out[cTheta] = 0;
+	// Theta (no rotation in these models): the FP64 deviance at the result, the fit's log-likelihood ratio
+	out[cSigmaX] = sx; out[cSigmaY] = sy; out[cTheta] = dev;
 	out[cQualityXY] = qxy; out[cQualityZ] = qz;
 	out[cAmplitude] = (sx > 0 && sy > 0) ? t[1] / (6.283185307179586 * sx * sy) : t[1];
 	out[cOffset] = t[0];
 	out[cSegIntensity] = cd.intensity; out[cSurface] = cd.surf;
 	out[cCircularity] = (sx > kEps && sy > kEps) ? std::min(sx, sy) / std::max(sx, sy) : 1;
-	(void)dev;
 }
 
 }  // namespace
@@ -1426,6 +1428,134 @@ void ProcessFrame(const uint16_t* img, int H, int W, double thr, double ratio, s
 		}
 	}
 	std::sort(rows.begin(), rows.end(), RowLess);
+}
+
+}  // namespace
+
+namespace {
+
+// ---------------------------------------------------------------------------------------------
+// Spline calibration: the cubic B-spline coefficient table of a PSF volume (lib/signal_processing/BSpline3D.cpp,
+// constructed by the calibration at lib/signal_processing/Spline.cpp:52 with degree 3 and lambda = {0, 0, 100 / dz}).
+// Degree 3 only (the degree the calibration uses). Steps of BSpline3D::BSpline3D (:17-45):
+//   1. per axis, the exponential filters of its poles (getPolesFilter :171-214: lambda = 0 -> pole sqrt3 - 2, gain 6;
+//      lambda > 0 -> the roots of 1 - 4z + 6z^2 - 4z^3 + z^4 + (z + 4z^2 + z^3) / (6 lambda) with |z| <= 1 from
+//      Durand-Kerner (solvePolynomial :372-430), gain 1 / lambda), applied along every line with mirror
+//      initialisation over K0 = ceil(log(eps) / log|z|) terms (applyFilter :284-331, symExpFilt :438-449; Unser,
+//      Aldroubi & Eden 1991), the real part times the gain kept after each axis;
+//   2. reflection padding by one voxel (:23-41, Matrix.cpp ReflectIndex1D :426-444);
+//   3. the spline's values at the voxel centres (interpolateHDR :334-348, interpolate_at :351-385);
+//   4. those values upsampled by 3 as cubic B-spline control points with zeros outside
+//      (Interpolation3D::Upsample :188-229 with spline3D :114-145), and per cell the 64 monomial coefficients that
+//      reproduce its 4 x 4 x 4 samples, A^-1 samples with the Gauss-Jordan inverse of A (getFinalCoeff :99-164).
+// Coefficient k = l * 16 + m * 4 + n of cell (x, y, z) multiplies zf^l yf^m xf^n (the reference's naming: its "Dx"
+// runs along z).
+
+// BSpline3D::Eval(x, 3) (BSpline3D.cpp:76-88), same operations and order.
+double Bspline3(double x)
+{
+	constexpr double Edge = 4.0 / 3.0, Center = 2.0 / 3.0, A = 2.0, C = 1.0 / 6.0, D = 0.5;
+	const double X2 = x * x, X3 = X2 * x;
+	if (x >= -2 && x < -1) { return Edge + (A * x) + X2 + (C * X3); }
+	if (x >= -1 && x < 0) { return Center - X2 - (D * X3); }
+	if (x >= 0 && x < 1) { return Center - X2 + (D * X3); }
+	if (x >= 1 && x < 2) { return Edge - (A * x) + X2 - (C * X3); }
+	return 0;
+}
+
+using cplx = std::complex<double>;
+
+// Durand-Kerner roots of a real polynomial (coefficients from the highest degree), as solvePolynomial does for
+// degrees other than 3: 0.4 e^{2 pi i k / deg} start, simultaneous updates, stop when every |delta| <= tol.
+std::vector<cplx> DurandKerner(const std::vector<double>& c, double tol = 1e-12, int maxIter = 100)
+{
+	const size_t deg = c.size() - 1;
+	std::vector<cplx> roots(deg);
+	for (size_t k = 0; k < deg; ++k) {
+		const double th = 2.0 * std::numbers::pi * static_cast<double>(k) / static_cast<double>(deg);
+		roots[k] = 0.4 * cplx(std::cos(th), std::sin(th));
+	}
+	auto eval = [&](cplx x) {
+		cplx v = 0.0;
+		for (size_t i = 0; i <= deg; ++i) { v += c[i] * std::pow(x, static_cast<int>(deg - i)); }
+		return v;
+	};
+	for (int it = 0; it < maxIter; ++it) {
+		bool converged = true;
+		std::vector<cplx> next = roots;
+		for (size_t i = 0; i < deg; ++i) {
+			cplx den = 1.0;
+			for (size_t j = 0; j < deg; ++j) {
+				if (j != i) { den *= roots[i] - roots[j]; }
+			}
+			const cplx d = eval(roots[i]) / den;
+			next[i] = roots[i] - d;
+			if (std::abs(d) > tol) { converged = false; }
+		}
+		roots = next;
+		if (converged) { break; }
+	}
+	return roots;
+}
+
+// Poles and gain of the degree-3 smoothing-spline filter for one axis (getPolesFilter, case 3).
+void CubicPoles(double lambda, std::vector<cplx>& poles, double& gain)
+{
+	poles.clear();
+	if (lambda <= std::numeric_limits<double>::epsilon()) {
+		poles.emplace_back(std::numbers::sqrt3 - 2.0);
+		gain = 6.0;
+		return;
+	}
+	std::vector<double> p{1, -4, 6, -4, 1};
+	p[1] += 1.0 / (6.0 * lambda);
+	p[2] += 2.0 / (3.0 * lambda);
+	p[3] += 1.0 / (6.0 * lambda);
+	for (const cplx& z : DurandKerner(p)) {
+		if (std::abs(z) <= 1.0) { poles.push_back(z); }
+	}
+	gain = 1.0 / lambda;
+}
+
+// Mirror index sequence 0, 1, .., n-1, n-2, .., 1, 0, 1, .. (Matrix.cpp ReflectionIndices :413-423), entry k.
+size_t Reflection(size_t n, size_t k) { return n == 1 ? 0 : (k % (2 * n - 2) < n ? k % (2 * n - 2) : 2 * n - 2 - k % (2 * n - 2)); }
+
+// One line through the symmetric exponential filter of pole z (symExpFilt).
+void SymExpFilt(std::vector<cplx>& x, cplx z, size_t k0)
+{
+	const size_t n = x.size();
+	const cplx c0 = -z / (1.0 - z * z);
+	std::vector<cplx> y(n, 0.0);
+	for (size_t k = 0; k < k0; ++k) { y[0] += std::pow(z, static_cast<int>(k)) * x[Reflection(n, k)]; }
+	for (size_t k = 1; k < n; ++k) { y[k] = x[k] + z * y[k - 1]; }
+	y[n - 1] = (2.0 * y[n - 1] - x[n - 1]) * c0;
+	for (int k = static_cast<int>(n) - 2; k >= 0; --k) { y[k] = (y[k + 1] - y[k]) * z; }
+	x.swap(y);
+}
+
+// coeffs [nz][ny][nx] filtered along `axis` (0 x, 1 y, 2 z) by every pole, then real part times the gain (applyFilter).
+void FilterAxis(std::vector<double>& coeffs, const size_t dim[3], int axis, const std::vector<cplx>& poles, double gain)
+{
+	const size_t nx = dim[0], ny = dim[1], nz = dim[2];
+	const size_t n = dim[axis];
+	std::vector<cplx> tmp(coeffs.begin(), coeffs.end()), line(n);
+	auto at = [&](size_t x, size_t y, size_t z) { return (z * ny + y) * nx + x; };
+	const double k0tol = std::log(std::numeric_limits<double>::epsilon());
+	for (const cplx& z : poles) {
+		const auto k0 = static_cast<size_t>(std::ceil(k0tol / std::log(std::abs(z))));
+		const size_t outerA = axis == 2 ? ny : nz, outerB = axis == 0 ? ny : nx;
+		for (size_t a = 0; a < outerA; ++a) {
+			for (size_t b = 0; b < outerB; ++b) {
+				auto idx = [&](size_t i) {
+					return axis == 0 ? at(i, b, a) : axis == 1 ? at(b, i, a) : at(b, a, i);
+				};
+				for (size_t i = 0; i < n; ++i) { line[i] = tmp[idx(i)]; }
+				SymExpFilt(line, z, k0);
+				for (size_t i = 0; i < n; ++i) { tmp[idx(i)] = line[i]; }
+			}
+		}
+	}
+	for (size_t i = 0; i < coeffs.size(); ++i) { coeffs[i] = std::real(tmp[i]) * gain; }
 }
 
 }  // namespace
@@ -1810,6 +1940,145 @@ uint64_t orc_Tracking(const double* input, uint64_t* output, uint64_t nPoints, d
 		output[2 * k + 1] = track[k];
 	}
 	return 2 * nPoints;
+}
+
+
+// orc_SplineCoefficients: the coefficient table of a PSF volume [nz][ny][nx] (x fastest) as BSpline3D computes it
+// (degree 3, regularisation lambda[3] per axis x, y, z; NULL = none): out receives the reference's layout
+// [cell][64] with cells (z, y, x) over (nz - 1) x (ny - 1) x (nx - 1); hdr (optional) the spline's values at the
+// voxel centres (step 3). Returns the doubles written, 0 for a dimension below 2.
+uint64_t orc_SplineCoefficients(const double* volume, uint64_t nx, uint64_t ny, uint64_t nz, const double* lambda, double* out,
+                                double* hdrOut)
+{
+	if (nx < 2 || ny < 2 || nz < 2) { return 0; }
+	const size_t dim[3] = {nx, ny, nz};
+	const size_t n = nx * ny * nz;
+	std::vector<double> c(volume, volume + n);
+	for (int axis = 0; axis < 3; ++axis) {
+		std::vector<cplx> poles;
+		double gain = 1;
+		CubicPoles(lambda ? lambda[axis] : 0.0, poles, gain);
+		FilterAxis(c, dim, axis, poles, gain);
+	}
+	// reflection padding by 1 (dimPadded = dim + 3) and the values at the voxel centres
+	const size_t px = nx + 3, py = ny + 3, pz = nz + 3;
+	auto refl = [](size_t len, long i) {  // ReflectIndex1D(len, 1) entry i + 1
+		const long period = 2 * static_cast<long>(len) - 2;
+		const long w = ((i % period) + period) % period;
+		return static_cast<size_t>(w < static_cast<long>(len) ? w : period - w);
+	};
+	std::vector<double> padded(px * py * pz);
+	for (size_t z = 0; z < pz; ++z) {
+		for (size_t y = 0; y < py; ++y) {
+			for (size_t x = 0; x < px; ++x) {
+				const size_t src = (refl(nz, static_cast<long>(z) - 1) * ny + refl(ny, static_cast<long>(y) - 1)) * nx + refl(nx, static_cast<long>(x) - 1);
+				padded[(z * py + y) * px + x] = c[src];
+			}
+		}
+	}
+	std::vector<double> hdr(n);
+	for (size_t z = 0; z < nz; ++z) {
+		for (size_t y = 0; y < ny; ++y) {
+			for (size_t x = 0; x < nx; ++x) {
+				// interpolate_at(x + 1, y + 1, z + 1) on the padded coefficients
+				const double X = static_cast<double>(x) + 1, Y = static_cast<double>(y) + 1, Z = static_cast<double>(z) + 1;
+				const long kx = static_cast<long>(std::floor(X)) - 1, ky = static_cast<long>(std::floor(Y)) - 1,
+				           kz = static_cast<long>(std::floor(Z)) - 1;
+				double r = 0.0;
+				for (long q = 0; q <= 3; ++q) {
+					const long iz = kz + q;
+					if (iz < 0 || iz >= static_cast<long>(pz)) { continue; }
+					const double bz = Bspline3(Z - static_cast<double>(iz));
+					for (long i = 0; i <= 3; ++i) {
+						const long iy = ky + i;
+						if (iy < 0 || iy >= static_cast<long>(py)) { continue; }
+						const double byz = Bspline3(Y - static_cast<double>(iy)) * bz;
+						for (long j = 0; j <= 3; ++j) {
+							const long ix = kx + j;
+							if (ix < 0 || ix >= static_cast<long>(px)) { continue; }
+							const double bx = Bspline3(X - static_cast<double>(ix));
+							r += padded[(static_cast<size_t>(iz) * py + static_cast<size_t>(iy)) * px + static_cast<size_t>(ix)] * bx * byz;
+						}
+					}
+				}
+				hdr[(z * ny + y) * nx + x] = r;
+			}
+		}
+	}
+	if (hdrOut) { std::copy(hdr.begin(), hdr.end(), hdrOut); }
+	// the 64 x 64 system of the monomials at the 1/3 samples, inverted once
+	std::vector<double> A(64 * 64), Ai(64 * 64);
+	for (int i = 0; i < 4; ++i) {
+		const double dx = static_cast<double>(i) / 3.0;
+		for (int j = 0; j < 4; ++j) {
+			const double dy = static_cast<double>(j) / 3.0;
+			for (int k = 0; k < 4; ++k) {
+				const double dz = static_cast<double>(k) / 3.0;
+				const int row = i * 16 + j * 4 + k;
+				for (int l = 0; l < 4; ++l) {
+					for (int m = 0; m < 4; ++m) {
+						for (int q = 0; q < 4; ++q) {
+							A[row * 64 + l * 16 + m * 4 + q] = std::pow(dx, l) * std::pow(dy, m) * std::pow(dz, q);
+						}
+					}
+				}
+			}
+		}
+	}
+	if (!InvertGaussJordan(A, Ai, 64)) { return 0; }
+	// upsampled values (Upsample by 3 with spline3D on hdr, zeros outside)
+	const size_t ux = (nx - 1) * 3 + 1, uy = (ny - 1) * 3 + 1, uz = (nz - 1) * 3 + 1;
+	const double step = 1.0 / 3.0;
+	auto get = [&](long x, long y, long z) {
+		if (x < 0 || x >= static_cast<long>(nx) || y < 0 || y >= static_cast<long>(ny) || z < 0 || z >= static_cast<long>(nz)) { return 0.0; }
+		return hdr[(static_cast<size_t>(z) * ny + static_cast<size_t>(y)) * nx + static_cast<size_t>(x)];
+	};
+	std::vector<double> up(ux * uy * uz);
+	for (size_t z = 0; z < uz; ++z) {
+		const double pzp = static_cast<double>(z) * step;
+		for (size_t y = 0; y < uy; ++y) {
+			const double pyp = static_cast<double>(y) * step;
+			for (size_t x = 0; x < ux; ++x) {
+				const double pxp = static_cast<double>(x) * step;
+				const long ix = static_cast<long>(std::floor(pxp)), iy = static_cast<long>(std::floor(pyp)), iz = static_cast<long>(std::floor(pzp));
+				double v = 0.0;
+				for (long dz = -1; dz <= 2; ++dz) {
+					const long Zi = iz + dz;
+					const double bz = Bspline3(pzp - static_cast<double>(Zi));
+					for (long dy = -1; dy <= 2; ++dy) {
+						const long Yi = iy + dy;
+						const double byz = Bspline3(pyp - static_cast<double>(Yi)) * bz;
+						for (long dx = -1; dx <= 2; ++dx) {
+							const long Xi = ix + dx;
+							v += get(Xi, Yi, Zi) * (Bspline3(pxp - static_cast<double>(Xi)) * byz);
+						}
+					}
+				}
+				up[(z * uy + y) * ux + x] = v;
+			}
+		}
+	}
+	const size_t cx = nx - 1, cy = ny - 1, cz = nz - 1;
+	size_t base = 0;
+	for (size_t z = 0; z < cz; ++z) {
+		for (size_t y = 0; y < cy; ++y) {
+			for (size_t x = 0; x < cx; ++x, base += 64) {
+				double t[64];
+				size_t q = 0;
+				for (size_t k = 0; k < 4; ++k) {
+					for (size_t j = 0; j < 4; ++j) {
+						for (size_t i = 0; i < 4; ++i, ++q) { t[q] = up[((z * 3 + k) * uy + (y * 3 + j)) * ux + (x * 3 + i)]; }
+					}
+				}
+				for (size_t i = 0; i < 64; ++i) {
+					double acc = 0.0;
+					for (size_t j = 0; j < 64; ++j) { acc += Ai[i * 64 + j] * t[j]; }
+					out[base + i] = acc;
+				}
+			}
+		}
+	}
+	return static_cast<uint64_t>(cx * cy * cz * 64);
 }
 
 }  // extern "C"

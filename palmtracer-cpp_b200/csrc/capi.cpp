@@ -2,9 +2,9 @@
 // entry point catches, records the message for PTB_LastError() and returns the reference's neutral value.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <exception>
 #include <iostream>
-#include <mutex>
 
 #include "../../include/palmtracer_b200.h"
 #include "engine.h"
@@ -26,8 +26,8 @@ PTB_API uint64_t Localization(const uint16_t* input, double* output, uint64_t ou
 {
 	ptb::ClearError();
 	try {
-		std::unique_lock<std::mutex> lock;
-		ptb::Engine& e = ptb::EngineFor(lock);
+		ptb::EngineLease lease;
+		ptb::Engine& e = *lease;
 		const long long n = e.Localize(input, false, output, false, outputSize, height, width, planes, thresholdVal,
 		                               watershedRatio, fit, fit_params);
 		if (n < 0) { Report("Localization"); return 0; }
@@ -45,8 +45,8 @@ PTB_API uint64_t Fitting(const uint16_t* input, const double* positions, uint64_
 {
 	ptb::ClearError();
 	try {
-		std::unique_lock<std::mutex> lock;
-		ptb::Engine& e = ptb::EngineFor(lock);
+		ptb::EngineLease lease;
+		ptb::Engine& e = *lease;
 		const long long n = e.FitPositions(input, positions, nPoints, output, height, width, planes, fit, fit_params);
 		if (n < 0) { Report("Fitting"); return 0; }
 		return static_cast<uint64_t>(n);
@@ -65,8 +65,8 @@ PTB_API void Wavelett(const uint16_t* input, double* output, uint64_t height, ui
 		if (planes == 0) { return; }
 		if (levelOutput == 0) { levelOutput = 1; }
 		const int level = static_cast<int>(std::min<uint64_t>(levelOutput - 1, 2));
-		std::unique_lock<std::mutex> lock;
-		ptb::Engine& e = ptb::EngineFor(lock);
+		ptb::EngineLease lease;
+		ptb::Engine& e = *lease;
 		if (!e.Planes(input, output, height, width, planes, level)) { Report("Wavelett"); }
 	}
 	catch (const std::exception& ex) {
@@ -79,8 +79,8 @@ PTB_API double AutoThreshold(const uint16_t* input, uint64_t height, uint64_t wi
 {
 	ptb::ClearError();
 	try {
-		std::unique_lock<std::mutex> lock;
-		ptb::Engine& e = ptb::EngineFor(lock);
+		ptb::EngineLease lease;
+		ptb::Engine& e = *lease;
 		const double t = e.AutoThreshold(input, height, width, fit_params);
 		if (!ptb::LastError().empty()) { Report("AutoThreshold"); }
 		return t;
@@ -98,8 +98,8 @@ PTB_API void Astigmatism3DEstimation(const double* input, double* output, uint64
 	ptb::ClearError();
 	try {
 		if (size == 0) { return; }
-		std::unique_lock<std::mutex> lock;
-		if (!ptb::EngineFor(lock).AstigEstimate(input, output, size, pixelSize, model, zMax)) { Report("Astigmatism3DEstimation"); }
+		ptb::EngineLease lease;
+		if (!lease->AstigEstimate(input, output, size, pixelSize, model, zMax)) { Report("Astigmatism3DEstimation"); }
 	}
 	catch (const std::exception& ex) {
 		ptb::SetError(ex.what());
@@ -111,8 +111,8 @@ PTB_API void Tracking(const double* input, uint64_t* output, uint64_t nPoints, d
 {
 	ptb::ClearError();
 	try {
-		std::unique_lock<std::mutex> lock;
-		if (!ptb::EngineFor(lock).Track(input, output, nPoints, maxDistance)) { Report("Tracking"); }
+		ptb::EngineLease lease;
+		if (!lease->Track(input, output, nPoints, maxDistance)) { Report("Tracking"); }
 	}
 	catch (const std::exception& ex) {
 		ptb::SetError(ex.what());
@@ -120,12 +120,30 @@ PTB_API void Tracking(const double* input, uint64_t* output, uint64_t nPoints, d
 	}
 }
 
+PTB_API uint64_t PTB_SplineCoefficients(const double* psf, uint64_t nx, uint64_t ny, uint64_t nz, const double* lambda, double* coeffs)
+{
+	ptb::ClearError();
+	try {
+		ptb::EngineLease lease;
+		if (!lease->Init() || !ptb::SplineCoefficients(psf, nx, ny, nz, lambda, coeffs, lease->Stream())) {
+			Report("PTB_SplineCoefficients");
+			return 0;
+		}
+		return 64 * (nx - 1) * (ny - 1) * (nz - 1);
+	}
+	catch (const std::exception& ex) {
+		ptb::SetError(ex.what());
+		Report("PTB_SplineCoefficients");
+		return 0;
+	}
+}
+
 PTB_API uint64_t PTB_TrackingDevice(const double* d_input, uint64_t* d_output, uint64_t nPoints, double maxDistance, void* stream)
 {
 	ptb::ClearError();
 	try {
-		std::unique_lock<std::mutex> lock;
-		ptb::Engine& e = ptb::EngineFor(lock);
+		ptb::EngineLease lease;
+		ptb::Engine& e = *lease;
 		if (!e.Init()) { Report("PTB_TrackingDevice"); return 0; }
 		if (!ptb::TrackDevice(d_input, d_output, nPoints, maxDistance, static_cast<cudaStream_t>(stream))) {
 			Report("PTB_TrackingDevice");
@@ -181,8 +199,8 @@ PTB_API uint64_t PTB_LocalizationTiff(const char* path, double* output, uint64_t
 		ptb::TiffStack t;
 		if (!t.Open(path)) { Report("PTB_LocalizationTiff"); return 0; }
 		const ptb::Engine::PageSource source = [&t](uint64_t first, uint64_t count, uint16_t* dst) { return t.Read(first, count, dst); };
-		std::unique_lock<std::mutex> lock;
-		ptb::Engine& e = ptb::EngineFor(lock);
+		ptb::EngineLease lease;
+		ptb::Engine& e = *lease;
 		const long long n = e.Localize(nullptr, false, output, false, outputSize, t.Height(), t.Width(), t.Planes(), thresholdVal,
 		                               watershedRatio, fit, fit_params, &source);
 		if (n < 0) { Report("PTB_LocalizationTiff"); return 0; }
@@ -201,8 +219,8 @@ PTB_API uint64_t PTB_LocalizationDevice(const uint16_t* d_input, double* d_outpu
 {
 	ptb::ClearError();
 	try {
-		std::unique_lock<std::mutex> lock;
-		ptb::Engine& e = ptb::EngineFor(lock);
+		ptb::EngineLease lease;
+		ptb::Engine& e = *lease;
 		if (!e.Init()) { Report("PTB_LocalizationDevice"); return 0; }
 		const cudaStream_t own = e.Stream();
 		cudaStream_t user = static_cast<cudaStream_t>(stream);
@@ -232,11 +250,7 @@ PTB_API uint64_t PTB_FittingDeviceNoAlloc(const uint16_t* d_input, const double*
 {
 	ptb::ClearError();
 	try {
-		int precision = 0;
-		{
-			std::unique_lock<std::mutex> lock;
-			precision = ptb::EngineFor(lock).Precision();  // reads a setting; initialises no device state
-		}
+		const int precision = ptb::SettingsFor().precision.load();  // a setting; initialises no device state
 		const long long n = ptb::FittingDeviceNoAlloc(d_input, d_positions, nPoints, d_output, height, width, planes, fit,
 		                                              fit_params, precision, ptb::EnvLanes(), static_cast<cudaStream_t>(stream));
 		if (n < 0) { Report("PTB_FittingDeviceNoAlloc"); return 0; }
@@ -249,17 +263,9 @@ PTB_API uint64_t PTB_FittingDeviceNoAlloc(const uint16_t* d_input, const double*
 	}
 }
 
-PTB_API int PTB_SetSegmentationMode(int mode)
-{
-	std::unique_lock<std::mutex> lock;
-	return ptb::EngineFor(lock).SetStrict(mode ? 1 : 0);
-}
+PTB_API int PTB_SetSegmentationMode(int mode) { return ptb::SettingsFor().strict.exchange(mode ? 1 : 0); }
 
-PTB_API int PTB_SetFitPrecision(int mode)
-{
-	std::unique_lock<std::mutex> lock;
-	return ptb::EngineFor(lock).SetPrecision(mode < 0 ? 0 : (mode > 2 ? 2 : mode));
-}
+PTB_API int PTB_SetFitPrecision(int mode) { return ptb::SettingsFor().precision.exchange(mode < 0 ? 0 : (mode > 2 ? 2 : mode)); }
 
 PTB_API const char* PTB_LastError(void) { return ptb::LastError().c_str(); }
 
@@ -271,16 +277,26 @@ PTB_API double PTB_MeasureFmaPeak(int fp64)
 	return ptb::MeasureFmaPeak(fp64);
 }
 
-PTB_API int PTB_SetProfiling(int enable)
-{
-	std::unique_lock<std::mutex> lock;
-	return ptb::EngineFor(lock).SetProfiling(enable ? 1 : 0);
-}
+PTB_API int PTB_SetProfiling(int enable) { return ptb::SettingsFor().profiling.exchange(enable ? 1 : 0); }
 
 PTB_API void PTB_StageTimes(double* ms, uint64_t* launches, int n)
 {
-	std::unique_lock<std::mutex> lock;
-	ptb::EngineFor(lock).StageTimes(ms, launches, n);
+	constexpr int kMax = 16;
+	double sumMs[kMax] = {};
+	uint64_t sumL[kMax] = {};
+	n = std::max(0, std::min(n, kMax));
+	for (int i = 0;; ++i) {
+		ptb::EngineLease lease(i);
+		if (!lease) { break; }
+		double m[kMax] = {};
+		uint64_t l[kMax] = {};
+		lease->StageTimes(m, l, n);
+		for (int k = 0; k < n; ++k) { sumMs[k] += m[k]; sumL[k] += l[k]; }
+	}
+	for (int k = 0; k < n; ++k) {
+		if (ms) { ms[k] = sumMs[k]; }
+		if (launches) { launches[k] = sumL[k]; }
+	}
 }
 
 PTB_API int PTB_ServerStart(int slots, uint64_t budgetBytes)
@@ -324,6 +340,8 @@ PTB_API uint64_t PTB_SubmitStack(const uint16_t* input, double* output, uint64_t
 	}
 }
 
+PTB_API void PTB_ServerFuseStats(uint64_t* counts, int n) { ptb::ServerFuseStats(counts, n); }
+
 PTB_API int PTB_PollStack(uint64_t ticket)
 {
 	try {
@@ -349,16 +367,46 @@ PTB_API int64_t PTB_StackResult(uint64_t ticket, double* times)
 	}
 }
 
+}  // extern "C"
+
+namespace {
+
+// Sums a counter diagnostic over every engine of the current device's pool (each read resets that engine's counters).
+template <typename Fn>
+void SumOverEngines(uint64_t* counts, int n, Fn read)
+{
+	constexpr int kMax = 16;
+	uint64_t sum[kMax] = {};
+	n = std::max(0, std::min(n, kMax));
+	for (int i = 0;; ++i) {
+		ptb::EngineLease lease(i);
+		if (!lease) { break; }
+		uint64_t v[kMax] = {};
+		read(*lease, v, n);
+		for (int k = 0; k < n; ++k) { sum[k] += v[k]; }
+	}
+	for (int k = 0; k < n && counts; ++k) { counts[k] = sum[k]; }
+}
+
+}  // namespace
+
+extern "C" {
+
 PTB_API void PTB_MleEvaluations(uint64_t* counts, int n)
 {
-	std::unique_lock<std::mutex> lock;
-	ptb::EngineFor(lock).MleEvaluations(counts, n);
+	SumOverEngines(counts, n, [](ptb::Engine& e, uint64_t* v, int k) { e.MleEvaluations(v, k); });
 }
 
 PTB_API void PTB_GraphStats(uint64_t* counts, int n)
 {
-	std::unique_lock<std::mutex> lock;
-	ptb::EngineFor(lock).GraphStats(counts, n);
+	SumOverEngines(counts, n, [](ptb::Engine& e, uint64_t* v, int k) { e.GraphStats(v, k); });
 }
+
+PTB_API void PTB_SegmentationStats(uint64_t* counts, int n)
+{
+	SumOverEngines(counts, n, [](ptb::Engine& e, uint64_t* v, int k) { e.SegmentationStats(v, k); });
+}
+
+PTB_API void PTB_EnginePoolStats(uint64_t* counts, int n) { ptb::PoolStats(counts, n); }
 
 }  // extern "C"

@@ -307,6 +307,9 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 		}
 		scanSm[2 * kWarps] = sd ? atomicAdd(&ws.cnt->ndom, sd) : 0u;
 		scanSm[2 * kWarps + 1] = ss ? atomicAdd(&ws.cnt->nseed, ss) : 0u;
+		// per-frame counts: the watershed's exactness bound and the lists of frames flooded again frame-wide
+		if (sd) { atomicAdd(ws.frameDom + f, sd); }
+		if (ss) { atomicAdd(ws.frameSeeds + f, ss); }
 	}
 	__syncthreads();
 	uint32_t pd = scanSm[2 * kWarps] + scanSm[warp] + id - nd;
@@ -373,16 +376,16 @@ __global__ void __launch_bounds__(kThreads) PlaneKernel(const uint16_t* __restri
 	}
 }
 
+// Once per process (a function-local static is initialised once, also when several threads call at the same time).
 bool ConfigureSmem()
 {
-	static bool done = false;
-	if (done) { return true; }
-	const int bytes = static_cast<int>(sizeof(TileSmem));
-	bool ok = PTB_CUDA(cudaFuncSetAttribute(DetectKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-	                                        static_cast<int>(kDetectWords * sizeof(uint32_t))));
-	ok = ok && PTB_CUDA(cudaFuncSetAttribute(PlaneKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-	done = ok;
-	return ok;
+	static const bool done = [] {
+		const int bytes = static_cast<int>(sizeof(TileSmem));
+		bool ok = PTB_CUDA(cudaFuncSetAttribute(DetectKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                                        static_cast<int>(kDetectWords * sizeof(uint32_t))));
+		return ok && PTB_CUDA(cudaFuncSetAttribute(PlaneKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+	}();
+	return done;
 }
 
 }  // namespace

@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
 #include <iostream>
 #include <mutex>
@@ -229,6 +230,11 @@ static size_t PlanWorkspace(Workspace& ws, int H, int W, int B, uint32_t rowsCap
 	take(ws.fuNeighbour, capComp);
 	take(ws.fuBecome, capComp);
 	take(ws.fuLocked, capComp);
+	take(ws.frameDom, 3 * (static_cast<size_t>(B) + 1));  // frameDom, frameSeeds, frameRoute (zeroed together)
+	if (base) {
+		ws.frameSeeds = ws.frameDom + B + 1;
+		ws.frameRoute = ws.frameSeeds + B + 1;
+	}
 	take(ws.frameRegBase, static_cast<size_t>(B) + 1);
 	take(ws.frameCandBase, static_cast<size_t>(B) + 1);
 	take(ws.frameKeep, static_cast<size_t>(B) + 1);
@@ -408,7 +414,8 @@ static std::vector<uint64_t> ChainKey(int slot, const Workspace& ws, const uint1
 	d(f.intensityRatio); p(f.coeffs); u(static_cast<uint64_t>(f.lanes)); p(f.marks);
 	const MleParams& m = f.mle;
 	u(static_cast<uint64_t>(m.model)); u(static_cast<uint64_t>(m.roi)); u(static_cast<uint64_t>(m.half));
-	u(static_cast<uint64_t>(m.n)); u(static_cast<uint64_t>(m.maxIter)); d(m.sigma0); d(m.offset); d(m.gain); d(m.crlbMax);
+	u(static_cast<uint64_t>(m.n)); u(static_cast<uint64_t>(m.maxIter)); u(static_cast<uint64_t>(m.chunk)); d(m.sigma0);
+	d(m.offset); d(m.gain); d(m.crlbMax);
 	d(m.pixelSize); d(m.zMin); d(m.zMax);
 	for (double a : m.astig) { d(a); }
 	u(static_cast<uint64_t>(m.sx)); u(static_cast<uint64_t>(m.sy)); u(static_cast<uint64_t>(m.sz)); d(m.dz);
@@ -477,6 +484,7 @@ bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, d
 	ws.img = dImg;
 	cudaStream_t st = St(slot);
 	const bool prof = profiling_ != 0;
+	segCounts_[0] += static_cast<uint64_t>(B);
 	uint64_t l0 = LaunchCount();
 	auto mark = [&](int k) {
 		if (prof) {
@@ -485,12 +493,13 @@ bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, d
 		}
 	};
 	FitParams fpr = fp;
-	if (fpr.mode >= kMleGauss) {
-		if (fpr.lanes == 0) { fpr.lanes = TunedLanes(fpr, SizeClass(B, H, W)); }
+	const bool hooked = fitHook_ && fpr.mode >= kMleGauss;  // the fit runs in the hook's stage, outside this chain
+	if (fpr.mode >= kMleGauss && !hooked) {
+		if (fpr.lanes == 0) { TunedMapping(fpr, SizeClass(B, H, W)); }
 		fpr.mle.queue = ws.cnt->pad;  // this slot's work-queue counters
 	}
-	const bool tune = fpr.mode >= kMleGauss && fpr.lanes == 0;  // first chunk of this (mode, ROI): time both mappings
-	pendMleProf_ = prof && fpr.mode >= kMleGauss;
+	const bool tune = !hooked && fpr.mode >= kMleGauss && fpr.lanes == 0;  // first chunk of this class: time the mappings
+	pendMleProf_ = prof && fpr.mode >= kMleGauss && !hooked;
 	bool ok = true;
 	if (pendMleProf_) {
 		if (!evalDev_) { ok = ok && PTB_CUDA(cudaMalloc(&evalDev_, 3 * sizeof(unsigned long long))); }
@@ -502,6 +511,7 @@ bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, d
 	auto segmentAndDetect = [&]() {
 		bool k = PTB_CUDA(cudaMemsetAsync(ws.cnt, 0, sizeof(Counters), st));
 		k = k && PTB_CUDA(cudaMemsetAsync(ws.rootmask, 0, sizeof(uint32_t) * static_cast<size_t>(B) * H * ws.g.words, st));
+		k = k && PTB_CUDA(cudaMemsetAsync(ws.frameDom, 0, sizeof(uint32_t) * 3 * (static_cast<size_t>(B) + 1), st));
 		mark(0);
 		k = k && LaunchDetect(ws, thr, st);
 		mark(1);
@@ -511,11 +521,13 @@ bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, d
 		return k;
 	};
 	auto fit = [&]() {
+		if (hooked) { return true; }  // after the chain, below
 		return LaunchFit(dImg, H, W, ws.g.N, ws.cand, &ws.cnt->nfit, 0, ws.capRows, fpr, ws.rows, ws.fitFlag, precision_, st);
 	};
 	bool direct = true;
 	if (ok && !prof && !tune && !graphsOff_ && useGraphs_) {
 		std::vector<uint64_t> key = ChainKey(slot, ws, dImg, thr, ratio, strict_, maxPoints, rowsCap, precision_, fpr);
+		key.push_back(hooked ? 1u : 0u);
 		GraphEntry* g = FindGraph(slot, key);
 		if (!g) {
 			auto seen = std::find(seen_[slot].begin(), seen_[slot].end(), key);
@@ -541,6 +553,10 @@ bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, d
 		ok = ok && segmentAndDetect();
 		if (ok && tune) { ok = Autotune(fpr, dImg, H, W, slot, SizeClass(B, H, W)); }
 		ok = ok && fit();
+	}
+	if (ok && hooked) {
+		const FitJob job{st, FitImage{dImg, H, W, ws.g.N}, ws.cand, &ws.cnt->nfit, ws.capRows, ws.rows, fpr};
+		ok = fitHook_(job);
 	}
 	pendLanes_ = fpr.lanes;
 	mark(3);
@@ -581,6 +597,7 @@ long long Engine::CompleteChunk(int slot, uint32_t* truncatedFrames)
 		SetError("internal capacity overflow");
 		return -1;
 	}
+	segCounts_[1] += c.nroute;
 	if (truncatedFrames) { *truncatedFrames += c.truncated; }
 	return c.nfit;
 }
@@ -756,30 +773,54 @@ int EnvLanes()
 	return env ? std::atoi(env) : 0;
 }
 
-int Engine::TunedLanes(const FitParams& fp, int sizeClass) const
+int EnvChunk()
 {
-	if (const int env = EnvLanes()) { return env; }
-	const int key = TuneKey(fp, sizeClass);
-	for (const auto& kv : tuned_) {
-		if (kv.first == key) { return kv.second; }
-	}
-	return 0;  // not tuned yet: the first chunk of this class with candidates tunes it
+	const char* env = std::getenv("PTB_MLE_CHUNK");
+	return env ? std::max(1, std::atoi(env)) : 0;
 }
 
-// Times both ROI mappings (1: thread per ROI, 32: warp per ROI) on this chunk's candidates and keeps the faster for
-// (mode, ROI, chunk size class).
+// The ROI mapping of modes 6-8 for this chunk: PTB_MLE_LANES / PTB_MLE_CHUNK when set, else the autotuned choice of
+// (mode, ROI, chunk size class); lanes stays 0 when that class has not been tuned yet.
+void Engine::TunedMapping(FitParams& fp, int sizeClass) const
+{
+	const int envChunk = EnvChunk();
+	if (const int env = EnvLanes()) {
+		fp.lanes = env;
+		fp.mle.chunk = envChunk ? envChunk : 1;
+		return;
+	}
+	const int key = TuneKey(fp, sizeClass);
+	for (const auto& t : tuned_) {
+		if (t.key == key) {
+			fp.lanes = t.lanes;
+			fp.mle.chunk = envChunk ? envChunk : t.chunk;
+			return;
+		}
+	}
+	fp.lanes = 0;  // not tuned yet: the first chunk of this class with candidates tunes it
+}
+
+// Times the ROI mappings of modes 6-8 on this chunk's candidates - lanes per ROI (1: a thread per ROI through the
+// four-launch pipeline; 2, 4, 8, 16: lane groups in the LM and polish; 32: a warp per ROI, one launch) and the work
+// queue's chunk (candidates a lane takes at a time) - and keeps the fastest for (mode, ROI, chunk size class).
 bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slot, int sizeClass)
 {
 	Workspace& ws = Ws(slot);
 	cudaStream_t st = St(slot);
-	static const int kChoices[] = {1, 32};
+	struct Choice {
+		int lanes, chunk;
+	};
+	static const Choice kChoices[] = {{1, 1}, {1, 4}, {2, 1}, {4, 1}, {8, 1}, {16, 1}, {32, 1}};
 	cudaEvent_t a, b;
 	if (!PTB_CUDA(cudaEventCreate(&a)) || !PTB_CUDA(cudaEventCreate(&b))) { return false; }
 	float best = 1e30f;
-	int bestLanes = 32;
-	for (int lanes : kChoices) {
+	Choice pick{32, 1};
+	const int envChunk = EnvChunk();
+	for (const Choice& c : kChoices) {
+		if (envChunk && c.chunk != 1) { continue; }
 		FitParams t = fp;
-		t.lanes = lanes;
+		t.lanes = c.lanes;
+		t.mle.chunk = envChunk ? envChunk : c.chunk;
 		t.mle.queue = ws.cnt->pad;
 		cudaEventRecord(a, st);
 		if (!LaunchFit(dImg, H, W, ws.g.N, ws.cand, &ws.cnt->nfit, 0, ws.capRows, t, ws.rows, ws.fitFlag, precision_, st)) {
@@ -789,12 +830,13 @@ bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slo
 		if (!PTB_CUDA(cudaEventSynchronize(b))) { return false; }
 		float ms = 0;
 		cudaEventElapsedTime(&ms, a, b);
-		if (ms < best) { best = ms; bestLanes = lanes; }
+		if (ms < best) { best = ms; pick = c; }
 	}
 	cudaEventDestroy(a);
 	cudaEventDestroy(b);
-	fp.lanes = bestLanes;
-	tuned_.push_back({TuneKey(fp, sizeClass), bestLanes});
+	fp.lanes = pick.lanes;
+	fp.mle.chunk = envChunk ? envChunk : pick.chunk;
+	tuned_.push_back({TuneKey(fp, sizeClass), pick.lanes, pick.chunk});
 	return true;
 }
 
@@ -803,6 +845,14 @@ void Engine::GraphStats(uint64_t* out, int n)
 	for (int k = 0; k < 3 && k < n; ++k) {
 		if (out) { out[k] = graphCounts_[k]; }
 		graphCounts_[k] = 0;
+	}
+}
+
+void Engine::SegmentationStats(uint64_t* out, int n)
+{
+	for (int k = 0; k < 2 && k < n; ++k) {
+		if (out) { out[k] = segCounts_[k]; }
+		segCounts_[k] = 0;
 	}
 }
 
@@ -841,6 +891,7 @@ bool Engine::UploadSpline(FitParams& fp, const std::vector<double>& spline)
 		fp.mle.fallbacks = static_cast<unsigned int*>(fallbacks_);
 		fp.mle.queue = static_cast<unsigned int*>(fallbacks_) + 1;
 		fp.lanes = EnvLanes();  // 0: chosen per chunk by the autotuner
+		fp.mle.chunk = EnvChunk() ? EnvChunk() : 1;
 	}
 	if (fp.mode != kMleSpline && fp.mode != kSplineEmccd) { return true; }
 	// the same table as the last upload (a stack fitted chunk by chunk, or call after call): reuse the device copy
@@ -1051,7 +1102,6 @@ double Engine::AutoThreshold(const uint16_t* input, uint64_t height, uint64_t wi
 	return thr;
 }
 
-// One engine per device, guarded by a mutex (calls on one device are serialized).
 // Tracking over host buffers: [n][4] (Id, Plane, X, Y) -> [n][2] (Id, Track) in (Plane, Id) order.
 bool Engine::Track(const double* input, uint64_t* output, uint64_t n, double maxDistance)
 {
@@ -1086,16 +1136,107 @@ bool Engine::AstigEstimate(const double* input, double* output, uint64_t n, doub
 	return PTB_CUDA(cudaStreamSynchronize(stream_)) && ok;
 }
 
-Engine& EngineFor(std::unique_lock<std::mutex>& lock)
+// ---- engine pool --------------------------------------------------------------------------------------------
+// Per device: the engines, which of them are leased, and the settings every engine of the device follows.
+struct Pool {
+	std::mutex mu;
+	std::condition_variable freed;
+	std::vector<std::unique_ptr<Engine>> engines;
+	std::vector<char> busy;
+	int leased = 0;
+	int peak = 0;
+	EngineSettings settings;
+};
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+
+int MaxEngines()
 {
-	static std::mutex mu;
-	static std::vector<std::unique_ptr<Engine>> engines;
+	static const int n = [] {
+		const char* e = std::getenv("PTB_MAX_ENGINES");
+		const int v = e ? std::atoi(e) : 8;
+		return std::max(1, std::min(v, 64));
+	}();
+	return n;
+}
+
+Pool& PoolFor(int dev)
+{
+	static Pool pools[kMaxDevices];
+	return pools[std::max(0, std::min(dev, kMaxDevices - 1))];
+}
+
+int CurrentDevice()
+{
 	int dev = 0;
-	cudaGetDevice(&dev);
-	lock = std::unique_lock<std::mutex>(mu);
-	if (static_cast<int>(engines.size()) <= dev) { engines.resize(dev + 1); }
-	if (!engines[dev]) { engines[dev] = std::make_unique<Engine>(); }
-	return *engines[dev];
+	if (cudaGetDevice(&dev) != cudaSuccess) { dev = 0; }
+	return dev;
+}
+
+}  // namespace
+
+EngineSettings& SettingsFor() { return PoolFor(CurrentDevice()).settings; }
+
+EngineLease::EngineLease()
+{
+	pool_ = &PoolFor(CurrentDevice());
+	std::unique_lock<std::mutex> lock(pool_->mu);
+	for (;;) {
+		for (size_t i = 0; i < pool_->engines.size(); ++i) {
+			if (!pool_->busy[i]) {
+				index_ = static_cast<int>(i);
+				break;
+			}
+		}
+		if (index_ < 0 && static_cast<int>(pool_->engines.size()) < MaxEngines()) {
+			pool_->engines.push_back(std::make_unique<Engine>());
+			pool_->busy.push_back(0);
+			index_ = static_cast<int>(pool_->engines.size()) - 1;
+		}
+		if (index_ >= 0) { break; }
+		pool_->freed.wait(lock);
+	}
+	pool_->busy[index_] = 1;
+	pool_->peak = std::max(pool_->peak, ++pool_->leased);
+	engine_ = pool_->engines[index_].get();
+	engine_->SetStrict(pool_->settings.strict.load());
+	engine_->SetPrecision(pool_->settings.precision.load());
+	engine_->SetProfiling(pool_->settings.profiling.load());
+}
+
+EngineLease::EngineLease(int index)
+{
+	pool_ = &PoolFor(CurrentDevice());
+	std::unique_lock<std::mutex> lock(pool_->mu);
+	if (index < 0 || index >= static_cast<int>(pool_->engines.size())) { return; }
+	pool_->freed.wait(lock, [&] { return !pool_->busy[index]; });
+	index_ = index;
+	pool_->busy[index_] = 1;
+	pool_->peak = std::max(pool_->peak, ++pool_->leased);
+	engine_ = pool_->engines[index_].get();
+}
+
+EngineLease::~EngineLease()
+{
+	if (engine_ == nullptr) { return; }
+	{
+		std::lock_guard<std::mutex> lock(pool_->mu);
+		pool_->busy[index_] = 0;
+		--pool_->leased;
+	}
+	pool_->freed.notify_all();
+}
+
+void PoolStats(uint64_t* out, int n)
+{
+	Pool& p = PoolFor(CurrentDevice());
+	std::lock_guard<std::mutex> lock(p.mu);
+	const uint64_t v[2] = {p.engines.size(), static_cast<uint64_t>(p.peak)};
+	for (int k = 0; k < 2 && k < n; ++k) {
+		if (out) { out[k] = v[k]; }
+	}
 }
 
 }  // namespace ptb

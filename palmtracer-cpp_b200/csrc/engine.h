@@ -1,4 +1,5 @@
-// Host engine of the B200 localization path (one per device; calls on a device are serialized by a mutex).
+// Host engine of the B200 localization path. Each device has a pool of engines: a call leases one for its duration
+// (EngineLease), so concurrent callers run on their own streams and workspaces.
 #pragma once
 
 #include <atomic>
@@ -21,18 +22,36 @@ long long FittingDeviceNoAlloc(const uint16_t* dStack, const double* dPositions,
                                uint64_t height, uint64_t width, uint64_t planes, uint64_t fit, const double* fitParams,
                                int precision, int lanes, cudaStream_t st);
 int EnvLanes();
+int EnvChunk();
 // Serving (server.cpp)
 bool ServerStart(int slots, uint64_t budgetBytes);
 void ServerStop();
 uint64_t SubmitStack(const uint16_t* input, double* output, uint64_t outputSize, uint64_t height, uint64_t width, uint64_t planes,
                      double thr, double ratio, uint64_t fit, const double* fitParams, size_t nParams);
 int PollStack(uint64_t id);
+// [fused fit launches, chunks fitted by them] of the running server (zeros without one).
+void ServerFuseStats(uint64_t* out, int n);
 long long StackResult(uint64_t id, double* times);
 // Number of fit_params entries the given fit mode reads (0 for mode 0 or an unknown mode).
 size_t FitParamCount(uint64_t fit, const double* fp);
 uint64_t LaunchCount();
 bool TrackDevice(const double* dIn, uint64_t* dOut, uint64_t nPoints, double maxDistance, cudaStream_t st);
 double MeasureFmaPeak(int fp64);
+bool SplineCoefficients(const double* volume, uint64_t nx, uint64_t ny, uint64_t nz, const double* lambda, double* out, cudaStream_t st);
+
+// A chunk's maximum-likelihood fit handed to a stage outside the engine (the serving layer's fused fits). The
+// candidates and the frames are ready on `stream`; the stage must fill rows[0, *count) and order that work before
+// whatever `stream` runs next before it returns.
+struct FitJob {
+	cudaStream_t stream;
+	FitImage image;
+	const Cand* cands;
+	const uint32_t* count;  // device
+	uint32_t cap;
+	double* rows;           // [cap][18]
+	FitParams fp;
+};
+using FitHook = std::function<bool(const FitJob&)>;
 
 class Engine {
 public:
@@ -64,6 +83,8 @@ public:
 	void MleEvaluations(uint64_t* out, int n);
 	// [chunks captured into graphs, chunks replayed from graphs, chunks launched directly] since the last call.
 	void GraphStats(uint64_t* out, int n);
+	// [frames segmented, frames flooded again frame-wide after failing the exactness test] since the last call.
+	void SegmentationStats(uint64_t* out, int n);
 	int SetPrecision(int p) { const int o = precision_; precision_ = p; return o; }
 	int Precision() const { return precision_; }
 	cudaStream_t Stream() const { return stream_; }
@@ -74,13 +95,15 @@ public:
 	// Device bytes a Localize call of this shape would hold (chunk workspace and staging), for admission control.
 	size_t EstimateBytes(uint64_t height, uint64_t width, uint64_t planes, uint64_t outputSize) const;
 	void SetStream(cudaStream_t s) { stream_ = s; }
+	// Modes 6-8 fit through `hook` instead of the engine's own launches (empty: the engine fits).
+	void SetFitHook(FitHook hook) { fitHook_ = std::move(hook); }
 	bool Init();
 
 private:
 	bool Reserve(int H, int W, int B, uint32_t rowsCap, int slots);
 	bool ReserveImage(size_t bytes);
 	bool UploadSpline(FitParams& fp, const std::vector<double>& spline);
-	int TunedLanes(const FitParams& fp, int sizeClass) const;
+	void TunedMapping(FitParams& fp, int sizeClass) const;
 	bool Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slot, int sizeClass);
 	int ChunkFrames(int H, int W, uint64_t planes, uint32_t maxPoints, size_t budget) const;
 	// Chunk size and number of concurrent chunk slots (2 when the stack needs more than one chunk).
@@ -117,6 +140,7 @@ private:
 	std::vector<std::vector<uint64_t>> seen_[2];  // chains launched once directly (the next occurrence is captured)
 	uint64_t graphClock_ = 0;
 	uint64_t graphCounts_[3] = {};            // captured, replayed, direct
+	uint64_t segCounts_[2] = {};              // frames segmented, frames flooded again frame-wide
 	bool useGraphs_ = true;                   // PTB_GRAPHS=0 launches every chunk directly
 	bool graphsOff_ = false;                  // a capture failed: direct launches from then on
 	Workspace ws1_{};                        // second chunk slot's workspace and pool
@@ -139,9 +163,15 @@ private:
 	std::vector<double> splineCache_;         // the table behind spline_ (its upload is skipped when unchanged)
 	int splineCacheMode_ = -1;
 	void* fallbacks_ = nullptr;
-	std::vector<std::pair<int, int>> tuned_;  // ((mode * 64 + roi) * 64 + chunk size class) -> lanes per ROI
+	struct Tuned {
+		int key;    // (mode * 64 + roi) * 64 + chunk size class
+		int lanes;  // lanes per ROI
+		int chunk;  // work-queue chunk
+	};
+	std::vector<Tuned> tuned_;
 	size_t splineBytes_ = 0;
 	Workspace ws_{};
+	FitHook fitHook_;
 	int strict_ = 0;
 	int precision_ = 0;
 	int profiling_ = 0;
@@ -160,6 +190,39 @@ private:
 	int pendLanes_ = 0;
 };
 
-Engine& EngineFor(std::unique_lock<std::mutex>& lock);
+// Settings that PTB_SetSegmentationMode / PTB_SetFitPrecision / PTB_SetProfiling change for every engine of a device
+// (applied to an engine each time it is leased).
+struct EngineSettings {
+	std::atomic<int> strict{0};
+	std::atomic<int> precision{0};
+	std::atomic<int> profiling{0};
+};
+EngineSettings& SettingsFor();  // the current device's
+
+// One engine of the current device's pool, held for one call. A lease takes the first idle engine, creates a new one
+// when every engine is busy and the pool holds fewer than PTB_MAX_ENGINES (default 8), and otherwise waits for one to
+// be released; so concurrent callers get their own engines (own CUDA streams, chunk workspaces, graphs and autotuned
+// choices) and overlap on the device, and sequential callers keep reusing the first engine. Lease(index) takes that
+// specific engine (waiting while it is busy), for diagnostics that visit every engine; it is empty when the pool has
+// no such engine.
+class EngineLease {
+public:
+	EngineLease();
+	explicit EngineLease(int index);
+	~EngineLease();
+	EngineLease(const EngineLease&) = delete;
+	EngineLease& operator=(const EngineLease&) = delete;
+	Engine& operator*() const { return *engine_; }
+	Engine* operator->() const { return engine_; }
+	explicit operator bool() const { return engine_ != nullptr; }
+
+private:
+	struct Pool* pool_ = nullptr;
+	int index_ = -1;
+	Engine* engine_ = nullptr;
+};
+
+// [engines in the current device's pool, most engines leased at the same time] (diagnostics).
+void PoolStats(uint64_t* out, int n);
 
 }  // namespace ptb

@@ -21,7 +21,7 @@ __global__ void BuildCandidates(Workspace ws)
 		c.intensity = sv * kW1Unit;
 		c.surf = static_cast<double>(ws.regCount[r]);
 		c.frame = static_cast<int>(ws.candFrame[k]);
-		c.pad = 0;
+		c.image = 0;
 		ws.cand[k] = c;
 	}
 }

@@ -552,7 +552,7 @@ bool LaunchGaussT(const uint16_t* img, int H, int W, long long N, const Cand* ca
 
 bool LaunchSpline(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
                   uint32_t cap, const FitParams& fp, double* rows, cudaStream_t st);
-bool LaunchMle(int lanes, const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
+bool LaunchMle(int lanes, const FitImages& fi, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
                uint32_t cap, const MleParams& mp, double* rows, cudaEvent_t* marks, cudaStream_t st);
 bool LaunchExactFit(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
                     uint32_t cap, const FitParams& fp, double* rows, const uint8_t* only, cudaStream_t st);
@@ -564,7 +564,9 @@ bool LaunchFit(const uint16_t* img, int H, int W, long long N, const Cand* cands
                uint32_t cap, const FitParams& fp, double* rows, uint8_t* flags, int precision, cudaStream_t st)
 {
 	if (fp.mode == kSplineEmccd) { return LaunchSpline(img, H, W, N, cands, nptr, nconst, cap, fp, rows, st); }
-	if (fp.mode >= kMleGauss && fp.mode <= kMleSpline) { return LaunchMle(fp.lanes, img, H, W, N, cands, nptr, nconst, cap, fp.mle, rows, fp.marks, st); }
+	if (fp.mode >= kMleGauss && fp.mode <= kMleSpline) {
+		return LaunchMle(fp.lanes, OneImage(img, H, W, N), cands, nptr, nconst, cap, fp.mle, rows, fp.marks, st);
+	}
 	if (fp.mode < kG2Fixed || fp.mode > kG3Theta) {
 		const uint32_t blocks = std::min<uint32_t>((cap + 255) / 256 + 1, 148u * 8u);
 		NoFitKernel<<<blocks, 256, 0, st>>>(cands, nptr, nconst, rows);

@@ -48,7 +48,8 @@ constexpr int kStatusCol = 5;
 constexpr double kStOk = 0.0, kStFailed = 1.0, kStBorder = 2.0;
 
 // What one evaluation accumulates: deviance only; deviance, gradient and Fisher-scoring matrix; deviance, gradient,
-// exact Hessian and Fisher information; deviance and Fisher information.
+// exact Hessian and Fisher information; deviance and Fisher information (the FP64 final pass: the log-likelihood and
+// CRLB of the result).
 enum Kind { kDevOnly = 0, kFisher = 1, kExact = 2, kFinal = 3 };
 
 template <int KIND> struct Fields { static constexpr int value = KIND == kDevOnly ? 1 : (KIND == kExact ? 6 : 3); };
@@ -61,17 +62,28 @@ template <> __device__ __forceinline__ float Ex<float>(float x) { return __expf(
 template <> __device__ __forceinline__ double Ex<double>(double x) { return exp(x); }
 template <typename T> __device__ __forceinline__ T Ln(T x);
 template <> __device__ __forceinline__ float Ln<float>(float x) { return __logf(x); }  // hardware lg2 based
+template <> __device__ __forceinline__ double Ln<double>(double x) { return log(x); }
 
 // Division in the per-pixel sums: FP32 with the hardware approximation (divisors here are photon counts and model
 // values, far inside its range), FP64 exact.
 template <typename T> __device__ __forceinline__ T Div(T a, T b) { return a / b; }
 template <> __device__ __forceinline__ float Div<float>(float a, float b) { return __fdividef(a, b); }
 
-template <typename T>
-__device__ __forceinline__ T WarpSum(T v)
+// Lanes of the calling lane's group of L consecutive lanes (L a power of two, the groups of a warp disjoint).
+template <int L>
+__device__ __forceinline__ unsigned GroupMask()
+{
+	if constexpr (L >= 32) { return 0xffffffffu; }
+	else { return ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1)); }
+}
+
+// Sum over the calling lane's group of L lanes; every lane of the group receives the same value (each butterfly step
+// adds the same two partial sums on both partners, and addition is commutative).
+template <int L, typename T>
+__device__ __forceinline__ T GroupSum(T v)
 {
 	#pragma unroll
-	for (int d = 16; d > 0; d >>= 1) { v += __shfl_xor_sync(0xffffffffu, v, d); }
+	for (int d = L / 2; d > 0; d >>= 1) { v += __shfl_xor_sync(GroupMask<L>(), v, d); }
 	return v;
 }
 
@@ -266,8 +278,7 @@ template <typename T, int KIND>
 __device__ __forceinline__ void Accumulate(T d, T bg, T I, T psf, const T P1[3], const T P2[6], T& D, T G[5], T Hm[15], T Fm[15])
 {
 	const T mu = max(bg + I * psf, T(1e-6));
-	// the final pass needs only the Fisher information (the CRLB); its deviance would be discarded
-	if constexpr (KIND != kFinal) { D += d > T(0) ? T(2) * (mu - d - d * Ln<T>(Div<T>(mu, d))) : T(2) * mu; }
+	D += d > T(0) ? T(2) * (mu - d - d * Ln<T>(Div<T>(mu, d))) : T(2) * mu;
 	if constexpr (KIND != kDevOnly) {
 		const T gk[5] = {T(1), psf, I * P1[0], I * P1[1], I * P1[2]};
 		const T rmu = Div<T>(T(1), mu);
@@ -329,15 +340,16 @@ __device__ __forceinline__ T Photons(const Pix& px, int i, int j, int k)
 }
 
 // Deviance D at theta and, by KIND, the gradient G, the curvature Hm and the Fisher information Fm (upper
-// triangles, 15 entries). L = 1: the calling thread sums the whole ROI, the column factors go to its table xt. L = 32:
-// the warp shares the pixels, the column and row factors go to the warp's tables xt and yt, the sums are reduced
-// over the warp and every lane returns them.
+// triangles, 15 entries). L = 1: the calling thread sums the whole ROI, the column factors go to its table xt. L > 1:
+// a group of L consecutive lanes (the warp for L = 32) shares the pixels, the column and row factors go to the group's
+// tables xt and yt, the sums are reduced over the group and every lane of it returns them. All lanes of a group call
+// it together.
 template <typename T, int MODEL, int L, int KIND>
 __device__ T Normal(const MleParams& mp, const Pix& px, const T th[5], T G[5], T Hm[15], T Fm[15], FacTab<T> xt, FacTab<T> yt)
 {
 	constexpr int NF = Fields<KIND>::value;
 	const int roi = mp.roi, h = mp.half, n = mp.n;
-	const int gl = L == 1 ? 0 : (threadIdx.x & 31);
+	const int gl = L == 1 ? 0 : static_cast<int>(threadIdx.x & (L - 1));
 	T sx = th[4], sy = th[4], dsx = T(1), dsy = T(1), ssx = T(0), ssy = T(0);
 	if constexpr (MODEL == 7) {
 		AstigSigma<T>(mp.astig, mp.pixelSize, th[4], sx, dsx, ssx);
@@ -389,6 +401,30 @@ __device__ T Normal(const MleParams& mp, const Pix& px, const T th[5], T G[5], T
 			}
 		}
 	}
+	else if constexpr (L < 32) {
+		// factor c of the columns (q = c) or the rows (q = roi + c) by lane q mod L, from its two boundaries
+		const AxisConst<T> cx(sx), cy(sy);
+		for (int q = gl; q < 2 * roi; q += L) {
+			const bool isY = q >= roi;
+			const int c = isY ? q - roi : q;
+			const AxisConst<T>& ac = isY ? cy : cx;
+			const T pos = isY ? th[3] : th[2];
+			const Bound<T> a = MakeBound<T, NF>(c, h, pos, ac.k), b = MakeBound<T, NF>(c + 1, h, pos, ac.k);
+			(isY ? yt : xt).template Put<NF>(c, FacOf<T, NF>(a, b, ac));
+		}
+		__syncwarp(GroupMask<L>());
+		int i = gl / roi, j = gl - i * roi;
+		const int di = L / roi, dj = L - di * roi;
+		for (int k = gl; k < n; k += L) {
+			const T d = Photons<T>(px, i, j, k);
+			const T psf = GaussPixel<T, NF>(xt.template Get<NF>(j), yt.template Get<NF>(i), dsx, dsy, ssx, ssy, P1, P2);
+			Accumulate<T, KIND>(d, th[0], th[1], psf, P1, P2, D, G, Hm, Fm);
+			i += di;
+			j += dj;
+			if (j >= roi) { j -= roi; ++i; }
+		}
+		__syncwarp(GroupMask<L>());  // the tables are rewritten by the next evaluation
+	}
 	else {
 		// lanes 0..roi hold the x boundaries, lanes 16..16+roi the y boundaries; pixel factors from lane pairs
 		const AxisConst<T> cx(sx), cy(sy);
@@ -420,16 +456,16 @@ __device__ T Normal(const MleParams& mp, const Pix& px, const T th[5], T G[5], T
 		__syncwarp();  // the tables are rewritten by the next evaluation
 	}
 	if constexpr (L > 1) {
-		D = WarpSum(D);
+		D = GroupSum<L>(D);
 		if constexpr (KIND == kFisher || KIND == kExact) {
 			#pragma unroll
-			for (int a = 0; a < 5; ++a) { G[a] = WarpSum(G[a]); }
+			for (int a = 0; a < 5; ++a) { G[a] = GroupSum<L>(G[a]); }
 			#pragma unroll
-			for (int a = 0; a < 15; ++a) { Hm[a] = WarpSum(Hm[a]); }
+			for (int a = 0; a < 15; ++a) { Hm[a] = GroupSum<L>(Hm[a]); }
 		}
 		if constexpr (KIND == kFinal) {
 			#pragma unroll
-			for (int a = 0; a < 15; ++a) { Fm[a] = WarpSum(Fm[a]); }
+			for (int a = 0; a < 15; ++a) { Fm[a] = GroupSum<L>(Fm[a]); }
 		}
 	}
 	return D;
@@ -642,10 +678,14 @@ struct RoiAt {
 	unsigned long long ux, uy;
 	double x0, y0;
 	const uint16_t* base;
+	int W;  // row pitch of the ROI's frame
 };
 
-__device__ __forceinline__ bool Locate(const uint16_t* img, int H, int W, long long N, const MleParams& mp, const Cand& cd, RoiAt& r)
+__device__ __forceinline__ bool Locate(const FitImages& fi, const MleParams& mp, const Cand& cd, RoiAt& r)
 {
+	const FitImage& f = fi.im[cd.image];
+	const int H = f.H, W = f.W;
+	r.W = W;
 	const bool nonneg = cd.x >= 0.0 && cd.y >= 0.0;
 	r.ux = nonneg ? static_cast<unsigned long long>(cd.x) : 0ull;
 	r.uy = nonneg ? static_cast<unsigned long long>(cd.y) : 0ull;
@@ -655,7 +695,7 @@ __device__ __forceinline__ bool Locate(const uint16_t* img, int H, int W, long l
 	}
 	r.x0 = cd.x - static_cast<double>(r.ux);
 	r.y0 = cd.y - static_cast<double>(r.uy);
-	r.base = img + static_cast<long long>(cd.frame) * N + static_cast<long long>(r.uy - hh) * W + static_cast<long long>(r.ux - hh);
+	r.base = f.img + static_cast<long long>(cd.frame) * f.N + static_cast<long long>(r.uy - hh) * W + static_cast<long long>(r.ux - hh);
 	return true;
 }
 
@@ -782,13 +822,15 @@ __device__ int Polish(const MleParams& mp, const Pix& px, float x0, float y0, fl
 	return evals;
 }
 
-// FP64 Fisher information at t; CRLB = sqrt(diag(F^-1)). False when it cannot be inverted or t is not finite (the
-// oracle's final step, which computes no deviance either).
+// FP64 final pass at t: the Poisson deviance D (the log-likelihood ratio against the saturated model, -2 log(L/L_sat),
+// the fit's goodness of fit) and the Fisher information; CRLB = sqrt(diag(F^-1)). False when F cannot be inverted or t
+// is not finite (the oracle's final step).
 template <int MODEL, int L>
-__device__ bool Final(const MleParams& mp, const Pix& px, const double t[5], double crlb[5], FacTab<double> xt, FacTab<double> yt)
+__device__ bool Final(const MleParams& mp, const Pix& px, const double t[5], double crlb[5], double& dev, FacTab<double> xt,
+                      FacTab<double> yt)
 {
 	double Fm[15], cv[5];
-	Normal<double, MODEL, L, kFinal>(mp, px, t, nullptr, nullptr, Fm, xt, yt);  // a non-finite entry fails the Cholesky
+	dev = Normal<double, MODEL, L, kFinal>(mp, px, t, nullptr, nullptr, Fm, xt, yt);  // a non-finite entry fails the Cholesky
 	if (!InverseDiag5<double>(Fm, cv)) { return false; }
 	#pragma unroll
 	for (int a = 0; a < 5; ++a) { crlb[a] = cv[a] > 0 ? sqrt(cv[a]) : 0.0; }
@@ -799,9 +841,10 @@ __device__ bool Final(const MleParams& mp, const Pix& px, const double t[5], dou
 	return true;
 }
 
-// Output row; col < 0: the calling thread writes all 18 columns, else only column col.
+// Output row; col < 0: the calling thread writes all 18 columns, else only column col. The Theta column (the models
+// have no rotation) holds the FP64 deviance of the fit, -1 for a failed one.
 __device__ void StoreMleRow(double* row, int col, const MleParams& mp, const Cand& cd, const double t[5], const double crlb[5],
-                            unsigned long long ux, unsigned long long uy, bool ok)
+                            double dev, unsigned long long ux, unsigned long long uy, bool ok)
 {
 	double v[kCols];
 	v[cId] = 0; v[cPlane] = 0; v[cIndex] = 0; v[cChannel] = -1;
@@ -825,7 +868,7 @@ __device__ void StoreMleRow(double* row, int col, const MleParams& mp, const Can
 		v[cY] = static_cast<double>(uy) + t[3];
 		v[cZ] = z;
 		v[cIntensity] = t[1];
-		v[cSigmaX] = sx; v[cSigmaY] = sy; v[cTheta] = 0;
+		v[cSigmaX] = sx; v[cSigmaY] = sy; v[cTheta] = dev;
 		v[cQualityXY] = qxy; v[cQualityZ] = qz;
 		v[cAmplitude] = (sx > 0 && sy > 0) ? t[1] / (6.283185307179586 * sx * sy) : t[1];
 		v[cOffset] = t[0];
@@ -851,7 +894,7 @@ __device__ __forceinline__ uint32_t CandCount(const uint32_t* nptr, uint32_t nco
 
 // Initial values; shared memory: per thread the FP32 column factors of the axial pre-scan (roi floats).
 template <int MODEL>
-__global__ void __launch_bounds__(kThreads) MleInitKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
+__global__ void __launch_bounds__(kThreads) MleInitKernel(FitImages fi,
                                                           const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
                                                           MleParams mp, double* rows)
 {
@@ -862,11 +905,11 @@ __global__ void __launch_bounds__(kThreads) MleInitKernel(const uint16_t* __rest
 	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
 		double* row = rows + static_cast<long long>(k) * kCols;
 		RoiAt r;
-		if (!Locate(img, H, W, N, mp, cands[k], r)) {
+		if (!Locate(fi, mp, cands[k], r)) {
 			row[kStatusCol] = kStBorder;
 			continue;
 		}
-		const Pix px = MakePix(mp, r.base, W, nullptr, 0);
+		const Pix px = MakePix(mp, r.base, r.W, nullptr, 0);
 		double t[5];
 		evals += InitTheta<MODEL, 1>(mp, px, r, t, xt, xt);
 		#pragma unroll
@@ -880,13 +923,18 @@ constexpr uint32_t kNone = 0xffffffffu;
 
 // Work queue of the persistent kernels. With a counter (zeroed before the launch) it is global: lanes that need work
 // take the next candidates with one atomic per warp, so warps that finish early keep taking work until all
-// candidates are out. Without one, warp w owns the static range [w * chunk, (w + 1) * chunk), chunk >= 32.
+// candidates are out; each taking lane receives `chunk` consecutive candidates (neighbouring ROIs of one frame) and
+// starts the next of them without an atomic. Without a counter, warp w owns the static range
+// [w * c, (w + 1) * c), c >= 32.
 struct WarpQueue {
-	uint32_t cursor, end;
+	uint32_t cursor, end, chunk;
+	uint32_t next, last;  // this lane's taken candidates not started yet: [next, last)
 	unsigned int* counter;
-	__device__ __forceinline__ bool Init(uint32_t n, unsigned int* ctr)
+	__device__ __forceinline__ bool Init(uint32_t n, unsigned int* ctr, int chunkSize)
 	{
 		counter = ctr;
+		chunk = static_cast<uint32_t>(max(chunkSize, 1));
+		next = last = 0;
 		if (counter) {
 			cursor = 0;
 			end = n;
@@ -894,44 +942,74 @@ struct WarpQueue {
 		}
 		const uint32_t warps = gridDim.x * (blockDim.x / 32);
 		const uint32_t gw = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-		const uint32_t chunk = max(32u, (n + warps - 1) / warps);
-		const unsigned long long begin = static_cast<unsigned long long>(gw) * chunk;
+		const uint32_t c = max(32u, (n + warps - 1) / warps);
+		const unsigned long long begin = static_cast<unsigned long long>(gw) * c;
 		cursor = static_cast<uint32_t>(min(begin, static_cast<unsigned long long>(n)));
-		end = static_cast<uint32_t>(min(begin + chunk, static_cast<unsigned long long>(n)));
+		end = static_cast<uint32_t>(min(begin + c, static_cast<unsigned long long>(n)));
 		return cursor < end;
 	}
 	// Called by all 32 lanes; returns the candidate taken by a lane with `need` set (kNone when the queue is done).
 	__device__ __forceinline__ uint32_t Take(bool need)
 	{
-		const unsigned mask = __ballot_sync(0xffffffffu, need);
 		const int lane = threadIdx.x & 31;
 		if (counter) {
-			if (mask == 0 || cursor >= end) { return kNone; }
-			const int leader = __ffs(mask) - 1;
-			uint32_t base = 0;
-			if (lane == leader) { base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask))); }
-			base = __shfl_sync(0xffffffffu, base, leader);
-			if (base + static_cast<uint32_t>(__popc(mask)) >= end) { cursor = end; }  // the queue ran out: stop taking
-			const uint32_t k = base + __popc(mask & ((1u << lane) - 1u));
-			return need && k < end ? k : kNone;
+			const bool fetch = need && next >= last;
+			const unsigned mask = __ballot_sync(0xffffffffu, fetch);
+			if (mask != 0 && cursor < end) {
+				const int leader = __ffs(mask) - 1;
+				const uint32_t want = static_cast<uint32_t>(__popc(mask)) * chunk;
+				uint32_t base = 0;
+				if (lane == leader) { base = atomicAdd(counter, want); }
+				base = __shfl_sync(0xffffffffu, base, leader);
+				if (base + want >= end) { cursor = end; }  // the queue ran out: stop taking
+				if (fetch) {
+					next = min(base + __popc(mask & ((1u << lane) - 1u)) * chunk, end);
+					last = min(next + chunk, end);
+				}
+			}
+			return need && next < last ? next++ : kNone;
 		}
+		const unsigned mask = __ballot_sync(0xffffffffu, need);
 		const uint32_t k = cursor + __popc(mask & ((1u << lane) - 1u));
 		cursor = min(end, cursor + static_cast<uint32_t>(__popc(mask)));
 		return need && k < end ? k : kNone;
 	}
-	__device__ __forceinline__ bool Done() const { return cursor >= end; }
+	// Called by all 32 lanes: nothing left to take, neither in the queue nor in any lane's chunk.
+	__device__ __forceinline__ bool Done() const { return cursor >= end && __ballot_sync(0xffffffffu, next < last) == 0; }
 };
 
-// Stages the ROI of candidate k for the calling lane: FP32 photons at ph[q * T], theta from the row, position.
-__device__ __forceinline__ void LoadRoi(const uint16_t* img, int H, int W, long long N, const MleParams& mp, const Cand* cands,
-                                        const double* rows, uint32_t k, float* ph, int T, Pix& px, float th[5], float& x0, float& y0)
+// The calling lane's share of a group of L lanes that handles one ROI: its index in the group, the group's first lane
+// and whether it is that lane (which takes the queue's candidates, counts and writes the rows).
+template <int L>
+struct Group {
+	int gl, first;
+	bool leader;
+	__device__ __forceinline__ Group()
+	{
+		const int lane = threadIdx.x & 31;
+		gl = lane & (L - 1);
+		first = lane - gl;
+		leader = gl == 0;
+	}
+};
+
+// Stages the ROI of candidate k: FP32 photons at ph[q * T] (the L lanes of a group share the pixels), theta from the
+// row, position.
+template <int L>
+__device__ __forceinline__ void LoadRoi(const FitImages& fi, const MleParams& mp, const Cand* cands, const double* rows, uint32_t k,
+                                        float* ph, int T, Pix& px, float th[5], float& x0, float& y0)
 {
 	RoiAt r;
-	Locate(img, H, W, N, mp, cands[k], r);
+	Locate(fi, mp, cands[k], r);
+	const int W = r.W;
 	px.g = r.base;
-	for (int i = 0, q = 0; i < mp.roi; ++i) {
-		for (int j = 0; j < mp.roi; ++j, ++q) { ph[q * T] = fmaxf((float(__ldg(r.base + i * W + j)) - px.off32) * px.inv32, 0.f); }
+	px.W = W;
+	const int gl = L == 1 ? 0 : static_cast<int>(threadIdx.x & (L - 1));
+	for (int q = gl; q < mp.n; q += L) {
+		const int i = q / mp.roi, j = q - i * mp.roi;
+		ph[q * T] = fmaxf((float(__ldg(r.base + i * W + j)) - px.off32) * px.inv32, 0.f);
 	}
+	if constexpr (L > 1) { __syncwarp(GroupMask<L>()); }
 	const double* row = rows + static_cast<long long>(k) * kCols;
 	#pragma unroll
 	for (int a = 0; a < 5; ++a) { th[a] = static_cast<float>(row[a]); }
@@ -939,30 +1017,61 @@ __device__ __forceinline__ void LoadRoi(const uint16_t* img, int H, int W, long 
 	y0 = static_cast<float>(r.y0);
 }
 
-// Persistent FP32 LM (WarpQueue). Every pass of the loop makes each busy lane evaluate the deviance, gradient and
-// Fisher matrix once: at the start point of a new candidate, or at the trial point of an LM step. Shared memory per
-// lane, lane-interleaved: the ROI photons (n floats) and the column factors (3 roi floats).
-template <int MODEL>
-__global__ void __launch_bounds__(kThreads) MleLmKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
+// Shared memory of the persistent kernels per ROI slot, in floats: the photons and the column (and, for L > 1, row)
+// factor tables with NF fields. L = 1: lane-interleaved slots (stride = block size); L > 1: one contiguous slot per
+// group.
+__host__ __device__ __forceinline__ int SlotFloats(int n, int roi, int nf, int L) { return n + (L == 1 ? 1 : 2) * nf * roi; }
+
+template <int L>
+struct SlotView {
+	float* ph;
+	int stride;
+	FacTab<float> xt, yt;
+	__device__ __forceinline__ SlotView(unsigned char* smem, const MleParams& mp, int nf)
+	{
+		float* base = reinterpret_cast<float*>(smem);
+		if constexpr (L == 1) {
+			const int T = blockDim.x;
+			ph = base + threadIdx.x;
+			stride = T;
+			xt = FacTab<float>{base + mp.n * T + threadIdx.x, T};
+			yt = xt;
+		}
+		else {
+			float* slot = base + (threadIdx.x / L) * SlotFloats(mp.n, mp.roi, nf, L);
+			ph = slot;
+			stride = 1;
+			xt = FacTab<float>{slot + mp.n, 1};
+			yt = FacTab<float>{slot + mp.n + nf * mp.roi, 1};
+		}
+	}
+};
+
+// Persistent FP32 LM (WarpQueue). Every pass of the loop makes each busy ROI evaluate the deviance, gradient and
+// Fisher matrix once: at the start point of a new candidate, or at the trial point of an LM step. L lanes per ROI
+// (1: a thread per ROI); the lanes of a group hold the same state and take the same branches. Shared memory per ROI
+// slot: the photons and the factor tables (SlotFloats, NF = 3).
+template <int MODEL, int L>
+__global__ void __launch_bounds__(kThreads) MleLmKernel(FitImages fi,
                                                         const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
                                                         MleParams mp, double* rows)
 {
 	extern __shared__ __align__(16) unsigned char smem[];
-	const int T = blockDim.x;
-	float* ph = reinterpret_cast<float*>(smem) + threadIdx.x;
-	const FacTab<float> xt{reinterpret_cast<float*>(smem) + mp.n * T + threadIdx.x, T};
+	const SlotView<L> sv(smem, mp, 3);
+	const Group<L> grp;
 	WarpQueue q;
-	if (!q.Init(CandCount(nptr, nconst), mp.queue)) { return; }
+	if (!q.Init(CandCount(nptr, nconst), mp.queue, mp.chunk)) { return; }
 	uint32_t k = kNone;
 	bool fresh = false;
 	float th[5] = {0, 0, 0, 0, 0}, G[5], Hm[15], D = 0.f, lambda = 1e-3f, x0 = 0.f, y0 = 0.f;
 	int it = 0;
 	unsigned long long evals = 0;
-	Pix px = MakePix(mp, img, W, ph, T);
+	Pix px = MakePix(mp, nullptr, 0, sv.ph, sv.stride);
 	while (true) {
-		const uint32_t kk = q.Take(k == kNone);
+		uint32_t kk = q.Take(grp.leader && k == kNone);
+		if constexpr (L > 1) { kk = __shfl_sync(0xffffffffu, kk, grp.first); }
 		if (kk != kNone && rows[static_cast<long long>(kk) * kCols + kStatusCol] == kStOk) {
-			LoadRoi(img, H, W, N, mp, cands, rows, kk, ph, T, px, th, x0, y0);
+			LoadRoi<L>(fi, mp, cands, rows, kk, sv.ph, sv.stride, px, th, x0, y0);
 			k = kk;
 			fresh = true;
 		}
@@ -984,7 +1093,7 @@ __global__ void __launch_bounds__(kThreads) MleLmKernel(const uint16_t* __restri
 				#pragma unroll
 				for (int a = 0; a < 5; ++a) { rhs[a] = -G[a]; }
 				FixActive32<MODEL>(mp, x0, y0, th, G, Hm, rhs);  // in place: Hm is replaced when a step is accepted
-				if (Solve32(Hm, 1.f + lambda, rhs, dt, mp.fallbacks, true)) {
+				if (Solve32(Hm, 1.f + lambda, rhs, dt, mp.fallbacks, grp.leader)) {
 					#pragma unroll
 					for (int a = 0; a < 5; ++a) { tt[a] = th[a] + dt[a]; }
 					Clamp32<MODEL>(mp, x0, y0, tt);
@@ -999,8 +1108,8 @@ __global__ void __launch_bounds__(kThreads) MleLmKernel(const uint16_t* __restri
 		}
 		float Gt[5], Ht[15], Dt = 0.f;
 		if (eval) {
-			Dt = Normal<float, MODEL, 1, kFisher>(mp, px, tt, Gt, Ht, nullptr, xt, xt);
-			++evals;
+			Dt = Normal<float, MODEL, L, kFisher>(mp, px, tt, Gt, Ht, nullptr, sv.xt, sv.yt);
+			evals += grp.leader ? 1 : 0;
 			if (fresh) {
 				fresh = false;
 				D = Dt;
@@ -1033,41 +1142,43 @@ __global__ void __launch_bounds__(kThreads) MleLmKernel(const uint16_t* __restri
 			}
 		}
 		if (finish) {
-			double* row = rows + static_cast<long long>(k) * kCols;
-			#pragma unroll
-			for (int a = 0; a < 5; ++a) { row[a] = th[a]; }
-			row[kStatusCol] = failed ? kStFailed : kStOk;
+			if (grp.leader) {
+				double* row = rows + static_cast<long long>(k) * kCols;
+				#pragma unroll
+				for (int a = 0; a < 5; ++a) { row[a] = th[a]; }
+				row[kStatusCol] = failed ? kStFailed : kStOk;
+			}
 			k = kNone;
 		}
 	}
 	if (mp.evals && evals) { atomicAdd(mp.evals, evals); }
 }
 
-// Persistent FP32 Newton polish (WarpQueue), the steps of Polish() as a per-lane state machine: each pass evaluates
-// the deviance, gradient and exact Hessian once per busy lane - at the LM result of a new
-// candidate or at a trial point - and then accepts, halves or ends. Shared memory per lane: the ROI photons (n
-// floats) and the column factors with second derivatives (6 roi floats).
-template <int MODEL>
-__global__ void __launch_bounds__(kThreads) MlePolishKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
+// Persistent FP32 Newton polish (WarpQueue), the steps of Polish() as a per-ROI state machine: each pass evaluates
+// the deviance, gradient and exact Hessian once per busy ROI - at the LM result of a new candidate or at a trial
+// point - and then accepts, halves or ends. L lanes per ROI as in the LM. Shared memory per ROI slot: the photons and
+// the factor tables with second derivatives (SlotFloats, NF = 6).
+template <int MODEL, int L>
+__global__ void __launch_bounds__(kThreads) MlePolishKernel(FitImages fi,
                                                             const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
                                                             MleParams mp, double* rows)
 {
 	extern __shared__ __align__(16) unsigned char smem[];
-	const int T = blockDim.x;
-	float* ph = reinterpret_cast<float*>(smem) + threadIdx.x;
-	const FacTab<float> xt{reinterpret_cast<float*>(smem) + mp.n * T + threadIdx.x, T};
+	const SlotView<L> sv(smem, mp, 6);
+	const Group<L> grp;
 	WarpQueue q;
-	if (!q.Init(CandCount(nptr, nconst), mp.queue ? mp.queue + 1 : nullptr)) { return; }
+	if (!q.Init(CandCount(nptr, nconst), mp.queue ? mp.queue + 1 : nullptr, mp.chunk)) { return; }
 	uint32_t k = kNone;
 	bool fresh = false;
 	float th[5] = {0, 0, 0, 0, 0}, dt[5] = {0, 0, 0, 0, 0}, G[5], Hm[15], D = 0.f, x0 = 0.f, y0 = 0.f;
 	int it = 0, hv = 0;
 	unsigned long long evals = 0;
-	Pix px = MakePix(mp, img, W, ph, T);
+	Pix px = MakePix(mp, nullptr, 0, sv.ph, sv.stride);
 	while (true) {
-		const uint32_t kk = q.Take(k == kNone);
+		uint32_t kk = q.Take(grp.leader && k == kNone);
+		if constexpr (L > 1) { kk = __shfl_sync(0xffffffffu, kk, grp.first); }
 		if (kk != kNone && rows[static_cast<long long>(kk) * kCols + kStatusCol] == kStOk) {
-			LoadRoi(img, H, W, N, mp, cands, rows, kk, ph, T, px, th, x0, y0);
+			LoadRoi<L>(fi, mp, cands, rows, kk, sv.ph, sv.stride, px, th, x0, y0);
 			k = kk;
 			fresh = true;
 		}
@@ -1082,8 +1193,8 @@ __global__ void __launch_bounds__(kThreads) MlePolishKernel(const uint16_t* __re
 			#pragma unroll
 			for (int a = 0; a < 5; ++a) { tt[a] = fresh ? th[a] : th[a] + dt[a]; }
 			if (!fresh) { Clamp32<MODEL>(mp, x0, y0, tt); }
-			Dt = Normal<float, MODEL, 1, kExact>(mp, px, tt, Gt, Ht, nullptr, xt, xt);
-			++evals;
+			Dt = Normal<float, MODEL, L, kExact>(mp, px, tt, Gt, Ht, nullptr, sv.xt, sv.yt);
+			evals += grp.leader ? 1 : 0;
 			bool moved = false;
 			if (fresh) {
 				fresh = false;
@@ -1114,17 +1225,19 @@ __global__ void __launch_bounds__(kThreads) MlePolishKernel(const uint16_t* __re
 				if (!finish) {
 					auto fisher = [&](float Hf[15]) {
 						float Gf[5];
-						Normal<float, MODEL, 1, kFisher>(mp, px, th, Gf, Hf, nullptr, xt, xt);
-						++evals;
+						Normal<float, MODEL, L, kFisher>(mp, px, th, Gf, Hf, nullptr, sv.xt, sv.yt);
+						evals += grp.leader ? 1 : 0;
 					};
 					finish = !NewtonDirection<MODEL>(mp, x0, y0, th, G, Hm, dt, fisher) || ApplyIfTiny<MODEL>(mp, x0, y0, th, dt);
 				}
 			}
 		}
 		if (finish) {
-			double* row = rows + static_cast<long long>(k) * kCols;
-			#pragma unroll
-			for (int a = 0; a < 5; ++a) { row[a] = th[a]; }
+			if (grp.leader) {
+				double* row = rows + static_cast<long long>(k) * kCols;
+				#pragma unroll
+				for (int a = 0; a < 5; ++a) { row[a] = th[a]; }
+			}
 			k = kNone;
 		}
 	}
@@ -1134,7 +1247,7 @@ __global__ void __launch_bounds__(kThreads) MlePolishKernel(const uint16_t* __re
 // FP64 deviance, Fisher information and CRLB at the polished theta; writes the output row. Shared memory per thread:
 // the FP64 column factors (3 roi doubles).
 template <int MODEL>
-__global__ void __launch_bounds__(kThreads) MleFinalKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
+__global__ void __launch_bounds__(kThreads) MleFinalKernel(FitImages fi,
                                                            const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
                                                            MleParams mp, double* rows)
 {
@@ -1146,15 +1259,15 @@ __global__ void __launch_bounds__(kThreads) MleFinalKernel(const uint16_t* __res
 		double* row = rows + static_cast<long long>(k) * kCols;
 		const Cand cd = cands[k];
 		RoiAt r;
-		double t[5] = {0, 0, 0, 0, 0}, crlb[5] = {0, 0, 0, 0, 0};
-		bool ok = Locate(img, H, W, N, mp, cd, r) && row[kStatusCol] == kStOk;
+		double t[5] = {0, 0, 0, 0, 0}, crlb[5] = {0, 0, 0, 0, 0}, dev = 0;
+		bool ok = Locate(fi, mp, cd, r) && row[kStatusCol] == kStOk;
 		if (ok) {
 			#pragma unroll
 			for (int a = 0; a < 5; ++a) { t[a] = row[a]; }
-			ok = Final<MODEL, 1>(mp, MakePix(mp, r.base, W, nullptr, 0), t, crlb, xt, xt);
+			ok = Final<MODEL, 1>(mp, MakePix(mp, r.base, r.W, nullptr, 0), t, crlb, dev, xt, xt);
 			++evals;
 		}
-		StoreMleRow(row, -1, mp, cd, t, crlb, r.ux, r.uy, ok);
+		StoreMleRow(row, -1, mp, cd, t, crlb, dev, r.ux, r.uy, ok);
 	}
 	if (mp.evals && evals) { atomicAdd(mp.evals + 2, evals); }
 }
@@ -1169,7 +1282,7 @@ struct WarpSmem {
 };
 
 template <int MODEL>
-__global__ void __launch_bounds__(kThreads) MleWarpKernel(const uint16_t* __restrict__ img, int H, int W, long long N,
+__global__ void __launch_bounds__(kThreads) MleWarpKernel(FitImages fi,
                                                           const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
                                                           MleParams mp, double* rows)
 {
@@ -1184,17 +1297,17 @@ __global__ void __launch_bounds__(kThreads) MleWarpKernel(const uint16_t* __rest
 	for (uint32_t k = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; k < n; k += warps) {
 		const Cand cd = cands[k];
 		double* row = rows + static_cast<long long>(k) * kCols;
-		double t[5] = {0, 0, 0, 0, 0}, crlb[5] = {0, 0, 0, 0, 0};
+		double t[5] = {0, 0, 0, 0, 0}, crlb[5] = {0, 0, 0, 0, 0}, dev = 0;
 		RoiAt r;
-		if (!Locate(img, H, W, N, mp, cd, r)) {
-			StoreMleRow(row, lane, mp, cd, t, crlb, r.ux, r.uy, false);
+		if (!Locate(fi, mp, cd, r)) {
+			StoreMleRow(row, lane, mp, cd, t, crlb, 0.0, r.ux, r.uy, false);
 			continue;
 		}
-		Pix px = MakePix(mp, r.base, W, nullptr, 0);
+		Pix px = MakePix(mp, r.base, r.W, nullptr, 0);
 		ev[2] += InitTheta<MODEL, 32>(mp, px, r, t, xt32, yt32);
 		for (int q = lane; q < mp.n; q += 32) {
 			const int i = q / mp.roi, j = q - i * mp.roi;
-			ws.photons[q] = fmaxf((float(__ldg(r.base + i * W + j)) - px.off32) * px.inv32, 0.f);
+			ws.photons[q] = fmaxf((float(__ldg(r.base + i * r.W + j)) - px.off32) * px.inv32, 0.f);
 		}
 		__syncwarp();
 		Pix ps = px;
@@ -1245,11 +1358,11 @@ __global__ void __launch_bounds__(kThreads) MleWarpKernel(const uint16_t* __rest
 			ev[1] += Polish<MODEL, 32>(mp, ps, x0, y0, th, xt32, yt32);
 			#pragma unroll
 			for (int a = 0; a < 5; ++a) { t[a] = th[a]; }
-			ok = Final<MODEL, 32>(mp, px, t, crlb, xt64, yt64);
+			ok = Final<MODEL, 32>(mp, px, t, crlb, dev, xt64, yt64);
 			++ev[2];
 		}
 		__syncwarp();  // photons are rewritten for the next candidate
-		StoreMleRow(row, lane, mp, cd, t, crlb, r.ux, r.uy, ok);
+		StoreMleRow(row, lane, mp, cd, t, crlb, dev, r.ux, r.uy, ok);
 	}
 	if (mp.evals && lane == 0) {
 		#pragma unroll
@@ -1285,27 +1398,30 @@ int PersistentBlocks(K kernel, size_t smemBytes, int sms, uint32_t cap)
 	return static_cast<int>(std::min<uint32_t>((std::max<uint32_t>(cap, 1) + kThreads - 1) / kThreads, static_cast<uint32_t>(sms * perSm)));
 }
 
-template <int MODEL>
-bool LaunchThreadPerRoi(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
-                        uint32_t cap, const MleParams& mp, double* rows, cudaEvent_t* marks, cudaStream_t st)
+// The four-launch pipeline; the LM and polish run with L lanes per ROI (1: a thread per ROI; 2-16: lane groups).
+template <int MODEL, int L>
+bool LaunchPipeline(const FitImages& fi, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
+                    uint32_t cap, const MleParams& mp, double* rows, cudaEvent_t* marks, cudaStream_t st)
 {
 	const int sms = SmCount();
 	const uint32_t blocks = std::min<uint32_t>((std::max<uint32_t>(cap, 1) + kThreads - 1) / kThreads, static_cast<uint32_t>(sms) * 32u);
 	const size_t initBytes = static_cast<size_t>(mp.roi) * sizeof(float) * kThreads;
-	const size_t lmBytes = static_cast<size_t>(mp.n + 3 * mp.roi) * sizeof(float) * kThreads;
-	const size_t polishBytes = static_cast<size_t>(mp.n + 6 * mp.roi) * sizeof(float) * kThreads;
+	const size_t slots = L == 1 ? kThreads : kThreads / L;
+	const size_t lmBytes = static_cast<size_t>(SlotFloats(mp.n, mp.roi, 3, L)) * sizeof(float) * slots;
+	const size_t polishBytes = static_cast<size_t>(SlotFloats(mp.n, mp.roi, 6, L)) * sizeof(float) * slots;
 	const size_t finalBytes = static_cast<size_t>(3 * mp.roi) * sizeof(double) * kThreads;
-	const int lmBlocks = PersistentBlocks(MleLmKernel<MODEL>, lmBytes, sms, cap);
-	const int polishBlocks = PersistentBlocks(MlePolishKernel<MODEL>, polishBytes, sms, cap);
+	const uint32_t rois = static_cast<uint32_t>(std::min<unsigned long long>(static_cast<unsigned long long>(cap) * L, 0xffffffffull));
+	const int lmBlocks = PersistentBlocks(MleLmKernel<MODEL, L>, lmBytes, sms, rois);
+	const int polishBlocks = PersistentBlocks(MlePolishKernel<MODEL, L>, polishBytes, sms, rois);
 	if (mp.queue && !PTB_CUDA(cudaMemsetAsync(mp.queue, 0, 2 * sizeof(unsigned int), st))) { return false; }
 	if (marks) { cudaEventRecord(marks[0], st); }
-	MleInitKernel<MODEL><<<blocks, kThreads, initBytes, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows);
+	MleInitKernel<MODEL><<<blocks, kThreads, initBytes, st>>>(fi, cands, nptr, nconst, mp, rows);
 	if (marks) { cudaEventRecord(marks[1], st); }
-	MleLmKernel<MODEL><<<lmBlocks, kThreads, lmBytes, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows);
+	MleLmKernel<MODEL, L><<<lmBlocks, kThreads, lmBytes, st>>>(fi, cands, nptr, nconst, mp, rows);
 	if (marks) { cudaEventRecord(marks[2], st); }
-	MlePolishKernel<MODEL><<<polishBlocks, kThreads, polishBytes, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows);
+	MlePolishKernel<MODEL, L><<<polishBlocks, kThreads, polishBytes, st>>>(fi, cands, nptr, nconst, mp, rows);
 	if (marks) { cudaEventRecord(marks[3], st); }
-	MleFinalKernel<MODEL><<<blocks, kThreads, finalBytes, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows);
+	MleFinalKernel<MODEL><<<blocks, kThreads, finalBytes, st>>>(fi, cands, nptr, nconst, mp, rows);
 	if (marks) { cudaEventRecord(marks[4], st); }
 	CountLaunch(4);
 	return PTB_LAUNCHED();
@@ -1313,7 +1429,7 @@ bool LaunchThreadPerRoi(const uint16_t* img, int H, int W, long long N, const Ca
 
 // marks: the single launch is timed as the LM phase (marks 0-1 before it, marks 2-4 after it).
 template <int MODEL>
-bool LaunchWarpPerRoi(const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
+bool LaunchWarpPerRoi(const FitImages& fi, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
                       uint32_t cap, const MleParams& mp, double* rows, cudaEvent_t* marks, cudaStream_t st)
 {
 	const uint32_t perBlock = kThreads / 32;
@@ -1322,7 +1438,7 @@ bool LaunchWarpPerRoi(const uint16_t* img, int H, int W, long long N, const Cand
 		cudaEventRecord(marks[0], st);
 		cudaEventRecord(marks[1], st);
 	}
-	MleWarpKernel<MODEL><<<blocks, kThreads, 0, st>>>(img, H, W, N, cands, nptr, nconst, mp, rows);
+	MleWarpKernel<MODEL><<<blocks, kThreads, 0, st>>>(fi, cands, nptr, nconst, mp, rows);
 	if (marks) {
 		cudaEventRecord(marks[2], st);
 		cudaEventRecord(marks[3], st);
@@ -1333,17 +1449,25 @@ bool LaunchWarpPerRoi(const uint16_t* img, int H, int W, long long N, const Cand
 }
 
 template <int MODEL>
-bool LaunchModel(int lanes, const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr,
+bool LaunchModel(int lanes, const FitImages& fi, const Cand* cands, const uint32_t* nptr,
                  uint32_t nconst, uint32_t cap, const MleParams& mp, double* rows, cudaEvent_t* marks, cudaStream_t st)
 {
-	if (lanes == 1) { return LaunchThreadPerRoi<MODEL>(img, H, W, N, cands, nptr, nconst, cap, mp, rows, marks, st); }
-	return LaunchWarpPerRoi<MODEL>(img, H, W, N, cands, nptr, nconst, cap, mp, rows, marks, st);
+	switch (lanes) {
+		case 1: return LaunchPipeline<MODEL, 1>(fi, cands, nptr, nconst, cap, mp, rows, marks, st);
+		case 2: return LaunchPipeline<MODEL, 2>(fi, cands, nptr, nconst, cap, mp, rows, marks, st);
+		case 4: return LaunchPipeline<MODEL, 4>(fi, cands, nptr, nconst, cap, mp, rows, marks, st);
+		case 8: return LaunchPipeline<MODEL, 8>(fi, cands, nptr, nconst, cap, mp, rows, marks, st);
+		case 16: return LaunchPipeline<MODEL, 16>(fi, cands, nptr, nconst, cap, mp, rows, marks, st);
+		default: return LaunchWarpPerRoi<MODEL>(fi, cands, nptr, nconst, cap, mp, rows, marks, st);
+	}
 }
 
 }  // namespace
 
-// lanes: 1 = thread per ROI, anything else = warp per ROI. marks: profiling events (5) or null.
-bool LaunchMle(int lanes, const uint16_t* img, int H, int W, long long N, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
+// lanes: 1 = thread per ROI, 2 / 4 / 8 / 16 = lane groups per ROI in the LM and polish, anything else = warp per ROI
+// (one launch). mp.chunk: candidates a lane or group takes from the work queue at a time. marks: profiling events (5)
+// or null.
+bool LaunchMle(int lanes, const FitImages& fi, const Cand* cands, const uint32_t* nptr, uint32_t nconst,
                uint32_t cap, const MleParams& mp, double* rows, cudaEvent_t* marks, cudaStream_t st)
 {
 	if (mp.roi < 1 || mp.roi > kMaxRoi) {
@@ -1351,9 +1475,9 @@ bool LaunchMle(int lanes, const uint16_t* img, int H, int W, long long N, const 
 		return false;
 	}
 	switch (mp.model) {
-		case 6: return LaunchModel<6>(lanes, img, H, W, N, cands, nptr, nconst, cap, mp, rows, marks, st);
-		case 7: return LaunchModel<7>(lanes, img, H, W, N, cands, nptr, nconst, cap, mp, rows, marks, st);
-		case 8: return LaunchModel<8>(lanes, img, H, W, N, cands, nptr, nconst, cap, mp, rows, marks, st);
+		case 6: return LaunchModel<6>(lanes, fi, cands, nptr, nconst, cap, mp, rows, marks, st);
+		case 7: return LaunchModel<7>(lanes, fi, cands, nptr, nconst, cap, mp, rows, marks, st);
+		case 8: return LaunchModel<8>(lanes, fi, cands, nptr, nconst, cap, mp, rows, marks, st);
 		default: return false;
 	}
 }

@@ -51,7 +51,7 @@ __global__ void NoAllocPrepare(const double* __restrict__ pos, uint32_t n, uint6
 		c.y = p[3];
 		c.intensity = p[4];
 		c.surf = p[5];
-		c.pad = 0;
+		c.image = 0;
 		const double pl = p[1];
 		if (!(pl >= 1.0) || static_cast<uint64_t>(pl) > planes) {
 			c.x = -1.0;
@@ -142,7 +142,9 @@ long long FittingDeviceNoAlloc(const uint16_t* dStack, const double* dPositions,
 		SetError("PTB_FittingDeviceNoAlloc: spline modes 5 and 8 are not available without device allocation");
 		return -1;
 	}
-	if (height == 0 || width == 0 || planes == 0 || height * width > (1ull << 31) - 1) {
+	// each dimension is bounded before the product is formed, so the product cannot wrap
+	constexpr uint64_t kMaxPixels = (1ull << 31) - 1;
+	if (height == 0 || width == 0 || planes == 0 || height > kMaxPixels || width > kMaxPixels || height > kMaxPixels / width) {
 		SetError("PTB_FittingDeviceNoAlloc: invalid stack dimensions");
 		return -1;
 	}
@@ -154,6 +156,9 @@ long long FittingDeviceNoAlloc(const uint16_t* dStack, const double* dPositions,
 	fp.mle.fallbacks = &s->fallbacks;
 	fp.mle.queue = s->mleQueue;
 	fp.lanes = lanes;
+	// modes 6-8: the ROI mapping the Fitting export picks for the same call (a warp per ROI while the points fill the
+	// GPU a few times at most, else a thread per ROI), so that both give the same rows
+	if (fp.mode >= kMleGauss && fp.lanes == 0) { fp.lanes = nPoints <= 148ull * 64 ? 32 : 1; }
 	const uint32_t n = static_cast<uint32_t>(nPoints);
 	const uint32_t blocks = std::min<uint32_t>((n + 255) / 256, 148u * 4u);
 	NoAllocPrepare<<<blocks, 256, 0, st>>>(dPositions, n, planes, s);

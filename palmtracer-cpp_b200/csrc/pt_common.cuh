@@ -62,19 +62,41 @@ struct Counters {
 	uint32_t overflow;  // a list outgrew its capacity (the chunk must be redone with room)
 	uint32_t truncated; // some plane had more candidates than the per-plane capacity
 	uint32_t refit;     // FP32 fits redone in FP64
-	uint32_t pad[6];
+	uint32_t nroute;    // frames whose per-component flood could differ from the frame-wide one (flooded again)
+	uint32_t pad[5];    // [0..1]: work-queue counters of the persistent fit kernels
 };
 
 // One fit input: a segmentation candidate (x_, y_, intensity_, surf_ of SegmentationInfo) or a caller position.
 struct Cand {
 	double x, y, intensity, surf;
 	int frame;  // plane within the device stack the ROI is read from
-	int pad;
+	int image;  // entry of the launch's FitImages holding that stack (0 unless a launch fuses several stacks)
 };
+
+// The device stacks a maximum-likelihood fit launch reads: one, or several when the serving layer fuses the
+// candidates of concurrent requests into one launch (Cand::image selects the entry).
+constexpr int kMaxFitImages = 16;
+struct FitImage {
+	const uint16_t* img;
+	int H, W;
+	long long N;  // H * W
+};
+struct FitImages {
+	int n;
+	FitImage im[kMaxFitImages];
+};
+inline FitImages OneImage(const uint16_t* img, int H, int W, long long N)
+{
+	FitImages f{};
+	f.n = 1;
+	f.im[0] = FitImage{img, H, W, N};
+	return f;
+}
 
 // Maximum-likelihood modes 6-8 (fit_params layouts in include/palmtracer_b200.h).
 struct MleParams {
 	int model, roi, half, n, maxIter;
+	int chunk;  // candidates taken from the persistent kernels' work queue at a time (0 or 1: one)
 	double sigma0, offset, gain, crlbMax, pixelSize, zMin, zMax;
 	double astig[10];
 	int sx, sy, sz;
@@ -143,7 +165,8 @@ struct Workspace {
 	const uint16_t* img;  // the chunk's frames (device)
 	uint8_t* code;
 	long long* w1;        // W1 in 2^-16 units, valid on domain pixels only
-	uint32_t* par;        // union-find parent, then component id tag at roots
+	uint32_t* par;        // union-find parent, then component id tag at roots; once the groups are scattered, the
+	                      // parent-chain minimum of W1 of each pixel a global-memory flood pushes (its exactness check)
 	uint32_t* lab;        // region id + 1 on labelled domain pixels
 	uint32_t* rootmask;   // [B][H][words] bit set at root seeds
 	uint32_t* rowcnt;     // [B*H + 1] root seeds per row, scanned in place to row offsets
@@ -166,7 +189,9 @@ struct Workspace {
 	// fusion scratch, indexed by region id
 	double* fuMaxWN; double* fuMinP; double* fuMaxP; uint32_t* fuMaxPos; uint32_t* fuWNPos; uint32_t* fuNeighbour;
 	uint32_t* fuBecome; uint8_t* fuLocked;
-	// per frame [B + 1]
+	// per frame [B + 1]: domain pixels and seeds (counted by the detection kernel), 1 where the frame is flooded again
+	// frame-wide (its per-component flood failed the exactness check)
+	uint32_t* frameDom; uint32_t* frameSeeds; uint32_t* frameRoute;
 	uint32_t* frameRegBase; uint32_t* frameCandBase; uint32_t* frameKeep; uint32_t* frameOutBase;
 	// candidates / rows
 	uint32_t capRows;

@@ -11,7 +11,22 @@
 //      -v + pops * 1e-7 (Segmentation2D.cpp:336-385) and a pop counter local to the group. In strict mode a group is
 //      a whole frame and the counter is frame-global, which is the reference's process exactly;
 //   4. basin fusion (Segmentation2D.cpp:181-291) per group, then a second flood from one seed per basin;
-//   5. exact integer region sums (W1 is an integer in 2^-16 units) and the surf > 4 filter, in label order.
+//   5. exactness check of every per-component flood (below); a frame that fails it is flooded again as one unit
+//      with the frame-global counter (the strict process), so the labels always equal the reference's;
+//   6. exact integer region sums (W1 is an integer in 2^-16 units) and the surf > 4 filter, in label order.
+//
+// Why a per-component flood equals the frame-wide one, and when it may not. Labels only spread inside a component,
+// so a group's labels depend only on the order in which ITS pixels leave the heap; the frame-wide flood interleaves
+// the other components' pops, which changes the aging term it * 1e-7 of the keys but nothing else. Every key of the
+// frame-wide flood lies in [-v, -v + T * 1e-7], T = the frame's domain pixels (each is popped at most once). A
+// flooded pixel N takes the label of whichever neighbour leaves the heap first. Let y be N's parent in the
+// per-component flood and c the minimum W1 along y's parent chain down to its seed. If every element of that chain
+// has a frame-wide key below the key of a competing neighbour z (another label), the chain is popped, element by
+// element, before z can be: each element is pushed no later than its parent's pop and is then smaller than z. That
+// holds when c - W1(z) > T * 1e-7. So if every flooded pixel N and every neighbour z of N with another label satisfy
+// it, then (induction over the frame-wide flood's labelling order) every pixel receives its per-component label.
+// In 2^-16 units the test is (c - W1(z)) * 152 > T (2^-16 / 152 exceeds 1e-7 by 4e-10 per pop, which covers the
+// rounding of the FP64 keys, below 2e-11). Frames failing it at any boundary pixel are flooded again frame-wide.
 #include "pt_common.cuh"
 
 namespace ptb {
@@ -340,6 +355,68 @@ __global__ void GroupSizesStrict(Workspace ws)
 	}
 }
 
+// Frame-wide groups of the routed frames (one CTA): exclusive scans of their pixel, seed and region counts (zero for
+// the frames that are not routed; the counts come from the detection kernel and the row scan of root seeds), cursors
+// reset. Nothing to do when no frame is routed.
+constexpr int kRedoThreads = 1024;
+
+__global__ void __launch_bounds__(kRedoThreads) RedoOffsets(Workspace ws)
+{
+	__shared__ uint32_t warpSum[3][kRedoThreads / 32];
+	__shared__ uint32_t carry[3];
+	if (ws.cnt->nroute == 0) { return; }
+	const int B = ws.g.B, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	if (threadIdx.x < 3) { carry[threadIdx.x] = 0; }
+	__syncthreads();
+	for (int base = 0; base <= B; base += kRedoThreads) {
+		const int f = base + threadIdx.x;
+		uint32_t v[3] = {0u, 0u, 0u};
+		if (f < B && ws.frameRoute[f]) {
+			v[0] = ws.frameDom[f];
+			v[1] = ws.frameSeeds[f];
+			v[2] = ws.rowcnt[static_cast<long long>(f + 1) * ws.g.H] - ws.rowcnt[static_cast<long long>(f) * ws.g.H];
+		}
+		uint32_t x[3];
+		#pragma unroll
+		for (int a = 0; a < 3; ++a) {
+			x[a] = v[a];
+			#pragma unroll
+			for (int d = 1; d < 32; d <<= 1) {
+				const uint32_t y = __shfl_up_sync(0xffffffffu, x[a], d);
+				if (lane >= d) { x[a] += y; }
+			}
+			if (lane == 31) { warpSum[a][warp] = x[a]; }
+		}
+		__syncthreads();
+		if (warp == 0) {
+			#pragma unroll
+			for (int a = 0; a < 3; ++a) {
+				uint32_t w = warpSum[a][lane];
+				#pragma unroll
+				for (int d = 1; d < 32; d <<= 1) {
+					const uint32_t y = __shfl_up_sync(0xffffffffu, w, d);
+					if (lane >= d) { w += y; }
+				}
+				warpSum[a][lane] = w;  // inclusive over warps
+			}
+		}
+		__syncthreads();
+		if (f <= B) {
+			uint32_t* out[3] = {ws.gOff, ws.gSeedOff, ws.gRegOff};
+			#pragma unroll
+			for (int a = 0; a < 3; ++a) {
+				out[a][f] = carry[a] + (warp ? warpSum[a][warp - 1] : 0u) + x[a] - v[a];
+			}
+			ws.gCurPix[f] = 0;
+			ws.gCurSeed[f] = 0;
+			ws.gCurReg[f] = 0;
+		}
+		__syncthreads();
+		if (threadIdx.x < 3) { carry[threadIdx.x] += warpSum[threadIdx.x][kRedoThreads / 32 - 1]; }
+		__syncthreads();
+	}
+}
+
 __device__ __forceinline__ int GroupOf(const Workspace& ws, uint32_t p, int strict)
 {
 	if (strict) { return Decompose(p, ws.g).f; }
@@ -350,16 +427,20 @@ __device__ __forceinline__ int GroupOf(const Workspace& ws, uint32_t p, int stri
 // Domain pixels: labels of the non-seed pixels (single-region components take their region outright; flooded
 // pixels of groups start unlabelled, seeds keep theirs) and the pixel lists of the groups. compRegion holds the
 // region of a single-region component and the group index of a multi-region one.
+// strict: 0 per-component groups, 1 every frame is a group, 2 only the frames routed to the frame-wide flood are
+// (their seeds get their labels back, since a fusion may have cleared them; nothing to do when no frame is routed).
 __global__ void GroupScatter(Workspace ws, int strict)
 {
+	if (strict == 2 && ws.cnt->nroute == 0) { return; }
 	const uint32_t nd = min(ws.cnt->ndom, ws.capDom);
 	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nd; k += gridDim.x * blockDim.x) {
 		const uint32_t p = ws.dom[k];
 		const bool seed = (ws.code[p] & kSeed) != 0;
 		int m;
 		if (strict) {
-			if (!seed) { ws.lab[p] = 0u; }
 			m = Decompose(p, ws.g).f;
+			if (strict == 2 && ws.frameRoute[m] == 0) { continue; }
+			if (!seed) { ws.lab[p] = 0u; }
 		}
 		else {
 			const uint32_t c = CompOf(ws.par, p);
@@ -375,6 +456,11 @@ __global__ void GroupScatter(Workspace ws, int strict)
 		const uint32_t s = ws.seeds[k];
 		const int m = GroupOf(ws, s, strict);
 		if (m < 0) { continue; }
+		if (strict == 2) {
+			if (ws.frameRoute[m] == 0) { continue; }
+			const uint32_t r = RegionOfRoot(ws, SeedRoot(ws, s));
+			if (r < ws.capRegion) { ws.lab[s] = r + 1; }
+		}
 		ws.gSeed[ws.gSeedOff[m] + atomicAdd(ws.gCurSeed + m, 1u)] = s;
 		if (((ws.code[s] >> kDirShift) & 7) == 0) { ws.gReg[ws.gRegOff[m] + atomicAdd(ws.gCurReg + m, 1u)] = ws.lab[s] - 1; }
 	}
@@ -503,6 +589,10 @@ struct GlobalView {
 	__device__ __forceinline__ uint32_t Lab(uint32_t p, int, int) const { return ws.lab[p]; }
 	__device__ __forceinline__ void SetLab(uint32_t p, int, int, uint32_t v) const { ws.lab[p] = v; }
 	__device__ __forceinline__ double W1(uint32_t p, int, int) const { return static_cast<double>(__ldg(ws.w1 + p)); }
+	__device__ __forceinline__ uint32_t W1Fixed(uint32_t p, int, int) const { return static_cast<uint32_t>(__ldg(ws.w1 + p)); }
+	// parent-chain minimum of W1 (kNoChain on the flood's seeds), kept in par once the groups are scattered
+	__device__ __forceinline__ uint32_t Chain(uint32_t p, int, int) const { return ws.par[p]; }
+	__device__ __forceinline__ void SetChain(uint32_t p, int, int, uint32_t v) const { ws.par[p] = v; }
 };
 
 // ... or staged in shared memory: the group's bounding box with a one-pixel ring, row-major from (bx0, by0). Every
@@ -514,9 +604,10 @@ constexpr int kBoxWarps = 8;          // groups (warps) per CTA
 struct BoxSmem {
 	double key[kBoxHeap];
 	uint32_t pix[kBoxHeap];
-	uint32_t w1[kBoxCap];   // W1 in 2^-16 units (0 < W1 < 2^32 on the domain)
+	uint32_t w1[kBoxCap];     // W1 in 2^-16 units (0 < W1 < 2^32 on the domain)
 	uint32_t lab[kBoxCap];
-	uint8_t flag[kBoxCap];  // bit 0: domain; bit 1: unlabelled when staged (the flood's labels are written back)
+	uint32_t chain[kBoxCap];  // parent-chain minimum of W1 of the flooded pixels
+	uint8_t flag[kBoxCap];    // bit 0: domain; bit 1: unlabelled when staged (the flood's labels are written back)
 };
 
 struct BoxView {
@@ -527,10 +618,50 @@ struct BoxView {
 	__device__ __forceinline__ uint32_t Lab(uint32_t, int y, int x) const { return sm.lab[At(y, x)]; }
 	__device__ __forceinline__ void SetLab(uint32_t, int y, int x, uint32_t v) const { sm.lab[At(y, x)] = v; }
 	__device__ __forceinline__ double W1(uint32_t, int y, int x) const { return static_cast<double>(sm.w1[At(y, x)]); }
+	__device__ __forceinline__ uint32_t W1Fixed(uint32_t, int y, int x) const { return sm.w1[At(y, x)]; }
+	__device__ __forceinline__ uint32_t Chain(uint32_t, int y, int x) const { return sm.chain[At(y, x)]; }
+	__device__ __forceinline__ void SetChain(uint32_t, int y, int x, uint32_t v) const { sm.chain[At(y, x)] = v; }
 };
 
+constexpr uint32_t kNoChain = 0xffffffffu;  // chain minimum of a flood's seeds (they were not pushed)
+
+// The exactness test of one boundary pair: N (flooded, parent-chain minimum `chain`) against a neighbour of another
+// label with W1 `w1z`, T = domain pixels of the frame (the bound of the frame-wide flood's pop counter).
+__device__ __forceinline__ bool PairExact(uint32_t chain, uint32_t w1z, uint32_t T)
+{
+	return (static_cast<long long>(chain) - static_cast<long long>(w1z)) * 152 > static_cast<long long>(T);
+}
+
+// Marks frame f for the frame-wide flood (once).
+__device__ __forceinline__ void RouteFrame(const Workspace& ws, int f)
+{
+	if (atomicExch(ws.frameRoute + f, 1u) == 0u) { atomicAdd(&ws.cnt->nroute, 1u); }
+}
+
+// Exactness test of a flooded pixel p against its 8 neighbours in global memory; false routes the frame.
+__device__ bool PixelExactGlobal(const Workspace& ws, uint32_t p, uint32_t T)
+{
+	const uint32_t chain = ws.par[p];
+	if (chain == kNoChain) { return true; }
+	const Pix q = Decompose(p, ws.g);
+	const uint32_t L = ws.lab[p];
+	for (int dy = -1; dy <= 1; ++dy) {
+		const int yy = q.y + dy;
+		if (yy < 0 || yy >= ws.g.H) { continue; }
+		for (int dx = -1; dx <= 1; ++dx) {
+			const int xx = q.x + dx;
+			if ((dx == 0 && dy == 0) || xx < 0 || xx >= ws.g.W) { continue; }
+			const uint32_t nb = p + static_cast<uint32_t>(dy * ws.g.W + dx);
+			if (!(__ldg(ws.code + nb) & kDomain) || ws.lab[nb] == L) { continue; }
+			if (!PairExact(chain, static_cast<uint32_t>(__ldg(ws.w1 + nb)), T)) { return false; }
+		}
+	}
+	return true;
+}
+
 // Priority flood of one group from its labelled seeds (sorted ascending = raster order), Segmentation2D.cpp:336-385.
-template <class View>
+// kChain: record each pushed pixel's parent-chain minimum of W1 (the seeds must hold kNoChain) for the exactness test.
+template <bool kChain, class View>
 __device__ void FloodGroup(const Geometry& geo, const View& v, const uint32_t* seedList, uint32_t nSeeds, Heap& heap)
 {
 	for (uint32_t i = 0; i < nSeeds; ++i) {
@@ -578,6 +709,7 @@ __device__ void FloodGroup(const Geometry& geo, const View& v, const uint32_t* s
 			wv[t] = dm[t] ? v.W1(nb[t], ny[t], nx[t]) : 0.0;
 		}
 		const double age = __dmul_rn(static_cast<double>(pops), kEps);
+		const uint32_t chain = kChain ? min(v.Chain(p, q.y, q.x), v.W1Fixed(p, q.y, q.x)) : 0u;
 		#pragma unroll
 		for (int t = 0; t < 8; ++t) {
 			if (dm[t] && lb[t] == 0) {
@@ -585,28 +717,34 @@ __device__ void FloodGroup(const Geometry& geo, const View& v, const uint32_t* s
 				const double k = __dadd_rn(-(wv[t] * kW1Unit), age);
 				heap.Push(k, nb[t]);
 				v.SetLab(nb[t], ny[t], nx[t], L);
+				if (kChain) { v.SetChain(nb[t], ny[t], nx[t], chain); }
 			}
 		}
 	}
 }
 
 // Flood with the heap in this thread's shared-memory slice, moving to the group's global slice (hk, hp) if it outgrows it.
+template <bool kChain>
 __device__ void FloodGroupGlobal(const Workspace& ws, const uint32_t* seedList, uint32_t nSeeds, double* hk, uint32_t* hp,
                                  FloodSmem& sm)
 {
 	Heap heap{sm.key + threadIdx.x, sm.pix + threadIdx.x, 0, kFloodThreads, kSmemHeap, hk, hp};
-	FloodGroup(ws.g, GlobalView{ws}, seedList, nSeeds, heap);
+	FloodGroup<kChain>(ws.g, GlobalView{ws}, seedList, nSeeds, heap);
 }
 
-__global__ void __launch_bounds__(kFloodThreads) GroupFlood(Workspace ws, uint32_t nGroupsStrict)
+// Frame-wide floods (groups = frames): every frame (strict mode) or only the frames that failed the exactness test of
+// their per-component floods (routed: nothing to do when no frame did).
+__global__ void __launch_bounds__(kFloodThreads) GroupFlood(Workspace ws, uint32_t nGroupsStrict, int routed)
 {
 	__shared__ FloodSmem sm;
+	if (routed && ws.cnt->nroute == 0) { return; }
 	const uint32_t n = nGroupsStrict ? nGroupsStrict : ws.cnt->nmulti;
 	for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+		if (routed && ws.frameRoute[m] == 0) { continue; }
 		const uint32_t nSeeds = ws.gSeedOff[m + 1] - ws.gSeedOff[m];
 		uint32_t* seeds = ws.gSeed + ws.gSeedOff[m];
 		SortSlice(seeds, nSeeds);
-		FloodGroupGlobal(ws, seeds, nSeeds, ws.heapKey + ws.gOff[m], ws.heapPix + ws.gOff[m], sm);
+		FloodGroupGlobal<false>(ws, seeds, nSeeds, ws.heapKey + ws.gOff[m], ws.heapPix + ws.gOff[m], sm);
 	}
 }
 
@@ -643,13 +781,19 @@ __global__ void __launch_bounds__(kBoxWarps * 32) GroupFloodBox(Workspace ws)
 		const int bw = min(x1 + 1, geo.W - 1) - bx0 + 1, bh = min(y1 + 1, geo.H - 1) - by0 + 1;
 		double* hk = ws.heapKey + off;
 		uint32_t* hp = ws.heapPix + off;
+		const uint32_t T = ws.frameDom[f];
 		if (nPix == 0 || bw * bh > kBoxCap) {
+			for (uint32_t i = lane; i < nPix; i += 32) { ws.par[ws.gPix[off + i]] = kNoChain; }
+			__syncwarp();
 			if (lane == 0 && nPix > 0) {
 				SortSlice(seeds, nSeeds);
 				Heap heap{sm.key, sm.pix, 0, 1, kBoxHeap, hk, hp};
-				FloodGroup(geo, GlobalView{ws}, seeds, nSeeds, heap);
+				FloodGroup<true>(geo, GlobalView{ws}, seeds, nSeeds, heap);
 			}
 			__syncwarp();
+			bool exact = true;
+			for (uint32_t i = lane; i < nPix && exact; i += 32) { exact = PixelExactGlobal(ws, ws.gPix[off + i], T); }
+			if (__any_sync(0xffffffffu, !exact) && lane == 0) { RouteFrame(ws, f); }
 			continue;
 		}
 		const uint32_t base = static_cast<uint32_t>(f) * static_cast<uint32_t>(geo.N) + static_cast<uint32_t>(by0 * geo.W + bx0);
@@ -660,32 +804,48 @@ __global__ void __launch_bounds__(kBoxWarps * 32) GroupFloodBox(Workspace ws)
 			const uint32_t lb = dom ? ws.lab[p] : 0u;
 			sm.w1[i] = dom ? static_cast<uint32_t>(__ldg(ws.w1 + p)) : 0u;
 			sm.lab[i] = lb;
+			sm.chain[i] = kNoChain;
 			sm.flag[i] = static_cast<uint8_t>((dom ? 1u : 0u) | (dom && lb == 0 ? 2u : 0u));
 		}
 		__syncwarp();
 		if (lane == 0) {
 			SortSlice(seeds, nSeeds);
 			Heap heap{sm.key, sm.pix, 0, 1, kBoxHeap, hk, hp};
-			FloodGroup(geo, BoxView{sm, bx0, by0, bw}, seeds, nSeeds, heap);
+			FloodGroup<true>(geo, BoxView{sm, bx0, by0, bw}, seeds, nSeeds, heap);
 		}
 		__syncwarp();
+		bool exact = true;
 		for (int i = lane; i < bw * bh; i += 32) {
-			if ((sm.flag[i] & 2u) && sm.lab[i] != 0) {
-				const int r = i / bw, c = i - r * bw;
-				ws.lab[base + static_cast<uint32_t>(r * geo.W + c)] = sm.lab[i];
+			if (!(sm.flag[i] & 2u) || sm.lab[i] == 0) { continue; }
+			const int r = i / bw, c = i - r * bw;
+			ws.lab[base + static_cast<uint32_t>(r * geo.W + c)] = sm.lab[i];
+			// exactness test against the neighbours of other labels (every neighbour in the frame lies in the box)
+			const uint32_t L = sm.lab[i], chain = sm.chain[i];
+			for (int dy = -1; dy <= 1; ++dy) {
+				if (r + dy < 0 || r + dy >= bh) { continue; }
+				for (int dx = -1; dx <= 1; ++dx) {
+					if ((dx == 0 && dy == 0) || c + dx < 0 || c + dx >= bw) { continue; }
+					const int j = i + dy * bw + dx;
+					if ((sm.flag[j] & 1u) && sm.lab[j] != L && !PairExact(chain, sm.w1[j], T)) { exact = false; }
+				}
 			}
 		}
+		if (__any_sync(0xffffffffu, !exact) && lane == 0) { RouteFrame(ws, f); }
 		__syncwarp();
 	}
 }
 
 // Basin fusion of one group (Segmentation2D.cpp:181-291) followed by the reseeded second flood.
-__global__ void __launch_bounds__(kFloodThreads) GroupFuse(Workspace ws, uint32_t nGroupsStrict, double ratio)
+// Groups: the per-component groups (nGroupsStrict = 0; the second flood is checked for exactness), every frame
+// (strict mode) or only the frames flooded again frame-wide (routed).
+__global__ void __launch_bounds__(kFloodThreads) GroupFuse(Workspace ws, uint32_t nGroupsStrict, double ratio, int routed)
 {
 	__shared__ FloodSmem sm;
+	if (routed && ws.cnt->nroute == 0) { return; }
 	const uint32_t n = nGroupsStrict ? nGroupsStrict : ws.cnt->nmulti;
 	const Geometry& geo = ws.g;
 	for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+		if (routed && ws.frameRoute[m] == 0) { continue; }
 		uint32_t* regs = ws.gReg + ws.gRegOff[m];
 		uint32_t nReg = ws.gRegOff[m + 1] - ws.gRegOff[m];
 		const uint32_t* pix = ws.gPix + ws.gOff[m];
@@ -768,7 +928,11 @@ __global__ void __launch_bounds__(kFloodThreads) GroupFuse(Workspace ws, uint32_
 			nReg = kept;
 		}
 		// one seed per basin at its first maximum, then flood again
-		for (uint32_t i = 0; i < nPix; ++i) { ws.lab[pix[i]] = 0; }
+		const bool check = nGroupsStrict == 0;
+		for (uint32_t i = 0; i < nPix; ++i) {
+			ws.lab[pix[i]] = 0;
+			if (check) { ws.par[pix[i]] = kNoChain; }
+		}
 		uint32_t* seeds = ws.gSeed + ws.gSeedOff[m];  // reuse the seed slice (nReg <= number of seeds)
 		for (uint32_t i = 0; i < nReg; ++i) {
 			const uint32_t r = regs[i];
@@ -776,7 +940,19 @@ __global__ void __launch_bounds__(kFloodThreads) GroupFuse(Workspace ws, uint32_
 			ws.lab[ws.fuMaxPos[r]] = r + 1;
 		}
 		SortSlice(seeds, nReg);
-		FloodGroupGlobal(ws, seeds, nReg, ws.heapKey + ws.gOff[m], ws.heapPix + ws.gOff[m], sm);
+		if (!check) {
+			FloodGroupGlobal<false>(ws, seeds, nReg, ws.heapKey + ws.gOff[m], ws.heapPix + ws.gOff[m], sm);
+			continue;
+		}
+		FloodGroupGlobal<true>(ws, seeds, nReg, ws.heapKey + ws.gOff[m], ws.heapPix + ws.gOff[m], sm);
+		const int f = Decompose(pix[0], geo).f;
+		const uint32_t T = ws.frameDom[f];
+		for (uint32_t i = 0; i < nPix; ++i) {
+			if (!PixelExactGlobal(ws, pix[i], T)) {
+				RouteFrame(ws, f);
+				break;
+			}
+		}
 	}
 }
 
@@ -904,18 +1080,33 @@ bool LaunchSegment(const Workspace& ws, double ratio, int strict, uint32_t maxPo
 		ok = ok && ExclusiveScan(ws.gSeedOff, &ws.cnt->nmulti, 0, ws.capComp, ws.scanBlock, nullptr, st);
 		ok = ok && ExclusiveScan(ws.gRegOff, &ws.cnt->nmulti, 0, ws.capComp, ws.scanBlock, nullptr, st);
 	}
-	GroupScatter<<<kGrid, kThreads, 0, st>>>(ws, strict);
+	GroupScatter<<<kGrid, kThreads, 0, st>>>(ws, strict ? 1 : 0);
 	if (strict) {  // frame-wide groups: one thread per group, small CTAs so that many SMs share the frames
-		GroupFlood<<<kGrid * 2, kFloodThreads, 0, st>>>(ws, groupsStrict);
+		GroupFlood<<<kGrid * 2, kFloodThreads, 0, st>>>(ws, groupsStrict, 0);
 	}
 	else {  // one warp per group, staged in shared memory
 		GroupFloodBox<<<kGrid, kBoxWarps * 32, 0, st>>>(ws);
 	}
 	CountLaunch(2);
 	ok = ok && PTB_LAUNCHED();
-	if (static_cast<int>(ratio) > 0) {  // WatershedIntelligent, Segmentation2D.cpp:77-85
-		GroupFuse<<<kGrid * 2, kFloodThreads, 0, st>>>(ws, groupsStrict, ratio);
+	const bool fuse = static_cast<int>(ratio) > 0;  // WatershedIntelligent, Segmentation2D.cpp:77-85
+	if (fuse) {
+		GroupFuse<<<kGrid * 2, kFloodThreads, 0, st>>>(ws, groupsStrict, ratio, 0);
 		CountLaunch();
+		ok = ok && PTB_LAUNCHED();
+	}
+	if (!strict) {
+		// frames whose per-component floods failed the exactness test: flooded again as one unit with the frame-global
+		// pop counter (each kernel returns at once when no frame was routed)
+		const uint32_t frames = static_cast<uint32_t>(g.B);
+		RedoOffsets<<<1, kRedoThreads, 0, st>>>(ws);
+		GroupScatter<<<kGrid, kThreads, 0, st>>>(ws, 2);
+		GroupFlood<<<kGrid * 2, kFloodThreads, 0, st>>>(ws, frames, 1);
+		CountLaunch(3);
+		if (fuse) {
+			GroupFuse<<<kGrid * 2, kFloodThreads, 0, st>>>(ws, frames, ratio, 1);
+			CountLaunch();
+		}
 		ok = ok && PTB_LAUNCHED();
 	}
 	RegionStats<<<kGrid, kThreads, 0, st>>>(ws);

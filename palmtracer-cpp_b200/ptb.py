@@ -15,9 +15,10 @@ COLS = 18
 # every symbol the public header declares
 EXPORTS = ["Localization", "Fitting", "Wavelett", "AutoThreshold", "Astigmatism3DEstimation", "PTB_LocalizationDevice",
            "PTB_SetSegmentationMode", "PTB_SetFitPrecision", "PTB_LastError", "PTB_KernelLaunchCount",
-           "PTB_SetProfiling", "PTB_StageTimes", "PTB_MleEvaluations", "PTB_GraphStats", "PTB_MeasureFmaPeak", "PTB_FittingDeviceNoAlloc",
-           "PTB_ServerStart", "PTB_SubmitStack", "PTB_PollStack", "PTB_StackResult", "PTB_ServerStop",
-           "PTB_TiffInfo", "PTB_TiffRead", "PTB_LocalizationTiff", "Tracking", "PTB_TrackingDevice"]
+           "PTB_SetProfiling", "PTB_StageTimes", "PTB_MleEvaluations", "PTB_GraphStats", "PTB_SegmentationStats", "PTB_EnginePoolStats",
+           "PTB_MeasureFmaPeak", "PTB_FittingDeviceNoAlloc",
+           "PTB_ServerStart", "PTB_SubmitStack", "PTB_PollStack", "PTB_StackResult", "PTB_ServerStop", "PTB_ServerFuseStats",
+           "PTB_TiffInfo", "PTB_TiffRead", "PTB_LocalizationTiff", "Tracking", "PTB_TrackingDevice", "PTB_SplineCoefficients"]
 
 _u16p = ctypes.POINTER(ctypes.c_uint16)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -74,6 +75,14 @@ def load(path=LIB_PATH):
     L.PTB_LocalizationTiff.argtypes = [ctypes.c_char_p, _f64p, _u64, _f64, _f64, _u64, _f64p]
     L.PTB_GraphStats.restype = None
     L.PTB_GraphStats.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
+    L.PTB_SegmentationStats.restype = None
+    L.PTB_SegmentationStats.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
+    L.PTB_EnginePoolStats.restype = None
+    L.PTB_EnginePoolStats.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
+    L.PTB_SplineCoefficients.restype = _u64
+    L.PTB_SplineCoefficients.argtypes = [_f64p, _u64, _u64, _u64, _f64p, _f64p]
+    L.PTB_ServerFuseStats.restype = None
+    L.PTB_ServerFuseStats.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
     L.PTB_FittingDeviceNoAlloc.restype = _u64
     L.PTB_FittingDeviceNoAlloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _u64, ctypes.c_void_p, _u64, _u64, _u64, _u64,
                                            _f64p, ctypes.c_void_p]
@@ -269,6 +278,36 @@ def graph_stats():
     return {"captured": int(out[0]), "replayed": int(out[1]), "direct": int(out[2])}
 
 
+def segmentation_stats():
+    """{"frames", "routed"}: frames segmented by this device's engine and, of those, frames flooded again frame-wide
+    after their per-component floods failed the exactness test, since the last call."""
+    out = np.zeros(2, dtype=np.uint64)
+    load().PTB_SegmentationStats(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 2)
+    return {"frames": int(out[0]), "routed": int(out[1])}
+
+
+def spline_coefficients(psf, lam=None):
+    """Cubic-spline coefficient table of a PSF volume [nz, ny, nx] (PTB_SplineCoefficients): [64, nz-1, ny-1, nx-1]."""
+    psf = np.ascontiguousarray(psf, dtype=np.float64)
+    nz, ny, nx = psf.shape
+    out = np.zeros((64, nz - 1, ny - 1, nx - 1))
+    lam_p = None
+    if lam is not None:
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        lam_p = lam.ctypes.data_as(_f64p)
+    n = load().PTB_SplineCoefficients(psf.ctypes.data_as(_f64p), nx, ny, nz, lam_p, out.ctypes.data_as(_f64p))
+    if n == 0 or n != out.size:
+        raise RuntimeError("PTB_SplineCoefficients failed: " + last_error())
+    return out
+
+
+def engine_pool_stats():
+    """{"engines", "peak_leased"}: engines in this device's pool and the most leased at the same time."""
+    out = np.zeros(2, dtype=np.uint64)
+    load().PTB_EnginePoolStats(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 2)
+    return {"engines": int(out[0]), "peak_leased": int(out[1])}
+
+
 def fma_peak(fp64):
     """Measured FMA FLOP/s of the current device (FP64 when fp64 is true, else FP32)."""
     return load().PTB_MeasureFmaPeak(int(bool(fp64)))
@@ -318,6 +357,12 @@ class Server:
             raise RuntimeError("PTB_StackResult failed: " + last_error())
         out = held[1]
         return out[:n].reshape(-1, COLS).copy(), float(times[0]), float(times[1])
+
+    def fuse_stats(self):
+        """{"launches", "chunks"}: fused fit launches of this server and the chunks they fitted."""
+        out = np.zeros(2, dtype=np.uint64)
+        load().PTB_ServerFuseStats(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 2)
+        return {"launches": int(out[0]), "chunks": int(out[1])}
 
     def stop(self):
         load().PTB_ServerStop()

@@ -5,6 +5,8 @@ Reads (text and TIFF only, nothing executed) from the reference tree:
   Tests_CPU/Input/ref/stack-localizations-*.csv,
   Tests_CPU/Input/ref/stack_quadrant-localizations-*.csv                  -> localizations.npz
   Tests_CPU/Input/ref/stack-tracking-*-5.csv                              -> tracking.npz
+  Tests_CPU/Input/Beads.tiff (a 29 x 29 x 61 crop around the bead at x 25, y 19 that the reference's spline
+  calibration test lists first, Tests_CPU/test_sp_Spline.cpp:47-51; focus near plane 88) -> beads.npz
 The AutoThreshold known answers come from Tests_CPU/test_Palm.cpp:307-310 and are stored beside them.
 
 Usage: python tests/golden/make_golden.py REFERENCE_ROOT   (or set PTB_REFERENCE_ROOT)
@@ -62,7 +64,10 @@ def main(ref_root):
         _, data = load_csv(path)
         tracks[os.path.basename(path)[:-4]] = data
     np.savez_compressed(os.path.join(HERE, "tracking.npz"), **tracks)
-    print({k: v.shape for k, v in stacks.items()}, len(locs) - 1, "csv tables")
+    beads = load_tiff_stack(os.path.join(inp, "Beads.tiff"))
+    crop = beads[58:119, 19 - 14:19 + 15, 25 - 14:25 + 15]
+    np.savez_compressed(os.path.join(HERE, "beads.npz"), bead=crop, origin=np.array([25 - 14, 19 - 14, 58]))
+    print({k: v.shape for k, v in stacks.items()}, len(locs) - 1, "csv tables", "bead crop", crop.shape)
 
 
 if __name__ == "__main__":

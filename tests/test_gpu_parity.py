@@ -87,6 +87,40 @@ def test_detection_strict_mode_low_threshold_bitwise(lib, orc, scale):
         lib.set_segmentation_mode(prev)
 
 
+@pytest.mark.parametrize("size,frames", [((256, 256), 3), ((1024, 1024), 1)])
+@pytest.mark.parametrize("scale", [1.0, 0.3, 0.1, 0.0])
+def test_detection_default_mode_low_threshold_bitwise(lib, orc, size, frames, scale):
+    """Default mode at any threshold: per-component floods, the exactness test, and the frame-wide flood for frames
+    that fail it give the reference's candidates bit for bit. Below the benchmark threshold the aging term decides
+    contested pixels (the per-component order differs from the frame-wide one), so frames must be routed; at the
+    benchmark threshold none is."""
+    s, thr = _synth("c2", frames, 21, orc, size)
+    assert lib.set_segmentation_mode(0) == 0
+    for ratio in (0.0, 10.0):
+        lib.segmentation_stats()
+        a = lib.localization(s, thr * scale, ratio, 0, GAUSS_PARAMS)
+        stats = lib.segmentation_stats()
+        b = orc.localization(s, thr * scale, ratio, 0, GAUSS_PARAMS)
+        assert a.shape == b.shape and np.array_equal(a, b), (ratio, stats)
+        assert stats["frames"] == frames
+        print("scale", scale, "ratio", ratio, "size", size, "routed", stats["routed"], "of", frames)
+        if scale == 1.0:
+            assert stats["routed"] == 0, stats
+        if scale <= 0.1:
+            assert stats["routed"] >= 1, stats
+
+
+def test_detection_benchmark_frames_not_routed(lib, orc):
+    """At the benchmark's own threshold no 1024 x 1024 benchmark-statistics frame needs the frame-wide flood."""
+    s, thr = _synth("c2", 6, 1000, orc)
+    lib.segmentation_stats()
+    a = lib.localization(s, thr, 0.0, 0, GAUSS_PARAMS)
+    stats = lib.segmentation_stats()
+    assert stats == {"frames": 6, "routed": 0}
+    b = orc.localization(s, thr, 0.0, 0, GAUSS_PARAMS)
+    assert a.shape == b.shape and np.array_equal(a, b)
+
+
 def test_detection_edge_cases(lib, orc):
     # black stack, empty output capacity, single plane, plateaus, tiny frames
     assert lib.localization(np.zeros((3, 12, 16), np.uint16), 0.0, 0.0, 0, GAUSS_PARAMS).shape[0] == 0
@@ -331,14 +365,15 @@ def _deviances(orc, stack, thr, model, params, a, e, idx):
     return out
 
 
-def _mle_check(a, b, name, model, flip_share, orc=None, stack=None, thr=None, params=None):
+def _mle_check(a, b, name, model, flip_share, orc=None, stack=None, thr=None, params=None, other_optima=2):
     """Per-result error table (median, p99, max per quantity) of the GPU rows against the oracle's, over the fits
     that converged to the oracle's optimum; asserts the stated tolerances on them.
 
     Fits beyond tolerance are the ones whose FP32 path ended in another local optimum of the deviance (overlapping
     emitters, parameters on bounds). Each is classified by the FP64 deviance of both results: "gpu_better" (the GPU's
     optimum is at least as likely) or "gpu_worse". At most a `flip_share` of the fits may be gpu_worse or change
-    between success and the failure sentinel. With PTB_ERROR_TABLE set the record is appended to that file."""
+    between success and the failure sentinel, and at most `other_optima` fits (an explicit count) may end in another
+    optimum that is at least as likely. The record is printed; with PTB_ERROR_TABLE set it is appended to that file."""
     bad, worst, pairs = match_rows(a, b, atol=1e9, rtol=0, keys=(C_X, C_Y))
     if bad and os.environ.get("PTB_ERROR_TABLE"):
         np.savez_compressed(os.environ["PTB_ERROR_TABLE"] + "." + name.replace(" ", "_").replace("=", "") + ".npz", gpu=a, oracle=b)
@@ -376,45 +411,103 @@ def _mle_check(a, b, name, model, flip_share, orc=None, stack=None, thr=None, pa
     flips = int(np.sum(ok != got))
     record = {"case": name, "fits": int(both.sum()), "within_tolerance": int(same.sum()), "other_optimum_gpu_better": better,
               "other_optimum_gpu_worse": worse, "flips": flips, "errors": table}
+    print(json.dumps(record))
     if os.environ.get("PTB_ERROR_TABLE"):
         with open(os.environ["PTB_ERROR_TABLE"], "a") as f:
             f.write(json.dumps(record) + "\n")
     assert flips + worse <= max(1, int(both.sum() * flip_share)), record
-    assert better <= max(1, int(both.sum() * 0.05)), record
+    assert better <= other_optima, record
     for key, row in table.items():
         assert row["max"] <= row["tol"], (key, record)
     return record
 
 
-@pytest.mark.parametrize("lanes", ["1", "32"])
-def test_mle_gauss_mode6_vs_oracle(lib, orc, lanes, monkeypatch):
+# ROI mappings of the MLE fits: lanes per ROI (1 thread, 2-16 lane groups, 32 a warp) and the work queue's chunk
+MAPPINGS = [("1", "1"), ("1", "4"), ("2", "1"), ("4", "1"), ("8", "1"), ("16", "1"), ("32", "1")]
+_ORACLE_ROWS = {}
+
+
+def _oracle_rows(orc, s, thr, fit, params, key, **kw):
+    """The oracle's rows of one synthetic case, computed once per test session."""
+    if key not in _ORACLE_ROWS:
+        _ORACLE_ROWS[key] = orc.localization(s, thr, 0.0, fit, params, **kw)
+    return _ORACLE_ROWS[key]
+
+
+def _mapping(monkeypatch, lanes, chunk):
     monkeypatch.setenv("PTB_MLE_LANES", lanes)
+    monkeypatch.setenv("PTB_MLE_CHUNK", chunk)
+    return "lanes=%s chunk=%s" % (lanes, chunk)
+
+
+@pytest.mark.parametrize("lanes,chunk", MAPPINGS)
+def test_mle_gauss_mode6_vs_oracle(lib, orc, lanes, chunk, monkeypatch):
+    name = _mapping(monkeypatch, lanes, chunk)
     s, thr = _synth("c1", 6, 31, orc)
     a = lib.localization(s, thr, 0.0, 6, MLE6)
-    b = orc.localization(s, thr, 0.0, 6, MLE6)
+    b = _oracle_rows(orc, s, thr, 6, MLE6, "c1-6")
     assert a.shape == b.shape and a.shape[0] > 100
-    _mle_check(a, b, "mode6 gauss c1 lanes=" + lanes, 6, 1 / 500, orc, s, thr, MLE6)
+    _mle_check(a, b, "mode6 gauss c1 " + name, 6, 1 / 500, orc, s, thr, MLE6)
 
 
-@pytest.mark.parametrize("lanes", ["1", "32"])
-def test_mle_astig_mode7_vs_oracle(lib, orc, lanes, monkeypatch):
-    monkeypatch.setenv("PTB_MLE_LANES", lanes)
+# The benchmark's own configuration: 1024 x 1024 frames with ~2700 emitters (overlaps), sigma 1.0-1.6 px,
+# background 10-80 as a cosine field, photons 300-8000; the FP32 path against the FP64 oracle on every candidate.
+C2_MLE6 = np.array([7.0, 1.3, 100.0, 2.0, 20.0, 0.0])
+
+
+@pytest.mark.parametrize("lanes,chunk", [("1", "1"), ("1", "4"), ("8", "1"), ("32", "1")])
+def test_mle_gauss_mode6_c2_vs_oracle(lib, orc, lanes, chunk, monkeypatch):
+    name = _mapping(monkeypatch, lanes, chunk)
+    s, thr = _synth("c2", 8, 1000, orc)
+    a = lib.localization(s, thr, 0.0, 6, C2_MLE6, capacity_doubles=8192 * 8 * 18)
+    b = _oracle_rows(orc, s, thr, 6, C2_MLE6, "c2-8", capacity_doubles=8192 * 8 * 18)
+    assert a.shape == b.shape and a.shape[0] > 15000
+    _mle_check(a, b, "mode6 gauss c2 " + name, 6, 1 / 1000, orc, s, thr, C2_MLE6,
+               other_optima=max(2, a.shape[0] // 5000))
+
+
+@pytest.mark.parametrize("lanes,chunk", MAPPINGS)
+def test_mle_astig_mode7_vs_oracle(lib, orc, lanes, chunk, monkeypatch):
+    name = _mapping(monkeypatch, lanes, chunk)
     s, thr = _synth("c3", 2, 33, orc)
     a = lib.localization(s, thr, 0.0, 7, MLE7)
-    b = orc.localization(s, thr, 0.0, 7, MLE7)
+    b = _oracle_rows(orc, s, thr, 7, MLE7, "c3-2")
     assert a.shape == b.shape
-    _mle_check(a, b, "mode7 astig c3 lanes=" + lanes, 7, 1 / 200, orc, s, thr, MLE7)
+    _mle_check(a, b, "mode7 astig c3 " + name, 7, 1 / 200, orc, s, thr, MLE7)
 
 
-@pytest.mark.parametrize("lanes", ["1", "32"])
-def test_mle_spline_mode8_vs_oracle(lib, orc, lanes, monkeypatch):
-    monkeypatch.setenv("PTB_MLE_LANES", lanes)
+@pytest.mark.parametrize("lanes,chunk", MAPPINGS)
+def test_mle_spline_mode8_vs_oracle(lib, orc, lanes, chunk, monkeypatch):
+    name = _mapping(monkeypatch, lanes, chunk)
     s, thr = _synth("c4", 2, 35, orc)
     p = _mle8_params()
     a = lib.localization(s, thr, 0.0, 8, p)
-    b = orc.localization(s, thr, 0.0, 8, p)
+    b = _oracle_rows(orc, s, thr, 8, p, "c4-2")
     assert a.shape == b.shape
-    _mle_check(a, b, "mode8 spline c4 lanes=" + lanes, 8, 1 / 200, orc, s, thr, p)
+    _mle_check(a, b, "mode8 spline c4 " + name, 8, 1 / 200, orc, s, thr, p)
+
+
+@pytest.mark.parametrize("lanes", ["1", "8", "32"])
+@pytest.mark.parametrize("model", [6, 7, 8])
+def test_mle_fp64_deviance_column(lib, orc, model, lanes, monkeypatch):
+    """The Theta column of modes 6-8 holds the FP64 Poisson deviance of each fit (its log-likelihood ratio against
+    the saturated model): equal to the oracle's FP64 deviance evaluated at the GPU's parameters, to 1e-9 relative."""
+    monkeypatch.setenv("PTB_MLE_LANES", lanes)
+    wl, frames, params = {6: ("c1", 3, MLE6), 7: ("c3", 1, MLE7), 8: ("c4", 1, None)}[model]
+    if params is None:
+        params = _mle8_params()
+    s, thr = _synth(wl, frames, 41, orc)
+    a = lib.localization(s, thr, 0.0, model, params)
+    ok = np.where(a[:, C_SX] >= 0)[0]
+    assert ok.size > 50
+    idx = ok[:: max(1, ok.size // 200)]
+    pairs = _deviances(orc, s, thr, model, params, a, a, idx)
+    got = a[idx, 10]
+    want = np.array([p[0] for p in pairs])
+    rel = np.abs(got - want) / np.maximum(np.abs(want), 1e-300)
+    assert np.all(np.isfinite(want)) and float(np.max(rel)) <= 1e-9, float(np.max(rel))
+    failed = a[:, C_SX] < 0
+    assert np.all(a[failed, 10] == -1)
 
 
 def test_mle_autotuned_matches_fixed(lib, orc):

@@ -1,5 +1,7 @@
 """Serving (PTB_ServerStart / PTB_SubmitStack / PTB_StackResult): every stack's result is the same when it runs in a
 mix of concurrent stacks of other shapes, lengths and fit modes as when it runs alone, and equals Localization's.
+The maximum-likelihood fits of concurrent requests are fused into shared launches; stacks wait for device memory
+when the budget admits only one at a time.
 
 The fit mapping is pinned (PTB_MLE_LANES=1) so that the autotuner of each slot cannot pick a different, equally
 valid mapping; with it the kernels are deterministic per ROI and the rows must match bit for bit.
@@ -29,8 +31,12 @@ def _mix(orc):
     return cases
 
 
-def test_served_mix_equals_alone(lib, orc, monkeypatch):
+@pytest.mark.parametrize("fuse", ["1", "0"])
+def test_served_mix_equals_alone(lib, orc, monkeypatch, fuse):
     monkeypatch.setenv("PTB_MLE_LANES", "1")
+    monkeypatch.setenv("PTB_FUSE_FITS", fuse)
+    # a long window: the fit stage waits for every busy slot's chunk, so concurrent requests are fused for sure
+    monkeypatch.setenv("PTB_FUSE_WINDOW_US", "200000")
     cases = _mix(orc)
     alone = [lib.localization(s, thr, 0.0, fit, p) for s, thr, fit, p in cases]
     server = lib.Server(slots=4, budget_bytes=8 << 30)
@@ -38,12 +44,19 @@ def test_served_mix_equals_alone(lib, orc, monkeypatch):
         # all at once: the stacks overlap on the device
         tickets = [server.submit(s, thr, 0.0, fit, p) for s, thr, fit, p in cases]
         mixed = [server.result(t) for t in tickets]
+        fused = server.fuse_stats()
         # one at a time through the server
         served_alone = []
         for s, thr, fit, p in cases:
             served_alone.append(server.result(server.submit(s, thr, 0.0, fit, p)))
     finally:
         server.stop()
+    print("fused fit launches", fused)
+    if fuse == "1":
+        # chunks of different requests (modes 6 and 7 separately) shared launches
+        assert fused["launches"] >= 1 and fused["chunks"] > fused["launches"], fused
+    else:
+        assert fused == {"launches": 0, "chunks": 0}
     for i, (ref, (m, q, lat), (a, _, _)) in enumerate(zip(alone, mixed, served_alone)):
         assert ref.shape[0] > 0 or cases[i][2] == 0
         assert m.shape == ref.shape and np.array_equal(m, ref), i
@@ -63,3 +76,25 @@ def test_server_reports_errors_and_restarts(lib):
         server.stop()
     server = lib.Server(slots=1)
     server.stop()
+
+
+def test_budget_admission_makes_stacks_wait(lib, orc, monkeypatch):
+    """A budget below one stack's estimate admits one stack at a time: every later stack waits in the queue until the
+    one before it has completed (all are submitted together)."""
+    import synth
+    monkeypatch.setenv("PTB_MLE_LANES", "1")
+    cases = []
+    for k in range(3):
+        st, _ = synth.stack("c1", frames=40, seed=700 + k)
+        cases.append((st, synth.mad_threshold(orc.planes(st[0])[1])))
+    server = lib.Server(slots=3, budget_bytes=1)
+    try:
+        tickets = [server.submit(st, thr, 0.0, 6, MLE6) for st, thr in cases]
+        res = [server.result(t) for t in tickets]
+    finally:
+        server.stop()
+    for i in range(1, len(res)):
+        (_, q_prev, lat_prev), (_, q, _) = res[i - 1], res[i]
+        assert q >= 0.9 * lat_prev, (i, q, lat_prev)
+    for (st, thr), (rows, _, _) in zip(cases, res):
+        assert np.array_equal(rows, lib.localization(st, thr, 0.0, 6, MLE6))

@@ -1,10 +1,12 @@
-"""The allocation-free fit entry point (PTB_FittingDeviceNoAlloc) against the regular Fitting export.
+"""The allocation-free fit entry point (PTB_FittingDeviceNoAlloc) against the regular Fitting export and the oracle.
 
 PTB_FittingDeviceNoAlloc serves callers that cannot allocate device memory themselves (for example code running
 inside another runtime's stream callbacks, or under a fixed pre-sized memory pool): they pass device buffers for the
 stack, the positions and the output, and the library works in a static device array instead of allocating. This file
 is collected last so that a failure here never hides the other tests; it passes alone and after them.
 """
+import json
+
 import numpy as np
 import pytest
 
@@ -12,21 +14,37 @@ from conftest import GAUSS_PARAMS
 
 pytestmark = pytest.mark.gpu
 
+ASTIG = [150.0, 400.0, 0.05, 0.0, 1.3 * 160, -150.0, 400.0, -0.05, 0.0, 1.3 * 160]
+MLE_PARAMS = {6: np.array([7.0, 1.3, 100.0, 2.0, 20.0, 0.0]),
+              7: np.array([11.0, 160.0] + ASTIG + [100.0, 2.0, 20.0, -600.0, 600.0, 0.0])}
+
 
 def _positions(rows):
     return np.ascontiguousarray(np.stack([rows[:, 0], rows[:, 1], rows[:, 4], rows[:, 5], rows[:, 15], rows[:, 16]], axis=1))
 
 
-def _call_noalloc(lib, torch, stack, pos, fit, params):
+def _device_inputs(torch, stack, pos):
     d_stack = torch.from_numpy(np.ascontiguousarray(stack).view(np.int16)).cuda()
     d_pos = torch.from_numpy(pos).cuda()
     d_out = torch.full((pos.shape[0] * 18,), -7.0, dtype=torch.float64, device="cuda")
+    return d_stack, d_pos, d_out
+
+
+def _call_noalloc(lib, torch, stack, pos, fit, params, inputs=None):
+    d_stack, d_pos, d_out = inputs or _device_inputs(torch, stack, pos)
     stream = torch.cuda.current_stream()
     n = lib.fitting_device_noalloc(d_stack.data_ptr(), d_pos.data_ptr(), pos.shape[0], d_out.data_ptr(), stack.shape, fit, params,
                                    stream.cuda_stream)
     torch.cuda.synchronize()
     assert n == pos.shape[0] * 18, lib.last_error()
     return d_out.cpu().numpy().reshape(-1, 18)
+
+
+def _same_as_fitting(got, expected):
+    assert got.shape == expected.shape
+    # same kernels on the same inputs: identical within the tests' tolerance (in practice bit for bit)
+    assert np.allclose(got, expected, rtol=1e-12, atol=1e-12, equal_nan=True)
+    assert np.array_equal(got[:, 2], expected[:, 2])  # per-plane Index column
 
 
 def test_no_alloc_fitting_matches_fitting_on_two_calls(lib, orc, stacks):
@@ -38,12 +56,73 @@ def test_no_alloc_fitting_matches_fitting_on_two_calls(lib, orc, stacks):
     pos_b[5, 1] = st.shape[0] + 4  # a plane outside the stack: border sentinel row, like Fitting
     # two calls in a row on the same static scratch: different sizes and modes; the second must not see the first
     for pos, fit in ((pos_a, 2), (pos_b, 4)):
-        expected = lib.fitting(st, pos, fit, GAUSS_PARAMS)
-        got = _call_noalloc(lib, torch, st, pos, fit, GAUSS_PARAMS)
-        assert got.shape == expected.shape
-        # same kernels on the same inputs: identical within the tests' tolerance (in practice bit for bit)
-        assert np.allclose(got, expected, rtol=1e-12, atol=1e-12, equal_nan=True)
-        assert np.array_equal(got[:, 2], expected[:, 2])  # per-plane Index column
+        _same_as_fitting(_call_noalloc(lib, torch, st, pos, fit, GAUSS_PARAMS), lib.fitting(st, pos, fit, GAUSS_PARAMS))
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("fit", [0, 1, 2, 3, 4])
+def test_no_alloc_gaussian_modes(lib, orc, stacks, fit, precision):
+    """Modes 0-4 at both fit precisions (FP32 iterations with FP64 re-fits use the scratch's flag array)."""
+    import torch
+    st = stacks["stack"]
+    pos = _positions(orc.localization(st, 103.6, 0.0, 0, GAUSS_PARAMS))
+    prev = lib.set_fit_precision(precision)
+    try:
+        for _ in range(2):
+            _same_as_fitting(_call_noalloc(lib, torch, st, pos, fit, GAUSS_PARAMS), lib.fitting(st, pos, fit, GAUSS_PARAMS))
+    finally:
+        lib.set_fit_precision(prev)
+
+
+def _mle_within_oracle(got, want, fit, other_optima):
+    """Fits that succeeded on both sides lie within the stated tolerances of the FP64 oracle (x, y 1e-3 px, photons
+    1e-4 relative), except at most `other_optima` fits that ended in another local optimum."""
+    ok = (got[:, 8] >= 0) & (want[:, 8] >= 0)
+    beyond = (np.abs(got[:, 4] - want[:, 4]) > 1e-3) | (np.abs(got[:, 5] - want[:, 5]) > 1e-3) | \
+             (np.abs(got[:, 7] - want[:, 7]) > 1e-4 * np.abs(want[:, 7]))
+    record = {"fit": fit, "fits": int(ok.sum()), "beyond": int((ok & beyond).sum()),
+              "flips": int(np.sum((got[:, 8] >= 0) != (want[:, 8] >= 0)))}
+    print(json.dumps(record))
+    assert ok.sum() > 0.9 * len(got), record
+    assert record["beyond"] <= other_optima and record["flips"] <= max(1, len(got) // 500), record
+
+
+@pytest.mark.parametrize("fit", [6, 7])
+def test_no_alloc_mle_modes_vs_fitting_and_oracle(lib, orc, fit):
+    """MLE modes: the entry point's rows equal the Fitting export's, call after call, and lie within tolerance of
+    the FP64 oracle. Mode 6 runs on 4 benchmark-statistics 1024 x 1024 frames (more than 9472 points, where both
+    entry points switch to a thread per ROI), mode 7 on 2 astigmatic 512 x 512 frames."""
+    import torch
+    import synth
+    wl, frames = ("c2", 4) if fit == 6 else ("c3", 2)
+    s, _ = synth.stack(wl, frames=frames, seed=77)
+    thr = synth.mad_threshold(orc.planes(s[0])[1])
+    pos = _positions(orc.localization(s, thr, 0.0, 0, GAUSS_PARAMS))
+    if fit == 6:
+        assert pos.shape[0] > 148 * 64
+    params = MLE_PARAMS[fit]
+    expected = lib.fitting(s, pos, fit, params)
+    inputs = _device_inputs(torch, s, pos)
+    for _ in range(2):
+        _same_as_fitting(_call_noalloc(lib, torch, s, pos, fit, params, inputs), expected)
+    _mle_within_oracle(expected, orc.fitting(s, pos, fit, params), fit, other_optima=max(2, pos.shape[0] // 5000))
+
+
+@pytest.mark.parametrize("fit", [2, 6])
+def test_no_alloc_call_allocates_nothing(lib, orc, stacks, fit):
+    """A warmed-up call leaves the device's free memory unchanged (no cudaMalloc, no pool growth)."""
+    import torch
+    st = stacks["stack"]
+    pos = _positions(orc.localization(st, 103.6, 0.0, 0, GAUSS_PARAMS))
+    params = GAUSS_PARAMS if fit == 2 else MLE_PARAMS[6]
+    inputs = _device_inputs(torch, st, pos)
+    _call_noalloc(lib, torch, st, pos, fit, params, inputs)  # loads the kernels' code, looks up the scratch address
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        _call_noalloc(lib, torch, st, pos, fit, params, inputs)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
 
 
 def test_no_alloc_rejects_oversized_calls(lib, stacks):
@@ -57,3 +136,7 @@ def test_no_alloc_rejects_oversized_calls(lib, stacks):
     d_out = torch.zeros(n * 18, dtype=torch.float64, device="cuda")
     got = lib.fitting_device_noalloc(d_stack.data_ptr(), d_pos.data_ptr(), n, d_out.data_ptr(), st.shape, 2, GAUSS_PARAMS)
     assert got == 0 and "65536" in lib.last_error()
+    # dimensions whose product would wrap in 64 bits are rejected before anything runs
+    got = lib.fitting_device_noalloc(d_stack.data_ptr(), d_pos.data_ptr(), 1, d_out.data_ptr(), (1, 1 << 33, 1 << 33), 2,
+                                     GAUSS_PARAMS)
+    assert got == 0 and "dimensions" in lib.last_error()
