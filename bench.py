@@ -282,6 +282,7 @@ def serving_run(ptb, torch, n_req, seed=2026):
     torch.cuda.empty_cache()
     fit_of = {0: (6, PARAMS_BY_MODE[6]), 1: (7, MLE7_PARAMS)}
     server = ptb.Server(slots=SERVE_SLOTS)
+    fused = None
 
     def submit(i):
         _, arr, thr = base[(int(sizes[i]), int(kinds[i]))]
@@ -312,8 +313,24 @@ def serving_run(ptb, torch, n_req, seed=2026):
         t0 = time.perf_counter()
         rows_sat, lat_sat = collect([submit(i) for i in range(n_req)])
         sat_s = time.perf_counter() - t0
+        fused = server.fuse_stats()
     finally:
         server.stop()
+    # the same saturated run with every slot fitting its own chunks (no fused launches), for comparison
+    os.environ["PTB_FUSE_FITS"] = "0"
+    try:
+        server = ptb.Server(slots=SERVE_SLOTS)
+        try:
+            for kind in (0, 1):
+                i = int(np.argmin(np.where(kinds == kind, sizes * lengths, 1 << 40)))
+                collect([submit(i)])
+            t0 = time.perf_counter()
+            rows_unf, lat_unf = collect([submit(i) for i in range(n_req)])
+            unf_s = time.perf_counter() - t0
+        finally:
+            server.stop()
+    finally:
+        del os.environ["PTB_FUSE_FITS"]
     # plain form: one Localization call per frame, on the first frames of the same requests (bounded sample)
     plain_rows, plain_frames, plain_lat, t_start = 0, 0, [], time.perf_counter()
     for i in range(n_req):
@@ -340,7 +357,10 @@ def serving_run(ptb, torch, n_req, seed=2026):
                     "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))}},
         "saturated": {"localizations_per_s": rows_sat / sat_s, "frames_per_s": frames_total / sat_s, "seconds": sat_s,
                       "h2d_gbs": in_bytes / sat_s / 1e9,
-                      "latency_ms": {"p50": float(np.percentile(lat_sat, 50)), "p99": float(np.percentile(lat_sat, 99))}},
+                      "latency_ms": {"p50": float(np.percentile(lat_sat, 50)), "p99": float(np.percentile(lat_sat, 99))},
+                      "fused_fit_launches": fused},
+        "saturated_unfused": {"localizations_per_s": rows_unf / unf_s, "seconds": unf_s,
+                              "latency_ms": {"p50": float(np.percentile(lat_unf, 50)), "p99": float(np.percentile(lat_unf, 99))}},
         "plain_per_frame": {"localizations_per_s": plain_rows / plain_s, "frames_per_s": plain_frames / plain_s,
                             "sample_frames": plain_frames,
                             "call_latency_ms": {"p50": float(np.percentile(plain_lat, 50)), "p99": float(np.percentile(plain_lat, 99))}},
