@@ -126,7 +126,14 @@ static_assert(kRows2 * kPV <= kRows1 * kP1, "C2 must fit in the C1 space");
 static_assert(kInRows * kInW * 2 <= kRows1 * kPV * 4, "the staged input must fit in the V1 space");
 static_assert(kP1 + 1 <= kInW, "C1 columns read staged columns 1 .. kP1");
 static_assert(kRows2 <= 36, "pass C covers C2 rows in three runs of 12");
-static_assert(TY * 16 <= 2 * kThreads, "pass E: two tasks of 8 pixels per thread");
+constexpr int kRunA = 13, kRunsA = (kRows1 + kRunA - 1) / kRunA;  // pass A: rows per run, runs per column
+constexpr int kTasksD = (TX + 2 + 3) / 4;                          // pass D: 4-column tasks per ring row
+constexpr int kTasksE = (TY * (TX / 4) + kThreads - 1) / kThreads;  // pass E: 4-pixel tasks per thread
+static_assert(kPV % 4 == 0 && kP1 % 4 == 0, "16-byte rows");
+static_assert(4 * (kPV / 4 - 1) + 7 < kP1, "pass B reads C1 columns 4m .. 4m + 7");
+static_assert(4 * (kTasksD - 1) + 11 < kPV && 4 * (kTasksD - 1) + 7 < kPV, "pass D stays inside C2 and V1 rows");
+static_assert(4 * 31 + 11 < kPV, "pass E reads ring columns 4m .. 4m + 7");
+static_assert(TX / 4 == 32 && kTasksE * 4 <= 32, "pass E: one warp per tile row, 4 bits per task in a mask");
 
 __device__ __forceinline__ uint32_t Tap(uint32_t m2, uint32_t m1, uint32_t c, uint32_t p1, uint32_t p2)
 {
@@ -170,33 +177,35 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 		}
 	}
 	__syncthreads();
-	// A: C1, one lane per column (C1 column i = staged column i + 1)
-	for (int i = tid; i < kP1; i += kThreads) {
+	// A: C1, one lane per column and run of rows (C1 column i = staged column i + 1); the three runs of a column
+	// spread the 152 columns' work over all the block's threads
+	for (int task = tid; task < kP1 * kRunsA; task += kThreads) {
+		const int q = task / kP1, i = task - q * kP1;
+		const int r0 = q * kRunA, r1 = min(kRows1, r0 + kRunA);
 		const uint16_t* col = in + i + 1;
-		uint32_t w0 = col[0], w1 = col[kInW], w2 = col[2 * kInW], w3 = col[3 * kInW];
-		#pragma unroll 6
-		for (int r = 0; r < kRows1; ++r) {
+		uint32_t w0 = col[r0 * kInW], w1 = col[(r0 + 1) * kInW], w2 = col[(r0 + 2) * kInW], w3 = col[(r0 + 3) * kInW];
+		#pragma unroll 4
+		for (int r = r0; r < r1; ++r) {
 			const uint32_t w4 = col[(r + 4) * kInW];
 			c1[r * kP1 + i] = Tap(w0, w1, w2, w3, w4);
 			w0 = w1; w1 = w2; w2 = w3; w3 = w4;
 		}
-		const int rlo = max(0, 5 - y0), rhi = min(kRows1 - 1, H - 1 - y0 + 5);
-		for (int r = 0; r < rlo; ++r) { c1[r * kP1 + i] = c1[rlo * kP1 + i]; }
-		for (int r = rhi + 1; r < kRows1; ++r) { c1[r * kP1 + i] = c1[rhi * kP1 + i]; }
 	}
 	__syncthreads();
-	// B: V1, 8 columns per task
-	for (int task = tid; task < kRows1 * 18; task += kThreads) {
-		const int r = task / 18, m = task - r * 18;
-		const uint4* src = reinterpret_cast<const uint4*>(c1 + r * kP1 + 8 * m);
-		const uint4 a = src[0], b = src[1], c = src[2];
-		const uint32_t v[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
-		uint32_t o[8];
-		#pragma unroll
-		for (int k = 0; k < 8; ++k) { o[k] = Tap(v[k], v[k + 1], v[k + 2], v[k + 3], v[k + 4]); }
-		uint4* dst = reinterpret_cast<uint4*>(v1 + r * kPV + 8 * m);
-		dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
-		dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+	// B: V1, 4 columns per task from two 16-byte loads (consecutive tasks read and write consecutive 16-byte words,
+	// so no two lanes of a quarter warp share a bank). C1 rows outside the frame are read at the nearest in-frame row:
+	// the edge replication of the vertical pass.
+	{
+		const int rlo = max(0, 5 - y0), rhi = min(kRows1 - 1, H - 1 - y0 + 5);
+		for (int task = tid; task < kRows1 * (kPV / 4); task += kThreads) {
+			const int r = task / (kPV / 4), m = task - r * (kPV / 4);
+			const int rs = min(max(r, rlo), rhi);
+			const uint4* src = reinterpret_cast<const uint4*>(c1 + rs * kP1 + 4 * m);
+			const uint4 a = src[0], b = src[1];
+			const uint4 o = make_uint4(Tap(a.x, a.y, a.z, a.w, b.x), Tap(a.y, a.z, a.w, b.x, b.y), Tap(a.z, a.w, b.x, b.y, b.z),
+			                           Tap(a.w, b.x, b.y, b.z, b.w));
+			*reinterpret_cast<uint4*>(v1 + r * kPV + 4 * m) = o;
+		}
 	}
 	__syncthreads();
 	{
@@ -223,73 +232,73 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 		}
 	}
 	__syncthreads();
-	// D: W1 on the ring, in place of V1
-	for (int task = tid; task < kRows2 * 17; task += kThreads) {
-		const int q = task / 17, m = task - q * 17;
-		const uint4* src = reinterpret_cast<const uint4*>(c2 + q * kPV + 8 * m);
-		const uint4 a = src[0], b = src[1], c = src[2], d = src[3];
-		const uint32_t u[16] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w};
-		uint4* vp = reinterpret_cast<uint4*>(v1 + (q + 4) * kPV + 8 * m + 4);
-		const uint4 e = vp[0], g = vp[1];
-		const uint32_t v[8] = {e.x, e.y, e.z, e.w, g.x, g.y, g.z, g.w};
-		const int y = y0 + q - 1, xs = x0 + 8 * m - 1;
+	// D: W1 on the ring, in place of V1, 4 ring columns per task (three 16-byte loads of C2, one of V1, one store;
+	// consecutive tasks on consecutive 16-byte words)
+	for (int task = tid; task < kRows2 * kTasksD; task += kThreads) {
+		const int q = task / kTasksD, m = task - q * kTasksD;
+		const uint4* src = reinterpret_cast<const uint4*>(c2 + q * kPV + 4 * m);
+		const uint4 a = src[0], b = src[1], c = src[2];
+		const uint32_t u[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+		uint4* vp = reinterpret_cast<uint4*>(v1 + (q + 4) * kPV + 4 * m + 4);
+		const uint4 e = *vp;
+		const uint32_t v[4] = {e.x, e.y, e.z, e.w};
+		const int y = y0 + q - 1, xs = x0 + 4 * m - 1;
 		const bool rowIn = y >= 0 && y < H;
-		uint32_t o[8];
-		if (rowIn && xs >= 0 && xs + 8 <= W) {
-			// all eight inside the frame: max(W1, 0) = max(V1 * 256, V2) - V2
+		uint32_t o[4];
+		if (rowIn && xs >= 0 && xs + 4 <= W) {
+			// all four inside the frame: max(W1, 0) = max(V1 * 256, V2) - V2
 			#pragma unroll
-			for (int k = 0; k < 8; ++k) {
+			for (int k = 0; k < 4; ++k) {
 				const uint32_t v2 = Tap(u[k], u[k + 2], u[k + 4], u[k + 6], u[k + 8]);
 				o[k] = max(v[k] << 8, v2) - v2;
 			}
 		}
 		else {
 			#pragma unroll
-			for (int k = 0; k < 8; ++k) {
+			for (int k = 0; k < 4; ++k) {
 				const uint32_t v2 = Tap(u[k], u[k + 2], u[k + 4], u[k + 6], u[k + 8]);
 				const uint32_t v1s = v[k] << 8;
 				const int x = xs + k;
 				o[k] = (rowIn && x >= 0 && x < W && v1s > v2) ? v1s - v2 : 0u;
 			}
 		}
-		vp[0] = make_uint4(o[0], o[1], o[2], o[3]);
-		vp[1] = make_uint4(o[4], o[5], o[6], o[7]);
+		*vp = make_uint4(o[0], o[1], o[2], o[3]);
 	}
 	__syncthreads();
-	// E: domain and seeds, 8 pixels per task, two tasks per thread
+	// E: domain and seeds, 4 pixels per task (a warp covers one tile row: consecutive 16-byte loads), up to four
+	// tasks per thread; the masks of the thread's tasks are packed 4 bits per task
 	const uint32_t thr = thrFixed <= 0 ? 0u : (thrFixed >= 0xffffffffll ? 0xffffffffu : static_cast<uint32_t>(thrFixed));
-	uint32_t dmask[2] = {0, 0}, smask[2] = {0, 0};
+	uint32_t dmask = 0, smask = 0;
 	#pragma unroll
-	for (int h = 0; h < 2; ++h) {
+	for (int h = 0; h < kTasksE; ++h) {
 		const int task = tid + h * kThreads;
-		const int ty = task >> 4, m = task & 15;
-		if (ty >= TY) { continue; }  // 16 tasks per tile row; the last thread slots have none
-		uint32_t a[3][12];
+		const int ty = task >> 5, m = task & 31;
+		if (ty >= TY) { continue; }  // 32 tasks per tile row; the last thread slots have none
+		uint32_t a[3][8];
 		#pragma unroll
 		for (int rr = 0; rr < 3; ++rr) {
-			const uint4* src = reinterpret_cast<const uint4*>(v1 + (ty + 4 + rr) * kPV + 8 * m + 4);
-			const uint4 p = src[0], q = src[1], r = src[2];
+			const uint4* src = reinterpret_cast<const uint4*>(v1 + (ty + 4 + rr) * kPV + 4 * m + 4);
+			const uint4 p = src[0], q = src[1];
 			a[rr][0] = p.x; a[rr][1] = p.y; a[rr][2] = p.z; a[rr][3] = p.w;
 			a[rr][4] = q.x; a[rr][5] = q.y; a[rr][6] = q.z; a[rr][7] = q.w;
-			a[rr][8] = r.x; a[rr][9] = r.y; a[rr][10] = r.z; a[rr][11] = r.w;
 		}
 		// 3 x 3 maximum as column maxima, then the maximum of three of them; a seed is not below the maximum of its
 		// window, which holds the pixel itself, so this equals "no neighbour strictly greater"
-		uint32_t cm[10];
+		uint32_t cm[6];
 		#pragma unroll
-		for (int j = 0; j < 10; ++j) { cm[j] = __vimax3_u32(a[0][j], a[1][j], a[2][j]); }
-		const int inFrame = y0 + ty < H ? W - (x0 + 8 * m) : 0;  // pixels k < inFrame lie inside the frame
+		for (int j = 0; j < 6; ++j) { cm[j] = __vimax3_u32(a[0][j], a[1][j], a[2][j]); }
+		const int inFrame = y0 + ty < H ? W - (x0 + 4 * m) : 0;  // pixels k < inFrame lie inside the frame
 		#pragma unroll
-		for (int k = 0; k < 8; ++k) {
+		for (int k = 0; k < 4; ++k) {
 			const uint32_t v = a[1][k + 1];
 			const bool dom = k < inFrame && v > thr;
-			dmask[h] |= static_cast<uint32_t>(dom) << k;
-			smask[h] |= static_cast<uint32_t>(dom && v >= __vimax3_u32(cm[k], cm[k + 1], cm[k + 2])) << k;
+			dmask |= static_cast<uint32_t>(dom) << (4 * h + k);
+			smask |= static_cast<uint32_t>(dom && v >= __vimax3_u32(cm[k], cm[k + 1], cm[k + 2])) << (4 * h + k);
 		}
 	}
 	// block-wide positions in the domain and seed lists: one atomic per list
 	const int lane = tid & 31, warp = tid >> 5;
-	const uint32_t nd = __popc(dmask[0]) + __popc(dmask[1]), ns = __popc(smask[0]) + __popc(smask[1]);
+	const uint32_t nd = __popc(dmask), ns = __popc(smask);
 	uint32_t id = nd, is = ns;
 	#pragma unroll
 	for (int d = 1; d < 32; d <<= 1) {
@@ -315,22 +324,21 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 	uint32_t pd = scanSm[2 * kWarps] + scanSm[warp] + id - nd;
 	uint32_t ps = scanSm[2 * kWarps + 1] + scanSm[kWarps + warp] + is - ns;
 	#pragma unroll
-	for (int h = 0; h < 2; ++h) {
+	for (int h = 0; h < kTasksE; ++h) {
 		const int task = tid + h * kThreads;
-		const int ty = task >> 4, m = task & 15;
-		const int y = y0 + ty, xb = x0 + 8 * m;
+		const int ty = task >> 5, m = task & 31;
+		const int y = y0 + ty, xb = x0 + 4 * m;
 		if (ty >= TY || y >= H || xb >= W) { continue; }
 		const long long g = static_cast<long long>(f) * ws.g.N + static_cast<long long>(y) * W + xb;
-		// code bytes of the eight pixels: each mask bit spread to the low bit of its byte, times the flag
-		const uint32_t dm = dmask[h], sm = smask[h];
-		const uint32_t lo = Spread4(dm & 15u) * kDomain | Spread4(sm & 15u) * kSeed;
-		const uint32_t hi = Spread4(dm >> 4) * kDomain | Spread4(sm >> 4) * kSeed;
-		if (xb + 8 <= W && (g & 7) == 0) { *reinterpret_cast<uint2*>(ws.code + g) = make_uint2(lo, hi); }
+		// code bytes of the four pixels: each mask bit spread to the low bit of its byte, times the flag
+		const uint32_t dm = (dmask >> (4 * h)) & 15u, sm = (smask >> (4 * h)) & 15u;
+		const uint32_t bytes = Spread4(dm) * kDomain | Spread4(sm) * kSeed;
+		if (xb + 4 <= W && (g & 3) == 0) { *reinterpret_cast<uint32_t*>(ws.code + g) = bytes; }
 		else {
-			for (int k = 0; k < 8 && xb + k < W; ++k) { ws.code[g + k] = static_cast<uint8_t>((k < 4 ? lo >> (8 * k) : hi >> (8 * k - 32))); }
+			for (int k = 0; k < 4 && xb + k < W; ++k) { ws.code[g + k] = static_cast<uint8_t>(bytes >> (8 * k)); }
 		}
 		// domain pixels (their W1 is still in shared memory) and seeds, lowest pixel first
-		const uint32_t* w1row = v1 + (ty + 5) * kPV + 8 * m + 5;
+		const uint32_t* w1row = v1 + (ty + 5) * kPV + 4 * m + 5;
 		for (uint32_t b = dm; b; b &= b - 1u) {
 			const int k = __ffs(b) - 1;
 			ws.w1[g + k] = static_cast<long long>(w1row[k]);
