@@ -10,7 +10,7 @@
 //   V1 = sum h' * T1          (units 1/256, < 2^24)
 //   T2 = sum h' * V1 at +-2,4 (units 2^-12, < 2^28)
 //   V2 = sum h' * T2          (units 2^-16, < 2^32, fits uint32)
-//   W1 = V1 * 256 - V2        (units 2^-16, |W1| < 2^32, int64)
+//   W1 = V1 * 256 - V2        (units 2^-16, |W1| < 2^32; kept as max(W1, 0) in uint32)
 // with h' = {1, 4, 6, 4, 1}. Each pass evaluates its output at the CLAMPED coordinate, exactly like the reference's
 // offsetTest() clamping of every neighbour access, so border tiles need no special case. The strict threshold
 // W1 > thr is evaluated as W1_fixed > floor(thr * 2^16), which is the same test for an integer W1_fixed.
@@ -106,16 +106,19 @@ __device__ __forceinline__ long long W1At(const TileSmem& s, int r, int c)
 // slower for 2 % less halo work). Borders: every intermediate array is kept edge-replicated
 // (an entry whose coordinate lies outside the frame holds the value of the nearest in-frame entry), which is what
 // the reference's clamping of every neighbour access amounts to, so no pass clamps an index:
-//   A  C1 = vertical level-1 taps of the input, one lane per column sliding down 42 clamped input rows (rows outside
-//      the frame are then replicated);   tile rows [-5, 33), cols [-7, 145)
-//   B  V1 = horizontal level-1 taps of C1, 8 columns per task from 3 vector loads (columns outside the frame are
-//      then replicated);                 tile rows [-5, 33), cols [-5, 139)
+//   A  C1 = vertical level-1 taps of the input, one lane per column and run of 13 rows sliding down the clamped
+//      input rows;                       tile rows [-5, 33), cols [-7, 145)
+//   B  V1 = horizontal level-1 taps of C1, 4 columns per task from 2 vector loads, each C1 row outside the frame
+//      read at the nearest in-frame row (columns outside the frame are then replicated);
+//                                        tile rows [-5, 33), cols [-5, 139)
 //   C  C2 = vertical level-2 taps (rows +-2, +-4) of V1, one lane per column and 12-row run;   rows [-1, 29)
-//   D  W1 = V1 * 256 - V2 on the ring (tile +-1), V2 = horizontal level-2 taps of C2, 8 columns per task, stored
+//   D  W1 = V1 * 256 - V2 on the ring (tile +-1), V2 = horizontal level-2 taps of C2, 4 columns per task, stored
 //      in place of V1 as max(W1, 0) (W1 < 2^32; a non-positive W1 can neither be in the domain nor dominate a
 //      domain pixel) and 0 outside the frame (the reference skips neighbours outside the frame);
-//   E  threshold and 3 x 3 maximum for 8 pixels per task; code bytes, W1 of domain pixels, and the domain and seed
-//      lists with one atomic per block and list.
+//   E  threshold and 3 x 3 maximum for 4 pixels per task; code bytes, W1 of domain pixels (uint32), and the domain
+//      and seed lists with one atomic per block and list.
+// In passes B, D and E consecutive lanes read and write consecutive 16-byte words, so no two lanes of a quarter
+// warp share a shared-memory bank.
 constexpr int kP1 = 152;  // C1 pitch (tile col = index - 7); C2 (pitch kPV, tile col = index - 5) reuses its space
 constexpr int kPV = 144;  // V1 pitch (tile col = index - 5, tile row = index - 5); W1 ring in place
 constexpr int kRows1 = TY + 10;  // C1 and V1 rows
@@ -341,7 +344,7 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 		const uint32_t* w1row = v1 + (ty + 5) * kPV + 4 * m + 5;
 		for (uint32_t b = dm; b; b &= b - 1u) {
 			const int k = __ffs(b) - 1;
-			ws.w1[g + k] = static_cast<long long>(w1row[k]);
+			ws.w1[g + k] = w1row[k];
 			if (pd < ws.capDom) { ws.dom[pd] = static_cast<uint32_t>(g + k); }
 			else { atomicExch(&ws.cnt->overflow, 1u); }
 			++pd;

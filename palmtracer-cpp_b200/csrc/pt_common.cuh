@@ -164,7 +164,7 @@ struct Workspace {
 	// dense
 	const uint16_t* img;  // the chunk's frames (device)
 	uint8_t* code;
-	long long* w1;        // W1 in 2^-16 units, valid on domain pixels only
+	uint32_t* w1;         // W1 in 2^-16 units, valid on domain pixels only (there 0 < W1 < 2^32)
 	uint32_t* par;        // union-find parent, then component id tag at roots; once the groups are scattered, the
 	                      // parent-chain minimum of W1 of each pixel a global-memory flood pushes (its exactness check)
 	uint32_t* lab;        // region id + 1 on labelled domain pixels

@@ -589,7 +589,7 @@ struct GlobalView {
 	__device__ __forceinline__ uint32_t Lab(uint32_t p, int, int) const { return ws.lab[p]; }
 	__device__ __forceinline__ void SetLab(uint32_t p, int, int, uint32_t v) const { ws.lab[p] = v; }
 	__device__ __forceinline__ double W1(uint32_t p, int, int) const { return static_cast<double>(__ldg(ws.w1 + p)); }
-	__device__ __forceinline__ uint32_t W1Fixed(uint32_t p, int, int) const { return static_cast<uint32_t>(__ldg(ws.w1 + p)); }
+	__device__ __forceinline__ uint32_t W1Fixed(uint32_t p, int, int) const { return __ldg(ws.w1 + p); }
 	// parent-chain minimum of W1 (kNoChain on the flood's seeds), kept in par once the groups are scattered
 	__device__ __forceinline__ uint32_t Chain(uint32_t p, int, int) const { return ws.par[p]; }
 	__device__ __forceinline__ void SetChain(uint32_t p, int, int, uint32_t v) const { ws.par[p] = v; }
@@ -653,7 +653,7 @@ __device__ bool PixelExactGlobal(const Workspace& ws, uint32_t p, uint32_t T)
 			if ((dx == 0 && dy == 0) || xx < 0 || xx >= ws.g.W) { continue; }
 			const uint32_t nb = p + static_cast<uint32_t>(dy * ws.g.W + dx);
 			if (!(__ldg(ws.code + nb) & kDomain) || ws.lab[nb] == L) { continue; }
-			if (!PairExact(chain, static_cast<uint32_t>(__ldg(ws.w1 + nb)), T)) { return false; }
+			if (!PairExact(chain, __ldg(ws.w1 + nb), T)) { return false; }
 		}
 	}
 	return true;
@@ -802,7 +802,7 @@ __global__ void __launch_bounds__(kBoxWarps * 32) GroupFloodBox(Workspace ws)
 			const uint32_t p = base + static_cast<uint32_t>(r * geo.W + c);
 			const bool dom = (__ldg(ws.code + p) & kDomain) != 0;
 			const uint32_t lb = dom ? ws.lab[p] : 0u;
-			sm.w1[i] = dom ? static_cast<uint32_t>(__ldg(ws.w1 + p)) : 0u;
+			sm.w1[i] = dom ? __ldg(ws.w1 + p) : 0u;
 			sm.lab[i] = lb;
 			sm.chain[i] = kNoChain;
 			sm.flag[i] = static_cast<uint8_t>((dom ? 1u : 0u) | (dom && lb == 0 ? 2u : 0u));
