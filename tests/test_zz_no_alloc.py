@@ -74,17 +74,31 @@ def test_no_alloc_gaussian_modes(lib, orc, stacks, fit, precision):
         lib.set_fit_precision(prev)
 
 
-def _mle_within_oracle(got, want, fit, other_optima):
+def _deviance(orc, stack, pos, row, fit, params):
+    """FP64 deviance (the oracle's objective) of an output row's parameters, for the fit at caller position pos."""
+    frame = stack[int(pos[1]) - 1]
+    ux, uy = np.floor(pos[2]), np.floor(pos[3])
+    s = row[8] if fit == 6 else row[6]
+    r = orc.mle_evaluate(frame, pos[2], pos[3], fit, params, np.array([row[14], row[7], row[4] - ux, row[5] - uy, s]))
+    return np.inf if r is None else r[0]
+
+
+def _mle_within_oracle(orc, stack, pos, got, want, fit, params):
     """Fits that succeeded on both sides lie within the stated tolerances of the FP64 oracle (x, y 1e-3 px, photons
-    1e-4 relative), except at most `other_optima` fits that ended in another local optimum."""
+    1e-4 relative), except fits that ended in another local optimum of the deviance: at most 1 in 1000 (and 2) may
+    be less likely than the oracle's optimum; those at least as likely are counted. Status flips: 1 in 500."""
     ok = (got[:, 8] >= 0) & (want[:, 8] >= 0)
-    beyond = (np.abs(got[:, 4] - want[:, 4]) > 1e-3) | (np.abs(got[:, 5] - want[:, 5]) > 1e-3) | \
-             (np.abs(got[:, 7] - want[:, 7]) > 1e-4 * np.abs(want[:, 7]))
-    record = {"fit": fit, "fits": int(ok.sum()), "beyond": int((ok & beyond).sum()),
+    beyond = ok & ((np.abs(got[:, 4] - want[:, 4]) > 1e-3) | (np.abs(got[:, 5] - want[:, 5]) > 1e-3) |
+                   (np.abs(got[:, 7] - want[:, 7]) > 1e-4 * np.abs(want[:, 7])))
+    worse = 0
+    for i in np.where(beyond)[0]:
+        dg, do = _deviance(orc, stack, pos[i], got[i], fit, params), _deviance(orc, stack, pos[i], want[i], fit, params)
+        worse += int(dg > do + 1e-6 * max(1.0, abs(do)))
+    record = {"fit": fit, "fits": int(ok.sum()), "beyond": int(beyond.sum()), "other_optimum_gpu_worse": worse,
               "flips": int(np.sum((got[:, 8] >= 0) != (want[:, 8] >= 0)))}
     print(json.dumps(record))
     assert ok.sum() > 0.9 * len(got), record
-    assert record["beyond"] <= other_optima and record["flips"] <= max(1, len(got) // 500), record
+    assert worse <= max(2, len(got) // 1000) and record["flips"] <= max(1, len(got) // 500), record
 
 
 @pytest.mark.parametrize("fit", [6, 7])
@@ -105,7 +119,7 @@ def test_no_alloc_mle_modes_vs_fitting_and_oracle(lib, orc, fit):
     inputs = _device_inputs(torch, s, pos)
     for _ in range(2):
         _same_as_fitting(_call_noalloc(lib, torch, s, pos, fit, params, inputs), expected)
-    _mle_within_oracle(expected, orc.fitting(s, pos, fit, params), fit, other_optima=max(2, pos.shape[0] // 5000))
+    _mle_within_oracle(orc, s, pos, expected, orc.fitting(s, pos, fit, params), fit, params)
 
 
 @pytest.mark.parametrize("fit", [2, 6])
