@@ -608,6 +608,9 @@ def main():
     else:
         rows_all = float(rows)
     value = rows_all * args.steps / (total_ms / 1000.0)
+    # the ROI mapping the autotuner chose for the timed steps (lanes per ROI 1: a thread per ROI; 32: a warp)
+    mapping = [m for m in ptb.mle_mappings() if m["mode"] == FIT_MODE]
+    lanes_txt = ", ".join(sorted({"%d lanes, chunk %d" % (m["lanes"], m["chunk"]) for m in mapping})) or "not tuned"
 
     # stage breakdown of one more (untimed) pass, with the MLE phases timed by CUDA events on the library's stream
     ptb.set_profiling(1)
@@ -636,7 +639,8 @@ def main():
         lm_ms = stages["fit_lm"][0]
         flops = FLOP_PER_PIXEL_LM * 49 * evals["lm"]
         achieved = flops / (lm_ms / 1000.0) / 1e12
-        fit_roofline = {"kernel": "MleLmKernel<6> (persistent FP32 LM, thread per ROI)", "bound": "fp32", "achieved": achieved,
+        fit_roofline = {"kernel": "MleLmKernel<6> (persistent FP32 LM; ROI mapping %s)" % lanes_txt, "bound": "fp32",
+                    "achieved": achieved,
                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                     "traffic": LM_DRAM_BYTES_PER_FRAME * frames / max(1, stages["fit_lm"][1]),
                     "traffic_unit": "bytes per launch (ncu, scaled)",
@@ -741,7 +745,7 @@ def main():
                 "dtype": ("f32 (axial pre-scan, LM and Newton polish; f64 Cholesky fallback, Fisher information, CRLB)" if FIT_MODE >= 6 else
                           "f64" if args.precision != 1 else "f32 (f64 re-fit)"),
                 "data": "synthetic (seeded, generated on the GPU; no public dataset)",
-                "config": config, "fit_precision": args.precision,
+                "config": config, "fit_precision": args.precision, "mle_mapping": mapping,
                 "frames_per_s": frames * world * args.steps / (total_ms / 1000.0),
                 "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
                 "localizations_per_step": int(rows_all), "roofline": roofline, "fit_roofline": fit_roofline,

@@ -182,6 +182,11 @@ PTB_API void PTB_SegmentationStats(uint64_t* counts, int n);
  * the same time (up to n entries). */
 PTB_API void PTB_EnginePoolStats(uint64_t* counts, int n);
 
+/* ROI mappings the autotuner chose for the maximum-likelihood modes 6-8 on the current device's engines
+ * (diagnostics): up to n entries of 5 ints (mode, ROI size, chunk size class, lanes per ROI, work-queue chunk), one
+ * per engine and tuned class. Returns the entries written. */
+PTB_API int PTB_MleMappings(int* entries, int n);
+
 /* Fit arithmetic for the Gaussian least-squares modes 1-4. 0 (default): FP64, one thread per ROI, in the
  * reference's exact order of operations (same iteration path as the reference); 1: FP32 iterations, one warp per
  * ROI, with an FP64 re-fit of every ROI whose FP32 run did not stop cleanly; 2: FP64, one warp per ROI.

@@ -409,4 +409,15 @@ PTB_API void PTB_SegmentationStats(uint64_t* counts, int n)
 
 PTB_API void PTB_EnginePoolStats(uint64_t* counts, int n) { ptb::PoolStats(counts, n); }
 
+PTB_API int PTB_MleMappings(int* entries, int n)
+{
+	int written = 0;
+	for (int i = 0; written < n; ++i) {
+		ptb::EngineLease lease(i);
+		if (!lease) { break; }
+		written += lease->TunedMappings(entries + 5 * written, n - written, 0);
+	}
+	return written;
+}
+
 }  // extern "C"

@@ -840,6 +840,21 @@ bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slo
 	return true;
 }
 
+int Engine::TunedMappings(int* out, int n, int skip) const
+{
+	int k = 0;
+	for (int i = skip; i < static_cast<int>(tuned_.size()) && k < n; ++i, ++k) {
+		const int key = tuned_[i].key;
+		int* e = out + 5 * k;
+		e[0] = key / (64 * 64);
+		e[1] = (key / 64) % 64;
+		e[2] = key % 64;
+		e[3] = tuned_[i].lanes;
+		e[4] = tuned_[i].chunk;
+	}
+	return k;
+}
+
 void Engine::GraphStats(uint64_t* out, int n)
 {
 	for (int k = 0; k < 3 && k < n; ++k) {

@@ -85,6 +85,9 @@ public:
 	void GraphStats(uint64_t* out, int n);
 	// [frames segmented, frames flooded again frame-wide after failing the exactness test] since the last call.
 	void SegmentationStats(uint64_t* out, int n);
+	// The autotuned ROI mappings of modes 6-8: up to n entries of (mode, roi, chunk size class, lanes, chunk) after
+	// the first `skip` entries; returns the entries written.
+	int TunedMappings(int* out, int n, int skip) const;
 	int SetPrecision(int p) { const int o = precision_; precision_ = p; return o; }
 	int Precision() const { return precision_; }
 	cudaStream_t Stream() const { return stream_; }

@@ -16,6 +16,7 @@ COLS = 18
 EXPORTS = ["Localization", "Fitting", "Wavelett", "AutoThreshold", "Astigmatism3DEstimation", "PTB_LocalizationDevice",
            "PTB_SetSegmentationMode", "PTB_SetFitPrecision", "PTB_LastError", "PTB_KernelLaunchCount",
            "PTB_SetProfiling", "PTB_StageTimes", "PTB_MleEvaluations", "PTB_GraphStats", "PTB_SegmentationStats", "PTB_EnginePoolStats",
+           "PTB_MleMappings",
            "PTB_MeasureFmaPeak", "PTB_FittingDeviceNoAlloc",
            "PTB_ServerStart", "PTB_SubmitStack", "PTB_PollStack", "PTB_StackResult", "PTB_ServerStop", "PTB_ServerFuseStats",
            "PTB_TiffInfo", "PTB_TiffRead", "PTB_LocalizationTiff", "Tracking", "PTB_TrackingDevice", "PTB_SplineCoefficients"]
@@ -79,6 +80,8 @@ def load(path=LIB_PATH):
     L.PTB_SegmentationStats.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
     L.PTB_EnginePoolStats.restype = None
     L.PTB_EnginePoolStats.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
+    L.PTB_MleMappings.restype = ctypes.c_int
+    L.PTB_MleMappings.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     L.PTB_SplineCoefficients.restype = _u64
     L.PTB_SplineCoefficients.argtypes = [_f64p, _u64, _u64, _u64, _f64p, _f64p]
     L.PTB_ServerFuseStats.restype = None
@@ -306,6 +309,14 @@ def engine_pool_stats():
     out = np.zeros(2, dtype=np.uint64)
     load().PTB_EnginePoolStats(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 2)
     return {"engines": int(out[0]), "peak_leased": int(out[1])}
+
+
+def mle_mappings():
+    """Autotuned ROI mappings of modes 6-8 on this device's engines: a list of {"mode", "roi", "size_class",
+    "lanes", "chunk"}."""
+    out = np.zeros((64, 5), dtype=np.int32)
+    n = load().PTB_MleMappings(out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), 64)
+    return [dict(zip(("mode", "roi", "size_class", "lanes", "chunk"), map(int, row))) for row in out[:n]]
 
 
 def fma_peak(fp64):

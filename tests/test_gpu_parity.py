@@ -516,6 +516,9 @@ def test_mle_autotuned_matches_fixed(lib, orc):
     a = lib.localization(s, thr, 0.0, 6, MLE6)
     b = orc.localization(s, thr, 0.0, 6, MLE6)
     _mle_check(a, b, "mode6 gauss c1 autotuned", 6, 1 / 500, orc, s, thr, MLE6)
+    # the autotuner's choice is reported per engine and tuned class, among the timed mappings
+    tuned = [m for m in lib.mle_mappings() if m["mode"] == 6 and m["roi"] == 7]
+    assert tuned and all((m["lanes"], m["chunk"]) in {(int(l), int(c)) for l, c in MAPPINGS} for m in tuned), tuned
 
 
 # ---- Astigmatism3DEstimation: bit-exact against the oracle (itself pinned to the reference build) ---------------

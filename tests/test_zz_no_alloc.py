@@ -85,8 +85,9 @@ def _deviance(orc, stack, pos, row, fit, params):
 
 def _mle_within_oracle(orc, stack, pos, got, want, fit, params):
     """Fits that succeeded on both sides lie within the stated tolerances of the FP64 oracle (x, y 1e-3 px, photons
-    1e-4 relative), except fits that ended in another local optimum of the deviance: at most 1 in 1000 (and 2) may
-    be less likely than the oracle's optimum; those at least as likely are counted. Status flips: 1 in 500."""
+    1e-4 relative), except fits that ended in another local optimum of the deviance, with the parity tests' share per
+    mode: fits less likely than the oracle's optimum plus status flips at most 1 in 1000 for mode 6 and 1 in 200 for
+    the astigmatic mode 7, whose z has two optima near focus (and at least 2); those at least as likely are counted."""
     ok = (got[:, 8] >= 0) & (want[:, 8] >= 0)
     beyond = ok & ((np.abs(got[:, 4] - want[:, 4]) > 1e-3) | (np.abs(got[:, 5] - want[:, 5]) > 1e-3) |
                    (np.abs(got[:, 7] - want[:, 7]) > 1e-4 * np.abs(want[:, 7])))
@@ -98,7 +99,8 @@ def _mle_within_oracle(orc, stack, pos, got, want, fit, params):
               "flips": int(np.sum((got[:, 8] >= 0) != (want[:, 8] >= 0)))}
     print(json.dumps(record))
     assert ok.sum() > 0.9 * len(got), record
-    assert worse <= max(2, len(got) // 1000) and record["flips"] <= max(1, len(got) // 500), record
+    share = {6: 1000, 7: 200}[fit]
+    assert worse + record["flips"] <= max(2, len(got) // share), record
 
 
 @pytest.mark.parametrize("fit", [6, 7])
