@@ -654,7 +654,8 @@ def main():
     parity = None
     if rank == 0 and not args.no_parity:
         parity = parity_run(ptb, d_in, thr)
-        parity["frames_flooded_again_frame_wide"] = {"timed_steps": seg["routed"], "frames_segmented": seg["frames"]}
+        parity["frames_flooded_again_frame_wide"] = {"timed_steps": seg["routed"], "frames_segmented": seg["frames"],
+                                                     "frames_given_the_rank_test": seg["rank_tested"]}
 
     # end to end through the reference-facing C ABI with host buffers
     host_in = torch.empty((frames, h, w), dtype=torch.int16, pin_memory=True)

@@ -168,14 +168,18 @@ PTB_API uint64_t PTB_FittingDeviceNoAlloc(const uint16_t* d_input, const double*
 /* Segmentation mode. Both modes give the reference's labels (Segmentation2D.cpp:336-385) for any threshold.
  * 0 (default): each 8-connected component of the thresholded potential is flooded on its own, in parallel, and then
  * tested: the flood of a component equals the reference's frame-wide flood when, at every basin boundary, the lowest
- * W1 along the winning parent chain exceeds the competing neighbour's W1 by more than the largest aging term the
- * frame-wide flood can add (the frame's domain pixel count x 1e-7). A frame failing the test anywhere is flooded
- * again as one unit with the frame-global pop counter. 1 (strict): every frame is flooded as one unit.
- * Returns the previous mode. */
+ * W1 along the winning parent chain exceeds the competing neighbour's W1 by more than the largest difference of aging
+ * terms the frame-wide flood can give them. First test: the frame's domain pixel count x 1e-7 bounds that difference.
+ * Boundaries failing it get the rank test, whose bound comes from the counts of the frame's pixels above and below
+ * the two W1 levels (the frame-wide flood pops in W1 order up to the aging term). A frame failing the rank test is
+ * flooded again as one unit with the frame-global pop counter. 1 (strict): every frame is flooded as one unit.
+ * 2: as 0 with the first test only (every frame failing it is flooded again frame-wide; for comparisons).
+ * Other values select 0. Returns the previous mode. */
 PTB_API int PTB_SetSegmentationMode(int mode);
 
 /* Segmentation diagnostics of the current device's engines since the last call: counts[0] frames segmented,
- * counts[1] frames flooded again frame-wide in mode 0 (up to n entries). */
+ * counts[1] frames flooded again frame-wide in mode 0, counts[2] frames whose per-component floods needed the rank
+ * test (the second exactness test) in mode 0 (up to n entries). */
 PTB_API void PTB_SegmentationStats(uint64_t* counts, int n);
 
 /* Engine pool of the current device (diagnostics): counts[0] engines created, counts[1] the most engines leased at

@@ -263,7 +263,10 @@ PTB_API uint64_t PTB_FittingDeviceNoAlloc(const uint16_t* d_input, const double*
 	}
 }
 
-PTB_API int PTB_SetSegmentationMode(int mode) { return ptb::SettingsFor().strict.exchange(mode ? 1 : 0); }
+PTB_API int PTB_SetSegmentationMode(int mode)
+{
+	return ptb::SettingsFor().strict.exchange(mode == 1 || mode == 2 ? mode : 0);
+}
 
 PTB_API int PTB_SetFitPrecision(int mode) { return ptb::SettingsFor().precision.exchange(mode < 0 ? 0 : (mode > 2 ? 2 : mode)); }
 

@@ -159,6 +159,9 @@ namespace {
 
 size_t Align(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
 
+// Words of the per-chunk frame arrays zeroed before each chunk: four [B + 1] arrays.
+size_t FrameWords(int B) { return 4 * (static_cast<size_t>(B) + 1); }
+
 uint32_t IndepBound(int H, int W) { return static_cast<uint32_t>(((H + 1) / 2)) * static_cast<uint32_t>(((W + 1) / 2)); }
 
 }  // namespace
@@ -230,11 +233,18 @@ static size_t PlanWorkspace(Workspace& ws, int H, int W, int B, uint32_t rowsCap
 	take(ws.fuNeighbour, capComp);
 	take(ws.fuBecome, capComp);
 	take(ws.fuLocked, capComp);
-	take(ws.frameDom, 3 * (static_cast<size_t>(B) + 1));  // frameDom, frameSeeds, frameRoute (zeroed together)
+	// frameDom, frameSeeds, frameRoute and frameSuspect (zeroed together for each chunk)
+	take(ws.frameDom, FrameWords(B));
 	if (base) {
 		ws.frameSeeds = ws.frameDom + B + 1;
 		ws.frameRoute = ws.frameSeeds + B + 1;
+		ws.frameSuspect = ws.frameRoute + B + 1;
 	}
+	take(ws.suspect, kSuspectCap);
+	take(ws.rankOrder, kSuspectCap);
+	take(ws.rankSlotOff, kRankSlots + 1);
+	take(ws.rankCount, 2 * kSuspectCap);
+	ws.capSuspect = kSuspectCap;
 	take(ws.frameRegBase, static_cast<size_t>(B) + 1);
 	take(ws.frameCandBase, static_cast<size_t>(B) + 1);
 	take(ws.frameKeep, static_cast<size_t>(B) + 1);
@@ -496,7 +506,7 @@ bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, d
 	const bool hooked = fitHook_ && fpr.mode >= kMleGauss;  // the fit runs in the hook's stage, outside this chain
 	if (fpr.mode >= kMleGauss && !hooked) {
 		if (fpr.lanes == 0) { TunedMapping(fpr, SizeClass(B, H, W)); }
-		fpr.mle.queue = ws.cnt->pad;  // this slot's work-queue counters
+		fpr.mle.queue = ws.cnt->queue;  // this slot's work-queue counters
 	}
 	const bool tune = !hooked && fpr.mode >= kMleGauss && fpr.lanes == 0;  // first chunk of this class: time the mappings
 	pendMleProf_ = prof && fpr.mode >= kMleGauss && !hooked;
@@ -511,7 +521,7 @@ bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, d
 	auto segmentAndDetect = [&]() {
 		bool k = PTB_CUDA(cudaMemsetAsync(ws.cnt, 0, sizeof(Counters), st));
 		k = k && PTB_CUDA(cudaMemsetAsync(ws.rootmask, 0, sizeof(uint32_t) * static_cast<size_t>(B) * H * ws.g.words, st));
-		k = k && PTB_CUDA(cudaMemsetAsync(ws.frameDom, 0, sizeof(uint32_t) * 3 * (static_cast<size_t>(B) + 1), st));
+		k = k && PTB_CUDA(cudaMemsetAsync(ws.frameDom, 0, sizeof(uint32_t) * FrameWords(B), st));
 		mark(0);
 		k = k && LaunchDetect(ws, thr, st);
 		mark(1);
@@ -598,6 +608,7 @@ long long Engine::CompleteChunk(int slot, uint32_t* truncatedFrames)
 		return -1;
 	}
 	segCounts_[1] += c.nroute;
+	segCounts_[2] += c.nslots;
 	if (truncatedFrames) { *truncatedFrames += c.truncated; }
 	return c.nfit;
 }
@@ -821,7 +832,7 @@ bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slo
 		FitParams t = fp;
 		t.lanes = c.lanes;
 		t.mle.chunk = envChunk ? envChunk : c.chunk;
-		t.mle.queue = ws.cnt->pad;
+		t.mle.queue = ws.cnt->queue;
 		cudaEventRecord(a, st);
 		if (!LaunchFit(dImg, H, W, ws.g.N, ws.cand, &ws.cnt->nfit, 0, ws.capRows, t, ws.rows, ws.fitFlag, precision_, st)) {
 			return false;
@@ -865,7 +876,7 @@ void Engine::GraphStats(uint64_t* out, int n)
 
 void Engine::SegmentationStats(uint64_t* out, int n)
 {
-	for (int k = 0; k < 2 && k < n; ++k) {
+	for (int k = 0; k < 3 && k < n; ++k) {
 		if (out) { out[k] = segCounts_[k]; }
 		segCounts_[k] = 0;
 	}

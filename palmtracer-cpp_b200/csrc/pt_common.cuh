@@ -34,6 +34,12 @@ constexpr uint8_t kSeed = 2;    // local maximum of the thresholded potential
 constexpr int kDirShift = 2;    // bits 2..4: raster-earlier seed neighbour a seed inherits its label from (0 = root)
 constexpr uint8_t kUnion = 32;  // bit 5: the pixel joins two union-find trees (set by CclInit for CclUnion)
 
+// Rank test of the per-component floods: at most kRankSlots frames per chunk, kSuspectCap boundary pairs per chunk
+// and kPairsPerFrame per frame (a frame beyond these limits is flooded again frame-wide instead).
+constexpr uint32_t kRankSlots = 64u;
+constexpr uint32_t kSuspectCap = 16384u;
+constexpr uint32_t kPairsPerFrame = 512u;
+
 // W1 values are exact multiples of 2^-16 (B3 taps are dyadic and the input is uint16), kept as int64 "fixed" units.
 constexpr double kW1Unit = 1.0 / 65536.0;
 
@@ -63,7 +69,10 @@ struct Counters {
 	uint32_t truncated; // some plane had more candidates than the per-plane capacity
 	uint32_t refit;     // FP32 fits redone in FP64
 	uint32_t nroute;    // frames whose per-component flood could differ from the frame-wide one (flooded again)
-	uint32_t pad[5];    // [0..1]: work-queue counters of the persistent fit kernels
+	uint32_t queue[2];  // work-queue counters of the persistent fit kernels
+	uint32_t nsuspect;  // boundary pairs that failed the flood's first exactness test (kept for the rank test)
+	uint32_t nslots;    // frames given the rank test (histogram slots in use)
+	uint32_t pad;
 };
 
 // One fit input: a segmentation candidate (x_, y_, intensity_, surf_ of SegmentationInfo) or a caller position.
@@ -192,6 +201,12 @@ struct Workspace {
 	// per frame [B + 1]: domain pixels and seeds (counted by the detection kernel), 1 where the frame is flooded again
 	// frame-wide (its per-component flood failed the exactness check)
 	uint32_t* frameDom; uint32_t* frameSeeds; uint32_t* frameRoute;
+	// per frame [B + 1]: nonzero where a boundary pair failed the first exactness test (then the frame's rank-test slot
+	// + 1); the failing pairs (frame, parent-chain minimum, W1 of the other-label neighbour z, W1 of z's highest
+	// domain neighbour); the pairs ordered by slot, with [kRankSlots + 1] slot offsets; two pixel counts per pair
+	uint32_t* frameSuspect;
+	uint4* suspect; uint32_t capSuspect;
+	uint32_t* rankOrder; uint32_t* rankSlotOff; uint32_t* rankCount;
 	uint32_t* frameRegBase; uint32_t* frameCandBase; uint32_t* frameKeep; uint32_t* frameOutBase;
 	// candidates / rows
 	uint32_t capRows;

@@ -11,8 +11,9 @@
 //      -v + pops * 1e-7 (Segmentation2D.cpp:336-385) and a pop counter local to the group. In strict mode a group is
 //      a whole frame and the counter is frame-global, which is the reference's process exactly;
 //   4. basin fusion (Segmentation2D.cpp:181-291) per group, then a second flood from one seed per basin;
-//   5. exactness check of every per-component flood (below); a frame that fails it is flooded again as one unit
-//      with the frame-global counter (the strict process), so the labels always equal the reference's;
+//   5. exactness check of every per-component flood (below): a first test per boundary pair, then the rank test of
+//      the pairs that fail it; a frame that fails both is flooded again as one unit with the frame-global counter
+//      (the strict process), so the labels always equal the reference's;
 //   6. exact integer region sums (W1 is an integer in 2^-16 units) and the surf > 4 filter, in label order.
 //
 // Why a per-component flood equals the frame-wide one, and when it may not. Labels only spread inside a component,
@@ -26,7 +27,12 @@
 // holds when c - W1(z) > T * 1e-7. So if every flooded pixel N and every neighbour z of N with another label satisfy
 // it, then (induction over the frame-wide flood's labelling order) every pixel receives its per-component label.
 // In 2^-16 units the test is (c - W1(z)) * 152 > T (2^-16 / 152 exceeds 1e-7 by 4e-10 per pop, which covers the
-// rounding of the FP64 keys, below 2e-11). Frames failing it at any boundary pixel are flooded again frame-wide.
+// rounding of the FP64 keys, below 2e-11). About 3 % of the 1024 x 1024 benchmark frames have a pair failing it.
+// Those pairs get the rank test (SuspectCheck), which bounds the two aging terms by the frame's pixel counts above
+// and below the two W1 levels instead of by T; a frame failing that too is flooded again frame-wide. The rank test
+// needs every pixel of the flood to be joined to a seed by a path that never falls below it, which holds for the
+// first flood (every local maximum is a seed) but not for the second flood of a basin fusion (one seed per basin):
+// there a pair failing the first test routes the frame directly.
 #include "pt_common.cuh"
 
 namespace ptb {
@@ -638,8 +644,44 @@ __device__ __forceinline__ void RouteFrame(const Workspace& ws, int f)
 	if (atomicExch(ws.frameRoute + f, 1u) == 0u) { atomicAdd(&ws.cnt->nroute, 1u); }
 }
 
-// Exactness test of a flooded pixel p against its 8 neighbours in global memory; false routes the frame.
-__device__ bool PixelExactGlobal(const Workspace& ws, uint32_t p, uint32_t T)
+// A boundary pair of frame f that failed the first test, kept for the rank test: the parent-chain minimum of the
+// flooded pixel, W1 of the neighbour z of another label and W1 of z's highest domain neighbour (0 when z is a seed of
+// the flood). Routes the frame, and returns false, when the list is full.
+__device__ __forceinline__ bool SuspectPair(const Workspace& ws, int f, uint32_t chain, uint32_t w1z, uint32_t zmax)
+{
+	const uint32_t i = atomicAdd(&ws.cnt->nsuspect, 1u);
+	if (i >= ws.capSuspect) {
+		RouteFrame(ws, f);
+		return false;
+	}
+	ws.suspect[i] = make_uint4(static_cast<uint32_t>(f), chain, w1z, zmax);
+	ws.frameSuspect[f] = 1u;
+	return true;
+}
+
+// Highest W1 among the domain neighbours of pixel z (in global memory).
+__device__ uint32_t HighestNeighbourGlobal(const Workspace& ws, uint32_t z)
+{
+	const Pix q = Decompose(z, ws.g);
+	uint32_t best = 0;
+	for (int dy = -1; dy <= 1; ++dy) {
+		const int yy = q.y + dy;
+		if (yy < 0 || yy >= ws.g.H) { continue; }
+		for (int dx = -1; dx <= 1; ++dx) {
+			const int xx = q.x + dx;
+			if ((dx == 0 && dy == 0) || xx < 0 || xx >= ws.g.W) { continue; }
+			const uint32_t nb = z + static_cast<uint32_t>(dy * ws.g.W + dx);
+			if (__ldg(ws.code + nb) & kDomain) { best = max(best, __ldg(ws.w1 + nb)); }
+		}
+	}
+	return best;
+}
+
+// Exactness test of a flooded pixel p of frame f against its 8 neighbours in global memory. A pair failing the first
+// test is kept for the rank test (rank = true: a first flood, seeded at every local maximum) or routes the frame
+// (rank = false: the second flood of a basin fusion, seeded at one maximum per basin, for which the rank bounds do
+// not hold). Returns false when the frame was routed.
+__device__ bool PixelExactGlobal(const Workspace& ws, uint32_t p, uint32_t T, int f, bool rank)
 {
 	const uint32_t chain = ws.par[p];
 	if (chain == kNoChain) { return true; }
@@ -653,7 +695,15 @@ __device__ bool PixelExactGlobal(const Workspace& ws, uint32_t p, uint32_t T)
 			if ((dx == 0 && dy == 0) || xx < 0 || xx >= ws.g.W) { continue; }
 			const uint32_t nb = p + static_cast<uint32_t>(dy * ws.g.W + dx);
 			if (!(__ldg(ws.code + nb) & kDomain) || ws.lab[nb] == L) { continue; }
-			if (!PairExact(chain, __ldg(ws.w1 + nb), T)) { return false; }
+			const uint32_t w1z = __ldg(ws.w1 + nb);
+			if (PairExact(chain, w1z, T)) { continue; }
+			if (!rank) {
+				RouteFrame(ws, f);
+				return false;
+			}
+			// z pushed by the flood (a chain value) or one of its seeds
+			const uint32_t zmax = ws.par[nb] == kNoChain ? 0u : HighestNeighbourGlobal(ws, nb);
+			if (!SuspectPair(ws, f, chain, w1z, zmax)) { return false; }
 		}
 	}
 	return true;
@@ -752,7 +802,8 @@ __global__ void __launch_bounds__(kFloodThreads) GroupFlood(Workspace ws, uint32
 // one-pixel ring in shared memory, lane 0 floods it there (the flood is one serial chain of heap operations; with
 // the box in shared memory each of its steps waits on shared memory instead of on L2 or DRAM), and the lanes write
 // back the labels the flood set. A group whose box exceeds kBoxCap pixels is flooded in global memory by lane 0.
-__global__ void __launch_bounds__(kBoxWarps * 32) GroupFloodBox(Workspace ws)
+// rank: pairs failing the first exactness test are kept for the rank test (else they route the frame directly).
+__global__ void __launch_bounds__(kBoxWarps * 32) GroupFloodBox(Workspace ws, int rank)
 {
 	__shared__ BoxSmem boxes[kBoxWarps];
 	BoxSmem& sm = boxes[threadIdx.x / 32];
@@ -792,8 +843,7 @@ __global__ void __launch_bounds__(kBoxWarps * 32) GroupFloodBox(Workspace ws)
 			}
 			__syncwarp();
 			bool exact = true;
-			for (uint32_t i = lane; i < nPix && exact; i += 32) { exact = PixelExactGlobal(ws, ws.gPix[off + i], T); }
-			if (__any_sync(0xffffffffu, !exact) && lane == 0) { RouteFrame(ws, f); }
+			for (uint32_t i = lane; i < nPix && exact; i += 32) { exact = PixelExactGlobal(ws, ws.gPix[off + i], T, f, rank != 0); }
 			continue;
 		}
 		const uint32_t base = static_cast<uint32_t>(f) * static_cast<uint32_t>(geo.N) + static_cast<uint32_t>(by0 * geo.W + bx0);
@@ -814,23 +864,39 @@ __global__ void __launch_bounds__(kBoxWarps * 32) GroupFloodBox(Workspace ws)
 			FloodGroup<true>(geo, BoxView{sm, bx0, by0, bw}, seeds, nSeeds, heap);
 		}
 		__syncwarp();
-		bool exact = true;
 		for (int i = lane; i < bw * bh; i += 32) {
 			if (!(sm.flag[i] & 2u) || sm.lab[i] == 0) { continue; }
 			const int r = i / bw, c = i - r * bw;
 			ws.lab[base + static_cast<uint32_t>(r * geo.W + c)] = sm.lab[i];
-			// exactness test against the neighbours of other labels (every neighbour in the frame lies in the box)
+			// exactness test against the neighbours of other labels (every neighbour in the frame lies in the box); a
+			// pair failing the first test is kept for the rank test
 			const uint32_t L = sm.lab[i], chain = sm.chain[i];
 			for (int dy = -1; dy <= 1; ++dy) {
 				if (r + dy < 0 || r + dy >= bh) { continue; }
 				for (int dx = -1; dx <= 1; ++dx) {
 					if ((dx == 0 && dy == 0) || c + dx < 0 || c + dx >= bw) { continue; }
 					const int j = i + dy * bw + dx;
-					if ((sm.flag[j] & 1u) && sm.lab[j] != L && !PairExact(chain, sm.w1[j], T)) { exact = false; }
+					if (!(sm.flag[j] & 1u) || sm.lab[j] == L || PairExact(chain, sm.w1[j], T)) { continue; }
+					if (!rank) {
+						RouteFrame(ws, f);
+						continue;
+					}
+					// z = pixel j is a group pixel, so its neighbours in the frame lie in the box as well
+					uint32_t zmax = 0;
+					if (sm.chain[j] != kNoChain) {
+						const int zr = r + dy, zc = c + dx;
+						for (int ey = -1; ey <= 1; ++ey) {
+							if (zr + ey < 0 || zr + ey >= bh) { continue; }
+							for (int ex = -1; ex <= 1; ++ex) {
+								if ((ex == 0 && ey == 0) || zc + ex < 0 || zc + ex >= bw) { continue; }
+								zmax = max(zmax, sm.w1[j + ey * bw + ex]);  // 0 off the domain
+							}
+						}
+					}
+					SuspectPair(ws, f, chain, sm.w1[j], zmax);
 				}
 			}
 		}
-		if (__any_sync(0xffffffffu, !exact) && lane == 0) { RouteFrame(ws, f); }
 		__syncwarp();
 	}
 }
@@ -948,11 +1014,191 @@ __global__ void __launch_bounds__(kFloodThreads) GroupFuse(Workspace ws, uint32_
 		const int f = Decompose(pix[0], geo).f;
 		const uint32_t T = ws.frameDom[f];
 		for (uint32_t i = 0; i < nPix; ++i) {
-			if (!PixelExactGlobal(ws, pix[i], T)) {
+			if (!PixelExactGlobal(ws, pix[i], T, f, false)) { break; }
+		}
+	}
+}
+
+// ---- Rank test of the per-component floods ---------------------------------------------------------------------
+// The frame-wide flood pops in W1 order up to its aging term: a pixel whose W1 exceeds another's by more than
+// delta = T * 1e-7 (the largest aging term, T = the frame's domain pixels) leaves the heap first, since the path that
+// joins it to its component's maximum (a seed) never falls below its W1 and some pixel of that path is always in the
+// heap. So a pixel p is popped at a position g(p) <= B(p) = #{domain pixels with W1 >= W1(p) - delta} and its pushes
+// age by g(p) * 1e-7, while a pixel n is popped at g(n) > #{poppable pixels with W1 > W1(n) + delta}. For a pair
+// with parent-chain minimum c (every chain element has W1 >= c and was pushed by a chain element, so with aging at
+// most B_c * 1e-7, B_c = #{W1 >= c - delta}) and competing neighbour z (pushed by one of its neighbours, none higher
+// than zmax, so with aging at least A_z * 1e-7, A_z = #{poppable W1 > zmax + delta} + 1; 0 when z is a seed), every
+// chain element leaves the frame-wide heap before z when
+//   (c - W1(z)) * 2^-16 > (B_c - A_z + 1) * 1e-7,   i.e. (c - W1(z)) * 78125 > (B_c - A_z + 1) * 512,
+// the + 1 covering the rounding of the FP64 keys. The counts are exact: SuspectCount compares every domain pixel of
+// the frame with the pair's two levels. A pair failing this too routes its frame to the frame-wide flood.
+
+constexpr int kPlanThreads = 1024;
+
+// Step 1 (one CTA): a slot for each frame with pairs kept for the rank test, in frame order (frameSuspect[f] =
+// slot + 1), and the pairs ordered by slot with zeroed counts. Frames beyond kRankSlots slots or with more than
+// kPairsPerFrame pairs are routed instead (and get no slot). Nothing to do without such pairs.
+__global__ void __launch_bounds__(kPlanThreads) SuspectPlan(Workspace ws)
+{
+	__shared__ uint32_t warpSum[kPlanThreads / 32];
+	__shared__ uint32_t carry;
+	__shared__ uint32_t slotCount[kRankSlots], slotCur[kRankSlots];
+	if (ws.cnt->nsuspect == 0) { return; }
+	const int B = ws.g.B, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	if (threadIdx.x == 0) { carry = 0; }
+	if (threadIdx.x < kRankSlots) { slotCount[threadIdx.x] = 0; }
+	__syncthreads();
+	for (int base = 0; base < B; base += kPlanThreads) {
+		const int f = base + static_cast<int>(threadIdx.x);
+		const uint32_t v = (f < B && ws.frameSuspect[f] != 0u) ? 1u : 0u;
+		uint32_t x = v;
+		#pragma unroll
+		for (int d = 1; d < 32; d <<= 1) {
+			const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+			if (lane >= d) { x += y; }
+		}
+		if (lane == 31) { warpSum[warp] = x; }
+		__syncthreads();
+		if (warp == 0) {
+			uint32_t w = warpSum[lane];
+			#pragma unroll
+			for (int d = 1; d < 32; d <<= 1) {
+				const uint32_t y = __shfl_up_sync(0xffffffffu, w, d);
+				if (lane >= d) { w += y; }
+			}
+			warpSum[lane] = w;
+		}
+		__syncthreads();
+		if (v) {
+			const uint32_t slot = carry + (warp ? warpSum[warp - 1] : 0u) + x - 1u;
+			if (slot < kRankSlots) { ws.frameSuspect[f] = slot + 1u; }
+			else {
+				ws.frameSuspect[f] = 0u;
 				RouteFrame(ws, f);
-				break;
 			}
 		}
+		__syncthreads();
+		if (threadIdx.x == 0) { carry += warpSum[kPlanThreads / 32 - 1]; }
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) { ws.cnt->nslots = carry; }
+	const uint32_t nrec = min(ws.cnt->nsuspect, ws.capSuspect);
+	for (uint32_t i = threadIdx.x; i < nrec; i += kPlanThreads) {
+		const uint32_t s = ws.frameSuspect[ws.suspect[i].x];
+		if (s != 0u) { atomicAdd(slotCount + (s - 1u), 1u); }
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		uint32_t off = 0;
+		for (uint32_t k = 0; k < kRankSlots; ++k) {
+			ws.rankSlotOff[k] = off;
+			slotCur[k] = off;
+			off += slotCount[k];
+		}
+		ws.rankSlotOff[kRankSlots] = off;
+	}
+	__syncthreads();
+	for (uint32_t i = threadIdx.x; i < nrec; i += kPlanThreads) {
+		const uint32_t f = ws.suspect[i].x, s = ws.frameSuspect[f];
+		if (s == 0u) { continue; }
+		ws.rankOrder[atomicAdd(slotCur + (s - 1u), 1u)] = i;
+		ws.rankCount[2 * i] = 0u;
+		ws.rankCount[2 * i + 1] = 0u;
+	}
+	__syncthreads();
+	// frames with too many pairs: routed; their slots stay empty in the counting pass (frameSuspect = 0)
+	for (uint32_t i = threadIdx.x; i < nrec; i += kPlanThreads) {
+		const uint32_t f = ws.suspect[i].x, s = ws.frameSuspect[f];
+		if (s != 0u && slotCount[s - 1u] > kPairsPerFrame) { RouteFrame(ws, static_cast<int>(f)); }
+	}
+	__syncthreads();
+	for (int f = threadIdx.x; f < B; f += kPlanThreads) {
+		const uint32_t s = ws.frameSuspect[f];
+		if (s != 0u && slotCount[s - 1u] > kPairsPerFrame) { ws.frameSuspect[f] = 0u; }
+	}
+}
+
+// The two levels of pair i of frame f: B_c counts W1 >= lowB, A_z counts poppable W1 > lowA (lowA = 2^32 - 1 when
+// there is nothing to count: z a seed, or a level beyond the W1 range).
+__device__ __forceinline__ void PairLevels(const Workspace& ws, const uint4& r, uint32_t& lowB, uint32_t& lowA)
+{
+	const uint32_t T = ws.frameDom[r.x];
+	const uint32_t delta = static_cast<uint32_t>((static_cast<unsigned long long>(T) * 65536ull) / 10000000ull) + 1u;
+	lowB = r.y > delta ? r.y - delta : 0u;
+	const unsigned long long a = static_cast<unsigned long long>(r.w) + delta;
+	lowA = (r.w == 0u || a >= 0xffffffffull) ? 0xffffffffu : static_cast<uint32_t>(a);
+}
+
+// Step 2: exact counts of every pair's two levels over its frame's domain pixels, one pass over the domain list. The
+// lanes of a warp holding pixels of one slot compare them with each of the slot's pairs and add the ballot counts.
+__global__ void SuspectCount(Workspace ws)
+{
+	if (ws.cnt->nsuspect == 0) { return; }
+	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
+	const int lane = threadIdx.x & 31;
+	const uint32_t stride = gridDim.x * blockDim.x;
+	// every lane of a warp runs the same iterations (the bound is rounded up to whole warps)
+	const uint32_t nWarps = (n + 31u) & ~31u;
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nWarps; i += stride) {
+		uint32_t s = 0, w = 0;
+		bool poppable = false;
+		if (i < n) {
+			const uint32_t p = ws.dom[i];
+			s = ws.frameSuspect[FastDivide(p, ws.g.divN)];
+			if (s != 0u) {
+				w = __ldg(ws.w1 + p);
+				// every non-seed domain pixel is pushed and popped once; a seed only if it has a neighbour that is
+				// not a seed (the reference's initial heap takes the labelled pixels next to an unlabelled one)
+				poppable = !(__ldg(ws.code + p) & kSeed);
+				if (!poppable) {
+					const Pix q = Decompose(p, ws.g);
+					for (int dy = -1; dy <= 1 && !poppable; ++dy) {
+						const int yy = q.y + dy;
+						if (yy < 0 || yy >= ws.g.H) { continue; }
+						for (int dx = -1; dx <= 1 && !poppable; ++dx) {
+							const int xx = q.x + dx;
+							if ((dx == 0 && dy == 0) || xx < 0 || xx >= ws.g.W) { continue; }
+							const uint32_t nb = p + static_cast<uint32_t>(dy * ws.g.W + dx);  // in the frame: no wrap
+							poppable = !(__ldg(ws.code + nb) & kSeed);
+						}
+					}
+				}
+			}
+		}
+		unsigned pending = __ballot_sync(0xffffffffu, s != 0u);
+		while (pending) {
+			const uint32_t slot = __shfl_sync(0xffffffffu, s, __ffs(pending) - 1);
+			const bool mine = s == slot;
+			pending &= ~__ballot_sync(0xffffffffu, mine);
+			const uint32_t k0 = ws.rankSlotOff[slot - 1u], k1 = ws.rankSlotOff[slot];
+			for (uint32_t k = k0; k < k1; ++k) {
+				const uint32_t idx = ws.rankOrder[k];
+				const uint4 r = ws.suspect[idx];
+				uint32_t lowB, lowA;
+				PairLevels(ws, r, lowB, lowA);
+				const uint32_t nb = __popc(__ballot_sync(0xffffffffu, mine && w >= lowB));
+				const uint32_t na = __popc(__ballot_sync(0xffffffffu, mine && poppable && w > lowA));
+				if (lane == 0) {
+					if (nb) { atomicAdd(ws.rankCount + 2 * idx, nb); }
+					if (na) { atomicAdd(ws.rankCount + 2 * idx + 1, na); }
+				}
+			}
+		}
+	}
+}
+
+// Step 3: the rank test of every counted pair.
+__global__ void SuspectCheck(Workspace ws)
+{
+	if (ws.cnt->nsuspect == 0) { return; }
+	const uint32_t nrec = min(ws.cnt->nsuspect, ws.capSuspect);
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nrec; i += gridDim.x * blockDim.x) {
+		const uint4 r = ws.suspect[i];
+		if (ws.frameSuspect[r.x] == 0u) { continue; }  // no slot: the frame is routed already
+		const long long bc = ws.rankCount[2 * i];
+		const long long az = r.w == 0u ? 0ll : static_cast<long long>(ws.rankCount[2 * i + 1]) + 1;
+		const long long lhs = (static_cast<long long>(r.y) - static_cast<long long>(r.z)) * 78125ll;
+		if (!(lhs > (bc - az + 1) * 512ll)) { RouteFrame(ws, static_cast<int>(r.x)); }
 	}
 }
 
@@ -1057,6 +1303,9 @@ bool LaunchSegment(const Workspace& ws, double ratio, int strict, uint32_t maxPo
 	SeedLabel<<<kGrid, kThreads, 0, st>>>(ws);
 	CountLaunch();
 	ok = ok && PTB_LAUNCHED();
+	// mode 0: per-component floods with both exactness tests; 2: with the first test only; 1: frame-wide floods
+	const int rank = strict == 0 ? 1 : 0;
+	strict = strict == 1 ? 1 : 0;
 	const uint32_t groupsStrict = strict ? static_cast<uint32_t>(g.B) : 0u;
 	if (strict) {
 		PTB_CUDA(cudaMemsetAsync(ws.gOff, 0, sizeof(uint32_t) * (g.B + 1), st));
@@ -1085,7 +1334,7 @@ bool LaunchSegment(const Workspace& ws, double ratio, int strict, uint32_t maxPo
 		GroupFlood<<<kGrid * 2, kFloodThreads, 0, st>>>(ws, groupsStrict, 0);
 	}
 	else {  // one warp per group, staged in shared memory
-		GroupFloodBox<<<kGrid, kBoxWarps * 32, 0, st>>>(ws);
+		GroupFloodBox<<<kGrid, kBoxWarps * 32, 0, st>>>(ws, rank);
 	}
 	CountLaunch(2);
 	ok = ok && PTB_LAUNCHED();
@@ -1096,7 +1345,16 @@ bool LaunchSegment(const Workspace& ws, double ratio, int strict, uint32_t maxPo
 		ok = ok && PTB_LAUNCHED();
 	}
 	if (!strict) {
-		// frames whose per-component floods failed the exactness test: flooded again as one unit with the frame-global
+		// boundary pairs that failed the first exactness test: the rank test of their frames (each kernel returns at
+		// once when no pair failed)
+		if (rank) {
+			SuspectPlan<<<1, kPlanThreads, 0, st>>>(ws);
+			SuspectCount<<<kGrid, kThreads, 0, st>>>(ws);
+			SuspectCheck<<<64, kThreads, 0, st>>>(ws);
+			CountLaunch(3);
+			ok = ok && PTB_LAUNCHED();
+		}
+		// frames whose per-component floods failed the exactness tests: flooded again as one unit with the frame-global
 		// pop counter (each kernel returns at once when no frame was routed)
 		const uint32_t frames = static_cast<uint32_t>(g.B);
 		RedoOffsets<<<1, kRedoThreads, 0, st>>>(ws);

@@ -282,11 +282,12 @@ def graph_stats():
 
 
 def segmentation_stats():
-    """{"frames", "routed"}: frames segmented by this device's engine and, of those, frames flooded again frame-wide
-    after their per-component floods failed the exactness test, since the last call."""
-    out = np.zeros(2, dtype=np.uint64)
-    load().PTB_SegmentationStats(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 2)
-    return {"frames": int(out[0]), "routed": int(out[1])}
+    """{"frames", "routed", "rank_tested"}: frames segmented by this device's engines since the last call; of those,
+    frames whose per-component floods needed the second (rank) exactness test, and frames flooded again frame-wide
+    because they failed it."""
+    out = np.zeros(3, dtype=np.uint64)
+    load().PTB_SegmentationStats(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 3)
+    return {"frames": int(out[0]), "routed": int(out[1]), "rank_tested": int(out[2])}
 
 
 def spline_coefficients(psf, lam=None):
