@@ -172,14 +172,17 @@ PTB_API uint64_t PTB_FittingDeviceNoAlloc(const uint16_t* d_input, const double*
  * terms the frame-wide flood can give them. First test: the frame's domain pixel count x 1e-7 bounds that difference.
  * Boundaries failing it get the rank test, whose bound comes from the counts of the frame's pixels above and below
  * the two W1 levels (the frame-wide flood pops in W1 order up to the aging term). A frame failing the rank test is
- * flooded again as one unit with the frame-global pop counter. 1 (strict): every frame is flooded as one unit.
+ * flooded again per component with each pop's aging set to its estimated frame-wide position, and tested again with
+ * per-element bounds; only a frame failing that too (or, with basin fusion, the rank test) is flooded again as one
+ * unit with the frame-global pop counter. 1 (strict): every frame is flooded as one unit.
  * 2: as 0 with the first test only (every frame failing it is flooded again frame-wide; for comparisons).
  * Other values select 0. Returns the previous mode. */
 PTB_API int PTB_SetSegmentationMode(int mode);
 
 /* Segmentation diagnostics of the current device's engines since the last call: counts[0] frames segmented,
- * counts[1] frames flooded again frame-wide in mode 0, counts[2] frames whose per-component floods needed the rank
- * test (the second exactness test) in mode 0 (up to n entries). */
+ * counts[1] frames flooded again frame-wide, counts[2] frames whose per-component floods needed the rank test (the
+ * second exactness test) in mode 0, counts[3] frames flooded again per component with estimated frame-wide aging
+ * after failing it (up to n entries). */
 PTB_API void PTB_SegmentationStats(uint64_t* counts, int n);
 
 /* Engine pool of the current device (diagnostics): counts[0] engines created, counts[1] the most engines leased at

@@ -159,8 +159,8 @@ namespace {
 
 size_t Align(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
 
-// Words of the per-chunk frame arrays zeroed before each chunk: four [B + 1] arrays.
-size_t FrameWords(int B) { return 4 * (static_cast<size_t>(B) + 1); }
+// Words of the per-chunk frame arrays zeroed before each chunk: five [B + 1] arrays.
+size_t FrameWords(int B) { return 5 * (static_cast<size_t>(B) + 1); }
 
 uint32_t IndepBound(int H, int W) { return static_cast<uint32_t>(((H + 1) / 2)) * static_cast<uint32_t>(((W + 1) / 2)); }
 
@@ -233,13 +233,17 @@ static size_t PlanWorkspace(Workspace& ws, int H, int W, int B, uint32_t rowsCap
 	take(ws.fuNeighbour, capComp);
 	take(ws.fuBecome, capComp);
 	take(ws.fuLocked, capComp);
-	// frameDom, frameSeeds, frameRoute and frameSuspect (zeroed together for each chunk)
+	// frameDom, frameSeeds, frameRoute, frameSuspect and frameReflood (zeroed together for each chunk)
 	take(ws.frameDom, FrameWords(B));
 	if (base) {
 		ws.frameSeeds = ws.frameDom + B + 1;
 		ws.frameRoute = ws.frameSeeds + B + 1;
 		ws.frameSuspect = ws.frameRoute + B + 1;
+		ws.frameReflood = ws.frameSuspect + B + 1;
 	}
+	take(ws.rfVals, static_cast<size_t>(kRefloodSlots) * 2 * kRefloodCap);
+	take(ws.rfInfo, static_cast<size_t>(kRefloodSlots) * 4);
+	take(ws.rfPix, static_cast<size_t>(kRefloodSlots) * static_cast<size_t>(g.N) * 2);
 	take(ws.suspect, kSuspectCap);
 	take(ws.rankOrder, kSuspectCap);
 	take(ws.rankSlotOff, kRankSlots + 1);
@@ -609,6 +613,7 @@ long long Engine::CompleteChunk(int slot, uint32_t* truncatedFrames)
 	}
 	segCounts_[1] += c.nroute;
 	segCounts_[2] += c.nslots;
+	segCounts_[3] += c.nreflood;
 	if (truncatedFrames) { *truncatedFrames += c.truncated; }
 	return c.nfit;
 }
@@ -813,7 +818,8 @@ void Engine::TunedMapping(FitParams& fp, int sizeClass) const
 
 // Times the ROI mappings of modes 6-8 on this chunk's candidates - lanes per ROI (1: a thread per ROI through the
 // four-launch pipeline; 2, 4, 8, 16: lane groups in the LM and polish; 32: a warp per ROI, one launch) and the work
-// queue's chunk (candidates a lane takes at a time) - and keeps the fastest for (mode, ROI, chunk size class).
+// queue's chunk (candidates a lane takes at a time) - and keeps the fastest for (mode, ROI, chunk size class). Each
+// choice runs once untimed before its timed run.
 bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slot, int sizeClass)
 {
 	Workspace& ws = Ws(slot);
@@ -833,6 +839,10 @@ bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slo
 		t.lanes = c.lanes;
 		t.mle.chunk = envChunk ? envChunk : c.chunk;
 		t.mle.queue = ws.cnt->queue;
+		// one untimed run first: the first launch of a kernel also loads its code, which is not what the choice costs
+		if (!LaunchFit(dImg, H, W, ws.g.N, ws.cand, &ws.cnt->nfit, 0, ws.capRows, t, ws.rows, ws.fitFlag, precision_, st)) {
+			return false;
+		}
 		cudaEventRecord(a, st);
 		if (!LaunchFit(dImg, H, W, ws.g.N, ws.cand, &ws.cnt->nfit, 0, ws.capRows, t, ws.rows, ws.fitFlag, precision_, st)) {
 			return false;
@@ -876,7 +886,7 @@ void Engine::GraphStats(uint64_t* out, int n)
 
 void Engine::SegmentationStats(uint64_t* out, int n)
 {
-	for (int k = 0; k < 3 && k < n; ++k) {
+	for (int k = 0; k < 4 && k < n; ++k) {
 		if (out) { out[k] = segCounts_[k]; }
 		segCounts_[k] = 0;
 	}

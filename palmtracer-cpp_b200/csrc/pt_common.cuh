@@ -39,6 +39,10 @@ constexpr uint8_t kUnion = 32;  // bit 5: the pixel joins two union-find trees (
 constexpr uint32_t kRankSlots = 64u;
 constexpr uint32_t kSuspectCap = 16384u;
 constexpr uint32_t kPairsPerFrame = 512u;
+// Re-flood of the frames that fail the rank test: at most kRefloodSlots frames per chunk, each with at most
+// kRefloodCap domain pixels (their W1 values are sorted for the rank lookups); other frames are flooded frame-wide.
+constexpr uint32_t kRefloodSlots = 8u;
+constexpr uint32_t kRefloodCap = 65536u;
 
 // W1 values are exact multiples of 2^-16 (B3 taps are dyadic and the input is uint16), kept as int64 "fixed" units.
 constexpr double kW1Unit = 1.0 / 65536.0;
@@ -71,8 +75,8 @@ struct Counters {
 	uint32_t nroute;    // frames whose per-component flood could differ from the frame-wide one (flooded again)
 	uint32_t queue[2];  // work-queue counters of the persistent fit kernels
 	uint32_t nsuspect;  // boundary pairs that failed the flood's first exactness test (kept for the rank test)
-	uint32_t nslots;    // frames given the rank test (histogram slots in use)
-	uint32_t pad;
+	uint32_t nslots;    // frames given the rank test
+	uint32_t nreflood;  // frames that failed the rank test (flooded again with estimated frame-wide aging)
 };
 
 // One fit input: a segmentation candidate (x_, y_, intensity_, surf_ of SegmentationInfo) or a caller position.
@@ -207,6 +211,12 @@ struct Workspace {
 	uint32_t* frameSuspect;
 	uint4* suspect; uint32_t capSuspect;
 	uint32_t* rankOrder; uint32_t* rankSlotOff; uint32_t* rankCount;
+	// per frame [B + 1]: nonzero where the frame failed the rank test (then its re-flood slot + 1); per slot: the sorted
+	// W1 values of its domain pixels and of the pixels its frame-wide flood pops ([kRefloodSlots][2][kRefloodCap]), the
+	// two counts and the frame + 1 ([kRefloodSlots][4]); per slot and pixel of the frame: the estimated frame-wide pop
+	// position and the upper bound of it ([kRefloodSlots][N][2])
+	uint32_t* frameReflood;
+	uint32_t* rfVals; uint32_t* rfInfo; uint32_t* rfPix;
 	uint32_t* frameRegBase; uint32_t* frameCandBase; uint32_t* frameKeep; uint32_t* frameOutBase;
 	// candidates / rows
 	uint32_t capRows;

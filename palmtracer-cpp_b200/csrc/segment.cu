@@ -1187,8 +1187,20 @@ __global__ void SuspectCount(Workspace ws)
 	}
 }
 
-// Step 3: the rank test of every counted pair.
-__global__ void SuspectCheck(Workspace ws)
+// A frame that failed the rank test: flooded again per component with estimated frame-wide aging (reflood), or
+// routed to the frame-wide flood.
+__device__ __forceinline__ void FailRankTest(const Workspace& ws, int f, int reflood)
+{
+	if (!reflood) {
+		RouteFrame(ws, f);
+		return;
+	}
+	if (atomicExch(ws.frameReflood + f, 1u) == 0u) { atomicAdd(&ws.cnt->nreflood, 1u); }
+}
+
+// Step 3: the rank test of every counted pair. reflood: frames that fail it are flooded again per component with
+// estimated frame-wide aging (no basin fusion follows); else they are routed to the frame-wide flood.
+__global__ void SuspectCheck(Workspace ws, int reflood)
 {
 	if (ws.cnt->nsuspect == 0) { return; }
 	const uint32_t nrec = min(ws.cnt->nsuspect, ws.capSuspect);
@@ -1198,7 +1210,320 @@ __global__ void SuspectCheck(Workspace ws)
 		const long long bc = ws.rankCount[2 * i];
 		const long long az = r.w == 0u ? 0ll : static_cast<long long>(ws.rankCount[2 * i + 1]) + 1;
 		const long long lhs = (static_cast<long long>(r.y) - static_cast<long long>(r.z)) * 78125ll;
-		if (!(lhs > (bc - az + 1) * 512ll)) { RouteFrame(ws, static_cast<int>(r.x)); }
+		if (!(lhs > (bc - az + 1) * 512ll)) { FailRankTest(ws, static_cast<int>(r.x), reflood); }
+	}
+}
+
+// ---- Re-flood with estimated frame-wide aging -------------------------------------------------------------------
+// A frame whose pairs fail the rank test may still be flooded per component: the test proves the labels of ANY
+// per-component flood whose parent chains pass it, whatever aging that flood used. Its own flood used the local pop
+// counter, which can order a contested pair differently from the frame-wide flood (the labels then genuinely
+// differ); flooded again with each pop's push aging set to its estimated frame-wide position (the number of the
+// frame's domain pixels with a higher W1, which the frame-wide flood pops first up to its aging term), the groups
+// follow the frame-wide order, and the test, now with every chain element's own bound
+//   min over e of (W1(e) * 78125 - B(parent(e)) * 512) > W1(z) * 78125 - (A_z - 1) * 512,
+// B(p) = #{W1 >= W1(p) - delta}, proves it. The counts come from the frame's sorted W1 values. A frame failing again
+// (or beyond the slots or the value capacity) is flooded frame-wide.
+
+// Step 1 (one CTA): slots for the frames marked by the rank test, in frame order; the others are routed.
+__global__ void __launch_bounds__(kPlanThreads) RefloodPlan(Workspace ws)
+{
+	__shared__ uint32_t next;
+	if (ws.cnt->nreflood == 0) { return; }
+	if (threadIdx.x == 0) { next = 0; }
+	if (threadIdx.x < kRefloodSlots * 4) { ws.rfInfo[threadIdx.x] = 0u; }
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		for (int f = 0; f < ws.g.B; ++f) {
+			if (ws.frameReflood[f] == 0u) { continue; }
+			if (next < kRefloodSlots && ws.frameRoute[f] == 0u && ws.frameDom[f] <= kRefloodCap) {
+				ws.frameReflood[f] = next + 1u;
+				ws.rfInfo[next * 4 + 2] = static_cast<uint32_t>(f) + 1u;
+				++next;
+			}
+			else {
+				ws.frameReflood[f] = 0u;
+				RouteFrame(ws, f);
+			}
+		}
+	}
+}
+
+// Pixel p (domain) of the chunk is popped by the frame-wide flood: a non-seed, or a seed with a non-seed neighbour
+// (the reference's initial heap takes the labelled pixels next to an unlabelled one).
+__device__ __forceinline__ bool Poppable(const Workspace& ws, uint32_t p)
+{
+	if (!(__ldg(ws.code + p) & kSeed)) { return true; }
+	const Pix q = Decompose(p, ws.g);
+	for (int dy = -1; dy <= 1; ++dy) {
+		const int yy = q.y + dy;
+		if (yy < 0 || yy >= ws.g.H) { continue; }
+		for (int dx = -1; dx <= 1; ++dx) {
+			const int xx = q.x + dx;
+			if ((dx == 0 && dy == 0) || xx < 0 || xx >= ws.g.W) { continue; }
+			const uint32_t nb = p + static_cast<uint32_t>(dy * ws.g.W + dx);
+			if (!(__ldg(ws.code + nb) & kSeed)) { return true; }
+		}
+	}
+	return false;
+}
+
+// Step 2: the W1 values of the slotted frames' domain pixels (and of their poppable pixels), over the domain list.
+__global__ void RefloodGather(Workspace ws)
+{
+	if (ws.cnt->nreflood == 0) { return; }
+	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		const uint32_t p = ws.dom[i];
+		const uint32_t s = ws.frameReflood[FastDivide(p, ws.g.divN)];
+		if (s == 0u) { continue; }
+		const uint32_t slot = s - 1u, w = __ldg(ws.w1 + p);
+		const uint32_t a = atomicAdd(ws.rfInfo + slot * 4, 1u);
+		if (a < kRefloodCap) { ws.rfVals[(static_cast<size_t>(slot) * 2) * kRefloodCap + a] = w; }
+		if (Poppable(ws, p)) {
+			const uint32_t b = atomicAdd(ws.rfInfo + slot * 4 + 1, 1u);
+			if (b < kRefloodCap) { ws.rfVals[(static_cast<size_t>(slot) * 2 + 1) * kRefloodCap + b] = w; }
+		}
+	}
+}
+
+constexpr int kRfSortThreads = 1024;
+
+// Step 3 (one CTA per slot): both value lists sorted ascending (bitonic over the next power of two, padded with the
+// largest value), in place in global memory.
+__global__ void __launch_bounds__(kRfSortThreads) RefloodSort(Workspace ws)
+{
+	const uint32_t slot = blockIdx.x;
+	if (ws.cnt->nreflood == 0 || ws.rfInfo[slot * 4 + 2] == 0u) { return; }
+	for (int a = 0; a < 2; ++a) {
+		uint32_t* v = ws.rfVals + (static_cast<size_t>(slot) * 2 + a) * kRefloodCap;
+		const uint32_t n = min(ws.rfInfo[slot * 4 + a], kRefloodCap);
+		uint32_t len = 2;
+		while (len < n) { len <<= 1; }
+		for (uint32_t i = n + threadIdx.x; i < len; i += kRfSortThreads) { v[i] = 0xffffffffu; }
+		__syncthreads();
+		for (uint32_t size = 2; size <= len; size <<= 1) {
+			for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+				for (uint32_t t = threadIdx.x; t < len / 2; t += kRfSortThreads) {
+					const uint32_t lo = 2 * t - (t & (stride - 1)), hi = lo + stride;
+					const bool up = (lo & size) == 0;
+					const uint32_t x = v[lo], y = v[hi];
+					if (up ? (y < x) : (x < y)) {
+						v[lo] = y;
+						v[hi] = x;
+					}
+				}
+				__syncthreads();
+			}
+		}
+	}
+}
+
+// Entries of the ascending list v[0, n) that are >= x (strict: > x).
+__device__ __forceinline__ uint32_t CountAbove(const uint32_t* v, uint32_t n, uint32_t x, bool strict)
+{
+	uint32_t lo = 0, hi = n;  // first index whose value is >= x (> x when strict)
+	while (lo < hi) {
+		const uint32_t mid = (lo + hi) >> 1;
+		if (strict ? (v[mid] <= x) : (v[mid] < x)) { lo = mid + 1; }
+		else { hi = mid; }
+	}
+	return n - lo;
+}
+
+__device__ __forceinline__ uint32_t FrameDelta(const Workspace& ws, int f)
+{
+	return static_cast<uint32_t>((static_cast<unsigned long long>(ws.frameDom[f]) * 65536ull) / 10000000ull) + 1u;
+}
+
+// Step 4: for every pixel of the slotted frames' groups (a warp per group): the estimated frame-wide pop position
+// #{W1 > W1(p)} and its upper bound B(p) = #{W1 >= W1(p) - delta}.
+__global__ void RefloodCounts(Workspace ws)
+{
+	if (ws.cnt->nreflood == 0) { return; }
+	const uint32_t nGroups = ws.cnt->nmulti;
+	const int lane = threadIdx.x & 31;
+	const uint32_t warps = gridDim.x * (blockDim.x / 32);
+	for (uint32_t m = (blockIdx.x * blockDim.x + threadIdx.x) / 32; m < nGroups; m += warps) {
+		const uint32_t off = ws.gOff[m], nPix = ws.gOff[m + 1] - off;
+		if (nPix == 0) { continue; }
+		const int f = Decompose(ws.gPix[off], ws.g).f;
+		const uint32_t s = ws.frameReflood[f];
+		if (s == 0u) { continue; }
+		const uint32_t slot = s - 1u;
+		const uint32_t* all = ws.rfVals + (static_cast<size_t>(slot) * 2) * kRefloodCap;
+		const uint32_t nAll = min(ws.rfInfo[slot * 4], kRefloodCap);
+		const uint32_t delta = FrameDelta(ws, f);
+		uint32_t* out = ws.rfPix + static_cast<size_t>(slot) * static_cast<size_t>(ws.g.N) * 2;
+		for (uint32_t i = lane; i < nPix; i += 32) {
+			const uint32_t p = ws.gPix[off + i];
+			const uint32_t w = __ldg(ws.w1 + p);
+			const size_t local = static_cast<size_t>(p) - static_cast<size_t>(f) * static_cast<size_t>(ws.g.N);
+			out[local * 2] = CountAbove(all, nAll, w, true);
+			out[local * 2 + 1] = CountAbove(all, nAll, w > delta ? w - delta : 0u, false);
+		}
+	}
+}
+
+constexpr int kRfWarps = 3;  // groups (warps) per CTA of the re-flood
+
+struct RfBoxSmem {
+	double key[kBoxHeap];
+	uint32_t pix[kBoxHeap];
+	long long v[kBoxCap];      // W1 * 78125 - B(pusher) * 512 (seeds: W1 * 78125)
+	long long m[kBoxCap];      // minimum of v over the pusher's parent chain (seeds: none)
+	uint32_t w1[kBoxCap];
+	uint32_t lab[kBoxCap];
+	uint32_t chain[kBoxCap];   // parent-chain minimum of W1 (the first test)
+	uint32_t gest[kBoxCap];    // estimated frame-wide pop position
+	uint32_t bnd[kBoxCap];     // its upper bound B
+	uint8_t flag[kBoxCap];     // bit 0: domain; bit 1: a non-seed (flooded)
+};
+
+constexpr long long kNoM = 0x7fffffffffffffffll;
+
+// Step 5: warp per group of the slotted frames, box staged in shared memory (a frame with a larger group is routed):
+// the flood with push aging (estimated position + 1) * 1e-7, then the per-element test at every boundary pair that
+// fails the first test; a failing frame is routed to the frame-wide flood.
+__global__ void __launch_bounds__(kRfWarps * 32) RefloodBox(Workspace ws)
+{
+	__shared__ RfBoxSmem boxes[kRfWarps];
+	if (ws.cnt->nreflood == 0) { return; }
+	RfBoxSmem& sm = boxes[threadIdx.x / 32];
+	const int lane = threadIdx.x & 31;
+	const Geometry& geo = ws.g;
+	const uint32_t n = ws.cnt->nmulti;
+	for (uint32_t m = blockIdx.x * kRfWarps + threadIdx.x / 32; m < n; m += gridDim.x * kRfWarps) {
+		const uint32_t off = ws.gOff[m], nPix = ws.gOff[m + 1] - off;
+		if (nPix == 0) { continue; }
+		const int f = Decompose(ws.gPix[off], geo).f;  // every lane reads the group's first pixel
+		const uint32_t s = ws.frameReflood[f];
+		if (s == 0u || ws.frameRoute[f] != 0u) { continue; }
+		const uint32_t slot = s - 1u;
+		int x0 = geo.W, y0 = geo.H, x1 = -1, y1 = -1;
+		for (uint32_t i = lane; i < nPix; i += 32) {
+			const Pix q = Decompose(ws.gPix[off + i], geo);
+			x0 = min(x0, q.x); x1 = max(x1, q.x); y0 = min(y0, q.y); y1 = max(y1, q.y);
+		}
+		#pragma unroll
+		for (int d = 16; d > 0; d >>= 1) {
+			x0 = min(x0, __shfl_xor_sync(0xffffffffu, x0, d));
+			y0 = min(y0, __shfl_xor_sync(0xffffffffu, y0, d));
+			x1 = max(x1, __shfl_xor_sync(0xffffffffu, x1, d));
+			y1 = max(y1, __shfl_xor_sync(0xffffffffu, y1, d));
+		}
+		const int bx0 = max(x0 - 1, 0), by0 = max(y0 - 1, 0);
+		const int bw = min(x1 + 1, geo.W - 1) - bx0 + 1, bh = min(y1 + 1, geo.H - 1) - by0 + 1;
+		if (bw * bh > kBoxCap) {
+			if (lane == 0) { RouteFrame(ws, f); }
+			continue;
+		}
+		const uint32_t base = static_cast<uint32_t>(f) * static_cast<uint32_t>(geo.N) + static_cast<uint32_t>(by0 * geo.W + bx0);
+		const uint32_t* pix = ws.rfPix + static_cast<size_t>(slot) * static_cast<size_t>(geo.N) * 2;
+		const uint32_t local0 = static_cast<uint32_t>(by0 * geo.W + bx0);
+		for (int i = lane; i < bw * bh; i += 32) {
+			const int r = i / bw, c = i - r * bw;
+			const uint32_t p = base + static_cast<uint32_t>(r * geo.W + c);
+			const uint8_t code = __ldg(ws.code + p);
+			const bool dom = (code & kDomain) != 0, seed = (code & kSeed) != 0;
+			const uint32_t w = dom ? __ldg(ws.w1 + p) : 0u;
+			sm.w1[i] = w;
+			sm.lab[i] = dom && seed ? ws.lab[p] : 0u;
+			sm.chain[i] = kNoChain;
+			sm.flag[i] = static_cast<uint8_t>((dom ? 1u : 0u) | (dom && !seed ? 2u : 0u));
+			const size_t local = static_cast<size_t>(local0) + static_cast<size_t>(r) * geo.W + c;
+			sm.gest[i] = dom ? pix[local * 2] : 0u;
+			sm.bnd[i] = dom ? pix[local * 2 + 1] : 0u;
+			sm.v[i] = static_cast<long long>(w) * 78125ll;  // a seed's value (no aging); pushed pixels overwrite it
+			sm.m[i] = kNoM;
+		}
+		__syncwarp();
+		if (lane == 0) {
+			uint32_t* seeds = ws.gSeed + ws.gSeedOff[m];
+			const uint32_t nSeeds = ws.gSeedOff[m + 1] - ws.gSeedOff[m];
+			SortSlice(seeds, nSeeds);
+			Heap heap{sm.key, sm.pix, 0, 1, kBoxHeap, ws.heapKey + off, ws.heapPix + off};
+			auto at = [&](int y, int x) { return (y - by0) * bw + (x - bx0); };
+			for (uint32_t k = 0; k < nSeeds; ++k) {
+				const uint32_t sd = seeds[k];
+				const Pix q = Decompose(sd, geo);
+				bool open = false;
+				for (int dy = -1; dy <= 1 && !open; ++dy) {
+					const int yy = q.y + dy;
+					if (yy < 0 || yy >= geo.H) { continue; }
+					for (int dx = -1; dx <= 1 && !open; ++dx) {
+						const int xx = q.x + dx;
+						if ((dx == 0 && dy == 0) || xx < 0 || xx >= geo.W) { continue; }
+						const int j = at(yy, xx);
+						if (!(sm.flag[j] & 1u) || sm.lab[j] == 0) { open = true; }
+					}
+				}
+				if (open) { heap.Push(-(static_cast<double>(sm.w1[at(q.y, q.x)]) * kW1Unit), sd); }
+			}
+			while (heap.len > 0) {
+				const uint32_t p = heap.Pop();
+				const Pix q = Decompose(p, geo);
+				const int ip = at(q.y, q.x);
+				const uint32_t L = sm.lab[ip];
+				// pushes at this pop age by the estimated frame-wide position of the pop
+				const double age = __dmul_rn(static_cast<double>(sm.gest[ip]) + 1.0, kEps);
+				const uint32_t chain = min(sm.chain[ip], sm.w1[ip]);
+				const long long mch = min(sm.m[ip], sm.v[ip]);
+				const long long bpush = static_cast<long long>(sm.bnd[ip]) * 512ll;
+				for (int t = 0; t < 8; ++t) {
+					const int dy = t < 3 ? -1 : (t < 5 ? 0 : 1);
+					const int dx = t < 3 ? t - 1 : (t < 5 ? (t == 3 ? -1 : 1) : t - 6);
+					const int yy = q.y + dy, xx = q.x + dx;
+					if (yy < 0 || yy >= geo.H || xx < 0 || xx >= geo.W) { continue; }
+					const int j = at(yy, xx);
+					if (!(sm.flag[j] & 1u) || sm.lab[j] != 0) { continue; }
+					const double k = __dadd_rn(-(static_cast<double>(sm.w1[j]) * kW1Unit), age);
+					heap.Push(k, p + static_cast<uint32_t>(dy * geo.W + dx));
+					sm.lab[j] = L;
+					sm.chain[j] = chain;
+					sm.m[j] = mch;
+					sm.v[j] = static_cast<long long>(sm.w1[j]) * 78125ll - bpush;
+				}
+			}
+		}
+		__syncwarp();
+		const uint32_t T = ws.frameDom[f];
+		const uint32_t delta = FrameDelta(ws, f);
+		const uint32_t* pop = ws.rfVals + (static_cast<size_t>(slot) * 2 + 1) * kRefloodCap;
+		const uint32_t nPop = min(ws.rfInfo[slot * 4 + 1], kRefloodCap);
+		bool exact = true;
+		for (int i = lane; i < bw * bh; i += 32) {
+			if (!(sm.flag[i] & 2u) || sm.lab[i] == 0) { continue; }
+			const int r = i / bw, c = i - r * bw;
+			ws.lab[base + static_cast<uint32_t>(r * geo.W + c)] = sm.lab[i];
+			const uint32_t L = sm.lab[i], chain = sm.chain[i];
+			const long long mi = sm.m[i];
+			for (int dy = -1; dy <= 1; ++dy) {
+				if (r + dy < 0 || r + dy >= bh) { continue; }
+				for (int dx = -1; dx <= 1; ++dx) {
+					if ((dx == 0 && dy == 0) || c + dx < 0 || c + dx >= bw) { continue; }
+					const int j = i + dy * bw + dx;
+					if (!(sm.flag[j] & 1u) || sm.lab[j] == L || PairExact(chain, sm.w1[j], T)) { continue; }
+					long long az = 0;
+					if (sm.chain[j] != kNoChain) {  // z pushed: its pusher is one of its neighbours, none above zmax
+						uint32_t zmax = 0;
+						const int zr = r + dy, zc = c + dx;
+						for (int ey = -1; ey <= 1; ++ey) {
+							if (zr + ey < 0 || zr + ey >= bh) { continue; }
+							for (int ex = -1; ex <= 1; ++ex) {
+								if ((ex == 0 && ey == 0) || zc + ex < 0 || zc + ex >= bw) { continue; }
+								zmax = max(zmax, sm.w1[j + ey * bw + ex]);
+							}
+						}
+						const unsigned long long x = static_cast<unsigned long long>(zmax) + delta;
+						az = (x < 0xffffffffull ? static_cast<long long>(CountAbove(pop, nPop, static_cast<uint32_t>(x), true)) : 0ll) + 1;
+					}
+					if (!(mi > static_cast<long long>(sm.w1[j]) * 78125ll - (az - 1) * 512ll)) { exact = false; }
+				}
+			}
+		}
+		if (__any_sync(0xffffffffu, !exact) && lane == 0) { RouteFrame(ws, f); }
+		__syncwarp();
 	}
 }
 
@@ -1350,8 +1675,15 @@ bool LaunchSegment(const Workspace& ws, double ratio, int strict, uint32_t maxPo
 		if (rank) {
 			SuspectPlan<<<1, kPlanThreads, 0, st>>>(ws);
 			SuspectCount<<<kGrid, kThreads, 0, st>>>(ws);
-			SuspectCheck<<<64, kThreads, 0, st>>>(ws);
-			CountLaunch(3);
+			// frames failing the rank test: flooded again with estimated frame-wide aging (not after a basin fusion,
+			// which used the first flood's labels)
+			SuspectCheck<<<64, kThreads, 0, st>>>(ws, fuse ? 0 : 1);
+			RefloodPlan<<<1, kPlanThreads, 0, st>>>(ws);
+			RefloodGather<<<kGrid, kThreads, 0, st>>>(ws);
+			RefloodSort<<<kRefloodSlots, kRfSortThreads, 0, st>>>(ws);
+			RefloodCounts<<<kGrid, kThreads, 0, st>>>(ws);
+			RefloodBox<<<kGrid, kRfWarps * 32, 0, st>>>(ws);
+			CountLaunch(8);
 			ok = ok && PTB_LAUNCHED();
 		}
 		// frames whose per-component floods failed the exactness tests: flooded again as one unit with the frame-global

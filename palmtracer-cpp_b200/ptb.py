@@ -282,12 +282,12 @@ def graph_stats():
 
 
 def segmentation_stats():
-    """{"frames", "routed", "rank_tested"}: frames segmented by this device's engines since the last call; of those,
-    frames whose per-component floods needed the second (rank) exactness test, and frames flooded again frame-wide
-    because they failed it."""
-    out = np.zeros(3, dtype=np.uint64)
-    load().PTB_SegmentationStats(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 3)
-    return {"frames": int(out[0]), "routed": int(out[1]), "rank_tested": int(out[2])}
+    """{"frames", "routed", "rank_tested", "reflooded"}: frames segmented by this device's engines since the last call;
+    of those, frames whose per-component floods needed the rank test, frames flooded again per component with
+    estimated frame-wide aging because they failed it, and frames flooded again frame-wide."""
+    out = np.zeros(4, dtype=np.uint64)
+    load().PTB_SegmentationStats(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 4)
+    return {"frames": int(out[0]), "routed": int(out[1]), "rank_tested": int(out[2]), "reflooded": int(out[3])}
 
 
 def spline_coefficients(psf, lam=None):
