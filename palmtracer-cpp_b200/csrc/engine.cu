@@ -242,7 +242,9 @@ static size_t PlanWorkspace(Workspace& ws, int H, int W, int B, uint32_t rowsCap
 		ws.frameReflood = ws.frameSuspect + B + 1;
 	}
 	take(ws.rfVals, static_cast<size_t>(kRefloodSlots) * 2 * kRefloodCap);
-	take(ws.rfInfo, static_cast<size_t>(kRefloodSlots) * 4);
+	take(ws.rfGrp, static_cast<size_t>(kRefloodSlots) * 2 * kRefloodCap);
+	take(ws.rfOff, static_cast<size_t>(kRefloodSlots) * 2 * (kRefloodBuckets + 1));
+	take(ws.rfInfo, static_cast<size_t>(kRefloodSlots) * 8);
 	take(ws.rfPix, static_cast<size_t>(kRefloodSlots) * static_cast<size_t>(g.N) * 2);
 	take(ws.suspect, kSuspectCap);
 	take(ws.rankOrder, kSuspectCap);

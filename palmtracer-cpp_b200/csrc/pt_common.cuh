@@ -43,6 +43,7 @@ constexpr uint32_t kPairsPerFrame = 512u;
 // kRefloodCap domain pixels (their W1 values are sorted for the rank lookups); other frames are flooded frame-wide.
 constexpr uint32_t kRefloodSlots = 8u;
 constexpr uint32_t kRefloodCap = 65536u;
+constexpr uint32_t kRefloodBuckets = 32768u;  // value buckets of the rank lookups
 
 // W1 values are exact multiples of 2^-16 (B3 taps are dyadic and the input is uint16), kept as int64 "fixed" units.
 constexpr double kW1Unit = 1.0 / 65536.0;
@@ -211,12 +212,13 @@ struct Workspace {
 	uint32_t* frameSuspect;
 	uint4* suspect; uint32_t capSuspect;
 	uint32_t* rankOrder; uint32_t* rankSlotOff; uint32_t* rankCount;
-	// per frame [B + 1]: nonzero where the frame failed the rank test (then its re-flood slot + 1); per slot: the sorted
-	// W1 values of its domain pixels and of the pixels its frame-wide flood pops ([kRefloodSlots][2][kRefloodCap]), the
-	// two counts and the frame + 1 ([kRefloodSlots][4]); per slot and pixel of the frame: the estimated frame-wide pop
-	// position and the upper bound of it ([kRefloodSlots][N][2])
+	// per frame [B + 1]: nonzero where the frame failed the rank test (then its re-flood slot + 1); per slot and list
+	// (0: the W1 values of its domain pixels, 1: of the pixels its frame-wide flood pops): the values as gathered and
+	// grouped by value bucket ([kRefloodSlots][2][kRefloodCap]), the bucket offsets ([kRefloodSlots][2][buckets + 1]);
+	// per slot [8]: the two counts, the frame + 1, unused, and per list the lowest value and the bucket shift; per slot
+	// and pixel of the frame: the estimated frame-wide pop position and its upper bound ([kRefloodSlots][N][2])
 	uint32_t* frameReflood;
-	uint32_t* rfVals; uint32_t* rfInfo; uint32_t* rfPix;
+	uint32_t* rfVals; uint32_t* rfGrp; uint32_t* rfOff; uint32_t* rfInfo; uint32_t* rfPix;
 	uint32_t* frameRegBase; uint32_t* frameCandBase; uint32_t* frameKeep; uint32_t* frameOutBase;
 	// candidates / rows
 	uint32_t capRows;

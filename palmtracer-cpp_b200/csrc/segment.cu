@@ -1222,7 +1222,7 @@ __global__ void SuspectCheck(Workspace ws, int reflood)
 // frame's domain pixels with a higher W1, which the frame-wide flood pops first up to its aging term), the groups
 // follow the frame-wide order, and the test, now with every chain element's own bound
 //   min over e of (W1(e) * 78125 - B(parent(e)) * 512) > W1(z) * 78125 - (A_z - 1) * 512,
-// B(p) = #{W1 >= W1(p) - delta}, proves it. The counts come from the frame's sorted W1 values. A frame failing again
+// B(p) = #{W1 >= W1(p) - delta}, proves it. The counts come from the frame's W1 values grouped by value bucket. A frame failing again
 // (or beyond the slots or the value capacity) is flooded frame-wide.
 
 // Step 1 (one CTA): slots for the frames marked by the rank test, in frame order; the others are routed.
@@ -1231,14 +1231,14 @@ __global__ void __launch_bounds__(kPlanThreads) RefloodPlan(Workspace ws)
 	__shared__ uint32_t next;
 	if (ws.cnt->nreflood == 0) { return; }
 	if (threadIdx.x == 0) { next = 0; }
-	if (threadIdx.x < kRefloodSlots * 4) { ws.rfInfo[threadIdx.x] = 0u; }
+	if (threadIdx.x < kRefloodSlots * 8) { ws.rfInfo[threadIdx.x] = 0u; }
 	__syncthreads();
 	if (threadIdx.x == 0) {
 		for (int f = 0; f < ws.g.B; ++f) {
 			if (ws.frameReflood[f] == 0u) { continue; }
 			if (next < kRefloodSlots && ws.frameRoute[f] == 0u && ws.frameDom[f] <= kRefloodCap) {
 				ws.frameReflood[f] = next + 1u;
-				ws.rfInfo[next * 4 + 2] = static_cast<uint32_t>(f) + 1u;
+				ws.rfInfo[next * 8 + 2] = static_cast<uint32_t>(f) + 1u;
 				++next;
 			}
 			else {
@@ -1278,57 +1278,119 @@ __global__ void RefloodGather(Workspace ws)
 		const uint32_t s = ws.frameReflood[FastDivide(p, ws.g.divN)];
 		if (s == 0u) { continue; }
 		const uint32_t slot = s - 1u, w = __ldg(ws.w1 + p);
-		const uint32_t a = atomicAdd(ws.rfInfo + slot * 4, 1u);
+		const uint32_t a = atomicAdd(ws.rfInfo + slot * 8, 1u);
 		if (a < kRefloodCap) { ws.rfVals[(static_cast<size_t>(slot) * 2) * kRefloodCap + a] = w; }
 		if (Poppable(ws, p)) {
-			const uint32_t b = atomicAdd(ws.rfInfo + slot * 4 + 1, 1u);
+			const uint32_t b = atomicAdd(ws.rfInfo + slot * 8 + 1, 1u);
 			if (b < kRefloodCap) { ws.rfVals[(static_cast<size_t>(slot) * 2 + 1) * kRefloodCap + b] = w; }
 		}
 	}
 }
 
-constexpr int kRfSortThreads = 1024;
+constexpr int kRfBucketThreads = 1024;
+constexpr size_t kRfBucketSmem = kRefloodBuckets * sizeof(uint32_t);
 
-// Step 3 (one CTA per slot): both value lists sorted ascending (bitonic over the next power of two, padded with the
-// largest value), in place in global memory.
-__global__ void __launch_bounds__(kRfSortThreads) RefloodSort(Workspace ws)
+// Step 3 (one CTA per slot and list): the values grouped by bucket (bucket = (value - lowest) >> shift, the shift the
+// smallest that fits the value range in kRefloodBuckets buckets), bucket offsets by a counting pass in shared memory.
+__global__ void __launch_bounds__(kRfBucketThreads) RefloodBucket(Workspace ws)
 {
-	const uint32_t slot = blockIdx.x;
-	if (ws.cnt->nreflood == 0 || ws.rfInfo[slot * 4 + 2] == 0u) { return; }
-	for (int a = 0; a < 2; ++a) {
-		uint32_t* v = ws.rfVals + (static_cast<size_t>(slot) * 2 + a) * kRefloodCap;
-		const uint32_t n = min(ws.rfInfo[slot * 4 + a], kRefloodCap);
-		uint32_t len = 2;
-		while (len < n) { len <<= 1; }
-		for (uint32_t i = n + threadIdx.x; i < len; i += kRfSortThreads) { v[i] = 0xffffffffu; }
-		__syncthreads();
-		for (uint32_t size = 2; size <= len; size <<= 1) {
-			for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
-				for (uint32_t t = threadIdx.x; t < len / 2; t += kRfSortThreads) {
-					const uint32_t lo = 2 * t - (t & (stride - 1)), hi = lo + stride;
-					const bool up = (lo & size) == 0;
-					const uint32_t x = v[lo], y = v[hi];
-					if (up ? (y < x) : (x < y)) {
-						v[lo] = y;
-						v[hi] = x;
-					}
-				}
-				__syncthreads();
-			}
+	extern __shared__ uint32_t hist[];  // [kRefloodBuckets]: counts, then cursors
+	__shared__ uint32_t red[2][kRfBucketThreads / 32];
+	__shared__ uint32_t carry;
+	const uint32_t slot = blockIdx.x >> 1, a = blockIdx.x & 1u;
+	if (ws.cnt->nreflood == 0 || ws.rfInfo[slot * 8 + 2] == 0u) { return; }
+	const int tid = static_cast<int>(threadIdx.x), lane = tid & 31, warp = tid >> 5;
+	const uint32_t* v = ws.rfVals + (static_cast<size_t>(slot) * 2 + a) * kRefloodCap;
+	uint32_t* grp = ws.rfGrp + (static_cast<size_t>(slot) * 2 + a) * kRefloodCap;
+	uint32_t* off = ws.rfOff + (static_cast<size_t>(slot) * 2 + a) * (kRefloodBuckets + 1);
+	const uint32_t n = min(ws.rfInfo[slot * 8 + a], kRefloodCap);
+	// value range
+	uint32_t lo = 0xffffffffu, hi = 0u;
+	for (uint32_t i = tid; i < n; i += kRfBucketThreads) {
+		lo = min(lo, v[i]);
+		hi = max(hi, v[i]);
+	}
+	#pragma unroll
+	for (int d = 16; d > 0; d >>= 1) {
+		lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, d));
+		hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, d));
+	}
+	if (lane == 0) { red[0][warp] = lo; red[1][warp] = hi; }
+	for (uint32_t b = tid; b < kRefloodBuckets; b += kRfBucketThreads) { hist[b] = 0u; }
+	__syncthreads();
+	lo = 0xffffffffu;
+	hi = 0u;
+	for (int w = 0; w < kRfBucketThreads / 32; ++w) {
+		lo = min(lo, red[0][w]);
+		hi = max(hi, red[1][w]);
+	}
+	if (n == 0) { lo = hi = 0u; }
+	uint32_t shift = 0;
+	while (shift < 32 && ((hi - lo) >> shift) >= kRefloodBuckets) { ++shift; }
+	if (tid == 0) {
+		ws.rfInfo[slot * 8 + 4 + 2 * a] = lo;
+		ws.rfInfo[slot * 8 + 5 + 2 * a] = shift;
+		carry = 0;
+	}
+	for (uint32_t i = tid; i < n; i += kRfBucketThreads) { atomicAdd(hist + ((v[i] - lo) >> shift), 1u); }
+	__syncthreads();
+	// exclusive scan of the bucket counts: each thread a run of buckets, then the runs before it
+	constexpr uint32_t kRun = kRefloodBuckets / kRfBucketThreads;
+	uint32_t sum = 0;
+	for (uint32_t k = 0; k < kRun; ++k) { sum += hist[tid * kRun + k]; }
+	uint32_t x = sum;
+	#pragma unroll
+	for (int d = 1; d < 32; d <<= 1) {
+		const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+		if (lane >= d) { x += y; }
+	}
+	if (lane == 31) { red[0][warp] = x; }
+	__syncthreads();
+	if (warp == 0) {
+		uint32_t w = red[0][lane];
+		#pragma unroll
+		for (int d = 1; d < 32; d <<= 1) {
+			const uint32_t y = __shfl_up_sync(0xffffffffu, w, d);
+			if (lane >= d) { w += y; }
 		}
+		red[1][lane] = w;  // inclusive over warps
+	}
+	__syncthreads();
+	uint32_t run = (warp ? red[1][warp - 1] : 0u) + x - sum;
+	for (uint32_t k = 0; k < kRun; ++k) {
+		const uint32_t b = tid * kRun + k;
+		const uint32_t c = hist[b];
+		off[b] = run;
+		hist[b] = run;  // cursor
+		run += c;
+	}
+	if (tid == kRfBucketThreads - 1) { off[kRefloodBuckets] = run; }
+	__syncthreads();
+	for (uint32_t i = tid; i < n; i += kRfBucketThreads) {
+		const uint32_t val = v[i];
+		grp[atomicAdd(hist + ((val - lo) >> shift), 1u)] = val;
 	}
 }
 
-// Entries of the ascending list v[0, n) that are >= x (strict: > x).
-__device__ __forceinline__ uint32_t CountAbove(const uint32_t* v, uint32_t n, uint32_t x, bool strict)
+// Values of list a of the slot that are >= x (strict: > x): the buckets above x's bucket, plus the members of its
+// bucket counted one by one.
+__device__ uint32_t CountAbove(const Workspace& ws, uint32_t slot, uint32_t a, uint32_t x, bool strict)
 {
-	uint32_t lo = 0, hi = n;  // first index whose value is >= x (> x when strict)
-	while (lo < hi) {
-		const uint32_t mid = (lo + hi) >> 1;
-		if (strict ? (v[mid] <= x) : (v[mid] < x)) { lo = mid + 1; }
-		else { hi = mid; }
+	const uint32_t n = min(ws.rfInfo[slot * 8 + a], kRefloodCap);
+	const uint32_t lo = ws.rfInfo[slot * 8 + 4 + 2 * a], shift = ws.rfInfo[slot * 8 + 5 + 2 * a];
+	if (n == 0) { return 0u; }
+	if (x < lo) { return n; }
+	const uint32_t b = shift >= 32 ? 0u : ((x - lo) >> shift);
+	if (b >= kRefloodBuckets) { return 0u; }
+	const uint32_t* off = ws.rfOff + (static_cast<size_t>(slot) * 2 + a) * (kRefloodBuckets + 1);
+	const uint32_t* grp = ws.rfGrp + (static_cast<size_t>(slot) * 2 + a) * kRefloodCap;
+	const uint32_t b0 = off[b], b1 = off[b + 1];
+	uint32_t c = n - b1;
+	for (uint32_t i = b0; i < b1; ++i) {
+		const uint32_t y = grp[i];
+		c += strict ? (y > x ? 1u : 0u) : (y >= x ? 1u : 0u);
 	}
-	return n - lo;
+	return c;
 }
 
 __device__ __forceinline__ uint32_t FrameDelta(const Workspace& ws, int f)
@@ -1351,16 +1413,14 @@ __global__ void RefloodCounts(Workspace ws)
 		const uint32_t s = ws.frameReflood[f];
 		if (s == 0u) { continue; }
 		const uint32_t slot = s - 1u;
-		const uint32_t* all = ws.rfVals + (static_cast<size_t>(slot) * 2) * kRefloodCap;
-		const uint32_t nAll = min(ws.rfInfo[slot * 4], kRefloodCap);
 		const uint32_t delta = FrameDelta(ws, f);
 		uint32_t* out = ws.rfPix + static_cast<size_t>(slot) * static_cast<size_t>(ws.g.N) * 2;
 		for (uint32_t i = lane; i < nPix; i += 32) {
 			const uint32_t p = ws.gPix[off + i];
 			const uint32_t w = __ldg(ws.w1 + p);
 			const size_t local = static_cast<size_t>(p) - static_cast<size_t>(f) * static_cast<size_t>(ws.g.N);
-			out[local * 2] = CountAbove(all, nAll, w, true);
-			out[local * 2 + 1] = CountAbove(all, nAll, w > delta ? w - delta : 0u, false);
+			out[local * 2] = CountAbove(ws, slot, 0, w, true);
+			out[local * 2 + 1] = CountAbove(ws, slot, 0, w > delta ? w - delta : 0u, false);
 		}
 	}
 }
@@ -1489,8 +1549,6 @@ __global__ void __launch_bounds__(kRfWarps * 32) RefloodBox(Workspace ws)
 		__syncwarp();
 		const uint32_t T = ws.frameDom[f];
 		const uint32_t delta = FrameDelta(ws, f);
-		const uint32_t* pop = ws.rfVals + (static_cast<size_t>(slot) * 2 + 1) * kRefloodCap;
-		const uint32_t nPop = min(ws.rfInfo[slot * 4 + 1], kRefloodCap);
 		bool exact = true;
 		for (int i = lane; i < bw * bh; i += 32) {
 			if (!(sm.flag[i] & 2u) || sm.lab[i] == 0) { continue; }
@@ -1516,7 +1574,7 @@ __global__ void __launch_bounds__(kRfWarps * 32) RefloodBox(Workspace ws)
 							}
 						}
 						const unsigned long long x = static_cast<unsigned long long>(zmax) + delta;
-						az = (x < 0xffffffffull ? static_cast<long long>(CountAbove(pop, nPop, static_cast<uint32_t>(x), true)) : 0ll) + 1;
+						az = (x < 0xffffffffull ? static_cast<long long>(CountAbove(ws, slot, 1, static_cast<uint32_t>(x), true)) : 0ll) + 1;
 					}
 					if (!(mi > static_cast<long long>(sm.w1[j]) * 78125ll - (az - 1) * 512ll)) { exact = false; }
 				}
@@ -1680,7 +1738,10 @@ bool LaunchSegment(const Workspace& ws, double ratio, int strict, uint32_t maxPo
 			SuspectCheck<<<64, kThreads, 0, st>>>(ws, fuse ? 0 : 1);
 			RefloodPlan<<<1, kPlanThreads, 0, st>>>(ws);
 			RefloodGather<<<kGrid, kThreads, 0, st>>>(ws);
-			RefloodSort<<<kRefloodSlots, kRfSortThreads, 0, st>>>(ws);
+			static const bool bucketSmem = PTB_CUDA(cudaFuncSetAttribute(RefloodBucket, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			                                                             static_cast<int>(kRfBucketSmem)));
+			ok = ok && bucketSmem;
+			RefloodBucket<<<kRefloodSlots * 2, kRfBucketThreads, kRfBucketSmem, st>>>(ws);
 			RefloodCounts<<<kGrid, kThreads, 0, st>>>(ws);
 			RefloodBox<<<kGrid, kRfWarps * 32, 0, st>>>(ws);
 			CountLaunch(8);

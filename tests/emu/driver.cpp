@@ -95,7 +95,9 @@ int main(int argc, char** argv)
 	ws.frameReflood = Alloc<uint32_t>(B + 1);
 	for (int f = 0; f <= B; ++f) { ws.frameDom[f] = ws.frameSeeds[f] = ws.frameRoute[f] = ws.frameSuspect[f] = ws.frameReflood[f] = 0; }
 	ws.rfVals = Alloc<uint32_t>(static_cast<size_t>(kRefloodSlots) * 2 * kRefloodCap);
-	ws.rfInfo = Alloc<uint32_t>(kRefloodSlots * 4);
+	ws.rfGrp = Alloc<uint32_t>(static_cast<size_t>(kRefloodSlots) * 2 * kRefloodCap);
+	ws.rfOff = Alloc<uint32_t>(static_cast<size_t>(kRefloodSlots) * 2 * (kRefloodBuckets + 1));
+	ws.rfInfo = Alloc<uint32_t>(kRefloodSlots * 8);
 	ws.rfPix = Alloc<uint32_t>(static_cast<size_t>(kRefloodSlots) * g.N * 2);
 	ws.suspect = Alloc<uint4>(kSuspectCap); ws.capSuspect = kSuspectCap;
 	ws.rankOrder = Alloc<uint32_t>(kSuspectCap); ws.rankSlotOff = Alloc<uint32_t>(kRankSlots + 1);
@@ -155,10 +157,10 @@ int main(int argc, char** argv)
 		fprintf(stderr, "rank test: slots %u reflood %u routed %u\n", ws.cnt->nslots, ws.cnt->nreflood, ws.cnt->nroute);
 		emu::Launch(one, t1024, RefloodPlan, ws);
 		emu::Launch(one, t256, RefloodGather, ws);
-		emu::Launch(dim3(kRefloodSlots), t1024, RefloodSort, ws);
+		emu::Launch(dim3(kRefloodSlots * 2), t1024, RefloodBucket, ws);
 		emu::Launch(one, t256, RefloodCounts, ws);
 		emu::Launch(one, dim3(kRfWarps * 32), RefloodBox, ws);
-		fprintf(stderr, "reflood: routed %u counts %u %u\n", ws.cnt->nroute, ws.rfInfo[0], ws.rfInfo[1]);
+		fprintf(stderr, "reflood: routed %u\n", ws.cnt->nroute);
 		for (uint32_t i = 0; i < std::min(ws.cnt->nsuspect, 8u); ++i) {
 			const uint4 r = ws.suspect[i];
 			fprintf(stderr, "  pair %u: f %u c %u w1z %u zmax %u counts %u %u\n", i, r.x, r.y, r.z, r.w, ws.rankCount[2 * i], ws.rankCount[2 * i + 1]);

@@ -32,6 +32,8 @@ def emulator(tmp_path_factory):
     src = src[:cut] + src[end:]
     common = os.path.join(ROOT, "palmtracer-cpp_b200", "csrc", "pt_common.cuh")
     src = re.sub(r'#include "pt_common.cuh"', '#include "%s"' % common, src)
+    # dynamic shared memory: a static buffer (blocks run one at a time)
+    src = re.sub(r'extern __shared__ (\w+) (\w+)\[\];', r'static \1 \2[65536];', src)
     open(d / "segment_emu.inc", "w").write(src)
     exe = d / "emu"
     cmd = ["g++", "-std=c++20", "-O2", "-g", "-fsanitize=address", "-pthread", "-Wno-attributes", "-I" + CUDA_INCLUDE,
