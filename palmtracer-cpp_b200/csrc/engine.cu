@@ -13,6 +13,7 @@
 #include <iostream>
 #include <mutex>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 namespace ptb {
@@ -166,6 +167,36 @@ uint32_t IndepBound(int H, int W) { return static_cast<uint32_t>(((H + 1) / 2)) 
 
 }  // namespace
 
+// Host memcpy over several threads (pageable buffers go through pinned staging; one thread copies about 10 GB/s).
+void ParallelCopy(void* dst, const void* src, size_t bytes)
+{
+	const size_t piece = 32ull << 20;
+	const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+	const unsigned n = static_cast<unsigned>(std::min<size_t>(hw, (bytes + piece - 1) / piece));
+	if (n <= 1) {
+		std::memcpy(dst, src, bytes);
+		return;
+	}
+	std::vector<std::thread> th;
+	const size_t each = (bytes / n + 63) & ~static_cast<size_t>(63);
+	for (unsigned i = 0; i < n; ++i) {
+		const size_t a = std::min(bytes, each * i), b = std::min(bytes, each * (i + 1));
+		if (b > a) { th.emplace_back([=] { std::memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, b - a); }); }
+	}
+	for (auto& t : th) { t.join(); }
+}
+
+// True for host memory that is neither page-locked nor registered with CUDA.
+bool Pageable(const void* p)
+{
+	cudaPointerAttributes a{};
+	if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+		cudaGetLastError();
+		return true;
+	}
+	return a.type == cudaMemoryTypeUnregistered;
+}
+
 // Bytes of workspace for B frames of H x W with `rowsCap` fit rows.
 static size_t PlanWorkspace(Workspace& ws, int H, int W, int B, uint32_t rowsCap, char* base)
 {
@@ -278,6 +309,9 @@ Engine::~Engine()
 	if (pool_) { cudaFree(pool_); }
 	if (img_) { cudaFree(img_); }
 	if (hostStage_) { cudaFreeHost(hostStage_); }
+	for (void* h : hostOut_) {
+		if (h) { cudaFreeHost(h); }
+	}
 	if (spline_) { cudaFree(spline_); }
 	if (fallbacks_) { cudaFree(fallbacks_); }
 	if (evalDev_) { cudaFree(evalDev_); }
@@ -305,7 +339,8 @@ bool Engine::Init()
 	if (!PTB_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming))) { return false; }
 	if (!PTB_CUDA(cudaMallocHost(&hostCnt_, 2 * sizeof(Counters)))) { return false; }
 	if (!PTB_CUDA(cudaMalloc(&rowBase_, sizeof(unsigned long long)))) { return false; }
-	for (cudaEvent_t* e : {&h2d_[0], &h2d_[1], &h2d_[2], &imgFree_[0], &imgFree_[1], &imgFree_[2], &done_[0], &done_[1], &d2h_[0], &d2h_[1]}) {
+	for (cudaEvent_t* e : {&h2d_[0], &h2d_[1], &h2d_[2], &imgFree_[0], &imgFree_[1], &imgFree_[2], &done_[0], &done_[1], &d2h_[0], &d2h_[1],
+	                       &outEv_[0], &outEv_[1]}) {
 		if (!PTB_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming))) { return false; }
 	}
 	for (auto& e : ev_) {
@@ -678,6 +713,32 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 	if (!UploadSpline(fp, spline)) { return -1; }
 	const int H = static_cast<int>(height), W = static_cast<int>(width);
 	const uint32_t maxPoints = static_cast<uint32_t>(std::min<uint64_t>(perPlane, 0xffffffffu));
+	// pageable host buffers: the frames are copied into pinned staging by several host threads (a page source), and
+	// the rows reach the caller's buffer through pinned staging the same way; a copy from or to pageable memory would
+	// otherwise go through the driver's single staging buffer and block this thread
+	PageSource pageableIn;
+	if (!source && !inputOnDevice && !outputOnDevice && Pageable(input)) {
+		const size_t frameElems = static_cast<size_t>(H) * W;
+		pageableIn = [input, frameElems](uint64_t z0, uint64_t n, uint16_t* dst) {
+			ParallelCopy(dst, input + z0 * frameElems, static_cast<size_t>(n) * frameElems * sizeof(uint16_t));
+			return true;
+		};
+		source = &pageableIn;
+	}
+	const bool stageOut = !outputOnDevice && Pageable(output);
+	struct Pending {
+		double* dst = nullptr;
+		size_t bytes = 0;
+	} pending[2];
+	// the staged rows of buffer b into the caller's buffer (after their copy from the device)
+	auto flushOut = [&](int b) {
+		if (!pending[b].dst) { return true; }
+		if (!PTB_CUDA(cudaEventSynchronize(outEv_[b]))) { return false; }
+		ParallelCopy(pending[b].dst, hostOut_[b], pending[b].bytes);
+		pending[b].dst = nullptr;
+		return true;
+	};
+	uint64_t outCopies = 0;
 	int B = 1, slots = 1;
 	ChunkPlan(H, W, planes, maxPoints, B, slots);
 	const uint32_t rowsCap = static_cast<uint32_t>(std::min<uint64_t>(static_cast<uint64_t>(B) * maxPoints, 0xffffffffu));
@@ -739,8 +800,23 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 		const long long n = CompleteChunk(slot, &truncated);
 		if (n < 0) { return false; }
 		if (!outputOnDevice && n > 0) {
-			if (!PTB_CUDA(cudaMemcpyAsync(output + rows * kCols, outSlot[slot], static_cast<size_t>(n) * kCols * sizeof(double),
-			                              cudaMemcpyDeviceToHost, copyOut_))) {
+			const size_t bytes = static_cast<size_t>(n) * kCols * sizeof(double);
+			if (stageOut) {
+				const int b = static_cast<int>(outCopies++ & 1);
+				if (!flushOut(b)) { return false; }
+				if (hostOutBytes_[b] < bytes) {
+					if (hostOut_[b]) { cudaFreeHost(hostOut_[b]); hostOut_[b] = nullptr; hostOutBytes_[b] = 0; }
+					if (!PTB_CUDA(cudaMallocHost(&hostOut_[b], bytes))) { return false; }
+					hostOutBytes_[b] = bytes;
+				}
+				if (!PTB_CUDA(cudaMemcpyAsync(hostOut_[b], outSlot[slot], bytes, cudaMemcpyDeviceToHost, copyOut_)) ||
+				    !PTB_CUDA(cudaEventRecord(outEv_[b], copyOut_))) {
+					return false;
+				}
+				pending[b].dst = output + rows * kCols;
+				pending[b].bytes = bytes;
+			}
+			else if (!PTB_CUDA(cudaMemcpyAsync(output + rows * kCols, outSlot[slot], bytes, cudaMemcpyDeviceToHost, copyOut_))) {
 				return false;
 			}
 		}
@@ -772,6 +848,7 @@ long long Engine::Localize(const uint16_t* input, bool inputOnDevice, double* ou
 	// work ordered after this call on the first compute stream also follows the second's
 	if (ok && slots > 1) { ok = PTB_CUDA(cudaStreamWaitEvent(stream_, done_[1], 0)); }
 	ok = ok && PTB_CUDA(cudaStreamSynchronize(copy_)) && PTB_CUDA(cudaStreamSynchronize(copyOut_));
+	ok = ok && flushOut(static_cast<int>(outCopies & 1)) && flushOut(static_cast<int>((outCopies + 1) & 1));
 	if (!ok) {
 		cudaStreamSynchronize(stream_);
 		cudaStreamSynchronize(stream1_);

@@ -161,6 +161,9 @@ private:
 	size_t imgBytes_ = 0;
 	void* hostStage_ = nullptr;               // pinned frame staging of page sources (two slots)
 	size_t hostStageBytes_ = 0;
+	void* hostOut_[2] = {};                   // pinned row staging for pageable output (two buffers)
+	size_t hostOutBytes_[2] = {};
+	cudaEvent_t outEv_[2] = {};               // a staged row copy reached hostOut_
 	void* spline_ = nullptr;
 	std::vector<double> splineIn_;            // the call's spline table as given (reused between calls)
 	std::vector<double> splineCache_;         // the table behind spline_ (its upload is skipped when unchanged)
