@@ -1,6 +1,7 @@
 // CPU emulation shim for CUDA kernels: blocks run one after another, each thread of a block is a std::thread.
 #pragma once
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <barrier>
 #include <cmath>
 #include <cstdint>
@@ -66,6 +67,7 @@ inline unsigned __ballot_sync(unsigned, int pred)
 }
 inline int __any_sync(unsigned m, int pred) { return __ballot_sync(m, pred) != 0; }
 inline int __popc(unsigned v) { return __builtin_popcount(v); }
+inline unsigned __vimax3_u32(unsigned a, unsigned b, unsigned c) { return std::max(a, std::max(b, c)); }
 inline int __ffs(int v) { return __builtin_ffs(v); }
 inline int __clz(int v) { return v == 0 ? 32 : __builtin_clz(static_cast<unsigned>(v)); }
 template <class T> inline T __ldg(const T* p) { return *p; }
