@@ -68,8 +68,13 @@ int main(int argc, char** argv)
 	ws.frameSeeds = Alloc<uint32_t>(B + 1, 0);
 #ifdef PTB_EMU_STREAM
 	const int strips = (W + kStripOut - 1) / kStripOut;
-	emu::Launch(dim3((strips + kSWarps - 1) / kSWarps, (H + kRowsOut - 1) / kRowsOut, B), dim3(kSWarps * 32),
-	            DetectStream, static_cast<const uint16_t*>(img), ws, thr);
+	const dim3 grid((strips + kSWarps - 1) / kSWarps, (H + kRowsOut - 1) / kRowsOut, B);
+	if ((W & 3) == 0 && (reinterpret_cast<uintptr_t>(img) & 7) == 0) {  // the host's choice (LaunchDetectStream)
+		emu::Launch(grid, dim3(kSWarps * 32), DetectStream<true>, static_cast<const uint16_t*>(img), ws, thr);
+	}
+	else {
+		emu::Launch(grid, dim3(kSWarps * 32), DetectStream<false>, static_cast<const uint16_t*>(img), ws, thr);
+	}
 #else
 	emu::Launch(dim3((W + TX - 1) / TX, (H + TY - 1) / TY, B), dim3(kThreads), DetectKernel,
 	            static_cast<const uint16_t*>(img), ws, thr);

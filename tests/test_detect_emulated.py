@@ -30,6 +30,7 @@ def _kernels_only(src, cuts):
         b = src.index(stop, a)
         src = src[:a] + src[b:]
     src = src.replace('#include "pt_common.cuh"', '#include "%s"' % os.path.join(CSRC, "pt_common.cuh"))
+    src = src.replace('#include "async_copy.cuh"', '#include "async_copy_emu.h"')  # copies at once, checks alignment
     # dynamic shared memory: a static buffer (blocks run one at a time)
     return re.sub(r'extern __shared__ (__align__\(\d+\) )?([\w ]+?) (\w+)\[\];', r'static \1\2 \3[262144];', src)
 
@@ -42,7 +43,8 @@ def emulators(tmp_path_factory):
     for name, fname, cuts, flag in (
             ("tiles", "detect.cu", [("bool ConfigureSmem()", "}  // namespace\n"),
                                     ("long long ThresholdFixed(", "}  // namespace ptb")], None),
-            ("stream", "detect_stream.cu", [("bool StreamDetectFits(", "}  // namespace ptb")], "-DPTB_EMU_STREAM")):
+            ("stream", "detect_stream.cu", [("template <bool kVec> bool LaunchStream(", "}  // namespace\n"),
+                                            ("bool StreamDetectFits(", "}  // namespace ptb")], "-DPTB_EMU_STREAM")):
         d = tmp_path_factory.mktemp("emu_" + name)
         open(d / "detect_emu.inc", "w").write(_kernels_only(open(os.path.join(CSRC, fname)).read(), cuts))
         exe = d / "emu_detect"
@@ -104,7 +106,9 @@ CASES = [  # (H, W, frames, seed)
     (300, 250, 1, 2),   # three strips, the last of 26 columns; odd width: scalar loads
     (140, 232, 2, 3),   # width a multiple of 4: the middle strip takes the vector loads
     (16, 336, 1, 4),    # 16 rows, three full strips
-    (129, 225, 1, 5),   # last strip of one column, last row block of one row
+    (129, 225, 1, 5),   # last strip of one column
+    (270, 116, 1, 6),   # vector loads, a last strip of 4 columns, two row blocks (the second of 14 rows)
+    (257, 113, 1, 7),   # a last row block of one row, a last strip of one column
 ]
 
 
