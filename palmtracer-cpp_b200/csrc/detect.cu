@@ -18,7 +18,6 @@
 // Layout: a 128 x 28 output tile per CTA of 8 warps (the Wavelett planes: every stage loops rows over warps and
 // columns over lanes; shared buffers are reused across stages, input -> V1, T1 -> T2).
 #include <algorithm>
-#include <cstdlib>
 #include <cmath>
 
 #include "pt_common.cuh"
@@ -411,12 +410,8 @@ long long ThresholdFixed(double thr)
 	return static_cast<long long>(t);
 }
 
-bool StreamDetectFits(int H, int W);
-bool LaunchDetectStream(const Workspace& ws, double thr, cudaStream_t st);
-
 bool LaunchDetect(const Workspace& ws, double thr, cudaStream_t st)
 {
-	if (std::getenv("PTB_DETECT_TILES") == nullptr && StreamDetectFits(ws.g.H, ws.g.W)) { return LaunchDetectStream(ws, thr, st); }
 	if (!ConfigureSmem()) { return false; }
 	const dim3 grid((ws.g.W + TX - 1) / TX, (ws.g.H + TY - 1) / TY, ws.g.B);
 	DetectKernel<<<grid, kThreads, kDetectWords * sizeof(uint32_t), st>>>(ws.img, ws, ThresholdFixed(thr));

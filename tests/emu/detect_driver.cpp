@@ -1,6 +1,6 @@
-// Runs one detection kernel on a stack of frames on the CPU (each CUDA thread a host thread, shim.h): DetectKernel of
-// detect.cu, or DetectStream of detect_stream.cu when built with -DPTB_EMU_STREAM. Every device array is a separate
-// allocation, so AddressSanitizer reports any out-of-bounds access. Test harness only.
+// Runs the detection kernel (DetectKernel of detect.cu) on a stack of frames on the CPU (each CUDA thread a host
+// thread, shim.h). Every device array is a separate allocation, so AddressSanitizer reports any out-of-bounds access.
+// Test harness only.
 // Usage: emu_detect <in> <out>; in: int32 H, W, B, int64 threshold (2^-16 units), B * H * W uint16 pixels;
 // out: uint32 ndom, nseed, overflow, B per-frame domain counts, B per-frame seed counts, P code bytes, P uint32 W1
 // (as written: only domain pixels are defined), then the domain list and the seed list, each sorted.
@@ -66,19 +66,8 @@ int main(int argc, char** argv)
 	ws.cnt = Alloc<Counters>(1, 0);
 	ws.frameDom = Alloc<uint32_t>(B + 1, 0);
 	ws.frameSeeds = Alloc<uint32_t>(B + 1, 0);
-#ifdef PTB_EMU_STREAM
-	const int strips = (W + kStripOut - 1) / kStripOut;
-	const dim3 grid((strips + kSWarps - 1) / kSWarps, (H + kRowsOut - 1) / kRowsOut, B);
-	if ((W & 3) == 0 && (reinterpret_cast<uintptr_t>(img) & 7) == 0) {  // the host's choice (LaunchDetectStream)
-		emu::Launch(grid, dim3(kSWarps * 32), DetectStream<true>, static_cast<const uint16_t*>(img), ws, thr);
-	}
-	else {
-		emu::Launch(grid, dim3(kSWarps * 32), DetectStream<false>, static_cast<const uint16_t*>(img), ws, thr);
-	}
-#else
 	emu::Launch(dim3((W + TX - 1) / TX, (H + TY - 1) / TY, B), dim3(kThreads), DetectKernel,
 	            static_cast<const uint16_t*>(img), ws, thr);
-#endif
 	const uint32_t nd = std::min(ws.cnt->ndom, ws.capDom), ns = std::min(ws.cnt->nseed, ws.capSeed);
 	std::sort(ws.dom, ws.dom + nd);
 	std::sort(ws.seeds, ws.seeds + ns);

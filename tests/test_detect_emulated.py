@@ -1,13 +1,13 @@
-"""The two detection kernels run on the CPU under AddressSanitizer: same outputs, and the oracle's W1 and threshold.
+"""The detection kernel runs on the CPU under AddressSanitizer against the oracle's W1, threshold and local maxima.
 
-tests/emu/shim.h runs every CUDA thread of a block as a host thread and tests/emu/detect_driver.cpp runs one detection
-kernel on a stack of frames, each device array its own heap allocation: DetectKernel (detect.cu, 128 x 28 tiles) and
-DetectStream (detect_stream.cu, a warp per 112-column strip sweeping 128 rows). Both must write the same code bytes,
-the same W1 on domain pixels, the same domain and seed lists and per-frame counts, and these must equal the oracle's
-W1 (ATrous.cpp:23-80 restated in oracle/pt_oracle.cpp) thresholded strictly and above 1e-8, with seeds at the pixels
-not below any 3 x 3 neighbour (Segmentation2D.cpp:294-333, the frame surrounded by zeros). The shapes cover one strip,
-ragged last strips and row blocks, unaligned and aligned widths (the vector-load path), frames 16 rows high and
-several frames; threshold 0 makes most pixels domain, so the per-warp list stages fill and move many times.
+tests/emu/shim.h runs every CUDA thread of a block as a host thread and tests/emu/detect_driver.cpp runs DetectKernel
+(detect.cu, 128 x 28 tiles) on a stack of frames, each device array its own heap allocation, so that an out-of-bounds
+access anywhere in it aborts. Its code bytes, the W1 of domain pixels, the domain and seed lists and the per-frame
+counts must equal the oracle's W1 (ATrous.cpp:23-80 restated in oracle/pt_oracle.cpp) thresholded strictly and above
+1e-8, with seeds at the pixels not below any 3 x 3 neighbour (Segmentation2D.cpp:294-333, the frame surrounded by
+zeros). The shapes cover ragged last tiles in both directions, widths that do and do not allow the 16-byte staging
+loads, frames smaller than the halo and several frames; the stacks are full-range noise (sums up to the 2^32 limit
+of the level-2 taps) and C2 frames; threshold 0 makes most pixels domain.
 """
 import os
 import re
@@ -30,32 +30,24 @@ def _kernels_only(src, cuts):
         b = src.index(stop, a)
         src = src[:a] + src[b:]
     src = src.replace('#include "pt_common.cuh"', '#include "%s"' % os.path.join(CSRC, "pt_common.cuh"))
-    src = src.replace('#include "async_copy.cuh"', '#include "async_copy_emu.h"')  # copies at once, checks alignment
     # dynamic shared memory: a static buffer (blocks run one at a time)
     return re.sub(r'extern __shared__ (__align__\(\d+\) )?([\w ]+?) (\w+)\[\];', r'static \1\2 \3[262144];', src)
 
 
 @pytest.fixture(scope="module")
-def emulators(tmp_path_factory):
+def emulator(tmp_path_factory):
     if shutil.which("g++") is None or not os.path.exists(os.path.join(CUDA_INCLUDE, "cuda_runtime.h")):
         pytest.skip("g++ or the CUDA headers are missing")
-    exes = {}
-    for name, fname, cuts, flag in (
-            ("tiles", "detect.cu", [("bool ConfigureSmem()", "}  // namespace\n"),
-                                    ("long long ThresholdFixed(", "}  // namespace ptb")], None),
-            ("stream", "detect_stream.cu", [("template <bool kVec> bool LaunchStream(", "}  // namespace\n"),
-                                            ("bool StreamDetectFits(", "}  // namespace ptb")], "-DPTB_EMU_STREAM")):
-        d = tmp_path_factory.mktemp("emu_" + name)
-        open(d / "detect_emu.inc", "w").write(_kernels_only(open(os.path.join(CSRC, fname)).read(), cuts))
-        exe = d / "emu_detect"
-        cmd = ["g++", "-std=c++20", "-O2", "-g", "-fsanitize=address", "-pthread", "-Wno-attributes",
-               "-I" + CUDA_INCLUDE, "-I" + str(d), "-I" + os.path.join(HERE, "emu")]
-        cmd += [flag] if flag else []
-        cmd += [os.path.join(HERE, "emu", "detect_driver.cpp"), "-o", str(exe)]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        assert r.returncode == 0, r.stderr[-3000:]
-        exes[name] = exe
-    return exes
+    d = tmp_path_factory.mktemp("emu_detect")
+    cuts = [("bool ConfigureSmem()", "}  // namespace\n"), ("long long ThresholdFixed(", "}  // namespace ptb")]
+    open(d / "detect_emu.inc", "w").write(_kernels_only(open(os.path.join(CSRC, "detect.cu")).read(), cuts))
+    exe = d / "emu_detect"
+    cmd = ["g++", "-std=c++20", "-O2", "-g", "-fsanitize=address", "-pthread", "-Wno-attributes",
+           "-I" + CUDA_INCLUDE, "-I" + str(d), "-I" + os.path.join(HERE, "emu"),
+           os.path.join(HERE, "emu", "detect_driver.cpp"), "-o", str(exe)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    return exe
 
 
 def _run(exe, stack, thr_fixed):
@@ -101,34 +93,39 @@ def _expected(orc, stack, thr_fixed):
     return np.stack(code).reshape(-1), np.stack(w1s).reshape(-1).astype(np.uint32)
 
 
+def _thresholds(orc, stack):
+    import synth
+    base = synth.mad_threshold(orc.planes(stack[0])[1])
+    return int(np.floor(base * 65536)), int(np.floor(0.3 * base * 65536)), 0, -5
+
+
 CASES = [  # (H, W, frames, seed)
-    (130, 112, 2, 1),   # exactly one strip, two row blocks (the second of 2 rows)
-    (300, 250, 1, 2),   # three strips, the last of 26 columns; odd width: scalar loads
-    (140, 232, 2, 3),   # width a multiple of 4: the middle strip takes the vector loads
-    (16, 336, 1, 4),    # 16 rows, three full strips
-    (129, 225, 1, 5),   # last strip of one column
-    (270, 116, 1, 6),   # vector loads, a last strip of 4 columns, two row blocks (the second of 14 rows)
-    (257, 113, 1, 7),   # a last row block of one row, a last strip of one column
+    (130, 112, 2, 1),   # a last tile row of 18 rows, one tile column short of full
+    (300, 250, 1, 2),   # width not a multiple of 8: clamped 2-byte staging loads everywhere
+    (60, 400, 2, 3),    # width a multiple of 8: the interior tile column stages with 16-byte loads
+    (16, 336, 1, 4),    # one short tile row
+    (29, 129, 1, 5),    # one row and one column past full tiles
+    (3, 17, 2, 6),      # frames smaller than the 7-pixel halo in both directions
+    (257, 113, 1, 7),   # a last tile row of 5 rows
 ]
 
 
 @pytest.mark.parametrize("case", CASES, ids=["x".join(map(str, c[:3])) for c in CASES])
-def test_stream_detection_matches_tiles_and_oracle(emulators, orc, case):
+def test_emulated_detection_matches_oracle(emulator, orc, case):
     import synth
     h, w, b, seed = case
-    stack, _ = synth.stack("c2", frames=b, seed=seed, size=(h, w))
-    base = synth.mad_threshold(orc.planes(stack[0])[1])
-    for thr in (int(np.floor(base * 65536)), int(np.floor(0.3 * base * 65536)), 0, -5):
+    rng = np.random.default_rng(seed)
+    # full-range noise (intermediate sums up to the 2^32 limit of V2) on every shape, C2 frames where they fit
+    stacks = [rng.integers(0, 65536, size=(b, h, w), dtype=np.uint16)]
+    if min(h, w) >= 64:
+        stacks.append(synth.stack("c2", frames=b, seed=seed, size=(h, w))[0])
+    for stack, thr in ((st, t) for st in stacks for t in _thresholds(orc, st)):
         want_code, want_w1 = _expected(orc, stack, thr)
-        got = {k: _run(exe, stack, thr) for k, exe in emulators.items()}
-        for name, g in got.items():
-            assert g["overflow"] == 0, name
-            assert np.array_equal(g["code"], want_code), (name, thr, int(np.sum(g["code"] != want_code)))
-            assert np.array_equal(g["w1"], want_w1), (name, thr)
-            dom_idx = np.flatnonzero(want_code & 1).astype(np.uint32)
-            seed_idx = np.flatnonzero(want_code & 2).astype(np.uint32)
-            assert np.array_equal(g["dom"], dom_idx), name
-            assert np.array_equal(g["seeds"], seed_idx), name
-            per = (want_code.reshape(b, -1) & 1).sum(axis=1)
-            assert np.array_equal(g["fdom"], per), name
-            assert np.array_equal(g["fseed"], ((want_code.reshape(b, -1) & 2) != 0).sum(axis=1)), name
+        g = _run(emulator, stack, thr)
+        assert g["overflow"] == 0
+        assert np.array_equal(g["code"], want_code), (thr, int(np.sum(g["code"] != want_code)))
+        assert np.array_equal(g["w1"], want_w1), thr
+        assert np.array_equal(g["dom"], np.flatnonzero(want_code & 1).astype(np.uint32)), thr
+        assert np.array_equal(g["seeds"], np.flatnonzero(want_code & 2).astype(np.uint32)), thr
+        assert np.array_equal(g["fdom"], (want_code.reshape(b, -1) & 1).sum(axis=1)), thr
+        assert np.array_equal(g["fseed"], ((want_code.reshape(b, -1) & 2) != 0).sum(axis=1)), thr
