@@ -277,6 +277,7 @@ static size_t PlanWorkspace(Workspace& ws, int H, int W, int B, uint32_t rowsCap
 	take(ws.rfOff, static_cast<size_t>(kRefloodSlots) * 2 * (kRefloodBuckets + 1));
 	take(ws.rfInfo, static_cast<size_t>(kRefloodSlots) * 8);
 	take(ws.rfPix, static_cast<size_t>(kRefloodSlots) * static_cast<size_t>(g.N) * 2);
+	take(ws.rfGroups, capComp);
 	take(ws.suspect, kSuspectCap);
 	take(ws.rankOrder, kSuspectCap);
 	take(ws.rankSlotOff, kRankSlots + 1);

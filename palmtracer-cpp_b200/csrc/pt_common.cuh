@@ -78,6 +78,7 @@ struct Counters {
 	uint32_t nsuspect;  // boundary pairs that failed the flood's first exactness test (kept for the rank test)
 	uint32_t nslots;    // frames given the rank test
 	uint32_t nreflood;  // frames that failed the rank test (flooded again with estimated frame-wide aging)
+	uint32_t nrfgroup;  // multi-label groups of the frames given a re-flood slot (listed in rfGroups)
 };
 
 // One fit input: a segmentation candidate (x_, y_, intensity_, surf_ of SegmentationInfo) or a caller position.
@@ -216,9 +217,10 @@ struct Workspace {
 	// (0: the W1 values of its domain pixels, 1: of the pixels its frame-wide flood pops): the values as gathered and
 	// grouped by value bucket ([kRefloodSlots][2][kRefloodCap]), the bucket offsets ([kRefloodSlots][2][buckets + 1]);
 	// per slot [8]: the two counts, the frame + 1, unused, and per list the lowest value and the bucket shift; per slot
-	// and pixel of the frame: the estimated frame-wide pop position and its upper bound ([kRefloodSlots][N][2])
+	// and pixel of the frame: the estimated frame-wide pop position and its upper bound ([kRefloodSlots][N][2]); the
+	// multi-label groups of the slotted frames ([capComp])
 	uint32_t* frameReflood;
-	uint32_t* rfVals; uint32_t* rfGrp; uint32_t* rfOff; uint32_t* rfInfo; uint32_t* rfPix;
+	uint32_t* rfVals; uint32_t* rfGrp; uint32_t* rfOff; uint32_t* rfInfo; uint32_t* rfPix; uint32_t* rfGroups;
 	uint32_t* frameRegBase; uint32_t* frameCandBase; uint32_t* frameKeep; uint32_t* frameOutBase;
 	// candidates / rows
 	uint32_t capRows;

@@ -1268,22 +1268,61 @@ __device__ __forceinline__ bool Poppable(const Workspace& ws, uint32_t p)
 	return false;
 }
 
-// Step 2: the W1 values of the slotted frames' domain pixels (and of their poppable pixels), over the domain list.
+// Step 2: the W1 values of the slotted frames' domain pixels (and of their poppable pixels), read from the frames'
+// code bytes, 16 pixels per thread with one atomic per warp and list; and the list of the slotted frames'
+// multi-label groups, which the next steps walk instead of every group of the chunk.
 __global__ void RefloodGather(Workspace ws)
 {
 	if (ws.cnt->nreflood == 0) { return; }
-	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
-	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-		const uint32_t p = ws.dom[i];
-		const uint32_t s = ws.frameReflood[FastDivide(p, ws.g.divN)];
-		if (s == 0u) { continue; }
-		const uint32_t slot = s - 1u, w = __ldg(ws.w1 + p);
-		const uint32_t a = atomicAdd(ws.rfInfo + slot * 8, 1u);
-		if (a < kRefloodCap) { ws.rfVals[(static_cast<size_t>(slot) * 2) * kRefloodCap + a] = w; }
-		if (Poppable(ws, p)) {
-			const uint32_t b = atomicAdd(ws.rfInfo + slot * 8 + 1, 1u);
-			if (b < kRefloodCap) { ws.rfVals[(static_cast<size_t>(slot) * 2 + 1) * kRefloodCap + b] = w; }
+	const int lane = threadIdx.x & 31;
+	const uint32_t N = static_cast<uint32_t>(ws.g.N);
+	const uint32_t stride = gridDim.x * blockDim.x;  // whole warps
+	// 16-pixel runs per frame, rounded up to whole warps: a warp never spans two slots, so it takes every branch below
+	// as one
+	const uint32_t per = ((N + 15u) / 16u + 31u) & ~31u;
+	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < kRefloodSlots * per; t += stride) {
+		const uint32_t slot = t / per, q = t - slot * per;
+		const uint32_t f1 = ws.rfInfo[slot * 8 + 2];  // frame + 1 (0: the slot is unused)
+		if (f1 == 0u) { continue; }
+		const uint32_t p0 = (f1 - 1u) * N;
+		uint32_t dmask = 0, pmask = 0;
+		for (uint32_t k = 0; k < 16u && q * 16u + k < N; ++k) {
+			const uint32_t p = p0 + q * 16u + k;
+			if (!(__ldg(ws.code + p) & kDomain)) { continue; }
+			dmask |= 1u << k;
+			if (Poppable(ws, p)) { pmask |= 1u << k; }
 		}
+		// both lists' positions from one scan (domain count in the low half, poppable count in the high half)
+		const uint32_t c = static_cast<uint32_t>(__popc(dmask)) | (static_cast<uint32_t>(__popc(pmask)) << 16);
+		uint32_t x = c;
+		#pragma unroll
+		for (int d = 1; d < 32; d <<= 1) {
+			const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+			if (lane >= d) { x += y; }
+		}
+		uint32_t b0 = 0, b1 = 0;
+		if (lane == 31) {
+			b0 = (x & 0xffffu) ? atomicAdd(ws.rfInfo + slot * 8, x & 0xffffu) : 0u;
+			b1 = (x >> 16) ? atomicAdd(ws.rfInfo + slot * 8 + 1, x >> 16) : 0u;
+		}
+		b0 = __shfl_sync(0xffffffffu, b0, 31) + ((x - c) & 0xffffu);
+		b1 = __shfl_sync(0xffffffffu, b1, 31) + ((x - c) >> 16);
+		uint32_t* vals = ws.rfVals + static_cast<size_t>(slot) * 2 * kRefloodCap;
+		for (uint32_t b = dmask; b; b &= b - 1u) {
+			const uint32_t k = static_cast<uint32_t>(__ffs(b) - 1), w = __ldg(ws.w1 + p0 + q * 16u + k);
+			if (b0 < kRefloodCap) { vals[b0] = w; }
+			++b0;
+			if ((pmask >> k) & 1u) {
+				if (b1 < kRefloodCap) { vals[kRefloodCap + b1] = w; }
+				++b1;
+			}
+		}
+	}
+	const uint32_t nGroups = ws.cnt->nmulti;
+	for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < nGroups; m += stride) {
+		const uint32_t off = ws.gOff[m];
+		if (ws.gOff[m + 1] == off || ws.frameReflood[FastDivide(ws.gPix[off], ws.g.divN)] == 0u) { continue; }
+		ws.rfGroups[atomicAdd(&ws.cnt->nrfgroup, 1u)] = m;
 	}
 }
 
@@ -1398,15 +1437,16 @@ __device__ __forceinline__ uint32_t FrameDelta(const Workspace& ws, int f)
 	return static_cast<uint32_t>((static_cast<unsigned long long>(ws.frameDom[f]) * 65536ull) / 10000000ull) + 1u;
 }
 
-// Step 4: for every pixel of the slotted frames' groups (a warp per group): the estimated frame-wide pop position
+// Step 4: for every pixel of the slotted frames' listed groups (a warp per group): the estimated frame-wide pop position
 // #{W1 > W1(p)} and its upper bound B(p) = #{W1 >= W1(p) - delta}.
 __global__ void RefloodCounts(Workspace ws)
 {
 	if (ws.cnt->nreflood == 0) { return; }
-	const uint32_t nGroups = ws.cnt->nmulti;
+	const uint32_t nList = ws.cnt->nrfgroup;
 	const int lane = threadIdx.x & 31;
 	const uint32_t warps = gridDim.x * (blockDim.x / 32);
-	for (uint32_t m = (blockIdx.x * blockDim.x + threadIdx.x) / 32; m < nGroups; m += warps) {
+	for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) / 32; g < nList; g += warps) {
+		const uint32_t m = ws.rfGroups[g];
 		const uint32_t off = ws.gOff[m], nPix = ws.gOff[m + 1] - off;
 		if (nPix == 0) { continue; }
 		const int f = Decompose(ws.gPix[off], ws.g).f;
@@ -1452,8 +1492,9 @@ __global__ void __launch_bounds__(kRfWarps * 32) RefloodBox(Workspace ws)
 	RfBoxSmem& sm = boxes[threadIdx.x / 32];
 	const int lane = threadIdx.x & 31;
 	const Geometry& geo = ws.g;
-	const uint32_t n = ws.cnt->nmulti;
-	for (uint32_t m = blockIdx.x * kRfWarps + threadIdx.x / 32; m < n; m += gridDim.x * kRfWarps) {
+	const uint32_t nList = ws.cnt->nrfgroup;
+	for (uint32_t g = blockIdx.x * kRfWarps + threadIdx.x / 32; g < nList; g += gridDim.x * kRfWarps) {
+		const uint32_t m = ws.rfGroups[g];
 		const uint32_t off = ws.gOff[m], nPix = ws.gOff[m + 1] - off;
 		if (nPix == 0) { continue; }
 		const int f = Decompose(ws.gPix[off], geo).f;  // every lane reads the group's first pixel

@@ -99,6 +99,7 @@ int main(int argc, char** argv)
 	ws.rfOff = Alloc<uint32_t>(static_cast<size_t>(kRefloodSlots) * 2 * (kRefloodBuckets + 1));
 	ws.rfInfo = Alloc<uint32_t>(kRefloodSlots * 8);
 	ws.rfPix = Alloc<uint32_t>(static_cast<size_t>(kRefloodSlots) * g.N * 2);
+	ws.rfGroups = Alloc<uint32_t>(ws.capComp);
 	ws.suspect = Alloc<uint4>(kSuspectCap); ws.capSuspect = kSuspectCap;
 	ws.rankOrder = Alloc<uint32_t>(kSuspectCap); ws.rankSlotOff = Alloc<uint32_t>(kRankSlots + 1);
 	ws.rankCount = Alloc<uint32_t>(2 * kSuspectCap);
