@@ -9,8 +9,8 @@
 // (__expf: a few ulp; __logf: absolute error about 2^-21 near 1) and erff; the per-pixel logarithm of the deviance
 // had been a fifth of the LM's time. Each 5x5 system is factored by an FP32 Cholesky;
 // when a pivot is not positive or the pivot ratio min(L_ii^2 / A_ii) falls below 1e-5 the same system is
-// re-factored in FP64. The Fisher information behind the CRLB is computed in FP64 (the final point's deviance is not
-// part of the output, so the final pass does not form it); the initial axial pre-scan, a handful of deviance
+// re-factored in FP64. The final pass forms the deviance (reported in the Theta column) and the Fisher information
+// behind the CRLB in FP64; the initial axial pre-scan, a handful of deviance
 // evaluations that choose the starting basin, runs in FP32 like the LM. The oracle
 // polishes in FP64 to a 1e-10 relative step; the FP32 polish stops at a 1e-6 relative step (the FP32 resolution of
 // the deviance), well inside the stated tolerance of 1e-3 px and 1e-4 relative photons.
