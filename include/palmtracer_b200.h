@@ -219,9 +219,8 @@ PTB_API void PTB_StageTimes(double* ms, uint64_t* launches, int n);
  * Levenberg-Marquardt iterations, [1] FP32 evaluations of the Newton polish (with the rare Fisher-scoring fallbacks),
  * [2] evaluations of the initial axial pre-scan (FP32) and of the final Fisher information (FP64); one evaluation
  * visits every pixel of one ROI. [3] FP32 Cholesky
- * factorisations redone in FP64 (ill-conditioned or failed), counted always. [4], [5] ROIs that the thread-per-ROI
- * LM and polish handed off to their resume launches (tail hand-off; counted while profiling). Copies up to n totals
- * into counts, then resets them. */
+ * factorisations redone in FP64 (ill-conditioned or failed), counted always. Copies up to n totals into counts,
+ * then resets them. */
 PTB_API void PTB_MleEvaluations(uint64_t* counts, int n);
 
 /* Launch-chain graphs of the current device's engines (diagnostics). A chunk's compute chain (counter reset,

@@ -51,16 +51,6 @@ bool CheckCuda(cudaError_t e, const char* what, const char* file, int line)
 	return false;
 }
 
-// The MLE fits' tail hand-off (thread-per-ROI LM and polish); PTB_MLE_TAIL=0 turns it off (the rows are the same).
-static bool TailHandoff()
-{
-	static const bool on = [] {
-		const char* e = std::getenv("PTB_MLE_TAIL");
-		return e == nullptr || std::atoi(e) != 0;
-	}();
-	return on;
-}
-
 // ---- fit parameters ------------------------------------------------------------------------------------------
 bool ParseFitParams(uint64_t fit, const double* fp, FitParams& out, std::vector<double>& splineHost)
 {
@@ -305,7 +295,6 @@ static size_t PlanWorkspace(Workspace& ws, int H, int W, int B, uint32_t rowsCap
 	take(ws.sortIdx, static_cast<size_t>(ws.capRows) * 2);
 	take(ws.sortKey, static_cast<size_t>(ws.capRows) * 4);
 	take(ws.fitFlag, ws.capRows);
-	take(ws.tailList, static_cast<size_t>(ws.capRows) + 2);
 	take(ws.scanBlock, P / 4096 + 64);
 	take(ws.cnt, 1);
 	return off;
@@ -560,14 +549,13 @@ bool Engine::EnqueueChunk(int slot, const uint16_t* dImg, int H, int W, int B, d
 	if (fpr.mode >= kMleGauss && !hooked) {
 		if (fpr.lanes == 0) { TunedMapping(fpr, SizeClass(B, H, W)); }
 		fpr.mle.queue = ws.cnt->queue;  // this slot's work-queue counters
-		fpr.mle.tail = TailHandoff() ? ws.tailList : nullptr;
 	}
 	const bool tune = !hooked && fpr.mode >= kMleGauss && fpr.lanes == 0;  // first chunk of this class: time the mappings
 	pendMleProf_ = prof && fpr.mode >= kMleGauss && !hooked;
 	bool ok = true;
 	if (pendMleProf_) {
-		if (!evalDev_) { ok = ok && PTB_CUDA(cudaMalloc(&evalDev_, 5 * sizeof(unsigned long long))); }
-		ok = ok && PTB_CUDA(cudaMemsetAsync(evalDev_, 0, 5 * sizeof(unsigned long long), st));
+		if (!evalDev_) { ok = ok && PTB_CUDA(cudaMalloc(&evalDev_, 3 * sizeof(unsigned long long))); }
+		ok = ok && PTB_CUDA(cudaMemsetAsync(evalDev_, 0, 3 * sizeof(unsigned long long), st));
 		fpr.marks = mleEv_;
 		fpr.mle.evals = evalDev_;
 	}
@@ -651,9 +639,9 @@ long long Engine::CompleteChunk(int slot, uint32_t* truncatedFrames)
 			stageMs_[5 + k] += ms;
 			stageLaunches_[5 + k] += (k == 1 || pendLanes_ == 1) ? 1 : 0;
 		}
-		unsigned long long ev[5] = {};
+		unsigned long long ev[3] = {};
 		if (!PTB_CUDA(cudaMemcpy(ev, evalDev_, sizeof(ev), cudaMemcpyDeviceToHost))) { return -1; }
-		for (int k = 0; k < 5; ++k) { evalTotals_[k] += ev[k]; }
+		for (int k = 0; k < 3; ++k) { evalTotals_[k] += ev[k]; }
 		pendMleProf_ = false;
 	}
 	const Counters& c = hostCnt_[slot];
@@ -931,7 +919,6 @@ bool Engine::Autotune(FitParams& fp, const uint16_t* dImg, int H, int W, int slo
 		t.lanes = c.lanes;
 		t.mle.chunk = envChunk ? envChunk : c.chunk;
 		t.mle.queue = ws.cnt->queue;
-		t.mle.tail = TailHandoff() ? ws.tailList : nullptr;
 		// one untimed run first: the first launch of a kernel also loads its code, which is not what the choice costs
 		if (!LaunchFit(dImg, H, W, ws.g.N, ws.cand, &ws.cnt->nfit, 0, ws.capRows, t, ws.rows, ws.fitFlag, precision_, st)) {
 			return false;
@@ -1009,11 +996,6 @@ void Engine::MleEvaluations(uint64_t* out, int n)
 			cudaMemset(fallbacks_, 0, sizeof(unsigned int));
 		}
 		if (out) { out[3] = fb; }
-	}
-	// [4], [5]: ROIs the LM and the polish handed off to their resume launches (tail hand-off)
-	for (int k = 4; k < 6 && k < n; ++k) {
-		if (out) { out[k] = evalTotals_[k - 1]; }
-		evalTotals_[k - 1] = 0;
 	}
 }
 

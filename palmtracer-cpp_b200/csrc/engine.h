@@ -189,7 +189,7 @@ private:
 	double stageMs_[kStages] = {};
 	uint64_t stageLaunches_[kStages] = {};
 	unsigned long long* evalDev_ = nullptr;      // device counters of model evaluations (profiling)
-	unsigned long long evalTotals_[5] = {};      // FP32 LM, FP32 polish, FP64; ROIs handed off by the LM, the polish
+	unsigned long long evalTotals_[3] = {};      // FP32 LM, FP32 polish, FP64
 	// profiling bookkeeping of the chunk in flight
 	uint64_t pendLaunches_[kStages] = {};
 	bool pendMleProf_ = false;

@@ -1047,51 +1047,20 @@ struct SlotView {
 	}
 };
 
-// Tail hand-off of the thread-per-ROI persistent kernels. Once a warp's work queue is empty and at most kTailLanes
-// of its lanes still iterate, those lanes save their ROI's state in its output row (theta in columns 0-4 as usual,
-// the rest as FP32 bit patterns in columns 6-17, which only the final pass writes) and list the candidate, and the
-// warp ends: a warp with few busy lanes issues as many instructions per pass as a full one. A second launch of the
-// same kernel (resume) takes the listed candidates 32 to a warp, restores each state exactly and carries on, so every
-// ROI follows the same sequence of FP32 operations as without the hand-off.
-constexpr int kTailLanes = 8;
-
-__device__ __forceinline__ uint32_t* TailWords(double* rows, uint32_t k)
-{
-	return reinterpret_cast<uint32_t*>(rows + static_cast<long long>(k) * kCols + kStatusCol + 1);  // 24 words
-}
-
-// Lists the calling lane's candidate k (when `save`) in the hand-off list; called by all 32 lanes.
-__device__ __forceinline__ void TailList(const MleParams& mp, bool save, uint32_t k)
-{
-	const int lane = threadIdx.x & 31;
-	const unsigned m = __ballot_sync(0xffffffffu, save);
-	if (m == 0) { return; }
-	const int leader = __ffs(m) - 1;
-	uint32_t base = 0;
-	if (lane == leader) { base = atomicAdd(mp.tail, static_cast<unsigned int>(__popc(m))); }
-	base = __shfl_sync(0xffffffffu, base, leader);
-	if (save) { mp.tail[2 + base + __popc(m & ((1u << lane) - 1u))] = k; }
-}
-
 // Persistent FP32 LM (WarpQueue). Every pass of the loop makes each busy ROI evaluate the deviance, gradient and
 // Fisher matrix once: at the start point of a new candidate, or at the trial point of an LM step. L lanes per ROI
 // (1: a thread per ROI); the lanes of a group hold the same state and take the same branches. Shared memory per ROI
-// slot: the photons and the factor tables (SlotFloats, NF = 3). resume: the launch that finishes the ROIs handed off by
-// the first one (tail hand-off, thread per ROI only).
+// slot: the photons and the factor tables (SlotFloats, NF = 3).
 template <int MODEL, int L>
-__global__ void __launch_bounds__(kThreads, L > 1 ? 0 : (MODEL == 6 ? 8 : (MODEL == 7 ? 7 : 6))) MleLmKernel(FitImages fi,
+__global__ void __launch_bounds__(kThreads) MleLmKernel(FitImages fi,
                                                         const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
-                                                        MleParams mp, double* rows, int resume)
+                                                        MleParams mp, double* rows)
 {
 	extern __shared__ __align__(16) unsigned char smem[];
 	const SlotView<L> sv(smem, mp, 3);
 	const Group<L> grp;
 	WarpQueue q;
-	const bool tail = L == 1 && mp.tail != nullptr;
-	if (resume && !tail) { return; }
-	const bool res = L == 1 && resume != 0;  // a compile-time false for lane groups
-	if (res && mp.evals && blockIdx.x == 0 && threadIdx.x == 0 && mp.tail[0]) { atomicAdd(mp.evals + 3, mp.tail[0]); }
-	if (!q.Init(res ? mp.tail[0] : CandCount(nptr, nconst), res ? mp.tail + 1 : mp.queue, res ? 1 : mp.chunk)) { return; }
+	if (!q.Init(CandCount(nptr, nconst), mp.queue, mp.chunk)) { return; }
 	uint32_t k = kNone;
 	bool fresh = false;
 	float th[5] = {0, 0, 0, 0, 0}, G[5], Hm[15], D = 0.f, lambda = 1e-3f, x0 = 0.f, y0 = 0.f;
@@ -1101,47 +1070,15 @@ __global__ void __launch_bounds__(kThreads, L > 1 ? 0 : (MODEL == 6 ? 8 : (MODEL
 	while (true) {
 		uint32_t kk = q.Take(grp.leader && k == kNone);
 		if constexpr (L > 1) { kk = __shfl_sync(0xffffffffu, kk, grp.first); }
-		if (res && kk != kNone) { kk = mp.tail[2 + kk]; }
 		if (kk != kNone && rows[static_cast<long long>(kk) * kCols + kStatusCol] == kStOk) {
 			LoadRoi<L>(fi, mp, cands, rows, kk, sv.ph, sv.stride, px, th, x0, y0);
 			k = kk;
 			fresh = true;
-			if (res) {  // the state saved by the hand-off (an iteration count of -1: not evaluated yet)
-				const uint32_t* s = TailWords(rows, kk);
-				it = static_cast<int>(s[22]);
-				if (it >= 0) {
-					fresh = false;
-					#pragma unroll
-					for (int a = 0; a < 5; ++a) { G[a] = __uint_as_float(s[a]); }
-					#pragma unroll
-					for (int a = 0; a < 15; ++a) { Hm[a] = __uint_as_float(s[5 + a]); }
-					D = __uint_as_float(s[20]);
-					lambda = __uint_as_float(s[21]);
-				}
-			}
 		}
 		const bool busy = k != kNone;
-		const unsigned busyMask = __ballot_sync(0xffffffffu, busy);
-		if (busyMask == 0) {
+		if (__ballot_sync(0xffffffffu, busy) == 0) {
 			if (q.Done()) { break; }
 			continue;
-		}
-		if (tail && !res && __popc(busyMask) <= kTailLanes && q.Done()) {
-			if (busy) {
-				double* row = rows + static_cast<long long>(k) * kCols;
-				#pragma unroll
-				for (int a = 0; a < 5; ++a) { row[a] = th[a]; }
-				uint32_t* s = TailWords(rows, k);
-				#pragma unroll
-				for (int a = 0; a < 5; ++a) { s[a] = __float_as_uint(G[a]); }
-				#pragma unroll
-				for (int a = 0; a < 15; ++a) { s[5 + a] = __float_as_uint(Hm[a]); }
-				s[20] = __float_as_uint(D);
-				s[21] = __float_as_uint(lambda);
-				s[22] = static_cast<uint32_t>(fresh ? -1 : it);
-			}
-			TailList(mp, busy, k);
-			break;
 		}
 		float tt[5];
 		bool eval = false, finish = false, failed = false;
@@ -1224,20 +1161,13 @@ __global__ void __launch_bounds__(kThreads, L > 1 ? 0 : (MODEL == 6 ? 8 : (MODEL
 template <int MODEL, int L>
 __global__ void __launch_bounds__(kThreads) MlePolishKernel(FitImages fi,
                                                             const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
-                                                            MleParams mp, double* rows, int resume)
+                                                            MleParams mp, double* rows)
 {
 	extern __shared__ __align__(16) unsigned char smem[];
 	const SlotView<L> sv(smem, mp, 6);
 	const Group<L> grp;
 	WarpQueue q;
-	const bool tail = L == 1 && mp.tail != nullptr;
-	if (resume && !tail) { return; }
-	const bool res = L == 1 && resume != 0;  // a compile-time false for lane groups
-	if (res && mp.evals && blockIdx.x == 0 && threadIdx.x == 0 && mp.tail[0]) { atomicAdd(mp.evals + 4, mp.tail[0]); }
-	if (!q.Init(res ? mp.tail[0] : CandCount(nptr, nconst), res ? mp.tail + 1 : (mp.queue ? mp.queue + 1 : nullptr),
-	            res ? 1 : mp.chunk)) {
-		return;
-	}
+	if (!q.Init(CandCount(nptr, nconst), mp.queue ? mp.queue + 1 : nullptr, mp.chunk)) { return; }
 	uint32_t k = kNone;
 	bool fresh = false;
 	float th[5] = {0, 0, 0, 0, 0}, dt[5] = {0, 0, 0, 0, 0}, G[5], Hm[15], D = 0.f, x0 = 0.f, y0 = 0.f;
@@ -1247,43 +1177,15 @@ __global__ void __launch_bounds__(kThreads) MlePolishKernel(FitImages fi,
 	while (true) {
 		uint32_t kk = q.Take(grp.leader && k == kNone);
 		if constexpr (L > 1) { kk = __shfl_sync(0xffffffffu, kk, grp.first); }
-		if (res && kk != kNone) { kk = mp.tail[2 + kk]; }
 		if (kk != kNone && rows[static_cast<long long>(kk) * kCols + kStatusCol] == kStOk) {
 			LoadRoi<L>(fi, mp, cands, rows, kk, sv.ph, sv.stride, px, th, x0, y0);
 			k = kk;
 			fresh = true;
-			if (res) {  // the state saved by the hand-off (an iteration count of -1: not evaluated yet)
-				const uint32_t* s = TailWords(rows, kk);
-				it = static_cast<int>(s[7]);
-				if (it >= 0) {
-					fresh = false;
-					#pragma unroll
-					for (int a = 0; a < 5; ++a) { dt[a] = __uint_as_float(s[a]); }
-					D = __uint_as_float(s[5]);
-					hv = static_cast<int>(s[6]);
-				}
-			}
 		}
 		const bool busy = k != kNone;
-		const unsigned busyMask = __ballot_sync(0xffffffffu, busy);
-		if (busyMask == 0) {
+		if (__ballot_sync(0xffffffffu, busy) == 0) {
 			if (q.Done()) { break; }
 			continue;
-		}
-		if (tail && !res && __popc(busyMask) <= kTailLanes && q.Done()) {
-			if (busy) {  // between passes a ROI needs theta, the step, the deviance and the two counters
-				double* row = rows + static_cast<long long>(k) * kCols;
-				#pragma unroll
-				for (int a = 0; a < 5; ++a) { row[a] = th[a]; }
-				uint32_t* s = TailWords(rows, k);
-				#pragma unroll
-				for (int a = 0; a < 5; ++a) { s[a] = __float_as_uint(dt[a]); }
-				s[5] = __float_as_uint(D);
-				s[6] = static_cast<uint32_t>(hv);
-				s[7] = static_cast<uint32_t>(fresh ? -1 : it);
-			}
-			TailList(mp, busy, k);
-			break;
 		}
 		float tt[5], Gt[5], Ht[15], Dt = 0.f;
 		bool finish = false;
@@ -1512,23 +1414,16 @@ bool LaunchPipeline(const FitImages& fi, const Cand* cands, const uint32_t* nptr
 	const int lmBlocks = PersistentBlocks(MleLmKernel<MODEL, L>, lmBytes, sms, rois);
 	const int polishBlocks = PersistentBlocks(MlePolishKernel<MODEL, L>, polishBytes, sms, rois);
 	if (mp.queue && !PTB_CUDA(cudaMemsetAsync(mp.queue, 0, 2 * sizeof(unsigned int), st))) { return false; }
-	// tail hand-off (thread per ROI): each persistent kernel runs a second time over the ROIs its first launch handed off
-	const bool tail = L == 1 && mp.tail != nullptr;
-	auto clearTail = [&]() { return !tail || PTB_CUDA(cudaMemsetAsync(mp.tail, 0, 2 * sizeof(unsigned int), st)); };
 	if (marks) { cudaEventRecord(marks[0], st); }
 	MleInitKernel<MODEL><<<blocks, kThreads, initBytes, st>>>(fi, cands, nptr, nconst, mp, rows);
 	if (marks) { cudaEventRecord(marks[1], st); }
-	if (!clearTail()) { return false; }
-	MleLmKernel<MODEL, L><<<lmBlocks, kThreads, lmBytes, st>>>(fi, cands, nptr, nconst, mp, rows, 0);
-	if (tail) { MleLmKernel<MODEL, L><<<lmBlocks, kThreads, lmBytes, st>>>(fi, cands, nptr, nconst, mp, rows, 1); }
+	MleLmKernel<MODEL, L><<<lmBlocks, kThreads, lmBytes, st>>>(fi, cands, nptr, nconst, mp, rows);
 	if (marks) { cudaEventRecord(marks[2], st); }
-	if (!clearTail()) { return false; }
-	MlePolishKernel<MODEL, L><<<polishBlocks, kThreads, polishBytes, st>>>(fi, cands, nptr, nconst, mp, rows, 0);
-	if (tail) { MlePolishKernel<MODEL, L><<<polishBlocks, kThreads, polishBytes, st>>>(fi, cands, nptr, nconst, mp, rows, 1); }
+	MlePolishKernel<MODEL, L><<<polishBlocks, kThreads, polishBytes, st>>>(fi, cands, nptr, nconst, mp, rows);
 	if (marks) { cudaEventRecord(marks[3], st); }
 	MleFinalKernel<MODEL><<<blocks, kThreads, finalBytes, st>>>(fi, cands, nptr, nconst, mp, rows);
 	if (marks) { cudaEventRecord(marks[4], st); }
-	CountLaunch(tail ? 6 : 4);
+	CountLaunch(4);
 	return PTB_LAUNCHED();
 }
 

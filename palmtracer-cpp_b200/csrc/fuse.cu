@@ -92,7 +92,6 @@ bool LaunchFusedMle(const FitJob* jobs, int n, int lanes, Cand* fusedCands, doub
 	MleParams mp = jobs[0].fp.mle;
 	mp.fallbacks = counters;
 	mp.queue = counters + 1;
-	mp.tail = nullptr;  // no tail hand-off in the fused launch
 	mp.evals = nullptr;
 	const int grid = 148 * 4;
 	FuseOffsets<<<1, 32, 0, st>>>(t, offsets);

@@ -120,11 +120,7 @@ struct MleParams {
 	const double* table64;     // mode 8: the same in FP64 (FP64 phases)
 	unsigned int* fallbacks;   // FP64 Cholesky re-factorisations (diagnostics)
 	unsigned int* queue;       // 2 work-queue counters of the persistent fit kernels (zeroed by the launch), or null
-	// tail hand-off of the thread-per-ROI LM and polish, or null: [0] ROIs handed off, [1] resume work-queue counter
-	// (zeroed by the launch), then the handed-off candidates (room for every candidate of the launch)
-	unsigned int* tail;
-	unsigned long long* evals; // profiling, or null: model evaluations [FP32 LM, FP32 polish, FP64 pre-scan + final],
-	                           // then the ROIs handed off [LM, polish]
+	unsigned long long* evals; // profiling, or null: model evaluations [FP32 LM, FP32 polish, FP64 pre-scan + final]
 };
 
 // Fit configuration passed by value to the fit kernels.
@@ -234,7 +230,6 @@ struct Workspace {
 	double* rows;          // [capRows][18], unsorted fit results
 	double* sortedRows;    // [capRows][18], per-frame (Y, X) order with Id/Plane/Index
 	uint32_t* sortIdx;     // scratch for the per-frame sort
-	uint32_t* tailList;    // [capRows + 2]: the fit's tail hand-off (MleParams::tail)
 	double* sortKey;
 	uint8_t* fitFlag;      // FP32 fits that need an FP64 re-run
 	// scan scratch

@@ -218,13 +218,11 @@ def stage_times():
 
 def mle_evaluations():
     """{"lm": FP32 LM evaluations, "polish": FP32 polish evaluations, "init_final": axial pre-scan (FP32) and final
-    Fisher (FP64) evaluations, "lm_handoff" / "polish_handoff": ROIs the LM and the polish handed off to their resume
-    launches} counted while profiling was on (modes 6-8), and "fp64_cholesky": FP32 Cholesky solves redone in FP64,
-    since the last call."""
-    out = np.zeros(6, dtype=np.uint64)
-    load().PTB_MleEvaluations(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 6)
-    return {"lm": int(out[0]), "polish": int(out[1]), "init_final": int(out[2]), "fp64_cholesky": int(out[3]),
-            "lm_handoff": int(out[4]), "polish_handoff": int(out[5])}
+    Fisher (FP64) evaluations} counted while profiling was on (modes 6-8), and "fp64_cholesky": FP32 Cholesky solves
+    redone in FP64, since the last call."""
+    out = np.zeros(4, dtype=np.uint64)
+    load().PTB_MleEvaluations(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 4)
+    return {"lm": int(out[0]), "polish": int(out[1]), "init_final": int(out[2]), "fp64_cholesky": int(out[3])}
 
 
 def tracking(points, max_distance):
