@@ -189,6 +189,7 @@ def workload_runs(ptb, torch, steps=3, warmup=3):
         for _ in range(warmup):
             n = step()
         torch.cuda.synchronize()
+        ptb.segmentation_stats()  # counts of the timed steps only
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(steps):
@@ -196,9 +197,18 @@ def workload_runs(ptb, torch, steps=3, warmup=3):
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / steps
+        seg = ptb.segmentation_stats()
+        # stage breakdown of one more (untimed) pass, chunks serialised
+        ptb.set_profiling(1)
+        ptb.stage_times()
+        step()
+        torch.cuda.synchronize()
+        stages = ptb.stage_times()
+        ptb.set_profiling(0)
         rows = n // 18
         out[name] = {"frames": z, "height": h, "width": w, "fit_mode": fit, "roi": roi, "localizations_per_step": int(rows),
-                     "ms_per_step": ms, "localizations_per_s": rows / (ms / 1000.0), "frames_per_s": z / (ms / 1000.0)}
+                     "ms_per_step": ms, "localizations_per_s": rows / (ms / 1000.0), "frames_per_s": z / (ms / 1000.0),
+                     "segmentation": seg, "stage_ms": {k: round(v[0], 3) for k, v in stages.items()}}
         del d_in, d_out
         torch.cuda.empty_cache()
     return out
