@@ -182,7 +182,10 @@ PTB_API int PTB_SetSegmentationMode(int mode);
 /* Segmentation diagnostics of the current device's engines since the last call: counts[0] frames segmented,
  * counts[1] frames flooded again frame-wide, counts[2] frames whose per-component floods needed the rank test (the
  * second exactness test) in mode 0, counts[3] frames flooded again per component with estimated frame-wide aging
- * after failing it (up to n entries). */
+ * after failing it, counts[4..10] the frames of counts[1] by the first reason they were flooded frame-wide: the list
+ * of failing boundary pairs full, a pair failing the first test in mode 2, no rank-test slot left in the chunk, too
+ * many failing pairs in the frame, a failed rank test after a basin fusion, no re-flood slot or too many domain
+ * pixels for the re-flood, a failed re-flood test (up to n entries). */
 PTB_API void PTB_SegmentationStats(uint64_t* counts, int n);
 
 /* Engine pool of the current device (diagnostics): counts[0] engines created, counts[1] the most engines leased at

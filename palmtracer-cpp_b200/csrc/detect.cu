@@ -299,7 +299,8 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 			smask |= static_cast<uint32_t>(dom && v >= __vimax3_u32(cm[k], cm[k + 1], cm[k + 2])) << (4 * h + k);
 		}
 	}
-	// block-wide positions in the domain and seed lists: one atomic per list
+	// block-wide positions in the domain and seed lists: one atomic per list, issued by thread 0 while the other
+	// threads write the code bytes and the W1 of domain pixels, which need no list position
 	const int lane = tid & 31, warp = tid >> 5;
 	const uint32_t nd = __popc(dmask), ns = __popc(smask);
 	uint32_t id = nd, is = ns;
@@ -323,35 +324,47 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 		if (sd) { atomicAdd(ws.frameDom + f, sd); }
 		if (ss) { atomicAdd(ws.frameSeeds + f, ss); }
 	}
-	__syncthreads();
-	uint32_t pd = scanSm[2 * kWarps] + scanSm[warp] + id - nd;
-	uint32_t ps = scanSm[2 * kWarps + 1] + scanSm[kWarps + warp] + is - ns;
+	// code bytes of the four pixels of each task and the W1 of its domain pixels (still in shared memory); a chunk's
+	// pixel indices fit in 31 bits
+	const uint32_t frameBase = static_cast<uint32_t>(f) * static_cast<uint32_t>(ws.g.N);
 	#pragma unroll
 	for (int h = 0; h < kTasksE; ++h) {
 		const int task = tid + h * kThreads;
 		const int ty = task >> 5, m = task & 31;
 		const int y = y0 + ty, xb = x0 + 4 * m;
 		if (ty >= TY || y >= H || xb >= W) { continue; }
-		const long long g = static_cast<long long>(f) * ws.g.N + static_cast<long long>(y) * W + xb;
-		// code bytes of the four pixels: each mask bit spread to the low bit of its byte, times the flag
+		const uint32_t g = frameBase + static_cast<uint32_t>(y * W + xb);
+		// each mask bit spread to the low bit of its byte, times the flag
 		const uint32_t dm = (dmask >> (4 * h)) & 15u, sm = (smask >> (4 * h)) & 15u;
 		const uint32_t bytes = Spread4(dm) * kDomain | Spread4(sm) * kSeed;
-		if (xb + 4 <= W && (g & 3) == 0) { *reinterpret_cast<uint32_t*>(ws.code + g) = bytes; }
+		if (xb + 4 <= W && (g & 3u) == 0) { *reinterpret_cast<uint32_t*>(ws.code + g) = bytes; }
 		else {
 			for (int k = 0; k < 4 && xb + k < W; ++k) { ws.code[g + k] = static_cast<uint8_t>(bytes >> (8 * k)); }
 		}
-		// domain pixels (their W1 is still in shared memory) and seeds, lowest pixel first
 		const uint32_t* w1row = v1 + (ty + 5) * kPV + 4 * m + 5;
+		#pragma unroll
+		for (int k = 0; k < 4; ++k) {
+			if ((dm >> k) & 1u) { ws.w1[g + k] = w1row[k]; }
+		}
+	}
+	__syncthreads();
+	// the list entries, lowest pixel first
+	uint32_t pd = scanSm[2 * kWarps] + scanSm[warp] + id - nd;
+	uint32_t ps = scanSm[2 * kWarps + 1] + scanSm[kWarps + warp] + is - ns;
+	#pragma unroll
+	for (int h = 0; h < kTasksE; ++h) {
+		const uint32_t dm = (dmask >> (4 * h)) & 15u, sm = (smask >> (4 * h)) & 15u;
+		if ((dm | sm) == 0) { continue; }  // also every task outside the tile or the frame (its masks are empty)
+		const int task = tid + h * kThreads;
+		const int ty = task >> 5, m = task & 31;
+		const uint32_t g = frameBase + static_cast<uint32_t>((y0 + ty) * W + x0 + 4 * m);
 		for (uint32_t b = dm; b; b &= b - 1u) {
-			const int k = __ffs(b) - 1;
-			ws.w1[g + k] = w1row[k];
-			if (pd < ws.capDom) { ws.dom[pd] = static_cast<uint32_t>(g + k); }
+			if (pd < ws.capDom) { ws.dom[pd] = g + static_cast<uint32_t>(__ffs(b) - 1); }
 			else { atomicExch(&ws.cnt->overflow, 1u); }
 			++pd;
 		}
 		for (uint32_t b = sm; b; b &= b - 1u) {
-			const int k = __ffs(b) - 1;
-			if (ps < ws.capSeed) { ws.seeds[ps] = static_cast<uint32_t>(g + k); }
+			if (ps < ws.capSeed) { ws.seeds[ps] = g + static_cast<uint32_t>(__ffs(b) - 1); }
 			else { atomicExch(&ws.cnt->overflow, 1u); }
 			++ps;
 		}

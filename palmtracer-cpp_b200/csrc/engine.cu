@@ -276,7 +276,7 @@ static size_t PlanWorkspace(Workspace& ws, int H, int W, int B, uint32_t rowsCap
 	take(ws.rfGrp, static_cast<size_t>(kRefloodSlots) * 2 * kRefloodCap);
 	take(ws.rfOff, static_cast<size_t>(kRefloodSlots) * 2 * (kRefloodBuckets + 1));
 	take(ws.rfInfo, static_cast<size_t>(kRefloodSlots) * 8);
-	take(ws.rfPix, static_cast<size_t>(kRefloodSlots) * static_cast<size_t>(g.N) * 2);
+	take(ws.rfPix, static_cast<size_t>(kRefloodSlots) * static_cast<size_t>(g.N) * kRfWords);
 	take(ws.rfGroups, capComp);
 	take(ws.suspect, kSuspectCap);
 	take(ws.rankOrder, kSuspectCap);
@@ -652,6 +652,7 @@ long long Engine::CompleteChunk(int slot, uint32_t* truncatedFrames)
 	segCounts_[1] += c.nroute;
 	segCounts_[2] += c.nslots;
 	segCounts_[3] += c.nreflood;
+	for (int k = 0; k < 7; ++k) { segCounts_[4 + k] += c.routeWhy[k]; }
 	if (truncatedFrames) { *truncatedFrames += c.truncated; }
 	return c.nfit;
 }
@@ -966,7 +967,7 @@ void Engine::GraphStats(uint64_t* out, int n)
 
 void Engine::SegmentationStats(uint64_t* out, int n)
 {
-	for (int k = 0; k < 4 && k < n; ++k) {
+	for (int k = 0; k < 11 && k < n; ++k) {
 		if (out) { out[k] = segCounts_[k]; }
 		segCounts_[k] = 0;
 	}

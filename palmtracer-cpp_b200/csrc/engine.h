@@ -143,7 +143,8 @@ private:
 	std::vector<std::vector<uint64_t>> seen_[2];  // chains launched once directly (the next occurrence is captured)
 	uint64_t graphClock_ = 0;
 	uint64_t graphCounts_[3] = {};            // captured, replayed, direct
-	uint64_t segCounts_[4] = {};              // frames segmented, flooded frame-wide, given the rank test, re-flooded
+	uint64_t segCounts_[11] = {};             // frames segmented, flooded frame-wide, given the rank test, re-flooded;
+	                                          // flooded frame-wide by reason (RouteReason)
 	bool useGraphs_ = true;                   // PTB_GRAPHS=0 launches every chunk directly
 	bool graphsOff_ = false;                  // a capture failed: direct launches from then on
 	Workspace ws1_{};                        // second chunk slot's workspace and pool

@@ -44,6 +44,10 @@ constexpr uint32_t kPairsPerFrame = 512u;
 constexpr uint32_t kRefloodSlots = 8u;
 constexpr uint32_t kRefloodCap = 65536u;
 constexpr uint32_t kRefloodBuckets = 32768u;  // value buckets of the rank lookups
+// Words per pixel and re-flood slot of rfPix: the estimated frame-wide pop position, its bound B, and for groups
+// re-flooded in global memory (larger than the shared-memory box) the element value and its chain minimum (int64
+// each).
+constexpr uint32_t kRfWords = 6u;
 
 // W1 values are exact multiples of 2^-16 (B3 taps are dyadic and the input is uint16), kept as int64 "fixed" units.
 constexpr double kW1Unit = 1.0 / 65536.0;
@@ -79,6 +83,18 @@ struct Counters {
 	uint32_t nslots;    // frames given the rank test
 	uint32_t nreflood;  // frames that failed the rank test (flooded again with estimated frame-wide aging)
 	uint32_t nrfgroup;  // multi-label groups of the frames given a re-flood slot (listed in rfGroups)
+	uint32_t routeWhy[7];  // frames flooded frame-wide, by the first reason (RouteReason)
+};
+
+// Why a frame is flooded again frame-wide (diagnostics, counted per frame by the first reason).
+enum RouteReason : int {
+	kRouteSuspectFull = 0,  // the list of boundary pairs that failed the first test was full
+	kRouteFirstTest = 1,    // a pair failed the first test where no rank test follows (segmentation mode 2)
+	kRouteRankSlots = 2,    // more frames needed the rank test than a chunk has slots
+	kRoutePairs = 3,        // the frame had more failing pairs than the rank test takes per frame
+	kRouteRankFused = 4,    // failed the rank test after a basin fusion (no re-flood)
+	kRouteRefloodSlots = 5, // failed the rank test beyond the re-flood slots or the re-flood's domain-pixel capacity
+	kRouteRefloodTest = 6   // the re-flooded labels failed the per-element rank test
 };
 
 // One fit input: a segmentation candidate (x_, y_, intensity_, surf_ of SegmentationInfo) or a caller position.
@@ -217,7 +233,8 @@ struct Workspace {
 	// (0: the W1 values of its domain pixels, 1: of the pixels its frame-wide flood pops): the values as gathered and
 	// grouped by value bucket ([kRefloodSlots][2][kRefloodCap]), the bucket offsets ([kRefloodSlots][2][buckets + 1]);
 	// per slot [8]: the two counts, the frame + 1, unused, and per list the lowest value and the bucket shift; per slot
-	// and pixel of the frame: the estimated frame-wide pop position and its upper bound ([kRefloodSlots][N][2]); the
+	// and pixel of the frame: the estimated frame-wide pop position and its upper bound, then the global re-flood's
+	// element value and chain minimum ([kRefloodSlots][N][kRfWords]); the
 	// multi-label groups of the slotted frames ([capComp])
 	uint32_t* frameReflood;
 	uint32_t* rfVals; uint32_t* rfGrp; uint32_t* rfOff; uint32_t* rfInfo; uint32_t* rfPix; uint32_t* rfGroups;

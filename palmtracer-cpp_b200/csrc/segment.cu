@@ -639,9 +639,12 @@ __device__ __forceinline__ bool PairExact(uint32_t chain, uint32_t w1z, uint32_t
 }
 
 // Marks frame f for the frame-wide flood (once).
-__device__ __forceinline__ void RouteFrame(const Workspace& ws, int f)
+__device__ __forceinline__ void RouteFrame(const Workspace& ws, int f, RouteReason why)
 {
-	if (atomicExch(ws.frameRoute + f, 1u) == 0u) { atomicAdd(&ws.cnt->nroute, 1u); }
+	if (atomicExch(ws.frameRoute + f, 1u) == 0u) {
+		atomicAdd(&ws.cnt->nroute, 1u);
+		atomicAdd(ws.cnt->routeWhy + why, 1u);
+	}
 }
 
 // A boundary pair of frame f that failed the first test, kept for the rank test: the parent-chain minimum of the
@@ -651,7 +654,7 @@ __device__ __forceinline__ bool SuspectPair(const Workspace& ws, int f, uint32_t
 {
 	const uint32_t i = atomicAdd(&ws.cnt->nsuspect, 1u);
 	if (i >= ws.capSuspect) {
-		RouteFrame(ws, f);
+		RouteFrame(ws, f, kRouteSuspectFull);
 		return false;
 	}
 	ws.suspect[i] = make_uint4(static_cast<uint32_t>(f), chain, w1z, zmax);
@@ -698,7 +701,7 @@ __device__ bool PixelExactGlobal(const Workspace& ws, uint32_t p, uint32_t T, in
 			const uint32_t w1z = __ldg(ws.w1 + nb);
 			if (PairExact(chain, w1z, T)) { continue; }
 			if (!rank) {
-				RouteFrame(ws, f);
+				RouteFrame(ws, f, kRouteFirstTest);
 				return false;
 			}
 			// z pushed by the flood (a chain value) or one of its seeds
@@ -878,7 +881,7 @@ __global__ void __launch_bounds__(kBoxWarps * 32) GroupFloodBox(Workspace ws, in
 					const int j = i + dy * bw + dx;
 					if (!(sm.flag[j] & 1u) || sm.lab[j] == L || PairExact(chain, sm.w1[j], T)) { continue; }
 					if (!rank) {
-						RouteFrame(ws, f);
+						RouteFrame(ws, f, kRouteFirstTest);
 						continue;
 					}
 					// z = pixel j is a group pixel, so its neighbours in the frame lie in the box as well
@@ -1074,7 +1077,7 @@ __global__ void __launch_bounds__(kPlanThreads) SuspectPlan(Workspace ws)
 			if (slot < kRankSlots) { ws.frameSuspect[f] = slot + 1u; }
 			else {
 				ws.frameSuspect[f] = 0u;
-				RouteFrame(ws, f);
+				RouteFrame(ws, f, kRouteRankSlots);
 			}
 		}
 		__syncthreads();
@@ -1109,7 +1112,7 @@ __global__ void __launch_bounds__(kPlanThreads) SuspectPlan(Workspace ws)
 	// frames with too many pairs: routed; their slots stay empty in the counting pass (frameSuspect = 0)
 	for (uint32_t i = threadIdx.x; i < nrec; i += kPlanThreads) {
 		const uint32_t f = ws.suspect[i].x, s = ws.frameSuspect[f];
-		if (s != 0u && slotCount[s - 1u] > kPairsPerFrame) { RouteFrame(ws, static_cast<int>(f)); }
+		if (s != 0u && slotCount[s - 1u] > kPairsPerFrame) { RouteFrame(ws, static_cast<int>(f), kRoutePairs); }
 	}
 	__syncthreads();
 	for (int f = threadIdx.x; f < B; f += kPlanThreads) {
@@ -1192,7 +1195,7 @@ __global__ void SuspectCount(Workspace ws)
 __device__ __forceinline__ void FailRankTest(const Workspace& ws, int f, int reflood)
 {
 	if (!reflood) {
-		RouteFrame(ws, f);
+		RouteFrame(ws, f, kRouteRankFused);
 		return;
 	}
 	if (atomicExch(ws.frameReflood + f, 1u) == 0u) { atomicAdd(&ws.cnt->nreflood, 1u); }
@@ -1243,7 +1246,7 @@ __global__ void __launch_bounds__(kPlanThreads) RefloodPlan(Workspace ws)
 			}
 			else {
 				ws.frameReflood[f] = 0u;
-				RouteFrame(ws, f);
+				RouteFrame(ws, f, kRouteRefloodSlots);
 			}
 		}
 	}
@@ -1454,13 +1457,13 @@ __global__ void RefloodCounts(Workspace ws)
 		if (s == 0u) { continue; }
 		const uint32_t slot = s - 1u;
 		const uint32_t delta = FrameDelta(ws, f);
-		uint32_t* out = ws.rfPix + static_cast<size_t>(slot) * static_cast<size_t>(ws.g.N) * 2;
+		uint32_t* out = ws.rfPix + static_cast<size_t>(slot) * static_cast<size_t>(ws.g.N) * kRfWords;
 		for (uint32_t i = lane; i < nPix; i += 32) {
 			const uint32_t p = ws.gPix[off + i];
 			const uint32_t w = __ldg(ws.w1 + p);
 			const size_t local = static_cast<size_t>(p) - static_cast<size_t>(f) * static_cast<size_t>(ws.g.N);
-			out[local * 2] = CountAbove(ws, slot, 0, w, true);
-			out[local * 2 + 1] = CountAbove(ws, slot, 0, w > delta ? w - delta : 0u, false);
+			out[local * kRfWords] = CountAbove(ws, slot, 0, w, true);
+			out[local * kRfWords + 1] = CountAbove(ws, slot, 0, w > delta ? w - delta : 0u, false);
 		}
 	}
 }
@@ -1482,7 +1485,128 @@ struct RfBoxSmem {
 
 constexpr long long kNoM = 0x7fffffffffffffffll;
 
-// Step 5: warp per group of the slotted frames, box staged in shared memory (a frame with a larger group is routed):
+// Step 5 for a group larger than the shared-memory box (called by the whole warp): the same flood and test in global
+// memory. Labels go to lab (the group's non-seed pixels restart unlabelled), chain minima to par (dead since the
+// groups were scattered), element values v and their chain minima m to the slot's rfPix words 2-5; the heap spills to
+// the group's global heap slice. Returns false when the frame must be flooded frame-wide.
+__device__ bool RefloodGroupGlobal(const Workspace& ws, RfBoxSmem& sm, uint32_t m, uint32_t off, uint32_t nPix, int f,
+                                   uint32_t slot)
+{
+	const int lane = threadIdx.x & 31;
+	const Geometry& geo = ws.g;
+	uint32_t* pix = ws.rfPix + static_cast<size_t>(slot) * static_cast<size_t>(geo.N) * kRfWords;
+	const uint32_t frame0 = static_cast<uint32_t>(f) * static_cast<uint32_t>(geo.N);
+	auto word = [&](uint32_t p) { return pix + static_cast<size_t>(p - frame0) * kRfWords; };
+	auto getV = [&](uint32_t p, int k) {
+		const uint32_t* q = word(p) + 2 + 2 * k;
+		return static_cast<long long>((static_cast<unsigned long long>(q[1]) << 32) | q[0]);
+	};
+	auto setV = [&](uint32_t p, int k, long long x) {
+		uint32_t* q = word(p) + 2 + 2 * k;
+		q[0] = static_cast<uint32_t>(static_cast<unsigned long long>(x));
+		q[1] = static_cast<uint32_t>(static_cast<unsigned long long>(x) >> 32);
+	};
+	for (uint32_t i = lane; i < nPix; i += 32) {
+		const uint32_t p = ws.gPix[off + i];
+		const bool seed = (__ldg(ws.code + p) & kSeed) != 0;
+		if (!seed) { ws.lab[p] = 0u; }
+		ws.par[p] = kNoChain;
+		setV(p, 0, static_cast<long long>(__ldg(ws.w1 + p)) * 78125ll);  // a seed's value (no aging)
+		setV(p, 1, kNoM);
+	}
+	__syncwarp();
+	if (lane == 0) {
+		uint32_t* seeds = ws.gSeed + ws.gSeedOff[m];
+		const uint32_t nSeeds = ws.gSeedOff[m + 1] - ws.gSeedOff[m];
+		SortSlice(seeds, nSeeds);
+		Heap heap{sm.key, sm.pix, 0, 1, kBoxHeap, ws.heapKey + off, ws.heapPix + off};
+		auto open = [&](uint32_t p, int y, int x) {
+			for (int dy = -1; dy <= 1; ++dy) {
+				const int yy = y + dy;
+				if (yy < 0 || yy >= geo.H) { continue; }
+				for (int dx = -1; dx <= 1; ++dx) {
+					const int xx = x + dx;
+					if ((dx == 0 && dy == 0) || xx < 0 || xx >= geo.W) { continue; }
+					const uint32_t nb = p + static_cast<uint32_t>(dy * geo.W + dx);  // in the frame: no wrap
+					if (!(__ldg(ws.code + nb) & kDomain) || ws.lab[nb] == 0u) { return true; }
+				}
+			}
+			return false;
+		};
+		for (uint32_t k = 0; k < nSeeds; ++k) {
+			const uint32_t sd = seeds[k];
+			const Pix q = Decompose(sd, geo);
+			if (open(sd, q.y, q.x)) { heap.Push(-(static_cast<double>(__ldg(ws.w1 + sd)) * kW1Unit), sd); }
+		}
+		while (heap.len > 0) {
+			const uint32_t p = heap.Pop();
+			const Pix q = Decompose(p, geo);
+			const uint32_t L = ws.lab[p];
+			const uint32_t* wp = word(p);
+			// pushes at this pop age by the estimated frame-wide position of the pop
+			const double age = __dmul_rn(static_cast<double>(wp[0]) + 1.0, kEps);
+			const uint32_t chain = min(ws.par[p], __ldg(ws.w1 + p));
+			const long long mch = min(getV(p, 1), getV(p, 0));
+			const long long bpush = static_cast<long long>(wp[1]) * 512ll;
+			for (int t = 0; t < 8; ++t) {
+				const int dy = t < 3 ? -1 : (t < 5 ? 0 : 1);
+				const int dx = t < 3 ? t - 1 : (t < 5 ? (t == 3 ? -1 : 1) : t - 6);
+				const int yy = q.y + dy, xx = q.x + dx;
+				if (yy < 0 || yy >= geo.H || xx < 0 || xx >= geo.W) { continue; }
+				const uint32_t j = p + static_cast<uint32_t>(dy * geo.W + dx);
+				if (!(__ldg(ws.code + j) & kDomain) || ws.lab[j] != 0u) { continue; }
+				const uint32_t wj = __ldg(ws.w1 + j);
+				heap.Push(__dadd_rn(-(static_cast<double>(wj) * kW1Unit), age), j);
+				ws.lab[j] = L;
+				ws.par[j] = chain;
+				setV(j, 1, mch);
+				setV(j, 0, static_cast<long long>(wj) * 78125ll - bpush);
+			}
+		}
+	}
+	__syncwarp();
+	// the per-element test at every boundary pair of a flooded pixel that fails the first test
+	const uint32_t T = ws.frameDom[f];
+	const uint32_t delta = FrameDelta(ws, f);
+	bool exact = true;
+	for (uint32_t i = lane; i < nPix && exact; i += 32) {
+		const uint32_t p = ws.gPix[off + i];
+		if (__ldg(ws.code + p) & kSeed) { continue; }
+		const uint32_t L = ws.lab[p], chain = ws.par[p];
+		if (L == 0u) { continue; }
+		const long long mi = getV(p, 1);
+		const Pix q = Decompose(p, geo);
+		for (int dy = -1; dy <= 1 && exact; ++dy) {
+			if (q.y + dy < 0 || q.y + dy >= geo.H) { continue; }
+			for (int dx = -1; dx <= 1 && exact; ++dx) {
+				if ((dx == 0 && dy == 0) || q.x + dx < 0 || q.x + dx >= geo.W) { continue; }
+				const uint32_t j = p + static_cast<uint32_t>(dy * geo.W + dx);
+				if (!(__ldg(ws.code + j) & kDomain) || ws.lab[j] == L) { continue; }
+				const uint32_t wj = __ldg(ws.w1 + j);
+				if (PairExact(chain, wj, T)) { continue; }
+				long long az = 0;
+				if (ws.par[j] != kNoChain) {  // z pushed: its pusher is one of its neighbours, none above zmax
+					uint32_t zmax = 0;
+					const int zy = q.y + dy, zx = q.x + dx;
+					for (int ey = -1; ey <= 1; ++ey) {
+						if (zy + ey < 0 || zy + ey >= geo.H) { continue; }
+						for (int ex = -1; ex <= 1; ++ex) {
+							if ((ex == 0 && ey == 0) || zx + ex < 0 || zx + ex >= geo.W) { continue; }
+							const uint32_t e = j + static_cast<uint32_t>(ey * geo.W + ex);
+							if (__ldg(ws.code + e) & kDomain) { zmax = max(zmax, __ldg(ws.w1 + e)); }
+						}
+					}
+					const unsigned long long x = static_cast<unsigned long long>(zmax) + delta;
+					az = (x < 0xffffffffull ? static_cast<long long>(CountAbove(ws, slot, 1, static_cast<uint32_t>(x), true)) : 0ll) + 1;
+				}
+				if (!(mi > static_cast<long long>(wj) * 78125ll - (az - 1) * 512ll)) { exact = false; }
+			}
+		}
+	}
+	return __all_sync(0xffffffffu, exact) != 0;
+}
+
+// Step 5: warp per group of the slotted frames, box staged in shared memory (a larger group: RefloodGroupGlobal):
 // the flood with push aging (estimated position + 1) * 1e-7, then the per-element test at every boundary pair that
 // fails the first test; a failing frame is routed to the frame-wide flood.
 __global__ void __launch_bounds__(kRfWarps * 32) RefloodBox(Workspace ws)
@@ -1516,11 +1640,11 @@ __global__ void __launch_bounds__(kRfWarps * 32) RefloodBox(Workspace ws)
 		const int bx0 = max(x0 - 1, 0), by0 = max(y0 - 1, 0);
 		const int bw = min(x1 + 1, geo.W - 1) - bx0 + 1, bh = min(y1 + 1, geo.H - 1) - by0 + 1;
 		if (bw * bh > kBoxCap) {
-			if (lane == 0) { RouteFrame(ws, f); }
+			if (!RefloodGroupGlobal(ws, sm, m, off, nPix, f, slot) && lane == 0) { RouteFrame(ws, f, kRouteRefloodTest); }
 			continue;
 		}
 		const uint32_t base = static_cast<uint32_t>(f) * static_cast<uint32_t>(geo.N) + static_cast<uint32_t>(by0 * geo.W + bx0);
-		const uint32_t* pix = ws.rfPix + static_cast<size_t>(slot) * static_cast<size_t>(geo.N) * 2;
+		const uint32_t* pix = ws.rfPix + static_cast<size_t>(slot) * static_cast<size_t>(geo.N) * kRfWords;
 		const uint32_t local0 = static_cast<uint32_t>(by0 * geo.W + bx0);
 		for (int i = lane; i < bw * bh; i += 32) {
 			const int r = i / bw, c = i - r * bw;
@@ -1533,8 +1657,8 @@ __global__ void __launch_bounds__(kRfWarps * 32) RefloodBox(Workspace ws)
 			sm.chain[i] = kNoChain;
 			sm.flag[i] = static_cast<uint8_t>((dom ? 1u : 0u) | (dom && !seed ? 2u : 0u));
 			const size_t local = static_cast<size_t>(local0) + static_cast<size_t>(r) * geo.W + c;
-			sm.gest[i] = dom ? pix[local * 2] : 0u;
-			sm.bnd[i] = dom ? pix[local * 2 + 1] : 0u;
+			sm.gest[i] = dom ? pix[local * kRfWords] : 0u;
+			sm.bnd[i] = dom ? pix[local * kRfWords + 1] : 0u;
 			sm.v[i] = static_cast<long long>(w) * 78125ll;  // a seed's value (no aging); pushed pixels overwrite it
 			sm.m[i] = kNoM;
 		}
@@ -1621,7 +1745,7 @@ __global__ void __launch_bounds__(kRfWarps * 32) RefloodBox(Workspace ws)
 				}
 			}
 		}
-		if (__any_sync(0xffffffffu, !exact) && lane == 0) { RouteFrame(ws, f); }
+		if (__any_sync(0xffffffffu, !exact) && lane == 0) { RouteFrame(ws, f, kRouteRefloodTest); }
 		__syncwarp();
 	}
 }

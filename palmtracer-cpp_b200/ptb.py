@@ -282,12 +282,16 @@ def graph_stats():
 
 
 def segmentation_stats():
-    """{"frames", "routed", "rank_tested", "reflooded"}: frames segmented by this device's engines since the last call;
-    of those, frames whose per-component floods needed the rank test, frames flooded again per component with
-    estimated frame-wide aging because they failed it, and frames flooded again frame-wide."""
-    out = np.zeros(4, dtype=np.uint64)
-    load().PTB_SegmentationStats(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 4)
-    return {"frames": int(out[0]), "routed": int(out[1]), "rank_tested": int(out[2]), "reflooded": int(out[3])}
+    """{"frames", "routed", "rank_tested", "reflooded", "routed_why"}: frames segmented by this device's engines since
+    the last call; of those, frames flooded again frame-wide, frames whose per-component floods needed the rank test,
+    frames flooded again per component with estimated frame-wide aging because they failed it, and the nonzero counts
+    of the frames flooded frame-wide by the first reason."""
+    out = np.zeros(11, dtype=np.uint64)
+    load().PTB_SegmentationStats(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 11)
+    why = ("pair_list_full", "first_test_only", "no_rank_slot", "too_many_pairs", "after_fusion", "no_reflood_slot",
+           "reflood_test_failed")
+    return {"frames": int(out[0]), "routed": int(out[1]), "rank_tested": int(out[2]), "reflooded": int(out[3]),
+            "routed_why": {k: int(out[4 + i]) for i, k in enumerate(why) if out[4 + i]}}
 
 
 def spline_coefficients(psf, lam=None):

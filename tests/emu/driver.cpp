@@ -1,7 +1,8 @@
 // Runs the segmentation kernels of one frame on the CPU (each CUDA thread a host thread, shim.h), every device array a
 // separate allocation so that AddressSanitizer reports any out-of-bounds access. Test harness only.
 // Usage: emu <in> <out> [mode]; in: int32 H, W, int64 threshold (2^-16 units), H * W int64 W1 values (2^-16 units);
-// out: H * W uint32 labels, H * W code bytes, then 5 uint32 (routed, rank-tested, re-flooded, suspect pairs, fits).
+// out: H * W uint32 labels, H * W code bytes, then 6 uint32 (routed, rank-tested, re-flooded, suspect pairs, fits, groups
+// of the re-flooded frame re-flooded in global memory).
 #include "shim.h"
 
 thread_local uint3 threadIdx;
@@ -98,7 +99,7 @@ int main(int argc, char** argv)
 	ws.rfGrp = Alloc<uint32_t>(static_cast<size_t>(kRefloodSlots) * 2 * kRefloodCap);
 	ws.rfOff = Alloc<uint32_t>(static_cast<size_t>(kRefloodSlots) * 2 * (kRefloodBuckets + 1));
 	ws.rfInfo = Alloc<uint32_t>(kRefloodSlots * 8);
-	ws.rfPix = Alloc<uint32_t>(static_cast<size_t>(kRefloodSlots) * g.N * 2);
+	ws.rfPix = Alloc<uint32_t>(static_cast<size_t>(kRefloodSlots) * g.N * kRfWords);
 	ws.rfGroups = Alloc<uint32_t>(ws.capComp);
 	ws.suspect = Alloc<uint4>(kSuspectCap); ws.capSuspect = kSuspectCap;
 	ws.rankOrder = Alloc<uint32_t>(kSuspectCap); ws.rankSlotOff = Alloc<uint32_t>(kRankSlots + 1);
@@ -148,6 +149,7 @@ int main(int argc, char** argv)
 	ExclusiveScan(ws.gRegOff, &ws.cnt->nmulti, 0, ws.capComp, ws.scanBlock, nullptr, nullptr);
 	fprintf(stderr, "components %u groups %u regions %u\n", ws.cnt->ncomp, ws.cnt->nmulti, ws.cnt->nregion);
 	emu::Launch(one, t256, GroupScatter, ws, 0);
+	uint32_t bigGroups = 0;
 	const int rank = strictMode == 0 ? 1 : 0;  // mode 2: the first test only
 	emu::Launch(one, t256, GroupFloodBox, ws, rank);
 	fprintf(stderr, "flooded: suspect pairs %u routed %u\n", ws.cnt->nsuspect, ws.cnt->nroute);
@@ -161,7 +163,18 @@ int main(int argc, char** argv)
 		emu::Launch(dim3(kRefloodSlots * 2), t1024, RefloodBucket, ws);
 		emu::Launch(one, t256, RefloodCounts, ws);
 		emu::Launch(one, dim3(kRfWarps * 32), RefloodBox, ws);
-		fprintf(stderr, "reflood: routed %u\n", ws.cnt->nroute);
+		// groups of the re-flooded frame too large for the shared-memory box (re-flooded in global memory)
+		for (uint32_t g = 0; g < ws.cnt->nrfgroup; ++g) {
+			const uint32_t m = ws.rfGroups[g];
+			int x0 = W, y0 = H, x1 = -1, y1 = -1;
+			for (uint32_t i = ws.gOff[m]; i < ws.gOff[m + 1]; ++i) {
+				const int y = static_cast<int>((ws.gPix[i] % (uint32_t)(H * W)) / W), x = static_cast<int>(ws.gPix[i] % W);
+				x0 = std::min(x0, x); x1 = std::max(x1, x); y0 = std::min(y0, y); y1 = std::max(y1, y);
+			}
+			const int bw = std::min(x1 + 1, W - 1) - std::max(x0 - 1, 0) + 1, bh = std::min(y1 + 1, H - 1) - std::max(y0 - 1, 0) + 1;
+			if (bw * bh > kBoxCap) { ++bigGroups; }
+		}
+		fprintf(stderr, "reflood: routed %u, groups re-flooded in global memory %u\n", ws.cnt->nroute, bigGroups);
 		for (uint32_t i = 0; i < std::min(ws.cnt->nsuspect, 8u); ++i) {
 			const uint4 r = ws.suspect[i];
 			fprintf(stderr, "  pair %u: f %u c %u w1z %u zmax %u counts %u %u\n", i, r.x, r.y, r.z, r.w, ws.rankCount[2 * i], ws.rankCount[2 * i + 1]);
@@ -183,8 +196,8 @@ int main(int argc, char** argv)
 	FILE* lf = fopen(argv[2], "wb");
 	fwrite(ws.lab, sizeof(uint32_t), P, lf);
 	fwrite(ws.code, 1, P, lf);
-	const uint32_t st[5] = {ws.cnt->nroute, ws.cnt->nslots, ws.cnt->nreflood, ws.cnt->nsuspect, ws.cnt->nfit};
-	fwrite(st, sizeof(uint32_t), 5, lf);
+	const uint32_t st[6] = {ws.cnt->nroute, ws.cnt->nslots, ws.cnt->nreflood, ws.cnt->nsuspect, ws.cnt->nfit, bigGroups};
+	fwrite(st, sizeof(uint32_t), 6, lf);
 	fclose(lf);
 	return 0;
 }

@@ -66,6 +66,7 @@ inline unsigned __ballot_sync(unsigned, int pred)
 	return b;
 }
 inline int __any_sync(unsigned m, int pred) { return __ballot_sync(m, pred) != 0; }
+inline int __all_sync(unsigned m, int pred) { return __ballot_sync(m, !pred) == 0; }
 inline int __popc(unsigned v) { return __builtin_popcount(v); }
 inline unsigned __vimax3_u32(unsigned a, unsigned b, unsigned c) { return std::max(a, std::max(b, c)); }
 inline int __ffs(int v) { return __builtin_ffs(v); }

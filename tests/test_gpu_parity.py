@@ -168,6 +168,22 @@ def test_detection_reflood_frames_bitwise(lib, orc):
     assert checked >= 1
 
 
+def test_detection_reflood_large_groups_bitwise(lib, orc):
+    """A frame at 0.15x its threshold fails the rank test with groups larger than the re-flood's shared-memory box:
+    those groups are flooded again in global memory (seven of them in this frame, counted by the CPU emulation of the
+    same kernels), the frame passes the per-element test and no frame-wide flood is needed; candidates bit for bit."""
+    import synth
+    s, _ = synth.stack("c2", frames=1, seed=21, size=(512, 512))
+    thr = 0.15 * synth.mad_threshold(orc.planes(s[0])[1])
+    lib.segmentation_stats()
+    a = lib.localization(s, thr, 0.0, 0, GAUSS_PARAMS)
+    stats = lib.segmentation_stats()
+    print(stats, a.shape)
+    assert stats["routed"] == 0 and stats["reflooded"] == 1, stats
+    b = orc.localization(s, thr, 0.0, 0, GAUSS_PARAMS)
+    assert a.shape == b.shape and np.array_equal(a, b)
+
+
 def test_detection_edge_cases(lib, orc):
     # black stack, empty output capacity, single plane, plateaus, tiny frames
     assert lib.localization(np.zeros((3, 12, 16), np.uint16), 0.0, 0.0, 0, GAUSS_PARAMS).shape[0] == 0
