@@ -184,6 +184,32 @@ def test_detection_reflood_large_groups_bitwise(lib, orc):
     assert a.shape == b.shape and np.array_equal(a, b)
 
 
+def test_detection_reflood_c4_frames_bitwise(lib, orc):
+    """The C4 benchmark stack (1500 x 512^2, up to 1500 emitters per frame): the frames that fail the rank test are
+    re-flooded, their groups too large for the shared-memory box in global memory, and none is flooded frame-wide;
+    every re-flooded frame's candidates equal the oracle's bit for bit."""
+    import synth
+    d, _ = synth.stack_cuda("c4", seed=4242)
+    host = d.cpu().numpy().view(np.uint16)
+    del d
+    thr = synth.mad_threshold(orc.planes(host[0])[1])
+    lib.segmentation_stats()
+    lib.localization(host, thr, 0.0, 0, GAUSS_PARAMS)
+    stats = lib.segmentation_stats()
+    print(stats)
+    assert stats["frames"] == host.shape[0] and stats["routed"] == 0 and stats["reflooded"] >= 1, stats
+    checked = 0
+    for f in range(host.shape[0]):
+        lib.segmentation_stats()
+        a = lib.localization(host[f:f + 1], thr, 0.0, 0, GAUSS_PARAMS)
+        if lib.segmentation_stats()["reflooded"] == 0:
+            continue
+        b = orc.localization(host[f:f + 1], thr, 0.0, 0, GAUSS_PARAMS)
+        assert a.shape == b.shape and np.array_equal(a, b), f
+        checked += 1
+    assert checked >= 1
+
+
 def test_detection_edge_cases(lib, orc):
     # black stack, empty output capacity, single plane, plateaus, tiny frames
     assert lib.localization(np.zeros((3, 12, 16), np.uint16), 0.0, 0.0, 0, GAUSS_PARAMS).shape[0] == 0
