@@ -40,7 +40,8 @@ constexpr uint32_t kRankSlots = 64u;
 constexpr uint32_t kSuspectCap = 16384u;
 constexpr uint32_t kPairsPerFrame = 512u;
 // Re-flood of the frames that fail the rank test: at most kRefloodSlots frames per chunk, each with at most
-// kRefloodCap domain pixels (their W1 values are sorted for the rank lookups); other frames are flooded frame-wide.
+// kRefloodCap domain pixels (their W1 values are grouped by value bucket for the rank lookups); other frames are
+// flooded frame-wide.
 constexpr uint32_t kRefloodSlots = 8u;
 constexpr uint32_t kRefloodCap = 65536u;
 constexpr uint32_t kRefloodBuckets = 32768u;  // value buckets of the rank lookups

@@ -12,8 +12,10 @@
 //      a whole frame and the counter is frame-global, which is the reference's process exactly;
 //   4. basin fusion (Segmentation2D.cpp:181-291) per group, then a second flood from one seed per basin;
 //   5. exactness check of every per-component flood (below): a first test per boundary pair, then the rank test of
-//      the pairs that fail it; a frame that fails both is flooded again as one unit with the frame-global counter
-//      (the strict process), so the labels always equal the reference's;
+//      the pairs that fail it; a frame that fails both is flooded again per component with estimated frame-wide
+//      aging and proven by a per-element test (the re-flood: shared-memory boxes, global memory for larger groups),
+//      and a frame that fails that too is flooded again as one unit with the frame-global counter (the strict
+//      process), so the labels always equal the reference's;
 //   6. exact integer region sums (W1 is an integer in 2^-16 units) and the surf > 4 filter, in label order.
 //
 // Why a per-component flood equals the frame-wide one, and when it may not. Labels only spread inside a component,
@@ -27,9 +29,10 @@
 // holds when c - W1(z) > T * 1e-7. So if every flooded pixel N and every neighbour z of N with another label satisfy
 // it, then (induction over the frame-wide flood's labelling order) every pixel receives its per-component label.
 // In 2^-16 units the test is (c - W1(z)) * 152 > T (2^-16 / 152 exceeds 1e-7 by 4e-10 per pop, which covers the
-// rounding of the FP64 keys, below 2e-11). About 3 % of the 1024 x 1024 benchmark frames have a pair failing it.
+// rounding of the FP64 keys, below 2e-11). About 4.5 % of the 1024 x 1024 benchmark frames have a pair failing it.
 // Those pairs get the rank test (SuspectCheck), which bounds the two aging terms by the frame's pixel counts above
-// and below the two W1 levels instead of by T; a frame failing that too is flooded again frame-wide. The rank test
+// and below the two W1 levels instead of by T; a frame failing that too is re-flooded (RefloodPlan .. RefloodBox)
+// and, failing the re-flood's test, flooded again frame-wide. The rank test
 // needs every pixel of the flood to be joined to a seed by a path that never falls below it, which holds for the
 // first flood (every local maximum is a seed) but not for the second flood of a basin fusion (one seed per basin):
 // there a pair failing the first test routes the frame directly.
