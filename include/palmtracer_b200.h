@@ -232,6 +232,12 @@ PTB_API void PTB_MleEvaluations(uint64_t* counts, int n);
  * counts: [chunks captured, chunks replayed, chunks launched directly] since the last call (up to n entries). */
 PTB_API void PTB_GraphStats(uint64_t* counts, int n);
 
+/* Input staging of the detection kernel (diagnostics, whole process): counts[0] = launches whose input tiles were
+ * copied by the tensor memory accelerator (one bulk tensor copy per tile; frames whose width is a multiple of 8 in a
+ * 16-byte aligned buffer, unless PTB_DETECT_TMA=0), counts[1] = launches staged with per-thread loads; launches issued
+ * since the last call (a replay of a captured launch chain is not counted again), up to n entries. */
+PTB_API void PTB_DetectStagingStats(uint64_t* counts, int n);
+
 /* FMA throughput probe of the current device (diagnostics): FLOP/s (2 per FMA) of FP64 (fp64 != 0) or FP32
  * arithmetic, timed with CUDA events over a grid of independent FMA chains; -1 on error. */
 PTB_API double PTB_MeasureFmaPeak(int fp64);

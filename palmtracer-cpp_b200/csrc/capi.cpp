@@ -400,6 +400,11 @@ PTB_API void PTB_MleEvaluations(uint64_t* counts, int n)
 	SumOverEngines(counts, n, [](ptb::Engine& e, uint64_t* v, int k) { e.MleEvaluations(v, k); });
 }
 
+PTB_API void PTB_DetectStagingStats(uint64_t* counts, int n)
+{
+	ptb::DetectStagingStats(counts, n);
+}
+
 PTB_API void PTB_GraphStats(uint64_t* counts, int n)
 {
 	SumOverEngines(counts, n, [](ptb::Engine& e, uint64_t* v, int k) { e.GraphStats(v, k); });

@@ -649,6 +649,10 @@ long long Engine::CompleteChunk(int slot, uint32_t* truncatedFrames)
 		SetError("internal capacity overflow");
 		return -1;
 	}
+	if (c.fault) {
+		SetError("the detection kernel's wait for its staged input tile ran out");
+		return -1;
+	}
 	segCounts_[1] += c.nroute;
 	segCounts_[2] += c.nslots;
 	segCounts_[3] += c.nreflood;

@@ -232,4 +232,7 @@ private:
 // [engines in the current device's pool, most engines leased at the same time] (diagnostics).
 void PoolStats(uint64_t* out, int n);
 
+// [detection launches staged by the TMA, by per-thread loads] since the last call, whole process (diagnostics).
+void DetectStagingStats(uint64_t* out, int n);
+
 }  // namespace ptb

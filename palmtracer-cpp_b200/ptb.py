@@ -16,7 +16,7 @@ COLS = 18
 EXPORTS = ["Localization", "Fitting", "Wavelett", "AutoThreshold", "Astigmatism3DEstimation", "PTB_LocalizationDevice",
            "PTB_SetSegmentationMode", "PTB_SetFitPrecision", "PTB_LastError", "PTB_KernelLaunchCount",
            "PTB_SetProfiling", "PTB_StageTimes", "PTB_MleEvaluations", "PTB_GraphStats", "PTB_SegmentationStats", "PTB_EnginePoolStats",
-           "PTB_MleMappings",
+           "PTB_MleMappings", "PTB_DetectStagingStats",
            "PTB_MeasureFmaPeak", "PTB_FittingDeviceNoAlloc",
            "PTB_ServerStart", "PTB_SubmitStack", "PTB_PollStack", "PTB_StackResult", "PTB_ServerStop", "PTB_ServerFuseStats",
            "PTB_TiffInfo", "PTB_TiffRead", "PTB_LocalizationTiff", "Tracking", "PTB_TrackingDevice", "PTB_SplineCoefficients"]
@@ -74,6 +74,8 @@ def load(path=LIB_PATH):
     L.PTB_TiffRead.argtypes = [ctypes.c_char_p, _u16p, _u64, _u64]
     L.PTB_LocalizationTiff.restype = _u64
     L.PTB_LocalizationTiff.argtypes = [ctypes.c_char_p, _f64p, _u64, _f64, _f64, _u64, _f64p]
+    L.PTB_DetectStagingStats.restype = None
+    L.PTB_DetectStagingStats.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
     L.PTB_GraphStats.restype = None
     L.PTB_GraphStats.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
     L.PTB_SegmentationStats.restype = None
@@ -279,6 +281,14 @@ def graph_stats():
     out = np.zeros(3, dtype=np.uint64)
     load().PTB_GraphStats(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 3)
     return {"captured": int(out[0]), "replayed": int(out[1]), "direct": int(out[2])}
+
+
+def detect_staging_stats():
+    """{"tma", "loads"}: detection launches (whole process) whose input tiles were staged by the tensor memory
+    accelerator and by per-thread loads, since the last call."""
+    out = np.zeros(2, dtype=np.uint64)
+    load().PTB_DetectStagingStats(out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), 2)
+    return {"tma": int(out[0]), "loads": int(out[1])}
 
 
 def segmentation_stats():

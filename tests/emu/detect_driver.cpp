@@ -66,8 +66,13 @@ int main(int argc, char** argv)
 	ws.cnt = Alloc<Counters>(1, 0);
 	ws.frameDom = Alloc<uint32_t>(B + 1, 0);
 	ws.frameSeeds = Alloc<uint32_t>(B + 1, 0);
+	// widths the TMA can describe take the TMA staging path (emulated: the same box copy with zero fill, then the
+	// kernel's own border replication), the others the per-thread loads, as on the GPU
+	CUtensorMap map;
+	std::memset(&map, 0, sizeof(map));
+	const int useTma = (W % 8) == 0 ? 1 : 0;
 	emu::Launch(dim3((W + TX - 1) / TX, (H + TY - 1) / TY, B), dim3(kThreads), DetectKernel,
-	            static_cast<const uint16_t*>(img), ws, thr);
+	            static_cast<const uint16_t*>(img), ws, thr, map, useTma);
 	const uint32_t nd = std::min(ws.cnt->ndom, ws.capDom), ns = std::min(ws.cnt->nseed, ws.capSeed);
 	std::sort(ws.dom, ws.dom + nd);
 	std::sort(ws.seeds, ws.seeds + ns);

@@ -68,6 +68,7 @@ inline unsigned __ballot_sync(unsigned, int pred)
 inline int __any_sync(unsigned m, int pred) { return __ballot_sync(m, pred) != 0; }
 inline int __all_sync(unsigned m, int pred) { return __ballot_sync(m, !pred) == 0; }
 inline int __popc(unsigned v) { return __builtin_popcount(v); }
+inline size_t __cvta_generic_to_shared(const void* p) { return reinterpret_cast<uintptr_t>(p); }
 inline unsigned __vimax3_u32(unsigned a, unsigned b, unsigned c) { return std::max(a, std::max(b, c)); }
 inline int __ffs(int v) { return __builtin_ffs(v); }
 inline int __clz(int v) { return v == 0 ? 32 : __builtin_clz(static_cast<unsigned>(v)); }

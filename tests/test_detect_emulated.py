@@ -6,7 +6,9 @@ access anywhere in it aborts. Its code bytes, the W1 of domain pixels, the domai
 counts must equal the oracle's W1 (ATrous.cpp:23-80 restated in oracle/pt_oracle.cpp) thresholded strictly and above
 1e-8, with seeds at the pixels not below any 3 x 3 neighbour (Segmentation2D.cpp:294-333, the frame surrounded by
 zeros). The shapes cover ragged last tiles in both directions, widths that do and do not allow the 16-byte staging
-loads, frames smaller than the halo and several frames; the stacks are full-range noise (sums up to the 2^32 limit
+loads, the widths that are multiples of 8 through the TMA staging path (its box copy emulated with the same zero fill,
+then the kernel's own replication of the nearest in-frame rows and columns), frames smaller than the halo and several
+frames; the stacks are full-range noise (sums up to the 2^32 limit
 of the level-2 taps) and C2 frames; threshold 0 makes most pixels domain.
 """
 import os
@@ -102,11 +104,12 @@ def _thresholds(orc, stack):
 CASES = [  # (H, W, frames, seed)
     (130, 112, 2, 1),   # a last tile row of 18 rows, one tile column short of full
     (300, 250, 1, 2),   # width not a multiple of 8: clamped 2-byte staging loads everywhere
-    (60, 400, 2, 3),    # width a multiple of 8: the interior tile column stages with 16-byte loads
+    (60, 400, 2, 3),    # width a multiple of 8: TMA staging (on the GPU), border tiles replicate edges
     (16, 336, 1, 4),    # one short tile row
     (29, 129, 1, 5),    # one row and one column past full tiles
     (3, 17, 2, 6),      # frames smaller than the 7-pixel halo in both directions
     (257, 113, 1, 7),   # a last tile row of 5 rows
+    (5, 8, 2, 8),       # the narrowest frames the TMA describes: its box reaches past every side
 ]
 
 

@@ -73,6 +73,32 @@ def test_detection_synthetic_bitwise(lib, orc, workload, frames, size, ratio):
     assert a.shape == b.shape and np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("h,w", [(5, 8), (40, 136), (300, 256), (61, 1032), (130, 112), (200, 333), (77, 250)])
+def test_detection_staging_paths_bitwise(lib, orc, h, w):
+    """Frames whose width is a multiple of 8 stage each tile's input box with one TMA bulk tensor copy (zero fill past
+    the frame, then the nearest in-frame rows and columns replicated in shared memory, as the reference clamps its
+    neighbour accesses); other widths stage with per-thread loads. Both give the oracle's candidates bit for bit, on
+    full-range noise and on C2 frames, and the staging counters show which path ran (each shape is new to the process,
+    so its chain is launched, not replayed)."""
+    import synth
+    rng = np.random.default_rng(h * 7919 + w)
+    stacks = [rng.integers(0, 65536, size=(2, h, w), dtype=np.uint16)]
+    if min(h, w) >= 64:
+        stacks.append(synth.stack("c2", frames=2, seed=h + w, size=(h, w))[0])
+    for s in stacks:
+        thr = synth.mad_threshold(orc.planes(s[0])[1])
+        for scale in (1.0, 0.0):
+            lib.detect_staging_stats()
+            a = lib.localization(s, thr * scale, 0.0, 0, GAUSS_PARAMS)
+            st = lib.detect_staging_stats()
+            b = orc.localization(s, thr * scale, 0.0, 0, GAUSS_PARAMS)
+            assert a.shape == b.shape and np.array_equal(a, b), (h, w, scale)
+            if w % 8 == 0:
+                assert st["tma"] >= 1 and st["loads"] == 0, st
+            else:
+                assert st["tma"] == 0 and st["loads"] >= 1, st
+
+
 @pytest.mark.parametrize("scale", [0.3, 0.1, 0.0])
 def test_detection_strict_mode_low_threshold_bitwise(lib, orc, scale):
     """Giant components: the frame-wide flood (strict mode) reproduces the reference exactly."""
