@@ -47,9 +47,9 @@ REF_FIT_MODE = 2  # the reference's own 5-parameter Gaussian fit, for the CPU ar
 FLOP_PER_PIXEL_LM = 71
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per frame of one launch, from ncu captures of smaller
 # chunks of the same workload, scaled by the frames a benchmark launch processes (traffic grows with the frames):
-# MleLmKernel<6> 127.38 MB and DetectKernel 251.74 MB over one 64-frame chunk.
+# MleLmKernel<6> 127.38 MB and DetectKernel 252.41 MB over one 64-frame chunk.
 LM_DRAM_BYTES_PER_FRAME = 127.38e6 / 64
-DETECT_DRAM_BYTES_PER_FRAME = 251.74e6 / 64
+DETECT_DRAM_BYTES_PER_FRAME = 252.41e6 / 64
 RATIO = 0.0
 PER_PLANE = 8192
 # Serving mix (C5): Poisson arrivals at 20 stacks/s of square frames from {128, 256, 512, 1024, 2048}, lengths 1-500,

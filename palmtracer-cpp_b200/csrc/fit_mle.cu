@@ -278,42 +278,46 @@ template <typename T, int KIND>
 __device__ __forceinline__ void Accumulate(T d, T bg, T I, T psf, const T P1[3], const T P2[6], T& D, T G[5], T Hm[15], T Fm[15])
 {
 	const T mu = max(bg + I * psf, T(1e-6));
+	if constexpr (KIND == kFinal) {
+		// FP64: log(mu / d) = -log(d * (1 / mu)), the reciprocal shared with the Fisher weights (one FP64 division
+		// per pixel instead of two; the two forms differ by an ulp of the ratio)
+		const T rmu = T(1) / mu;
+		D += d > T(0) ? T(2) * (mu - d + d * Ln<T>(d * rmu)) : T(2) * mu;
+		const T gk[5] = {T(1), psf, I * P1[0], I * P1[1], I * P1[2]};
+		int q = 0;
+		#pragma unroll
+		for (int a = 0; a < 5; ++a) {
+			const T wa = rmu * gk[a];
+			#pragma unroll
+			for (int b = a; b < 5; ++b) { Fm[q++] += wa * gk[b]; }
+		}
+		return;
+	}
 	D += d > T(0) ? T(2) * (mu - d - d * Ln<T>(Div<T>(mu, d))) : T(2) * mu;
 	if constexpr (KIND != kDevOnly) {
 		const T gk[5] = {T(1), psf, I * P1[0], I * P1[1], I * P1[2]};
 		const T rmu = Div<T>(T(1), mu);
-		if constexpr (KIND == kFinal) {
-			int q = 0;
+		const T w1 = T(2) * (T(1) - d * rmu);
+		const T w2 = KIND == kExact ? T(2) * d * rmu * rmu : T(2) * rmu;
+		int q = 0;
+		#pragma unroll
+		for (int a = 0; a < 5; ++a) {
+			G[a] += w1 * gk[a];
+			const T wa = w2 * gk[a];
 			#pragma unroll
-			for (int a = 0; a < 5; ++a) {
-				const T wa = rmu * gk[a];
-				#pragma unroll
-				for (int b = a; b < 5; ++b) { Fm[q++] += wa * gk[b]; }
-			}
+			for (int b = a; b < 5; ++b) { Hm[q++] += wa * gk[b]; }
 		}
-		else {
-			const T w1 = T(2) * (T(1) - d * rmu);
-			const T w2 = KIND == kExact ? T(2) * d * rmu * rmu : T(2) * rmu;
-			int q = 0;
-			#pragma unroll
-			for (int a = 0; a < 5; ++a) {
-				G[a] += w1 * gk[a];
-				const T wa = w2 * gk[a];
-				#pragma unroll
-				for (int b = a; b < 5; ++b) { Hm[q++] += wa * gk[b]; }
-			}
-			if constexpr (KIND == kExact) {
-				// d2mu in the packed upper triangle: (I, x) = Px, (I, y) = Py, (I, s) = Ps, (x, x) = I Pxx, ...
-				Hm[6] += w1 * P1[0];
-				Hm[7] += w1 * P1[1];
-				Hm[8] += w1 * P1[2];
-				Hm[9] += w1 * I * P2[0];
-				Hm[10] += w1 * I * P2[1];
-				Hm[11] += w1 * I * P2[2];
-				Hm[12] += w1 * I * P2[3];
-				Hm[13] += w1 * I * P2[4];
-				Hm[14] += w1 * I * P2[5];
-			}
+		if constexpr (KIND == kExact) {
+			// d2mu in the packed upper triangle: (I, x) = Px, (I, y) = Py, (I, s) = Ps, (x, x) = I Pxx, ...
+			Hm[6] += w1 * P1[0];
+			Hm[7] += w1 * P1[1];
+			Hm[8] += w1 * P1[2];
+			Hm[9] += w1 * I * P2[0];
+			Hm[10] += w1 * I * P2[1];
+			Hm[11] += w1 * I * P2[2];
+			Hm[12] += w1 * I * P2[3];
+			Hm[13] += w1 * I * P2[4];
+			Hm[14] += w1 * I * P2[5];
 		}
 	}
 }
@@ -1245,9 +1249,10 @@ __global__ void __launch_bounds__(kThreads) MlePolishKernel(FitImages fi,
 }
 
 // FP64 deviance, Fisher information and CRLB at the polished theta; writes the output row. Shared memory per thread:
-// the FP64 column factors (3 roi doubles).
+// the FP64 column factors (3 roi doubles). Mode 6 is held to 128 registers (8 blocks of 64 threads per SM), which it
+// fits without spilling; modes 7 and 8 keep the compiler's own allocation (a bound spills them).
 template <int MODEL>
-__global__ void __launch_bounds__(kThreads) MleFinalKernel(FitImages fi,
+__global__ void __launch_bounds__(kThreads, MODEL == 6 ? 8 : 0) MleFinalKernel(FitImages fi,
                                                            const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
                                                            MleParams mp, double* rows)
 {
