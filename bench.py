@@ -72,17 +72,32 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampler running during the timed region."""
+    """nvidia-smi sampler running during the timed region: started, and waited for until it has printed its first
+    sample (nvidia-smi takes a fraction of a second to start), before the timed region; mark() at the start of the
+    timed region, and stop() keeps the samples taken after it."""
 
     def __init__(self, index):
         self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.skip = 0
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+                                          "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+        t0 = time.perf_counter()
+        while self.proc is not None and self._lines() == 0 and time.perf_counter() - t0 < 5.0 and self.proc.poll() is None:
+            time.sleep(0.02)
+
+    def _lines(self):
+        with open(self.file.name) as f:
+            return sum(1 for line in f if line.endswith("\n"))
+
+    def mark(self):
+        """Samples printed so far predate the timed region."""
+        if self.proc is not None:
+            self.skip = self._lines()
 
     def stop(self):
         if self.proc is None:
@@ -96,7 +111,10 @@ class Clocks:
         self.file.seek(0)
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.file.read().splitlines():
+        lines = self.file.read().splitlines()
+        if len(lines) > self.skip:
+            lines = lines[self.skip:]
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -600,6 +618,7 @@ def main():
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     counts = []
     torch.cuda.synchronize()
+    clocks.mark()
     for e0, e1 in ev:
         e0.record(stream)
         counts.append(step())

@@ -338,12 +338,15 @@ __global__ void __launch_bounds__(kThreads) DetectKernel(const uint16_t* __restr
 	}
 	__syncthreads();
 	{
+		// V1 columns outside the frame (the first clo and those after chi) take the nearest in-frame column's value;
+		// only those columns are visited
 		const int clo = max(0, 5 - x0), chi = min(kPV - 1, W - 1 - x0 + 5);
-		if (clo > 0 || chi < kPV - 1) {
-			for (int idx = tid; idx < kRows1 * kPV; idx += kThreads) {
-				const int r = idx / kPV, i = idx - r * kPV;
-				if (i < clo) { v1[r * kPV + i] = v1[r * kPV + clo]; }
-				else if (i > chi) { v1[r * kPV + i] = v1[r * kPV + chi]; }
+		const int ncol = clo + (kPV - 1 - chi);
+		if (ncol > 0) {
+			for (int idx = tid; idx < kRows1 * ncol; idx += kThreads) {
+				const int r = idx / ncol, j = idx - r * ncol;
+				const int i = j < clo ? j : chi + 1 + (j - clo);
+				v1[r * kPV + i] = v1[r * kPV + (j < clo ? clo : chi)];
 			}
 			__syncthreads();
 		}

@@ -1161,9 +1161,10 @@ __global__ void __launch_bounds__(kThreads) MleLmKernel(FitImages fi,
 // Persistent FP32 Newton polish (WarpQueue), the steps of Polish() as a per-ROI state machine: each pass evaluates
 // the deviance, gradient and exact Hessian once per busy ROI - at the LM result of a new candidate or at a trial
 // point - and then accepts, halves or ends. L lanes per ROI as in the LM. Shared memory per ROI slot: the photons and
-// the factor tables with second derivatives (SlotFloats, NF = 6).
+// the factor tables with second derivatives (SlotFloats, NF = 6). Mode 6 with a thread per ROI is held to 128
+// registers (8 blocks of 64 threads per SM instead of 6 at its own 150), which it fits without spilling.
 template <int MODEL, int L>
-__global__ void __launch_bounds__(kThreads) MlePolishKernel(FitImages fi,
+__global__ void __launch_bounds__(kThreads, MODEL == 6 && L == 1 ? 8 : 0) MlePolishKernel(FitImages fi,
                                                             const Cand* __restrict__ cands, const uint32_t* nptr, uint32_t nconst,
                                                             MleParams mp, double* rows)
 {
