@@ -86,6 +86,7 @@ struct Counters {
 	uint32_t nrfgroup;  // multi-label groups of the frames given a re-flood slot (listed in rfGroups)
 	uint32_t routeWhy[7];  // frames flooded frame-wide, by the first reason (RouteReason)
 	uint32_t fault;        // a kernel's bounded wait ran out (its results are void; the call fails)
+	uint32_t boxNext;      // work queue of the shared-memory group floods: next multi-label group to take
 };
 
 // Why a frame is flooded again frame-wide (diagnostics, counted per frame by the first reason).

@@ -442,23 +442,35 @@ __global__ void GroupScatter(Workspace ws, int strict)
 {
 	if (strict == 2 && ws.cnt->nroute == 0) { return; }
 	const uint32_t nd = min(ws.cnt->ndom, ws.capDom);
-	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nd; k += gridDim.x * blockDim.x) {
-		const uint32_t p = ws.dom[k];
-		const bool seed = (ws.code[p] & kSeed) != 0;
-		int m;
-		if (strict) {
-			m = Decompose(p, ws.g).f;
-			if (strict == 2 && ws.frameRoute[m] == 0) { continue; }
-			if (!seed) { ws.lab[p] = 0u; }
+	const int lane = threadIdx.x & 31;
+	PTB_WARP_LOOP(k, nd)
+	{
+		uint32_t p = 0;
+		int m = -1;
+		if (k < nd) {
+			p = ws.dom[k];
+			const bool seed = (ws.code[p] & kSeed) != 0;
+			if (strict) {
+				const int f = Decompose(p, ws.g).f;
+				if (strict != 2 || ws.frameRoute[f] != 0) {
+					if (!seed) { ws.lab[p] = 0u; }
+					m = f;
+				}
+			}
+			else {
+				const uint32_t c = CompOf(ws.par, p);
+				const uint32_t nroot = ws.compNRoot[c], r = ws.compRegion[c];
+				if (!seed) { ws.lab[p] = nroot == 1 ? r + 1 : 0u; }
+				m = nroot >= 2 ? static_cast<int>(r) : -1;
+			}
 		}
-		else {
-			const uint32_t c = CompOf(ws.par, p);
-			const uint32_t nroot = ws.compNRoot[c], r = ws.compRegion[c];
-			if (!seed) { ws.lab[p] = nroot == 1 ? r + 1 : 0u; }
-			m = nroot >= 2 ? static_cast<int>(r) : -1;
-		}
-		if (m < 0) { continue; }
-		ws.gPix[ws.gOff[m] + atomicAdd(ws.gCurPix + m, 1u)] = p;
+		// the group's pixel slots: one atomic per group and warp (consecutive domain pixels mostly share their group)
+		const unsigned peers = __match_any_sync(0xffffffffu, m);
+		const int leader = __ffs(peers) - 1;
+		uint32_t at = 0;
+		if (m >= 0 && lane == leader) { at = atomicAdd(ws.gCurPix + m, static_cast<uint32_t>(__popc(peers))); }
+		at = __shfl_sync(0xffffffffu, at, leader) + static_cast<uint32_t>(__popc(peers & ((1u << lane) - 1u)));
+		if (m >= 0) { ws.gPix[ws.gOff[m] + at] = p; }
 	}
 	const uint32_t ns = min(ws.cnt->nseed, ws.capSeed);
 	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ns; k += gridDim.x * blockDim.x) {
@@ -816,7 +828,13 @@ __global__ void __launch_bounds__(kBoxWarps * 32) GroupFloodBox(Workspace ws, in
 	const int lane = threadIdx.x & 31;
 	const Geometry& geo = ws.g;
 	const uint32_t n = ws.cnt->nmulti;
-	for (uint32_t m = blockIdx.x * kBoxWarps + threadIdx.x / 32; m < n; m += gridDim.x * kBoxWarps) {
+	// each warp takes the next group from a work queue when its previous one is done: group floods vary in length,
+	// and the CTAs beyond the resident ones (the box staging limits an SM to a few) find little left
+	for (;;) {
+		uint32_t m = 0;
+		if (lane == 0) { m = atomicAdd(&ws.cnt->boxNext, 1u); }
+		m = __shfl_sync(0xffffffffu, m, 0);
+		if (m >= n) { break; }
 		const uint32_t off = ws.gOff[m], nPix = ws.gOff[m + 1] - off;
 		const uint32_t nSeeds = ws.gSeedOff[m + 1] - ws.gSeedOff[m];
 		uint32_t* seeds = ws.gSeed + ws.gSeedOff[m];

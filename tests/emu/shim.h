@@ -65,6 +65,15 @@ inline unsigned __ballot_sync(unsigned, int pred)
 	emu::wsync();
 	return b;
 }
+template <class T> inline unsigned __match_any_sync(unsigned, T v)
+{
+	emu::xbuf[threadIdx.x] = emu::bits(v);
+	emu::wsync();
+	unsigned b = 0;
+	for (int l = 0; l < 32; ++l) { if (emu::xbuf[emu::wid() * 32 + l] == emu::bits(v)) { b |= 1u << l; } }
+	emu::wsync();
+	return b;
+}
 inline int __any_sync(unsigned m, int pred) { return __ballot_sync(m, pred) != 0; }
 inline int __all_sync(unsigned m, int pred) { return __ballot_sync(m, !pred) == 0; }
 inline int __popc(unsigned v) { return __builtin_popcount(v); }
