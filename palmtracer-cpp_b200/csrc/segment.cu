@@ -123,11 +123,26 @@ __device__ void Unite(uint32_t* par, uint32_t a, uint32_t b)
 	}
 }
 
+// Component of a domain pixel once the components are enumerated; called only by kernels that do not write par, so
+// its reads take the read-only cached path.
 __device__ __forceinline__ uint32_t CompOf(const uint32_t* par, uint32_t p)
 {
-	const uint32_t x = __ldcg(par + p);
+	const uint32_t x = __ldg(par + p);
 	if (x & kCompTag) { return x & ~kCompTag; }
-	return __ldcg(par + x) & ~kCompTag;
+	return __ldg(par + x) & ~kCompTag;
+}
+
+// Find for the flatten pass, through the SM's L1: during the flatten a parent only ever changes to one of its
+// ancestors (the root) and roots do not change, so a stale cached parent is still an ancestor and the walk still ends
+// at the root; the pixels of a CTA mostly walk the same chains.
+__device__ __forceinline__ uint32_t FindCached(const uint32_t* par, uint32_t x)
+{
+	uint32_t p = __ldca(par + x);
+	while (p != x) {
+		x = p;
+		p = __ldca(par + x);
+	}
+	return x;
 }
 
 // 8-connectivity decision tree over the raster-earlier neighbours a = (y-1, x-1), b = (y-1, x), c = (y-1, x+1),
@@ -183,7 +198,7 @@ __global__ void CclFlatten(Workspace ws)
 	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
 	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
 		const uint32_t p = ws.dom[k];
-		ws.par[p] = Find(ws.par, p);
+		ws.par[p] = FindCached(ws.par, p);
 	}
 }
 
