@@ -32,7 +32,6 @@ enum FitMode : int { kNone = 0, kG2Fixed = 1, kG2Sigma = 2, kG3Fixed = 3, kG3The
 constexpr uint8_t kDomain = 1;  // thresholded potential > 1e-8: the watershed floods it
 constexpr uint8_t kSeed = 2;    // local maximum of the thresholded potential
 constexpr int kDirShift = 2;    // bits 2..4: raster-earlier seed neighbour a seed inherits its label from (0 = root)
-constexpr uint8_t kUnion = 32;  // bit 5: the pixel joins two union-find trees (set by CclInit for CclUnion)
 
 // Rank test of the per-component floods: at most kRankSlots frames per chunk, kSuspectCap boundary pairs per chunk
 // and kPairsPerFrame per frame (a frame beyond these limits is flooded again frame-wide instead).
@@ -87,6 +86,7 @@ struct Counters {
 	uint32_t routeWhy[7];  // frames flooded frame-wide, by the first reason (RouteReason)
 	uint32_t fault;        // a kernel's bounded wait ran out (its results are void; the call fails)
 	uint32_t boxNext;      // work queue of the shared-memory group floods: next multi-label group to take
+	uint32_t nunion;       // domain pixels that join two union-find trees (listed in lab for the union pass)
 };
 
 // Why a frame is flooded again frame-wide (diagnostics, counted per frame by the first reason).

@@ -169,24 +169,46 @@ __device__ __forceinline__ void EarlierNeighbours(const Workspace& ws, uint32_t 
 	else if (d) { link = p - 1; }
 }
 
+// Grid-stride loop in whole warps: every lane of a warp runs the same iterations (k may be >= n on the last one), so
+// warp-wide collectives are safe inside.
+#define PTB_WARP_LOOP(k, n)                                                                                        \
+	for (uint32_t k##Base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u, k = k##Base + (threadIdx.x & 31u); \
+	     k##Base < (n); k##Base += gridDim.x * blockDim.x, k = k##Base + (threadIdx.x & 31u))
+
+// Links every domain pixel to one raster-earlier neighbour and lists the few that join two trees (most pixels have
+// one raster-earlier link at most) for CclUnion, one atomic per warp. The list lives in lab, which nothing reads
+// before the seed labels and the group scatter have written every domain pixel's label.
 __global__ void CclInit(Workspace ws)
 {
 	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
-	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-		const uint32_t p = ws.dom[k];
-		uint32_t link, extra;
-		EarlierNeighbours(ws, p, link, extra);
-		ws.par[p] = link;
-		if (extra != p) { ws.code[p] = static_cast<uint8_t>(ws.code[p] | kUnion); }  // only this thread writes p's byte
+	const int lane = threadIdx.x & 31;
+	PTB_WARP_LOOP(k, n)
+	{
+		uint32_t p = 0;
+		bool join = false;
+		if (k < n) {
+			p = ws.dom[k];
+			uint32_t link, extra;
+			EarlierNeighbours(ws, p, link, extra);
+			ws.par[p] = link;
+			join = extra != p;
+		}
+		const unsigned m = __ballot_sync(0xffffffffu, join);
+		if (m != 0u) {
+			uint32_t at = 0;
+			if (lane == 0) { at = atomicAdd(&ws.cnt->nunion, static_cast<uint32_t>(__popc(m))); }
+			at = __shfl_sync(0xffffffffu, at, 0);
+			if (join) { ws.lab[at + static_cast<uint32_t>(__popc(m & ((1u << lane) - 1u)))] = p; }
+		}
 	}
 }
 
+// The second union of the listed pixels (at most one per domain pixel, so the list fits lab).
 __global__ void CclUnion(Workspace ws)
 {
-	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
+	const uint32_t n = ws.cnt->nunion;
 	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-		const uint32_t p = ws.dom[k];
-		if (!(ws.code[p] & kUnion)) { continue; }  // most pixels have one raster-earlier link at most
+		const uint32_t p = ws.lab[k];
 		uint32_t link, extra;
 		EarlierNeighbours(ws, p, link, extra);
 		Unite(ws.par, p, extra);
@@ -203,12 +225,6 @@ __global__ void CclFlatten(Workspace ws)
 }
 
 // Components: enumerate roots and tag par[root] with the component id.
-// Grid-stride loop in whole warps: every lane of a warp runs the same iterations (k may be >= n on the last one), so
-// warp-wide collectives are safe inside.
-#define PTB_WARP_LOOP(k, n)                                                                                        \
-	for (uint32_t k##Base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u, k = k##Base + (threadIdx.x & 31u); \
-	     k##Base < (n); k##Base += gridDim.x * blockDim.x, k = k##Base + (threadIdx.x & 31u))
-
 // Component ids: one atomic per block and grid-stride step (roots are few, but a single counter hit by every warp
 // serialises at the L2).
 __global__ void __launch_bounds__(kThreads) CompEnumerate(Workspace ws)
