@@ -132,17 +132,21 @@ __device__ __forceinline__ uint32_t CompOf(const uint32_t* par, uint32_t p)
 	return __ldg(par + x) & ~kCompTag;
 }
 
-// Find for the flatten pass, through the SM's L1: during the flatten a parent only ever changes to one of its
-// ancestors (the root) and roots do not change, so a stale cached parent is still an ancestor and the walk still ends
-// at the root; the pixels of a CTA mostly walk the same chains.
-__device__ __forceinline__ uint32_t FindCached(const uint32_t* par, uint32_t x)
+// Component of domain pixel p once the roots carry their component ids (CompEnumerate): p's union-find chain walked
+// to its tagged root through the SM's L1, and p then pointed at the root itself, as CompOf expects. While this runs a
+// parent only ever changes to the root and the roots do not change, so a stale cached parent is still an ancestor
+// and the walk still ends at the root; the pixels of a CTA mostly walk the same chains. A root left untagged (the
+// component list overflowed; the chunk is redone) gives 0xffffffff.
+__device__ __forceinline__ uint32_t CompWalk(uint32_t* par, uint32_t p)
 {
-	uint32_t p = __ldca(par + x);
-	while (p != x) {
-		x = p;
-		p = __ldca(par + x);
+	uint32_t x = p, v = __ldca(par + p);
+	while (!(v & kCompTag) && v != x) {
+		x = v;
+		v = __ldca(par + x);
 	}
-	return x;
+	if (!(v & kCompTag)) { return 0xffffffffu; }
+	if (x != p) { par[p] = x; }
+	return v & ~kCompTag;
 }
 
 // 8-connectivity decision tree over the raster-earlier neighbours a = (y-1, x-1), b = (y-1, x), c = (y-1, x+1),
@@ -215,15 +219,6 @@ __global__ void CclUnion(Workspace ws)
 	}
 }
 
-__global__ void CclFlatten(Workspace ws)
-{
-	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
-	for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-		const uint32_t p = ws.dom[k];
-		ws.par[p] = FindCached(ws.par, p);
-	}
-}
-
 // Components: enumerate roots and tag par[root] with the component id.
 // Component ids: one atomic per block and grid-stride step (roots are few, but a single counter hit by every warp
 // serialises at the L2).
@@ -270,7 +265,7 @@ __global__ void CompCount(Workspace ws)
 	const uint32_t n = min(ws.cnt->ndom, ws.capDom);
 	PTB_WARP_LOOP(k, n)
 	{
-		const uint32_t c = k < n ? CompOf(ws.par, ws.dom[k]) : 0xffffffffu;
+		const uint32_t c = k < n ? CompWalk(ws.par, ws.dom[k]) : 0xffffffffu;
 		bool head;
 		const uint32_t count = RunSum<uint32_t>(c, 1u, head);
 		if (head && c != 0xffffffffu) { atomicAdd(ws.compSize + c, count); }
@@ -1891,12 +1886,11 @@ bool LaunchSegment(const Workspace& ws, double ratio, int strict, uint32_t maxPo
 	bool ok = true;
 	CclInit<<<kGrid, kThreads, 0, st>>>(ws);
 	CclUnion<<<kGrid, kThreads, 0, st>>>(ws);
-	CclFlatten<<<kGrid, kThreads, 0, st>>>(ws);
 	CompEnumerate<<<kGrid, kThreads, 0, st>>>(ws);
 	CompCount<<<kGrid, kThreads, 0, st>>>(ws);
 	SeedParent<<<kGrid, kThreads, 0, st>>>(ws);
 	RowCount<<<kGrid, kThreads, 0, st>>>(ws);
-	CountLaunch(7);
+	CountLaunch(6);
 	ok = ok && PTB_LAUNCHED();
 	const uint32_t rows = static_cast<uint32_t>(g.B) * static_cast<uint32_t>(g.H);
 	ok = ok && ExclusiveScan(ws.rowcnt, nullptr, rows, rows, ws.scanBlock, &ws.cnt->nregion, st);

@@ -136,7 +136,6 @@ int main(int argc, char** argv)
 	const dim3 one(1), t256(256), t1024(1024), t64(64);
 	emu::Launch(one, t256, CclInit, ws);
 	emu::Launch(one, t256, CclUnion, ws);
-	emu::Launch(one, t256, CclFlatten, ws);
 	emu::Launch(one, t256, CompEnumerate, ws);
 	emu::Launch(one, t256, CompCount, ws);
 	emu::Launch(one, t256, SeedParent, ws);
