@@ -81,3 +81,16 @@ def test_emulated_segmentation_matches_oracle(emulator, orc):
         for k in seen:
             seen[k] += stats[k]
     assert all(v >= 1 for v in seen.values()), seen
+
+
+def test_emulated_segmentation_noise_frame(emulator, orc):
+    """Full-range noise at and just above threshold 0: about half the pixels join the domain in components of
+    arbitrary shape, so many pixels join two union-find trees (the union pass's list), the chains walked by the
+    component count are long, and most frames' groups are large."""
+    rng = np.random.default_rng(5)
+    frame = rng.integers(0, 65536, size=(150, 230), dtype=np.uint16)
+    w1 = orc.planes(frame)[1]
+    for thr in (0.0, float(np.quantile(w1[w1 > 0], 0.5))):
+        diff, stats = _run(emulator, orc, frame, thr, 0)
+        print("thr", thr, stats, "label differences", diff)
+        assert diff == 0, (thr, stats)
